@@ -1,0 +1,517 @@
+"""CPU oracle of the bake's plain particle-erosion path (test infrastructure).
+
+Only the tests, the smoke check and the benchmark's CPU-baseline leg import
+this module; the product never does.  It drives the C restatement in
+``erosion_oracle.c`` with the reference's own control flow, in numpy:
+
+* :class:`OracleState` -- ``ErosionState`` (bake/globe/erosion/maps.py:56-191)
+* :func:`spawn_particles` -- maps.py:793-833
+* :func:`run_iteration` -- maps.py:839-1047: rain spawns by inverse CDF on
+  sorted uniforms, pending re-injection, packed samples, the chunk loop
+  (trace on frozen samples, serial apply on the live terrain), fold, EMA
+* :func:`thermal_erosion` -- maps.py:1050-1085
+* :func:`apply_uplift` -- maps.py:1088-1147 (mean-free over the active interior)
+* :func:`start_replay` -- maps.py:1159-1213
+* :func:`hold_datum` -- maps.py:1446-1508
+* :func:`step` -- maps.py:1516-1617, plain path
+
+Every random number comes from ``params.rng("erosion", iteration)`` exactly
+as in the reference, so a GPU run and this oracle see the same spawns.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liberosion_oracle.so"
+
+MASK_OUTSIDE, MASK_ACTIVE, MASK_FROZEN = 0, 1, 2
+DEATH_NAMES = ("age", "ocean", "exit", "pit", "evap", "stop")
+SPREAD, LAKE_PARKS = 8, 8
+NS = 16
+S_SURF, S_SED, S_BASE = 0, 7, 15
+
+
+def build() -> Path:
+    """Compile the C oracle in place (gcc) and return the library path."""
+    src = HERE / "erosion_oracle.c"
+    if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_change_list_cap.restype = ctypes.c_int
+        L.orc_change_list_cap.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.orc_set_threads(int(os.environ.get("PGE_ORACLE_THREADS", os.cpu_count() or 1)))
+        _LIB = L
+    return _LIB
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+class TraceParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
+        "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
+        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor")] + [
+        (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F")]
+
+
+class ApplyParams(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("iter_erode", "iter_deposit", "fan_slope", "dep_floor", "offshore_writeoff")] + [
+        ("use_erode_cap", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+def _p(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"], "oracle arrays must be contiguous"
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def change_list_cap(max_steps: int) -> int:
+    return int(lib().orc_change_list_cap(int(max_steps), 0))
+
+
+# --------------------------------------------------------------------------
+# geometry wrappers (golden-vector tests)
+# --------------------------------------------------------------------------
+def to_sphere(face, u, v) -> np.ndarray:
+    face = np.ascontiguousarray(face, np.int32)
+    u = np.ascontiguousarray(u, np.float64)
+    v = np.ascontiguousarray(v, np.float64)
+    out = np.empty((face.size, 3))
+    lib().orc_to_sphere_batch(ctypes.c_int64(face.size), _p(face), _p(u), _p(v), _p(out))
+    return out
+
+
+def from_sphere(xyz):
+    xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    n = xyz.shape[0]
+    f = np.empty(n, np.int32)
+    u = np.empty(n)
+    v = np.empty(n)
+    lib().orc_from_sphere_batch(ctypes.c_int64(n), _p(xyz), _p(f), _p(u), _p(v))
+    return f, u, v
+
+
+def transfer_velocity(face, u, v, a, b):
+    face = np.ascontiguousarray(face, np.int32)
+    uvab = np.ascontiguousarray(np.stack([u, v, a, b], -1), np.float64)
+    n = face.size
+    f2 = np.empty(n, np.int32)
+    out = np.empty((n, 4))
+    lib().orc_transfer_velocity_batch(ctypes.c_int64(n), _p(face), _p(uvab), _p(f2), _p(out))
+    return f2, out[:, 0], out[:, 1], out[:, 2], out[:, 3]
+
+
+# --------------------------------------------------------------------------
+# state
+# --------------------------------------------------------------------------
+def _cu(ep, name, unit):
+    return float(getattr(ep, name)) / float(unit)
+
+
+@dataclass
+class OracleState:
+    height: np.ndarray
+    sediment: np.ndarray
+    discharge: np.ndarray
+    momentum: np.ndarray
+    hardness: np.ndarray
+    precip: np.ndarray
+    evap: np.ndarray
+    uplift: np.ndarray
+    mask: np.ndarray
+    metric: np.ndarray
+    metric_inv: np.ndarray
+    N: int
+    H: int
+    spherical: bool
+    height_unit_m: float
+    grid: object = None
+    base: np.ndarray = None
+    pending: np.ndarray = None
+    iteration: int = 0
+    land_target: float | None = None
+    deposit_on_exit: bool = False
+    samp: np.ndarray = field(default=None, repr=False)
+    acc: np.ndarray = field(default=None, repr=False)
+    disch_track: np.ndarray = field(default=None, repr=False)
+    mom_track: np.ndarray = field(default=None, repr=False)
+
+    def __post_init__(self):
+        F, NE = self.height.shape[0], self.height.shape[1]
+        z = lambda *s: np.zeros((F, NE, NE) + s, dtype=np.float64)
+        self.samp = np.zeros((F, NE, NE, NS), np.float32) if self.samp is None else self.samp
+        self.acc = z() if self.acc is None else self.acc
+        self.pending = z() if self.pending is None else self.pending
+        self.base = z() if self.base is None else self.base
+        self.disch_track = z() if self.disch_track is None else self.disch_track
+        self.mom_track = z(2) if self.mom_track is None else self.mom_track
+
+    @classmethod
+    def from_world(cls, world, params) -> "OracleState":
+        """Global six-face state from a synthetic world (metres -> cell units),
+        as ``ErosionState.from_grid`` builds it."""
+        grid = world.grid
+        unit = grid.cell_size_m
+        F, NE = 6, grid.NE
+        c = lambda a, dt: np.ascontiguousarray(np.asarray(a), dtype=dt)
+        return cls(
+            height=c(world.bedrock, np.float64) / unit,
+            sediment=np.zeros((F, NE, NE)),
+            discharge=np.zeros((F, NE, NE)),
+            momentum=np.zeros((F, NE, NE, 2)),
+            hardness=c(world.hardness, np.float32),
+            precip=c(world.precip, np.float32),
+            evap=c(world.evap, np.float32),
+            uplift=c(world.uplift, np.float64) / unit,
+            mask=np.ones((F, NE, NE), np.uint8),
+            metric=np.ascontiguousarray(np.broadcast_to(grid.metric_face, (F, NE, NE, 3)), np.float32),
+            metric_inv=np.ascontiguousarray(np.broadcast_to(grid.metric_inv_face, (F, NE, NE, 3)), np.float32),
+            N=grid.N, H=grid.H, spherical=True, height_unit_m=unit, grid=grid,
+            land_target=float(world.land_fraction),
+        )
+
+    @property
+    def F(self):
+        return self.height.shape[0]
+
+    @property
+    def NE(self):
+        return self.height.shape[1]
+
+    @property
+    def interior(self):
+        H, N = self.H, self.N
+        return (slice(None), slice(H, H + N), slice(H, H + N))
+
+    def surface(self):
+        return self.height + self.sediment
+
+    def total_mass(self) -> float:
+        act = self.mask[self.interior] == MASK_ACTIVE
+        return float(np.sum((self.height + self.sediment + self.pending)[self.interior][act]))
+
+    def pack(self):
+        n = self.height.size
+        lib().orc_pack(ctypes.c_int64(n), _p(self.samp), _p(self.height), _p(self.sediment), _p(self.discharge),
+                       _p(self.momentum), _p(self.evap), _p(self.hardness), _p(self.metric), _p(self.metric_inv),
+                       _p(self.base))
+
+    def exchange_halos(self):
+        if not self.spherical:
+            return
+        from pgerosion.geometry import exchange_halos as xh
+
+        for a in (self.height, self.sediment, self.discharge):
+            xh(self.grid, a)
+        xh(self.grid, self.momentum, vector=True)
+
+
+# --------------------------------------------------------------------------
+# the iteration
+# --------------------------------------------------------------------------
+def _ep(params):
+    return params.erosion if hasattr(params, "erosion") else params
+
+
+def max_steps_of(ep, N):
+    return int(ep.max_steps) if ep.max_steps > 0 else 2 * int(N)
+
+
+def chunk_size(ep, n):
+    return max(1, min(int(ep.chunk), -(-int(n) // 16)))
+
+
+def spawn_weights(state):
+    F, NE = state.F, state.NE
+    inter = np.zeros((F, NE, NE), dtype=bool)
+    inter[state.interior] = True
+    ok = inter & (state.mask == MASK_ACTIVE) & (state.height + state.sediment >= state.base) & (state.precip > 0)
+    idx = np.flatnonzero(ok)
+    return idx, state.precip.reshape(-1)[idx].astype(np.float64)
+
+
+def spawn_particles(state, n_particles, rng):
+    idx, w = spawn_weights(state)
+    if idx.size == 0 or n_particles <= 0:
+        return None
+    total = float(w.sum())
+    if total <= 0.0:
+        return None
+    cdf = np.cumsum(w)
+    u = np.sort(rng.random(n_particles))
+    off = rng.random((n_particles, 2))
+    k = np.empty(n_particles, np.int64)
+    lib().orc_spawn_cells(ctypes.c_int64(cdf.size), _p(cdf), ctypes.c_int64(n_particles), _p(u), _p(k))
+    flat = idx[k]
+    NE = state.NE
+    f = flat // (NE * NE)
+    rem = flat - f * NE * NE
+    ei = rem // NE
+    ej = rem - ei * NE
+    x = (ei - state.H).astype(np.float64) + off[:, 0]
+    y = (ej - state.H).astype(np.float64) + off[:, 1]
+    return f.astype(np.int64), x, y, total / n_particles
+
+
+def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -> TraceParams:
+    u = state.height_unit_m
+    return TraceParams(
+        dt=float(ep.dt), density=float(ep.density), friction=float(ep.friction), deposition_rate=float(ep.deposition_rate),
+        evap_rate=float(ep.evap_rate), k_mom=float(ep.k_mom), mom_scale=float(mom_scale), k_disc=float(ep.k_disc),
+        disc_saturation=float(ep.disc_saturation if disc_sat is None else disc_sat), disc_exponent=float(ep.disc_exponent),
+        slope_gain=float(ep.slope_gain), slope_sat=float(ep.slope_saturation), erodibility=float(ep.erodibility),
+        cover_depth=_cu(ep, "cover_depth", u), min_volume=float(ep.min_volume_frac) * float(volume0),
+        max_erode=_cu(ep, "max_erode", u), conc_scale=float(conc_scale), ocean_rate=float(ep.ocean_deposition_rate),
+        fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u),
+        max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
+        deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
+        F=int(state.F))
+
+
+def apply_params(state, ep, iter_deposit) -> ApplyParams:
+    u = state.height_unit_m
+    return ApplyParams(iter_erode=_cu(ep, "iter_erode", u), iter_deposit=float(iter_deposit), fan_slope=float(ep.fan_slope),
+                       dep_floor=_cu(ep, "dep_floor_m", u), offshore_writeoff=float(ep.offshore_writeoff),
+                       use_erode_cap=int(float(ep.slope_limit_erode) > 0.0))
+
+
+def trace(state, tp: TraceParams, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0):
+    """Trace particles on the current packed samples; returns the change list
+    ``(cl_cell, cl_delta, cl_vol, cl_mom, cl_count, cl_lo, cl_hi, sp_death)``."""
+    P = int(sp_face.shape[0])
+    cap = change_list_cap(tp.max_steps)
+    cl_cell = np.zeros(P * cap, np.int32)
+    cl_delta = np.zeros(P * cap)
+    cl_vol = np.zeros(P * cap, np.float32)
+    cl_mom = np.zeros((P * cap, 2), np.float32)
+    cnt = np.zeros(P, np.int64)
+    lo = np.zeros(P, np.int64)
+    hi = np.zeros(P, np.int64)
+    death = np.zeros(P, np.int8)
+    c = lambda a, dt: np.ascontiguousarray(a, dt)
+    lib().orc_trace(ctypes.byref(tp), _p(state.samp), _p(state.mask), ctypes.c_int64(P), _p(c(sp_face, np.int64)),
+                    _p(c(sp_x, np.float64)), _p(c(sp_y, np.float64)), _p(c(sp_sed, np.float64)), _p(c(sp_dir, np.float64)),
+                    ctypes.c_double(volume0), _p(cl_cell), _p(cl_delta), _p(cl_vol), _p(cl_mom), _p(cnt), _p(lo), _p(hi),
+                    _p(death))
+    return cl_cell, cl_delta, cl_vol, cl_mom, cnt, lo, hi, death
+
+
+def apply(state, ap: ApplyParams, cl, cap, ecap=None):
+    cl_cell, cl_delta, cl_vol, cl_mom, cnt = cl[:5]
+    out4 = np.zeros(4)
+    ecap = np.zeros(1) if ecap is None else ecap
+    lib().orc_apply(ctypes.byref(ap), _p(cl_cell), _p(cl_delta), _p(cl_vol), _p(cl_mom), ctypes.c_int64(cnt.size),
+                    _p(np.ascontiguousarray(cnt)), ctypes.c_int(cap), _p(state.height), _p(state.sediment), _p(state.acc),
+                    _p(state.pending), _p(state.samp), _p(state.disch_track), _p(state.mom_track), _p(state.mask), _p(ecap),
+                    _p(out4))
+    return int(out4[0]), float(out4[1]), float(out4[2]), float(out4[3])
+
+
+def run_iteration(state, params, iteration_key, n_particles=None, particles_per_cell=None, rng_stage="erosion", chunk=None) -> dict:
+    """One particle pass with the reference's chunked serial-apply semantics.
+    ``chunk`` overrides ``erosion.chunk`` (particles per chunk)."""
+    ep = _ep(params)
+    key = iteration_key if isinstance(iteration_key, (tuple, list)) else (int(iteration_key),)
+    rng = params.rng(rng_stage, *key)
+    t0 = time.time()
+    n_cells = int(np.count_nonzero(state.mask[state.interior] == MASK_ACTIVE))
+    if n_particles is None:
+        ppc = ep.particles_per_cell if particles_per_cell is None else particles_per_cell
+        n_particles = max(1, int(round(ppc * n_cells)))
+    sp = spawn_particles(state, n_particles, rng)
+    stats = {"particles": 0, "entries": 0, "steps_mean": 0.0}
+    if sp is None:
+        return stats
+    sp_face, sp_x, sp_y, volume0 = sp
+    sp_sed = np.zeros(sp_face.shape[0])
+    sp_dir = np.zeros(sp_face.shape[0])
+    pend_cells = np.flatnonzero(state.pending.reshape(-1) > 0.0)
+    released = 0.0
+    if pend_cells.size:
+        NE = state.NE
+        pf = pend_cells // (NE * NE)
+        rem = pend_cells - pf * NE * NE
+        pei = rem // NE
+        pej = rem - pei * NE
+        loads = state.pending.reshape(-1)[pend_cells]
+        released = float(loads.sum())
+        sp_face = np.concatenate([sp_face, pf.astype(np.int64)])
+        sp_x = np.concatenate([sp_x, (pei - state.H) + 0.5])
+        sp_y = np.concatenate([sp_y, (pej - state.H) + 0.5])
+        sp_sed = np.concatenate([sp_sed, loads])
+        sp_dir = np.concatenate([sp_dir, rng.random(pend_cells.size) * (2.0 * np.pi)])
+        state.pending.reshape(-1)[pend_cells] = 0.0
+    state.pack()
+    state.acc[...] = 0.0
+    disc_sat = float(ep.disc_saturation)
+    mom_scale = 1.0
+    if float(ep.disc_saturation_cells) > 0.0 or float(ep.momentum_saturation_cells) > 0.0:
+        total = float(volume0) * float(n_particles)
+        n_rain = max(int(spawn_weights(state)[0].size), 1)
+        rain_per_cell = total / n_rain
+        if float(ep.disc_saturation_cells) > 0.0:
+            disc_sat = float(ep.disc_saturation_cells) * rain_per_cell
+        if float(ep.momentum_saturation_cells) > 0.0:
+            mom_scale = float(volume0) / (float(ep.momentum_saturation_cells) * rain_per_cell)
+    use_ecap = float(ep.slope_limit_erode) > 0.0
+    ecap = None
+    if use_ecap:
+        ecap = np.empty_like(state.height)
+        lib().orc_slope_erode_cap(ctypes.c_int(state.F), ctypes.c_int(state.NE), _p(state.height), _p(state.sediment),
+                                  _p(state.mask), ctypes.c_double(float(ep.slope_limit_erode)),
+                                  ctypes.c_double(float(ep.slope_limit_exit)), _p(ecap))
+    iter_deposit = _cu(ep, "iter_deposit", state.height_unit_m)
+    if float(ep.slope_limit_deposit) > 0.0:
+        iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
+    max_steps = max_steps_of(ep, state.N)
+    cap = change_list_cap(max_steps)
+    P = sp_face.shape[0]
+    chunk = chunk_size(ep, P) if chunk is None else int(chunk)
+    tp = trace_params(state, ep, volume0, chunk / (volume0 * P), mom_scale, disc_sat)
+    ap = apply_params(state, ep, iter_deposit)
+    deaths = np.zeros(len(DEATH_NAMES), np.int64)
+    entries = steps = n_clamp = 0
+    to_pending = lost = lost_offshore = 0.0
+    t_trace = t_apply = 0.0
+    for c0 in range(0, P, chunk):
+        c1 = min(P, c0 + chunk)
+        t1 = time.time()
+        cl = trace(state, tp, sp_face[c0:c1], sp_x[c0:c1], sp_y[c0:c1], sp_sed[c0:c1], sp_dir[c0:c1], volume0)
+        t2 = time.time()
+        nc, tpd, lo, lo_off = apply(state, ap, cl, cap, ecap)
+        t_trace += t2 - t1
+        t_apply += time.time() - t2
+        n_clamp += nc
+        to_pending += tpd
+        lost += lo
+        lost_offshore += lo_off
+        cnt = cl[4]
+        entries += int(cnt.sum())
+        steps += _count_steps(cl[2], cnt, cap)
+        deaths += np.bincount(cl[7], minlength=deaths.size)
+    lib().orc_fold(ctypes.c_int64(state.height.size), _p(state.height), _p(state.sediment), _p(state.acc), _p(state.mask))
+    lib().orc_ema(ctypes.c_int64(state.height.size), _p(state.discharge), _p(state.momentum), _p(state.disch_track),
+                  _p(state.mom_track), _p(state.mask), ctypes.c_double(float(ep.ema)))
+    stats.update({"particles": int(P), "entries": entries, "steps_mean": entries / max(P, 1), "volume": float(volume0),
+                  "seconds": time.time() - t0, "droplet_steps": steps})
+    stats["deaths"] = {n: int(c) for n, c in zip(DEATH_NAMES, deaths)}
+    stats["clamped"] = n_clamp
+    stats["to_pending"] = to_pending
+    stats["released"] = released
+    stats["pending_total"] = float(state.pending[state.interior].sum())
+    stats["deficit_out"] = lost
+    stats["lost_offshore"] = lost_offshore
+    stats["seconds_trace"] = t_trace
+    stats["seconds_apply"] = t_apply
+    stats["chunk"] = int(chunk)
+    return stats
+
+
+def _count_steps(cl_vol, cnt, cap) -> int:
+    """Droplet-steps: change-list entries with volume >= 0."""
+    P = cnt.size
+    idx = np.arange(cap)[None, :] < cnt[:, None]
+    return int(np.count_nonzero((cl_vol[: P * cap].reshape(P, cap) >= 0.0) & idx))
+
+
+def thermal_erosion(state, params):
+    ep = _ep(params)
+    hard = state.hardness
+    talus = (np.float32(ep.talus_slope_soft) + np.float32(ep.talus_slope_hard - ep.talus_slope_soft) * hard).astype(np.float64)
+    dep_floor = _cu(ep, "dep_floor_m", state.height_unit_m)
+    cap = _cu(ep, "thermal_max", state.height_unit_m)
+    _mass_wasting(state, talus, float(ep.thermal_rate), cap, state.mask, dep_floor)
+    if ep.creep_rate > 0.0:
+        cmask = np.where(state.height + state.sediment < state.base, np.uint8(MASK_FROZEN), state.mask).astype(np.uint8)
+        _mass_wasting(state, np.zeros_like(talus), float(ep.creep_rate), cap, cmask, dep_floor)
+
+
+def _mass_wasting(state, talus, rate, cap, mask, dep_floor):
+    sh = state.height.shape
+    scratch = [np.empty(sh) for _ in range(5)]
+    lib().orc_mass_wasting(ctypes.c_int(state.F), ctypes.c_int(state.NE), _p(state.height), _p(state.sediment),
+                           _p(state.metric), _p(np.ascontiguousarray(talus)), _p(np.ascontiguousarray(mask)),
+                           ctypes.c_double(rate), ctypes.c_double(cap), ctypes.c_double(dep_floor), *[_p(s) for s in scratch])
+
+
+def _applied_uplift(state, cap=None):
+    u = state.uplift if cap is None else np.minimum(state.uplift, float(cap))
+    mean = 0.0
+    if state.spherical:
+        iact = state.mask[state.interior] == MASK_ACTIVE
+        mean = float(u[state.interior][iact].mean()) if iact.any() else 0.0
+    return u, mean
+
+
+def apply_uplift(state, cap=None):
+    act = state.mask == MASK_ACTIVE
+    u, mean = _applied_uplift(state, cap)
+    state.height[act] += u[act] - mean
+
+
+def start_replay(state, params):
+    ep = _ep(params)
+    if not state.spherical or str(getattr(ep, "uplift_mode", "stack")) != "replay":
+        return None
+    u, mean = _applied_uplift(state, None)
+    act = state.mask == MASK_ACTIVE
+    total = np.zeros_like(state.height)
+    total[act] = float(int(ep.iterations)) * (u[act] - mean)
+    state.height -= total
+    state.exchange_halos()
+    shift = hold_datum(state, state.land_target)
+    return {"datum_shift": shift}
+
+
+def hold_datum(state, land_fraction, level=0.0):
+    surf = (state.height[state.interior] + state.sediment[state.interior]).ravel()
+    M = surf.size
+    n_land = min(max(int(round(float(land_fraction) * M)), 0), M)
+    if n_land == 0:
+        q = float(surf.max()) + 1.0
+    elif n_land == M:
+        q = float(surf.min())
+    else:
+        k = M - n_land
+        q = float(np.partition(surf, k)[k])
+    q -= float(level)
+    if q != 0.0:
+        state.height -= q
+        np.subtract(state.base, q, out=state.base, where=state.base < 0.0)
+    return q
+
+
+def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
+    st = run_iteration(state, params, iteration_key, n_particles=n_particles, chunk=chunk)
+    thermal_erosion(state, params)
+    apply_uplift(state, None)
+    if state.spherical:
+        st["datum_shift"] = hold_datum(state, state.land_target)
+    state.exchange_halos()
+    state.iteration += 1
+    return st

@@ -1,0 +1,249 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Run from the repository root where the bake project is available::
+
+    NUMBA_CACHE_DIR=/tmp/numba python tests/golden/gen_golden.py /path/to/bake
+
+It imports the bake's own numba code (``globe.cubesphere``,
+``globe.erosion.particle``, ``globe.erosion.maps``) and records what it
+computes on seeded synthetic inputs built by ``pgerosion.synth``:
+
+* ``cubesphere_vectors.npz`` -- to_sphere / from_sphere / transfer_velocity
+  of the scalar functions the particle kernel uses (cubesphere.py:70-220),
+  on uniform points plus points within 1e-4 of face edges and corners.
+* ``halo_N8_H2.npz`` -- the Grid's halo tables, owner and metric at N=8, H=2,
+  and SHA-256 digests of the tables at two larger grids.
+* ``trace_isolated.npz`` -- a six-face N=48 world after three reference
+  iterations, a set of droplets whose touched cells (plus a one-cell ring)
+  are pairwise disjoint, and the reference ``trace_particles`` change lists
+  and ``apply_changes`` results for them (particle.py:275-1042).
+* ``step_tiny.npz`` -- a six-face N=32 world run through the reference
+  ``maps.step`` (plain knobs, uplift replay) for a few iterations: the
+  initial state, the final state and the per-iteration stats.
+
+The fixtures are small (well under a few MB) and committed; the tests never
+import the bake.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT / "procedural-generation_b200"))
+
+
+def _ref(bake: str):
+    sys.path.insert(0, bake)
+    import globe.cubesphere as cs
+    import globe.erosion.maps as maps
+    import globe.erosion.particle as pk
+    from globe.config import WorldParams
+
+    return cs, maps, pk, WorldParams
+
+
+def gen_vectors(cs):
+    rng = np.random.default_rng(20261203)
+    K = 3000
+    face = rng.integers(0, 6, K)
+    u = rng.random(K)
+    v = rng.random(K)
+    e = K // 4
+    i1 = rng.choice(K, e, replace=False)
+    u[i1] = np.where(rng.random(e) < 0.5, rng.random(e) * 1e-4, 1.0 - rng.random(e) * 1e-4)
+    i2 = rng.choice(K, e, replace=False)
+    v[i2] = np.where(rng.random(e) < 0.5, rng.random(e) * 1e-4, 1.0 - rng.random(e) * 1e-4)
+    xyz = np.array([cs.to_sphere(int(f), float(a), float(b)) for f, a, b in zip(face, u, v)])
+    back = [cs.from_sphere(*p) for p in xyz]
+    f2 = np.array([b[0] for b in back], np.int32)
+    u2 = np.array([b[1] for b in back])
+    v2 = np.array([b[2] for b in back])
+    # transfer_velocity on points just outside an edge (the particle crossing)
+    T = 2000
+    tf = rng.integers(0, 6, T)
+    tu = rng.random(T)
+    tv = rng.random(T)
+    side = rng.integers(0, 4, T)
+    d = rng.random(T) * 0.02 + 1e-6
+    tu = np.where(side == 0, -d, np.where(side == 1, 1.0 + d, tu))
+    tv = np.where(side == 2, -d, np.where(side == 3, 1.0 + d, tv))
+    ta, tb = rng.normal(size=(2, T))
+    tr = np.array([cs.transfer_velocity(int(f), float(a), float(b), float(c), float(g)) for f, a, b, c, g in zip(tf, tu, tv, ta, tb)])
+    np.savez_compressed(HERE / "cubesphere_vectors.npz", face=face.astype(np.int32), u=u, v=v, xyz=xyz, face2=f2, u2=u2, v2=v2,
+                        t_face=tf.astype(np.int32), t_u=tu, t_v=tv, t_a=ta, t_b=tb, t_face2=tr[:, 0].astype(np.int32),
+                        t_out=tr[:, 1:].astype(np.float64))
+
+
+def gen_halo(cs):
+    g = cs.Grid(8, 2, 50.0)
+    hm = g.halo
+    dig = {}
+    for N, H, c in ((16, 2, 50.0), (32, 4, 9773.0)):
+        gg = cs.Grid(N, H, c)
+        h = gg.halo
+        for k in ("dst", "src", "w", "w_lin", "rot", "nearest"):
+            dig[f"{N}_{H}_{k}"] = hashlib.sha256(np.ascontiguousarray(getattr(h, k)).tobytes()).hexdigest()
+        dig[f"{N}_{H}_owner"] = hashlib.sha256(np.ascontiguousarray(gg.owner).tobytes()).hexdigest()
+        dig[f"{N}_{H}_metric"] = hashlib.sha256(np.ascontiguousarray(gg.metric[0]).tobytes()).hexdigest()
+    np.savez_compressed(HERE / "halo_N8_H2.npz", dst=hm.dst, src=hm.src, w=hm.w, w_lin=hm.w_lin, rot=hm.rot, nearest=hm.nearest,
+                        owner=g.owner, metric=g.metric[0], metric_inv=g.metric_inv[0], digests=json.dumps(dig))
+
+
+def _world_params(WorldParams, N, H, cell, seed, land, **erosion):
+    from pgerosion.params import plain_knobs
+
+    p = WorldParams.tiny_world(seed)
+    kn = plain_knobs()
+    kn.update(erosion)
+    return p.with_overrides(world={"N_c": N, "halo": H, "cell_size_m": cell, "land_fraction": land, "T": N, "R": 2}, erosion=kn)
+
+
+def _ref_state(cs, maps, world, p):
+    grid = cs.get_grid(world.grid.N, world.grid.H, world.grid.cell_size_m)
+    st = maps.ErosionState.from_grid(grid, world.bedrock, world.hardness, world.precip, world.evap, world.uplift, p.erosion)
+    st.land_target = float(world.land_fraction)
+    return st
+
+
+def gen_trace(cs, maps, pk, WorldParams):
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=3, N=48, H=2, cell_size_m=50.0, land_fraction=0.35)
+    p = _world_params(WorldParams, 48, 2, 50.0, 3, 0.35, iterations=10, max_steps=64, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="stack")
+    st = _ref_state(cs, maps, world, p)
+    for it in range(3):
+        maps.step(st, p, it)
+    st.pack()
+    ep = p.erosion
+    NE, H, N = st.NE, st.H, st.N
+    rng = np.random.default_rng(77)
+    # candidates: rain on land plus loaded droplets (a re-injected stockpile) on land and sea cells
+    idx, w = maps.spawn_weights(st)
+    nc = 3000
+    pick = idx[rng.integers(0, idx.size, nc)]
+    f = pick // (NE * NE)
+    rem = pick - f * NE * NE
+    ei, ej = rem // NE, rem % NE
+    x = (ei - H) + rng.random(nc)
+    y = (ej - H) + rng.random(nc)
+    sed = np.zeros(nc)
+    dirs = np.zeros(nc)
+    nl = 600
+    allc = np.flatnonzero(np.ones(st.height.shape, bool) & (np.pad(np.ones((6, N, N), bool), ((0, 0), (H, H), (H, H)))))
+    lp = allc[rng.integers(0, allc.size, nl)]
+    lf = lp // (NE * NE)
+    lrem = lp - lf * NE * NE
+    f = np.concatenate([f, lf])
+    x = np.concatenate([x, (lrem // NE - H) + 0.5])
+    y = np.concatenate([y, (lrem % NE - H) + 0.5])
+    sed = np.concatenate([sed, rng.random(nl) * 0.5 + 1e-3])
+    dirs = np.concatenate([dirs, rng.random(nl) * 2 * np.pi])
+    P = f.size
+    volume0 = float(w.sum()) / 2048.0
+    max_steps = maps.max_steps_of(ep, N)
+    cap = int(pk.change_list_cap(max_steps, False))
+
+    def trace(ff, xx, yy, ss, dd, conc):
+        n = ff.size
+        out = dict(cl_cell=np.zeros(n * cap, np.int32), cl_delta=np.zeros(n * cap), cl_vol=np.zeros(n * cap, np.float32),
+                   cl_mom=np.zeros((n * cap, 2), np.float32), cl_count=np.zeros(n, np.int64), cl_lo=np.zeros(n, np.int64),
+                   cl_hi=np.zeros(n, np.int64), sp_death=np.zeros(n, np.int8))
+        cu = lambda k: float(getattr(ep, k)) / st.height_unit_m
+        pk.trace_particles(ff.astype(np.int64), xx, yy, ss, dd, volume0, st.samp, False, st.mask, N, H, True,
+                           float(ep.dt), float(ep.density), float(ep.friction), float(ep.deposition_rate), float(ep.evap_rate),
+                           float(ep.k_mom), 1.0, float(ep.k_disc), float(ep.disc_saturation), float(ep.disc_exponent),
+                           float(ep.slope_gain), float(ep.slope_saturation), float(ep.erodibility), cu("cover_depth"),
+                           float(ep.min_volume_frac) * volume0, int(max_steps), cu("max_erode"), conc, int(ep.pit_steps), False,
+                           float(ep.ocean_deposition_rate), int(ep.ocean_steps), cu("fan_room"), cu("dep_floor_m"),
+                           float(ep.lake_trap), 0.0, 0.0, np.zeros((1, 1, 1), np.float32), False,
+                           out["cl_cell"], out["cl_delta"], out["cl_vol"], out["cl_mom"], out["cl_count"], out["cl_lo"],
+                           out["cl_hi"], out["sp_death"])
+        return out
+
+    conc = 1.0 / volume0
+    allt = trace(f, x, y, sed, dirs, conc)
+    own = st.grid.owner.reshape(-1)
+    taken = np.zeros(st.height.size, bool)
+    keep = []
+    for q in range(P):
+        cells = allt["cl_cell"][q * cap: q * cap + allt["cl_count"][q]].astype(np.int64)
+        fi = int(f[q])
+        c0 = (fi * NE + int(np.floor(x[q])) + H) * NE + int(np.floor(y[q])) + H
+        cells = np.unique(np.concatenate([cells, [c0]]))
+        cf = cells // (NE * NE)
+        cr = cells - cf * NE * NE
+        ci, cj = cr // NE, cr % NE
+        ring = []
+        for di in (-1, 0, 1):
+            for dj in (-1, 0, 1):
+                ii = np.clip(ci + di, 0, NE - 1)
+                jj = np.clip(cj + dj, 0, NE - 1)
+                ring.append(own[(cf * NE + ii) * NE + jj])
+        ring = np.unique(np.concatenate(ring))
+        if taken[ring].any():
+            continue
+        taken[ring] = True
+        keep.append(q)
+    keep = np.array(keep)
+    f, x, y, sed, dirs = f[keep], x[keep], y[keep], sed[keep], dirs[keep]
+    res = trace(f, x, y, sed, dirs, conc)
+    acc = np.zeros_like(st.height)
+    pending = np.zeros_like(st.height)
+    dtr = np.zeros_like(st.height)
+    mtr = np.zeros_like(st.momentum)
+    samp = st.samp.copy()
+    cu = lambda k: float(getattr(ep, k)) / st.height_unit_m
+    ap = pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                          st.height, st.sediment, acc, pending, samp, dtr, mtr, st.mask, cu("iter_erode"), cu("iter_deposit"),
+                          float(ep.fan_slope), False, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                          st.lake_load, st.lake_id, st.lake_room)
+    np.savez_compressed(
+        HERE / "trace_isolated.npz", N=N, H=H, height=st.height, sediment=st.sediment, discharge=st.discharge,
+        momentum=st.momentum, hardness=st.hardness, evap=st.evap, base=st.base, mask=st.mask,
+        sp_face=f.astype(np.int64), sp_x=x, sp_y=y, sp_sed=sed, sp_dir=dirs, volume0=volume0, conc_scale=conc, cap=cap,
+        max_steps=max_steps, params=json.dumps({k: getattr(ep, k) for k in ep.__dataclass_fields__}),
+        cell_size_m=st.height_unit_m, **res, acc=acc, pending=pending, disch_track=dtr, mom_track=mtr,
+        apply_out=np.array([float(a) for a in ap]))
+    print(f"trace_isolated: {keep.size} isolated droplets of {P}; deaths {np.bincount(res['sp_death'], minlength=6)}")
+
+
+def gen_step(cs, maps, pk, WorldParams):
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=5, N=32, H=2, cell_size_m=50.0, land_fraction=0.3)
+    iters = 6
+    p = _world_params(WorldParams, 32, 2, 50.0, 5, 0.3, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay")
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    stats = []
+    for it in range(iters):
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "to_pending", "released", "pending_total",
+                                         "deficit_out", "lost_offshore", "deaths", "datum_shift")})
+    np.savez_compressed(HERE / "step_tiny.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.3, seed=5, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h_start, height=st.height, sediment=st.sediment, discharge=st.discharge, momentum=st.momentum,
+                        pending=st.pending, stats=json.dumps(stats), **init)
+    print("step_tiny:", stats[-1])
+
+
+def main(bake: str):
+    cs, maps, pk, WorldParams = _ref(bake)
+    gen_vectors(cs)
+    gen_halo(cs)
+    gen_trace(cs, maps, pk, WorldParams)
+    gen_step(cs, maps, pk, WorldParams)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/bake")
