@@ -1,0 +1,345 @@
+"""Benchmark: droplet-steps/s of the erosion stage on the Earth-default world.
+
+Workload (one "step" = one full plain erosion iteration): cube-sphere
+N_c = 1024, halo 2, 6 x 1028 x 1028 float32 fBm + ridge bedrock (-8000..+6000 m,
+29 % land), latitude-banded rain 0.1..3.0, uplift replay 0..2 mm/iteration,
+1,572,864 droplets per iteration (+ re-injected stockpiles), max lifetime 96
+steps.  A droplet-step is one change-list entry of volume >= 0 (one step
+that reaches the mass-transfer section).  Data: seeded synthetic world.
+
+Arms
+  default          the CUDA library (libpgerosion.so) through pgerosion.maps
+  --impl reference the reference algorithm's CPU restatement (the oracle, a
+                   port of the numba code; the numba code itself cannot run
+                   on the GPU box), timed on all host cores
+
+Multi-GPU: ``torchrun --nproc-per-node N bench.py --gpus N``: every rank
+erodes its own world (seed = rank), no collective on the data path (weak
+scaling); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT, ROOT / "procedural-generation_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+#: algorithmic bytes of one droplet-step on the plain path: gathered 2x2
+#: surface (16 B), 2x2 momentum a/b and discharge (48 B), inverse metric and
+#: metric (24 B), base / evap / hardness / sediment (16 B), mask (1 B);
+#: scattered int64 terrain change, discharge and two momentum tracks (32 B)
+BYTES_PER_STEP = 137
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_world(seed: int, N: int | None = None):
+    from pgerosion import synth
+
+    params, P = synth.config_params("earth", seed=seed)
+    if N is not None and N != params.world.N_c:
+        params.world.N_c = N
+        P = 6 * N * N // 4
+    w = synth.earth_world(seed=seed, N=params.world.N_c)
+    return params, P, w
+
+
+def cpu_baseline(params, P, world, seconds=20.0):
+    """The oracle (CPU restatement of the reference) on all host cores: full
+    iterations of the same workload until ``seconds`` have passed."""
+    from oracle import oracle as orc
+
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    steps, t_all, n_it = 0, 0.0, 0
+    while t_all < seconds and n_it < 50:
+        t0 = time.perf_counter()
+        s = orc.step(st, params, n_it, n_particles=P)
+        t_all += time.perf_counter() - t0
+        steps += s["droplet_steps"]
+        n_it += 1
+    return {"value": steps / t_all, "unit": "droplet-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n_it} full iteration(s) of the same N_c={params.world.N_c} world, {t_all:.1f} s"}
+
+
+def launches_per_iteration(nw: int, pending: bool, creep: bool) -> int:
+    """Kernels of this library one plain iteration launches (library kernels
+    -- CUB scan / sort / select -- not counted)."""
+    spawn = 3 + (1 if pending else 0)
+    droplets = 2 + nw + (nw - 1) + 1          # pack x2, waves, refreshes, fold+EMA
+    thermal = 4 * (2 if creep else 1)
+    uplift = 3
+    datum = 1 + 8 * 2 + 1
+    halo = 4
+    return spawn + droplets + thermal + uplift + datum + halo
+
+
+def run_b200(args, rank, world_size, dist):
+    import torch
+
+    from pgerosion import _lib
+    from pgerosion import maps as gm
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    params, P, world = make_world(seed=rank, N=args.n)
+    st = gm.ErosionState.from_world(world)
+    gm.start_replay(st, params)
+    prec = _lib.PREC_F64 if args.precision == "f64" else _lib.PREC_F32
+    wave = None if args.wave == 0 else args.wave
+    apply = _lib.APPLY_ORDERED if args.apply == "ordered" else _lib.APPLY_WAVE
+    kw = dict(n_particles=P, wave=wave, precision=prec, blocks_per_sm=args.blocks_per_sm, apply=apply)
+    n_total = args.warmup + args.steps
+
+    # value: spawn uniforms of every iteration drawn up front and resident in HBM
+    pre = []
+    for it in range(n_total):
+        rng, u, off = gm.draw_spawns(params, "erosion", (it,), P)
+        pre.append((rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)))
+    for it in range(args.warmup):
+        gm.step(st, params, it, predrawn=pre[it], **kw)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    # the droplet pass (pge_trace_apply) timed on its own stream with events
+    ta = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    steps_done = 0
+    n_waves = 0
+    pend_any = False
+    with ClockSampler(dev.index) as clk:
+        torch.cuda.synchronize()
+        ev[0].record()
+        for k in range(args.steps):
+            it = args.warmup + k
+            st_k = gm.step(st, params, it, predrawn=pre[it], events=ta[k], **kw)
+            steps_done += st_k["droplet_steps"]
+            n_waves += -(-st_k["particles"] // st_k["chunk"])
+            pend_any |= st_k["released"] > 0
+        ev[1].record()
+        torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1])
+    ta_ms = [a.elapsed_time(b) for a, b in ta]
+    # e2e: the public API with host buffers: spawns drawn on the host and
+    # copied from pinned memory every step, stats read back every step
+    h2d = d2h = 0
+    e2e_steps = 0
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = time.perf_counter()
+    ee = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ee[0].record()
+    for k in range(args.steps):
+        it = n_total + k
+        rng, u, off = gm.draw_spawns(params, "erosion", (it,), P)
+        u_p = torch.from_numpy(u).pin_memory()
+        off_p = torch.from_numpy(off).pin_memory()
+        u_d = u_p.to(dev, non_blocking=True)
+        off_d = off_p.to(dev, non_blocking=True)
+        s = gm.step(st, params, it, predrawn=(rng, u_d, off_d), **kw)
+        h2d += u_p.numel() * 8 + off_p.numel() * 8 + 8 * _n_pending(s)
+        d2h += (_lib.STATS_WORDS + 4 + 4) * 8
+        e2e_steps += s["droplet_steps"]
+    ee[1].record()
+    torch.cuda.synchronize()
+    e2e_ms = ee[0].elapsed_time(ee[1])
+    tot = torch.tensor([steps_done, e2e_steps], dtype=torch.float64, device=dev)
+    tm = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(tot)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    steps_all, e2e_all = float(tot[0]), float(tot[1])
+    ms_max, e2e_ms_max = float(tm[0]), float(tm[1])
+    if rank != 0:
+        return None
+    peak, peak_kind = _peaks()
+    per_launch_steps = steps_done / max(args.steps, 1)
+    avg_ta = float(np.mean(ta_ms))
+    achieved = per_launch_steps * BYTES_PER_STEP / (avg_ta * 1e-3) / 1e9
+    traffic = _profiled_traffic()
+    out = {
+        "metric": "droplet-steps/s", "value": steps_all / (ms_max * 1e-3), "unit": "droplet-steps/s", "n_gpus": world_size,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == _lib.PREC_F64 else "f32",
+        "data": "synthetic (seeded fBm + ridge Earth-default world per rank)",
+        "config": {"workload": f"plain erosion iteration, cube-sphere N_c={params.world.N_c}, H=2, {P} droplets/iteration, "
+                               f"max_steps 96, uplift replay", "N_c": params.world.N_c, "droplets_per_iteration": P,
+                   "wave": "reference chunk" if wave is None else wave, "apply": args.apply,
+                   "l2": "inputs larger than L2 (state > 1 GB)",
+                   "parallelism": f"replicas x{world_size}"},
+        "e2e": {"value": e2e_all / (e2e_ms_max * 1e-3), "unit": "droplet-steps/s", "h2d_bytes_per_step": h2d // max(args.steps, 1),
+                "d2h_bytes_per_step": d2h // max(args.steps, 1)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "droplet pass (pge_trace_apply: droplet waves + wave refreshes + pack + fold)",
+                     "ms_per_launch": avg_ta, "bytes_per_step": BYTES_PER_STEP},
+        "gpu_launches": launches_per_iteration(max(n_waves // max(args.steps, 1), 1), pend_any, params.erosion.creep_rate > 0) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if world_size == 1 and not args.no_cpu:
+        w_host = world
+        out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
+    return out
+
+
+def _n_pending(stats) -> int:
+    """Stockpile droplets of an iteration (their directions are host-drawn and copied)."""
+    return int(stats.get("n_pending", 0))
+
+
+def _profiled_traffic():
+    """DRAM bytes per droplet-pass launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bytes_per_launch"])
+        except (KeyError, ValueError):
+            return None
+    return None
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    params, P, world = make_world(seed=0, N=args.n)
+    from oracle import oracle as orc
+
+    threads = os.cpu_count() or 1
+    orc.set_threads(threads)
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    for it in range(args.warmup):
+        orc.step(st, params, it, n_particles=P)
+    steps = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s = orc.step(st, params, args.warmup + k, n_particles=P)
+        steps += s["droplet_steps"]
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    return {"metric": "droplet-steps/s", "value": v, "unit": "droplet-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fBm + ridge Earth-default world)", "impl": "reference",
+            "config": {"workload": f"plain erosion iteration, cube-sphere N_c={params.world.N_c}, H=2, {P} droplets/iteration, "
+                                   f"max_steps 96, uplift replay", "N_c": params.world.N_c, "droplets_per_iteration": P},
+            "cpu_baseline": {"value": v, "unit": "droplet-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} full iterations after {args.warmup} warm-up"},
+            "e2e": {"value": v, "unit": "droplet-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--wave", type=int, default=-1, help="droplets per wave; 0 = the reference's chunk; -1 = default")
+    ap.add_argument("--precision", default="f64", choices=("f64", "f32"))
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="droplet kernel: 2 selects the two-blocks-per-SM variant")
+    ap.add_argument("--apply", default="ordered", choices=("ordered", "wave"),
+                    help="ordered: the reference's serial apply (default); wave: per-droplet ledgers against wave-start terrain")
+    ap.add_argument("--n", type=int, default=None, help="override N_c (tests)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        args.warmup = 3
+    if args.wave == -1:
+        args.wave = DEFAULT_WAVE
+    rank = int(os.environ.get("RANK", 0))
+    world_size = int(os.environ.get("WORLD_SIZE", 1))
+    dist = None
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        if world_size > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        out = run_b200(args, rank, world_size, dist)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+#: droplets per wave of the default run (0 = the reference's chunk of 2048)
+DEFAULT_WAVE = 0
+
+if __name__ == "__main__":
+    main()

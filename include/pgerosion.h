@@ -1,0 +1,239 @@
+/*
+ * pgerosion.h -- C ABI of the B200 particle-erosion library (libpgerosion.so).
+ *
+ * The library replaces the per-iteration particle pass of the bake's erosion
+ * stage and the plain map passes around it.  Paths below are within the
+ * reference project (Gkrumbach07/procedural-generation, directory bake/):
+ *
+ *   pge_spawn_rain        maps.spawn_weights / spawn_particles /
+ *                         particle.spawn_cells     globe/erosion/maps.py:793-833,
+ *                                                  globe/erosion/particle.py:1245-1260
+ *   pge_collect_pending   pending re-injection     globe/erosion/maps.py:886-903
+ *   pge_trace_apply       pack_samples + the chunk loop of trace_particles /
+ *                         apply_changes + fold_changes + ema_update
+ *                                                  globe/erosion/maps.py:904-1047,
+ *                                                  globe/erosion/particle.py:164-1101, 1230-1242
+ *   pge_trace_changelist  trace_particles' change list, for parity checks
+ *                                                  globe/erosion/particle.py:275-818
+ *   pge_thermal           thermal_erosion (talus pass + creep pass)
+ *                                                  globe/erosion/maps.py:1050-1085,
+ *                                                  globe/erosion/particle.py:1107-1227
+ *   pge_uplift            apply_uplift             globe/erosion/maps.py:1088-1147
+ *   pge_hold_datum        hold_datum               globe/erosion/maps.py:1446-1508
+ *   pge_halo_gather       FaceField.exchange_halos globe/field.py:104-125
+ *
+ * Conventions
+ *   - Every pointer in the structs is a DEVICE pointer unless marked "host".
+ *     Cell arrays are (F, NE, NE) row-major with NE = N + 2H; vector fields
+ *     (momentum) are (F, NE, NE, 2).  Heights are in cell units.
+ *   - The library never allocates device memory.  The caller passes one
+ *     workspace of pge_workspace_bytes() bytes, 256-byte aligned.
+ *   - Every call is asynchronous on the given CUDA stream (a cudaStream_t
+ *     passed as void*; NULL = the legacy default stream) and returns 0 or a
+ *     negative PGE_E* code; pge_last_error() describes the last failure of
+ *     the calling thread.  Launch errors are checked with
+ *     cudaPeekAtLastError; device-side overflow is counted in PgeStats.
+ *   - Results do not depend on thread scheduling: terrain changes, tracks,
+ *     stockpiles and stat totals are summed as int64 fixed point.
+ *   - Calls on one state are not reentrant; order them on one stream.
+ */
+#ifndef PGEROSION_H
+#define PGEROSION_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PGE_API __attribute__((visibility("default")))
+#else
+#define PGE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGE_VERSION 1
+
+enum {
+    PGE_OK = 0,
+    PGE_E_ARG = -1,       /* a null pointer, size or parameter out of range */
+    PGE_E_WORKSPACE = -2, /* workspace too small */
+    PGE_E_CUDA = -3,      /* a CUDA call failed */
+    PGE_E_UNSUPPORTED = -4
+};
+
+/* droplet arithmetic precision of the trace (the ledger is always float64) */
+enum { PGE_PREC_F64 = 0, PGE_PREC_F32 = 1 };
+
+/* PGE_APPLY_ORDERED: the wave's change lists are applied in droplet order
+ *   against the live terrain, float64 -- the reference's serial apply
+ *   (particle.py:821-1042); with wave = the reference's chunk the whole pass
+ *   is the reference's.
+ * PGE_APPLY_WAVE: each droplet applies its own list against the wave-start
+ *   terrain plus its own changes, merged with int64 fixed-point atomics:
+ *   exact for droplets that share no cell, faster, but droplets that share
+ *   cells each see the wave-start terrain. */
+enum { PGE_APPLY_ORDERED = 0, PGE_APPLY_WAVE = 1 };
+
+/* mask codes and death causes, as in globe/erosion/particle.py:54-76 */
+enum { PGE_MASK_OUTSIDE = 0, PGE_MASK_ACTIVE = 1, PGE_MASK_FROZEN = 2 };
+enum { PGE_DEATH_AGE = 0, PGE_DEATH_OCEAN, PGE_DEATH_EXIT, PGE_DEATH_PIT, PGE_DEATH_EVAP, PGE_DEATH_STOP, PGE_N_DEATHS };
+
+/* fixed-point scales: value = integer * 2^-shift */
+#define PGE_FX_MASS_SHIFT 40  /* terrain change, stockpiles, mass totals (cell units) */
+#define PGE_FX_TRACK_SHIFT 32 /* discharge and momentum tracks (volume units) */
+
+typedef struct PgeGrid {
+    int32_t F;               /* faces: 6 on the sphere, 1 for a window */
+    int32_t N;               /* interior cells per face edge */
+    int32_t H;               /* halo width */
+    int32_t spherical;       /* 1: droplets cross faces; 0: window, leaving it kills */
+    int32_t deposit_on_exit; /* window mode: leaving droplets drop their load */
+    int32_t metric_shared;   /* 1: metric tables are (NE, NE, 3), the same on every face */
+    int32_t max_steps;       /* workspace capacity: the largest erosion.max_steps any call uses */
+    int64_t max_droplets;    /* workspace capacity: the most spawns (rain + stockpiles) of one pass */
+    int64_t max_wave;        /* workspace capacity: the largest wave of the exact (ordered) apply */
+} PgeGrid;
+
+/* the ErosionState arrays (globe/erosion/maps.py:56-115) on the device */
+typedef struct PgeState {
+    double *height;          /* (F,NE,NE) bedrock height */
+    double *sediment;        /* (F,NE,NE) */
+    double *discharge;       /* (F,NE,NE) EMA of volume per iteration */
+    double *momentum;        /* (F,NE,NE,2) EMA of volume * velocity */
+    double *pending;         /* (F,NE,NE) stockpile re-injected next iteration */
+    double *base;            /* (F,NE,NE) local base level (0 on the plain path) */
+    const double *uplift;    /* (F,NE,NE) per-iteration uplift (cell units) */
+    const float *hardness;   /* (F,NE,NE) */
+    const float *precip;     /* (F,NE,NE) spawn weight */
+    const float *evap;       /* (F,NE,NE) evaporation multiplier */
+    const uint8_t *mask;     /* (F,NE,NE) or NULL: every cell active */
+    const float *metric;     /* (NE,NE,3) or (F,NE,NE,3): g_ii, g_ij, g_jj */
+    const float *metric_inv; /* same shape: inverse metric */
+} PgeState;
+
+/* droplet spawns of one iteration: rain first, then re-injected stockpiles */
+typedef struct PgeSpawns {
+    int32_t *face;
+    double *x, *y;           /* fractional interior cell coordinates */
+    double *sed;             /* initial load (0 for rain) */
+    double *dir;             /* initial direction (radians) of a loaded droplet */
+    int64_t count;
+    double volume0;          /* spawn volume (host value) */
+} PgeSpawns;
+
+/* the plain-path scalar knobs, already in cell units (maps.py:958-1008) */
+typedef struct PgeParams {
+    double dt, density, friction, deposition_rate, evap_rate, k_mom, mom_scale, k_disc, disc_saturation,
+        disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
+        ocean_rate, fan_room, dep_floor, iter_erode, iter_deposit, fan_slope, offshore_writeoff, ema;
+    int32_t max_steps, pit_steps, ocean_steps;
+    int32_t wave;            /* droplets traced against one frozen terrain (the reference's chunk) */
+    int32_t precision;       /* PGE_PREC_* */
+    int32_t apply;           /* PGE_APPLY_*: how a wave's changes meet the terrain */
+    int32_t use_erode_cap;   /* slope_limit_erode > 0: erode_cap passed to pge_trace_apply */
+    int32_t threads_per_block; /* 0 = default */
+    int32_t blocks_per_sm;     /* 0 = occupancy maximum */
+} PgeParams;
+
+/* counters of one droplet pass (device struct; the caller zeroes it) */
+typedef struct PgeStats {
+    int64_t droplets;
+    int64_t droplet_steps;   /* change-list entries with volume >= 0 */
+    int64_t entries;
+    int64_t deaths[PGE_N_DEATHS];
+    int64_t clamped;
+    int64_t overflow;        /* droplets whose ledger table overflowed (never expected) */
+    int64_t to_pending_fx;   /* mass totals, fixed point 2^-40 */
+    int64_t deficit_out_fx;
+    int64_t lost_offshore_fx;
+    int64_t released_fx;
+    int64_t eroded_fx;       /* terrain removed by the ledger (applied erosion) */
+    int64_t deposited_fx;    /* terrain added by the ledger (applied deposition) */
+    int64_t errors;          /* nonzero: an ordered-apply wait gave up (the pass is invalid) */
+} PgeStats;
+
+/* halo gather tables (bake/globe/cubesphere.py:540-662) */
+typedef struct PgeHalo {
+    int64_t K;               /* halo rows */
+    const int32_t *dst;      /* (K) flat halo cell */
+    const int32_t *src;      /* (K,16) flat interior sources */
+    const double *w;         /* (K,16) weights */
+    const double *rot;       /* (K,16,2,2) vector rotations, or NULL */
+} PgeHalo;
+
+PGE_API int pge_version(void);
+/* copies the calling thread's last error message (host buffer); returns its length */
+PGE_API int pge_last_error(char *buf, size_t n);
+
+/* Workspace bytes for a grid and its capacities (g->max_droplets,
+ * g->max_steps).  Every call on that grid must be passed the same PgeGrid
+ * and a workspace at least this large. */
+PGE_API size_t pge_workspace_bytes(const PgeGrid *g);
+
+/* Rain spawns (maps.spawn_particles): spawnable cells are interior, active,
+ * surface >= base and precip > 0; u (count) host-drawn uniforms in [0,1)
+ * (unsorted: the library sorts them), off (count,2) offsets.  Writes
+ * spawns->face/x/y/sed/dir[0:count] and the spawn total weight to
+ * *total_dev (device double; volume0 = total / count).  *nspawnable_dev
+ * (device int64) receives the number of spawnable cells. */
+PGE_API int pge_spawn_rain(const PgeGrid *g, const PgeState *s, const double *u, const double *off, int64_t count,
+                   PgeSpawns *spawns, double *total_dev, int64_t *nspawnable_dev, void *ws, size_t ws_bytes,
+                   void *stream);
+
+/* Pending re-injection, stage 1: counts the cells with pending > 0 into
+ * *count_dev (device int64). */
+PGE_API int pge_count_pending(const PgeGrid *g, const PgeState *s, int64_t *count_dev, void *ws, size_t ws_bytes, void *stream);
+
+/* Pending re-injection, stage 2: appends one loaded droplet per cell with
+ * pending > 0, in flat-index order, at spawns[offset ...] (cell centre,
+ * sed = the stockpile), adds the released mass to stats->released_fx and
+ * zeroes pending.  dir must already hold the host-drawn directions. */
+PGE_API int pge_collect_pending(const PgeGrid *g, PgeState *s, PgeSpawns *spawns, int64_t offset, PgeStats *stats,
+                        void *ws, size_t ws_bytes, void *stream);
+
+/* One droplet pass: pack the samples, trace every spawn in waves of
+ * p->wave droplets (terrain frozen within a wave, refreshed between waves),
+ * apply each droplet's erosion / deposition ledger against the wave-start
+ * terrain plus its own changes, then fold the net change into
+ * height / sediment, EMA-update discharge / momentum and write pending. */
+PGE_API int pge_trace_apply(const PgeGrid *g, PgeState *s, const PgeSpawns *spawns, const PgeParams *p,
+                    const double *erode_cap, PgeStats *stats, void *ws, size_t ws_bytes, void *stream);
+
+/* Parity hook: trace and apply one wave exactly like pge_trace_apply and
+ * also write every droplet's change list in the reference layout
+ * (cap = max_steps + 2*8 + 1 + 8 + 8 entries per droplet): cell (int32),
+ * requested delta (float64), volume and momentum (float32), count (int64)
+ * and death cause (int8).  No fold / EMA; the net change stays in the
+ * workspace accumulators (read them with pge_read_accumulators). */
+PGE_API int pge_trace_changelist(const PgeGrid *g, PgeState *s, const PgeSpawns *spawns, const PgeParams *p,
+                         int32_t *cl_cell, double *cl_delta, float *cl_vol, float *cl_mom, int64_t *cl_count,
+                         int8_t *cl_death, PgeStats *stats, void *ws, size_t ws_bytes, void *stream);
+
+/* Converts the workspace accumulators of the last pass to float64:
+ * acc (F,NE,NE), disch_track (F,NE,NE), mom_track (F,NE,NE,2), pending (F,NE,NE). */
+PGE_API int pge_read_accumulators(const PgeGrid *g, double *acc, double *disch_track, double *mom_track, double *pending,
+                          void *ws, size_t ws_bytes, void *stream);
+
+/* Talus pass, then (creep_rate > 0) the creep pass with submerged cells frozen. */
+PGE_API int pge_thermal(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max,
+                double talus_soft, double talus_hard, double dep_floor, void *ws, size_t ws_bytes, void *stream);
+
+/* height += min(uplift, cap) - mean over the active interior (cap < 0: none;
+ * the mean is taken only when spherical). */
+PGE_API int pge_uplift(const PgeGrid *g, PgeState *s, double cap, double scale, void *ws, size_t ws_bytes, void *stream);
+
+/* Rigid shift so that round(land_fraction * M) interior cells have
+ * height + sediment >= level; writes the shift (cell units) to *shift_dev. */
+PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, double level, double *shift_dev, void *ws,
+                   size_t ws_bytes, void *stream);
+
+/* Fills the halo rows of one field from its interior: a scalar (F,NE,NE)
+ * field, or with vector = 1 a (F,NE,NE,2) field rotated per source. */
+PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,470 @@
+// pge_api.cu -- the extern "C" entry points of libpgerosion (include/pgerosion.h).
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "pge_internal.cuh"
+#include "pge_maps.cuh"
+#include "pge_ordered.cuh"
+
+namespace pge {
+
+namespace {
+thread_local char g_err[512] = "";
+
+int fail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    return fail(PGE_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
+}
+
+int check_grid(const PgeGrid *g)
+{
+    if (!g) return fail(PGE_E_ARG, "grid is NULL");
+    if (g->F < 1 || g->N < 2 || g->H < 1 || g->N < 2 * g->H) return fail(PGE_E_ARG, "bad grid F=%d N=%d H=%d", g->F, g->N, g->H);
+    if (g->spherical && g->F != 6) return fail(PGE_E_ARG, "a spherical grid has 6 faces (F=%d)", g->F);
+    const long long NE = g->N + 2LL * g->H;
+    if ((long long)g->F * NE * NE >= (1LL << 31)) return fail(PGE_E_ARG, "grid too large for int32 cell indices");
+    if (g->max_steps < 1 || g->max_droplets < 1 || g->max_wave < 1) return fail(PGE_E_ARG, "workspace capacities must be positive");
+    if (g->max_wave > (1LL << 20)) return fail(PGE_E_ARG, "max_wave above 2^20");
+    return PGE_OK;
+}
+
+int check_ws(const PgeGrid *g, void *ws, size_t bytes, Layout &lay)
+{
+    lay = layout(*g);
+    if (!ws) return fail(PGE_E_ARG, "workspace is NULL");
+    if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(PGE_E_ARG, "workspace must be 256-byte aligned");
+    if (bytes < lay.total) return fail(PGE_E_WORKSPACE, "workspace %zu bytes, need %zu", bytes, lay.total);
+    return PGE_OK;
+}
+
+int check_state(const PgeState *s)
+{
+    if (!s || !s->height || !s->sediment || !s->discharge || !s->momentum || !s->pending || !s->base || !s->hardness ||
+        !s->evap || !s->metric || !s->metric_inv)
+        return fail(PGE_E_ARG, "state has a NULL array");
+    return PGE_OK;
+}
+
+int check_params(const PgeGrid *g, const PgeParams *p)
+{
+    if (!p) return fail(PGE_E_ARG, "params is NULL");
+    if (p->max_steps < 1 || p->max_steps > g->max_steps) return fail(PGE_E_ARG, "max_steps %d outside 1..%d", p->max_steps, g->max_steps);
+    if (p->wave < 1) return fail(PGE_E_ARG, "wave must be >= 1");
+    if (p->apply != PGE_APPLY_ORDERED && p->apply != PGE_APPLY_WAVE) return fail(PGE_E_ARG, "unknown apply mode %d", p->apply);
+    if (p->apply == PGE_APPLY_ORDERED && p->wave > g->max_wave)
+        return fail(PGE_E_ARG, "wave %d above the workspace's max_wave %lld", p->wave, (long long)g->max_wave);
+    if (p->precision != PGE_PREC_F64 && p->precision != PGE_PREC_F32) return fail(PGE_E_ARG, "unknown precision %d", p->precision);
+    if (p->threads_per_block != 0 && (p->threads_per_block < 32 || p->threads_per_block > 256 || p->threads_per_block % 32))
+        return fail(PGE_E_ARG, "threads_per_block must be a multiple of 32 in 32..256");
+    return PGE_OK;
+}
+
+int sm_count()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return sms;
+}
+
+}  // namespace
+
+
+// droplet threads resident at once (the kernel runs at most 1024 threads per SM)
+__global__ void report_errors_kernel(const int *error, PgeStats *stats)
+{
+    if (*error) stats->errors = 1;
+}
+
+void report_errors(const int *error, PgeStats *stats, cudaStream_t st) { report_errors_kernel<<<1, 1, 0, st>>>(error, stats); }
+
+__global__ void set_mode_kernel(unsigned long long *slot, unsigned long long v) { *slot = v; }
+
+int64_t droplet_slots() { return (int64_t)sm_count() * 1024; }
+
+Layout layout(const PgeGrid &g)
+{
+    Layout L{};
+    const long long NE = g.N + 2LL * g.H;
+    L.ncell = (long long)g.F * NE * NE;
+    L.nmetric = g.metric_shared ? NE * NE : L.ncell;
+    L.nslots = droplet_slots();
+    L.table_cap = ledger_table_cap(g.max_steps);
+    L.table_slots = ledger_table_slots(g.max_steps);
+    L.max_droplets = g.max_droplets;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o = align256(o + bytes);
+        return at;
+    };
+    L.cellA = take(16 * L.ncell);
+    L.cellB = take(16 * L.ncell);
+    L.live = take(16 * L.ncell);
+    L.metric8 = take(32 * L.nmetric);
+    L.acc4 = take(32 * L.ncell);
+    L.pend = take(8 * L.ncell);
+    L.tkey = take(8 * L.nslots * L.table_slots);
+    L.town = take(8 * L.nslots * L.table_slots);
+    L.counters = take(256);
+    L.sortkeys = take(8 * L.max_droplets);
+    L.sortvals = L.sortkeys;
+    L.cdf = take(16 * L.ncell);
+    L.cubtmp_bytes = cub_temp_bytes(L.ncell, L.max_droplets);
+    L.cubtmp = take(L.cubtmp_bytes);
+    L.partial = take(64 * 1024);
+    L.thermal = take(40 * L.ncell);
+    L.flags = take(8 * L.ncell);
+    // ordered apply
+    L.cap = change_list_cap(g.max_steps);
+    L.max_wave = g.max_wave;
+    L.wave_slots = L.max_wave * L.cap;
+    const long long ws = L.wave_slots;
+    L.w_cell = take(4 * ws);
+    L.w_delta = take(8 * ws);
+    L.w_vol = take(4 * ws);
+    L.w_mom = take(8 * ws);
+    L.w_count = take(8 * L.max_wave);
+    L.w_death = take(L.max_wave);
+    L.w_D = take(4 * ws);
+    L.w_last = take(ws);
+    L.w_keys0 = take(8 * ws);
+    L.w_keys1 = take(8 * ws);
+    L.w_vals0 = take(4 * ws);
+    L.w_vals1 = take(4 * ws);
+    L.w_runstart = take(4 * ws);
+    L.w_segpos = take(4 * ws);
+    L.w_runscan = take(4 * ws);
+    L.w_segscan = take(4 * ws);
+    L.w_temp_bytes = ordered_temp_bytes(ws);
+    L.w_temp = take(L.w_temp_bytes);
+    L.done = take(8 * L.ncell);
+    L.error = take(256);
+    L.total = o;
+    return L;
+}
+
+namespace {
+int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, const double *ecap, PgeStats *stats,
+              void *ws, const Layout &lay, cudaStream_t st, int32_t *rec_cell, double *rec_delta, float *rec_vol,
+              float *rec_mom, int64_t *rec_count, int8_t *rec_death)
+{
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.acc4), 0, 32 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset acc");
+    if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.pend), 0, 8 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset pending");
+    if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.counters), 0, 16, st)) != cudaSuccess) return cuda_fail(e, "memset counters");
+    // own-change tables: generation 0 everywhere (free); waves then use generations (w + 1) << 24 onwards
+    if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.tkey), 0, 8 * lay.nslots * lay.table_slots, st)) != cudaSuccess)
+        return cuda_fail(e, "memset tables");
+    pack(*g, *s, lay, ws, st);
+    const long long P = sp->count;
+    if (P > 0) {
+        const int threads = p->threads_per_block ? p->threads_per_block : 256;
+        // blocks_per_sm >= 2 selects the kernel variant compiled for two resident blocks per SM
+        const int minb = p->blocks_per_sm >= 2 ? 2 : 1;
+        int bps = p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
+        if (p->blocks_per_sm > 0 && p->blocks_per_sm < bps) bps = p->blocks_per_sm;
+        long long maxblocks = (long long)sm_count() * bps;
+        if (maxblocks * threads > lay.nslots) maxblocks = lay.nslots / threads;
+        DropArgs a{};
+        a.F = g->F;
+        a.N = g->N;
+        a.H = g->H;
+        a.NE = g->N + 2 * g->H;
+        a.spherical = g->spherical;
+        a.deposit_on_exit = g->deposit_on_exit;
+        a.metric_shared = g->metric_shared;
+        a.A = ws_ptr<float4>(ws, lay.cellA);
+        a.B = ws_ptr<float4>(ws, lay.cellB);
+        a.L = ws_ptr<double2>(ws, lay.live);
+        a.G = ws_ptr<float4>(ws, lay.metric8);
+        a.mask = s->mask;
+        a.ecap = p->use_erode_cap ? ecap : nullptr;
+        a.sp_face = sp->face;
+        a.sp_x = sp->x;
+        a.sp_y = sp->y;
+        a.sp_sed = sp->sed;
+        a.sp_dir = sp->dir;
+        a.volume0 = sp->volume0;
+        a.p = *p;
+        a.acc4 = ws_ptr<long long>(ws, lay.acc4);
+        a.pend = ws_ptr<long long>(ws, lay.pend);
+        a.stats = stats;
+        a.tkey = ws_ptr<unsigned long long>(ws, lay.tkey);
+        a.town = ws_ptr<double>(ws, lay.town);
+        a.table_mask = (unsigned)(lay.table_slots - 1);
+        a.table_cap = (int)lay.table_cap;
+        a.rec_cell = rec_cell;
+        a.rec_delta = rec_delta;
+        a.rec_vol = rec_vol;
+        a.rec_mom = rec_mom;
+        a.rec_count = rec_count;
+        a.rec_death = rec_death;
+        a.rec_cap = change_list_cap(p->max_steps);
+        a.rec_base = 0;
+        a.ledger = 1;
+        a.minb = minb;
+        unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
+        const long long wave = p->wave;
+        const long long nw = (P + wave - 1) / wave;
+        if (p->apply == PGE_APPLY_ORDERED && !rec_cell) {
+            // exact mode: record each wave's change lists, then apply them in droplet order
+            if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.done), 0, 8 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset done");
+            if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.error), 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset error");
+            a.ledger = 0;
+            a.rec_cell = ws_ptr<int32_t>(ws, lay.w_cell);
+            a.rec_delta = ws_ptr<double>(ws, lay.w_delta);
+            a.rec_vol = ws_ptr<float>(ws, lay.w_vol);
+            a.rec_mom = ws_ptr<float>(ws, lay.w_mom);
+            a.rec_count = ws_ptr<int64_t>(ws, lay.w_count);
+            a.rec_death = ws_ptr<int8_t>(ws, lay.w_death);
+            a.rec_cap = (int)lay.cap;
+            OrderedWave ow{};
+            OrderedArgs &oa = ow.a;
+            oa.cell = a.rec_cell;
+            oa.delta = a.rec_delta;
+            oa.vol = a.rec_vol;
+            oa.mom = a.rec_mom;
+            oa.count = a.rec_count;
+            oa.cap = (int)lay.cap;
+            oa.D = ws_ptr<int32_t>(ws, lay.w_D);
+            oa.last = ws_ptr<uint8_t>(ws, lay.w_last);
+            oa.L = a.L;
+            oa.sediment = s->sediment;
+            oa.A = ws_ptr<float4>(ws, lay.cellA);
+            oa.B = ws_ptr<float4>(ws, lay.cellB);
+            oa.mask = s->mask;
+            oa.ecap = a.ecap;
+            oa.acc4 = ws_ptr<double>(ws, lay.acc4);
+            oa.pend = ws_ptr<double>(ws, lay.pend);
+            oa.done = ws_ptr<unsigned long long>(ws, lay.done);
+            oa.p = *p;
+            oa.stats = stats;
+            oa.error = ws_ptr<int>(ws, lay.error);
+            ow.cap = (int)lay.cap;
+            int kbits = 0, pbits = 0, cbits = 0;
+            while ((1LL << kbits) < lay.cap) kbits++;
+            while ((1LL << pbits) < wave) pbits++;
+            while ((1LL << cbits) < lay.ncell + 1) cbits++;
+            ow.kbits = kbits;
+            ow.pbits = pbits;
+            ow.end_bit = cbits + pbits + kbits;
+            if (ow.end_bit > 63) return fail(PGE_E_ARG, "grid, wave and max_steps too large for 63-bit sort keys");
+            ow.invalid = (1ull << ow.end_bit) - 1ull;
+            ow.keys_in = ws_ptr<unsigned long long>(ws, lay.w_keys0);
+            ow.keys_out = ws_ptr<unsigned long long>(ws, lay.w_keys1);
+            ow.vals_in = ws_ptr<int32_t>(ws, lay.w_vals0);
+            ow.vals_out = ws_ptr<int32_t>(ws, lay.w_vals1);
+            ow.runstart = ws_ptr<int32_t>(ws, lay.w_runstart);
+            ow.segpos = ws_ptr<int32_t>(ws, lay.w_segpos);
+            ow.runscan = ws_ptr<int32_t>(ws, lay.w_runscan);
+            ow.segscan = ws_ptr<int32_t>(ws, lay.w_segscan);
+            ow.temp = ws_ptr<void>(ws, lay.w_temp);
+            ow.temp_bytes = lay.w_temp_bytes;
+            ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(256);
+            for (long long w = 0; w < nw; w++) {
+                a.d_begin = w * wave;
+                a.d_end = a.d_begin + wave < P ? a.d_begin + wave : P;
+                a.rec_base = a.d_begin;
+                a.counter = ctr + (w & 1);
+                a.counter_next = ctr + ((w + 1) & 1);
+                long long blocks = (a.d_end - a.d_begin + threads - 1) / threads;
+                if (blocks > maxblocks) blocks = maxblocks;
+                e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
+                                                 : launch_droplets_f32(a, (int)blocks, threads, st);
+                if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
+                ow.nw = a.d_end - a.d_begin;
+                oa.nw = ow.nw;
+                oa.epoch = (unsigned long long)(w + 1) << 24;
+                if ((e = ordered_wave(ow, st)) != cudaSuccess) return cuda_fail(e, "ordered apply");
+            }
+            report_errors(ws_ptr<int>(ws, lay.error), stats, st);
+            if ((e = cudaPeekAtLastError()) != cudaSuccess) return cuda_fail(e, "droplet pass");
+            return PGE_OK;
+        }
+        for (long long w = 0; w < nw; w++) {
+            a.d_begin = w * wave;
+            a.d_end = a.d_begin + wave < P ? a.d_begin + wave : P;
+            a.counter = ctr + (w & 1);
+            a.counter_next = ctr + ((w + 1) & 1);
+            // 2^24 droplet generations per thread and wave; after 255 waves the tables are cleared again
+            if (w > 0 && w % 255 == 0) {
+                if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.tkey), 0, 8 * lay.nslots * lay.table_slots, st)) != cudaSuccess)
+                    return cuda_fail(e, "memset tables");
+            }
+            a.gen_base = (unsigned long long)(w % 255 + 1) << 24;
+            long long blocks = (a.d_end - a.d_begin + threads - 1) / threads;
+            if (blocks > maxblocks) blocks = maxblocks;
+            e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
+                                             : launch_droplets_f32(a, (int)blocks, threads, st);
+            if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
+            if (w + 1 < nw) refresh(*s, lay, ws, st);
+        }
+    }
+    if ((e = cudaPeekAtLastError()) != cudaSuccess) return cuda_fail(e, "droplet pass");
+    return PGE_OK;
+}
+}  // namespace
+}  // namespace pge
+
+using namespace pge;
+
+extern "C" {
+
+PGE_API int pge_version(void) { return PGE_VERSION; }
+
+PGE_API int pge_last_error(char *buf, size_t n)
+{
+    const int len = (int)strlen(g_err);
+    if (buf && n) {
+        strncpy(buf, g_err, n - 1);
+        buf[n - 1] = 0;
+    }
+    return len;
+}
+
+PGE_API size_t pge_workspace_bytes(const PgeGrid *g)
+{
+    if (check_grid(g) != PGE_OK) return 0;
+    return layout(*g).total;
+}
+
+PGE_API int pge_spawn_rain(const PgeGrid *g, const PgeState *s, const double *u, const double *off, int64_t count, PgeSpawns *sp,
+                   double *total_dev, int64_t *nspawnable_dev, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    if (!s->precip || !u || !off || !sp || !sp->face || !sp->x || !sp->y || !sp->sed || !sp->dir || !total_dev)
+        return fail(PGE_E_ARG, "spawn_rain: NULL pointer");
+    if (count < 1 || count > g->max_droplets) return fail(PGE_E_ARG, "spawn count %lld outside 1..%lld", (long long)count, (long long)g->max_droplets);
+    cudaError_t e = spawn_rain(*g, *s, lay, ws, u, off, count, *sp, total_dev, reinterpret_cast<long long *>(nspawnable_dev),
+                               (cudaStream_t)stream);
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "spawn_rain");
+}
+
+PGE_API int pge_count_pending(const PgeGrid *g, const PgeState *s, int64_t *count_dev, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    cudaError_t e = count_pending(*g, *s, lay, ws, reinterpret_cast<long long *>(count_dev), (cudaStream_t)stream);
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "count_pending");
+}
+
+PGE_API int pge_collect_pending(const PgeGrid *g, PgeState *s, PgeSpawns *sp, int64_t offset, PgeStats *stats, void *ws,
+                        size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    if (!sp || !sp->face || !sp->x || !sp->y || !sp->sed || !stats) return fail(PGE_E_ARG, "collect_pending: NULL pointer");
+    if (offset < 0 || offset > g->max_droplets) return fail(PGE_E_ARG, "collect_pending: bad offset");
+    cudaError_t e = collect_pending(*g, *s, lay, ws, *sp, offset, stats, (cudaStream_t)stream);
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "collect_pending");
+}
+
+PGE_API int pge_trace_apply(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, const double *erode_cap,
+                    PgeStats *stats, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s)) || (r = check_params(g, p))) return r;
+    if (!sp || !stats) return fail(PGE_E_ARG, "trace_apply: NULL spawns or stats");
+    if (sp->count < 0 || sp->count > g->max_droplets) return fail(PGE_E_ARG, "spawn count %lld outside 0..%lld", (long long)sp->count, (long long)g->max_droplets);
+    if (sp->count > 0 && (!sp->face || !sp->x || !sp->y || !sp->sed || !sp->dir || !(sp->volume0 > 0.0)))
+        return fail(PGE_E_ARG, "trace_apply: incomplete spawns");
+    if (p->use_erode_cap && !erode_cap) return fail(PGE_E_ARG, "use_erode_cap without erode_cap");
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((r = run_waves(g, s, sp, p, erode_cap, stats, ws, lay, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr))) return r;
+    const int exact = p->apply == PGE_APPLY_ORDERED;
+    set_mode_kernel<<<1, 1, 0, st>>>(ws_ptr<unsigned long long>(ws, lay.counters) + 4, exact);
+    fold_ema(*s, lay, ws, p->ema, exact, st);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "fold_ema");
+}
+
+PGE_API int pge_trace_changelist(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, int32_t *cl_cell,
+                         double *cl_delta, float *cl_vol, float *cl_mom, int64_t *cl_count, int8_t *cl_death,
+                         PgeStats *stats, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s)) || (r = check_params(g, p))) return r;
+    if (!sp || !stats || !cl_cell || !cl_delta || !cl_vol || !cl_mom || !cl_count || !cl_death)
+        return fail(PGE_E_ARG, "trace_changelist: NULL pointer");
+    if (sp->count < 1 || sp->count > g->max_droplets) return fail(PGE_E_ARG, "spawn count outside 1..max_droplets");
+    r = run_waves(g, s, sp, p, nullptr, stats, ws, lay, (cudaStream_t)stream, cl_cell, cl_delta, cl_vol, cl_mom, cl_count, cl_death);
+    if (r) return r;
+    set_mode_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(ws_ptr<unsigned long long>(ws, lay.counters) + 4, 0ull);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "trace_changelist");
+}
+
+PGE_API int pge_read_accumulators(const PgeGrid *g, double *acc, double *disch_track, double *mom_track, double *pending, void *ws,
+                          size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay))) return r;
+    read_accumulators(lay, ws, acc, disch_track, mom_track, pending, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "read_accumulators");
+}
+
+PGE_API int pge_thermal(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max, double talus_soft,
+                double talus_hard, double dep_floor, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    // talus = soft + (hard - soft) * hardness in float32 (numpy types the product by the float32 field)
+    const float soft = (float)talus_soft, diff = (float)(talus_hard - talus_soft);
+    thermal(*g, *s, lay, ws, thermal_rate, creep_rate, thermal_max, soft, diff, dep_floor, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "thermal");
+}
+
+PGE_API int pge_uplift(const PgeGrid *g, PgeState *s, double cap, double scale, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    if (!s->uplift) return fail(PGE_E_ARG, "uplift field is NULL");
+    uplift(*g, *s, lay, ws, cap, scale, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "uplift");
+}
+
+PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, double level, double *shift_dev, void *ws,
+                   size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    if (!shift_dev) return fail(PGE_E_ARG, "shift_dev is NULL");
+    hold_datum(*g, *s, lay, ws, land_fraction, level, shift_dev, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "hold_datum");
+}
+
+PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream)
+{
+    if (!h || !field || (h->K > 0 && (!h->dst || !h->src || !h->w || (vector && !h->rot))))
+        return fail(PGE_E_ARG, "halo_gather: NULL pointer");
+    halo_gather(*h, field, vector, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "halo_gather");
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// pge_internal.cuh -- shared device-side definitions of libpgerosion.
+//
+// Packed per-iteration cell data (written by the pack kernel, frozen for the
+// length of one wave, refreshed between waves):
+//   cellA[c] = float4(surface, discharge, momentum_a, momentum_b)  -- read as
+//              a 2x2 bilinear stencil every droplet step (one float4 per corner)
+//   cellB[c] = float4(evap, hardness, sediment, base)              -- the cell's
+//              own scalars
+//   live[c]  = double2(height + sediment, net change at wave start) -- the
+//              float64 terrain the ledger applies against
+//   metric8  = two float4 per (face-shared) cell: (g_ii, g_ij, g_jj, ginv_ii),
+//              (ginv_ij, ginv_jj, 0, 0)
+// These are the channels of the reference's packed float32 sample array
+// (bake/globe/erosion/particle.py:146-191) split by access pattern.
+//
+// Accumulators (int64 fixed point, summed with integer atomics so a wave's
+// result does not depend on thread order):
+//   acc4[c] = (terrain change 2^-40, discharge track 2^-32, momentum a, b 2^-32)
+//   pend[c] = stockpile 2^-40
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pgerosion.h"
+
+namespace pge {
+
+constexpr int SPREAD = 8;
+constexpr int LAKE_PARKS = 8;
+constexpr double FX_MASS = 1099511627776.0;  // 2^40
+constexpr double FX_TRACK = 4294967296.0;    // 2^32
+constexpr double INV_FX_MASS = 1.0 / FX_MASS;
+constexpr double INV_FX_TRACK = 1.0 / FX_TRACK;
+
+__host__ __device__ inline int change_list_cap(int max_steps) { return max_steps + 2 * SPREAD + 1 + SPREAD + LAKE_PARKS; }
+// distinct cells one droplet's ledger can change: one per step entry plus its final deposits
+__host__ __device__ inline int ledger_table_cap(int max_steps) { return max_steps + SPREAD + 2; }
+// hash slots per droplet thread: a power of two at least twice the table capacity
+inline unsigned ledger_table_slots(int max_steps)
+{
+    unsigned s = 16;
+    while (s < 2u * (unsigned)ledger_table_cap(max_steps)) s <<= 1;
+    return s;
+}
+
+__device__ __forceinline__ long long fx_mass(double v) { return __double2ll_rn(v * FX_MASS); }
+__device__ __forceinline__ long long fx_track(double v) { return __double2ll_rn(v * FX_TRACK); }
+__device__ __forceinline__ void red_add(long long *p, long long v)
+{
+    atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+
+// ---------------------------------------------------------------------------
+// workspace layout
+// ---------------------------------------------------------------------------
+struct Layout {
+    size_t cellA, cellB, live, metric8, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
+        partial, thermal, flags, total;
+    // ordered apply (exact mode): one wave's change lists and ranks
+    size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_D, w_last, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
+        w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, done, error;
+    int64_t ncell, nmetric, nslots, table_cap, table_slots, max_droplets, max_wave, wave_slots, cap;
+};
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// number of per-thread ledger tables (one per resident droplet thread)
+int64_t droplet_slots();
+Layout layout(const PgeGrid &g);
+
+template <typename T>
+inline T *ws_ptr(void *ws, size_t off) { return reinterpret_cast<T *>(static_cast<char *>(ws) + off); }
+
+struct DropArgs {
+    int F, N, H, NE, spherical, deposit_on_exit, metric_shared;
+    const float4 *__restrict__ A;
+    const float4 *__restrict__ B;
+    const double2 *__restrict__ L;
+    const float4 *__restrict__ G;
+    const uint8_t *__restrict__ mask;  // nullptr: all active
+    const double *__restrict__ ecap;   // nullptr unless use_erode_cap
+    const int32_t *sp_face;
+    const double *sp_x, *sp_y, *sp_sed, *sp_dir;
+    double volume0;
+    long long d_begin, d_end;
+    PgeParams p;
+    long long *acc4;
+    long long *pend;
+    PgeStats *stats;
+    unsigned long long *counter;       // this wave's droplet counter
+    unsigned long long *counter_next;  // zeroed for the next wave
+    unsigned long long *tkey;  // per-thread own-change hash tables (table_mask + 1 slots each)
+    double *town;
+    unsigned table_mask;
+    int table_cap;
+    unsigned long long gen_base;  // generation of this wave's first droplet (keys of older waves read as free)
+    // change-list recording (parity hook); rec_cell == nullptr: off
+    int32_t *rec_cell;
+    double *rec_delta;
+    float *rec_vol, *rec_mom;
+    int64_t *rec_count;
+    int8_t *rec_death;
+    int rec_cap;
+    long long rec_base;  // recorded droplet index = d - rec_base
+    int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
+    int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
+};
+
+// launchers of the two precisions (separate translation units: the float64
+// one is compiled without FMA contraction so it rounds like the reference)
+cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+int droplet_blocks_per_sm_f64(int threads, int minb);
+int droplet_blocks_per_sm_f32(int threads, int minb);
+
+}  // namespace pge

@@ -1,0 +1,713 @@
+// pge_maps.cu -- the per-iteration map passes around the droplet pass.
+//
+// Compiled with -fmad=false like the float64 droplet trace, so the float64
+// stencils round like the reference's numba / numpy code.
+//
+//   pack / refresh / fold+EMA   particle.py:164-191, 1005-1012, 1079-1101, 1230-1242
+//   thermal passes a / r / b    particle.py:1107-1227, maps.py:1050-1085
+//   uplift                      maps.py:1088-1147
+//   datum order statistic       maps.py:1446-1508 (radix select instead of np.partition)
+//   halo gather                 field.py:104-125
+//   spawn weights / inverse CDF maps.py:793-833, particle.py:1245-1260
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include "pge_internal.cuh"
+#include "pge_maps.cuh"
+
+namespace pge {
+
+namespace {
+__constant__ int kD8[8][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, -1}};
+
+__device__ __forceinline__ bool interior(long long c, int NE, int H, int N)
+{
+    const long long r = c % ((long long)NE * NE);
+    const int i = (int)(r / NE), j = (int)(r % NE);
+    return i >= H && i < H + N && j >= H && j < H + N;
+}
+
+inline int grid_for(long long n, int threads = 256)
+{
+    long long b = (n + threads - 1) / threads;
+    return (int)(b < 1 ? 1 : (b > 1048576 ? 1048576 : b));
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// pack / refresh / fold + EMA
+// ---------------------------------------------------------------------------
+__global__ void pack_kernel(long long ncell, const double *__restrict__ h, const double *__restrict__ s,
+                            const double *__restrict__ q, const double *__restrict__ mom, const float *__restrict__ evap,
+                            const float *__restrict__ hard, const double *__restrict__ base, float4 *A, float4 *B, double2 *L)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const double sd = s[c];
+        const double hs = h[c] + sd;
+        A[c] = make_float4((float)hs, (float)q[c], (float)mom[2 * c], (float)mom[2 * c + 1]);
+        B[c] = make_float4(evap[c], hard[c], (float)sd, (float)base[c]);
+        L[c] = make_double2(hs, 0.0);
+    }
+}
+
+__global__ void pack_metric_kernel(long long n, const float *__restrict__ g, const float *__restrict__ gi, float4 *G)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        G[2 * c] = make_float4(g[3 * c], g[3 * c + 1], g[3 * c + 2], gi[3 * c]);
+        G[2 * c + 1] = make_float4(gi[3 * c + 1], gi[3 * c + 2], 0.f, 0.f);
+    }
+}
+
+// between waves: the packed surface / sediment and the ledger's wave-start
+// change follow the net change so far (apply_changes' samp sync, particle.py:1005-1009)
+__global__ void refresh_kernel(long long ncell, const double *__restrict__ s, const long long *__restrict__ acc4, float4 *A,
+                               float4 *B, double2 *L)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const double a = (double)acc4[4 * c] * INV_FX_MASS;
+        double2 l = L[c];
+        if (l.y == a) continue;  // unchanged since the last refresh
+        l.y = a;
+        L[c] = l;
+        A[c].x = (float)(l.x + a);
+        const double sd = s[c] + a;
+        B[c].z = (float)(sd > 0.0 ? sd : 0.0);
+    }
+}
+
+// the accumulators as float64: fixed point (wave apply) or plain float64 (ordered apply)
+__device__ __forceinline__ void acc_values(const long long *acc4, const long long *pend, long long c, int exact, double &a,
+                                           double &q, double &ma, double &mb, double &pd)
+{
+    if (exact) {
+        const double *d4 = reinterpret_cast<const double *>(acc4);
+        a = d4[4 * c];
+        q = d4[4 * c + 1];
+        ma = d4[4 * c + 2];
+        mb = d4[4 * c + 3];
+        pd = reinterpret_cast<const double *>(pend)[c];
+    } else {
+        a = (double)acc4[4 * c] * INV_FX_MASS;
+        q = (double)acc4[4 * c + 1] * INV_FX_TRACK;
+        ma = (double)acc4[4 * c + 2] * INV_FX_TRACK;
+        mb = (double)acc4[4 * c + 3] * INV_FX_TRACK;
+        pd = (double)pend[c] * INV_FX_MASS;
+    }
+}
+
+__global__ void fold_ema_kernel(long long ncell, double *h, double *s, double *q, double *mom, double *pending,
+                                const uint8_t *__restrict__ mask, const long long *__restrict__ acc4,
+                                const long long *__restrict__ pend, double ema, int exact)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const bool act = mask ? mask[c] == PGE_MASK_ACTIVE : true;
+        double a, tq, tma, tmb, pd;
+        acc_values(acc4, pend, c, exact, a, tq, tma, tmb, pd);
+        if (a != 0.0 && act) {
+            if (a > 0.0) {
+                s[c] += a;
+            } else {
+                const double take = -a, sd = s[c];
+                if (sd >= take) {
+                    s[c] = sd - take;
+                } else {
+                    h[c] -= take - sd;
+                    s[c] = 0.0;
+                }
+            }
+        }
+        if (act) {
+            q[c] = (1.0 - ema) * q[c] + ema * tq;
+            mom[2 * c] = (1.0 - ema) * mom[2 * c] + ema * tma;
+            mom[2 * c + 1] = (1.0 - ema) * mom[2 * c + 1] + ema * tmb;
+        }
+        if (pd != 0.0) pending[c] += pd;
+    }
+}
+
+__global__ void read_acc_kernel(long long ncell, const long long *__restrict__ acc4, const long long *__restrict__ pend,
+                                const unsigned long long *mode, double *acc, double *dtr, double *mtr, double *pending)
+{
+    const int exact = (int)*mode;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        double a, q, ma, mb, pd;
+        acc_values(acc4, pend, c, exact, a, q, ma, mb, pd);
+        if (acc) acc[c] = a;
+        if (dtr) dtr[c] = q;
+        if (mtr) {
+            mtr[2 * c] = ma;
+            mtr[2 * c + 1] = mb;
+        }
+        if (pending) pending[c] = pd;
+    }
+}
+
+void pack(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, cudaStream_t st)
+{
+    const long long n = lay.ncell;
+    pack_kernel<<<grid_for(n), 256, 0, st>>>(n, s.height, s.sediment, s.discharge, s.momentum, s.evap, s.hardness, s.base,
+                                             ws_ptr<float4>(ws, lay.cellA), ws_ptr<float4>(ws, lay.cellB),
+                                             ws_ptr<double2>(ws, lay.live));
+    pack_metric_kernel<<<grid_for(lay.nmetric), 256, 0, st>>>(lay.nmetric, s.metric, s.metric_inv, ws_ptr<float4>(ws, lay.metric8));
+}
+
+void refresh(const PgeState &s, const Layout &lay, void *ws, cudaStream_t st)
+{
+    refresh_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.sediment, ws_ptr<long long>(ws, lay.acc4),
+                                                       ws_ptr<float4>(ws, lay.cellA), ws_ptr<float4>(ws, lay.cellB),
+                                                       ws_ptr<double2>(ws, lay.live));
+}
+
+void fold_ema(PgeState &s, const Layout &lay, void *ws, double ema, int exact, cudaStream_t st)
+{
+    fold_ema_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.height, s.sediment, s.discharge, s.momentum, s.pending,
+                                                        s.mask, ws_ptr<long long>(ws, lay.acc4), ws_ptr<long long>(ws, lay.pend),
+                                                        ema, exact);
+}
+
+void read_accumulators(const Layout &lay, void *ws, double *acc, double *dtr, double *mtr, double *pending, cudaStream_t st)
+{
+    read_acc_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, ws_ptr<long long>(ws, lay.acc4),
+                                                        ws_ptr<long long>(ws, lay.pend),
+                                                        ws_ptr<unsigned long long>(ws, lay.counters) + 4, acc, dtr, mtr, pending);
+}
+
+// ---------------------------------------------------------------------------
+// thermal erosion (talus / creep mass wasting)
+// ---------------------------------------------------------------------------
+struct ThermalArgs {
+    int F, NE;
+    const double *h, *s;
+    const float *metric;  // (NE,NE,3) shared or (F,NE,NE,3)
+    int metric_shared;
+    const float *hard;    // talus = soft + (hard - soft) * hardness, in float32; nullptr: talus 0
+    float talus_soft, talus_diff;
+    const uint8_t *mask;  // nullptr: all active
+    const double *base;   // creep: submerged cells (h + s < base) are frozen
+    int creep;
+    double rate, cap, dep_floor;
+    double *out_total, *scale, *rscale, *new_h, *new_s;
+};
+
+__device__ __forceinline__ int tmask(const ThermalArgs &t, long long c)
+{
+    int m = t.mask ? t.mask[c] : PGE_MASK_ACTIVE;
+    if (t.creep && t.h[c] + t.s[c] < t.base[c]) m = PGE_MASK_FROZEN;
+    return m;
+}
+
+__device__ __forceinline__ double tout(const ThermalArgs &t, long long c, int k)
+{
+    const int di = kD8[k][0], dj = kD8[k][1];
+    const long long nc = c + (long long)di * t.NE + dj;
+    const double d = (t.h[c] + t.s[c]) - (t.h[nc] + t.s[nc]);
+    if (d <= 0.0) return 0.0;
+    const long long mc = t.metric_shared ? c % ((long long)t.NE * t.NE) : c;
+    const double g0 = t.metric[3 * mc], g1 = t.metric[3 * mc + 1], g2 = t.metric[3 * mc + 2];
+    const double dist = sqrt(g0 * di * di + 2.0 * g1 * di * dj + g2 * dj * dj);
+    double talus = 0.0;
+    if (t.hard) talus = (double)__fadd_rn(t.talus_soft, __fmul_rn(t.talus_diff, t.hard[c]));
+    const double ex = d - talus * dist;
+    if (ex <= 0.0) return 0.0;
+    return 0.5 * t.rate * ex;
+}
+
+#define THERMAL_LOOP                                                                                            \
+    const long long total = (long long)t.F * t.NE * t.NE;                                                       \
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x)
+
+__global__ void thermal_a_kernel(const ThermalArgs t)
+{
+    THERMAL_LOOP
+    {
+        const int i = (int)((c / t.NE) % t.NE), j = (int)(c % t.NE);
+        double ot = 0.0, sc_out = 0.0;
+        if (i >= 1 && i < t.NE - 1 && j >= 1 && j < t.NE - 1 && tmask(t, c) == PGE_MASK_ACTIVE) {
+            double S = 0.0, mx = 0.0;
+            for (int k = 0; k < 8; k++) {
+                if (tmask(t, c + (long long)kD8[k][0] * t.NE + kD8[k][1]) != PGE_MASK_ACTIVE) continue;
+                const double o = tout(t, c, k);
+                S += o;
+                if (o > mx) mx = o;
+            }
+            if (S > 0.0) {
+                double sc = 1.0;
+                if (S > 2.0 * mx) sc = 2.0 * mx / S;
+                if (t.cap > 0.0 && S * sc > t.cap) sc = t.cap / S;
+                ot = S * sc;
+                sc_out = sc;
+            }
+        }
+        t.out_total[c] = ot;
+        t.scale[c] = sc_out;
+    }
+}
+
+__global__ void thermal_r_kernel(const ThermalArgs t)
+{
+    THERMAL_LOOP
+    {
+        const int i = (int)((c / t.NE) % t.NE), j = (int)(c % t.NE);
+        double rs = 1.0;
+        if (i >= 1 && i < t.NE - 1 && j >= 1 && j < t.NE - 1) {
+            const double surf = t.h[c] + t.s[c];
+            if (!(surf >= 0.0 || tmask(t, c) != PGE_MASK_ACTIVE)) {
+                double inflow = 0.0;
+                for (int k = 0; k < 8; k++) {
+                    const long long nc = c + (long long)kD8[k][0] * t.NE + kD8[k][1];
+                    const double sc = t.scale[nc];
+                    if (sc <= 0.0 || tmask(t, nc) == PGE_MASK_OUTSIDE) continue;
+                    inflow += sc * tout(t, nc, (k + 4) % 8);
+                }
+                double room = -t.dep_floor - surf;
+                if (room < 0.0) room = 0.0;
+                if (inflow > room) rs = room / inflow;
+            }
+        }
+        t.rscale[c] = rs;
+    }
+}
+
+__global__ void thermal_b_kernel(const ThermalArgs t)
+{
+    THERMAL_LOOP
+    {
+        const int i = (int)((c / t.NE) % t.NE), j = (int)(c % t.NE);
+        double h = t.h[c], s = t.s[c];
+        if (i >= 1 && i < t.NE - 1 && j >= 1 && j < t.NE - 1 && tmask(t, c) == PGE_MASK_ACTIVE) {
+            double inflow = 0.0, out = 0.0;
+            const double sc_self = t.scale[c];
+            for (int k = 0; k < 8; k++) {
+                const long long nc = c + (long long)kD8[k][0] * t.NE + kD8[k][1];
+                const int mn = tmask(t, nc);
+                if (mn == PGE_MASK_OUTSIDE) continue;
+                if (sc_self > 0.0 && mn == PGE_MASK_ACTIVE) out += sc_self * t.rscale[nc] * tout(t, c, k);
+                const double sc = t.scale[nc];
+                if (sc <= 0.0) continue;
+                inflow += sc * tout(t, nc, (k + 4) % 8);
+            }
+            inflow *= t.rscale[c];
+            if (out > 0.0) {
+                if (s >= out) {
+                    s -= out;
+                } else {
+                    h -= out - s;
+                    s = 0.0;
+                }
+            }
+            s = s + inflow;
+        }
+        t.new_h[c] = h;
+        t.new_s[c] = s;
+    }
+}
+
+__global__ void copy2_kernel(long long n, const double *a, const double *b, double *da, double *db)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        da[c] = a[c];
+        db[c] = b[c];
+    }
+}
+
+void thermal(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double rate, double creep_rate, double cap,
+             float soft, float diff, double dep_floor, cudaStream_t st)
+{
+    double *tb = ws_ptr<double>(ws, lay.thermal);
+    const long long n = lay.ncell;
+    ThermalArgs t;
+    t.F = g.F;
+    t.NE = g.N + 2 * g.H;
+    t.h = s.height;
+    t.s = s.sediment;
+    t.metric = s.metric;
+    t.metric_shared = g.metric_shared;
+    t.talus_soft = soft;
+    t.talus_diff = diff;
+    t.mask = s.mask;
+    t.base = s.base;
+    t.dep_floor = dep_floor;
+    t.cap = cap;
+    t.out_total = tb;
+    t.scale = tb + n;
+    t.rscale = tb + 2 * n;
+    t.new_h = tb + 3 * n;
+    t.new_s = tb + 4 * n;
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1 && !(creep_rate > 0.0)) break;
+        t.hard = pass == 0 ? s.hardness : nullptr;
+        t.creep = pass;
+        t.rate = pass == 0 ? rate : creep_rate;
+        thermal_a_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        thermal_r_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        thermal_b_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        copy2_kernel<<<grid_for(n), 256, 0, st>>>(n, t.new_h, t.new_s, s.height, s.sediment);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// deterministic reductions (fixed block count, fixed tree order)
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCKS = 1024;
+
+__global__ void uplift_sum_kernel(long long ncell, int NE, int H, int N, const double *u, const uint8_t *mask, double cap,
+                                  int use_cap, double *partial, long long *pcount)
+{
+    __shared__ double sh[256];
+    __shared__ long long shc[256];
+    double acc = 0.0;
+    long long cnt = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        if (!interior(c, NE, H, N) || (mask && mask[c] != PGE_MASK_ACTIVE)) continue;
+        double v = u[c];
+        if (use_cap && v > cap) v = cap;
+        acc += v;
+        cnt++;
+    }
+    sh[threadIdx.x] = acc;
+    shc[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sh[threadIdx.x] += sh[threadIdx.x + o];
+            shc[threadIdx.x] += shc[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = sh[0];
+        pcount[blockIdx.x] = shc[0];
+    }
+}
+
+__global__ void mean_final_kernel(const double *partial, const long long *pcount, int n, double *mean_out)
+{
+    __shared__ double sh[RED_BLOCKS];
+    __shared__ long long shc[RED_BLOCKS];
+    for (int i = threadIdx.x; i < RED_BLOCKS; i += blockDim.x) {
+        sh[i] = i < n ? partial[i] : 0.0;
+        shc[i] = i < n ? pcount[i] : 0;
+    }
+    __syncthreads();
+    for (int o = RED_BLOCKS / 2; o > 0; o >>= 1) {
+        for (int i = threadIdx.x; i < o; i += blockDim.x) {
+            sh[i] += sh[i + o];
+            shc[i] += shc[i + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *mean_out = shc[0] > 0 ? sh[0] / (double)shc[0] : 0.0;
+}
+
+__global__ void uplift_add_kernel(long long ncell, double *h, const double *u, const uint8_t *mask, double cap, int use_cap,
+                                  const double *mean, double scale)
+{
+    const double m = mean ? *mean : 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        if (mask && mask[c] != PGE_MASK_ACTIVE) continue;
+        double v = u[c];
+        if (use_cap && v > cap) v = cap;
+        h[c] += scale * (v - m);
+    }
+}
+
+void uplift(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double cap, double scale, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    const int use_cap = cap >= 0.0;
+    double *partial = ws_ptr<double>(ws, lay.partial);
+    long long *pcount = reinterpret_cast<long long *>(partial + RED_BLOCKS);
+    double *mean = partial + 2 * RED_BLOCKS;
+    if (g.spherical) {
+        uplift_sum_kernel<<<RED_BLOCKS, 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.uplift, s.mask, cap, use_cap, partial, pcount);
+        mean_final_kernel<<<1, 1024, 0, st>>>(partial, pcount, RED_BLOCKS, mean);
+    }
+    uplift_add_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.height, s.uplift, s.mask, cap, use_cap,
+                                                           g.spherical ? mean : nullptr, scale);
+}
+
+// ---------------------------------------------------------------------------
+// datum: k-th smallest interior surface by an 8-pass radix select on the
+// order-preserving 64-bit image of the float64 keys
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long okey(double v)
+{
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+__device__ __forceinline__ double unokey(unsigned long long k)
+{
+    const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+struct SelectState {
+    unsigned long long prefix;  // digits found so far (high bits)
+    long long k;                // rank still sought inside the prefix
+    unsigned int hist[256];
+};
+
+__global__ void select_hist_kernel(long long ncell, int NE, int H, int N, const double *h, const double *s, SelectState *ss,
+                                   int shift)
+{
+    __shared__ unsigned int sh[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const unsigned long long prefix = ss->prefix;
+    const unsigned long long hmask = shift >= 56 ? 0ull : (~0ull << (shift + 8));
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        if (!interior(c, NE, H, N)) continue;
+        const unsigned long long k = okey(h[c] + s[c]);
+        if ((k & hmask) != (prefix & hmask)) continue;
+        atomicAdd(&sh[(k >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x)
+        if (sh[i]) atomicAdd(&ss->hist[i], sh[i]);
+}
+
+__global__ void select_pick_kernel(SelectState *ss, int shift)
+{
+    if (threadIdx.x == 0) {
+        long long k = ss->k;
+        int d = 0;
+        for (; d < 255; d++) {
+            const long long c = ss->hist[d];
+            if (k < c) break;
+            k -= c;
+        }
+        ss->k = k;
+        ss->prefix |= (unsigned long long)d << shift;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) ss->hist[i] = 0;
+}
+
+__global__ void select_init_kernel(SelectState *ss, long long k)
+{
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) ss->hist[i] = 0;
+    if (threadIdx.x == 0) {
+        ss->prefix = 0;
+        ss->k = k;
+    }
+}
+
+__global__ void datum_shift_kernel(long long ncell, double *h, double *base, const SelectState *ss, double level, int plus_one,
+                                   double *shift_out)
+{
+    double q = unokey(ss->prefix);
+    if (plus_one) q += 1.0;
+    q -= level;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *shift_out = q;
+    if (q == 0.0) return;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        h[c] -= q;
+        if (base[c] < 0.0) base[c] -= q;
+    }
+}
+
+void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double land_fraction, double level,
+                double *shift_dev, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    const long long M = (long long)g.F * g.N * g.N;
+    long long n_land = (long long)llrint(land_fraction * (double)M);  // numpy round: half to even
+    if (n_land < 0) n_land = 0;
+    if (n_land > M) n_land = M;
+    long long k;
+    int plus_one = 0;
+    if (n_land == 0) {
+        k = M - 1;
+        plus_one = 1;
+    } else {
+        k = M - n_land;
+    }
+    SelectState *ss = ws_ptr<SelectState>(ws, lay.partial + 4 * RED_BLOCKS * sizeof(double));
+    select_init_kernel<<<1, 256, 0, st>>>(ss, k);
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        select_hist_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, ss, shift);
+        select_pick_kernel<<<1, 256, 0, st>>>(ss, shift);
+    }
+    datum_shift_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.height, s.base, ss, level, plus_one, shift_dev);
+}
+
+// ---------------------------------------------------------------------------
+// halo gather
+// ---------------------------------------------------------------------------
+__global__ void halo_scalar_kernel(long long K, const int32_t *dst, const int32_t *src, const double *w, double *f)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < K; k += (long long)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < 16; q++) acc += w[16 * k + q] * f[src[16 * k + q]];
+        f[dst[k]] = acc;
+    }
+}
+
+__global__ void halo_vector_kernel(long long K, const int32_t *dst, const int32_t *src, const double *w, const double *rot,
+                                   double *f)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < K; k += (long long)gridDim.x * blockDim.x) {
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll 4
+        for (int q = 0; q < 16; q++) {
+            const long long sidx = src[16 * k + q];
+            const double va = f[2 * sidx], vb = f[2 * sidx + 1];
+            const double *R = rot + 4 * (16 * k + q);
+            const double wq = w[16 * k + q];
+            a0 += wq * (R[0] * va + R[1] * vb);
+            a1 += wq * (R[2] * va + R[3] * vb);
+        }
+        f[2 * (long long)dst[k]] = a0;
+        f[2 * (long long)dst[k] + 1] = a1;
+    }
+}
+
+void halo_gather(const PgeHalo &h, double *field, int vector, cudaStream_t st)
+{
+    if (h.K <= 0) return;
+    if (vector)
+        halo_vector_kernel<<<grid_for(h.K), 256, 0, st>>>(h.K, h.dst, h.src, h.w, h.rot, field);
+    else
+        halo_scalar_kernel<<<grid_for(h.K), 256, 0, st>>>(h.K, h.dst, h.src, h.w, field);
+}
+
+// ---------------------------------------------------------------------------
+// spawns
+// ---------------------------------------------------------------------------
+__global__ void spawn_weight_kernel(long long ncell, int NE, int H, int N, const double *h, const double *s, const double *base,
+                                    const uint8_t *mask, const float *precip, double *w, long long *lastc)
+{
+    long long last = -1;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const bool ok = interior(c, NE, H, N) && (!mask || mask[c] == PGE_MASK_ACTIVE) && (h[c] + s[c] >= base[c]) && precip[c] > 0.0f;
+        w[c] = ok ? (double)precip[c] : 0.0;
+        if (ok && c > last) last = c;
+    }
+    if (last >= 0) atomicMax(reinterpret_cast<unsigned long long *>(lastc), (unsigned long long)last);
+}
+
+__global__ void spawn_count_kernel(long long ncell, const double *w, long long *count)
+{
+    long long n = 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+        n += w[c] > 0.0;
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(reinterpret_cast<unsigned long long *>(count), (unsigned long long)n);
+}
+
+__global__ void spawn_search_kernel(long long ncell, int NE, int H, const double *cdf, const long long *lastc, const double *u,
+                                    const double *off, long long P, int32_t *face, double *x, double *y, double *sed, double *dir,
+                                    double *total_out)
+{
+    const double total = cdf[ncell - 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total_out) *total_out = total;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+        const double target = u[p] * total;
+        // first index with cdf > target (the reference walks its compacted cdf the same way)
+        long long lo = 0, hi = ncell;
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (cdf[mid] <= target) lo = mid + 1;
+            else hi = mid;
+        }
+        long long c = lo < ncell ? lo : *lastc;
+        const long long fa = c / ((long long)NE * NE);
+        const long long rem = c - fa * NE * NE;
+        const long long ei = rem / NE, ej = rem - ei * NE;
+        face[p] = (int32_t)fa;
+        x[p] = (double)(ei - H) + off[2 * p];
+        y[p] = (double)(ej - H) + off[2 * p + 1];
+        sed[p] = 0.0;
+        dir[p] = 0.0;
+    }
+}
+
+struct PendFlag {
+    const double *pending;
+    __device__ __forceinline__ bool operator()(const long long c) const { return pending[c] > 0.0; }
+};
+
+__global__ void pending_emit_kernel(const long long *idx, const long long *count, int NE, int H, double *pending, int32_t *face,
+                                    double *x, double *y, double *sed, long long *released_fx)
+{
+    const long long n = *count;
+    long long rel = 0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx[k];
+        const long long fa = c / ((long long)NE * NE);
+        const long long rem = c - fa * NE * NE;
+        const long long ei = rem / NE, ej = rem - ei * NE;
+        face[k] = (int32_t)fa;
+        x[k] = (double)(ei - H) + 0.5;
+        y[k] = (double)(ej - H) + 0.5;
+        sed[k] = pending[c];
+        rel += __double2ll_rn(pending[c] * FX_MASS);
+        pending[c] = 0.0;
+    }
+    for (int o = 16; o > 0; o >>= 1) rel += __shfl_down_sync(0xffffffffu, rel, o);
+    if ((threadIdx.x & 31) == 0 && rel) atomicAdd(reinterpret_cast<unsigned long long *>(released_fx), (unsigned long long)rel);
+}
+
+size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets)
+{
+    size_t a = 0, b = 0, c = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, a, (double *)nullptr, (double *)nullptr, (int)ncell);
+    cub::DeviceRadixSort::SortKeys(nullptr, b, (double *)nullptr, (double *)nullptr, (int)(max_droplets > 0 ? max_droplets : 1));
+    cub::DeviceSelect::If(nullptr, c, thrust::counting_iterator<long long>(0), (long long *)nullptr, (long long *)nullptr,
+                          (int)ncell, PendFlag{nullptr});
+    size_t m = a > b ? a : b;
+    return m > c ? m : c;
+}
+
+cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
+                       long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    double *w = ws_ptr<double>(ws, lay.cdf);
+    double *cdf = w + lay.ncell;
+    double *keys = ws_ptr<double>(ws, lay.sortkeys);
+    long long *lastc = ws_ptr<long long>(ws, lay.counters) + 2;
+    cudaError_t e = cudaMemsetAsync(lastc, 0, sizeof(long long), st);
+    if (e != cudaSuccess) return e;
+    if (nspawn_dev && (e = cudaMemsetAsync(nspawn_dev, 0, sizeof(long long), st)) != cudaSuccess) return e;
+    spawn_weight_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, s.base, s.mask,
+                                                             s.precip, w, lastc);
+    if (nspawn_dev) spawn_count_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, w, nspawn_dev);
+    size_t tb = lay.cubtmp_bytes;
+    e = cub::DeviceScan::InclusiveSum(ws_ptr<void>(ws, lay.cubtmp), tb, w, cdf, (int)lay.ncell, st);
+    if (e != cudaSuccess) return e;
+    tb = lay.cubtmp_bytes;
+    e = cub::DeviceRadixSort::SortKeys(ws_ptr<void>(ws, lay.cubtmp), tb, u, keys, (int)P, 0, 64, st);
+    if (e != cudaSuccess) return e;
+    spawn_search_kernel<<<grid_for(P), 256, 0, st>>>(lay.ncell, NE, g.H, cdf, lastc, keys, off, P, sp.face, sp.x, sp.y, sp.sed,
+                                                     sp.dir, total_dev);
+    return cudaPeekAtLastError();
+}
+
+cudaError_t count_pending(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, long long *count_dev, cudaStream_t st)
+{
+    long long *idx = ws_ptr<long long>(ws, lay.flags);
+    long long *cnt = ws_ptr<long long>(ws, lay.counters) + 3;
+    size_t tb = lay.cubtmp_bytes;
+    cudaError_t e = cub::DeviceSelect::If(ws_ptr<void>(ws, lay.cubtmp), tb, thrust::counting_iterator<long long>(0), idx, cnt,
+                                          (int)lay.ncell, PendFlag{s.pending}, st);
+    if (e != cudaSuccess) return e;
+    if (count_dev) e = cudaMemcpyAsync(count_dev, cnt, sizeof(long long), cudaMemcpyDeviceToDevice, st);
+    return e;
+}
+
+cudaError_t collect_pending(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, PgeSpawns &sp, long long offset,
+                            PgeStats *stats, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    long long *idx = ws_ptr<long long>(ws, lay.flags);
+    const long long *count_dev = ws_ptr<long long>(ws, lay.counters) + 3;
+    pending_emit_kernel<<<grid_for(lay.ncell / 64 + 1), 256, 0, st>>>(idx, count_dev, NE, g.H, s.pending, sp.face + offset,
+                                                                     sp.x + offset, sp.y + offset, sp.sed + offset,
+                                                                     reinterpret_cast<long long *>(&stats->released_fx));
+    return cudaPeekAtLastError();
+}
+
+}  // namespace pge

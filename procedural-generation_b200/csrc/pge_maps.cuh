@@ -1,0 +1,22 @@
+// pge_maps.cuh -- host-side launchers of the map passes (pge_maps.cu).
+#pragma once
+#include "pge_internal.cuh"
+
+namespace pge {
+void pack(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, cudaStream_t st);
+void refresh(const PgeState &s, const Layout &lay, void *ws, cudaStream_t st);
+void fold_ema(PgeState &s, const Layout &lay, void *ws, double ema, int exact, cudaStream_t st);
+void read_accumulators(const Layout &lay, void *ws, double *acc, double *dtr, double *mtr, double *pending, cudaStream_t st);
+void thermal(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double rate, double creep_rate, double cap, float soft,
+             float diff, double dep_floor, cudaStream_t st);
+void uplift(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double cap, double scale, cudaStream_t st);
+void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double land_fraction, double level,
+                double *shift_dev, cudaStream_t st);
+void halo_gather(const PgeHalo &h, double *field, int vector, cudaStream_t st);
+size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
+                       long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st);
+cudaError_t count_pending(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, long long *count_dev, cudaStream_t st);
+cudaError_t collect_pending(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, PgeSpawns &sp, long long offset,
+                            PgeStats *stats, cudaStream_t st);
+}  // namespace pge

@@ -1,0 +1,539 @@
+"""GPU erosion state and the per-iteration driver (the drop-in for the bake's
+``globe.erosion.maps`` plain path).
+
+Same names and argument meaning as the reference module
+(bake/globe/erosion/maps.py):
+
+* :class:`ErosionState` -- ``maps.ErosionState`` (maps.py:56-191), its arrays
+  held as CUDA tensors: float64 height / sediment / discharge / momentum /
+  pending / base / uplift, float32 hardness / precip / evap, uint8 mask, and
+  the face-shared float32 metric tables.
+* :func:`run_iteration` -- maps.py:839-1047: spawns drawn on the host by
+  ``params.rng(rng_stage, *key)`` in the reference's order (rain uniforms,
+  rain offsets, then the stockpiles' directions), inverse CDF, stockpile
+  re-injection and the droplet pass on the device (``pge_spawn_rain``,
+  ``pge_collect_pending``, ``pge_trace_apply``).  Returns the reference's
+  stats dict.
+* :func:`thermal_erosion`, :func:`apply_uplift`, :func:`start_replay`,
+  :func:`hold_datum`, :func:`step` -- maps.py:1050-1213, 1446-1617, plain path.
+
+Waves.  The reference freezes the terrain for a chunk of particles and
+applies their changes serially; here a wave of ``wave`` droplets is traced on
+frozen terrain and each droplet applies its own ledger (see
+``csrc/pge_droplets.cuh``).  ``wave=None`` uses the reference's own chunk
+size (``erosion.chunk`` / 16 chunks minimum); a larger wave keeps more of
+the GPU busy, and the trace-time concurrency divisor ``conc_scale`` follows
+the wave size as the reference's follows its chunk.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PgeGrid, PgeHalo, PgeParams, PgeSpawns, PgeState, PgeStats, check
+from .params import cell_units, check_plain, chunk_size, erosion_group, max_steps_of
+
+MASK_OUTSIDE, MASK_ACTIVE, MASK_FROZEN = 0, 1, 2
+
+
+def _ptr(t: torch.Tensor | None):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class ErosionState:
+    """GPU-resident erosion state (see the module docstring)."""
+
+    height: torch.Tensor
+    sediment: torch.Tensor
+    discharge: torch.Tensor
+    momentum: torch.Tensor
+    hardness: torch.Tensor
+    precip: torch.Tensor
+    evap: torch.Tensor
+    uplift: torch.Tensor
+    mask: torch.Tensor | None
+    metric: torch.Tensor  # (NE, NE, 3) float32, shared by every face
+    metric_inv: torch.Tensor
+    N: int
+    H: int
+    spherical: bool
+    height_unit_m: float
+    grid: object = None
+    pending: torch.Tensor = None
+    base: torch.Tensor = None
+    iteration: int = 0
+    land_target: float | None = None
+    deposit_on_exit: bool = False
+    max_droplets: int = 0
+    max_steps: int = 0
+    max_wave: int = 0
+    _ws: torch.Tensor = field(default=None, repr=False)
+    _halo: tuple = field(default=None, repr=False)
+    _spawn: dict = field(default=None, repr=False)
+
+    def __post_init__(self):
+        dev = self.height.device
+        if dev.type != "cuda":
+            raise RuntimeError("ErosionState lives on a CUDA device (the b200 backend has no CPU path)")
+        if self.pending is None:
+            self.pending = torch.zeros_like(self.height)
+        if self.base is None:
+            self.base = torch.zeros_like(self.height)
+
+    # -- constructors ----------------------------------------------------------
+    @classmethod
+    def from_arrays(cls, grid, height, sediment, discharge, momentum, hardness, precip, evap, uplift, mask=None,
+                    height_unit_m=None, pending=None, base=None, device="cuda", land_target=None) -> "ErosionState":
+        """From (6, NE, NE[, 2]) numpy arrays already in cell units."""
+        d = torch.device(device)
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=d)
+        f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=d)
+        m = None if mask is None or np.all(np.asarray(mask) == MASK_ACTIVE) else torch.as_tensor(np.ascontiguousarray(mask, np.uint8), device=d)
+        return cls(height=f64(height), sediment=f64(sediment), discharge=f64(discharge), momentum=f64(momentum),
+                   hardness=f32(hardness), precip=f32(precip), evap=f32(evap), uplift=f64(uplift), mask=m,
+                   metric=f32(grid.metric_face), metric_inv=f32(grid.metric_inv_face), N=grid.N, H=grid.H, spherical=True,
+                   height_unit_m=float(grid.cell_size_m if height_unit_m is None else height_unit_m), grid=grid,
+                   pending=None if pending is None else f64(pending), base=None if base is None else f64(base),
+                   land_target=land_target)
+
+    @classmethod
+    def from_grid(cls, grid, bedrock_m, hardness, precip, evap, uplift_m, eparams=None, mask=None, device="cuda") -> "ErosionState":
+        """Global six-face state from extended arrays in metres, as the
+        reference's ``ErosionState.from_grid`` (maps.py:152-191) builds it."""
+        unit = float(grid.cell_size_m)
+        arr = lambda x: np.asarray(getattr(x, "data", x))
+        F, NE = 6, grid.NE
+        return cls.from_arrays(grid, arr(bedrock_m).astype(np.float64) / unit, np.zeros((F, NE, NE)), np.zeros((F, NE, NE)),
+                               np.zeros((F, NE, NE, 2)), arr(hardness), arr(precip), arr(evap),
+                               arr(uplift_m).astype(np.float64) / unit, mask=mask, height_unit_m=unit, device=device)
+
+    @classmethod
+    def from_world(cls, world, device="cuda") -> "ErosionState":
+        st = cls.from_grid(world.grid, world.bedrock, world.hardness, world.precip, world.evap, world.uplift, device=device)
+        st.land_target = float(world.land_fraction)
+        return st
+
+    # -- views ------------------------------------------------------------------
+    @property
+    def F(self) -> int:
+        return self.height.shape[0]
+
+    @property
+    def NE(self) -> int:
+        return self.height.shape[1]
+
+    @property
+    def interior(self):
+        H, N = self.H, self.N
+        return (slice(None), slice(H, H + N), slice(H, H + N))
+
+    def surface(self) -> torch.Tensor:
+        return self.height + self.sediment
+
+    def total_mass(self) -> float:
+        """Sum of height + sediment + pending over the active interior (cell units)."""
+        t = (self.height + self.sediment + self.pending)[self.interior]
+        if self.mask is not None:
+            t = t[self.mask[self.interior] == MASK_ACTIVE]
+        return float(t.sum().item())
+
+    def to_numpy(self) -> dict:
+        return {k: getattr(self, k).detach().cpu().numpy() for k in ("height", "sediment", "discharge", "momentum", "pending", "base")}
+
+    # -- library plumbing ---------------------------------------------------------
+    def pge_grid(self) -> PgeGrid:
+        return PgeGrid(F=self.F, N=self.N, H=self.H, spherical=int(bool(self.spherical)),
+                       deposit_on_exit=int(bool(self.deposit_on_exit)), metric_shared=1, max_steps=int(self.max_steps),
+                       max_droplets=int(self.max_droplets), max_wave=int(self.max_wave))
+
+    def pge_state(self) -> PgeState:
+        return PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
+                        momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
+                        hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
+                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv))
+
+    def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1) -> None:
+        """Size the library workspace and spawn buffers for up to
+        ``max_droplets`` spawns of ``max_steps`` steps and ordered-apply
+        waves of up to ``max_wave`` droplets (grows, never shrinks)."""
+        if max_droplets <= self.max_droplets and max_steps <= self.max_steps and max_wave <= self.max_wave and self._ws is not None:
+            return
+        self.max_droplets = max(int(max_droplets), self.max_droplets)
+        self.max_steps = max(int(max_steps), self.max_steps)
+        self.max_wave = max(int(max_wave), self.max_wave, 1)
+        L = _lib.load()
+        g = self.pge_grid()
+        nbytes = int(L.pge_workspace_bytes(ctypes.byref(g)))
+        if nbytes == 0:
+            raise _lib.PgeError("pge_workspace_bytes rejected the grid: " + _lib.last_error())
+        self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.height.device)
+        n = self.max_droplets
+        d = self.height.device
+        self._spawn = {
+            "face": torch.empty(n, dtype=torch.int32, device=d),
+            "x": torch.empty(n, dtype=torch.float64, device=d),
+            "y": torch.empty(n, dtype=torch.float64, device=d),
+            "sed": torch.empty(n, dtype=torch.float64, device=d),
+            "dir": torch.empty(n, dtype=torch.float64, device=d),
+            "scal": torch.zeros(4, dtype=torch.float64, device=d),  # spawn total weight, datum shift
+            "cnt": torch.zeros(4, dtype=torch.int64, device=d),  # spawnable cells, stockpiles
+            "stats": torch.zeros(_lib.STATS_WORDS, dtype=torch.int64, device=d),
+            "host_scal": torch.zeros(4, dtype=torch.float64).pin_memory(),
+            "host_cnt": torch.zeros(4, dtype=torch.int64).pin_memory(),
+            "host_stats": torch.zeros(_lib.STATS_WORDS, dtype=torch.int64).pin_memory(),
+        }
+
+    @property
+    def workspace(self) -> torch.Tensor:
+        return self._ws
+
+    def halo_tables(self):
+        if self._halo is None:
+            hm = self.grid.halo
+            d = self.height.device
+            self._halo = (torch.as_tensor(hm.dst.astype(np.int32), device=d), torch.as_tensor(hm.src.astype(np.int32), device=d),
+                          torch.as_tensor(hm.w, device=d), torch.as_tensor(np.ascontiguousarray(hm.rot), device=d))
+        return self._halo
+
+    def exchange_halos(self) -> None:
+        """Refresh the halos of height, sediment, discharge and the rotated
+        momentum (maps.py:329-340)."""
+        if not self.spherical:
+            return
+        dst, src, w, rot = self.halo_tables()
+        h = PgeHalo(K=int(dst.shape[0]), dst=_ptr(dst), src=_ptr(src), w=_ptr(w), rot=_ptr(rot))
+        L = _lib.load()
+        st = _stream()
+        for t in (self.height, self.sediment, self.discharge):
+            check(L.pge_halo_gather(ctypes.byref(h), _ptr(t), 0, st), "pge_halo_gather")
+        check(L.pge_halo_gather(ctypes.byref(h), _ptr(self.momentum), 1, st), "pge_halo_gather")
+
+    def n_active_interior(self) -> int:
+        if self.mask is None:
+            return self.F * self.N * self.N
+        return int((self.mask[self.interior] == MASK_ACTIVE).sum().item())
+
+
+# --------------------------------------------------------------------------
+# one iteration
+# --------------------------------------------------------------------------
+def default_wave(ep, n_particles: int) -> int:
+    """The reference's chunk size: the wave that reproduces its terrain freezes."""
+    return chunk_size(ep, n_particles)
+
+
+def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, precision: int, mom_scale=1.0, disc_sat=None,
+                iter_deposit=None, threads_per_block=0, blocks_per_sm=0, apply=_lib.APPLY_ORDERED) -> PgeParams:
+    u = state.height_unit_m
+    return PgeParams(
+        dt=float(ep.dt), density=float(ep.density), friction=float(ep.friction), deposition_rate=float(ep.deposition_rate),
+        evap_rate=float(ep.evap_rate), k_mom=float(ep.k_mom), mom_scale=float(mom_scale), k_disc=float(ep.k_disc),
+        disc_saturation=float(ep.disc_saturation if disc_sat is None else disc_sat), disc_exponent=float(ep.disc_exponent),
+        slope_gain=float(ep.slope_gain), slope_sat=float(ep.slope_saturation), erodibility=float(ep.erodibility),
+        cover_depth=cell_units(ep, "cover_depth", u), min_volume=float(ep.min_volume_frac) * float(volume0),
+        max_erode=cell_units(ep, "max_erode", u), conc_scale=float(wave / (volume0 * P)), ocean_rate=float(ep.ocean_deposition_rate),
+        fan_room=cell_units(ep, "fan_room", u), dep_floor=cell_units(ep, "dep_floor_m", u), iter_erode=cell_units(ep, "iter_erode", u),
+        iter_deposit=float(cell_units(ep, "iter_deposit", u) if iter_deposit is None else iter_deposit),
+        fan_slope=float(ep.fan_slope), offshore_writeoff=float(ep.offshore_writeoff), ema=float(ep.ema),
+        max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
+        precision=int(precision), apply=int(apply), use_erode_cap=0, threads_per_block=int(threads_per_block),
+        blocks_per_sm=int(blocks_per_sm))
+
+
+def draw_spawns(params, rng_stage: str, key, P: int):
+    """The rain draws of one iteration in the reference's order: ``P``
+    uniforms, then ``(P, 2)`` offsets; the generator is returned for the
+    stockpile directions that follow."""
+    rng = params.rng(rng_stage, *key)
+    u = rng.random(P)
+    off = rng.random((P, 2))
+    return rng, u, off
+
+
+def run_iteration(state: ErosionState, params, iteration_key, n_particles: int | None = None,
+                  particles_per_cell: float | None = None, rng_stage: str = "erosion", log=None, wave: int | None = None,
+                  precision: int = _lib.PREC_F64, predrawn=None, threads_per_block: int = 0, blocks_per_sm: int = 0,
+                  events=None, apply: int = _lib.APPLY_ORDERED) -> dict:
+    """One particle pass (maps.py:839-1047) on the device; see the module
+    docstring.  ``predrawn`` may carry ``draw_spawns``' result for this
+    iteration (drawn ahead, host or device arrays); ``events`` a pair of
+    CUDA events recorded around the droplet pass (``pge_trace_apply``)."""
+    ep = erosion_group(params)
+    check_plain(ep)
+    key = iteration_key if isinstance(iteration_key, (tuple, list)) else (int(iteration_key),)
+    t0 = time.time()
+    if n_particles is None:
+        ppc = ep.particles_per_cell if particles_per_cell is None else particles_per_cell
+        n_particles = max(1, int(round(ppc * state.n_active_interior())))
+    P = int(n_particles)
+    max_steps = max_steps_of(ep, state.N)
+    # stockpiles re-injected: at most one per interior cell; the reference's chunk is at most erosion.chunk
+    state.reserve(P + state.F * state.N * state.N, max_steps,
+                  (int(ep.chunk) if wave is None else int(wave)) if apply == _lib.APPLY_ORDERED else 1)
+    rng, u, off = predrawn if predrawn is not None else draw_spawns(params, rng_stage, key, P)
+    L = _lib.load()
+    g = state.pge_grid()
+    s = state.pge_state()
+    sp = state._spawn
+    ws = state.workspace
+    st = _stream()
+    dev = state.height.device
+    u_d = torch.as_tensor(u, device=dev)
+    off_d = torch.as_tensor(off, device=dev)
+    spawns = PgeSpawns(face=_ptr(sp["face"]), x=_ptr(sp["x"]), y=_ptr(sp["y"]), sed=_ptr(sp["sed"]), dir=_ptr(sp["dir"]),
+                       count=P, volume0=0.0)
+    scal, cnt = sp["scal"], sp["cnt"]
+    nsp_ptr = ctypes.c_void_p(cnt.data_ptr())
+    npend_ptr = ctypes.c_void_p(cnt.data_ptr() + 8)
+    check(L.pge_spawn_rain(ctypes.byref(g), ctypes.byref(s), _ptr(u_d), _ptr(off_d), P, ctypes.byref(spawns), _ptr(scal),
+                           nsp_ptr, _ptr(ws), ws.numel(), st), "pge_spawn_rain")
+    check(L.pge_count_pending(ctypes.byref(g), ctypes.byref(s), npend_ptr, _ptr(ws), ws.numel(), st), "pge_count_pending")
+    hs, hc = sp["host_scal"], sp["host_cnt"]
+    hs.copy_(scal, non_blocking=True)
+    hc.copy_(cnt, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    total = float(hs[0])
+    n_spawnable, n_pend = int(hc[0]), int(hc[1])
+    stats = {"particles": 0, "entries": 0, "steps_mean": 0.0}
+    if n_spawnable == 0 or not (total > 0.0):
+        return stats
+    volume0 = total / P
+    stats_d = sp["stats"]
+    stats_d.zero_()
+    if n_pend:
+        dirs = torch.as_tensor(rng.random(n_pend) * (2.0 * np.pi), device=dev)
+        sp["dir"][P:P + n_pend].copy_(dirs)
+        check(L.pge_collect_pending(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), P, _ptr(stats_d), _ptr(ws), ws.numel(),
+                                    st), "pge_collect_pending")
+    Ptot = P + n_pend
+    spawns.count = Ptot
+    spawns.volume0 = volume0
+    disc_sat = float(ep.disc_saturation)
+    mom_scale = 1.0
+    if float(ep.disc_saturation_cells) > 0.0 or float(ep.momentum_saturation_cells) > 0.0:
+        rain_per_cell = volume0 * P / max(n_spawnable, 1)
+        if float(ep.disc_saturation_cells) > 0.0:
+            disc_sat = float(ep.disc_saturation_cells) * rain_per_cell
+        if float(ep.momentum_saturation_cells) > 0.0:
+            mom_scale = volume0 / (float(ep.momentum_saturation_cells) * rain_per_cell)
+    if float(ep.slope_limit_erode) > 0.0:
+        raise _lib.PgeError("erosion.slope_limit_erode is not supported by the b200 backend yet")
+    iter_deposit = cell_units(ep, "iter_deposit", state.height_unit_m)
+    if float(ep.slope_limit_deposit) > 0.0:
+        iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
+    w = default_wave(ep, Ptot) if wave is None else int(wave)
+    prm = make_params(state, ep, volume0, Ptot, w, precision, mom_scale, disc_sat, iter_deposit, threads_per_block, blocks_per_sm,
+                      apply)
+    if events is not None:
+        events[0].record()
+    check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), None, _ptr(stats_d),
+                            _ptr(ws), ws.numel(), st), "pge_trace_apply")
+    if events is not None:
+        events[1].record()
+    hst = sp["host_stats"]
+    hst.copy_(stats_d, non_blocking=True)
+    torch.cuda.current_stream().synchronize()
+    r = PgeStats.from_buffer_copy(hst.numpy().tobytes())
+    if r.errors:
+        raise _lib.PgeError("ordered apply: a cell hand-off wait gave up; the pass is invalid")
+    fx = _lib.FX_MASS
+    stats.update({"particles": Ptot, "entries": int(r.entries), "steps_mean": r.entries / max(Ptot, 1), "volume": volume0,
+                  "seconds": time.time() - t0, "droplet_steps": int(r.droplet_steps)})
+    stats["deaths"] = {n: int(r.deaths[k]) for k, n in enumerate(_lib.DEATH_NAMES)}
+    stats["clamped"] = int(r.clamped)
+    stats["to_pending"] = r.to_pending_fx / fx
+    stats["released"] = r.released_fx / fx
+    stats["pending_total"] = r.to_pending_fx / fx
+    stats["deficit_out"] = r.deficit_out_fx / fx
+    stats["lost_offshore"] = r.lost_offshore_fx / fx
+    stats["overflow"] = int(r.overflow)
+    stats["eroded"] = r.eroded_fx / fx
+    stats["deposited"] = r.deposited_fx / fx
+    stats["chunk"] = int(w)
+    stats["apply"] = "ordered" if apply == _lib.APPLY_ORDERED else "wave"
+    stats["n_pending"] = int(n_pend)
+    stats["disc_saturation"] = disc_sat
+    stats["mom_scale"] = mom_scale
+    if log is not None:
+        log(f"  particles {Ptot} volume {volume0:.3f} mean steps {stats['steps_mean']:.1f} deaths {stats['deaths']} "
+            f"clamped {stats['clamped']} pending {stats['pending_total']:.1f} ({stats['seconds']:.2f}s)")
+    return stats
+
+
+def _ensure_workspace(state: ErosionState, ep=None) -> None:
+    if state.workspace is None:
+        state.reserve(max(state.max_droplets, 1), max(state.max_steps, max_steps_of(ep, state.N) if ep is not None else 1))
+
+
+def thermal_erosion(state: ErosionState, params) -> None:
+    """Talus pass, then the creep pass (maps.py:1050-1085)."""
+    ep = erosion_group(params)
+    _ensure_workspace(state, ep)
+    L = _lib.load()
+    u = state.height_unit_m
+    check(L.pge_thermal(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), float(ep.thermal_rate),
+                        float(ep.creep_rate), cell_units(ep, "thermal_max", u), float(ep.talus_slope_soft),
+                        float(ep.talus_slope_hard), cell_units(ep, "dep_floor_m", u), _ptr(state.workspace),
+                        state.workspace.numel(), _stream()), "pge_thermal")
+
+
+def uplift_cap(state: ErosionState, ep) -> float | None:
+    if not state.spherical or float(getattr(ep, "uplift_max_m", 0.0)) <= 0.0:
+        return None
+    return cell_units(ep, "uplift_max_m", state.height_unit_m)
+
+
+def apply_uplift(state: ErosionState, cap: float | None = None, scale: float = 1.0) -> None:
+    """height += min(uplift, cap) - mean over the active interior (maps.py:1088-1147)."""
+    _ensure_workspace(state)
+    L = _lib.load()
+    check(L.pge_uplift(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), -1.0 if cap is None else float(cap),
+                       float(scale), _ptr(state.workspace), state.workspace.numel(), _stream()), "pge_uplift")
+
+
+def hold_datum(state: ErosionState, land_fraction: float, level: float = 0.0) -> float:
+    """Rigid shift holding round(land_fraction * M) interior cells at or
+    above ``level`` (maps.py:1446-1508); returns the shift (cell units)."""
+    _ensure_workspace(state)
+    L = _lib.load()
+    scal = state._spawn["scal"]
+    check(L.pge_hold_datum(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), float(land_fraction), float(level),
+                           ctypes.c_void_p(scal.data_ptr() + 8), _ptr(state.workspace), state.workspace.numel(), _stream()),
+          "pge_hold_datum")
+    return float(scal[1].item())
+
+
+def held_land_fraction(state: ErosionState, params) -> float:
+    if state.land_target is not None:
+        return float(state.land_target)
+    if float(getattr(getattr(params, "tectonics", None), "shelf_fraction", 0.0) or 0.0) > 0.0:
+        raise ValueError("shelf mode holds the bedrock's land fraction: set state.land_target")
+    return float(params.world.land_fraction)
+
+
+def start_replay(state: ErosionState, params) -> dict | None:
+    """``uplift_mode = 'replay'``: lower the start by the run's total applied
+    uplift, refresh the halos and hold the datum (maps.py:1178-1213)."""
+    ep = erosion_group(params)
+    if not state.spherical or str(getattr(ep, "uplift_mode", "stack")) != "replay":
+        return None
+    _ensure_workspace(state, ep)
+    apply_uplift(state, uplift_cap(state, ep), scale=-float(int(ep.iterations)))
+    state.exchange_halos()
+    info = {"datum_shift": 0.0}
+    if hasattr(params, "world"):
+        info["datum_shift"] = hold_datum(state, held_land_fraction(state, params))
+    return info
+
+
+def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
+    """One plain iteration (maps.py:1516-1617): particles, thermal erosion,
+    uplift, datum hold, halo exchange; increments ``state.iteration``."""
+    ep = erosion_group(params)
+    t0 = time.time()
+    st = run_iteration(state, params, iteration_key, log=log, **kw)
+    t1 = time.time()
+    thermal_erosion(state, params)
+    apply_uplift(state, uplift_cap(state, ep))
+    if state.spherical and hasattr(params, "world"):
+        st["datum_shift"] = hold_datum(state, held_land_fraction(state, params))
+    state.exchange_halos()
+    state.iteration += 1
+    st["seconds_route"] = 0.0
+    st["seconds_particles"] = t1 - t0
+    st["seconds_total"] = time.time() - t0
+    return st
+
+
+def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0: float, conc_scale: float,
+                     precision: int = _lib.PREC_F64, wave: int | None = None) -> dict:
+    """Parity hook: trace and apply the given droplets in one wave (or waves
+    of ``wave``) on the current state, recording each droplet's change list
+    in the reference layout (particle.py:275-818) and returning it with the
+    pass's accumulators.  The state's terrain is left unchanged."""
+    ep = erosion_group(params)
+    P = int(len(sp_face))
+    max_steps = max_steps_of(ep, state.N)
+    state.reserve(P, max_steps, 1)
+    L = _lib.load()
+    dev = state.height.device
+    cap = max_steps + 2 * 8 + 1 + 8 + 8
+    face = torch.as_tensor(np.asarray(sp_face, np.int32), device=dev)
+    xs = [torch.as_tensor(np.asarray(a, np.float64), device=dev) for a in (sp_x, sp_y, sp_sed, sp_dir)]
+    spawns = PgeSpawns(face=_ptr(face), x=_ptr(xs[0]), y=_ptr(xs[1]), sed=_ptr(xs[2]), dir=_ptr(xs[3]), count=P,
+                       volume0=float(volume0))
+    w = P if wave is None else int(wave)
+    prm = make_params(state, ep, volume0, P, w, precision, apply=_lib.APPLY_WAVE)
+    prm.conc_scale = float(conc_scale)
+    out = {"cl_cell": torch.zeros(P * cap, dtype=torch.int32, device=dev), "cl_delta": torch.zeros(P * cap, dtype=torch.float64, device=dev),
+           "cl_vol": torch.zeros(P * cap, dtype=torch.float32, device=dev), "cl_mom": torch.zeros(P * cap * 2, dtype=torch.float32, device=dev),
+           "cl_count": torch.zeros(P, dtype=torch.int64, device=dev), "sp_death": torch.zeros(P, dtype=torch.int8, device=dev)}
+    stats_d = torch.zeros(_lib.STATS_WORDS, dtype=torch.int64, device=dev)
+    ws = state.workspace
+    st = _stream()
+    g, s = state.pge_grid(), state.pge_state()
+    check(L.pge_trace_changelist(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), _ptr(out["cl_cell"]),
+                                 _ptr(out["cl_delta"]), _ptr(out["cl_vol"]), _ptr(out["cl_mom"]), _ptr(out["cl_count"]),
+                                 _ptr(out["sp_death"]), _ptr(stats_d), _ptr(ws), ws.numel(), st), "pge_trace_changelist")
+    acc = torch.zeros_like(state.height)
+    dtr = torch.zeros_like(state.height)
+    mtr = torch.zeros_like(state.momentum)
+    pend = torch.zeros_like(state.height)
+    check(L.pge_read_accumulators(ctypes.byref(g), _ptr(acc), _ptr(dtr), _ptr(mtr), _ptr(pend), _ptr(ws), ws.numel(), st),
+          "pge_read_accumulators")
+    torch.cuda.synchronize()
+    res = {k: v.cpu().numpy() for k, v in out.items()}
+    res["cl_mom"] = res["cl_mom"].reshape(-1, 2)
+    res.update(acc=acc.cpu().numpy(), disch_track=dtr.cpu().numpy(), mom_track=mtr.cpu().numpy(), pending=pend.cpu().numpy(),
+               cap=cap)
+    r = PgeStats.from_buffer_copy(stats_d.cpu().numpy().tobytes())
+    fx = _lib.FX_MASS
+    res["apply_out"] = np.array([float(r.clamped), r.to_pending_fx / fx, r.deficit_out_fx / fx, r.lost_offshore_fx / fx])
+    res["droplet_steps"] = int(r.droplet_steps)
+    return res
+
+
+def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0: float, n_rain: int | None = None,
+                 wave: int | None = None, precision: int = _lib.PREC_F64, apply: int = _lib.APPLY_ORDERED) -> dict:
+    """One droplet pass over explicitly given spawns (no random draws): pack,
+    waves, apply, fold and EMA, exactly as :func:`run_iteration` does after
+    spawning.  ``n_rain`` is the rain count the concurrency divisor is
+    computed with (the reference divides by the whole spawn count)."""
+    ep = erosion_group(params)
+    P = int(len(sp_face))
+    max_steps = max_steps_of(ep, state.N)
+    w = default_wave(ep, P) if wave is None else int(wave)
+    state.reserve(P, max_steps, w if apply == _lib.APPLY_ORDERED else 1)
+    L = _lib.load()
+    dev = state.height.device
+    sp = state._spawn
+    sp["face"][:P].copy_(torch.as_tensor(np.asarray(sp_face, np.int32)))
+    for k, a in (("x", sp_x), ("y", sp_y), ("sed", sp_sed), ("dir", sp_dir)):
+        sp[k][:P].copy_(torch.as_tensor(np.asarray(a, np.float64)))
+    spawns = PgeSpawns(face=_ptr(sp["face"]), x=_ptr(sp["x"]), y=_ptr(sp["y"]), sed=_ptr(sp["sed"]), dir=_ptr(sp["dir"]), count=P,
+                       volume0=float(volume0))
+    iter_deposit = cell_units(ep, "iter_deposit", state.height_unit_m)
+    prm = make_params(state, ep, volume0, P, w, precision, iter_deposit=iter_deposit, apply=apply)
+    stats_d = sp["stats"]
+    stats_d.zero_()
+    ws = state.workspace
+    check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns), ctypes.byref(prm),
+                            None, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
+    r = PgeStats.from_buffer_copy(stats_d.cpu().numpy().tobytes())
+    if r.errors:
+        raise _lib.PgeError("ordered apply: a cell hand-off wait gave up; the pass is invalid")
+    fx = _lib.FX_MASS
+    return {"droplets": int(r.droplets), "droplet_steps": int(r.droplet_steps), "entries": int(r.entries), "clamped": int(r.clamped),
+            "deaths": [int(v) for v in r.deaths], "to_pending": r.to_pending_fx / fx, "lost_offshore": r.lost_offshore_fx / fx,
+            "deficit_out": r.deficit_out_fx / fx, "eroded": r.eroded_fx / fx, "deposited": r.deposited_fx / fx}

@@ -23,10 +23,39 @@ import numpy as np
 from .geometry import Grid, exchange_halos, get_grid
 
 
-def value_noise(p: np.ndarray, rng: np.random.Generator, freq: float) -> np.ndarray:
-    """One octave of lattice value noise in [0, 1] at unit vectors ``p``."""
+def _device():
+    try:
+        import torch
+
+        return torch.device("cuda") if torch.cuda.is_available() else None
+    except ImportError:  # pragma: no cover
+        return None
+
+
+def value_noise(p, rng: np.random.Generator, freq: float):
+    """One octave of lattice value noise in [0, 1] at unit vectors ``p``
+    (numpy array, or a float64 torch tensor on any device)."""
     n = int(np.ceil(freq)) + 2
     lattice = rng.random((n + 1, n + 1, n + 1))
+    if not isinstance(p, np.ndarray):
+        import torch
+
+        lat = torch.as_tensor(lattice, device=p.device).reshape(-1)
+        q = (p + 1.0) * 0.5 * freq
+        i0 = torch.floor(q).to(torch.int64)
+        t = q - i0
+        t = t * t * (3.0 - 2.0 * t)
+        i0 = i0.clamp(0, n - 1)
+        out = torch.zeros(p.shape[:-1], dtype=p.dtype, device=p.device)
+        for dx in (0, 1):
+            wx = t[..., 0] if dx else 1.0 - t[..., 0]
+            for dy in (0, 1):
+                wy = t[..., 1] if dy else 1.0 - t[..., 1]
+                for dz in (0, 1):
+                    wz = t[..., 2] if dz else 1.0 - t[..., 2]
+                    idx = ((i0[..., 0] + dx) * (n + 1) + (i0[..., 1] + dy)) * (n + 1) + (i0[..., 2] + dz)
+                    out += wx * wy * wz * lat[idx]
+        return out
     q = (p + 1.0) * 0.5 * freq
     i0 = np.floor(q).astype(np.int64)
     t = q - i0
@@ -43,16 +72,20 @@ def value_noise(p: np.ndarray, rng: np.random.Generator, freq: float) -> np.ndar
     return out
 
 
-def fbm(p: np.ndarray, rng: np.random.Generator, octaves: int = 6, base_freq: float = 2.0, ridged: bool = False) -> np.ndarray:
+def fbm(p, rng: np.random.Generator, octaves: int = 6, base_freq: float = 2.0, ridged: bool = False):
     """Fractal sum of ``octaves`` octaves in [-1, 1] (ridged: in [0, 1])."""
-    out = np.zeros(p.shape[:-1])
+    out = 0.0
     amp, total = 1.0, 0.0
     for o in range(octaves):
         n = value_noise(p, rng, base_freq * 2 ** o)
-        out += amp * ((1.0 - np.abs(2.0 * n - 1.0)) if ridged else (2.0 * n - 1.0))
+        out = out + amp * ((1.0 - abs(2.0 * n - 1.0)) if ridged else (2.0 * n - 1.0))
         total += amp
         amp *= 0.5
     return out / total
+
+
+def _host(a) -> np.ndarray:
+    return a if isinstance(a, np.ndarray) else a.detach().cpu().numpy()
 
 
 def rank_map(v: np.ndarray, land_fraction: float, lo: float, hi: float) -> np.ndarray:
@@ -63,11 +96,17 @@ def rank_map(v: np.ndarray, land_fraction: float, lo: float, hi: float) -> np.nd
     return np.where(v < q, lo * (q - v) / max(q - vmin, 1e-30), hi * (v - q) / max(vmax - q, 1e-30))
 
 
-def interior_points(grid: Grid) -> np.ndarray:
-    """(6, N, N, 3) unit vectors of the interior cell centres."""
+def interior_points(grid: Grid, device=None):
+    """(6, N, N, 3) unit vectors of the interior cell centres (a torch
+    tensor on ``device`` when one is given)."""
     i = np.arange(grid.N) + grid.H
     EI, EJ = np.meshgrid(i, i, indexing="ij")
-    return np.stack([grid.centers_of(f, EI, EJ) for f in range(6)])
+    p = np.stack([grid.centers_of(f, EI, EJ) for f in range(6)])
+    if device is None:
+        return p
+    import torch
+
+    return torch.as_tensor(p, device=device)
 
 
 def _extend(grid: Grid, interior: np.ndarray, dtype) -> np.ndarray:
@@ -105,22 +144,27 @@ def plain_small_world(seed: int = 0, N: int = 128, H: int = 2, cell_size_m: floa
                  np.zeros((6, grid.NE, grid.NE), np.float32), land_fraction)
 
 
-def earth_world(seed: int = 0, N: int = 1024, H: int = 2, cell_size_m: float = 9773.0, land_fraction: float = 0.29) -> World:
+def earth_world(seed: int = 0, N: int = 1024, H: int = 2, cell_size_m: float = 9773.0, land_fraction: float = 0.29,
+                device="auto") -> World:
     """Earth-default world: fBm (6 octaves) plus ridged noise (4 octaves)
     mapped to -8000..+6000 m with 29 % land; latitude-banded rain 0.1..3.0
     modulated by fBm; uplift 0..2 mm per iteration from fBm; hardness
-    0.5 +- 0.25 fBm; evaporation multiplier 1."""
+    0.5 +- 0.25 fBm; evaporation multiplier 1.  The noise is evaluated on
+    the GPU when one is present (``device="auto"``), in the same float64
+    operations as on the host."""
     grid = get_grid(N, H, cell_size_m)
     rng = np.random.default_rng([seed, 1024])
-    p = interior_points(grid)
-    base = fbm(p, rng, 6) + 0.6 * fbm(p, rng, 4, base_freq=4.0, ridged=True)
+    dev = _device() if device == "auto" else device
+    p = interior_points(grid, dev)
+    base = _host(fbm(p, rng, 6) + 0.6 * fbm(p, rng, 4, base_freq=4.0, ridged=True))
     bed = rank_map(base, land_fraction, -8000.0, 6000.0)
-    lat = np.arcsin(np.clip(p[..., 2], -1.0, 1.0))
+    ph = _host(p)
+    lat = np.arcsin(np.clip(ph[..., 2], -1.0, 1.0))
     band = np.exp(-(lat / 0.25) ** 2) + 0.6 * np.exp(-((np.abs(lat) - 1.0) / 0.2) ** 2)
     band = band / band.max()
-    rain = np.clip(0.1 + 2.9 * band * (0.6 + 0.8 * (0.5 + 0.5 * fbm(p, rng, 4))), 0.1, 3.0)
-    upl = 0.002 * np.clip(0.5 + 0.5 * fbm(p, rng, 4), 0.0, 1.0)
-    hard = np.clip(0.5 + 0.25 * fbm(p, rng, 4), 0.0, 1.0)
+    rain = np.clip(0.1 + 2.9 * band * (0.6 + 0.8 * (0.5 + 0.5 * _host(fbm(p, rng, 4)))), 0.1, 3.0)
+    upl = 0.002 * np.clip(0.5 + 0.5 * _host(fbm(p, rng, 4)), 0.0, 1.0)
+    hard = np.clip(0.5 + 0.25 * _host(fbm(p, rng, 4)), 0.0, 1.0)
     ones = np.ones((6, grid.NE, grid.NE), np.float32)
     return World(grid, _extend(grid, bed, np.float32), _extend(grid, hard, np.float32),
                  np.clip(_extend(grid, rain, np.float32), 0.1, 3.0), ones, _extend(grid, upl, np.float32), land_fraction)

@@ -1,0 +1,92 @@
+"""Parity cases shared by the tests and the smoke check (test infrastructure).
+
+Each case is built from a committed golden fixture (tests/golden/, written
+by gen_golden.py from the reference itself) and carries an ``oracle``
+callable that recomputes the reference result with the C oracle.
+"""
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+for p in (ROOT, ROOT / "procedural-generation_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+from pgerosion.geometry import get_grid  # noqa: E402
+from pgerosion.params import ErosionParams, WorldGroup, WorldParams  # noqa: E402
+
+GOLDEN = ROOT / "tests" / "golden"
+
+
+def erosion_params(js: str) -> ErosionParams:
+    d = json.loads(js)
+    return ErosionParams(**{k: v for k, v in d.items() if k in ErosionParams.__dataclass_fields__})
+
+
+def isolated_case(path=GOLDEN / "trace_isolated.npz") -> dict:
+    """Droplets with pairwise-disjoint paths on an N=48 six-face world."""
+    t = np.load(path)
+    N, H = int(t["N"]), int(t["H"])
+    cs = float(t["cell_size_m"])
+    grid = get_grid(N, H, cs)
+    ep = erosion_params(str(t["params"]))
+    case = {k: t[k] for k in t.files if k not in ("params",)}
+    case.update(grid=grid, params=ep, N=N, H=H, cell_size_m=cs, volume0=float(t["volume0"]), conc_scale=float(t["conc_scale"]),
+                cap=int(t["cap"]))
+
+    def oracle():
+        from oracle import oracle as orc
+
+        F, NE = 6, N + 2 * H
+        st = orc.OracleState(height=t["height"].copy(), sediment=t["sediment"].copy(), discharge=t["discharge"].copy(),
+                             momentum=t["momentum"].copy(), hardness=t["hardness"], precip=np.ones((F, NE, NE), np.float32),
+                             evap=t["evap"], uplift=np.zeros((F, NE, NE)), mask=t["mask"],
+                             metric=np.ascontiguousarray(np.broadcast_to(grid.metric_face, (F, NE, NE, 3))),
+                             metric_inv=np.ascontiguousarray(np.broadcast_to(grid.metric_inv_face, (F, NE, NE, 3))),
+                             N=N, H=H, spherical=True, height_unit_m=cs, grid=grid, base=t["base"].copy())
+        st.pack()
+        tp = orc.trace_params(st, ep, case["volume0"], case["conc_scale"])
+        cl = orc.trace(st, tp, t["sp_face"], t["sp_x"], t["sp_y"], t["sp_sed"], t["sp_dir"], case["volume0"])
+        out = orc.apply(st, orc.apply_params(st, ep, ep.iter_deposit / cs), cl, case["cap"])
+        names = ("cl_cell", "cl_delta", "cl_vol", "cl_mom", "cl_count", "cl_lo", "cl_hi", "sp_death")
+        r = dict(zip(names, cl))
+        r.update(acc=st.acc, pending=st.pending, disch_track=st.disch_track, mom_track=st.mom_track, apply_out=np.array(out, float))
+        return r
+
+    case["oracle"] = oracle
+    return case
+
+
+def step_case(path=GOLDEN / "step_tiny.npz") -> dict:
+    """A six-face N=32 world and the reference's state after a few steps."""
+    from pgerosion.synth import World
+
+    t = np.load(path)
+    N, H, cs = int(t["N"]), int(t["H"]), float(t["cell_size_m"])
+    ep = erosion_params(str(t["params"]))
+    params = WorldParams(world=WorldGroup(seed=int(t["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(t["land_fraction"]),
+                                          halo=H), erosion=ep)
+    world = World(get_grid(N, H, cs), t["bedrock"], t["hardness"], t["precip"], t["evap"], t["uplift"], float(t["land_fraction"]))
+    return {"t": t, "params": params, "world": world, "iterations": int(t["iterations"]), "n_particles": int(t["n_particles"]),
+            "stats": json.loads(str(t["stats"]))}
+
+
+def changelist_rows(res: dict, cap: int):
+    """Per-droplet (cells, deltas, vols, moms) lists of a change list."""
+    cnt = res["cl_count"]
+    rows = []
+    for p in range(cnt.size):
+        sl = slice(p * cap, p * cap + int(cnt[p]))
+        rows.append((res["cl_cell"][sl], res["cl_delta"][sl], res["cl_vol"][sl], np.asarray(res["cl_mom"]).reshape(-1, 2)[sl]))
+    return rows
+
+
+def hypsometry(height, sediment, interior, unit, pct=(1, 5, 10, 25, 50, 75, 90, 95, 99)):
+    """Cell-count percentiles (metres) of the interior surface."""
+    s = (np.asarray(height) + np.asarray(sediment))[interior] * unit
+    return np.percentile(s, pct)
