@@ -133,11 +133,14 @@ def cpu_baseline(params, P, world, seconds=20.0):
             "sample": f"{n_it} full iteration(s) of the same N_c={params.world.N_c} world, {t_all:.1f} s"}
 
 
-def launches_per_iteration(nw: int, pending: bool, creep: bool) -> int:
+def launches_per_iteration(nw: int, pending: bool, creep: bool, ordered: bool) -> int:
     """Kernels of this library one plain iteration launches (library kernels
     -- CUB scan / sort / select -- not counted)."""
     spawn = 3 + (1 if pending else 0)
-    droplets = 2 + nw + (nw - 1) + 1          # pack x2, waves, refreshes, fold+EMA
+    if ordered:   # pack x2; per wave: trace, keys, flags, ranks, ordered apply; error report, mode, fold+EMA
+        droplets = 2 + 5 * nw + 3
+    else:         # pack x2; waves and the refreshes between them; mode, fold+EMA
+        droplets = 2 + nw + (nw - 1) + 2
     thermal = 4 * (2 if creep else 1)
     uplift = 3
     datum = 1 + 8 * 2 + 1
@@ -222,6 +225,44 @@ def run_b200(args, rank, world_size, dist):
         dist.all_reduce(tm, op=dist.ReduceOp.MAX)
     steps_all, e2e_all = float(tot[0]), float(tot[1])
     ms_max, e2e_ms_max = float(tm[0]), float(tm[1])
+    alt = None
+    if apply == _lib.APPLY_ORDERED and not args.no_alt:
+        # the order-free wave apply on the same world (one wave per iteration): faster, not the
+        # reference's serial apply
+        kw_alt = dict(kw, apply=_lib.APPLY_WAVE, wave=max(P + P // 8, 1))
+        it0 = n_total + args.steps
+        for k in range(3):
+            rng, u, off = gm.draw_spawns(params, "erosion", (it0 + k,), P)
+            gm.step(st, params, it0 + k, predrawn=(rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)), **kw_alt)
+        pre_alt = []
+        for k in range(args.alt_steps):
+            rng, u, off = gm.draw_spawns(params, "erosion", (it0 + 3 + k,), P)
+            pre_alt.append((rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)))
+        ta2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.alt_steps)]
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        e2[0].record()
+        alt_steps = 0
+        for k in range(args.alt_steps):
+            s2 = gm.step(st, params, it0 + 3 + k, predrawn=pre_alt[k], events=ta2[k], **kw_alt)
+            alt_steps += s2["droplet_steps"]
+        e2[1].record()
+        torch.cuda.synchronize()
+        alt_ms = e2[0].elapsed_time(e2[1])
+        t2 = torch.tensor([alt_steps, alt_ms], dtype=torch.float64, device=dev)
+        if dist:
+            dist.all_reduce(t2[:1])
+            dist.all_reduce(t2[1:], op=dist.ReduceOp.MAX)
+        avg2 = float(np.mean([a.elapsed_time(b) for a, b in ta2]))
+        ach2 = alt_steps / max(args.alt_steps, 1) * BYTES_PER_STEP / (avg2 * 1e-3) / 1e9
+        peak, _ = _peaks()
+        alt = {"apply": "wave (order-free, int64 fixed point; not the reference's serial apply)",
+               "value": float(t2[0]) / (float(t2[1]) * 1e-3), "unit": "droplet-steps/s", "steps": args.alt_steps,
+               "ms_per_step": float(t2[1]) / args.alt_steps,
+               "roofline": {"bound": "hbm", "achieved": ach2, "peak": peak, "unit": "GB/s", "frac": ach2 / peak,
+                            "ms_per_launch": avg2}}
     if rank != 0:
         return None
     peak, peak_kind = _peaks()
@@ -243,11 +284,14 @@ def run_b200(args, rank, world_size, dist):
                 "d2h_bytes_per_step": d2h // max(args.steps, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "droplet pass (pge_trace_apply: droplet waves + wave refreshes + pack + fold)",
+                     "kernel": "droplet pass (pge_trace_apply: trace waves, ordered apply or wave refreshes, pack, fold)",
                      "ms_per_launch": avg_ta, "bytes_per_step": BYTES_PER_STEP},
-        "gpu_launches": launches_per_iteration(max(n_waves // max(args.steps, 1), 1), pend_any, params.erosion.creep_rate > 0) * args.steps,
+        "gpu_launches": launches_per_iteration(max(n_waves // max(args.steps, 1), 1), pend_any, params.erosion.creep_rate > 0,
+                                               apply == _lib.APPLY_ORDERED) * args.steps,
         "clocks": clk.summary(),
     }
+    if alt is not None:
+        out["alt_wave_apply"] = alt
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
@@ -312,6 +356,8 @@ def main():
                     help="ordered: the reference's serial apply (default); wave: per-droplet ledgers against wave-start terrain")
     ap.add_argument("--n", type=int, default=None, help="override N_c (tests)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
+    ap.add_argument("--alt-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":

@@ -233,6 +233,7 @@ PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, 
  * field, or with vector = 1 a (F,NE,NE,2) field rotated per source. */
 PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream);
 
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,19 @@ int fail(int code, const char *fmt, ...)
     return code;
 }
 
+}  // namespace
+
+int pge_set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+namespace {
+
 int cuda_fail(cudaError_t e, const char *where)
 {
     return fail(PGE_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
@@ -278,12 +291,16 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 a.rec_base = a.d_begin;
                 a.counter = ctr + (w & 1);
                 a.counter_next = ctr + ((w + 1) & 1);
-                long long blocks = (a.d_end - a.d_begin + threads - 1) / threads;
-                if (blocks > maxblocks) blocks = maxblocks;
-                e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
-                                                 : launch_droplets_f32(a, (int)blocks, threads, st);
+                // a small wave is latency-bound: spread it over every SM (one or two warps each)
+                const long long nd = a.d_end - a.d_begin;
+                int tpb = threads;
+                while (tpb > 32 && (nd + tpb - 1) / tpb < 2LL * sm_count()) tpb >>= 1;
+                long long blocks = (nd + tpb - 1) / tpb;
+                if (blocks * tpb > lay.nslots) blocks = lay.nslots / tpb;
+                e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, tpb, st)
+                                                 : launch_droplets_f32(a, (int)blocks, tpb, st);
                 if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
-                ow.nw = a.d_end - a.d_begin;
+                ow.nw = nd;
                 oa.nw = ow.nw;
                 oa.epoch = (unsigned long long)(w + 1) << 24;
                 if ((e = ordered_wave(ow, st)) != cudaSuccess) return cuda_fail(e, "ordered apply");

@@ -479,7 +479,7 @@ __device__ __forceinline__ void sync_own(LCell &x, const LCell &changed)
 enum { ST_DROP, ST_STEPS, ST_ENTRIES, ST_CLAMPED, ST_OVER, ST_TOPEND, ST_DEFICIT, ST_LOSTOFF, ST_ERODED, ST_DEPOSITED,
        ST_DEATH0, ST_N = ST_DEATH0 + PGE_N_DEATHS };
 
-template <int MINB>
+template <int MINB, bool LEDGER>
 __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
 {
     const PgeParams &p = a.p;
@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             load_view(a, nf, nx, ny, nei, nej, nv);
             // the droplet's own change of the new cell, probed while its loads are in flight
             nxt.cell = nv.cell;
-            nxt.own = a.ledger ? t.lookup(nv.cell, nxt.tidx) : 0.0;
+            nxt.own = LEDGER ? t.lookup(nv.cell, nxt.tidx) : 0.0;
             if (nv.m == PGE_MASK_OUTSIDE) { exited = true; cause = PGE_DEATH_EXIT; break; }
             const R h1 = bilin(nv, 0);
             const R b1 = R(nv.base);
@@ -752,7 +752,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         // ---- the ledger, one entry behind the trace
         if (have_entry) {
             // `cur` still describes the cell the entry was made at
-            if (has_pe && a.ledger) {
+            if (has_pe && LEDGER) {
                 apply_entry(a, t, L, pe, pend, true, cur);
                 sync_own(cur, pend);
                 sync_own(nxt, pend);
@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             nout = cause == PGE_DEATH_OCEAN ? 1 : nring;
         }
         const int ring[SPREAD] = {r0, r1, r2, r3, r4, r5, r6, r7};
-        if (!a.ledger) {
+        if (!LEDGER) {
             // record-only: the final deposits go to the change list, the ordered apply does the rest
             for (int r = 0; r < nout; r++) {
                 if (a.rec_cell && rec_n < a.rec_cap) {

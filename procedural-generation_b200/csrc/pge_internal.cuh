@@ -62,6 +62,9 @@ struct Layout {
     int64_t ncell, nmetric, nslots, table_cap, table_slots, max_droplets, max_wave, wave_slots, cap;
 };
 
+// records the calling thread's error message (read back with pge_last_error) and returns code
+int pge_set_error(int code, const char *fmt, ...);
+
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // number of per-thread ledger tables (one per resident droplet thread)

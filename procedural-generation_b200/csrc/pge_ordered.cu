@@ -13,10 +13,14 @@
 //   * the entries of the wave are sorted by (cell, droplet, entry) and each
 //     entry learns D = the number of distinct earlier droplets that visit
 //     its cell, and whether it is its droplet's last visit there;
-//   * a droplet acquires a cell (waits until done[cell] == epoch + D) before
-//     its window reaches it, and releases it (done[cell] = epoch + D + 1)
-//     once its window has passed its last visit -- final deposits (and so
-//     the stockpile cell) are released after the droplet's last entry.
+//   * a droplet acquires a cell (waits until done[cell] == epoch + D) one
+//     entry before it writes there (the erosion floor and final-deposit
+//     ceiling read the next entry's cell), and releases it (done[cell] =
+//     epoch + D + 1) right after its last write there; the step-deposit
+//     ceiling of the following entry uses the live surface snapshotted at
+//     that write -- exactly what the serial order reads, since no other
+//     droplet runs between two entries of one droplet; the stockpile (death)
+//     cell is released after the stockpile update.
 // Every read and write of a cell therefore happens in exactly the
 // reference's serial order, and the float64 arithmetic is the reference's
 // (this file is compiled without FMA contraction).  Waits are bounded: a
@@ -157,101 +161,144 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
         if (K <= 0) continue;
         const long long b0 = q * a.cap;
         double deficit = 0.0, surplus = 0.0;
-        long long prev = -1, death = -1;
+        long long death = -1;
+        bool has_prev = false;
+        double prev_live = 0.0;  // the previous step entry's cell right after its write (the step-deposit ceiling)
         long long clamped = 0, eroded_fx = 0, deposited_fx = 0;
-        bool ok = acquire(a.done, a.cell[b0], a.epoch, a.D[b0], a.error);
-        if (ok && K > 1) ok = acquire(a.done, a.cell[b0 + 1], a.epoch, a.D[b0 + 1], a.error);
+        // entry descriptors: the current one and the next, loaded before any wait
+        long long c = a.cell[b0];
+        int Dc = a.D[b0];
+        bool lastc = a.last[b0];
+        double dlt = a.delta[b0];
+        float vv = a.vol[b0];
+        float m0 = a.mom[2 * b0], m1 = a.mom[2 * b0 + 1];
+        long long nc = -1;
+        int Dn = 0;
+        if (K > 1) {
+            nc = a.cell[b0 + 1];
+            Dn = a.D[b0 + 1];
+        }
+        bool ok = acquire(a.done, c, a.epoch, Dc, a.error);
         for (int k = 0; k < K && ok; k++) {
             const long long e = b0 + k;
             const bool has_next = k + 1 < K;
-            if (has_next && k >= 1) ok = acquire(a.done, a.cell[e + 1], a.epoch, a.D[e + 1], a.error);
+            // the next entry's cell: its live value is read now (erosion floor, final-deposit ceiling)
+            // and it is written next
+            if (has_next) ok = acquire(a.done, nc, a.epoch, Dn, a.error);
             if (!ok) break;
-            const long long c = a.cell[e];
+            // prefetch the descriptor after next
+            long long nnc = -1;
+            int Dnn = 0;
+            if (k + 2 < K) {
+                nnc = a.cell[e + 2];
+                Dnn = a.D[e + 2];
+            }
+            bool lastn = false;
+            double dltn = 0.0;
+            float vn = 0.0f, mn0 = 0.0f, mn1 = 0.0f;
+            if (has_next) {
+                lastn = a.last[e + 1];
+                dltn = a.delta[e + 1];
+                vn = a.vol[e + 1];
+                mn0 = a.mom[2 * (e + 1)];
+                mn1 = a.mom[2 * (e + 1) + 1];
+            }
+            const bool is_step = vv >= 0.0f;
             if (!(a.mask && a.mask[c] != PGE_MASK_ACTIVE)) {
-            const double d = a.delta[e];
-            const float v = a.vol[e];
-            const bool is_step = v >= 0.0f;
-            double *accp = a.acc4 + 4 * c;
-            const double hs = a.L[c].x;
-            const double acc = accp[0];
-            const double s_c = hs + acc;
-            const float b_c = a.B[c].w;
-            double acc_new;
-            if (d < 0.0) {
-                const double ew = -d;
-                double e_act = ew;
-                double room = p.iter_erode + acc;
-                if (a.ecap) {
-                    const double r2 = a.ecap[c] + acc;
-                    if (r2 < room) room = r2;
+                double *accp = a.acc4 + 4 * c;
+                const double hs = a.L[c].x;
+                const double acc = accp[0];
+                const double s_c = hs + acc;
+                const float b_c = a.B[c].w;
+                double nlive = 0.0;
+                if (has_next) nlive = a.L[nc].x + a.acc4[4 * nc];
+                double acc_new;
+                if (dlt < 0.0) {
+                    const double ew = -dlt;
+                    double e_act = ew;
+                    double room = p.iter_erode + acc;
+                    if (a.ecap) {
+                        const double r2 = a.ecap[c] + acc;
+                        if (r2 < room) room = r2;
+                    }
+                    if (e_act > room) e_act = room;
+                    double floor_ = s_c >= (double)b_c ? (double)b_c : s_c;
+                    if (has_next && nlive > floor_) floor_ = nlive;
+                    if (e_act > s_c - floor_) e_act = s_c - floor_;
+                    if (e_act < 0.0) e_act = 0.0;
+                    if (e_act < ew) {
+                        clamped++;
+                        deficit += ew - e_act;
+                    }
+                    acc_new = acc - e_act;
+                    eroded_fx += fx_mass(e_act);
+                } else {
+                    double want = dlt + surplus;
+                    surplus = 0.0;
+                    if (deficit > 0.0) {
+                        const double t = want < deficit ? want : deficit;
+                        want -= t;
+                        deficit -= t;
+                    }
+                    double d_act = want;
+                    const double room = p.iter_deposit - acc;
+                    if (d_act > room) d_act = room;
+                    bool has_ref = false;
+                    double ref_live = 0.0;
+                    if (is_step) {
+                        has_ref = has_prev;
+                        ref_live = prev_live;
+                    } else if (has_next) {
+                        has_ref = true;
+                        ref_live = nlive;
+                    }
+                    if (has_ref) {
+                        double ceil_ = ref_live + p.dep_floor;
+                        if (s_c < (double)b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
+                        const double lim = ceil_ - s_c;
+                        if (d_act > lim) d_act = lim;
+                    }
+                    if (s_c < (double)b_c) {
+                        const double lim = (double)b_c - p.dep_floor - s_c;
+                        if (d_act > lim) d_act = lim;
+                    }
+                    if (d_act < 0.0) d_act = 0.0;
+                    if (d_act < want) clamped++;
+                    surplus = want - d_act;
+                    acc_new = acc + d_act;
+                    deposited_fx += fx_mass(d_act);
+                    if (!is_step && death < 0) death = c;
                 }
-                if (e_act > room) e_act = room;
-                double floor_ = s_c >= (double)b_c ? (double)b_c : s_c;
-                if (has_next) {
-                    const long long nc = a.cell[e + 1];
-                    const double ns = a.L[nc].x + a.acc4[4 * nc];
-                    if (ns > floor_) floor_ = ns;
+                accp[0] = acc_new;
+                // the packed samples follow the live terrain (particle.py:1005-1009)
+                a.A[c].x = (float)(hs + acc_new);
+                const double sd = a.sediment[c] + acc_new;
+                a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
+                if (is_step) {
+                    if (vv > 0.0f) {
+                        accp[1] += (double)vv;
+                        accp[2] += (double)m0;
+                        accp[3] += (double)m1;
+                    }
+                    has_prev = true;
+                    prev_live = hs + acc_new;
                 }
-                if (e_act > s_c - floor_) e_act = s_c - floor_;
-                if (e_act < 0.0) e_act = 0.0;
-                if (e_act < ew) {
-                    clamped++;
-                    deficit += ew - e_act;
-                }
-                acc_new = acc - e_act;
-                eroded_fx += fx_mass(e_act);
-            } else {
-                double want = d + surplus;
-                surplus = 0.0;
-                if (deficit > 0.0) {
-                    const double t = want < deficit ? want : deficit;
-                    want -= t;
-                    deficit -= t;
-                }
-                double d_act = want;
-                const double room = p.iter_deposit - acc;
-                if (d_act > room) d_act = room;
-                long long ref = -1;
-                if (is_step) ref = prev;
-                else if (has_next) ref = a.cell[e + 1];
-                if (ref >= 0) {
-                    double ceil_ = a.L[ref].x + a.acc4[4 * ref] + p.dep_floor;
-                    if (s_c < (double)b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
-                    const double lim = ceil_ - s_c;
-                    if (d_act > lim) d_act = lim;
-                }
-                if (s_c < (double)b_c) {
-                    const double lim = (double)b_c - p.dep_floor - s_c;
-                    if (d_act > lim) d_act = lim;
-                }
-                if (d_act < 0.0) d_act = 0.0;
-                if (d_act < want) clamped++;
-                surplus = want - d_act;
-                acc_new = acc + d_act;
-                deposited_fx += fx_mass(d_act);
-                if (!is_step && death < 0) death = c;
             }
-            accp[0] = acc_new;
-            // the packed samples follow the live terrain (particle.py:1005-1009)
-            a.A[c].x = (float)(hs + acc_new);
-            const double sd = a.sediment[c] + acc_new;
-            a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
-            if (is_step) {
-                if (v > 0.0f) {
-                    accp[1] += (double)v;
-                    accp[2] += (double)a.mom[2 * e];
-                    accp[3] += (double)a.mom[2 * e + 1];
-                }
-                prev = c;
-            }
-            }
-            // the window has passed entry k-1: release its cell after its last visit (step entries;
-            // final deposits are held to the end, the stockpile cell among them)
-            if (k >= 1 && a.last[e - 1] && a.vol[e - 1] >= 0.0f)
-                release(a.done, a.cell[e - 1], a.epoch + (unsigned)a.D[e - 1] + 1ull);
+            // a cell is handed on right after the droplet's last write there; the stockpile (death)
+            // cell waits for the stockpile update
+            if (lastc && c != death) release(a.done, c, a.epoch + (unsigned)Dc + 1ull);
+            c = nc;
+            Dc = Dn;
+            lastc = lastn;
+            dlt = dltn;
+            vv = vn;
+            m0 = mn0;
+            m1 = mn1;
+            nc = nnc;
+            Dn = Dnn;
         }
         if (!ok) break;
-        long long topend = 0, lostoff = 0;  // (the stockpile cell is still held)
+        long long topend = 0, lostoff = 0;
         if (surplus > 0.0 && death >= 0) {
             if (a.L[death].x + a.acc4[4 * death] < (double)a.B[death].w) {
                 double keep = surplus * (1.0 - p.offshore_writeoff);
@@ -264,12 +311,15 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                 topend = fx_mass(surplus);
             }
         }
-        // release what is still held: the last entry's cell and every final deposit's
-        for (int k = K - 1; k >= 0; k--) {
-            const long long e = b0 + k;
-            const bool held = k == K - 1 || a.vol[e] < 0.0f;
-            if (!held) break;
-            if (a.last[e]) release(a.done, a.cell[e], a.epoch + (unsigned)a.D[e] + 1ull);
+        if (death >= 0) {
+            // the death cell's last visit is among the final deposits: find it and hand the cell on
+            for (int k = K - 1; k >= 0; k--) {
+                const long long e = b0 + k;
+                if (a.cell[e] == death) {
+                    release(a.done, death, a.epoch + (unsigned)a.D[e] + 1ull);
+                    break;
+                }
+            }
         }
         if (clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)clamped);
         if (topend) atomicAdd(&sstat[OS_TOPEND], (unsigned long long)topend);
