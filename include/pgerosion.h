@@ -233,6 +233,19 @@ PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, 
  * field, or with vector = 1 a (F,NE,NE,2) field rotated per source. */
 PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream);
 
+/* No counterpart in the reference.  pge_thermal for callers that cannot
+ * allocate device memory -- a host that owns the whole device heap through
+ * its own pool and forbids other allocations, or a loop that must not pay
+ * cudaMalloc's latency and implicit synchronisation: no workspace, the
+ * scratch is a static device array of PGE_NOALLOC_MAX_CELLS cells (10 MiB,
+ * held by every GPU that loads the library until exit).  Grids with more
+ * cells than that (F * NE * NE) are rejected with PGE_E_ARG.  The first call
+ * on a device looks up the array's device address (make it before any
+ * stream capture).  All calls share the array: calls that overlap on the
+ * GPU race, so order them. */
+#define PGE_NOALLOC_MAX_CELLS 262144
+PGE_API int pge_thermal_noalloc(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max,
+                                double talus_soft, double talus_hard, double dep_floor, void *stream);
 
 #ifdef __cplusplus
 }

@@ -345,6 +345,41 @@ void thermal(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double 
     }
 }
 
+// the same passes on caller-provided scratch (5 * ncell doubles), for the
+// entry point that allocates nothing (pge_static.cu)
+void thermal_on_scratch(const PgeGrid &g, PgeState &s, double *tb, long long n, double rate, double creep_rate, double cap,
+                        float soft, float diff, double dep_floor, cudaStream_t st)
+{
+    ThermalArgs t;
+    t.F = g.F;
+    t.NE = g.N + 2 * g.H;
+    t.h = s.height;
+    t.s = s.sediment;
+    t.metric = s.metric;
+    t.metric_shared = g.metric_shared;
+    t.talus_soft = soft;
+    t.talus_diff = diff;
+    t.mask = s.mask;
+    t.base = s.base;
+    t.dep_floor = dep_floor;
+    t.cap = cap;
+    t.out_total = tb;
+    t.scale = tb + n;
+    t.rscale = tb + 2 * n;
+    t.new_h = tb + 3 * n;
+    t.new_s = tb + 4 * n;
+    for (int pass = 0; pass < 2; pass++) {
+        if (pass == 1 && !(creep_rate > 0.0)) break;
+        t.hard = pass == 0 ? s.hardness : nullptr;
+        t.creep = pass;
+        t.rate = pass == 0 ? rate : creep_rate;
+        thermal_a_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        thermal_r_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        thermal_b_kernel<<<grid_for(n), 256, 0, st>>>(t);
+        copy2_kernel<<<grid_for(n), 256, 0, st>>>(n, t.new_h, t.new_s, s.height, s.sediment);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // deterministic reductions (fixed block count, fixed tree order)
 // ---------------------------------------------------------------------------

@@ -9,6 +9,8 @@ void fold_ema(PgeState &s, const Layout &lay, void *ws, double ema, int exact, c
 void read_accumulators(const Layout &lay, void *ws, double *acc, double *dtr, double *mtr, double *pending, cudaStream_t st);
 void thermal(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double rate, double creep_rate, double cap, float soft,
              float diff, double dep_floor, cudaStream_t st);
+void thermal_on_scratch(const PgeGrid &g, PgeState &s, double *tb, long long n, double rate, double creep_rate, double cap,
+                        float soft, float diff, double dep_floor, cudaStream_t st);
 void uplift(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double cap, double scale, cudaStream_t st);
 void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double land_fraction, double level,
                 double *shift_dev, cudaStream_t st);

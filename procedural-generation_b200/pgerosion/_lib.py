@@ -25,8 +25,10 @@ DEATH_NAMES = ("age", "ocean", "exit", "pit", "evap", "stop")
 EXPORTS = (
     "pge_version", "pge_last_error", "pge_workspace_bytes", "pge_spawn_rain", "pge_count_pending",
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
-    "pge_uplift", "pge_hold_datum", "pge_halo_gather",
+    "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc",
 )
+#: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
+NOALLOC_MAX_CELLS = 262144
 
 c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -105,6 +107,7 @@ def load(path: str | os.PathLike | None = None):
     L.pge_uplift.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, ctypes.c_size_t, c_vp]
     L.pge_hold_datum.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_halo_gather.argtypes = [P(PgeHalo), c_vp, c_i32, c_vp]
+    L.pge_thermal_noalloc.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_vp]
     for n in EXPORTS:
         if n not in ("pge_version", "pge_last_error", "pge_workspace_bytes"):
             getattr(L, n).restype = ctypes.c_int
