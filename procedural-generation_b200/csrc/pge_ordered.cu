@@ -178,14 +178,34 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
             nc = a.cell[b0 + 1];
             Dn = a.D[b0 + 1];
         }
-        bool ok = acquire(a.done, c, a.epoch, Dc, a.error);
+        bool ok = true;
+        bool have_c = false;       // the current entry's cell is acquired
+        bool acc_known = false;    // acc_c holds its net change (read when it was acquired as the next cell)
+        double acc_c = 0.0;
         for (int k = 0; k < K && ok; k++) {
             const long long e = b0 + k;
             const bool has_next = k + 1 < K;
-            // the next entry's cell: its live value is read now (erosion floor, final-deposit ceiling)
-            // and it is written next
-            if (has_next) ok = acquire(a.done, nc, a.epoch, Dn, a.error);
-            if (!ok) break;
+            // read-only data of this entry's cell, loaded before any wait
+            const double hs = a.L[c].x;
+            const float b_c = a.B[c].w;
+            const double sed_c = a.sediment[c];
+            if (!have_c) {
+                ok = acquire(a.done, c, a.epoch, Dc, a.error);
+                if (!ok) break;
+                have_c = true;
+            }
+            // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell
+            // live: acquire it now; a step deposit does not, and acquires it only before writing it
+            const bool is_step = vv >= 0.0f;
+            const bool reads_next = has_next && (dlt < 0.0 || !is_step);
+            double hs_n = 0.0, acc_n = 0.0;
+            if (reads_next) {
+                hs_n = a.L[nc].x;
+                ok = acquire(a.done, nc, a.epoch, Dn, a.error);
+                if (!ok) break;
+                acc_n = a.acc4[4 * nc];
+            }
+            if (!acc_known) acc_c = a.acc4[4 * c];
             // prefetch the descriptor after next
             long long nnc = -1;
             int Dnn = 0;
@@ -203,16 +223,12 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                 mn0 = a.mom[2 * (e + 1)];
                 mn1 = a.mom[2 * (e + 1) + 1];
             }
-            const bool is_step = vv >= 0.0f;
+            double acc_new = acc_c;
             if (!(a.mask && a.mask[c] != PGE_MASK_ACTIVE)) {
                 double *accp = a.acc4 + 4 * c;
-                const double hs = a.L[c].x;
-                const double acc = accp[0];
+                const double acc = acc_c;
                 const double s_c = hs + acc;
-                const float b_c = a.B[c].w;
-                double nlive = 0.0;
-                if (has_next) nlive = a.L[nc].x + a.acc4[4 * nc];
-                double acc_new;
+                const double nlive = hs_n + acc_n;
                 if (dlt < 0.0) {
                     const double ew = -dlt;
                     double e_act = ew;
@@ -272,7 +288,7 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                 accp[0] = acc_new;
                 // the packed samples follow the live terrain (particle.py:1005-1009)
                 a.A[c].x = (float)(hs + acc_new);
-                const double sd = a.sediment[c] + acc_new;
+                const double sd = sed_c + acc_new;
                 a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
                 if (is_step) {
                     if (vv > 0.0f) {
@@ -287,6 +303,17 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
             // a cell is handed on right after the droplet's last write there; the stockpile (death)
             // cell waits for the stockpile update
             if (lastc && c != death) release(a.done, c, a.epoch + (unsigned)Dc + 1ull);
+            // the next entry's cell: acquired (and its net change known) if this entry read it;
+            // the same cell again keeps its acquisition and its updated net change
+            if (has_next && nc == c) {
+                have_c = true;
+                acc_known = true;
+                acc_c = acc_new;
+            } else {
+                have_c = reads_next;
+                acc_known = reads_next;
+                acc_c = acc_n;
+            }
             c = nc;
             Dc = Dn;
             lastc = lastn;

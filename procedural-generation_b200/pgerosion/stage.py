@@ -1,0 +1,234 @@
+"""The erosion stage driver on the GPU: the drop-in for the bake's
+``globe.erosion.run`` plain path (bake/globe/erosion/run.py).
+
+Same contract: ``OUTPUTS`` and ``run(store, params, log) -> info``
+(run.py:63, 374-551).  The stage's inputs are the coarse fields ``bedrock``,
+``hardness``, ``uplift``, ``precip``, ``evap``; its outputs ``height``,
+``sediment``, ``discharge``, ``momentum`` as float32 metres (maps.py:738-752).
+Checkpoints keep the bake's format (run.py:100-225): ``erosion_iterNNNN.npz``
+with the float64 cell-unit arrays ``height, sediment, discharge, momentum,
+pending, lake_load``, written to ``.tmp`` then renamed, then a ``.json`` with
+the iteration and the parameter hash; the two newest checkpoints of a hash
+family are kept; a run resumes from the newest matching checkpoint at or
+below its end.  The hash adds this backend's token and apply mode, because
+its float results are not the CPU backend's bit for bit.
+
+``store`` is duck-typed: anything with ``load_field(name, grid)`` (returning
+an object with ``.data`` or an array), ``save_field(name, array)`` and a
+``checkpoint_dir`` path works -- the bake's ``WorldStore`` through a thin
+adapter, or :class:`LocalStore` below (the bake's ``coarse/<name>.f{k}.npy``
+layout).
+"""
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import json
+import re
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from . import maps as gm
+from .geometry import exchange_halos, get_grid
+from .params import check_plain, erosion_group
+
+OUTPUTS = ["height", "sediment", "discharge", "momentum"]
+#: bumped whenever a change alters this backend's results (part of the checkpoint hash)
+BACKEND_VERSION = 1
+_CKPT_RE = re.compile(r"erosion_iter(\d+)\.npz$")
+
+
+class LocalStore:
+    """A world directory with the bake's field layout: interior faces in
+    ``coarse/<name>.f{k}.npy``, checkpoints in ``checkpoints/``."""
+
+    def __init__(self, root):
+        self.root = Path(root)
+        self.coarse = self.root / "coarse"
+        self.checkpoint_dir = self.root / "checkpoints"
+
+    def save_field(self, name: str, arr: np.ndarray, H: int) -> None:
+        self.coarse.mkdir(parents=True, exist_ok=True)
+        for k in range(6):
+            np.save(self.coarse / f"{name}.f{k}.npy", np.ascontiguousarray(arr[k, H:-H, H:-H]))
+
+    def has_field(self, name: str) -> bool:
+        return (self.coarse / f"{name}.f0.npy").exists()
+
+    def load_field(self, name: str, grid, vector: bool = False) -> np.ndarray:
+        """The six faces with their halos filled by the grid's cubic exchange
+        (FaceField.load, bake/globe/field.py:327-338)."""
+        faces = np.stack([np.load(self.coarse / f"{name}.f{k}.npy") for k in range(6)])
+        H, NE = grid.H, grid.NE
+        out = np.zeros((6, NE, NE) + faces.shape[3:], dtype=faces.dtype)
+        out[:, H:H + grid.N, H:H + grid.N] = faces
+        exchange_halos(grid, out, vector=vector)
+        return out
+
+
+def _field(store, name, grid):
+    v = store.load_field(name, grid)
+    return np.asarray(getattr(v, "data", v))
+
+
+def ckpt_hash(params, apply: int) -> str:
+    """World and erosion parameters (run-control knobs normalised out, as
+    run.py:68-97 does), the backend token, its version and the apply mode."""
+    ep = erosion_group(params)
+    e = dataclasses.asdict(ep) if dataclasses.is_dataclass(ep) else dict(vars(ep))
+    replay = str(e.get("uplift_mode", "stack")) == "replay"
+    for k in ("checkpoint_every", "quicklook_every", "resume"):
+        e.pop(k, None)
+    if not replay:
+        e["iterations"] = 0
+    w = params.world
+    wd = dataclasses.asdict(w) if dataclasses.is_dataclass(w) else dict(vars(w))
+    s = json.dumps({"world": wd, "erosion": e}, sort_keys=True, default=str)
+    return hashlib.sha256(s.encode()).hexdigest()[:16] + f":b200v{BACKEND_VERSION}:apply{apply}"
+
+
+def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
+    d = Path(store.checkpoint_dir)
+    d.mkdir(parents=True, exist_ok=True)
+    it = state.iteration
+    p = d / f"erosion_iter{it:04d}.npz"
+    tmp = p.with_suffix(".npz.tmp")
+    a = state.to_numpy()
+    arrays = dict(height=a["height"], sediment=a["sediment"], discharge=a["discharge"], momentum=a["momentum"],
+                  pending=a["pending"], lake_load=np.zeros_like(a["height"]))
+    with open(tmp, "wb") as fh:
+        np.savez(fh, **arrays)
+    tmp.replace(p)
+    meta = {"iteration": it, "params_hash": ckpt_hash(params, apply), "height_unit_m": state.height_unit_m,
+            "time": time.strftime("%Y-%m-%dT%H:%M:%S")}
+    with open(p.with_suffix(".json"), "w") as fh:
+        json.dump(meta, fh, indent=1)
+    prune_checkpoints(d, meta["params_hash"], keep=2)
+    return p
+
+
+def prune_checkpoints(d: Path, params_hash: str, keep: int = 2) -> None:
+    """Keep the ``keep`` newest checkpoints of one hash family (run.py:140-164)."""
+    mine = []
+    for q in Path(d).glob("erosion_iter*.npz"):
+        m = _CKPT_RE.search(q.name)
+        jq = q.with_suffix(".json")
+        if not m or not jq.exists():
+            continue
+        try:
+            if json.loads(jq.read_text()).get("params_hash") != params_hash:
+                continue
+        except json.JSONDecodeError:
+            continue
+        mine.append((int(m.group(1)), q))
+    for _, q in sorted(mine)[: max(0, len(mine) - keep)]:
+        q.unlink(missing_ok=True)
+        q.with_suffix(".json").unlink(missing_ok=True)
+
+
+def find_checkpoint(store, params, apply: int, max_iteration: int | None = None):
+    """Newest checkpoint with a matching hash at or below ``max_iteration``
+    (run.py:167-192); a truncated ``.json`` is skipped."""
+    d = Path(store.checkpoint_dir)
+    if not d.exists():
+        return None
+    want = ckpt_hash(params, apply)
+    best = None
+    for p in d.glob("erosion_iter*.npz"):
+        if not _CKPT_RE.search(p.name):
+            continue
+        jp = p.with_suffix(".json")
+        if not jp.exists():
+            continue
+        try:
+            meta = json.loads(jp.read_text())
+        except json.JSONDecodeError:
+            continue
+        if meta.get("params_hash") != want:
+            continue
+        it = int(meta.get("iteration", -1))
+        if max_iteration is not None and it > max_iteration:
+            continue
+        if best is None or it > best[1]["iteration"]:
+            best = (p, meta)
+    return best
+
+
+def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
+    import torch
+
+    with np.load(path) as z:
+        for k in ("height", "sediment", "discharge", "momentum"):
+            getattr(state, k).copy_(torch.as_tensor(z[k]))
+        state.pending.copy_(torch.as_tensor(z["pending"]) if "pending" in z.files else torch.zeros_like(state.pending))
+    state.iteration = int(meta["iteration"])
+
+
+def build_state(store, params, device="cuda") -> gm.ErosionState:
+    """The iteration-0 state from the stage inputs (run.py:237-296, plain path)."""
+    w = params.world
+    grid = get_grid(int(w.N_c), int(w.halo), float(w.cell_size_m))
+    st = gm.ErosionState.from_grid(grid, _field(store, "bedrock", grid), _field(store, "hardness", grid),
+                                   _field(store, "precip", grid), _field(store, "evap", grid), _field(store, "uplift", grid),
+                                   device=device)
+    st.land_target = float(w.land_fraction)
+    return st
+
+
+def write_outputs(store, state: gm.ErosionState) -> None:
+    """float32 metres, as ErosionState.fields (maps.py:738-752)."""
+    a = state.to_numpy()
+    u = state.height_unit_m
+    H = state.H
+    store.save_field("height", (a["height"] * u).astype(np.float32), H)
+    store.save_field("sediment", (a["sediment"] * u).astype(np.float32), H)
+    store.save_field("discharge", a["discharge"].astype(np.float32), H)
+    store.save_field("momentum", a["momentum"].astype(np.float32), H)
+
+
+def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | None = None) -> dict:
+    """The erosion stage (run.py:374-551, plain path) on the GPU."""
+    ep = erosion_group(params)
+    check_plain(ep)
+    n_iter = int(ep.iterations)
+    state = build_state(store, params)
+    land0 = float((state.surface()[state.interior] >= 0).float().mean().item())
+    rep = gm.start_replay(state, params)
+    ck = find_checkpoint(store, params, apply, max_iteration=n_iter) if ep.resume else None
+    if ck is not None:
+        load_checkpoint(state, *ck)
+        log(f"[erosion] resumed from {ck[0].name} (iteration {state.iteration})")
+    times, clamped, lost_offshore, datum = [], 0, 0.0, 0.0
+    while state.iteration < n_iter:
+        it = state.iteration
+        t0 = time.time()
+        st = gm.step(state, params, it, apply=apply, wave=wave)
+        times.append(time.time() - t0)
+        clamped += int(st.get("clamped", 0))
+        lost_offshore += float(st.get("lost_offshore", 0.0))
+        datum += float(st.get("datum_shift", 0.0))
+        d = st.get("deaths", {})
+        log(f"[erosion] iter {it + 1}/{n_iter}: {st['particles']} particles, mean {st['steps_mean']:.0f} steps, "
+            f"deaths ocean {d.get('ocean', 0)} pit {d.get('pit', 0)} age {d.get('age', 0)}, clamped {st.get('clamped', 0)}, "
+            f"pending {st.get('pending_total', 0.0):.1f}, {times[-1]:.2f}s")
+        done = state.iteration
+        if ep.checkpoint_every > 0 and (done % ep.checkpoint_every == 0 or done == n_iter):
+            p = save_checkpoint(store, state, params, apply)
+            log(f"[erosion] checkpoint -> {p.name}")
+    write_outputs(store, state)
+    a = state.to_numpy()
+    inter = state.interior
+    surf = (a["height"] + a["sediment"])[inter]
+    u = state.height_unit_m
+    info = {"iterations": n_iter, "height_unit_m": u, "seconds_per_iteration": float(np.mean(times)) if times else 0.0,
+            "land_fraction": float(np.mean(surf >= 0)), "land_fraction_bedrock": land0,
+            "max_discharge": float(a["discharge"][inter].max()), "sediment_mean_m": float(a["sediment"][inter].mean() * u),
+            "pending_total_m": float(a["pending"][inter].sum() * u), "clamped_entries": clamped,
+            "datum_drift_m": datum * u, "lost_offshore_m": lost_offshore * u, "uplift_mode": str(ep.uplift_mode),
+            "backend": "b200", "apply": "ordered" if apply == _lib.APPLY_ORDERED else "wave"}
+    if rep is not None:
+        info["replay_datum_start_m"] = rep["datum_shift"] * u
+    return info

@@ -1,0 +1,43 @@
+"""The GPU stage driver end to end: outputs, checkpoints, and a resumed run
+that lands on the continuous run's outputs byte for byte
+(bake/tests/test_erosion.py:456-493 adapted)."""
+import numpy as np
+import pytest
+
+from pgerosion import stage, synth
+from pgerosion.params import ErosionParams, WorldGroup, WorldParams, plain_knobs
+
+pytestmark = pytest.mark.gpu
+
+
+def _world_store(tmp_path):
+    w = synth.earth_world(seed=4, N=32, H=2, cell_size_m=50.0, land_fraction=0.3)
+    st = stage.LocalStore(tmp_path)
+    for name in ("bedrock", "hardness", "precip", "evap", "uplift"):
+        st.save_field(name, getattr(w, name), w.grid.H)
+    p = WorldParams(world=WorldGroup(seed=4, N_c=32, cell_size_m=50.0, land_fraction=0.3, halo=2),
+                    erosion=ErosionParams(**{**plain_knobs(), "iterations": 6, "checkpoint_every": 3, "max_steps": 48,
+                                             "friction": 0.05, "erodibility": 0.3, "deposition_rate": 0.3, "evap_rate": 0.01,
+                                             "uplift_mode": "replay", "particles_per_cell": 0.5}))
+    return st, p
+
+
+def test_stage_run_checkpoints_and_resume(cuda, tmp_path):
+    st, p = _world_store(tmp_path)
+    info = stage.run(st, p, log=lambda m: None)
+    assert info["iterations"] == 6 and info["backend"] == "b200"
+    out = {n: np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)]) for n in stage.OUTPUTS}
+    assert out["height"].dtype == np.float32 and out["momentum"].shape[-1] == 2
+    assert (st.checkpoint_dir / "erosion_iter0003.npz").exists() and (st.checkpoint_dir / "erosion_iter0006.json").exists()
+    with np.load(st.checkpoint_dir / "erosion_iter0006.npz") as z:
+        assert set(z.files) >= {"height", "sediment", "discharge", "momentum", "pending", "lake_load"}
+        assert z["height"].dtype == np.float64
+    # drop the last checkpoint: the driver resumes from iteration 3 and lands on the same outputs
+    for suf in (".npz", ".json"):
+        (st.checkpoint_dir / f"erosion_iter0006{suf}").unlink()
+    msgs = []
+    stage.run(st, p, log=msgs.append)
+    assert any("resumed" in m and "iteration 3" in m for m in msgs), msgs
+    for n in stage.OUTPUTS:
+        again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
+        assert again.tobytes() == out[n].tobytes(), n
