@@ -161,7 +161,9 @@ Layout layout(const PgeGrid &g)
     L.w_segscan = take(4 * ws);
     L.w_temp_bytes = ordered_temp_bytes(ws);
     L.w_temp = take(L.w_temp_bytes);
-    L.done = take(8 * L.ncell);
+    L.w_dth = take(4 * L.max_wave);
+    L.w_keep = take(8 * L.max_wave);
+    L.hand = take(16 * L.ncell);
     L.error = take(256);
     L.total = o;
     return L;
@@ -232,7 +234,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         const long long nw = (P + wave - 1) / wave;
         if (p->apply == PGE_APPLY_ORDERED && !rec_cell) {
             // exact mode: record each wave's change lists, then apply them in droplet order
-            if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.done), 0, 8 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset done");
+            if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.hand), 0, 16 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset hand");
             if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.error), 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset error");
             a.ledger = 0;
             a.rec_cell = ws_ptr<int32_t>(ws, lay.w_cell);
@@ -260,20 +262,18 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.ecap = a.ecap;
             oa.acc4 = ws_ptr<double>(ws, lay.acc4);
             oa.pend = ws_ptr<double>(ws, lay.pend);
-            oa.done = ws_ptr<unsigned long long>(ws, lay.done);
+            oa.hand = ws_ptr<double2>(ws, lay.hand);
+            oa.dth = ws_ptr<int32_t>(ws, lay.w_dth);
+            oa.keep = ws_ptr<double>(ws, lay.w_keep);
             oa.p = *p;
             oa.stats = stats;
             oa.error = ws_ptr<int>(ws, lay.error);
             ow.cap = (int)lay.cap;
-            int kbits = 0, pbits = 0, cbits = 0;
-            while ((1LL << kbits) < lay.cap) kbits++;
-            while ((1LL << pbits) < wave) pbits++;
+            // sort keys: the cell, cbits wide; all ones marks a slot past its list's end
+            int cbits = 0;
             while ((1LL << cbits) < lay.ncell + 1) cbits++;
-            ow.kbits = kbits;
-            ow.pbits = pbits;
-            ow.end_bit = cbits + pbits + kbits;
-            if (ow.end_bit > 63) return fail(PGE_E_ARG, "grid, wave and max_steps too large for 63-bit sort keys");
-            ow.invalid = (1ull << ow.end_bit) - 1ull;
+            ow.end_bit = cbits;
+            ow.invalid = (1ull << cbits) - 1ull;
             ow.keys_in = ws_ptr<unsigned long long>(ws, lay.w_keys0);
             ow.keys_out = ws_ptr<unsigned long long>(ws, lay.w_keys1);
             ow.vals_in = ws_ptr<int32_t>(ws, lay.w_vals0);

@@ -8,19 +8,26 @@
 // c_k.  So the apply of droplet p depends on earlier droplets only through
 // the cells in its sliding window {c_{k-1}, c_k, c_{k+1}}.
 //
-// Here every droplet of a wave applies its own list on its own thread, and
+// Here every droplet of a wave applies its own list on its own warp, and
 // each cell is handed from droplet to droplet in droplet order:
 //   * the entries of the wave are sorted by (cell, droplet, entry) and each
 //     entry learns D = the number of distinct earlier droplets that visit
 //     its cell, and whether it is its droplet's last visit there;
-//   * a droplet acquires a cell (waits until done[cell] == epoch + D) one
-//     entry before it writes there (the erosion floor and final-deposit
-//     ceiling read the next entry's cell), and releases it (done[cell] =
-//     epoch + D + 1) right after its last write there; the step-deposit
-//     ceiling of the following entry uses the live surface snapshotted at
-//     that write -- exactly what the serial order reads, since no other
-//     droplet runs between two entries of one droplet; the stockpile (death)
-//     cell is released after the stockpile update.
+//   * a cell's live net change and its hand-off counter share one 16-byte
+//     word, read and written as single 128-bit accesses: a droplet acquires
+//     a cell (polls until the counter is epoch + D, and has the net change
+//     from the same load) one entry before it writes there (the erosion
+//     floor and final-deposit ceiling read the next entry's cell), and
+//     hands it on with one store of (net change, epoch + D + 1) right after
+//     its last write there; the step-deposit ceiling of the following entry
+//     uses the live surface snapshotted at that write -- exactly what the
+//     serial order reads, since no other droplet runs between two entries of
+//     one droplet; the stockpile (death) cell is handed on last.
+//   * The order-dependent float64 sums that nothing in the wave reads back
+//     -- the discharge and momentum tracks and the stockpile -- are summed
+//     after the apply, per cell, walking the sorted entries: (droplet,
+//     entry) order within a cell is the serial order.  The packed samples of
+//     the touched cells are refreshed in the same walk.
 // Every read and write of a cell therefore happens in exactly the
 // reference's serial order, and the float64 arithmetic is the reference's
 // (this file is compiled without FMA contraction).  Waits are bounded: a
@@ -42,31 +49,50 @@ inline int grid_for(long long n, int threads = 256)
 
 constexpr long long kSpinLimit = 1LL << 22;  // ~ seconds of polling: far beyond any real hand-off
 
-// wait until the D earlier droplets of this wave that visit cell c have released it
-__device__ __forceinline__ bool acquire(unsigned long long *done, long long c, unsigned long long epoch, int D, int *error)
+// a cell's hand-off word: x = live net change, y = hand-off counter (bits), one 128-bit access
+__device__ __forceinline__ void hand_load(const double2 *p, double &acc, unsigned long long &count)
 {
+    unsigned long long lo, hi;
+    asm volatile(
+        "{\n\t.reg .b128 t;\n\t"
+        "ld.relaxed.gpu.global.b128 t, [%2];\n\t"
+        "mov.b128 {%0, %1}, t;\n\t}"
+        : "=l"(lo), "=l"(hi)
+        : "l"(p)
+        : "memory");
+    acc = __longlong_as_double((long long)lo);
+    count = hi;
+}
+
+__device__ __forceinline__ void hand_store(double2 *p, double acc, unsigned long long count)
+{
+    const unsigned long long lo = (unsigned long long)__double_as_longlong(acc);
+    asm volatile(
+        "{\n\t.reg .b128 t;\n\t"
+        "mov.b128 t, {%1, %2};\n\t"
+        "st.relaxed.gpu.global.b128 [%0], t;\n\t}"
+        :
+        : "l"(p), "l"(lo), "l"(count)
+        : "memory");
+}
+
+// wait until the D earlier droplets of this wave that visit cell c have handed it on; acc = its net change
+__device__ __forceinline__ bool acquire(const double2 *hand, long long c, unsigned long long epoch, int D, int *error, double &acc)
+{
+    unsigned long long n;
+    hand_load(hand + c, acc, n);
     if (D == 0) return true;  // the first visitor of the wave: every earlier wave has finished
     const unsigned long long want = epoch + (unsigned long long)D;
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(done[c]);
-    // poll with relaxed loads; one acquire fence once the hand-off is seen
     for (long long i = 0; i < kSpinLimit; i++) {
-        if (r.load(cuda::memory_order_relaxed) == want) {
-            cuda::atomic_thread_fence(cuda::memory_order_acquire, cuda::thread_scope_device);
-            return true;
-        }
+        if (n == want) return true;
         if ((i & 255) == 255) {
             if (*(volatile int *)error) return false;  // another wait gave up: stop waiting
             __nanosleep(32);
         }
+        hand_load(hand + c, acc, n);
     }
     atomicExch(error, 1);
     return false;
-}
-
-__device__ __forceinline__ void release(unsigned long long *done, long long c, unsigned long long value)
-{
-    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(done[c]);
-    r.store(value, cuda::memory_order_release);
 }
 
 enum { OS_CLAMPED, OS_TOPEND, OS_DEFICIT, OS_LOSTOFF, OS_ERODED, OS_DEPOSITED, OS_N };
@@ -75,34 +101,32 @@ enum { OS_CLAMPED, OS_TOPEND, OS_DEFICIT, OS_LOSTOFF, OS_ERODED, OS_DEPOSITED, O
 // ---------------------------------------------------------------------------
 // ranks
 // ---------------------------------------------------------------------------
-__global__ void ordered_keys_kernel(long long nslots, int cap, const int32_t *cell, const int64_t *count, int kbits, int pbits,
+// key = the slot's cell (invalid past a list's end); the slots enter the stable sort in (droplet,
+// entry) order, so equal cells keep the serial order
+__global__ void ordered_keys_kernel(long long nslots, int cap, const int32_t *cell, const int64_t *count,
                                     unsigned long long invalid, unsigned long long *keys, int32_t *vals)
 {
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nslots; s += (long long)gridDim.x * blockDim.x) {
         const long long q = s / cap, k = s - q * cap;
-        if (k < count[q])
-            keys[s] = ((unsigned long long)cell[s] << (pbits + kbits)) | ((unsigned long long)q << kbits) | (unsigned long long)k;
-        else
-            keys[s] = invalid;
+        keys[s] = k < count[q] ? (unsigned long long)cell[s] : invalid;
         vals[s] = (int32_t)s;
     }
 }
 
-__global__ void ordered_flags_kernel(long long nslots, const unsigned long long *keys, int kbits, int pbits,
+// runstart: first slot of a (cell, droplet) run; segpos: position of a cell segment's first slot
+__global__ void ordered_flags_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
                                      unsigned long long invalid, int32_t *runstart, int32_t *segpos)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
         int rs = 0, sp = 0;
         if (k != invalid) {
-            const unsigned long long run = k >> kbits, seg = k >> (kbits + pbits);
             if (i == 0) {
                 rs = 1;
-                sp = 0;
             } else {
-                const unsigned long long kp = keys[i - 1];
-                rs = (kp >> kbits) != run;
-                sp = (kp >> (kbits + pbits)) != seg ? (int)i : 0;
+                const bool newseg = keys[i - 1] != k;
+                rs = newseg || vals[i - 1] / cap != vals[i] / cap;
+                sp = newseg ? (int)i : 0;
             }
         }
         runstart[i] = rs;
@@ -110,8 +134,9 @@ __global__ void ordered_flags_kernel(long long nslots, const unsigned long long 
     }
 }
 
-__global__ void ordered_rank_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, unsigned long long invalid,
-                                    int kbits, const int32_t *runscan, const int32_t *segscan, int32_t *D, uint8_t *last)
+__global__ void ordered_rank_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
+                                    unsigned long long invalid, const int32_t *runscan, const int32_t *segscan, int32_t *D,
+                                    uint8_t *last)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
@@ -119,10 +144,7 @@ __global__ void ordered_rank_kernel(long long nslots, const unsigned long long *
         const int32_t s = vals[i];
         D[s] = runscan[i] - runscan[segscan[i]];
         bool lst = true;
-        if (i + 1 < nslots) {
-            const unsigned long long kn = keys[i + 1];
-            lst = kn == invalid || (kn >> kbits) != (k >> kbits);
-        }
+        if (i + 1 < nslots) lst = keys[i + 1] != k || vals[i + 1] / cap != s / cap;
         last[s] = lst ? 1 : 0;
     }
 }
@@ -158,20 +180,27 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
     const bool lane0 = (threadIdx.x & 31) == 0;
     for (long long q = w0; lane0 && q < a.nw; q += T) {
         const int K = (int)a.count[q];
-        if (K <= 0) continue;
+        if (K <= 0) {
+            a.dth[q] = -1;
+            continue;
+        }
         const long long b0 = q * a.cap;
         double deficit = 0.0, surplus = 0.0;
         long long death = -1;
+        int Ddeath = 0;
         bool has_prev = false;
         double prev_live = 0.0;  // the previous step entry's cell right after its write (the step-deposit ceiling)
         long long clamped = 0, eroded_fx = 0, deposited_fx = 0;
-        // entry descriptors: the current one and the next, loaded before any wait
+        // the current entry: descriptor and read-only terrain; the next entry's cell and rank
         long long c = a.cell[b0];
         int Dc = a.D[b0];
         bool lastc = a.last[b0];
         double dlt = a.delta[b0];
         float vv = a.vol[b0];
-        float m0 = a.mom[2 * b0], m1 = a.mom[2 * b0 + 1];
+        double hs = a.L[c].x;
+        float b_c = a.B[c].w;
+        bool act_c = !a.mask || a.mask[c] == PGE_MASK_ACTIVE;
+        double cap_c = a.ecap ? a.ecap[c] : 0.0;
         long long nc = -1;
         int Dn = 0;
         if (K > 1) {
@@ -179,53 +208,44 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
             Dn = a.D[b0 + 1];
         }
         bool ok = true;
-        bool have_c = false;       // the current entry's cell is acquired
-        bool acc_known = false;    // acc_c holds its net change (read when it was acquired as the next cell)
+        bool have_c = false;  // the current entry's cell is acquired and acc_c holds its net change
         double acc_c = 0.0;
-        for (int k = 0; k < K && ok; k++) {
+        for (int k = 0; k < K; k++) {
             const long long e = b0 + k;
             const bool has_next = k + 1 < K;
-            // read-only data of this entry's cell, loaded before any wait
-            const double hs = a.L[c].x;
-            const float b_c = a.B[c].w;
-            const double sed_c = a.sediment[c];
-            if (!have_c) {
-                ok = acquire(a.done, c, a.epoch, Dc, a.error);
-                if (!ok) break;
-                have_c = true;
-            }
-            // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell
-            // live: acquire it now; a step deposit does not, and acquires it only before writing it
-            const bool is_step = vv >= 0.0f;
-            const bool reads_next = has_next && (dlt < 0.0 || !is_step);
-            double hs_n = 0.0, acc_n = 0.0;
-            if (reads_next) {
-                hs_n = a.L[nc].x;
-                ok = acquire(a.done, nc, a.epoch, Dn, a.error);
-                if (!ok) break;
-                acc_n = a.acc4[4 * nc];
-            }
-            if (!acc_known) acc_c = a.acc4[4 * c];
-            // prefetch the descriptor after next
+            // everything read-only the next entry needs, loaded before any wait
+            double hs_n = 0.0, cap_n = 0.0, dltn = 0.0;
+            float b_n = 0.0f, vn = 0.0f;
+            bool act_n = true, lastn = false;
             long long nnc = -1;
             int Dnn = 0;
-            if (k + 2 < K) {
-                nnc = a.cell[e + 2];
-                Dnn = a.D[e + 2];
-            }
-            bool lastn = false;
-            double dltn = 0.0;
-            float vn = 0.0f, mn0 = 0.0f, mn1 = 0.0f;
             if (has_next) {
+                hs_n = a.L[nc].x;
+                b_n = a.B[nc].w;
+                if (a.mask) act_n = a.mask[nc] == PGE_MASK_ACTIVE;
+                if (a.ecap) cap_n = a.ecap[nc];
                 lastn = a.last[e + 1];
                 dltn = a.delta[e + 1];
                 vn = a.vol[e + 1];
-                mn0 = a.mom[2 * (e + 1)];
-                mn1 = a.mom[2 * (e + 1) + 1];
+                if (k + 2 < K) {
+                    nnc = a.cell[e + 2];
+                    Dnn = a.D[e + 2];
+                }
+            }
+            if (!have_c && !(ok = acquire(a.hand, c, a.epoch, Dc, a.error, acc_c))) break;
+            // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
+            // acquire it now; a step deposit does not, and acquires it only before writing it
+            const bool is_step = vv >= 0.0f;
+            const bool reads_next = has_next && (dlt < 0.0 || !is_step);
+            double acc_n = 0.0;
+            if (reads_next) {
+                if (nc == c)
+                    acc_n = acc_c;
+                else if (!(ok = acquire(a.hand, nc, a.epoch, Dn, a.error, acc_n)))
+                    break;
             }
             double acc_new = acc_c;
-            if (!(a.mask && a.mask[c] != PGE_MASK_ACTIVE)) {
-                double *accp = a.acc4 + 4 * c;
+            if (act_c) {
                 const double acc = acc_c;
                 const double s_c = hs + acc;
                 const double nlive = hs_n + acc_n;
@@ -234,7 +254,7 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                     double e_act = ew;
                     double room = p.iter_erode + acc;
                     if (a.ecap) {
-                        const double r2 = a.ecap[c] + acc;
+                        const double r2 = cap_c + acc;
                         if (r2 < room) room = r2;
                     }
                     if (e_act > room) e_act = room;
@@ -283,35 +303,27 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                     surplus = want - d_act;
                     acc_new = acc + d_act;
                     deposited_fx += fx_mass(d_act);
-                    if (!is_step && death < 0) death = c;
-                }
-                accp[0] = acc_new;
-                // the packed samples follow the live terrain (particle.py:1005-1009)
-                a.A[c].x = (float)(hs + acc_new);
-                const double sd = sed_c + acc_new;
-                a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
-                if (is_step) {
-                    if (vv > 0.0f) {
-                        accp[1] += (double)vv;
-                        accp[2] += (double)m0;
-                        accp[3] += (double)m1;
+                    if (!is_step && death < 0) {
+                        death = c;
+                        Ddeath = Dc;
                     }
+                }
+                if (is_step) {
                     has_prev = true;
                     prev_live = hs + acc_new;
                 }
             }
-            // a cell is handed on right after the droplet's last write there; the stockpile (death)
-            // cell waits for the stockpile update
-            if (lastc && c != death) release(a.done, c, a.epoch + (unsigned)Dc + 1ull);
-            // the next entry's cell: acquired (and its net change known) if this entry read it;
-            // the same cell again keeps its acquisition and its updated net change
+            // publish the net change; a droplet's last write at a cell also hands the cell on, except
+            // the stockpile (death) cell, which waits for the stockpile
+            const bool handoff = lastc && c != death;
+            if (act_c || handoff) hand_store(a.hand + c, acc_new, a.epoch + (unsigned long long)Dc + (handoff ? 1ull : 0ull));
+            // the next entry's cell: acquired (with its net change) if this entry read it; the same
+            // cell again keeps its acquisition and its updated net change
             if (has_next && nc == c) {
                 have_c = true;
-                acc_known = true;
                 acc_c = acc_new;
             } else {
                 have_c = reads_next;
-                acc_known = reads_next;
                 acc_c = acc_n;
             }
             c = nc;
@@ -319,35 +331,38 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
             lastc = lastn;
             dlt = dltn;
             vv = vn;
-            m0 = mn0;
-            m1 = mn1;
+            hs = hs_n;
+            b_c = b_n;
+            act_c = act_n;
+            cap_c = cap_n;
             nc = nnc;
             Dn = Dnn;
         }
         if (!ok) break;
         long long topend = 0, lostoff = 0;
-        if (surplus > 0.0 && death >= 0) {
-            if (a.L[death].x + a.acc4[4 * death] < (double)a.B[death].w) {
-                double keep = surplus * (1.0 - p.offshore_writeoff);
-                if (keep < 1e-4) keep = 0.0;
-                a.pend[death] += keep;
-                topend = fx_mass(keep);
-                lostoff = fx_mass(surplus) - topend;
-            } else {
-                a.pend[death] += surplus;
-                topend = fx_mass(surplus);
-            }
-        }
+        int32_t dth = -1;
+        double add = 0.0;
         if (death >= 0) {
-            // the death cell's last visit is among the final deposits: find it and hand the cell on
-            for (int k = K - 1; k >= 0; k--) {
-                const long long e = b0 + k;
-                if (a.cell[e] == death) {
-                    release(a.done, death, a.epoch + (unsigned)a.D[e] + 1ull);
-                    break;
+            double accd;
+            unsigned long long nd;
+            hand_load(a.hand + death, accd, nd);  // this droplet's own last write there
+            if (surplus > 0.0) {
+                if (a.L[death].x + accd < (double)a.B[death].w) {
+                    double keep = surplus * (1.0 - p.offshore_writeoff);
+                    if (keep < 1e-4) keep = 0.0;
+                    add = keep;
+                    topend = fx_mass(keep);
+                    lostoff = fx_mass(surplus) - topend;
+                } else {
+                    add = surplus;
+                    topend = fx_mass(surplus);
                 }
+                dth = (int32_t)death;
             }
+            hand_store(a.hand + death, accd, a.epoch + (unsigned long long)Ddeath + 1ull);
         }
+        a.dth[q] = dth;
+        a.keep[q] = add;
         if (clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)clamped);
         if (topend) atomicAdd(&sstat[OS_TOPEND], (unsigned long long)topend);
         if (deficit > 0.0) atomicAdd(&sstat[OS_DEFICIT], (unsigned long long)fx_mass(deficit));
@@ -368,6 +383,79 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
     }
 }
 
+// ---------------------------------------------------------------------------
+// after the apply: per touched cell, in the serial (droplet, entry) order, the discharge and
+// momentum tracks (particle.py:1013-1018) and the stockpile (:1019-1041); then the cell's net
+// change to the accumulators and its packed samples (:1005-1009)
+// ---------------------------------------------------------------------------
+__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
+                                      unsigned long long invalid)
+{
+    constexpr int U = 8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[i];
+        if (key == invalid || (i > 0 && keys[i - 1] == key)) continue;  // not the first slot of a cell
+        const long long c = (long long)key;
+        const bool active = !a.mask || a.mask[c] == PGE_MASK_ACTIVE;
+        double *accp = a.acc4 + 4 * c;
+        double tq = accp[1], ta = accp[2], tb = accp[3], pd = a.pend[c];
+        bool more = true;
+        for (long long j = i; more; j += U) {
+            int32_t sl[U];
+            bool in[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                in[u] = j + u < nslots && keys[j + u] == key;
+                sl[u] = in[u] ? vals[j + u] : 0;
+            }
+            float v[U], m0[U], m1[U];
+            bool stock[U];
+            double kp[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                v[u] = 0.0f;
+                m0[u] = m1[u] = 0.0f;
+                stock[u] = false;
+                kp[u] = 0.0;
+                if (in[u]) {
+                    const int32_t s = sl[u], q = s / a.cap;
+                    v[u] = a.vol[s];
+                    if (active && v[u] > 0.0f) {
+                        m0[u] = a.mom[2 * (long long)s];
+                        m1[u] = a.mom[2 * (long long)s + 1];
+                    }
+                    if (a.last[s] && a.dth[q] == (int32_t)c) {
+                        stock[u] = true;
+                        kp[u] = a.keep[q];
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                if (!in[u]) continue;
+                if (active && v[u] > 0.0f) {
+                    tq += (double)v[u];
+                    ta += (double)m0[u];
+                    tb += (double)m1[u];
+                }
+                if (stock[u]) pd += kp[u];
+            }
+            more = in[U - 1];
+        }
+        accp[1] = tq;
+        accp[2] = ta;
+        accp[3] = tb;
+        a.pend[c] = pd;
+        const double acc = a.hand[c].x;
+        accp[0] = acc;
+        if (active) {
+            a.A[c].x = (float)(a.L[c].x + acc);
+            const double sd = a.sediment[c] + acc;
+            a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
+        }
+    }
+}
+
 int ordered_blocks_per_sm(int threads)
 {
     int n = 0;
@@ -378,22 +466,22 @@ int ordered_blocks_per_sm(int threads)
 cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
 {
     const long long nslots = w.nw * w.cap;
-    ordered_keys_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.cap, w.a.cell, w.a.count, w.kbits, w.pbits, w.invalid,
-                                                          w.keys_in, w.vals_in);
+    ordered_keys_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.cap, w.a.cell, w.a.count, w.invalid, w.keys_in, w.vals_in);
     size_t tb = w.temp_bytes;
     cudaError_t e = cub::DeviceRadixSort::SortPairs(w.temp, tb, w.keys_in, w.keys_out, w.vals_in, w.vals_out, (int)nslots, 0,
                                                     w.end_bit, st);
     if (e != cudaSuccess) return e;
-    ordered_flags_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.kbits, w.pbits, w.invalid, w.runstart, w.segpos);
+    ordered_flags_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runstart, w.segpos);
     tb = w.temp_bytes;
     if ((e = cub::DeviceScan::InclusiveSum(w.temp, tb, w.runstart, w.runscan, (int)nslots, st)) != cudaSuccess) return e;
     tb = w.temp_bytes;
     if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, w.segpos, w.segscan, MaxOp{}, (int)nslots, st)) != cudaSuccess) return e;
-    ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.invalid, w.kbits, w.runscan, w.segscan,
+    ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
                                                           const_cast<int32_t *>(w.a.D), const_cast<uint8_t *>(w.a.last));
     long long blocks = (w.nw * 32 + 255) / 256;  // a warp per droplet
     if (blocks > w.max_blocks) blocks = w.max_blocks;
     ordered_apply_kernel<<<(int)blocks, 256, 0, st>>>(w.a);
+    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
     return cudaPeekAtLastError();
 }
 

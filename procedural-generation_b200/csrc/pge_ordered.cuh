@@ -23,11 +23,15 @@ struct OrderedArgs {
     float4 *B;
     const uint8_t *mask;
     const double *ecap;
+    // per cell: the live net change and the hand-off counter, one 16-byte word
+    double2 *hand;
+    unsigned long long epoch;
+    // per droplet: the stockpile cell (-1: none) and the amount it adds there
+    int32_t *dth;
+    double *keep;
     // float64 accumulators in serial order: (net change, discharge, momentum a, b) and the stockpile
     double *acc4;
     double *pend;
-    unsigned long long *done;
-    unsigned long long epoch;
     PgeParams p;
     PgeStats *stats;
     int *error;
@@ -36,7 +40,7 @@ struct OrderedArgs {
 struct OrderedWave {
     OrderedArgs a;
     long long nw;
-    int cap, kbits, pbits, end_bit;
+    int cap, end_bit;
     unsigned long long invalid;
     unsigned long long *keys_in, *keys_out;
     int32_t *vals_in, *vals_out, *runstart, *segpos, *runscan, *segscan;
