@@ -137,8 +137,8 @@ def launches_per_iteration(nw: int, pending: bool, creep: bool, ordered: bool) -
     """Kernels of this library one plain iteration launches (library kernels
     -- CUB scan / sort / select -- not counted)."""
     spawn = 3 + (1 if pending else 0)
-    if ordered:   # pack x2; per wave: trace, keys, flags, ranks, ordered apply; error report, mode, fold+EMA
-        droplets = 2 + 5 * nw + 3
+    if ordered:   # pack x2, terrain; per wave: trace, keys, flags, ranks, ordered apply, finish; error report, mode, fold+EMA
+        droplets = 3 + 6 * nw + 3
     else:         # pack x2; waves and the refreshes between them; mode, fold+EMA
         droplets = 2 + nw + (nw - 1) + 2
     thermal = 4 * (2 if creep else 1)

@@ -149,8 +149,7 @@ Layout layout(const PgeGrid &g)
     L.w_mom = take(8 * ws);
     L.w_count = take(8 * L.max_wave);
     L.w_death = take(L.max_wave);
-    L.w_D = take(4 * ws);
-    L.w_last = take(ws);
+    L.w_desc = take(16 * ws);
     L.w_keys0 = take(8 * ws);
     L.w_keys1 = take(8 * ws);
     L.w_vals0 = take(4 * ws);
@@ -163,7 +162,9 @@ Layout layout(const PgeGrid &g)
     L.w_temp = take(L.w_temp_bytes);
     L.w_dth = take(4 * L.max_wave);
     L.w_keep = take(8 * L.max_wave);
+    L.w_act = take(8 * ws);
     L.hand = take(16 * L.ncell);
+    L.terr = take(16 * L.ncell);
     L.error = take(256);
     L.total = o;
     return L;
@@ -235,6 +236,9 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         if (p->apply == PGE_APPLY_ORDERED && !rec_cell) {
             // exact mode: record each wave's change lists, then apply them in droplet order
             if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.hand), 0, 16 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset hand");
+            if ((e = ordered_terrain(lay.ncell, ws_ptr<double2>(ws, lay.live), ws_ptr<float4>(ws, lay.cellB), s->mask,
+                                     ws_ptr<CellTerr>(ws, lay.terr), st)) != cudaSuccess)
+                return cuda_fail(e, "ordered terrain");
             if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.error), 0, 4, st)) != cudaSuccess) return cuda_fail(e, "memset error");
             a.ledger = 0;
             a.rec_cell = ws_ptr<int32_t>(ws, lay.w_cell);
@@ -252,8 +256,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.mom = a.rec_mom;
             oa.count = a.rec_count;
             oa.cap = (int)lay.cap;
-            oa.D = ws_ptr<int32_t>(ws, lay.w_D);
-            oa.last = ws_ptr<uint8_t>(ws, lay.w_last);
+            oa.desc = ws_ptr<EntryDesc>(ws, lay.w_desc);
+            oa.terr = ws_ptr<CellTerr>(ws, lay.terr);
             oa.L = a.L;
             oa.sediment = s->sediment;
             oa.A = ws_ptr<float4>(ws, lay.cellA);
@@ -265,6 +269,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.hand = ws_ptr<double2>(ws, lay.hand);
             oa.dth = ws_ptr<int32_t>(ws, lay.w_dth);
             oa.keep = ws_ptr<double>(ws, lay.w_keep);
+            oa.act = ws_ptr<double>(ws, lay.w_act);
             oa.p = *p;
             oa.stats = stats;
             oa.error = ws_ptr<int>(ws, lay.error);
@@ -285,6 +290,9 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(256);
+            int ebits = 1;
+            while ((1LL << ebits) <= wave) ebits++;
+            long long ebase = 0;
             for (long long w = 0; w < nw; w++) {
                 a.d_begin = w * wave;
                 a.d_end = a.d_begin + wave < P ? a.d_begin + wave : P;
@@ -302,7 +310,13 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
                 ow.nw = nd;
                 oa.nw = ow.nw;
-                oa.epoch = (unsigned long long)(w + 1) << 24;
+                // epochs step by 2^ebits > wave, so a counter never reaches the next wave's values;
+                // they are 32-bit, and start over (counters zeroed) before they would wrap
+                if (((unsigned long long)(w - ebase + 2) << ebits) >= (1ull << 32)) {
+                    if ((e = hand_reset(lay.ncell, oa.hand, st)) != cudaSuccess) return cuda_fail(e, "hand reset");
+                    ebase = w;
+                }
+                oa.epoch = (uint32_t)((unsigned long long)(w - ebase + 1) << ebits);
                 if ((e = ordered_wave(ow, st)) != cudaSuccess) return cuda_fail(e, "ordered apply");
             }
             report_errors(ws_ptr<int>(ws, lay.error), stats, st);

@@ -57,8 +57,8 @@ struct Layout {
     size_t cellA, cellB, live, metric8, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
         partial, thermal, flags, total;
     // ordered apply (exact mode): one wave's change lists and ranks
-    size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_D, w_last, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
-        w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, hand, error;
+    size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_desc, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
+        w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, w_act, hand, terr, error;
     int64_t ncell, nmetric, nslots, table_cap, table_slots, max_droplets, max_wave, wave_slots, cap;
 };
 

@@ -12,18 +12,25 @@
 // each cell is handed from droplet to droplet in droplet order:
 //   * the entries of the wave are sorted by (cell, droplet, entry) and each
 //     entry learns D = the number of distinct earlier droplets that visit
-//     its cell, and whether it is its droplet's last visit there;
+//     its cell, whether it is its droplet's first visit there, and whether
+//     it is the last;
 //   * a cell's live net change and its hand-off counter share one 16-byte
-//     word, read and written as single 128-bit accesses: a droplet acquires
-//     a cell (polls until the counter is epoch + D, and has the net change
-//     from the same load) one entry before it writes there (the erosion
-//     floor and final-deposit ceiling read the next entry's cell), and
-//     hands it on with one store of (net change, epoch + D + 1) right after
-//     its last write there; the step-deposit ceiling of the following entry
-//     uses the live surface snapshotted at that write -- exactly what the
-//     serial order reads, since no other droplet runs between two entries of
-//     one droplet; the stockpile (death) cell is handed on last.
-//   * The order-dependent float64 sums that nothing in the wave reads back
+//     word: a droplet acquires a cell (the counter reads epoch + D; the net
+//     change comes with it) one entry before it writes there (the erosion
+//     floor and final-deposit ceiling read the next entry's cell), and hands
+//     it on with one store of (net change, epoch + D + 1) right after its
+//     last write there; the step-deposit ceiling of the following entry uses
+//     the live surface snapshotted at that write -- exactly what the serial
+//     order reads, since no other droplet runs between two entries of one
+//     droplet.  The stockpile test (is the death cell submerged?) reads the
+//     death cell as the droplet's own last write there left it, so it is
+//     taken at that write and the death cell is handed on like any other;
+//   * a droplet's path through the wave is mostly its own entries one after
+//     another, so each entry's packed 16-byte descriptor, its cell's packed
+//     16-byte terrain and the cell's hand-off word are copied into a ring in
+//     shared memory several entries ahead (asynchronous copies, waited for
+//     by group count);
+//   * the order-dependent float64 sums that nothing in the wave reads back
 //     -- the discharge and momentum tracks and the stockpile -- are summed
 //     after the apply, per cell, walking the sorted entries: (droplet,
 //     entry) order within a cell is the serial order.  The packed samples of
@@ -33,7 +40,6 @@
 // (this file is compiled without FMA contraction).  Waits are bounded: a
 // wait that gives up sets an error flag the host reports.
 #include <cub/cub.cuh>
-#include <cuda/atomic>
 
 #include "pge_internal.cuh"
 #include "pge_ordered.cuh"
@@ -49,50 +55,83 @@ inline int grid_for(long long n, int threads = 256)
 
 constexpr long long kSpinLimit = 1LL << 22;  // ~ seconds of polling: far beyond any real hand-off
 
-// a cell's hand-off word: x = live net change, y = hand-off counter (bits), one 128-bit access
-__device__ __forceinline__ void hand_load(const double2 *p, double &acc, unsigned long long &count)
+// A cell's hand-off word: 16 bytes, two 8-byte halves (acc low 32 bits | count << 32) and (acc high
+// 32 bits | count << 32), where acc is the live net change and count the hand-off counter.  Each
+// half is one single-copy-atomic 64-bit access, so a reader that sees the same count in both halves
+// holds a consistent word, however the 16 bytes were read.
+__device__ __forceinline__ void hand_pack(double acc, uint32_t count, unsigned long long &w0, unsigned long long &w1)
 {
-    unsigned long long lo, hi;
-    asm volatile(
-        "{\n\t.reg .b128 t;\n\t"
-        "ld.relaxed.gpu.global.b128 t, [%2];\n\t"
-        "mov.b128 {%0, %1}, t;\n\t}"
-        : "=l"(lo), "=l"(hi)
-        : "l"(p)
-        : "memory");
-    acc = __longlong_as_double((long long)lo);
-    count = hi;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(acc);
+    w0 = ((unsigned long long)count << 32) | (bits & 0xffffffffull);
+    w1 = ((unsigned long long)count << 32) | (bits >> 32);
 }
 
-__device__ __forceinline__ void hand_store(double2 *p, double acc, unsigned long long count)
+__device__ __forceinline__ double hand_acc(unsigned long long w0, unsigned long long w1)
 {
-    const unsigned long long lo = (unsigned long long)__double_as_longlong(acc);
-    asm volatile(
-        "{\n\t.reg .b128 t;\n\t"
-        "mov.b128 t, {%1, %2};\n\t"
-        "st.relaxed.gpu.global.b128 [%0], t;\n\t}"
-        :
-        : "l"(p), "l"(lo), "l"(count)
-        : "memory");
+    return __longlong_as_double((long long)((w1 << 32) | (w0 & 0xffffffffull)));
+}
+
+__device__ __forceinline__ bool hand_ready(unsigned long long w0, unsigned long long w1, uint32_t want)
+{
+    return (uint32_t)(w0 >> 32) == want && (uint32_t)(w1 >> 32) == want;
+}
+
+__device__ __forceinline__ void hand_load(const double2 *p, unsigned long long &w0, unsigned long long &w1)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(p) : "memory");
+}
+
+__device__ __forceinline__ void hand_store(double2 *p, double acc, uint32_t count)
+{
+    unsigned long long w0, w1;
+    hand_pack(acc, count, w0, w1);
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" : : "l"(p), "l"(w0), "l"(w1) : "memory");
 }
 
 // wait until the D earlier droplets of this wave that visit cell c have handed it on; acc = its net change
-__device__ __forceinline__ bool acquire(const double2 *hand, long long c, unsigned long long epoch, int D, int *error, double &acc)
+__device__ __forceinline__ bool acquire(const double2 *hand, long long c, uint32_t epoch, int D, int *error, double &acc)
 {
-    unsigned long long n;
-    hand_load(hand + c, acc, n);
-    if (D == 0) return true;  // the first visitor of the wave: every earlier wave has finished
-    const unsigned long long want = epoch + (unsigned long long)D;
+    const uint32_t want = epoch + (uint32_t)D;
+    unsigned long long w0, w1;
     for (long long i = 0; i < kSpinLimit; i++) {
-        if (n == want) return true;
+        hand_load(hand + c, w0, w1);
+        if (D == 0 || hand_ready(w0, w1, want)) {  // D == 0: the wave's first visitor, no earlier writer
+            acc = hand_acc(w0, w1);
+            return true;
+        }
         if ((i & 255) == 255) {
             if (*(volatile int *)error) return false;  // another wait gave up: stop waiting
             __nanosleep(32);
         }
-        hand_load(hand + c, acc, n);
     }
     atomicExch(error, 1);
     return false;
+}
+
+// a cell this droplet holds and has written before: its own last write (coherent for the same thread)
+__device__ __forceinline__ double own_value(const double2 *hand, long long c)
+{
+    unsigned long long w0, w1;
+    hand_load(hand + c, w0, w1);
+    return hand_acc(w0, w1);
+}
+
+// asynchronous copies into shared memory: the waits count copy groups, so waiting for an old
+// entry's data never waits for the copies issued after it
+__device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_ca8(void *d, const void *g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)) : "memory");
+}
+__device__ __forceinline__ void cp_cg16(void *d, const void *g)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 enum { OS_CLAMPED, OS_TOPEND, OS_DEFICIT, OS_LOSTOFF, OS_ERODED, OS_DEPOSITED, OS_N };
@@ -135,17 +174,34 @@ __global__ void ordered_flags_kernel(long long nslots, const unsigned long long 
 }
 
 __global__ void ordered_rank_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
-                                    unsigned long long invalid, const int32_t *runscan, const int32_t *segscan, int32_t *D,
-                                    uint8_t *last)
+                                    unsigned long long invalid, const int32_t *runscan, const int32_t *segscan,
+                                    const double *delta, const float *vol, EntryDesc *desc)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
         if (k == invalid) continue;
         const int32_t s = vals[i];
-        D[s] = runscan[i] - runscan[segscan[i]];
+        const uint32_t D = (uint32_t)(runscan[i] - runscan[segscan[i]]);
         bool lst = true;
         if (i + 1 < nslots) lst = keys[i + 1] != k || vals[i + 1] / cap != s / cap;
-        last[s] = lst ? 1 : 0;
+        const bool fst = i == 0 || keys[i - 1] != k || vals[i - 1] / cap != s / cap;
+        EntryDesc d;
+        d.cell = (int32_t)k;
+        d.dflags = D | (lst ? ENTRY_LAST : 0u) | (fst ? ENTRY_FIRST : 0u) | (vol[s] >= 0.0f ? ENTRY_STEP : 0u);
+        d.delta = delta[s];
+        desc[s] = d;
+    }
+}
+
+// the ordered apply's read-only terrain record of every cell
+__global__ void ordered_terrain_kernel(long long ncell, const double2 *L, const float4 *B, const uint8_t *mask, CellTerr *terr)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        CellTerr t;
+        t.hs = L[c].x;
+        t.base = B[c].w;
+        t.active = !mask || mask[c] == PGE_MASK_ACTIVE ? 1u : 0u;
+        terr[c] = t;
     }
 }
 
@@ -167,114 +223,170 @@ size_t ordered_temp_bytes(long long nslots)
 // ---------------------------------------------------------------------------
 // the ordered apply
 // ---------------------------------------------------------------------------
+namespace {
+constexpr int RING = 8;  // entry slots per droplet: entries k .. k+5 are in flight
+
+// one entry of a droplet's list as the apply reads it, filled by asynchronous copies
+struct alignas(16) Slot {
+    EntryDesc d;                // descriptor
+    unsigned long long h0, h1;  // the cell's hand-off word as prefetched
+    CellTerr t;                 // the cell's read-only terrain
+    double cap;                 // the slope erode cap (when on)
+    double pad;
+};
+static_assert(sizeof(Slot) == 64, "slot layout");
+
+__device__ __forceinline__ void stage_desc(const OrderedArgs &a, Slot &s, long long e) { cp_cg16(&s.d, a.desc + e); }
+
+template <bool ECAP>
+__device__ __forceinline__ void stage_cell(const OrderedArgs &a, Slot &s)
+{
+    const long long c = s.d.cell;
+    cp_cg16(&s.h0, a.hand + c);
+    cp_cg16(&s.t, a.terr + c);
+    if (ECAP) cp_ca8(&s.cap, a.ecap + c);
+}
+
+// per droplet state carried from entry to entry
+struct Walk {
+    double deficit, surplus, prev_live, acc_c;
+    int clamped;
+    int32_t death;
+    // this droplet's last three writes (cell, net change after it)
+    int32_t w1c, w2c, w3c;
+    double w1v, w2v, w3v;
+    bool sub_death, has_prev, have_c, ok;
+};
+
+// the net change of a cell this droplet is about to read: a recent write of its own, its own
+// earlier write (a revisit), the prefetched word once the D earlier droplets have handed the cell
+// on, or a wait for them
+__device__ __forceinline__ bool cell_value(const OrderedArgs &a, const Walk &w, int32_t c, uint32_t df,
+                                           unsigned long long h0, unsigned long long h1, double &acc)
+{
+    if (c == w.w1c) {
+        acc = w.w1v;
+        return true;
+    }
+    if (c == w.w2c) {
+        acc = w.w2v;
+        return true;
+    }
+    if (c == w.w3c) {
+        acc = w.w3v;
+        return true;
+    }
+    if (!(df & ENTRY_FIRST)) {
+        acc = own_value(a.hand, c);
+        return true;
+    }
+    const uint32_t D = df & ENTRY_D_MASK;
+    if (D == 0 || hand_ready(h0, h1, a.epoch + D)) {
+        acc = hand_acc(h0, h1);
+        return true;
+    }
+    return acquire(a.hand, c, a.epoch, (int)D, a.error, acc);
+}
+}  // namespace
+
+template <bool ECAP>
 __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
 {
     __shared__ unsigned long long sstat[OS_N];
+    __shared__ Slot ring[8][RING];
     for (int k = threadIdx.x; k < OS_N; k += blockDim.x) sstat[k] = 0ull;
     __syncthreads();
     const PgeParams &p = a.p;
     // one droplet per warp (its lane 0): a droplet waits on earlier droplets' hand-offs, and lanes of
     // one warp waiting on each other would serialise the warp
     const long long T = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long wq0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const bool lane0 = (threadIdx.x & 31) == 0;
-    for (long long q = w0; lane0 && q < a.nw; q += T) {
+    Slot *R = ring[(threadIdx.x >> 5) & 7];
+    bool failed = false;
+    for (long long q = wq0; lane0 && !failed && q < a.nw; q += T) {
         const int K = (int)a.count[q];
         if (K <= 0) {
             a.dth[q] = -1;
             continue;
         }
         const long long b0 = q * a.cap;
-        double deficit = 0.0, surplus = 0.0;
-        long long death = -1;
-        int Ddeath = 0;
-        bool has_prev = false;
-        double prev_live = 0.0;  // the previous step entry's cell right after its write (the step-deposit ceiling)
-        long long clamped = 0, eroded_fx = 0, deposited_fx = 0;
-        // the current entry: descriptor and read-only terrain; the next entry's cell and rank
-        long long c = a.cell[b0];
-        int Dc = a.D[b0];
-        bool lastc = a.last[b0];
-        double dlt = a.delta[b0];
-        float vv = a.vol[b0];
-        double hs = a.L[c].x;
-        float b_c = a.B[c].w;
-        bool act_c = !a.mask || a.mask[c] == PGE_MASK_ACTIVE;
-        double cap_c = a.ecap ? a.ecap[c] : 0.0;
-        long long nc = -1;
-        int Dn = 0;
-        if (K > 1) {
-            nc = a.cell[b0 + 1];
-            Dn = a.D[b0 + 1];
-        }
-        bool ok = true;
-        bool have_c = false;  // the current entry's cell is acquired and acc_c holds its net change
-        double acc_c = 0.0;
+        // prologue: descriptors of entries 0..4, then the cell data of entries 0..2
+        for (int j = 0; j < 5 && j < K; j++) stage_desc(a, R[j], b0 + j);
+        cp_commit();
+        cp_wait<0>();
+        for (int j = 0; j < 3 && j < K; j++) stage_cell<ECAP>(a, R[j]);
+        cp_commit();
+        cp_wait<0>();
+        Walk w;
+        w.deficit = w.surplus = w.prev_live = w.acc_c = 0.0;
+        w.clamped = 0;
+        w.death = -1;
+        w.w1c = w.w2c = w.w3c = -1;
+        w.w1v = w.w2v = w.w3v = 0.0;
+        w.sub_death = w.has_prev = w.have_c = false;
+        w.ok = true;
         for (int k = 0; k < K; k++) {
-            const long long e = b0 + k;
+            // the copies issued two or more entries ago have landed: the descriptor of entry k+3
+            // and the cell data of entries k and k+1
+            cp_wait<1>();
+            if (k + 3 < K) stage_cell<ECAP>(a, R[(k + 3) & (RING - 1)]);
+            if (k + 5 < K) stage_desc(a, R[(k + 5) & (RING - 1)], b0 + k + 5);
+            cp_commit();
+            const Slot &cur = R[k & (RING - 1)];
+            const Slot &nx = R[(k + 1) & (RING - 1)];
             const bool has_next = k + 1 < K;
-            // everything read-only the next entry needs, loaded before any wait
-            double hs_n = 0.0, cap_n = 0.0, dltn = 0.0;
-            float b_n = 0.0f, vn = 0.0f;
-            bool act_n = true, lastn = false;
-            long long nnc = -1;
-            int Dnn = 0;
-            if (has_next) {
-                hs_n = a.L[nc].x;
-                b_n = a.B[nc].w;
-                if (a.mask) act_n = a.mask[nc] == PGE_MASK_ACTIVE;
-                if (a.ecap) cap_n = a.ecap[nc];
-                lastn = a.last[e + 1];
-                dltn = a.delta[e + 1];
-                vn = a.vol[e + 1];
-                if (k + 2 < K) {
-                    nnc = a.cell[e + 2];
-                    Dnn = a.D[e + 2];
-                }
-            }
-            if (!have_c && !(ok = acquire(a.hand, c, a.epoch, Dc, a.error, acc_c))) break;
+            const int32_t c = cur.d.cell;
+            const uint32_t df = cur.d.dflags;
+            const double dlt = cur.d.delta;
+            const double hs = cur.t.hs;
+            const double b_c = (double)cur.t.base;
+            const bool act = cur.t.active != 0;
+            if (!w.have_c && !(w.ok = cell_value(a, w, c, df, cur.h0, cur.h1, w.acc_c))) break;
             // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
             // acquire it now; a step deposit does not, and acquires it only before writing it
-            const bool is_step = vv >= 0.0f;
+            const bool is_step = (df & ENTRY_STEP) != 0;
             const bool reads_next = has_next && (dlt < 0.0 || !is_step);
-            double acc_n = 0.0;
+            const int32_t ncell = has_next ? nx.d.cell : -1;
+            double acc_n = 0.0, hs_n = 0.0;
             if (reads_next) {
-                if (nc == c)
-                    acc_n = acc_c;
-                else if (!(ok = acquire(a.hand, nc, a.epoch, Dn, a.error, acc_n)))
+                hs_n = nx.t.hs;
+                if (ncell == c)
+                    acc_n = w.acc_c;
+                else if (!(w.ok = cell_value(a, w, ncell, nx.d.dflags, nx.h0, nx.h1, acc_n)))
                     break;
             }
-            double acc_new = acc_c;
-            if (act_c) {
-                const double acc = acc_c;
+            const double acc = w.acc_c;
+            double acc_new = acc, amount = 0.0;
+            if (act) {
                 const double s_c = hs + acc;
                 const double nlive = hs_n + acc_n;
                 if (dlt < 0.0) {
                     const double ew = -dlt;
                     double e_act = ew;
                     double room = p.iter_erode + acc;
-                    if (a.ecap) {
-                        const double r2 = cap_c + acc;
+                    if (ECAP) {
+                        const double r2 = cur.cap + acc;
                         if (r2 < room) room = r2;
                     }
                     if (e_act > room) e_act = room;
-                    double floor_ = s_c >= (double)b_c ? (double)b_c : s_c;
+                    double floor_ = s_c >= b_c ? b_c : s_c;
                     if (has_next && nlive > floor_) floor_ = nlive;
                     if (e_act > s_c - floor_) e_act = s_c - floor_;
                     if (e_act < 0.0) e_act = 0.0;
                     if (e_act < ew) {
-                        clamped++;
-                        deficit += ew - e_act;
+                        w.clamped++;
+                        w.deficit += ew - e_act;
                     }
                     acc_new = acc - e_act;
-                    eroded_fx += fx_mass(e_act);
+                    amount = e_act;
                 } else {
-                    double want = dlt + surplus;
-                    surplus = 0.0;
-                    if (deficit > 0.0) {
-                        const double t = want < deficit ? want : deficit;
+                    double want = dlt + w.surplus;
+                    w.surplus = 0.0;
+                    if (w.deficit > 0.0) {
+                        const double t = want < w.deficit ? want : w.deficit;
                         want -= t;
-                        deficit -= t;
+                        w.deficit -= t;
                     }
                     double d_act = want;
                     const double room = p.iter_deposit - acc;
@@ -282,93 +394,82 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
                     bool has_ref = false;
                     double ref_live = 0.0;
                     if (is_step) {
-                        has_ref = has_prev;
-                        ref_live = prev_live;
+                        has_ref = w.has_prev;
+                        ref_live = w.prev_live;
                     } else if (has_next) {
                         has_ref = true;
                         ref_live = nlive;
                     }
                     if (has_ref) {
                         double ceil_ = ref_live + p.dep_floor;
-                        if (s_c < (double)b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
+                        if (s_c < b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
                         const double lim = ceil_ - s_c;
                         if (d_act > lim) d_act = lim;
                     }
-                    if (s_c < (double)b_c) {
-                        const double lim = (double)b_c - p.dep_floor - s_c;
+                    if (s_c < b_c) {
+                        const double lim = b_c - p.dep_floor - s_c;
                         if (d_act > lim) d_act = lim;
                     }
                     if (d_act < 0.0) d_act = 0.0;
-                    if (d_act < want) clamped++;
-                    surplus = want - d_act;
+                    if (d_act < want) w.clamped++;
+                    w.surplus = want - d_act;
                     acc_new = acc + d_act;
-                    deposited_fx += fx_mass(d_act);
-                    if (!is_step && death < 0) {
-                        death = c;
-                        Ddeath = Dc;
-                    }
+                    amount = d_act;
+                    if (!is_step && w.death < 0) w.death = c;
                 }
+                if (c == w.death) w.sub_death = hs + acc_new < b_c;
                 if (is_step) {
-                    has_prev = true;
-                    prev_live = hs + acc_new;
+                    w.has_prev = true;
+                    w.prev_live = hs + acc_new;
                 }
             }
-            // publish the net change; a droplet's last write at a cell also hands the cell on, except
-            // the stockpile (death) cell, which waits for the stockpile
-            const bool handoff = lastc && c != death;
-            if (act_c || handoff) hand_store(a.hand + c, acc_new, a.epoch + (unsigned long long)Dc + (handoff ? 1ull : 0ull));
+            // publish the net change; a droplet's last write at a cell also hands the cell on
+            const bool lastv = (df & ENTRY_LAST) != 0;
+            if (act || lastv) hand_store(a.hand + c, acc_new, a.epoch + (df & ENTRY_D_MASK) + (lastv ? 1u : 0u));
+            a.act[b0 + k] = amount;
+            w.w3c = w.w2c;
+            w.w3v = w.w2v;
+            w.w2c = w.w1c;
+            w.w2v = w.w1v;
+            w.w1c = c;
+            w.w1v = acc_new;
             // the next entry's cell: acquired (with its net change) if this entry read it; the same
             // cell again keeps its acquisition and its updated net change
-            if (has_next && nc == c) {
-                have_c = true;
-                acc_c = acc_new;
+            if (has_next && ncell == c) {
+                w.have_c = true;
+                w.acc_c = acc_new;
             } else {
-                have_c = reads_next;
-                acc_c = acc_n;
+                w.have_c = reads_next;
+                w.acc_c = acc_n;
             }
-            c = nc;
-            Dc = Dn;
-            lastc = lastn;
-            dlt = dltn;
-            vv = vn;
-            hs = hs_n;
-            b_c = b_n;
-            act_c = act_n;
-            cap_c = cap_n;
-            nc = nnc;
-            Dn = Dnn;
         }
-        if (!ok) break;
+        cp_wait<0>();
+        if (!w.ok) {
+            failed = true;
+            break;
+        }
         long long topend = 0, lostoff = 0;
         int32_t dth = -1;
         double add = 0.0;
-        if (death >= 0) {
-            double accd;
-            unsigned long long nd;
-            hand_load(a.hand + death, accd, nd);  // this droplet's own last write there
-            if (surplus > 0.0) {
-                if (a.L[death].x + accd < (double)a.B[death].w) {
-                    double keep = surplus * (1.0 - p.offshore_writeoff);
-                    if (keep < 1e-4) keep = 0.0;
-                    add = keep;
-                    topend = fx_mass(keep);
-                    lostoff = fx_mass(surplus) - topend;
-                } else {
-                    add = surplus;
-                    topend = fx_mass(surplus);
-                }
-                dth = (int32_t)death;
+        if (w.death >= 0 && w.surplus > 0.0) {
+            if (w.sub_death) {
+                double keep = w.surplus * (1.0 - p.offshore_writeoff);
+                if (keep < 1e-4) keep = 0.0;
+                add = keep;
+                topend = fx_mass(keep);
+                lostoff = fx_mass(w.surplus) - topend;
+            } else {
+                add = w.surplus;
+                topend = fx_mass(w.surplus);
             }
-            hand_store(a.hand + death, accd, a.epoch + (unsigned long long)Ddeath + 1ull);
+            dth = w.death;
         }
         a.dth[q] = dth;
         a.keep[q] = add;
-        if (clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)clamped);
+        if (w.clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)w.clamped);
         if (topend) atomicAdd(&sstat[OS_TOPEND], (unsigned long long)topend);
-        if (deficit > 0.0) atomicAdd(&sstat[OS_DEFICIT], (unsigned long long)fx_mass(deficit));
+        if (w.deficit > 0.0) atomicAdd(&sstat[OS_DEFICIT], (unsigned long long)fx_mass(w.deficit));
         if (lostoff) atomicAdd(&sstat[OS_LOSTOFF], (unsigned long long)lostoff);
-        if (eroded_fx) atomicAdd(&sstat[OS_ERODED], (unsigned long long)eroded_fx);
-        if (deposited_fx) atomicAdd(&sstat[OS_DEPOSITED], (unsigned long long)deposited_fx);
     }
     __syncthreads();
     if (threadIdx.x < OS_N && sstat[threadIdx.x]) {
@@ -386,12 +487,17 @@ __global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
 // ---------------------------------------------------------------------------
 // after the apply: per touched cell, in the serial (droplet, entry) order, the discharge and
 // momentum tracks (particle.py:1013-1018) and the stockpile (:1019-1041); then the cell's net
-// change to the accumulators and its packed samples (:1005-1009)
+// change to the accumulators and its packed samples (:1005-1009); and the wave's eroded and
+// deposited totals (integer fixed point, so their order does not matter)
 // ---------------------------------------------------------------------------
 __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
                                       unsigned long long invalid)
 {
     constexpr int U = 8;
+    __shared__ unsigned long long sfx[2];
+    if (threadIdx.x < 2) sfx[threadIdx.x] = 0ull;
+    __syncthreads();
+    long long eroded = 0, deposited = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long key = keys[i];
         if (key == invalid || (i > 0 && keys[i - 1] == key)) continue;  // not the first slot of a cell
@@ -410,21 +516,23 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
             }
             float v[U], m0[U], m1[U];
             bool stock[U];
-            double kp[U];
+            double kp[U], amt[U], dl[U];
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 v[u] = 0.0f;
                 m0[u] = m1[u] = 0.0f;
                 stock[u] = false;
-                kp[u] = 0.0;
+                kp[u] = amt[u] = dl[u] = 0.0;
                 if (in[u]) {
                     const int32_t s = sl[u], q = s / a.cap;
                     v[u] = a.vol[s];
+                    amt[u] = a.act[s];
+                    dl[u] = a.delta[s];
                     if (active && v[u] > 0.0f) {
                         m0[u] = a.mom[2 * (long long)s];
                         m1[u] = a.mom[2 * (long long)s + 1];
                     }
-                    if (a.last[s] && a.dth[q] == (int32_t)c) {
+                    if ((a.desc[s].dflags & ENTRY_LAST) && a.dth[q] == (int32_t)c) {
                         stock[u] = true;
                         kp[u] = a.keep[q];
                     }
@@ -439,6 +547,10 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
                     tb += (double)m1[u];
                 }
                 if (stock[u]) pd += kp[u];
+                if (dl[u] < 0.0)
+                    eroded += fx_mass(amt[u]);
+                else
+                    deposited += fx_mass(amt[u]);
             }
             more = in[U - 1];
         }
@@ -446,7 +558,8 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
         accp[2] = ta;
         accp[3] = tb;
         a.pend[c] = pd;
-        const double acc = a.hand[c].x;
+        const unsigned long long *hw = reinterpret_cast<const unsigned long long *>(a.hand + c);
+        const double acc = hand_acc(hw[0], hw[1]);
         accp[0] = acc;
         if (active) {
             a.A[c].x = (float)(a.L[c].x + acc);
@@ -454,12 +567,39 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
             a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
         }
     }
+    if (eroded) atomicAdd(&sfx[0], (unsigned long long)eroded);
+    if (deposited) atomicAdd(&sfx[1], (unsigned long long)deposited);
+    __syncthreads();
+    if (threadIdx.x == 0 && sfx[0]) red_add(reinterpret_cast<long long *>(&a.stats->eroded_fx), (long long)sfx[0]);
+    if (threadIdx.x == 1 && sfx[1]) red_add(reinterpret_cast<long long *>(&a.stats->deposited_fx), (long long)sfx[1]);
+}
+
+// zero the hand-off counters (the live net changes stay), so the 32-bit epochs can start over
+__global__ void hand_reset_kernel(long long ncell, double2 *hand)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        unsigned long long *hw = reinterpret_cast<unsigned long long *>(hand + c);
+        hw[0] &= 0xffffffffull;
+        hw[1] &= 0xffffffffull;
+    }
+}
+
+cudaError_t hand_reset(long long ncell, double2 *hand, cudaStream_t st)
+{
+    hand_reset_kernel<<<grid_for(ncell), 256, 0, st>>>(ncell, hand);
+    return cudaPeekAtLastError();
+}
+
+cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, const uint8_t *mask, CellTerr *terr, cudaStream_t st)
+{
+    ordered_terrain_kernel<<<grid_for(ncell), 256, 0, st>>>(ncell, L, B, mask, terr);
+    return cudaPeekAtLastError();
 }
 
 int ordered_blocks_per_sm(int threads)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel, threads, 0) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false>, threads, 0) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -477,10 +617,13 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     tb = w.temp_bytes;
     if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, w.segpos, w.segscan, MaxOp{}, (int)nslots, st)) != cudaSuccess) return e;
     ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
-                                                          const_cast<int32_t *>(w.a.D), const_cast<uint8_t *>(w.a.last));
+                                                          w.a.delta, w.a.vol, const_cast<EntryDesc *>(w.a.desc));
     long long blocks = (w.nw * 32 + 255) / 256;  // a warp per droplet
     if (blocks > w.max_blocks) blocks = w.max_blocks;
-    ordered_apply_kernel<<<(int)blocks, 256, 0, st>>>(w.a);
+    if (w.a.ecap)
+        ordered_apply_kernel<true><<<(int)blocks, 256, 0, st>>>(w.a);
+    else
+        ordered_apply_kernel<false><<<(int)blocks, 256, 0, st>>>(w.a);
     ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
     return cudaPeekAtLastError();
 }

@@ -4,6 +4,24 @@
 
 namespace pge {
 
+// one entry of a wave's change lists as the ordered apply reads it (built by the rank kernel)
+struct alignas(16) EntryDesc {
+    int32_t cell;
+    uint32_t dflags;  // D (distinct earlier droplets of the wave at the cell) | ENTRY_* flags
+    double delta;
+};
+constexpr uint32_t ENTRY_D_MASK = 0xffffffu;
+constexpr uint32_t ENTRY_LAST = 1u << 24;   // its droplet's last visit to the cell
+constexpr uint32_t ENTRY_FIRST = 1u << 25;  // its droplet's first visit to the cell
+constexpr uint32_t ENTRY_STEP = 1u << 26;   // a step entry (vol >= 0), not a final deposit
+
+// a cell's read-only terrain for the ordered apply (built once per pass)
+struct alignas(16) CellTerr {
+    double hs;        // height + sediment at the start of the pass
+    float base;
+    uint32_t active;  // 1: the cell's mask is PGE_MASK_ACTIVE
+};
+
 struct OrderedArgs {
     // the wave's change lists, `cap` slots per droplet
     const int32_t *cell;
@@ -13,9 +31,8 @@ struct OrderedArgs {
     const int64_t *count;
     int cap;
     long long nw;
-    // per slot: distinct earlier droplets at the slot's cell, last visit of its droplet there
-    const int32_t *D;
-    const uint8_t *last;
+    const EntryDesc *desc;
+    const CellTerr *terr;
     // terrain
     const double2 *L;  // x: height + sediment
     const double *sediment;
@@ -25,10 +42,12 @@ struct OrderedArgs {
     const double *ecap;
     // per cell: the live net change and the hand-off counter, one 16-byte word
     double2 *hand;
-    unsigned long long epoch;
+    uint32_t epoch;  // this wave's: a cell with D earlier visitors is free once its counter reads epoch + D
     // per droplet: the stockpile cell (-1: none) and the amount it adds there
     int32_t *dth;
     double *keep;
+    // per slot: the amount the entry actually eroded or deposited (its statistics are summed later)
+    double *act;
     // float64 accumulators in serial order: (net change, discharge, momentum a, b) and the stockpile
     double *acc4;
     double *pend;
@@ -52,5 +71,7 @@ struct OrderedWave {
 size_t ordered_temp_bytes(long long nslots);
 int ordered_blocks_per_sm(int threads);
 cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st);
+cudaError_t hand_reset(long long ncell, double2 *hand, cudaStream_t st);
+cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, const uint8_t *mask, CellTerr *terr, cudaStream_t st);
 
 }  // namespace pge
