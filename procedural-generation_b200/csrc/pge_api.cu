@@ -230,6 +230,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.rec_base = 0;
         a.ledger = 1;
         a.minb = minb;
+        a.lanes = 32;
         unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
         const long long wave = p->wave;
         const long long nw = (P + wave - 1) / wave;
@@ -290,6 +291,9 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(256);
+            const long long rec_warps =
+                (long long)sm_count() * (p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
+                                                                      : droplet_blocks_per_sm_f32(32, 1, false));
             int ebits = 1;
             while ((1LL << ebits) <= wave) ebits++;
             long long ebase = 0;
@@ -300,10 +304,14 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 a.counter = ctr + (w & 1);
                 a.counter_next = ctr + ((w + 1) & 1);
                 // a small wave is latency-bound: spread it over every SM (one or two warps each)
+                // a wave's trace is latency-bound (each droplet is a serial chain of steps): give each
+                // warp as few droplets as keeps every warp resident, so lanes do not wait on each
+                // other's branches
                 const long long nd = a.d_end - a.d_begin;
-                int tpb = threads;
-                while (tpb > 32 && (nd + tpb - 1) / tpb < 2LL * sm_count()) tpb >>= 1;
-                long long blocks = (nd + tpb - 1) / tpb;
+                long long lanes = (nd + rec_warps - 1) / rec_warps;
+                a.lanes = (int)(lanes < 1 ? 1 : (lanes > 32 ? 32 : lanes));
+                const int tpb = 32;
+                long long blocks = (nd + a.lanes - 1) / a.lanes;
                 if (blocks * tpb > lay.nslots) blocks = lay.nslots / tpb;
                 e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, tpb, st)
                                                  : launch_droplets_f32(a, (int)blocks, tpb, st);

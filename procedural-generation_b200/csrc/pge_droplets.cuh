@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
     t.reset(gen);
 
     // droplet registers
-    bool alive = false, done = false;
+    bool alive = false, done = lane >= a.lanes;  // lanes past a.lanes take no droplet
     long long d = 0;
     int f = 0, step = 0, uphill = 0, sea_steps = 0, nring = 0;
     R x = R(0), y = R(0), sa = R(0), sb = R(0), vol = R(0), sed = R(0);

@@ -14,10 +14,11 @@ cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cuda
         f32::droplet_kernel<1, true><<<blocks, threads, 0, st>>>(a);
     return cudaPeekAtLastError();
 }
-int droplet_blocks_per_sm_f32(int threads, int minb)
+int droplet_blocks_per_sm_f32(int threads, int minb, bool ledger)
 {
     int n = 0;
-    cudaError_t e = minb >= 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f32::droplet_kernel<2, true>, threads, 0)
+    cudaError_t e = !ledger     ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f32::droplet_kernel<1, false>, threads, 0)
+                    : minb >= 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f32::droplet_kernel<2, true>, threads, 0)
                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f32::droplet_kernel<1, true>, threads, 0);
     if (e != cudaSuccess) return 1;
     return n > 0 ? n : 1;

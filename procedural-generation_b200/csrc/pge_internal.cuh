@@ -107,13 +107,14 @@ struct DropArgs {
     long long rec_base;  // recorded droplet index = d - rec_base
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
+    int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
 };
 
 // launchers of the two precisions (separate translation units: the float64
 // one is compiled without FMA contraction so it rounds like the reference)
 cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);
-int droplet_blocks_per_sm_f64(int threads, int minb);
-int droplet_blocks_per_sm_f32(int threads, int minb);
+int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger = true);
+int droplet_blocks_per_sm_f32(int threads, int minb, bool ledger = true);
 
 }  // namespace pge
