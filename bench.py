@@ -42,6 +42,67 @@ for p in (ROOT, ROOT / "procedural-generation_b200"):
 BYTES_PER_STEP = 137
 
 
+def run_batched(args, rank, world_size, dist, dev):
+    """The batched workload: 64 Earth-like worlds, N_c drawn from 64..512, rates jittered +-30 %,
+    6 N^2 / 8 droplets and max_steps 2 N each, shared out between the ranks.  Timed per rank with
+    CUDA events (max over ranks): one iteration with the worlds stepped one by one on one stream,
+    then iterations with every world on its own stream at once (pgerosion.batch.Runner)."""
+    import torch
+
+    from pgerosion import batch
+    from pgerosion import maps as gm
+
+    worlds = batch.batch_worlds(args.batch_worlds, seed=0)
+    mine = batch.my_worlds([w.cost for w in worlds], rank, world_size)
+    sub = [worlds[i] for i in mine]
+    counts = [w.n_particles for w in sub]
+    k = max(1, args.batch_steps)
+    states = batch.build_states(sub, device=dev)
+    # every world's spawn uniforms for the timed iterations, drawn up front and resident in HBM
+    pre = {}
+    for i, w in enumerate(sub):
+        for it in range(1, 2 + k):
+            rng, u, off = gm.draw_spawns(w.params, "erosion", (it,), counts[i])
+            pre[(i, it)] = (rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev))
+    runner = batch.Runner(states, [w.params for w in sub], costs=[w.cost for w in sub]) if sub else None
+    if runner:
+        runner.step(1, n_particles=counts)  # warm-up: workspaces, first pass of every world
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev[0].record()
+    one, worst = 0, 0.0
+    for i, (st, w) in enumerate(zip(states, sub)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        one += gm.step(st, w.params, st.iteration, n_particles=counts[i], predrawn=pre[(i, st.iteration)])["droplet_steps"]
+        e1.record()
+        e1.synchronize()
+        worst = max(worst, e0.elapsed_time(e1))
+    ev[1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev[2].record()
+    res = runner.step(k, n_particles=counts, spawns=lambda i, it: pre[(i, it)]) if runner else []
+    ev[3].record()
+    torch.cuda.synchronize()
+    together = sum(s["droplet_steps"] for r in res for s in r)
+    (one_all, tog_all), (ms_one, ms_tog, worst) = batch.reduce_totals(
+        dist, [one, together], [ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), worst], device=dev)
+    sizes = sorted(w.N for w in worlds)
+    v_one, v_tog = one_all / (ms_one * 1e-3), tog_all / (ms_tog * 1e-3)
+    del runner, states
+    torch.cuda.empty_cache()
+    return {"workload": f"{len(worlds)} worlds, N_c {sizes[0]}..{sizes[-1]} (mean N_c^2 {np.mean(np.square(sizes)):.0f}), "
+                        "6 N^2/8 droplets, max_steps 2N, rates +-30 %, ordered apply",
+            "one_by_one": {"value": v_one, "unit": "droplet-steps/s", "ms_per_step": ms_one},
+            "concurrent": {"value": v_tog, "unit": "droplet-steps/s", "ms_per_step": ms_tog / k, "steps": k},
+            "speedup": v_tog / v_one,
+            "slowest_world_ms_per_step": worst}
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -153,6 +214,7 @@ def run_b200(args, rank, world_size, dist):
 
     from pgerosion import _lib
     from pgerosion import maps as gm
+    from pgerosion.batch import reduce_totals
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -218,13 +280,7 @@ def run_b200(args, rank, world_size, dist):
     ee[1].record()
     torch.cuda.synchronize()
     e2e_ms = ee[0].elapsed_time(ee[1])
-    tot = torch.tensor([steps_done, e2e_steps], dtype=torch.float64, device=dev)
-    tm = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(tot)
-        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-    steps_all, e2e_all = float(tot[0]), float(tot[1])
-    ms_max, e2e_ms_max = float(tm[0]), float(tm[1])
+    (steps_all, e2e_all), (ms_max, e2e_ms_max) = reduce_totals(dist, [steps_done, e2e_steps], [ms, e2e_ms], device=dev)
     alt = None
     if apply == _lib.APPLY_ORDERED and not args.no_alt:
         # the order-free wave apply on the same world (one wave per iteration): faster, not the
@@ -263,6 +319,9 @@ def run_b200(args, rank, world_size, dist):
                "ms_per_step": float(t2[1]) / args.alt_steps,
                "roofline": {"bound": "hbm", "achieved": ach2, "peak": peak, "unit": "GB/s", "frac": ach2 / peak,
                             "ms_per_launch": avg2}}
+    batched = None
+    if not args.no_batch:
+        batched = run_batched(args, rank, world_size, dist, dev)
     if rank != 0:
         return None
     peak, peak_kind = _peaks()
@@ -295,6 +354,8 @@ def run_b200(args, rank, world_size, dist):
     }
     if alt is not None:
         out["alt_wave_apply"] = alt
+    if batched is not None:
+        out["batched_worlds"] = batched
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
@@ -336,6 +397,9 @@ def run_reference(args, rank):
 
 
 def main():
+    # the batched measurement runs up to 64 streams at once: let the runtime give them 32 hardware
+    # queues instead of 8 (a property of this process's CUDA context, set before CUDA starts)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -351,6 +415,9 @@ def main():
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
+    ap.add_argument("--batch-worlds", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

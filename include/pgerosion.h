@@ -92,6 +92,9 @@ typedef struct PgeGrid {
     int32_t deposit_on_exit; /* window mode: leaving droplets drop their load */
     int32_t metric_shared;   /* 1: metric tables are (NE, NE, 3), the same on every face */
     int32_t max_steps;       /* workspace capacity: the largest erosion.max_steps any call uses */
+    int32_t wave_tables;     /* 1: the workspace holds the per-thread own-change tables that the wave
+                                apply and pge_trace_changelist need (they grow with max_steps);
+                                0: ordered apply and map passes only */
     int64_t max_droplets;    /* workspace capacity: the most spawns (rain + stockpiles) of one pass */
     int64_t max_wave;        /* workspace capacity: the largest wave of the exact (ordered) apply */
 } PgeGrid;
@@ -135,6 +138,12 @@ typedef struct PgeParams {
     int32_t use_erode_cap;   /* slope_limit_erode > 0: erode_cap passed to pge_trace_apply */
     int32_t threads_per_block; /* 0 = default */
     int32_t blocks_per_sm;     /* 0 = occupancy maximum */
+    int32_t trace_lanes;       /* ordered apply: droplets per warp in each wave's trace; 0 = as few as keep
+                                  every warp of the wave resident (fastest alone), up to 32 (smallest
+                                  footprint, for passes of several worlds running at once) */
+    int32_t apply_lanes;       /* ordered apply: droplets per warp in the apply, 0 = 1 .. 32; more hold
+                                  fewer warps but lanes waiting on different hand-offs take turns
+                                  (one per warp measured fastest, alone and with other passes) */
 } PgeParams;
 
 /* counters of one droplet pass (device struct; the caller zeroes it) */

@@ -79,6 +79,8 @@ int check_params(const PgeGrid *g, const PgeParams *p)
     if (p->precision != PGE_PREC_F64 && p->precision != PGE_PREC_F32) return fail(PGE_E_ARG, "unknown precision %d", p->precision);
     if (p->threads_per_block != 0 && (p->threads_per_block < 32 || p->threads_per_block > 256 || p->threads_per_block % 32))
         return fail(PGE_E_ARG, "threads_per_block must be a multiple of 32 in 32..256");
+    if (p->trace_lanes < 0 || p->trace_lanes > 32) return fail(PGE_E_ARG, "trace_lanes %d outside 0..32", p->trace_lanes);
+    if (p->apply_lanes < 0 || p->apply_lanes > 32) return fail(PGE_E_ARG, "apply_lanes %d outside 0..32", p->apply_lanes);
     return PGE_OK;
 }
 
@@ -127,6 +129,7 @@ Layout layout(const PgeGrid &g)
     L.metric8 = take(32 * L.nmetric);
     L.acc4 = take(32 * L.ncell);
     L.pend = take(8 * L.ncell);
+    if (!g.wave_tables) L.table_slots = 0;  // no own-change tables: ordered apply and map passes only
     L.tkey = take(8 * L.nslots * L.table_slots);
     L.town = take(8 * L.nslots * L.table_slots);
     L.counters = take(256);
@@ -180,7 +183,11 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.pend), 0, 8 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset pending");
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.counters), 0, 16, st)) != cudaSuccess) return cuda_fail(e, "memset counters");
     // own-change tables: generation 0 everywhere (free); waves then use generations (w + 1) << 24 onwards
-    if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.tkey), 0, 8 * lay.nslots * lay.table_slots, st)) != cudaSuccess)
+    const bool ledger_pass = p->apply == PGE_APPLY_WAVE || rec_cell != nullptr;
+    if (ledger_pass && !g->wave_tables)
+        return fail(PGE_E_WORKSPACE, "the wave apply and the change-list hook need a workspace built with wave_tables = 1");
+    if (lay.table_slots &&
+        (e = cudaMemsetAsync(ws_ptr<void>(ws, lay.tkey), 0, 8 * lay.nslots * lay.table_slots, st)) != cudaSuccess)
         return cuda_fail(e, "memset tables");
     pack(*g, *s, lay, ws, st);
     const long long P = sp->count;
@@ -218,7 +225,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.stats = stats;
         a.tkey = ws_ptr<unsigned long long>(ws, lay.tkey);
         a.town = ws_ptr<double>(ws, lay.town);
-        a.table_mask = (unsigned)(lay.table_slots - 1);
+        a.table_mask = lay.table_slots ? (unsigned)(lay.table_slots - 1) : 0u;
         a.table_cap = (int)lay.table_cap;
         a.rec_cell = rec_cell;
         a.rec_delta = rec_delta;
@@ -290,7 +297,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.segscan = ws_ptr<int32_t>(ws, lay.w_segscan);
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
-            ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(256);
+            oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
+            ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);
             const long long rec_warps =
                 (long long)sm_count() * (p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
                                                                       : droplet_blocks_per_sm_f32(32, 1, false));
@@ -308,7 +316,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 // warp as few droplets as keeps every warp resident, so lanes do not wait on each
                 // other's branches
                 const long long nd = a.d_end - a.d_begin;
-                long long lanes = (nd + rec_warps - 1) / rec_warps;
+                long long lanes = p->trace_lanes > 0 ? p->trace_lanes : (nd + rec_warps - 1) / rec_warps;
                 a.lanes = (int)(lanes < 1 ? 1 : (lanes > 32 ? 32 : lanes));
                 const int tpb = 32;
                 long long blocks = (nd + a.lanes - 1) / a.lanes;

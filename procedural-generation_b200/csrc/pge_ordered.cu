@@ -225,6 +225,9 @@ size_t ordered_temp_bytes(long long nslots)
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int RING = 8;  // entry slots per droplet: entries k .. k+5 are in flight
+// two droplets per block: a block's warp slots free up as soon as its two droplets are done, so
+// concurrent passes (other worlds' waves on other streams) pack around the long-lived droplets
+constexpr int APPLY_THREADS = 64;
 
 // one entry of a droplet's list as the apply reads it, filled by asynchronous copies
 struct alignas(16) Slot {
@@ -290,21 +293,22 @@ __device__ __forceinline__ bool cell_value(const OrderedArgs &a, const Walk &w, 
 }  // namespace
 
 template <bool ECAP>
-__global__ void __launch_bounds__(256) ordered_apply_kernel(const OrderedArgs a)
+__global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const OrderedArgs a)
 {
     __shared__ unsigned long long sstat[OS_N];
-    __shared__ Slot ring[8][RING];
+    extern __shared__ Slot ring[];  // per droplet lane: RING slots
     for (int k = threadIdx.x; k < OS_N; k += blockDim.x) sstat[k] = 0ull;
     __syncthreads();
     const PgeParams &p = a.p;
-    // one droplet per warp (its lane 0): a droplet waits on earlier droplets' hand-offs, and lanes of
-    // one warp waiting on each other would serialise the warp
-    const long long T = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long wq0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const bool lane0 = (threadIdx.x & 31) == 0;
-    Slot *R = ring[(threadIdx.x >> 5) & 7];
+    // a.lanes droplets per warp, one per lane (1 when a pass runs alone: lanes of one warp that wait
+    // on different hand-offs take turns; more when other passes share the GPU, to hold fewer warps).
+    // A lane only ever waits for earlier droplets, which independent thread scheduling lets run.
+    const int lane = threadIdx.x & 31, lanes = a.lanes;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    Slot *R = ring + ((size_t)(threadIdx.x >> 5) * lanes + lane) * RING;
     bool failed = false;
-    for (long long q = wq0; lane0 && !failed && q < a.nw; q += T) {
+    for (long long q = gw * lanes + lane; lane < lanes && !failed && q < a.nw; q += nwarps * lanes) {
         const int K = (int)a.count[q];
         if (K <= 0) {
             a.dth[q] = -1;
@@ -596,10 +600,11 @@ cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, 
     return cudaPeekAtLastError();
 }
 
-int ordered_blocks_per_sm(int threads)
+int ordered_blocks_per_sm(int lanes)
 {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false>, threads, 0) != cudaSuccess) return 1;
+    const size_t smem = (size_t)(APPLY_THREADS / 32) * lanes * RING * sizeof(Slot);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false>, APPLY_THREADS, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -618,12 +623,14 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, w.segpos, w.segscan, MaxOp{}, (int)nslots, st)) != cudaSuccess) return e;
     ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
                                                           w.a.delta, w.a.vol, const_cast<EntryDesc *>(w.a.desc));
-    long long blocks = (w.nw * 32 + 255) / 256;  // a warp per droplet
+    const long long warps = (w.nw + w.a.lanes - 1) / w.a.lanes;  // a lane per droplet
+    long long blocks = (warps * 32 + APPLY_THREADS - 1) / APPLY_THREADS;
     if (blocks > w.max_blocks) blocks = w.max_blocks;
+    const size_t smem = (size_t)(APPLY_THREADS / 32) * w.a.lanes * RING * sizeof(Slot);
     if (w.a.ecap)
-        ordered_apply_kernel<true><<<(int)blocks, 256, 0, st>>>(w.a);
+        ordered_apply_kernel<true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     else
-        ordered_apply_kernel<false><<<(int)blocks, 256, 0, st>>>(w.a);
+        ordered_apply_kernel<false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
     return cudaPeekAtLastError();
 }

@@ -43,6 +43,7 @@ struct OrderedArgs {
     // per cell: the live net change and the hand-off counter, one 16-byte word
     double2 *hand;
     uint32_t epoch;  // this wave's: a cell with D earlier visitors is free once its counter reads epoch + D
+    int lanes;  // droplets per warp in the apply
     // per droplet: the stockpile cell (-1: none) and the amount it adds there
     int32_t *dth;
     double *keep;
@@ -69,7 +70,7 @@ struct OrderedWave {
 };
 
 size_t ordered_temp_bytes(long long nslots);
-int ordered_blocks_per_sm(int threads);
+int ordered_blocks_per_sm(int lanes);  // resident blocks of the apply kernel per SM
 cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st);
 cudaError_t hand_reset(long long ncell, double2 *hand, cudaStream_t st);
 cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, const uint8_t *mask, CellTerr *terr, cudaStream_t st);

@@ -35,7 +35,8 @@ c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, cty
 
 class PgeGrid(ctypes.Structure):
     _fields_ = [("F", c_i32), ("N", c_i32), ("H", c_i32), ("spherical", c_i32), ("deposit_on_exit", c_i32),
-                ("metric_shared", c_i32), ("max_steps", c_i32), ("max_droplets", c_i64), ("max_wave", c_i64)]
+                ("metric_shared", c_i32), ("max_steps", c_i32), ("wave_tables", c_i32), ("max_droplets", c_i64),
+                ("max_wave", c_i64)]
 
 
 class PgeState(ctypes.Structure):
@@ -52,7 +53,7 @@ PARAM_DOUBLES = ("dt", "density", "friction", "deposition_rate", "evap_rate", "k
                  "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "iter_erode",
                  "iter_deposit", "fan_slope", "offshore_writeoff", "ema")
 PARAM_INTS = ("max_steps", "pit_steps", "ocean_steps", "wave", "precision", "apply", "use_erode_cap", "threads_per_block",
-              "blocks_per_sm")
+              "blocks_per_sm", "trace_lanes", "apply_lanes")
 
 
 class PgeParams(ctypes.Structure):

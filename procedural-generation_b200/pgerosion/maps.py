@@ -78,6 +78,7 @@ class ErosionState:
     max_droplets: int = 0
     max_steps: int = 0
     max_wave: int = 0
+    wave_tables: bool = False
     _ws: torch.Tensor = field(default=None, repr=False)
     _halo: tuple = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
@@ -155,7 +156,7 @@ class ErosionState:
     def pge_grid(self) -> PgeGrid:
         return PgeGrid(F=self.F, N=self.N, H=self.H, spherical=int(bool(self.spherical)),
                        deposit_on_exit=int(bool(self.deposit_on_exit)), metric_shared=1, max_steps=int(self.max_steps),
-                       max_droplets=int(self.max_droplets), max_wave=int(self.max_wave))
+                       wave_tables=int(self.wave_tables), max_droplets=int(self.max_droplets), max_wave=int(self.max_wave))
 
     def pge_state(self) -> PgeState:
         return PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
@@ -163,12 +164,14 @@ class ErosionState:
                         hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
                         metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv))
 
-    def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1) -> None:
+    def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to
         ``max_droplets`` spawns of ``max_steps`` steps and ordered-apply
         waves of up to ``max_wave`` droplets (grows, never shrinks)."""
-        if max_droplets <= self.max_droplets and max_steps <= self.max_steps and max_wave <= self.max_wave and self._ws is not None:
+        if (max_droplets <= self.max_droplets and max_steps <= self.max_steps and max_wave <= self.max_wave
+                and (self.wave_tables or not wave_tables) and self._ws is not None):
             return
+        self.wave_tables = bool(self.wave_tables or wave_tables)
         self.max_droplets = max(int(max_droplets), self.max_droplets)
         self.max_steps = max(int(max_steps), self.max_steps)
         self.max_wave = max(int(max_wave), self.max_wave, 1)
@@ -234,7 +237,8 @@ def default_wave(ep, n_particles: int) -> int:
 
 
 def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, precision: int, mom_scale=1.0, disc_sat=None,
-                iter_deposit=None, threads_per_block=0, blocks_per_sm=0, apply=_lib.APPLY_ORDERED) -> PgeParams:
+                iter_deposit=None, threads_per_block=0, blocks_per_sm=0, apply=_lib.APPLY_ORDERED, trace_lanes=0,
+                apply_lanes=0) -> PgeParams:
     u = state.height_unit_m
     return PgeParams(
         dt=float(ep.dt), density=float(ep.density), friction=float(ep.friction), deposition_rate=float(ep.deposition_rate),
@@ -248,7 +252,7 @@ def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, prec
         fan_slope=float(ep.fan_slope), offshore_writeoff=float(ep.offshore_writeoff), ema=float(ep.ema),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
         precision=int(precision), apply=int(apply), use_erode_cap=0, threads_per_block=int(threads_per_block),
-        blocks_per_sm=int(blocks_per_sm))
+        blocks_per_sm=int(blocks_per_sm), trace_lanes=int(trace_lanes), apply_lanes=int(apply_lanes))
 
 
 def draw_spawns(params, rng_stage: str, key, P: int):
@@ -264,7 +268,7 @@ def draw_spawns(params, rng_stage: str, key, P: int):
 def run_iteration(state: ErosionState, params, iteration_key, n_particles: int | None = None,
                   particles_per_cell: float | None = None, rng_stage: str = "erosion", log=None, wave: int | None = None,
                   precision: int = _lib.PREC_F64, predrawn=None, threads_per_block: int = 0, blocks_per_sm: int = 0,
-                  events=None, apply: int = _lib.APPLY_ORDERED) -> dict:
+                  events=None, apply: int = _lib.APPLY_ORDERED, trace_lanes: int = 0, apply_lanes: int = 0) -> dict:
     """One particle pass (maps.py:839-1047) on the device; see the module
     docstring.  ``predrawn`` may carry ``draw_spawns``' result for this
     iteration (drawn ahead, host or device arrays); ``events`` a pair of
@@ -280,7 +284,8 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     max_steps = max_steps_of(ep, state.N)
     # stockpiles re-injected: at most one per interior cell; the reference's chunk is at most erosion.chunk
     state.reserve(P + state.F * state.N * state.N, max_steps,
-                  (int(ep.chunk) if wave is None else int(wave)) if apply == _lib.APPLY_ORDERED else 1)
+                  (int(ep.chunk) if wave is None else int(wave)) if apply == _lib.APPLY_ORDERED else 1,
+                  wave_tables=apply == _lib.APPLY_WAVE)
     rng, u, off = predrawn if predrawn is not None else draw_spawns(params, rng_stage, key, P)
     L = _lib.load()
     g = state.pge_grid()
@@ -334,7 +339,7 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
         iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     w = default_wave(ep, Ptot) if wave is None else int(wave)
     prm = make_params(state, ep, volume0, Ptot, w, precision, mom_scale, disc_sat, iter_deposit, threads_per_block, blocks_per_sm,
-                      apply)
+                      apply, trace_lanes, apply_lanes)
     if events is not None:
         events[0].record()
     check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), None, _ptr(stats_d),
@@ -465,7 +470,7 @@ def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, s
     ep = erosion_group(params)
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
-    state.reserve(P, max_steps, 1)
+    state.reserve(P, max_steps, 1, wave_tables=True)
     L = _lib.load()
     dev = state.height.device
     cap = max_steps + 2 * 8 + 1 + 8 + 8
@@ -514,7 +519,7 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
     w = default_wave(ep, P) if wave is None else int(wave)
-    state.reserve(P, max_steps, w if apply == _lib.APPLY_ORDERED else 1)
+    state.reserve(P, max_steps, w if apply == _lib.APPLY_ORDERED else 1, wave_tables=apply == _lib.APPLY_WAVE)
     L = _lib.load()
     dev = state.height.device
     sp = state._spawn
