@@ -15,6 +15,9 @@
  *                                                  globe/erosion/particle.py:164-1101, 1230-1242
  *   pge_trace_changelist  trace_particles' change list, for parity checks
  *                                                  globe/erosion/particle.py:275-818
+ *   pge_slope_erode_cap   slope_erode_cap (erosion.slope_limit_erode > 0)
+ *                                                  globe/erosion/particle.py:1046-1076,
+ *                                                  globe/erosion/maps.py:922-927
  *   pge_thermal           thermal_erosion (talus pass + creep pass)
  *                                                  globe/erosion/maps.py:1050-1085,
  *                                                  globe/erosion/particle.py:1107-1227
@@ -33,8 +36,10 @@
  *     negative PGE_E* code; pge_last_error() describes the last failure of
  *     the calling thread.  Launch errors are checked with
  *     cudaPeekAtLastError; device-side overflow is counted in PgeStats.
- *   - Results do not depend on thread scheduling: terrain changes, tracks,
- *     stockpiles and stat totals are summed as int64 fixed point.
+ *   - Results do not depend on thread scheduling: the ordered apply does
+ *     every float64 read and write of a cell in the serial order; the wave
+ *     apply sums terrain changes, tracks and stockpiles as int64 fixed
+ *     point; stat totals are int64 fixed point in both.
  *   - Calls on one state are not reentrant; order them on one stream.
  */
 #ifndef PGEROSION_H
@@ -224,6 +229,14 @@ PGE_API int pge_trace_changelist(const PgeGrid *g, PgeState *s, const PgeSpawns 
  * acc (F,NE,NE), disch_track (F,NE,NE), mom_track (F,NE,NE,2), pending (F,NE,NE). */
 PGE_API int pge_read_accumulators(const PgeGrid *g, double *acc, double *disch_track, double *mom_track, double *pending,
                           void *ws, size_t ws_bytes, void *stream);
+
+/* soillib's pit-free erosion cap: erode_cap (F,NE,NE) = coef * sqrt(2) * the Godunov downhill
+ * slope of height + sediment (per axis the steeper one-sided downhill difference, exit_slope off
+ * the array, 0 outside the active mask).  Computed once per iteration before the droplet pass and
+ * passed to pge_trace_apply with p->use_erode_cap = 1 (coef = erosion.slope_limit_erode,
+ * exit_slope = erosion.slope_limit_exit). */
+PGE_API int pge_slope_erode_cap(const PgeGrid *g, const PgeState *s, double coef, double exit_slope, double *erode_cap,
+                                void *stream);
 
 /* Talus pass, then (creep_rate > 0) the creep pass with submerged cells frozen. */
 PGE_API int pge_thermal(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max,

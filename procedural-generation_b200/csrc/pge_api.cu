@@ -1,4 +1,5 @@
 // pge_api.cu -- the extern "C" entry points of libpgerosion (include/pgerosion.h).
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -39,13 +40,21 @@ int cuda_fail(cudaError_t e, const char *where)
     return fail(PGE_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
 }
 
-int check_grid(const PgeGrid *g)
+// the geometry alone (calls that use no workspace)
+int check_shape(const PgeGrid *g)
 {
     if (!g) return fail(PGE_E_ARG, "grid is NULL");
     if (g->F < 1 || g->N < 2 || g->H < 1 || g->N < 2 * g->H) return fail(PGE_E_ARG, "bad grid F=%d N=%d H=%d", g->F, g->N, g->H);
     if (g->spherical && g->F != 6) return fail(PGE_E_ARG, "a spherical grid has 6 faces (F=%d)", g->F);
     const long long NE = g->N + 2LL * g->H;
     if ((long long)g->F * NE * NE >= (1LL << 31)) return fail(PGE_E_ARG, "grid too large for int32 cell indices");
+    return PGE_OK;
+}
+
+int check_grid(const PgeGrid *g)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
     if (g->max_steps < 1 || g->max_droplets < 1 || g->max_wave < 1) return fail(PGE_E_ARG, "workspace capacities must be positive");
     if (g->max_wave > (1LL << 20)) return fail(PGE_E_ARG, "max_wave above 2^20");
     return PGE_OK;
@@ -480,6 +489,18 @@ PGE_API int pge_thermal(const PgeGrid *g, PgeState *s, double thermal_rate, doub
     thermal(*g, *s, lay, ws, thermal_rate, creep_rate, thermal_max, soft, diff, dep_floor, (cudaStream_t)stream);
     cudaError_t e = cudaPeekAtLastError();
     return e == cudaSuccess ? PGE_OK : cuda_fail(e, "thermal");
+}
+
+PGE_API int pge_slope_erode_cap(const PgeGrid *g, const PgeState *s, double coef, double exit_slope, double *erode_cap,
+                                void *stream)
+{
+    int r;
+    if ((r = check_shape(g)) || (r = check_state(s))) return r;
+    if (!erode_cap) return fail(PGE_E_ARG, "erode_cap is NULL");
+    // the reference's k = coef * sqrt(2) (its cell diagonal), taken on the host in float64
+    slope_erode_cap(*g, *s, coef * sqrt(2.0), exit_slope, erode_cap, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "slope erode cap");
 }
 
 PGE_API int pge_uplift(const PgeGrid *g, PgeState *s, double cap, double scale, void *ws, size_t ws_bytes, void *stream)

@@ -745,4 +745,40 @@ cudaError_t collect_pending(const PgeGrid &g, PgeState &s, const Layout &lay, vo
     return cudaPeekAtLastError();
 }
 
+// ---------------------------------------------------------------------------
+// soillib's pit-free erosion cap (particle.py:1046-1076): per active cell, k * |Godunov downhill
+// gradient| of the surface, each axis the steeper of its two one-sided downhill differences
+// (exit_slope off the array); float64 in the reference's operation order (no FMA in this file)
+// ---------------------------------------------------------------------------
+__global__ void slope_erode_cap_kernel(int F, int NE, const double *__restrict__ height, const double *__restrict__ sediment,
+                                       const uint8_t *__restrict__ mask, double k, double exit_slope, double *__restrict__ out)
+{
+    const long long n = (long long)F * NE * NE;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        if (mask && mask[c] != PGE_MASK_ACTIVE) {
+            out[c] = 0.0;
+            continue;
+        }
+        const long long r = c % ((long long)NE * NE);
+        const int i = (int)(r / NE), j = (int)(r - (long long)i * NE);
+        const double h = height[c] + sediment[c];
+        const double gxn = i == 0 ? exit_slope : h - (height[c - NE] + sediment[c - NE]);
+        const double gxp = i == NE - 1 ? exit_slope : h - (height[c + NE] + sediment[c + NE]);
+        const double gyn = j == 0 ? exit_slope : h - (height[c - 1] + sediment[c - 1]);
+        const double gyp = j == NE - 1 ? exit_slope : h - (height[c + 1] + sediment[c + 1]);
+        double gx = gxn > gxp ? gxn : gxp;
+        double gy = gyn > gyp ? gyn : gyp;
+        if (gx < 0.0) gx = 0.0;
+        if (gy < 0.0) gy = 0.0;
+        out[c] = k * sqrt(gx * gx + gy * gy);
+    }
+}
+
+void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_slope, double *out, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    slope_erode_cap_kernel<<<grid_for((long long)g.F * NE * NE), 256, 0, st>>>(g.F, NE, s.height, s.sediment, s.mask, k, exit_slope,
+                                                                             out);
+}
+
 }  // namespace pge

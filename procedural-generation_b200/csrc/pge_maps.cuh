@@ -15,6 +15,7 @@ void uplift(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double c
 void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double land_fraction, double level,
                 double *shift_dev, cudaStream_t st);
 void halo_gather(const PgeHalo &h, double *field, int vector, cudaStream_t st);
+void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_slope, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
 cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
                        long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st);

@@ -81,6 +81,7 @@ class ErosionState:
     wave_tables: bool = False
     _ws: torch.Tensor = field(default=None, repr=False)
     _halo: tuple = field(default=None, repr=False)
+    _erode_cap: torch.Tensor = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -332,17 +333,16 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
             disc_sat = float(ep.disc_saturation_cells) * rain_per_cell
         if float(ep.momentum_saturation_cells) > 0.0:
             mom_scale = volume0 / (float(ep.momentum_saturation_cells) * rain_per_cell)
-    if float(ep.slope_limit_erode) > 0.0:
-        raise _lib.PgeError("erosion.slope_limit_erode is not supported by the b200 backend yet")
     iter_deposit = cell_units(ep, "iter_deposit", state.height_unit_m)
     if float(ep.slope_limit_deposit) > 0.0:
         iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     w = default_wave(ep, Ptot) if wave is None else int(wave)
     prm = make_params(state, ep, volume0, Ptot, w, precision, mom_scale, disc_sat, iter_deposit, threads_per_block, blocks_per_sm,
                       apply, trace_lanes, apply_lanes)
+    ecap = _erode_cap(state, ep, prm)
     if events is not None:
         events[0].record()
-    check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), None, _ptr(stats_d),
+    check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), ecap, _ptr(stats_d),
                             _ptr(ws), ws.numel(), st), "pge_trace_apply")
     if events is not None:
         events[1].record()
@@ -374,6 +374,22 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
         log(f"  particles {Ptot} volume {volume0:.3f} mean steps {stats['steps_mean']:.1f} deaths {stats['deaths']} "
             f"clamped {stats['clamped']} pending {stats['pending_total']:.1f} ({stats['seconds']:.2f}s)")
     return stats
+
+
+def _erode_cap(state: ErosionState, ep, prm: PgeParams):
+    """soillib's pit-free erosion cap of this iteration's start terrain
+    (maps.py:922-927) when ``erosion.slope_limit_erode > 0``: computed on the
+    device, switched on in ``prm``; returns the pointer for pge_trace_apply
+    (None when off)."""
+    if float(ep.slope_limit_erode) <= 0.0:
+        return None
+    if state._erode_cap is None or state._erode_cap.shape != state.height.shape:
+        state._erode_cap = torch.empty_like(state.height)
+    check(_lib.load().pge_slope_erode_cap(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()),
+                                          float(ep.slope_limit_erode), float(ep.slope_limit_exit), _ptr(state._erode_cap),
+                                          _stream()), "pge_slope_erode_cap")
+    prm.use_erode_cap = 1
+    return _ptr(state._erode_cap)
 
 
 def _ensure_workspace(state: ErosionState, ep=None) -> None:
@@ -529,12 +545,15 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     spawns = PgeSpawns(face=_ptr(sp["face"]), x=_ptr(sp["x"]), y=_ptr(sp["y"]), sed=_ptr(sp["sed"]), dir=_ptr(sp["dir"]), count=P,
                        volume0=float(volume0))
     iter_deposit = cell_units(ep, "iter_deposit", state.height_unit_m)
+    if float(ep.slope_limit_deposit) > 0.0:
+        iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     prm = make_params(state, ep, volume0, P, w, precision, iter_deposit=iter_deposit, apply=apply)
+    ecap = _erode_cap(state, ep, prm)
     stats_d = sp["stats"]
     stats_d.zero_()
     ws = state.workspace
     check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns), ctypes.byref(prm),
-                            None, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
+                            ecap, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
     r = PgeStats.from_buffer_copy(stats_d.cpu().numpy().tobytes())
     if r.errors:
         raise _lib.PgeError("ordered apply: a cell hand-off wait gave up; the pass is invalid")

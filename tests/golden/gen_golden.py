@@ -17,6 +17,11 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
   iterations, a set of droplets whose touched cells (plus a one-cell ring)
   are pairwise disjoint, and the reference ``trace_particles`` change lists
   and ``apply_changes`` results for them (particle.py:275-1042).
+* ``window_trace.npz`` -- one face of that N=48 world cut out as a window
+  (``spherical=False``, F = 1; mask: an active basin inside a frozen
+  margin inside an outside ring; ``deposit_on_exit``), loaded and unloaded
+  droplets sharing cells, the reference ``trace_particles`` change lists
+  and the serial ``apply_changes`` results for all of them.
 * ``step_tiny.npz`` -- a six-face N=32 world run through the reference
   ``maps.step`` (plain knobs, uplift replay) for a few iterations: the
   initial state, the final state and the per-iteration stats.
@@ -214,6 +219,83 @@ def gen_trace(cs, maps, pk, WorldParams):
     print(f"trace_isolated: {keep.size} isolated droplets of {P}; deaths {np.bincount(res['sp_death'], minlength=6)}")
 
 
+def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit):
+    n = f.size
+    out = dict(cl_cell=np.zeros(n * cap, np.int32), cl_delta=np.zeros(n * cap), cl_vol=np.zeros(n * cap, np.float32),
+               cl_mom=np.zeros((n * cap, 2), np.float32), cl_count=np.zeros(n, np.int64), cl_lo=np.zeros(n, np.int64),
+               cl_hi=np.zeros(n, np.int64), sp_death=np.zeros(n, np.int8))
+    cu = lambda k: float(getattr(ep, k)) / unit
+    pk.trace_particles(f.astype(np.int64), x, y, sed, dirs, volume0, st_samp, False, mask, N, H, spherical,
+                       float(ep.dt), float(ep.density), float(ep.friction), float(ep.deposition_rate), float(ep.evap_rate),
+                       float(ep.k_mom), 1.0, float(ep.k_disc), float(ep.disc_saturation), float(ep.disc_exponent),
+                       float(ep.slope_gain), float(ep.slope_saturation), float(ep.erodibility), cu("cover_depth"),
+                       float(ep.min_volume_frac) * volume0, int(max_steps), cu("max_erode"), conc, int(ep.pit_steps),
+                       bool(deposit_on_exit), float(ep.ocean_deposition_rate), int(ep.ocean_steps), cu("fan_room"),
+                       cu("dep_floor_m"), float(ep.lake_trap), 0.0, 0.0, np.zeros((1, 1, 1), np.float32), False,
+                       out["cl_cell"], out["cl_delta"], out["cl_vol"], out["cl_mom"], out["cl_count"], out["cl_lo"],
+                       out["cl_hi"], out["sp_death"])
+    return out
+
+
+def gen_window(cs, maps, pk, WorldParams):
+    """A single-face window (spherical=False) cut from the evolved N=48 world."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=3, N=48, H=2, cell_size_m=50.0, land_fraction=0.35)
+    p = _world_params(WorldParams, 48, 2, 50.0, 3, 0.35, iterations=10, max_steps=64, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="stack")
+    st = _ref_state(cs, maps, world, p)
+    for it in range(3):
+        maps.step(st, p, it)
+    ep = p.erosion
+    NE, H, N = st.NE, st.H, st.N
+    land = [(st.height[k][H:H + N, H:H + N] + st.sediment[k][H:H + N, H:H + N] >= 0).mean() for k in range(6)]
+    fw = int(np.argsort(land)[3])  # a face with land and sea
+    sl = slice(fw, fw + 1)
+    w = {k: np.ascontiguousarray(getattr(st, k)[sl]) for k in ("height", "sediment", "discharge", "momentum", "evap", "hardness",
+                                                                "base", "metric", "metric_inv")}
+    # mask: outside ring (2 cells), frozen margin (3 cells), active basin
+    mask = np.zeros((1, NE, NE), np.uint8)
+    mask[0, 2:NE - 2, 2:NE - 2] = 2
+    mask[0, 5:NE - 5, 5:NE - 5] = 1
+    samp = np.zeros((1, NE, NE, st.samp.shape[-1]), np.float32)
+    pk.pack_samples(samp, w["height"], w["sediment"], w["height"], False, w["discharge"], w["momentum"], w["evap"], w["hardness"],
+                    w["metric"], w["metric_inv"], w["base"], np.zeros((1, NE, NE), np.uint8))
+    rng = np.random.default_rng(91)
+    act = np.flatnonzero(mask.reshape(-1) == 1)
+    n_rain, n_load = 1200, 250
+    pick = act[rng.integers(0, act.size, n_rain + n_load)]
+    ei, ej = pick // NE, pick % NE
+    x = (ei - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    y = (ej - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    sed = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 0.5 + 1e-3])
+    dirs = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 2 * np.pi])
+    f = np.zeros(x.size, np.int64)
+    volume0 = 0.02
+    conc = 1.0 / (volume0 * x.size)
+    max_steps = maps.max_steps_of(ep, N)
+    cap = int(pk.change_list_cap(max_steps, False))
+    res = _ref_trace(pk, ep, samp, mask, N, H, False, True, f, x, y, sed, dirs, volume0, conc, max_steps, cap, st.height_unit_m)
+    acc = np.zeros_like(w["height"])
+    pending = np.zeros_like(w["height"])
+    dtr = np.zeros_like(w["height"])
+    mtr = np.zeros_like(w["momentum"])
+    samp_after = samp.copy()
+    cu = lambda k: float(getattr(ep, k)) / st.height_unit_m
+    z = np.zeros((1, NE, NE))
+    ap = pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                          w["height"], w["sediment"], acc, pending, samp_after, dtr, mtr, mask, cu("iter_erode"), cu("iter_deposit"),
+                          float(ep.fan_slope), False, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                          z.copy(), np.zeros((1, NE, NE), np.int32), np.zeros(1))
+    np.savez_compressed(
+        HERE / "window_trace.npz", N=N, H=H, face=fw, **w, mask=mask, sp_face=f, sp_x=x, sp_y=y, sp_sed=sed, sp_dir=dirs,
+        volume0=volume0, conc_scale=conc, cap=cap, max_steps=max_steps, deposit_on_exit=True,
+        params=json.dumps({k: getattr(ep, k) for k in ep.__dataclass_fields__}), cell_size_m=st.height_unit_m, **res, acc=acc,
+        pending=pending, disch_track=dtr, mom_track=mtr, apply_out=np.array([float(a) for a in ap]))
+    print(f"window_trace: face {fw}, {x.size} droplets, entries {int(res['cl_count'].sum())}, deaths "
+          f"{np.bincount(res['sp_death'], minlength=6)}, clamped {ap[0]}")
+
+
 def gen_step(cs, maps, pk, WorldParams):
     from pgerosion import synth
 
@@ -237,13 +319,15 @@ def gen_step(cs, maps, pk, WorldParams):
     print("step_tiny:", stats[-1])
 
 
-def main(bake: str):
+def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
-    gen_vectors(cs)
-    gen_halo(cs)
-    gen_trace(cs, maps, pk, WorldParams)
-    gen_step(cs, maps, pk, WorldParams)
+    gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
+            "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
+            "step": lambda: gen_step(cs, maps, pk, WorldParams)}
+    for name, g in gens.items():
+        if only is None or name == only:
+            g()
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/bake")
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/bake", sys.argv[2] if len(sys.argv) > 2 else None)

@@ -25,7 +25,7 @@ import torch
 from oracle import oracle as orc
 from pgerosion import _lib
 from pgerosion import maps as gm
-from tests.parity_cases import changelist_rows, hypsometry, isolated_case, step_case
+from tests.parity_cases import changelist_rows, hypsometry, isolated_case, step_case, window_case
 
 pytestmark = pytest.mark.gpu
 
@@ -217,15 +217,9 @@ def _pass_inputs(c, it=0):
     return st, f, x, y, v0
 
 
-def test_ordered_apply_pass_matches_oracle(cuda):
-    """One particle pass with identical spawns: the ordered apply reproduces
-    the reference's serial apply cell by cell (float64 in the reference's
-    operation order).  The trace's tan / atan at face crossings come from
-    CUDA's libm instead of glibc's (both within 2 ulp), so a handful of
-    cells may differ in the last digits: at least 99 % of the heights are
-    bit-identical and every field is within 1e-5 relative (the stated
-    trajectory tolerance)."""
-    c = step_case()
+def _ordered_pass_vs_oracle(c, ecap_on=False):
+    """One ordered pass on the GPU and the oracle's chunked serial pass on
+    the same spawns and start terrain; asserts parity."""
     o, f, x, y, v0 = _pass_inputs(c)
     g = gm.ErosionState.from_world(c["world"])
     # the same start: the replayed heights of the oracle (the replay's uplift mean is a reduction
@@ -242,10 +236,18 @@ def test_ordered_apply_pass_matches_oracle(cuda):
     tp = orc.trace_params(o, ep, v0, chunk / (v0 * P))
     ap = orc.apply_params(o, ep, ep.iter_deposit / o.height_unit_m)
     cap = orc.change_list_cap(tp.max_steps)
+    ecap = None
+    if ecap_on:
+        import ctypes as _ct
+
+        ecap = np.empty_like(o.height)
+        orc.lib().orc_slope_erode_cap(_ct.c_int(o.F), _ct.c_int(o.NE), orc._p(o.height), orc._p(o.sediment), orc._p(o.mask),
+                                      _ct.c_double(float(ep.slope_limit_erode)), _ct.c_double(float(ep.slope_limit_exit)),
+                                      orc._p(ecap))
     clamped = 0
     for c0 in range(0, P, chunk):
         cl = orc.trace(o, tp, f[c0:c0 + chunk], x[c0:c0 + chunk], y[c0:c0 + chunk], z[c0:c0 + chunk], z[c0:c0 + chunk], v0)
-        clamped += orc.apply(o, ap, cl, cap)[0]
+        clamped += orc.apply(o, ap, cl, cap, ecap)[0]
     import ctypes
     lib = orc.lib()
     lib.orc_fold(ctypes.c_int64(o.height.size), orc._p(o.height), orc._p(o.sediment), orc._p(o.acc), orc._p(o.mask))
@@ -258,3 +260,128 @@ def test_ordered_apply_pass_matches_oracle(cuda):
     assert same > 0.99, same
     # a few trajectories differ in their last bits (libm), which can flip a clamp decision
     assert abs(s["clamped"] - clamped) <= 1e-3 * clamped, (s["clamped"], clamped)
+
+
+def test_ordered_apply_pass_matches_oracle(cuda):
+    """One particle pass with identical spawns: the ordered apply reproduces
+    the reference's serial apply cell by cell (float64 in the reference's
+    operation order).  The trace's tan / atan at face crossings come from
+    CUDA's libm instead of glibc's (both within 2 ulp), so a handful of
+    cells may differ in the last digits: at least 99 % of the heights are
+    bit-identical and every field is within 1e-5 relative (the stated
+    trajectory tolerance)."""
+    _ordered_pass_vs_oracle(step_case())
+
+
+def test_ordered_pass_with_slope_erode_cap_matches_oracle(cuda):
+    """The same pass with soillib's pit-free erosion cap on
+    (erosion.slope_limit_erode = 0.25, soillib's value; particle.py:1046-1076,
+    maps.py:922-927): the cap field is computed on the device from the
+    iteration's start terrain and limits every erosion entry of the ordered
+    apply, as in the reference; same tolerances."""
+    import dataclasses
+
+    c = step_case()
+    c["params"] = dataclasses.replace(c["params"], erosion=dataclasses.replace(c["params"].erosion, slope_limit_erode=0.25))
+    _ordered_pass_vs_oracle(c, ecap_on=True)
+
+
+def test_slope_erode_cap_field_matches_oracle(cuda):
+    """The cap field itself: bit-identical to the oracle's (float64, same
+    operation order, correctly rounded square root on both sides)."""
+    import ctypes
+
+    c = step_case()
+    g = gm.ErosionState.from_world(c["world"])
+    o = orc.OracleState.from_world(c["world"], c["params"])
+    # a rough surface: the seeded world's heights plus noise, and a sediment layer
+    rng = np.random.default_rng(5)
+    h = np.ascontiguousarray(o.height + rng.normal(0.0, 0.3, o.height.shape))
+    sd = np.ascontiguousarray(np.abs(rng.normal(0.0, 0.1, o.height.shape)))
+    g.height.copy_(torch.as_tensor(h))
+    g.sediment.copy_(torch.as_tensor(sd))
+    out = torch.empty_like(g.height)
+    L = _lib.load()
+    _lib.check(L.pge_slope_erode_cap(ctypes.byref(g.pge_grid()), ctypes.byref(g.pge_state()), 0.25, 0.02, gm._ptr(out),
+                                     gm._stream()), "pge_slope_erode_cap")
+    want = np.empty_like(h)
+    orc.lib().orc_slope_erode_cap(ctypes.c_int(o.F), ctypes.c_int(o.NE), orc._p(h), orc._p(sd), orc._p(o.mask), ctypes.c_double(0.25),
+                                  ctypes.c_double(0.02), orc._p(want))
+    got = out.cpu().numpy()
+    assert got.tobytes() == want.tobytes()
+    assert (got > 0).mean() > 0.3  # the surface is rough: most cells have a downhill side
+
+
+def _gpu_window_state(case):
+    """The window of ``window_case`` as a device state (F = 1, spherical=False)."""
+    dev = torch.device("cuda")
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    NE = case["N"] + 2 * case["H"]
+    return gm.ErosionState(height=f64(case["height"]), sediment=f64(case["sediment"]), discharge=f64(case["discharge"]),
+                           momentum=f64(case["momentum"]), hardness=f32(case["hardness"]), precip=f32(np.ones((1, NE, NE))),
+                           evap=f32(case["evap"]), uplift=f64(np.zeros((1, NE, NE))),
+                           mask=torch.as_tensor(np.ascontiguousarray(case["mask"], np.uint8), device=dev),
+                           metric=f32(case["metric"][0]), metric_inv=f32(case["metric_inv"][0]), N=case["N"], H=case["H"],
+                           spherical=False, height_unit_m=case["cell_size_m"], base=f64(case["base"]),
+                           deposit_on_exit=bool(case["deposit_on_exit"]))
+
+
+def test_window_change_lists_match_reference(cuda):
+    """Window mode (spherical=False, F = 1, outside / frozen / active masks,
+    deposit_on_exit; the reference's fixture): every droplet's change list
+    -- cells and death causes identical, deltas / volumes / momenta within
+    1e-5 relative, the trajectory tolerance."""
+    case = window_case()
+    st = _gpu_window_state(case)
+    res = gm.trace_changelist(st, case["params"], case["sp_face"], case["sp_x"], case["sp_y"], case["sp_sed"], case["sp_dir"],
+                              case["volume0"], case["conc_scale"], precision=_lib.PREC_F64)
+    cap = case["cap"]
+    assert np.array_equal(res["sp_death"], case["sp_death"])
+    assert np.array_equal(res["cl_count"], case["cl_count"])
+    for p, (a, b) in enumerate(zip(changelist_rows(res, cap), changelist_rows(case, cap))):
+        assert np.array_equal(a[0], b[0]), f"droplet {p}: cell path differs"
+        np.testing.assert_allclose(a[1], b[1], rtol=1e-5, atol=1e-12, err_msg=f"droplet {p} delta")
+        np.testing.assert_allclose(a[2], b[2], rtol=1e-5, atol=0, err_msg=f"droplet {p} volume")
+        np.testing.assert_allclose(a[3], b[3], rtol=1e-5, atol=1e-7, err_msg=f"droplet {p} momentum")
+
+
+def test_window_ordered_pass_matches_oracle(cuda):
+    """The window's droplets (sharing cells) through the ordered apply in the
+    reference's chunks against the oracle's chunked serial pass (trace,
+    apply, fold, EMA) on the same inputs: every field within 1e-5 relative
+    and >= 99 % of heights bit-identical, as for the sphere."""
+    import ctypes
+
+    case = window_case()
+    ep = case["params"]
+    g = _gpu_window_state(case)
+    f, x, y, sed, dirs, v0 = case["sp_face"], case["sp_x"], case["sp_y"], case["sp_sed"], case["sp_dir"], case["volume0"]
+    P = len(f)
+    s = gm.apply_spawns(g, ep, f, x, y, sed, dirs, v0)
+    o = orc.OracleState(height=case["height"].copy(), sediment=case["sediment"].copy(), discharge=case["discharge"].copy(),
+                        momentum=case["momentum"].copy(), hardness=case["hardness"], precip=np.ones_like(case["hardness"]),
+                        evap=case["evap"], uplift=np.zeros_like(case["height"]), mask=case["mask"], metric=case["metric"],
+                        metric_inv=case["metric_inv"], N=case["N"], H=case["H"], spherical=False,
+                        height_unit_m=case["cell_size_m"], base=case["base"].copy(), deposit_on_exit=bool(case["deposit_on_exit"]))
+    chunk = orc.chunk_size(ep, P)
+    o.pack()
+    o.acc[...] = 0.0
+    tp = orc.trace_params(o, ep, v0, chunk / (v0 * P))
+    ap = orc.apply_params(o, ep, ep.iter_deposit / o.height_unit_m)
+    cap = orc.change_list_cap(tp.max_steps)
+    clamped = 0
+    for c0 in range(0, P, chunk):
+        sl = slice(c0, c0 + chunk)
+        cl = orc.trace(o, tp, f[sl], x[sl], y[sl], sed[sl], dirs[sl], v0)
+        clamped += orc.apply(o, ap, cl, cap)[0]
+    lib = orc.lib()
+    lib.orc_fold(ctypes.c_int64(o.height.size), orc._p(o.height), orc._p(o.sediment), orc._p(o.acc), orc._p(o.mask))
+    lib.orc_ema(ctypes.c_int64(o.height.size), orc._p(o.discharge), orc._p(o.momentum), orc._p(o.disch_track), orc._p(o.mom_track),
+                orc._p(o.mask), ctypes.c_double(float(ep.ema)))
+    a = g.to_numpy()
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        np.testing.assert_allclose(a[k], getattr(o, k), rtol=1e-5, atol=1e-8, err_msg=k)
+    assert np.mean(a["height"] == o.height) > 0.99
+    assert abs(s["clamped"] - clamped) <= 1e-3 * clamped, (s["clamped"], clamped)
+

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as orc
-from tests.parity_cases import GOLDEN, changelist_rows, isolated_case, step_case
+from tests.parity_cases import GOLDEN, changelist_rows, isolated_case, step_case, window_case
 
 
 def test_cubesphere_vectors_bit_exact():
@@ -48,6 +48,24 @@ def test_trace_and_apply_match_reference_bit_exact():
     cap = case["cap"]
     for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
         assert np.array_equal(res[k], case[k]), k
+    for a, b in zip(changelist_rows(res, cap), changelist_rows(case, cap)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    for k in ("acc", "pending", "disch_track", "mom_track"):
+        assert np.array_equal(res[k], case[k]), k
+    assert np.array_equal(res["apply_out"], case["apply_out"])
+
+
+def test_window_trace_and_serial_apply_match_reference_bit_exact():
+    """Window mode (spherical=False, F = 1, outside / frozen / active masks,
+    deposit_on_exit) with droplets sharing cells: the oracle's trace and
+    serial apply equal the reference's bit for bit."""
+    case = window_case()
+    res = case["oracle"]()
+    cap = case["cap"]
+    for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
+        assert np.array_equal(res[k], case[k]), k
+    assert (case["sp_death"] == orc.DEATH_NAMES.index("exit")).sum() > 10  # droplets do leave the window
     for a, b in zip(changelist_rows(res, cap), changelist_rows(case, cap)):
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
