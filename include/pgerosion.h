@@ -18,6 +18,9 @@
  *   pge_slope_erode_cap   slope_erode_cap (erosion.slope_limit_erode > 0)
  *                                                  globe/erosion/particle.py:1046-1076,
  *                                                  globe/erosion/maps.py:922-927
+ *   pge_smooth_step       one step of apply_isostasy's flexural smoother
+ *                         (FaceField.laplacian)    globe/erosion/maps.py:1331-1410,
+ *                                                  globe/field.py:179-188, 372-404
  *   pge_thermal           thermal_erosion (talus pass + creep pass)
  *                                                  globe/erosion/maps.py:1050-1085,
  *                                                  globe/erosion/particle.py:1107-1227
@@ -237,6 +240,14 @@ PGE_API int pge_read_accumulators(const PgeGrid *g, double *acc, double *disch_t
  * exit_slope = erosion.slope_limit_exit). */
 PGE_API int pge_slope_erode_cap(const PgeGrid *g, const PgeState *s, double coef, double exit_slope, double *erode_cap,
                                 void *stream);
+
+/* One explicit step of the isostasy smoother on the sphere: the metric-aware Laplace-Beltrami
+ * operator of in (F,NE,NE) in flux form at extended indices 1..NE-2 (0 on the outer ring; halos
+ * exchanged first, with the linear tables), per m^2 and rounded to float32, then
+ * out = (keep ? in : 0) + (kappa * lap) * cell_m^2.  metric_inv is the (NE,NE,3) inverse metric,
+ * sqrt_det the (NE,NE) float32 sqrt(det g) of the metric, both shared by the faces.  in != out. */
+PGE_API int pge_smooth_step(const PgeGrid *g, const float *metric_inv, const float *sqrt_det, const double *in, double *out,
+                            double kappa, int32_t keep, double cell_m, void *stream);
 
 /* Talus pass, then (creep_rate > 0) the creep pass with submerged cells frozen. */
 PGE_API int pge_thermal(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max,

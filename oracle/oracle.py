@@ -13,7 +13,9 @@ this module; the product never does.  It drives the C restatement in
 * :func:`apply_uplift` -- maps.py:1088-1147 (mean-free over the active interior)
 * :func:`start_replay` -- maps.py:1159-1213
 * :func:`hold_datum` -- maps.py:1446-1508
-* :func:`step` -- maps.py:1516-1617, plain path
+* :func:`apply_isostasy` -- maps.py:1331-1410 (the Laplace-Beltrami smoother
+  of field.py:179-188, 372-404 restated in numpy)
+* :func:`step` -- maps.py:1516-1617, plain path (plus isostasy)
 
 Every random number comes from ``params.rng("erosion", iteration)`` exactly
 as in the reference, so a GPU run and this oracle see the same spawns.
@@ -160,6 +162,7 @@ class OracleState:
     acc: np.ndarray = field(default=None, repr=False)
     disch_track: np.ndarray = field(default=None, repr=False)
     mom_track: np.ndarray = field(default=None, repr=False)
+    iso_acc: np.ndarray = field(default=None, repr=False)
 
     def __post_init__(self):
         F, NE = self.height.shape[0], self.height.shape[1]
@@ -506,10 +509,120 @@ def hold_datum(state, land_fraction, level=0.0):
     return q
 
 
+def laplacian(state, d):
+    """FaceField.laplacian (field.py:179-188, 372-404): the flux-form
+    Laplace-Beltrami operator at extended indices 1..NE-2 (0 on the outer
+    ring), per m^2, as the float32 field the reference returns."""
+    from pgerosion.isostasy import sqrt_det_metric
+
+    grid = state.grid
+    gi = grid.metric_inv_face.astype(np.float64)[None]
+    sq = sqrt_det_metric(grid).astype(np.float64)[None]
+    C = slice(1, -1)
+    P = slice(2, None)
+    M = slice(None, -2)
+    fj_c = 0.5 * (d[:, C, P] - d[:, C, M])
+    fj_p = 0.5 * (d[:, P, P] - d[:, P, M])
+    fj_m = 0.5 * (d[:, M, P] - d[:, M, M])
+    fi_c = 0.5 * (d[:, P, C] - d[:, M, C])
+    fi_p = 0.5 * (d[:, P, P] - d[:, M, P])
+    fi_m = 0.5 * (d[:, P, M] - d[:, M, M])
+    gii = 0.5 * (gi[:, C, C, 0] + gi[:, P, C, 0])
+    gij = 0.5 * (gi[:, C, C, 1] + gi[:, P, C, 1])
+    sv = 0.5 * (sq[:, C, C] + sq[:, P, C])
+    Fi_p = sv * (gii * (d[:, P, C] - d[:, C, C]) + gij * 0.5 * (fj_c + fj_p))
+    gii = 0.5 * (gi[:, C, C, 0] + gi[:, M, C, 0])
+    gij = 0.5 * (gi[:, C, C, 1] + gi[:, M, C, 1])
+    sv = 0.5 * (sq[:, C, C] + sq[:, M, C])
+    Fi_m = sv * (gii * (d[:, C, C] - d[:, M, C]) + gij * 0.5 * (fj_c + fj_m))
+    gjj = 0.5 * (gi[:, C, C, 2] + gi[:, C, P, 2])
+    gij = 0.5 * (gi[:, C, C, 1] + gi[:, C, P, 1])
+    sv = 0.5 * (sq[:, C, C] + sq[:, C, P])
+    Fj_p = sv * (gjj * (d[:, C, P] - d[:, C, C]) + gij * 0.5 * (fi_c + fi_p))
+    gjj = 0.5 * (gi[:, C, C, 2] + gi[:, C, M, 2])
+    gij = 0.5 * (gi[:, C, C, 1] + gi[:, C, M, 1])
+    sv = 0.5 * (sq[:, C, C] + sq[:, C, M])
+    Fj_m = sv * (gjj * (d[:, C, C] - d[:, C, M]) + gij * 0.5 * (fi_c + fi_m))
+    out = np.zeros_like(d)
+    out[:, C, C] = (Fi_p - Fi_m + Fj_p - Fj_m) / sq[:, C, C]
+    out /= grid.cell_size_m ** 2
+    return out.astype(np.float32)
+
+
+_KAPPA_CACHE: dict = {}
+
+
+def smoothing_kappa(state) -> float:
+    """maps._smoothing_kappa (maps.py:1331-1363): 0.9 / lambda_max by 40 steps
+    of power iteration from default_rng(0) noise; cached per grid."""
+    from pgerosion.geometry import exchange_halos as xh
+
+    grid = state.grid
+    key = (grid.N, grid.H, float(grid.cell_size_m))
+    if key not in _KAPPA_CACHE:
+        rng = np.random.default_rng(0)
+        H, N, NE = grid.H, grid.N, grid.NE
+        f = np.zeros((6, NE, NE))
+        f[:, H:H + N, H:H + N] = rng.standard_normal((6, N, N))
+        xh(grid, f)
+        c2, lam = float(grid.cell_size_m) ** 2, 8.0
+        for _ in range(40):
+            xh(grid, f, linear=True)
+            Lv = laplacian(state, f).astype(np.float64) * c2
+            num = float(np.sqrt((Lv[:, H:-H, H:-H] ** 2).sum()))
+            den = float(np.sqrt((f[:, H:-H, H:-H] ** 2).sum()))
+            if num <= 0.0 or den <= 0.0:
+                break
+            lam = num / den
+            f = Lv / num
+        _KAPPA_CACHE[key] = 0.9 / max(lam, 1e-6)
+    return _KAPPA_CACHE[key]
+
+
+def apply_isostasy(state, params) -> dict:
+    """maps.apply_isostasy (maps.py:1366-1410): -isostasy x iso_acc, spread by
+    ceil(sigma^2 / (2 kappa)) explicit Laplace-Beltrami steps (linear halos
+    before each), added mean-free over the active interior; zeroes iso_acc."""
+    from pgerosion.geometry import exchange_halos as xh
+
+    ep = _ep(params)
+    d = state.iso_acc
+    k = float(ep.isostasy)
+    load = (-k * d).astype(np.float64)
+    cell = float(state.height_unit_m)
+    sig = float(ep.flexure_km) * 1000.0 / cell
+    sig = min(sig, state.N / 8.0)
+    kappa = smoothing_kappa(state)
+    n = int(np.ceil(sig * sig / (2.0 * kappa))) if sig >= 0.5 else 0
+    f = load.copy()
+    for _ in range(n):
+        xh(state.grid, f, linear=True)
+        f += kappa * laplacian(state, f).astype(np.float64) * (cell * cell)
+    xh(state.grid, f, linear=True)
+    act = state.mask == MASK_ACTIVE
+    iact = state.mask[state.interior] == MASK_ACTIVE
+    mean = float(f[state.interior][iact].mean()) if iact.any() else 0.0
+    state.height[act] += (f[act] - mean)
+    moved = float(np.abs(d[state.interior]).sum())
+    state.iso_acc[...] = 0.0
+    return {"sigma_cells": sig, "diffusion_steps": n, "kappa": kappa, "load_abs_cells": moved,
+            "rebound_max": float((f[state.interior] - mean).max()), "rebound_min": float((f[state.interior] - mean).min())}
+
+
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
+    ep = _ep(params)
+    iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
+    if iso:
+        if getattr(state, "iso_acc", None) is None:
+            state.iso_acc = np.zeros_like(state.height)
+        s0 = state.height + state.sediment
     st = run_iteration(state, params, iteration_key, n_particles=n_particles, chunk=chunk)
     thermal_erosion(state, params)
+    if iso:
+        state.iso_acc += (state.height + state.sediment) - s0
     apply_uplift(state, None)
+    if iso and (state.iteration + 1) % max(int(getattr(ep, "isostasy_every", 10)), 1) == 0:
+        st["isostasy"] = apply_isostasy(state, params)
     if state.spherical:
         st["datum_shift"] = hold_datum(state, state.land_target)
     state.exchange_halos()

@@ -503,6 +503,20 @@ PGE_API int pge_slope_erode_cap(const PgeGrid *g, const PgeState *s, double coef
     return e == cudaSuccess ? PGE_OK : cuda_fail(e, "slope erode cap");
 }
 
+PGE_API int pge_smooth_step(const PgeGrid *g, const float *metric_inv, const float *sqrt_det, const double *in, double *out,
+                            double kappa, int32_t keep, double cell_m, void *stream)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (!g->spherical) return fail(PGE_E_UNSUPPORTED, "the isostasy smoother runs on the sphere only");
+    if (!metric_inv || !sqrt_det || !in || !out) return fail(PGE_E_ARG, "smooth_step: NULL array");
+    if (in == out) return fail(PGE_E_ARG, "smooth_step: in and out must differ (every cell reads its neighbours' old values)");
+    if (!(cell_m > 0.0)) return fail(PGE_E_ARG, "smooth_step: cell size must be positive");
+    smooth_step(*g, in, metric_inv, sqrt_det, kappa, keep ? 1 : 0, cell_m, out, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "smooth step");
+}
+
 PGE_API int pge_uplift(const PgeGrid *g, PgeState *s, double cap, double scale, void *ws, size_t ws_bytes, void *stream)
 {
     int r;

@@ -781,4 +781,64 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
                                                                              out);
 }
 
+// ---------------------------------------------------------------------------
+// the isostasy smoother (maps.py:1331-1410): one explicit step of the metric-aware
+// Laplace-Beltrami diffusion, FaceField.laplacian (field.py:179-188, 372-404) in flux form,
+// (1/sqrt g) d_a(sqrt g g^ab d_b f), at extended indices 1..NE-2 of every face (0 on the outer
+// ring), per m^2 and rounded to float32 as the reference's field is; then
+//   out = a * in + (kappa * lap) * cell^2       (a = 1: a smoothing step; a = 0, kappa = 1: the
+//                                                  Laplacian in cell units, for the step bound)
+// float64 in the reference's operation order (no FMA in this file)
+// ---------------------------------------------------------------------------
+__global__ void smooth_step_kernel(int F, int NE, const double *__restrict__ d, const float *__restrict__ ginv_f,
+                                   const float *__restrict__ sq_f, double c2, double kappa, int keep, double *__restrict__ out)
+{
+    const long long n = (long long)F * NE * NE;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long r = c % ((long long)NE * NE);
+        const int i = (int)(r / NE), j = (int)(r - (long long)i * NE);
+        double lap64 = 0.0;
+        if (i >= 1 && i <= NE - 2 && j >= 1 && j <= NE - 2) {
+            // the metric tables are the same on every face: index them by (i, j)
+            auto G = [&](int ii, int jj, int k) { return (double)ginv_f[((long long)ii * NE + jj) * 3 + k]; };
+            auto S = [&](int ii, int jj) { return (double)sq_f[(long long)ii * NE + jj]; };
+            auto D = [&](int ii, int jj) { return d[c + (long long)(ii - i) * NE + (jj - j)]; };
+            const double fj_c = 0.5 * (D(i, j + 1) - D(i, j - 1));
+            const double fj_p = 0.5 * (D(i + 1, j + 1) - D(i + 1, j - 1));
+            const double fj_m = 0.5 * (D(i - 1, j + 1) - D(i - 1, j - 1));
+            const double fi_c = 0.5 * (D(i + 1, j) - D(i - 1, j));
+            const double fi_p = 0.5 * (D(i + 1, j + 1) - D(i - 1, j + 1));
+            const double fi_m = 0.5 * (D(i + 1, j - 1) - D(i - 1, j - 1));
+            double gii = 0.5 * (G(i, j, 0) + G(i + 1, j, 0));
+            double gij = 0.5 * (G(i, j, 1) + G(i + 1, j, 1));
+            double sv = 0.5 * (S(i, j) + S(i + 1, j));
+            const double Fi_p = sv * (gii * (D(i + 1, j) - D(i, j)) + gij * 0.5 * (fj_c + fj_p));
+            gii = 0.5 * (G(i, j, 0) + G(i - 1, j, 0));
+            gij = 0.5 * (G(i, j, 1) + G(i - 1, j, 1));
+            sv = 0.5 * (S(i, j) + S(i - 1, j));
+            const double Fi_m = sv * (gii * (D(i, j) - D(i - 1, j)) + gij * 0.5 * (fj_c + fj_m));
+            double gjj = 0.5 * (G(i, j, 2) + G(i, j + 1, 2));
+            gij = 0.5 * (G(i, j, 1) + G(i, j + 1, 1));
+            sv = 0.5 * (S(i, j) + S(i, j + 1));
+            const double Fj_p = sv * (gjj * (D(i, j + 1) - D(i, j)) + gij * 0.5 * (fi_c + fi_p));
+            gjj = 0.5 * (G(i, j, 2) + G(i, j - 1, 2));
+            gij = 0.5 * (G(i, j, 1) + G(i, j - 1, 1));
+            sv = 0.5 * (S(i, j) + S(i, j - 1));
+            const double Fj_m = sv * (gjj * (D(i, j) - D(i, j - 1)) + gij * 0.5 * (fi_c + fi_m));
+            const double lap = (Fi_p - Fi_m + Fj_p - Fj_m) / S(i, j);
+            lap64 = (double)(float)(lap / c2);  // per m^2, a float32 field
+        }
+        const double upd = kappa * lap64 * c2;
+        out[c] = keep ? d[c] + upd : upd;
+    }
+}
+
+void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
+                 double cell_m, double *out, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    const double c2 = cell_m * cell_m;
+    smooth_step_kernel<<<grid_for((long long)g.F * NE * NE), 256, 0, st>>>(g.F, NE, in, metric_inv, sqrt_det, c2, kappa, keep, out);
+}
+
 }  // namespace pge

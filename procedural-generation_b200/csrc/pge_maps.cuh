@@ -16,6 +16,8 @@ void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, doub
                 double *shift_dev, cudaStream_t st);
 void halo_gather(const PgeHalo &h, double *field, int vector, cudaStream_t st);
 void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_slope, double *out, cudaStream_t st);
+void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
+                 double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
 cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
                        long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st);

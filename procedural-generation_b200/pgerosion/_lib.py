@@ -26,6 +26,7 @@ EXPORTS = (
     "pge_version", "pge_last_error", "pge_workspace_bytes", "pge_spawn_rain", "pge_count_pending",
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
+    "pge_smooth_step",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -105,6 +106,7 @@ def load(path: str | os.PathLike | None = None):
                                        c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_read_accumulators.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_slope_erode_cap.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, c_vp]
+    L.pge_smooth_step.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_vp, c_f64, c_i32, c_f64, c_vp]
     L.pge_thermal.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_vp, ctypes.c_size_t, c_vp]
     L.pge_uplift.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, ctypes.c_size_t, c_vp]
     L.pge_hold_datum.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, c_vp, ctypes.c_size_t, c_vp]

@@ -82,6 +82,7 @@ class ErosionState:
     _ws: torch.Tensor = field(default=None, repr=False)
     _halo: tuple = field(default=None, repr=False)
     _erode_cap: torch.Tensor = field(default=None, repr=False)
+    iso_acc: torch.Tensor = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -202,13 +203,26 @@ class ErosionState:
     def workspace(self) -> torch.Tensor:
         return self._ws
 
-    def halo_tables(self):
+    def halo_tables(self, linear: bool = False):
+        """The grid's halo tables on the device (dst, src, weights, rotations):
+        cubic weights by default, the monotone linear ones with ``linear``."""
         if self._halo is None:
             hm = self.grid.halo
             d = self.height.device
             self._halo = (torch.as_tensor(hm.dst.astype(np.int32), device=d), torch.as_tensor(hm.src.astype(np.int32), device=d),
-                          torch.as_tensor(hm.w, device=d), torch.as_tensor(np.ascontiguousarray(hm.rot), device=d))
-        return self._halo
+                          torch.as_tensor(hm.w, device=d), torch.as_tensor(np.ascontiguousarray(hm.rot), device=d),
+                          torch.as_tensor(np.ascontiguousarray(hm.w_lin), device=d))
+        dst, src, w, rot, wl = self._halo
+        return dst, src, (wl if linear else w), rot
+
+    def exchange_field(self, field: torch.Tensor, vector: bool = False, linear: bool = False) -> None:
+        """Fill the halos of one (F, NE, NE[, 2]) float64 field from its interior
+        (FaceField.exchange_halos, field.py:104-125)."""
+        if not self.spherical:
+            return
+        dst, src, w, rot = self.halo_tables(linear)
+        h = PgeHalo(K=int(dst.shape[0]), dst=_ptr(dst), src=_ptr(src), w=_ptr(w), rot=_ptr(rot))
+        check(_lib.load().pge_halo_gather(ctypes.byref(h), _ptr(field), 1 if vector else 0, _stream()), "pge_halo_gather")
 
     def exchange_halos(self) -> None:
         """Refresh the halos of height, sediment, discharge and the rotated
@@ -460,13 +474,28 @@ def start_replay(state: ErosionState, params) -> dict | None:
 
 def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     """One plain iteration (maps.py:1516-1617): particles, thermal erosion,
-    uplift, datum hold, halo exchange; increments ``state.iteration``."""
+    uplift, isostasy (when ``erosion.isostasy > 0``: the surface change of
+    the particles and the mass wasting is the load, applied every
+    ``isostasy_every`` iterations, maps.py:1570-1603), datum hold, halo
+    exchange; increments ``state.iteration``."""
     ep = erosion_group(params)
     t0 = time.time()
+    iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
+    if iso:
+        if state.iso_acc is None:
+            state.iso_acc = torch.zeros_like(state.height)
+        s0 = state.height + state.sediment
     st = run_iteration(state, params, iteration_key, log=log, **kw)
     t1 = time.time()
     thermal_erosion(state, params)
+    if iso:
+        # only what surface processes moved: uplift and the datum shift are not loads
+        state.iso_acc += (state.height + state.sediment) - s0
     apply_uplift(state, uplift_cap(state, ep))
+    if iso and (state.iteration + 1) % max(int(getattr(ep, "isostasy_every", 10)), 1) == 0:
+        from .isostasy import apply_isostasy
+
+        st["isostasy"] = apply_isostasy(state, params)
     if state.spherical and hasattr(params, "world"):
         st["datum_shift"] = hold_datum(state, held_land_fraction(state, params))
     state.exchange_halos()

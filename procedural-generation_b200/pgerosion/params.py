@@ -190,7 +190,8 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (routing surface, lakes, glacial pass, isostasy, ice, lateral cut)."""
+    path (routing surface, lakes, glacial pass, ice, lateral cut).  Isostasy
+    is supported (on the sphere)."""
     bad = []
     if int(getattr(ep, "flood_every", 0)) > 0:
         bad.append("flood_every")
@@ -200,8 +201,6 @@ def check_plain(ep) -> None:
         bad.append("lake_balance")
     if int(getattr(ep, "glacial_every", 0)) > 0:
         bad.append("glacial_every")
-    if float(getattr(ep, "isostasy", 0.0)) > 0.0:
-        bad.append("isostasy")
     if float(getattr(ep, "lateral_rate", 0.0)) > 0.0:
         bad.append("lateral_rate")
     if bool(getattr(ep, "ice_sheet", False)):

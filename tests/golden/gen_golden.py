@@ -22,6 +22,10 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
   margin inside an outside ring; ``deposit_on_exit``), loaded and unloaded
   droplets sharing cells, the reference ``trace_particles`` change lists
   and the serial ``apply_changes`` results for all of them.
+* ``isostasy_tiny.npz`` -- the same kind of N=32 world run through the
+  reference ``maps.step`` with isostasy on (0.8, every 2 iterations): the
+  smoother's step bound and every iteration's isostasy statistics, and the
+  final state.
 * ``step_tiny.npz`` -- a six-face N=32 world run through the reference
   ``maps.step`` (plain knobs, uplift replay) for a few iterations: the
   initial state, the final state and the per-iteration stats.
@@ -319,10 +323,34 @@ def gen_step(cs, maps, pk, WorldParams):
     print("step_tiny:", stats[-1])
 
 
+def gen_isostasy(cs, maps, pk, WorldParams):
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=9, N=32, H=2, cell_size_m=50.0, land_fraction=0.3)
+    iters = 4
+    p = _world_params(WorldParams, 32, 2, 50.0, 9, 0.3, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", isostasy=0.8, isostasy_every=2)
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st, p)
+    stats = []
+    for it in range(iters):
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "datum_shift")})
+        if "isostasy" in s:
+            stats[-1]["isostasy"] = s["isostasy"]
+    np.savez_compressed(HERE / "isostasy_tiny.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.3, seed=9, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        kappa=maps._smoothing_kappa(st.grid), height=st.height, sediment=st.sediment, discharge=st.discharge,
+                        momentum=st.momentum, pending=st.pending, stats=json.dumps(stats), **init)
+    print("isostasy_tiny:", [x.get("isostasy") for x in stats])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
             "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
+            "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:

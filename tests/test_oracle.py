@@ -105,3 +105,25 @@ def test_oracle_conserves_mass_in_a_particle_pass():
         orc.apply_uplift(st)
         orc.hold_datum(st, st.land_target)
         st.exchange_halos()
+
+
+def test_isostasy_steps_match_reference_bit_exact():
+    """Four reference steps with isostasy on (0.8, every 2 iterations): the
+    oracle's step bound, its isostasy statistics and the final state are
+    the reference's, bit for bit."""
+    c = step_case(GOLDEN / "isostasy_tiny.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(st, c["params"])
+    assert orc.smoothing_kappa(st) == float(t["kappa"])
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        assert s["entries"] == r["entries"] and s["clamped"] == r["clamped"], it
+        assert ("isostasy" in s) == ("isostasy" in r), it
+        if "isostasy" in r:
+            for k, v in r["isostasy"].items():
+                assert s["isostasy"][k] == v, (it, k)
+        assert s["datum_shift"] == r["datum_shift"], it
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        assert np.array_equal(getattr(st, k), t[k]), k
