@@ -263,23 +263,24 @@ def run_b200(args, rank, world_size, dist):
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
+    # the public API's host feeder: each iteration's spawn uniforms drawn on the host (one iteration
+    # ahead, into pinned memory) and copied to the device inside the step
+    feeder = gm.SpawnFeeder(params, P, device=dev)
+    feeder.prefetch((n_total,))
     e0 = time.perf_counter()
     ee = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     ee[0].record()
     for k in range(args.steps):
         it = n_total + k
-        rng, u, off = gm.draw_spawns(params, "erosion", (it,), P)
-        u_p = torch.from_numpy(u).pin_memory()
-        off_p = torch.from_numpy(off).pin_memory()
-        u_d = u_p.to(dev, non_blocking=True)
-        off_d = off_p.to(dev, non_blocking=True)
+        rng, u_d, off_d, nbytes = feeder.get((it,))
         s = gm.step(st, params, it, predrawn=(rng, u_d, off_d), **kw)
-        h2d += u_p.numel() * 8 + off_p.numel() * 8 + 8 * _n_pending(s)
+        h2d += nbytes + 8 * _n_pending(s)
         d2h += (_lib.STATS_WORDS + 4 + 4) * 8
         e2e_steps += s["droplet_steps"]
     ee[1].record()
     torch.cuda.synchronize()
     e2e_ms = ee[0].elapsed_time(ee[1])
+    feeder.close()
     (steps_all, e2e_all), (ms_max, e2e_ms_max) = reduce_totals(dist, [steps_done, e2e_steps], [ms, e2e_ms], device=dev)
     alt = None
     if apply == _lib.APPLY_ORDERED and not args.no_alt:

@@ -280,6 +280,71 @@ def draw_spawns(params, rng_stage: str, key, P: int):
     return rng, u, off
 
 
+class SpawnFeeder:
+    """The host-drawn spawn uniforms of successive iterations, ready before
+    they are needed: while the device runs iteration ``k``, a background
+    thread draws iteration ``k + 1``'s ``P`` uniforms and ``(P, 2)`` offsets
+    (``draw_spawns``, the reference's order) into pinned host memory; ``get``
+    copies them to the device on the current stream and returns what
+    ``run_iteration(predrawn=...)`` takes.  Two pinned buffers alternate; a
+    buffer is refilled only after its last copy to the device has finished."""
+
+    def __init__(self, params, P: int, rng_stage: str = "erosion", device="cuda"):
+        from concurrent.futures import ThreadPoolExecutor
+
+        self.params, self.P, self.stage = params, int(P), rng_stage
+        self._pin = [(torch.empty(self.P, dtype=torch.float64).pin_memory(),
+                      torch.empty((self.P, 2), dtype=torch.float64).pin_memory()) for _ in range(2)]
+        self._copied = [None, None]
+        d = torch.device(device)
+        self._dev = [(torch.empty(self.P, dtype=torch.float64, device=d), torch.empty((self.P, 2), dtype=torch.float64, device=d))
+                     for _ in range(2)]
+        self._ex = ThreadPoolExecutor(max_workers=1)
+        self._fut = {}
+        self._slot = 0
+
+    @staticmethod
+    def _key(key):
+        return tuple(key) if isinstance(key, (tuple, list)) else (int(key),)
+
+    def _draw(self, key, slot):
+        ev = self._copied[slot]
+        if ev is not None:
+            ev.synchronize()  # the buffer's previous copy to the device is done
+        u, off = self._pin[slot]
+        rng = self.params.rng(self.stage, *key)
+        rng.random(out=u.numpy())
+        rng.random(out=off.numpy())
+        return rng
+
+    def prefetch(self, key) -> None:
+        key = self._key(key)
+        if key not in self._fut:
+            self._fut[key] = (self._ex.submit(self._draw, key, self._slot), self._slot)
+            self._slot ^= 1
+
+    def get(self, key):
+        """``(rng, u, off)`` of iteration ``key`` with ``u`` and ``off`` on the
+        device; starts drawing the next iteration.  Returns the bytes copied
+        to the device as a fourth item."""
+        key = self._key(key)
+        self.prefetch(key)
+        fut, slot = self._fut.pop(key)
+        rng = fut.result()
+        u_p, off_p = self._pin[slot]
+        u_d, off_d = self._dev[slot]
+        u_d.copy_(u_p, non_blocking=True)
+        off_d.copy_(off_p, non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record()
+        self._copied[slot] = ev
+        self.prefetch(key[:-1] + (key[-1] + 1,))
+        return rng, u_d, off_d, u_p.numel() * 8 + off_p.numel() * 8
+
+    def close(self) -> None:
+        self._ex.shutdown(wait=True)
+
+
 def run_iteration(state: ErosionState, params, iteration_key, n_particles: int | None = None,
                   particles_per_cell: float | None = None, rng_stage: str = "erosion", log=None, wave: int | None = None,
                   precision: int = _lib.PREC_F64, predrawn=None, threads_per_block: int = 0, blocks_per_sm: int = 0,

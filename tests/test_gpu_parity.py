@@ -385,3 +385,21 @@ def test_window_ordered_pass_matches_oracle(cuda):
     assert np.mean(a["height"] == o.height) > 0.99
     assert abs(s["clamped"] - clamped) <= 1e-3 * clamped, (s["clamped"], clamped)
 
+
+
+def test_spawn_feeder_gives_the_reference_draws(cuda):
+    """The prefetching host feeder hands over exactly draw_spawns' uniforms
+    (the reference's order), iteration after iteration, and the generator
+    in the state draw_spawns leaves it (for the stockpile directions)."""
+    c = step_case()
+    P = 5000
+    feeder = gm.SpawnFeeder(c["params"], P)
+    try:
+        for it in (3, 4, 5, 7):
+            rng, u, off, nbytes = feeder.get((it,))
+            r2, u2, off2 = gm.draw_spawns(c["params"], "erosion", (it,), P)
+            assert nbytes == 24 * P
+            assert np.array_equal(u.cpu().numpy(), u2) and np.array_equal(off.cpu().numpy(), off2)
+            assert rng.random() == r2.random()
+    finally:
+        feeder.close()
