@@ -90,24 +90,105 @@ def ckpt_hash(params, apply: int) -> str:
     return hashlib.sha256(s.encode()).hexdigest()[:16] + f":b200v{BACKEND_VERSION}:apply{apply}"
 
 
-def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
-    d = Path(store.checkpoint_dir)
-    d.mkdir(parents=True, exist_ok=True)
-    it = state.iteration
+#: the evolving arrays a checkpoint holds (run.py:100-139); iso_acc only while isostasy is on
+CKPT_FIELDS = ("height", "sediment", "discharge", "momentum", "pending")
+
+
+def _write_checkpoint(d: Path, it: int, arrays: dict, meta: dict) -> Path:
+    """npz to ``.tmp``, renamed, then the ``.json`` (a crash in between leaves
+    the previous checkpoint for :func:`find_checkpoint`), then pruning."""
     p = d / f"erosion_iter{it:04d}.npz"
     tmp = p.with_suffix(".npz.tmp")
-    a = state.to_numpy()
-    arrays = dict(height=a["height"], sediment=a["sediment"], discharge=a["discharge"], momentum=a["momentum"],
-                  pending=a["pending"], lake_load=np.zeros_like(a["height"]))
     with open(tmp, "wb") as fh:
         np.savez(fh, **arrays)
     tmp.replace(p)
-    meta = {"iteration": it, "params_hash": ckpt_hash(params, apply), "height_unit_m": state.height_unit_m,
-            "time": time.strftime("%Y-%m-%dT%H:%M:%S")}
     with open(p.with_suffix(".json"), "w") as fh:
         json.dump(meta, fh, indent=1)
     prune_checkpoints(d, meta["params_hash"], keep=2)
     return p
+
+
+def _ckpt_meta(state, params, apply) -> dict:
+    return {"iteration": state.iteration, "params_hash": ckpt_hash(params, apply), "height_unit_m": state.height_unit_m,
+            "time": time.strftime("%Y-%m-%dT%H:%M:%S")}
+
+
+def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
+    d = Path(store.checkpoint_dir)
+    d.mkdir(parents=True, exist_ok=True)
+    a = state.to_numpy()
+    arrays = {k: a[k] for k in CKPT_FIELDS}
+    arrays["lake_load"] = np.zeros_like(a["height"])
+    if state.iso_acc is not None:  # a rebound not yet applied is part of the state
+        arrays["iso_acc"] = state.iso_acc.detach().cpu().numpy()
+    return _write_checkpoint(d, state.iteration, arrays, _ckpt_meta(state, params, apply))
+
+
+class CheckpointWriter:
+    """Checkpoints written while the iterations go on: ``submit`` snapshots
+    the state's arrays on the device (a device-to-device copy on the current
+    stream, ordered with the iterations), copies the snapshot to pinned host
+    buffers on a side stream and hands the file writing to a background
+    thread; the next iterations run meanwhile.  The files are those of
+    :func:`save_checkpoint`, byte for byte.  One checkpoint is in flight at
+    a time (a new ``submit`` first waits for the previous one); ``wait``
+    before reading the files."""
+
+    def __init__(self, store):
+        import torch
+        from concurrent.futures import ThreadPoolExecutor
+
+        self.dir = Path(store.checkpoint_dir)
+        self._ex = ThreadPoolExecutor(max_workers=1)
+        self._pending = None
+        self._snap: dict = {}
+        self._host: dict = {}
+        self._stream = torch.cuda.Stream()
+
+    def submit(self, state: gm.ErosionState, params, apply: int) -> None:
+        import torch
+
+        self.wait()
+        self.dir.mkdir(parents=True, exist_ok=True)
+        names = list(CKPT_FIELDS) + (["iso_acc"] if state.iso_acc is not None else [])
+        for k in names:  # the snapshot, on the stream the iterations run on
+            src = getattr(state, k)
+            if k not in self._snap or self._snap[k].shape != src.shape:
+                self._snap[k] = torch.empty_like(src)
+                self._host[k] = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+            self._snap[k].copy_(src)
+        ready = torch.cuda.Event()
+        ready.record()
+        with torch.cuda.stream(self._stream):
+            self._stream.wait_event(ready)
+            for k in names:
+                self._host[k].copy_(self._snap[k], non_blocking=True)
+            copied = torch.cuda.Event()
+            copied.record()
+        meta = _ckpt_meta(state, params, apply)
+        it = state.iteration
+
+        def write():
+            copied.synchronize()
+            arrays = {k: self._host[k].numpy() for k in CKPT_FIELDS}
+            arrays["lake_load"] = np.zeros_like(arrays["height"])
+            if "iso_acc" in names:
+                arrays["iso_acc"] = self._host["iso_acc"].numpy()
+            # the writer reads the pinned buffers only until np.savez returns
+            return _write_checkpoint(self.dir, it, arrays, meta)
+
+        self._pending = self._ex.submit(write)
+
+    def wait(self) -> Path | None:
+        if self._pending is None:
+            return None
+        p = self._pending.result()
+        self._pending = None
+        return p
+
+    def close(self) -> None:
+        self.wait()
+        self._ex.shutdown(wait=True)
 
 
 def prune_checkpoints(d: Path, params_hash: str, keep: int = 2) -> None:
@@ -164,6 +245,7 @@ def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
         for k in ("height", "sediment", "discharge", "momentum"):
             getattr(state, k).copy_(torch.as_tensor(z[k]))
         state.pending.copy_(torch.as_tensor(z["pending"]) if "pending" in z.files else torch.zeros_like(state.pending))
+        state.iso_acc = torch.as_tensor(z["iso_acc"], device=state.height.device) if "iso_acc" in z.files else None
     state.iteration = int(meta["iteration"])
 
 
@@ -189,8 +271,11 @@ def write_outputs(store, state: gm.ErosionState) -> None:
     store.save_field("momentum", a["momentum"].astype(np.float32), H)
 
 
-def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | None = None) -> dict:
-    """The erosion stage (run.py:374-551, plain path) on the GPU."""
+def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | None = None,
+        async_checkpoints: bool = True) -> dict:
+    """The erosion stage (run.py:374-551, plain path) on the GPU.  With
+    ``async_checkpoints`` the checkpoint files are written in the background
+    while the next iterations run (:class:`CheckpointWriter`)."""
     ep = erosion_group(params)
     check_plain(ep)
     n_iter = int(ep.iterations)
@@ -202,6 +287,7 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
         load_checkpoint(state, *ck)
         log(f"[erosion] resumed from {ck[0].name} (iteration {state.iteration})")
     times, clamped, lost_offshore, datum = [], 0, 0.0, 0.0
+    writer = CheckpointWriter(store) if async_checkpoints and ep.checkpoint_every > 0 else None
     while state.iteration < n_iter:
         it = state.iteration
         t0 = time.time()
@@ -216,8 +302,14 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
             f"pending {st.get('pending_total', 0.0):.1f}, {times[-1]:.2f}s")
         done = state.iteration
         if ep.checkpoint_every > 0 and (done % ep.checkpoint_every == 0 or done == n_iter):
-            p = save_checkpoint(store, state, params, apply)
-            log(f"[erosion] checkpoint -> {p.name}")
+            if writer is not None:
+                writer.submit(state, params, apply)
+                log(f"[erosion] checkpoint -> erosion_iter{done:04d}.npz (writing)")
+            else:
+                p = save_checkpoint(store, state, params, apply)
+                log(f"[erosion] checkpoint -> {p.name}")
+    if writer is not None:
+        writer.close()
     write_outputs(store, state)
     a = state.to_numpy()
     inter = state.interior

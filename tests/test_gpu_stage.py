@@ -41,3 +41,41 @@ def test_stage_run_checkpoints_and_resume(cuda, tmp_path):
     for n in stage.OUTPUTS:
         again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
         assert again.tobytes() == out[n].tobytes(), n
+
+
+def test_background_checkpoints_equal_synchronous_ones(cuda, tmp_path):
+    """Checkpoints written while the iterations go on hold the same arrays
+    as the synchronous writer's, and the final outputs are the same."""
+    a_dir, b_dir = tmp_path / "a", tmp_path / "b"
+    sa, p = _world_store(a_dir)
+    sb, _ = _world_store(b_dir)
+    stage.run(sa, p, log=lambda m: None, async_checkpoints=True)
+    stage.run(sb, p, log=lambda m: None, async_checkpoints=False)
+    for it in (3, 6):
+        with np.load(sa.checkpoint_dir / f"erosion_iter{it:04d}.npz") as za, np.load(sb.checkpoint_dir / f"erosion_iter{it:04d}.npz") as zb:
+            assert set(za.files) == set(zb.files)
+            for k in za.files:
+                assert za[k].tobytes() == zb[k].tobytes(), (it, k)
+    for n in stage.OUTPUTS:
+        for k in range(6):
+            assert np.load(sa.coarse / f"{n}.f{k}.npy").tobytes() == np.load(sb.coarse / f"{n}.f{k}.npy").tobytes()
+
+
+def test_isostasy_state_is_checkpointed_and_resumed(cuda, tmp_path):
+    """With isostasy on, the rebound not yet applied (iso_acc) is part of the
+    checkpoint (run.py:100-139) and a resumed run lands on the continuous
+    run's outputs."""
+    import dataclasses
+
+    st, p = _world_store(tmp_path)
+    p = dataclasses.replace(p, erosion=dataclasses.replace(p.erosion, isostasy=0.8, isostasy_every=4))
+    stage.run(st, p, log=lambda m: None)
+    with np.load(st.checkpoint_dir / "erosion_iter0003.npz") as z:
+        assert "iso_acc" in z.files and np.abs(z["iso_acc"]).max() > 0.0
+    out = {n: np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)]) for n in stage.OUTPUTS}
+    for suf in (".npz", ".json"):
+        (st.checkpoint_dir / f"erosion_iter0006{suf}").unlink()
+    stage.run(st, p, log=lambda m: None)
+    for n in stage.OUTPUTS:
+        again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
+        assert again.tobytes() == out[n].tobytes(), n
