@@ -124,3 +124,59 @@ def hypsometry(height, sediment, interior, unit, pct=(1, 5, 10, 25, 50, 75, 90, 
     """Cell-count percentiles (metres) of the interior surface."""
     s = (np.asarray(height) + np.asarray(sediment))[interior] * unit
     return np.percentile(s, pct)
+
+
+def window_world(kind: str, N: int = 48, H: int = 2, cell: float = 50.0, seed: int = 0, writeoff: float | None = None):
+    """Single-face windows (spherical=False, deposit_on_exit) for the
+    reference's conservation tests (bake/tests/test_erosion.py:191-289):
+    ``closed`` -- a bowl above sea level, nothing can leave as ocean deposit;
+    ``tilt`` -- a plane tilted into the sea, an open coast; ``shelf`` -- land
+    sloping to a seafloor one ``dep_floor_m`` below the waterline, walled off
+    at the far edge, so every load that reaches the sea is surplus.
+    Returns the window arrays (cell units) and WorldParams."""
+    from pgerosion.params import ErosionParams, WorldGroup, WorldParams, plain_knobs
+
+    NE = N + 2 * H
+    g = get_grid(N, H, cell)
+    i, j = np.meshgrid(np.arange(NE), np.arange(NE), indexing="ij")
+    u = (i - H + 0.5) / N
+    v = (j - H + 0.5) / N
+    rough = 2.0 * np.random.default_rng(seed).standard_normal((NE, NE))
+    if kind == "closed":
+        bed = 60.0 + 400.0 * ((u - 0.5) ** 2 + (v - 0.5) ** 2) + rough
+    elif kind == "tilt":
+        bed = 80.0 * (0.55 - u) + 8.0 * np.sin(6.0 * v) + rough
+    elif kind == "shelf":
+        bed = np.where(u < 0.6, 60.0 * (0.6 - u) + 1.0 + np.abs(rough), -0.9)
+        bed = np.where(u >= 0.9, 300.0, bed)
+    else:
+        raise KeyError(kind)
+    mask = np.zeros((1, NE, NE), np.uint8)
+    mask[0, H:H + N, H:H + N] = 1
+    ep = ErosionParams(iterations=40, max_steps=64, friction=0.05, erodibility=0.3, deposition_rate=0.3, evap_rate=0.01,
+                       uplift_mode="stack", particles_per_cell=1.0, **plain_knobs())
+    if writeoff is not None:
+        ep.offshore_writeoff = float(writeoff)
+    p = WorldParams(world=WorldGroup(seed=seed, N_c=N, cell_size_m=cell, land_fraction=0.5, halo=H), erosion=ep)
+    arr = dict(height=(bed / cell)[None].astype(np.float64), mask=mask, metric=np.ascontiguousarray(g.metric_face[None]),
+               metric_inv=np.ascontiguousarray(g.metric_inv_face[None]), N=N, H=H, cell=cell)
+    return arr, p
+
+
+def gpu_window(arr):
+    """A device ErosionState of ``window_world``'s arrays."""
+    import torch
+
+    from pgerosion import maps as gm
+
+    dev = torch.device("cuda")
+    sh = arr["height"].shape
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    return gm.ErosionState(height=f64(arr["height"]), sediment=f64(np.zeros(sh)), discharge=f64(np.zeros(sh)),
+                           momentum=f64(np.zeros(sh + (2,))), hardness=f32(np.full(sh, 0.5)), precip=f32(np.ones(sh)),
+                           evap=f32(np.ones(sh)), uplift=f64(np.zeros(sh)),
+                           mask=torch.as_tensor(arr["mask"], device=dev), metric=f32(arr["metric"][0]),
+                           metric_inv=f32(arr["metric_inv"][0]), N=arr["N"], H=arr["H"], spherical=False,
+                           height_unit_m=arr["cell"], deposit_on_exit=True)
+
