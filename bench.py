@@ -103,6 +103,61 @@ def run_batched(args, rank, world_size, dist, dev):
             "slowest_world_ms_per_step": worst}
 
 
+def run_adjoint(args, dev):
+    """The calibration workload: N_c = 256 Earth-like world, 2^17 droplets per
+    iteration, 50 iterations, a checkpoint every 5; loss = mean squared
+    height difference over land to a target made by the same run with the
+    four rates jittered +-30 % (another seed); gradients with respect to a
+    per-cell erodibility field (1 +- 0.2) and the four rates.  Times the
+    forward (the run) and the adjoint (backward: recompute from the
+    checkpoints with the passes taped, then the reverse) with CUDA events, for
+    the default truncated gradient and for the exact one along the recorded
+    paths."""
+    import torch
+
+    from pgerosion import adjoint as adj
+
+    params = adj.calibration_params(seed=0)
+    st = adj.calibration_state(params, device=dev)
+    calib = adj.Calibration(st, params, adj.CALIB_ITERATIONS, adj.CALIB_DROPLETS, checkpoint_every=adj.CALIB_CHECKPOINT)
+    target = calib.run(None, adj.rates_of(adj.calibration_params(seed=0, jitter=0.3, jitter_seed=1)).tolist())
+    land = torch.zeros_like(target, dtype=torch.bool)
+    land[st.interior] = target[st.interior] > 0.0
+    out = {"workload": f"calibration: N_c={adj.CALIB_N}, {adj.CALIB_DROPLETS} droplets/iteration, {adj.CALIB_ITERATIONS} "
+                       f"iterations, checkpoint every {adj.CALIB_CHECKPOINT}, wave apply (one wave per iteration), loss = "
+                       "mean squared land height difference (m^2) to a target from rates +-30 %",
+           "metric": "adjoint/forward time ratio", "higher_is_better": False, "modes": {}}
+    for name, cp, ct in (("truncated", False, False), ("exact_on_paths", True, True)):
+        calib.carry_path, calib.carry_terrain = cp, ct
+        fw, bw = [], []
+        for rep in range(1 + max(1, args.adjoint_reps)):
+            erod = adj.erodibility_init(st, seed=0).requires_grad_(True)
+            rates = adj.rates_of(params).to(dev).requires_grad_(True)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            ev[0].record()
+            loss = adj.land_loss(adj.erode(erod, rates, calib), target, land, st.height_unit_m)
+            ev[1].record()
+            loss.backward()
+            ev[2].record()
+            torch.cuda.synchronize()
+            if rep > 0:  # the first repetition allocates the tapes
+                fw.append(ev[0].elapsed_time(ev[1]))
+                bw.append(ev[1].elapsed_time(ev[2]))
+        g = rates.grad.detach().cpu().tolist()
+        fin = bool(np.all(np.isfinite(g))) and bool(torch.isfinite(erod.grad).all())
+        out["modes"][name] = {"carry_path": cp, "carry_terrain": ct, "forward_ms": float(np.median(fw)),
+                              "adjoint_ms": float(np.median(bw)), "ratio": float(np.median(bw) / np.median(fw)),
+                              "loss_m2": float(loss.detach()), "finite": fin,
+                              "rate_gradient": g if fin else None,
+                              "field_gradient_l1": float(erod.grad.double().abs().sum()) if fin else None}
+    out["value"] = out["modes"]["truncated"]["ratio"]
+    out["droplet_steps_per_iteration"] = float(np.mean([s_.get("droplet_steps", 0) for s_ in calib.stats]))
+    del calib, st
+    torch.cuda.empty_cache()
+    return out
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -325,6 +380,9 @@ def run_b200(args, rank, world_size, dist):
         batched = run_batched(args, rank, world_size, dist, dev)
     if rank != 0:
         return None
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(args, dev)
     peak, peak_kind = _peaks()
     per_launch_steps = steps_done / max(args.steps, 1)
     avg_ta = float(np.mean(ta_ms))
@@ -357,6 +415,8 @@ def run_b200(args, rank, world_size, dist):
         out["alt_wave_apply"] = alt
     if batched is not None:
         out["batched_worlds"] = batched
+    if adjoint is not None:
+        out["adjoint"] = adjoint
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
@@ -419,6 +479,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     ap.add_argument("--batch-worlds", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the calibration (adjoint) measurement")
+    ap.add_argument("--adjoint-reps", type=int, default=2)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

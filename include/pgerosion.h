@@ -27,6 +27,16 @@
  *   pge_uplift            apply_uplift             globe/erosion/maps.py:1088-1147
  *   pge_hold_datum        hold_datum               globe/erosion/maps.py:1446-1508
  *   pge_halo_gather       FaceField.exchange_halos globe/field.py:104-125
+ *   pge_trace_apply_tape  pge_trace_apply (wave apply, one wave) recording each
+ *                         droplet's steps and ledger branches for the adjoint
+ *   pge_adjoint_pass      reverse of one taped droplet pass: gradients of the
+ *                         surface after the pass with respect to the surface
+ *                         before it, the per-cell erodibility field and the
+ *                         erodibility, deposition, evaporation and friction rates
+ *   pge_halo_adjoint      transpose of pge_halo_gather (scalar fields)
+ *                         (the adjoint has no reference counterpart; it
+ *                         differentiates the trace of particle.py:421-815 and the
+ *                         ledger of particle.py:934-1018 along frozen paths)
  *
  * Conventions
  *   - Every pointer in the structs is a DEVICE pointer unless marked "host".
@@ -122,6 +132,8 @@ typedef struct PgeState {
     const uint8_t *mask;     /* (F,NE,NE) or NULL: every cell active */
     const float *metric;     /* (NE,NE,3) or (F,NE,NE,3): g_ii, g_ij, g_jj */
     const float *metric_inv; /* same shape: inverse metric */
+    const float *erodibility; /* (F,NE,NE) per-cell multiplier of erosion.erodibility, or NULL (1 everywhere; the
+                                 reference's model): the calibrated field of the adjoint; wave apply only */
 } PgeState;
 
 /* droplet spawns of one iteration: rain first, then re-injected stockpiles */
@@ -170,6 +182,64 @@ typedef struct PgeStats {
     int64_t deposited_fx;    /* terrain added by the ledger (applied deposition) */
     int64_t errors;          /* nonzero: an ordered-apply wait gave up (the pass is invalid) */
 } PgeStats;
+
+/* The tape of one wave-apply droplet pass, for the adjoint.  Row r of each
+ * array is droplet r of the pass (rain, then re-injected stockpiles).  state[r, k] is
+ * the droplet's (x, y, a, b, sed, vol) at the start of its k-th step; the row
+ * after its last completed step is its final state.  bits[r, k] holds the
+ * face (bits 0-2) and the branches that step took (PGE_TB_*).  entry[r, j]
+ * is the ledger's j-th change: (cell, reference cell, branch code PGE_TE_*,
+ * step index or -1 for a final deposit).  count[r] = (state rows, entries).
+ * wave_acc[w] is the pass's int64 terrain accumulator (2^-40 cell units) as
+ * wave w started: the terrain wave w's droplets saw. */
+typedef struct PgeTape {
+    double *state;    /* (droplets, steps + 1, 6) */
+    int32_t *bits;    /* (droplets, steps + 1) */
+    int32_t *entry;   /* (droplets, entries, 4) */
+    int32_t *count;   /* (droplets, 2) */
+    int64_t droplets; /* rows (>= the pass's spawn count) */
+    int32_t steps;    /* >= max_steps */
+    int32_t entries;  /* >= max_steps + 8 */
+    int64_t *wave_acc; /* (waves, F*NE*NE) */
+    int64_t waves;     /* >= the pass's waves, ceil(count / p->wave) */
+} PgeTape;
+
+/* tape bits of a step (the trace's branches, particle.py:421-769); whether a
+ * bilinear weight was clamped to [0, 1] is not stored: it follows from the
+ * recorded coordinates */
+enum {
+    PGE_TB_FACE = 0x7,            /* face the step starts on */
+    PGE_TB_S2_ZERO = 1 << 5,      /* slope^2 clamped to 0 */
+    PGE_TB_Q_ZERO = 1 << 6,       /* discharge sample clamped to 0 */
+    PGE_TB_FR_ZERO = 1 << 7,      /* 1 - dt friction clamped to 0 */
+    PGE_TB_MOM = 1 << 8,          /* the momentum pull was applied */
+    PGE_TB_CROSS = 1 << 9,        /* the move left the face's square: transfer_velocity ran */
+    PGE_TB_SAME_FACE = 1 << 10,   /* ... and came back to the same face (coordinates clamped) */
+    PGE_TB_X_CLAMP = 1 << 11,     /* the new coordinate was clamped */
+    PGE_TB_Y_CLAMP = 1 << 12,
+    PGE_TB_H1_ABOVE = 1 << 15,    /* new height above the base: dh = h0 - h1 (else h0 - base) */
+    PGE_TB_LAND = 1 << 16,        /* land mass transfer made an entry */
+    PGE_TB_SEA = 1 << 17,         /* seafloor (fan) mass transfer made an entry */
+    PGE_TB_CEQ_ZERO = 1 << 18,    /* capacity clamped to 0 */
+    PGE_TB_COVER = 1 << 19,       /* capacity above the load: the cover / hardness blend */
+    PGE_TB_POS = 1 << 20,         /* cdiff > 0 (erosion) */
+    PGE_TB_NEG = 1 << 21,         /* cdiff < 0 (deposition) */
+    PGE_TB_CLAMP = 1 << 22,       /* cdiff limited by the erosion cap / the deposit room */
+    PGE_TB_ECAP_SHIFT = 23,       /* 2 bits: erosion cap = dh / kexp, max_erode, the cell's surface, 0 */
+    PGE_TB_ROOM_FLOOR = 1 << 25,  /* deposit room = its floor (dep_floor / fan_room), not h_prev - h_here */
+    PGE_TB_SEA_SHIFT = 26,        /* 2 bits: seafloor room as above, the base limit, or 0 */
+    PGE_TB_EV_CLAMP = 1 << 28     /* evaporation factor clamped to 0.01 */
+};
+
+/* tape code of a ledger entry (particle.py:934-1018) */
+enum {
+    PGE_TE_DEPOSIT = 1 << 0,      /* delta >= 0 */
+    PGE_TE_STEP = 1 << 1,         /* a step entry (else a final deposit) */
+    PGE_TE_SKIP = 1 << 2,         /* inactive cell: nothing applied */
+    PGE_TE_SRC_SHIFT = 4,         /* 3 bits, erosion: ew, room, floor = base, floor = surface, floor = next cell, 0;
+                                     deposit: want, room, reference ceiling, base limit, 0 */
+    PGE_TE_TAKE_SHIFT = 8         /* 2 bits, deposit: no deficit, all of want taken, all of the deficit taken */
+};
 
 /* halo gather tables (bake/globe/cubesphere.py:540-662) */
 typedef struct PgeHalo {
@@ -265,6 +335,43 @@ PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, 
 /* Fills the halo rows of one field from its interior: a scalar (F,NE,NE)
  * field, or with vector = 1 a (F,NE,NE,2) field rotated per source. */
 PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream);
+
+/* No counterpart in the reference: the adjoint of the particle pass.
+ *
+ * pge_trace_apply_tape: pge_trace_apply with p->apply = PGE_APPLY_WAVE,
+ * float64, recording the tape (PgeTape).  The pass's result is
+ * pge_trace_apply's, bit for bit.
+ *
+ * pge_adjoint_pass: the reverse of that pass.  s holds the pass's START
+ * state (the one pge_trace_apply_tape read) and tape its record; zbar_after
+ * is dL/d(surface after the pass) (F,NE,NE); writes dL/d(surface before the
+ * pass) to zbar_before (a different buffer; waves are reversed last to
+ * first, each against the terrain it saw) and ADDS dL/d(erodibility field)
+ * to ebar (F,NE,NE; may be NULL) and dL/d(erodibility, deposition_rate,
+ * evap_rate, friction) to pbar[0..3] (device doubles).  Each droplet's cell
+ * path and every branch it took are held fixed; within them the load and
+ * volume are differentiated along the whole path (capacity law, exchange
+ * rate, erosion cap, deposit room, evaporation, final load, the ledger's
+ * floors, ceilings, deficit and surplus) and the terrain through the
+ * bilinear samples.  carry_path = 1: the droplet's position and direction
+ * are differentiated along the whole path too (slope force, friction,
+ * momentum pull, metric normalisation, face transfer): the exact derivative
+ * of the pass on its path.  carry_path = 0: each step's incoming position
+ * and direction are held fixed and only the step's own move is
+ * differentiated (its new position's sample).  Held constant in both: the
+ * discharge and momentum tracks, sediment cover, hardness, evaporation
+ * field, base level, stockpiles and the droplet's own earlier changes inside
+ * its ledger's bounds.  Float64 atomics: the sums' order (last bits) varies.
+ * stats (may be NULL) gets errors != 0 if the tape and its steps disagree.
+ *
+ * pge_halo_adjoint: for each halo row, adds w * zbar[dst] to zbar[src] and
+ * zeroes zbar[dst] (the transpose of the scalar pge_halo_gather). */
+PGE_API int pge_trace_apply_tape(const PgeGrid *g, PgeState *s, const PgeSpawns *spawns, const PgeParams *p,
+                                 const PgeTape *tape, PgeStats *stats, void *ws, size_t ws_bytes, void *stream);
+PGE_API int pge_adjoint_pass(const PgeGrid *g, const PgeState *s, const PgeSpawns *spawns, const PgeParams *p,
+                             const PgeTape *tape, int32_t carry_path, const double *zbar_after, double *zbar_before,
+                             double *ebar, double *pbar, PgeStats *stats, void *ws, size_t ws_bytes, void *stream);
+PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream);
 
 /* No counterpart in the reference.  pge_thermal for callers that cannot
  * allocate device memory -- a host that owns the whole device heap through

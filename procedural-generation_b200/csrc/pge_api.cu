@@ -185,7 +185,7 @@ Layout layout(const PgeGrid &g)
 namespace {
 int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, const double *ecap, PgeStats *stats,
               void *ws, const Layout &lay, cudaStream_t st, int32_t *rec_cell, double *rec_delta, float *rec_vol,
-              float *rec_mom, int64_t *rec_count, int8_t *rec_death)
+              float *rec_mom, int64_t *rec_count, int8_t *rec_death, const PgeTape *tape = nullptr)
 {
     cudaError_t e;
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.acc4), 0, 32 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset acc");
@@ -204,7 +204,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         const int threads = p->threads_per_block ? p->threads_per_block : 256;
         // blocks_per_sm >= 2 selects the kernel variant compiled for two resident blocks per SM
         const int minb = p->blocks_per_sm >= 2 ? 2 : 1;
-        int bps = p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
+        int bps = tape ? droplet_blocks_per_sm_f64_tape(threads)
+                  : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
         if (p->blocks_per_sm > 0 && p->blocks_per_sm < bps) bps = p->blocks_per_sm;
         long long maxblocks = (long long)sm_count() * bps;
         if (maxblocks * threads > lay.nslots) maxblocks = lay.nslots / threads;
@@ -228,6 +229,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.sp_sed = sp->sed;
         a.sp_dir = sp->dir;
         a.volume0 = sp->volume0;
+        a.erod = s->erodibility;
+        if (tape) a.tape = *tape;
         a.p = *p;
         a.acc4 = ws_ptr<long long>(ws, lay.acc4);
         a.pend = ws_ptr<long long>(ws, lay.pend);
@@ -353,6 +356,11 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             a.d_end = a.d_begin + wave < P ? a.d_begin + wave : P;
             a.counter = ctr + (w & 1);
             a.counter_next = ctr + ((w + 1) & 1);
+            if (tape) {  // the terrain this wave sees: the accumulator's terrain column as the wave starts
+                e = cudaMemcpy2DAsync(tape->wave_acc + w * lay.ncell, sizeof(long long), ws_ptr<long long>(ws, lay.acc4),
+                                      4 * sizeof(long long), sizeof(long long), lay.ncell, cudaMemcpyDeviceToDevice, st);
+                if (e != cudaSuccess) return cuda_fail(e, "tape wave start");
+            }
             // 2^24 droplet generations per thread and wave; after 255 waves the tables are cleared again
             if (w > 0 && w % 255 == 0) {
                 if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.tkey), 0, 8 * lay.nslots * lay.table_slots, st)) != cudaSuccess)
@@ -361,8 +369,9 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             a.gen_base = (unsigned long long)(w % 255 + 1) << 24;
             long long blocks = (a.d_end - a.d_begin + threads - 1) / threads;
             if (blocks > maxblocks) blocks = maxblocks;
-            e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
-                                             : launch_droplets_f32(a, (int)blocks, threads, st);
+            e = tape ? launch_droplets_f64_tape(a, (int)blocks, threads, st)
+                     : p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
+                                                    : launch_droplets_f32(a, (int)blocks, threads, st);
             if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
             if (w + 1 < nw) refresh(*s, lay, ws, st);
         }
@@ -441,6 +450,8 @@ PGE_API int pge_trace_apply(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, 
     if (sp->count > 0 && (!sp->face || !sp->x || !sp->y || !sp->sed || !sp->dir || !(sp->volume0 > 0.0)))
         return fail(PGE_E_ARG, "trace_apply: incomplete spawns");
     if (p->use_erode_cap && !erode_cap) return fail(PGE_E_ARG, "use_erode_cap without erode_cap");
+    if (s->erodibility && p->apply != PGE_APPLY_WAVE)
+        return fail(PGE_E_UNSUPPORTED, "a per-cell erodibility field needs the wave apply");
     cudaStream_t st = (cudaStream_t)stream;
     if ((r = run_waves(g, s, sp, p, erode_cap, stats, ws, lay, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr))) return r;
     const int exact = p->apply == PGE_APPLY_ORDERED;
@@ -448,6 +459,62 @@ PGE_API int pge_trace_apply(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, 
     fold_ema(*s, lay, ws, p->ema, exact, st);
     cudaError_t e = cudaPeekAtLastError();
     return e == cudaSuccess ? PGE_OK : cuda_fail(e, "fold_ema");
+}
+
+PGE_API int pge_trace_apply_tape(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, const PgeTape *tape,
+                                 PgeStats *stats, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s)) || (r = check_params(g, p))) return r;
+    if (!sp || !stats || !tape) return fail(PGE_E_ARG, "trace_apply_tape: NULL spawns, tape or stats");
+    if (sp->count < 0 || sp->count > g->max_droplets)
+        return fail(PGE_E_ARG, "spawn count %lld outside 0..%lld", (long long)sp->count, (long long)g->max_droplets);
+    if (sp->count > 0 && (!sp->face || !sp->x || !sp->y || !sp->sed || !sp->dir || !(sp->volume0 > 0.0)))
+        return fail(PGE_E_ARG, "trace_apply_tape: incomplete spawns");
+    if (p->apply != PGE_APPLY_WAVE || p->precision != PGE_PREC_F64 || p->use_erode_cap)
+        return fail(PGE_E_UNSUPPORTED, "the tape records a float64 wave-apply pass without the erode cap");
+    if (!tape->state || !tape->bits || !tape->entry || !tape->count || !tape->wave_acc) return fail(PGE_E_ARG, "tape has a NULL array");
+    const long long nw = (sp->count + p->wave - 1) / p->wave;
+    if (tape->droplets < sp->count || tape->steps < p->max_steps || tape->entries < p->max_steps + SPREAD || tape->waves < nw)
+        return fail(PGE_E_ARG, "tape too small: %lld rows x %d steps x %d entries x %lld waves for %lld droplets, max_steps %d, "
+                    "%lld waves", (long long)tape->droplets, tape->steps, tape->entries, (long long)tape->waves,
+                    (long long)sp->count, p->max_steps, nw);
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((r = run_waves(g, s, sp, p, nullptr, stats, ws, lay, st, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, tape))) return r;
+    set_mode_kernel<<<1, 1, 0, st>>>(ws_ptr<unsigned long long>(ws, lay.counters) + 4, 0ull);
+    fold_ema(*s, lay, ws, p->ema, 0, st);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "trace_apply_tape");
+}
+
+PGE_API int pge_adjoint_pass(const PgeGrid *g, const PgeState *s, const PgeSpawns *sp, const PgeParams *p, const PgeTape *tape,
+                             int32_t carry_path, const double *zbar_after, double *zbar_before, double *ebar, double *pbar,
+                             PgeStats *stats, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s)) || (r = check_params(g, p))) return r;
+    if (!sp || !tape || !zbar_after || !zbar_before || !pbar) return fail(PGE_E_ARG, "adjoint_pass: NULL pointer");
+    if (zbar_after == zbar_before) return fail(PGE_E_ARG, "adjoint_pass: zbar_before must not alias zbar_after");
+    if (!tape->state || !tape->bits || !tape->entry || !tape->count || !tape->wave_acc || tape->droplets < sp->count ||
+        tape->steps < p->max_steps || tape->entries < 1 || tape->waves < (sp->count + p->wave - 1) / p->wave)
+        return fail(PGE_E_ARG, "adjoint_pass: the tape does not cover the pass");
+    if (sp->count > 0 && !(sp->volume0 > 0.0)) return fail(PGE_E_ARG, "adjoint_pass: volume0 must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = adjoint_pass(*g, *s, *sp, *p, *tape, carry_path, zbar_after, zbar_before, ebar, pbar, lay, ws, st);
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint_pass");
+    adjoint_errors(lay, ws, stats, st);
+    e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "adjoint_pass");
+}
+
+PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream)
+{
+    if (!h || !zbar || (h->K > 0 && (!h->dst || !h->src || !h->w))) return fail(PGE_E_ARG, "halo_adjoint: NULL pointer");
+    halo_adjoint(*h, zbar, (cudaStream_t)stream);
+    cudaError_t e = cudaPeekAtLastError();
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "halo_adjoint");
 }
 
 PGE_API int pge_trace_changelist(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParams *p, int32_t *cl_cell,

@@ -346,6 +346,7 @@ struct Entry {
     long long cell;
     double delta;
     float vol, ma, mb;
+    int sidx;  // the step that made it (-1: a final deposit); the tape only
 };
 
 struct Ledger {
@@ -353,6 +354,8 @@ struct Ledger {
     bool has_prev;
     double prev_live;
     long long death;
+    long long prev_cell;  // cell of the last step entry (the tape's reference cell)
+    int tap_n;            // entries taped
     int clamped;
     long long eroded_fx, deposited_fx;  // this thread's applied totals
 };
@@ -372,14 +375,30 @@ __device__ __forceinline__ void load_lcell(const DropArgs &a, const Table &t, lo
 // droplet's view of the terrain.  `nx` is the next entry's cell (has_next).
 // Updates c.own (and the table), emits the atomics and returns the applied
 // change (0 when nothing moved).
-__device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger &L, const Entry &e, LCell &c, bool has_next,
-                                            const LCell &nx)
+template <bool TAPE>
+__device__ __forceinline__ void tape_entry(const DropArgs &a, Ledger &L, long long row, const Entry &e, long long ref, int code)
 {
-    if (c.m != PGE_MASK_ACTIVE) return;
+    if (!TAPE) return;
+    if (L.tap_n < a.tape.entries) {
+        int4 *te = reinterpret_cast<int4 *>(a.tape.entry) + row * a.tape.entries + L.tap_n;
+        *te = make_int4((int)e.cell, (int)ref, code, e.sidx);
+    }
+    L.tap_n++;
+}
+
+template <bool TAPE = false>
+__device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger &L, const Entry &e, LCell &c, bool has_next,
+                                            const LCell &nx, long long row = 0)
+{
     const PgeParams &p = a.p;
     const double d = e.delta;
     const float v = e.vol;
     const bool is_step = v >= 0.0f;
+    const int kind = (d < 0.0 ? 0 : PGE_TE_DEPOSIT) | (is_step ? PGE_TE_STEP : 0);
+    if (c.m != PGE_MASK_ACTIVE) {
+        tape_entry<TAPE>(a, L, row, e, -1, kind | PGE_TE_SKIP);
+        return;
+    }
     const double a0 = c.acc();
     const double s_c = c.hs + a0;
     const float b_c = c.base;
@@ -392,53 +411,87 @@ __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger 
             const double r2 = __ldg(a.ecap + c.cell) + a0;
             if (r2 < room) room = r2;
         }
-        if (e_act > room) e_act = room;
+        int src = 0, fsrc = s_c >= (double)b_c ? 2 : 3;
+        if (e_act > room) {
+            e_act = room;
+            src = 1;
+        }
         double floor_ = s_c >= (double)b_c ? (double)b_c : s_c;
         if (has_next) {
             const double ns = nx.live();
-            if (ns > floor_) floor_ = ns;
+            if (ns > floor_) {
+                floor_ = ns;
+                fsrc = 4;
+            }
         }
-        if (e_act > s_c - floor_) e_act = s_c - floor_;
-        if (e_act < 0.0) e_act = 0.0;
+        if (e_act > s_c - floor_) {
+            e_act = s_c - floor_;
+            src = fsrc;
+        }
+        if (e_act < 0.0) {
+            e_act = 0.0;
+            src = 5;
+        }
         if (e_act < ew) {
             L.clamped++;
             L.deficit += ew - e_act;
         }
         applied = -e_act;
+        tape_entry<TAPE>(a, L, row, e, src == 4 ? nx.cell : -1, kind | (src << PGE_TE_SRC_SHIFT));
     } else {
         double want = d + L.surplus;
         L.surplus = 0.0;
+        int take_code = 0;
         if (L.deficit > 0.0) {
+            take_code = want < L.deficit ? 1 : 2;
             const double take = want < L.deficit ? want : L.deficit;
             want -= take;
             L.deficit -= take;
         }
         double d_act = want;
+        int src = 0;
         const double room = p.iter_deposit - a0;
-        if (d_act > room) d_act = room;
+        if (d_act > room) {
+            d_act = room;
+            src = 1;
+        }
         bool has_ref = false;
         double ref_live = 0.0;
+        long long ref_cell = -1;
         if (is_step) {
             has_ref = L.has_prev;
             ref_live = L.prev_live;
+            ref_cell = L.prev_cell;
         } else if (has_next) {
             has_ref = true;
             ref_live = nx.live();
+            ref_cell = nx.cell;
         }
         if (has_ref) {
             double ceil_ = ref_live + p.dep_floor;
             if (s_c < (double)b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
             const double lim = ceil_ - s_c;
-            if (d_act > lim) d_act = lim;
+            if (d_act > lim) {
+                d_act = lim;
+                src = 2;
+            }
         }
         if (s_c < (double)b_c) {
             const double lim = (double)b_c - p.dep_floor - s_c;
-            if (d_act > lim) d_act = lim;
+            if (d_act > lim) {
+                d_act = lim;
+                src = 3;
+            }
         }
-        if (d_act < 0.0) d_act = 0.0;
+        if (d_act < 0.0) {
+            d_act = 0.0;
+            src = 4;
+        }
         if (d_act < want) L.clamped++;
         L.surplus = want - d_act;
         applied = d_act;
+        tape_entry<TAPE>(a, L, row, e, src == 2 ? ref_cell : -1,
+                         kind | (src << PGE_TE_SRC_SHIFT) | (take_code << PGE_TE_TAKE_SHIFT));
         if (!is_step && L.death < 0) L.death = c.cell;
     }
     if (applied != 0.0) {
@@ -458,6 +511,7 @@ __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger 
         }
         L.has_prev = true;
         L.prev_live = c.live();
+        L.prev_cell = c.cell;
     }
 }
 
@@ -479,7 +533,8 @@ __device__ __forceinline__ void sync_own(LCell &x, const LCell &changed)
 enum { ST_DROP, ST_STEPS, ST_ENTRIES, ST_CLAMPED, ST_OVER, ST_TOPEND, ST_DEFICIT, ST_LOSTOFF, ST_ERODED, ST_DEPOSITED,
        ST_DEATH0, ST_N = ST_DEATH0 + PGE_N_DEATHS };
 
-template <int MINB, bool LEDGER>
+// TAPE (with LEDGER): also record the adjoint's tape (a.tape, row = the droplet's index in the pass)
+template <int MINB, bool LEDGER, bool TAPE = false>
 __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
 {
     const PgeParams &p = a.p;
@@ -557,6 +612,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     L.has_prev = false;
                     L.prev_live = 0.0;
                     L.death = -1;
+                    L.prev_cell = -1;
+                    L.tap_n = 0;
                     L.clamped = 0;
                     L.eroded_fx = L.deposited_fx = 0;
                     t.reset(++gen);
@@ -577,6 +634,18 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         if (!alive) continue;
 
         // ---- one step of the trace (particle.py:421-769)
+        int tb = 0;  // the tape's branch bits of this step
+        const long long trow = d;  // the tape's row: the droplet's index in the pass
+        if (TAPE) {
+            double *ts = a.tape.state + (trow * (a.tape.steps + 1) + step) * 6;
+            ts[0] = (double)x;
+            ts[1] = (double)y;
+            ts[2] = (double)sa;
+            ts[3] = (double)sb;
+            ts[4] = (double)sed;
+            ts[5] = (double)vol;
+            tb = f;
+        }
         int cause = -1;
         bool exited = false;
         bool have_entry = false;
@@ -609,15 +678,24 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             const R di = R(cv.q0) * gi + R(cv.q1) * gj;
             const R dj = R(cv.q1) * gi + R(cv.q2) * gj;
             R s2 = gi * di + gj * dj;
-            if (s2 < R(0)) s2 = R(0);
+            if (s2 < R(0)) {
+                s2 = R(0);
+                if (TAPE) tb |= PGE_TB_S2_ZERO;
+            }
             const R nrm = k_slope_sat > R(0) ? k_slope_gain / sqrt(s2 + k_slope_sat * k_slope_sat) : k_slope_gain / sqrt(R(1) + s2);
             const R na = -di * nrm, nb = -dj * nrm;
             const R ma = bilin(cv, 2), mb = bilin(cv, 3);
             R q = bilin(cv, 1);
-            if (q < R(0)) q = R(0);
+            if (q < R(0)) {
+                q = R(0);
+                if (TAPE) tb |= PGE_TB_Q_ZERO;
+            }
             const R vol_rel = vol / volume0;
             R fr = R(1) - k_dt * k_friction;
-            if (fr < R(0)) fr = R(0);
+            if (fr < R(0)) {
+                fr = R(0);
+                if (TAPE) tb |= PGE_TB_FR_ZERO;
+            }
             sa *= fr;
             sb *= fr;
             const R mlen = snorm(cv, ma, mb);
@@ -627,6 +705,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 const R k = k_kmom * cosang * k_momscale / (vol + k_momscale * q);
                 sa += k * ma;
                 sb += k * mb;
+                if (TAPE) tb |= PGE_TB_MOM;
             }
             const R accel = k_dt / (vol_rel * k_density);
             sa += accel * na;
@@ -643,6 +722,19 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     nf = transfer_velocity(f, u, v, sa, sb);
                     nx = u * Nf;
                     ny = v * Nf;
+                    if (TAPE) {
+                        // clamped coordinates: transfer_velocity's own clamp when the face stays, else the
+                        // clamps below
+                        tb |= PGE_TB_CROSS;
+                        if (nf == f) {
+                            tb |= PGE_TB_SAME_FACE;
+                            if (u <= R(0) || u >= R(0.999999999)) tb |= PGE_TB_X_CLAMP;
+                            if (v <= R(0) || v >= R(0.999999999)) tb |= PGE_TB_Y_CLAMP;
+                        } else {
+                            if (nx >= Nf || nx < R(0)) tb |= PGE_TB_X_CLAMP;
+                            if (ny >= Nf || ny < R(0)) tb |= PGE_TB_Y_CLAMP;
+                        }
+                    }
                     if (nx >= Nf) nx = Nf * R(0.999999999);
                     if (ny >= Nf) ny = Nf * R(0.999999999);
                     if (nx < R(0)) nx = R(0);
@@ -663,21 +755,38 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             const R b1 = R(nv.base);
             const R dh = h0 - (h1 > b1 ? h1 : b1);
             const R dhr = h0 - h1;
+            if (TAPE && h1 > b1) tb |= PGE_TB_H1_ABOVE;
             // mass transfer at the cell we leave (particle.py:562-671)
             if (m == PGE_MASK_ACTIVE && in_sea) {
                 R cdiff = -k_ocean * sed;
                 R room = has_hprev ? R(h_prev) - R(h_here) : k_fanroom;
-                if (room < k_fanroom) room = k_fanroom;
+                if (TAPE) tb |= PGE_TB_SEA | (has_hprev ? 0 : PGE_TB_ROOM_FLOOR);
+                if (room < k_fanroom) {
+                    room = k_fanroom;
+                    if (TAPE) tb |= PGE_TB_ROOM_FLOOR;
+                }
                 const R lim = R(b_here) - k_depfloor - R(h_here);
-                if (lim < room) room = lim;
-                if (room < R(0)) room = R(0);
-                if (-cdiff * vol_rel > room) cdiff = -room / vol_rel;
+                int ssrc = 0;
+                if (lim < room) {
+                    room = lim;
+                    ssrc = 1;
+                }
+                if (room < R(0)) {
+                    room = R(0);
+                    ssrc = 2;
+                }
+                if (-cdiff * vol_rel > room) {
+                    cdiff = -room / vol_rel;
+                    if (TAPE) tb |= PGE_TB_CLAMP;
+                }
+                if (TAPE) tb |= ssrc << PGE_TB_SEA_SHIFT;
                 sed += cdiff;
                 en.cell = cv.cell;
                 en.delta = (double)(-cdiff * vol_rel);
                 en.vol = 0.0f;
                 en.ma = 0.0f;
                 en.mb = 0.0f;
+                en.sidx = step;
                 have_entry = true;
             } else if (m == PGE_MASK_ACTIVE) {
                 R qe;
@@ -685,10 +794,17 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 else if (p.disc_exponent == 0.5) qe = sqrt(q * inv_sat);
                 else if (p.disc_exponent > 0.0) qe = pow(q * inv_sat, k_dexp);
                 else qe = erf(q * inv_sat);
-                R c_eq = k_erod * dh * (R(1) + k_kdisc * qe);
-                if (c_eq < R(0)) c_eq = R(0);
+                R ker = k_erod;
+                if (LEDGER && a.erod) ker = k_erod * R(__ldg(a.erod + cv.cell));  // the wave apply's calibration field
+                R c_eq = ker * dh * (R(1) + k_kdisc * qe);
+                if (TAPE) tb |= PGE_TB_LAND;
+                if (c_eq < R(0)) {
+                    c_eq = R(0);
+                    if (TAPE) tb |= PGE_TB_CEQ_ZERO;
+                }
                 R k_e;
                 if (c_eq > sed) {
+                    if (TAPE) tb |= PGE_TB_COVER;
                     const float sthick = cv.sed;
                     R w_cover;
                     if (k_cover > R(0)) {
@@ -705,14 +821,32 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 const R kexp = R(1) + q * k_conc;
                 if (cdiff > R(0)) {
                     R ecap = dh / kexp;
-                    if (ecap > k_maxe) ecap = k_maxe;
-                    if (ecap > R(h_here)) ecap = h_here > 0.0f ? R(h_here) : R(0);
-                    if (cdiff * vol_rel > ecap) cdiff = ecap / vol_rel;
+                    int esrc = 0;
+                    if (ecap > k_maxe) {
+                        ecap = k_maxe;
+                        esrc = 1;
+                    }
+                    if (ecap > R(h_here)) {
+                        ecap = h_here > 0.0f ? R(h_here) : R(0);
+                        esrc = h_here > 0.0f ? 2 : 3;
+                    }
+                    if (TAPE) tb |= PGE_TB_POS | (esrc << PGE_TB_ECAP_SHIFT);
+                    if (cdiff * vol_rel > ecap) {
+                        cdiff = ecap / vol_rel;
+                        if (TAPE) tb |= PGE_TB_CLAMP;
+                    }
                 } else if (cdiff < R(0)) {
                     R room = has_hprev ? R(h_prev) - R(h_here) : k_depfloor;
-                    if (room < k_depfloor) room = k_depfloor;
+                    if (TAPE) tb |= PGE_TB_NEG | (has_hprev ? 0 : PGE_TB_ROOM_FLOOR);
+                    if (room < k_depfloor) {
+                        room = k_depfloor;
+                        if (TAPE) tb |= PGE_TB_ROOM_FLOOR;
+                    }
                     const R dcap = room / kexp;
-                    if (-cdiff * vol_rel > dcap) cdiff = -dcap / vol_rel;
+                    if (-cdiff * vol_rel > dcap) {
+                        cdiff = -dcap / vol_rel;
+                        if (TAPE) tb |= PGE_TB_CLAMP;
+                    }
                 }
                 sed += cdiff;
                 en.cell = cv.cell;
@@ -720,11 +854,15 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 en.vol = (float)vol;
                 en.ma = (float)(vol * sa);
                 en.mb = (float)(vol * sb);
+                en.sidx = step;
                 have_entry = true;
             }
             // evaporation (mass conserving)
             R ev = R(1) - k_dt * k_evap * R(cv.evap);
-            if (ev < R(0.01)) ev = R(0.01);
+            if (ev < R(0.01)) {
+                ev = R(0.01);
+                if (TAPE) tb |= PGE_TB_EV_CLAMP;
+            }
             vol *= ev;
             sed /= ev;
             x = nx;
@@ -734,6 +872,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             has_hprev = true;
             cv = nv;
             moved = true;
+            if (TAPE) a.tape.bits[trow * (a.tape.steps + 1) + step] = tb;
             step++;
             // stop conditions
             if (nv.surf < nv.base && !in_sea) {
@@ -753,7 +892,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         if (have_entry) {
             // `cur` still describes the cell the entry was made at
             if (has_pe && LEDGER) {
-                apply_entry(a, t, L, pe, pend, true, cur);
+                apply_entry<TAPE>(a, t, L, pe, pend, true, cur, trow);
                 sync_own(cur, pend);
                 sync_own(nxt, pend);
             }
@@ -829,7 +968,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         }
         if (nout > 0) load_lcell(a, t, ring[0], nxt);
         if (has_pe) {
-            apply_entry(a, t, L, pe, pend, nout > 0, nxt);
+            apply_entry<TAPE>(a, t, L, pe, pend, nout > 0, nxt, trow);
             if (nout > 0) sync_own(nxt, pend);
         }
         for (int r = 0; r < nout; r++) {
@@ -841,7 +980,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             fe.delta = r == 0 ? load : 0.0;
             fe.vol = -1.0f;
             fe.ma = fe.mb = 0.0f;
-            apply_entry(a, t, L, fe, c, more, nxt);
+            fe.sidx = -1;
+            apply_entry<TAPE>(a, t, L, fe, c, more, nxt, trow);
             if (more) sync_own(nxt, c);
             if (a.rec_cell && rec_n < a.rec_cap) {
                 const long long o = (d - a.rec_base) * a.rec_cap + rec_n;
@@ -867,6 +1007,18 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 topend = fx_mass(L.surplus);
             }
             if (topend) red_add(a.pend + L.death, topend);
+        }
+        if (TAPE) {
+            const long long o = trow * (a.tape.steps + 1) + step;
+            double *ts = a.tape.state + o * 6;
+            ts[0] = (double)x;
+            ts[1] = (double)y;
+            ts[2] = (double)sa;
+            ts[3] = (double)sb;
+            ts[4] = (double)sed;
+            ts[5] = (double)vol;
+            a.tape.bits[o] = f;
+            reinterpret_cast<int2 *>(a.tape.count)[trow] = make_int2(step + 1, L.tap_n);
         }
         atomicAdd(&sstat[ST_DROP], 1ull);
         atomicAdd(&sstat[ST_STEPS], (unsigned long long)step_entries(rec_n, nout));

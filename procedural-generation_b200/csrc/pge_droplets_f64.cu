@@ -15,6 +15,17 @@ cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cuda
         f64::droplet_kernel<1, true><<<blocks, threads, 0, st>>>(a);
     return cudaPeekAtLastError();
 }
+cudaError_t launch_droplets_f64_tape(const DropArgs &a, int blocks, int threads, cudaStream_t st)
+{
+    f64::droplet_kernel<1, true, true><<<blocks, threads, 0, st>>>(a);
+    return cudaPeekAtLastError();
+}
+int droplet_blocks_per_sm_f64_tape(int threads)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, true, true>, threads, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
 int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger)
 {
     int n = 0;

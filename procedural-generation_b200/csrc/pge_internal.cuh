@@ -105,6 +105,8 @@ struct DropArgs {
     int8_t *rec_death;
     int rec_cap;
     long long rec_base;  // recorded droplet index = d - rec_base
+    const float *erod;   // per-cell erodibility multiplier, or nullptr (1); read by the ledger variants
+    PgeTape tape;        // the adjoint's record (the taped kernel variant only)
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
@@ -113,6 +115,8 @@ struct DropArgs {
 // launchers of the two precisions (separate translation units: the float64
 // one is compiled without FMA contraction so it rounds like the reference)
 cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+cudaError_t launch_droplets_f64_tape(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+int droplet_blocks_per_sm_f64_tape(int threads);
 cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger = true);
 int droplet_blocks_per_sm_f32(int threads, int minb, bool ledger = true);

@@ -19,6 +19,12 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// the adjoint (pge_adjoint.cu)
+cudaError_t adjoint_pass(const PgeGrid &g, const PgeState &s, const PgeSpawns &sp, const PgeParams &p, const PgeTape &tape,
+                         int carry_path, const double *zbar_after, double *zbar_before, double *ebar, double *pbar,
+                         const Layout &lay, void *ws, cudaStream_t st);
+void adjoint_errors(const Layout &lay, void *ws, PgeStats *stats, cudaStream_t st);
+void halo_adjoint(const PgeHalo &h, double *zbar, cudaStream_t st);
 cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
                        long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st);
 cudaError_t count_pending(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, long long *count_dev, cudaStream_t st);

@@ -26,7 +26,7 @@ EXPORTS = (
     "pge_version", "pge_last_error", "pge_workspace_bytes", "pge_spawn_rain", "pge_count_pending",
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
-    "pge_smooth_step",
+    "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -42,7 +42,7 @@ class PgeGrid(ctypes.Structure):
 
 class PgeState(ctypes.Structure):
     _fields_ = [(n, c_vp) for n in ("height", "sediment", "discharge", "momentum", "pending", "base", "uplift",
-                                    "hardness", "precip", "evap", "mask", "metric", "metric_inv")]
+                                    "hardness", "precip", "evap", "mask", "metric", "metric_inv", "erodibility")]
 
 
 class PgeSpawns(ctypes.Structure):
@@ -69,6 +69,15 @@ class PgeStats(ctypes.Structure):
 
 
 STATS_WORDS = ctypes.sizeof(PgeStats) // 8
+
+
+class PgeTape(ctypes.Structure):
+    _fields_ = [("state", c_vp), ("bits", c_vp), ("entry", c_vp), ("count", c_vp), ("droplets", c_i64), ("steps", c_i32),
+                ("entries", c_i32), ("wave_acc", c_vp), ("waves", c_i64)]
+
+
+#: ledger entries a droplet can make beyond its steps (its final deposits)
+TAPE_EXTRA_ENTRIES = 8
 
 
 class PgeHalo(ctypes.Structure):
@@ -112,6 +121,11 @@ def load(path: str | os.PathLike | None = None):
     L.pge_hold_datum.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_halo_gather.argtypes = [P(PgeHalo), c_vp, c_i32, c_vp]
     L.pge_thermal_noalloc.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_f64, c_f64, c_f64, c_f64, c_f64, c_vp]
+    L.pge_trace_apply_tape.argtypes = [P(PgeGrid), P(PgeState), P(PgeSpawns), P(PgeParams), P(PgeTape), c_vp, c_vp,
+                                       ctypes.c_size_t, c_vp]
+    L.pge_adjoint_pass.argtypes = [P(PgeGrid), P(PgeState), P(PgeSpawns), P(PgeParams), P(PgeTape), c_i32, c_vp, c_vp, c_vp,
+                                   c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]
+    L.pge_halo_adjoint.argtypes = [P(PgeHalo), c_vp, c_vp]
     for n in EXPORTS:
         if n not in ("pge_version", "pge_last_error", "pge_workspace_bytes"):
             getattr(L, n).restype = ctypes.c_int

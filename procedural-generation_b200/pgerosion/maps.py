@@ -83,6 +83,9 @@ class ErosionState:
     _halo: tuple = field(default=None, repr=False)
     _erode_cap: torch.Tensor = field(default=None, repr=False)
     iso_acc: torch.Tensor = field(default=None, repr=False)
+    #: per-cell multiplier of erosion.erodibility (float32, (F, NE, NE)) or None: the calibrated field of the
+    #: adjoint (pgerosion.adjoint); the wave apply only
+    erodibility: torch.Tensor = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -164,7 +167,7 @@ class ErosionState:
         return PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
                         momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
                         hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
-                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv))
+                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility))
 
     def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to
@@ -348,11 +351,16 @@ class SpawnFeeder:
 def run_iteration(state: ErosionState, params, iteration_key, n_particles: int | None = None,
                   particles_per_cell: float | None = None, rng_stage: str = "erosion", log=None, wave: int | None = None,
                   precision: int = _lib.PREC_F64, predrawn=None, threads_per_block: int = 0, blocks_per_sm: int = 0,
-                  events=None, apply: int = _lib.APPLY_ORDERED, trace_lanes: int = 0, apply_lanes: int = 0) -> dict:
+                  events=None, apply: int = _lib.APPLY_ORDERED, trace_lanes: int = 0, apply_lanes: int = 0,
+                  tape=None) -> dict:
     """One particle pass (maps.py:839-1047) on the device; see the module
     docstring.  ``predrawn`` may carry ``draw_spawns``' result for this
     iteration (drawn ahead, host or device arrays); ``events`` a pair of
-    CUDA events recorded around the droplet pass (``pge_trace_apply``)."""
+    CUDA events recorded around the droplet pass (``pge_trace_apply``).
+    ``tape``: a callable ``(n_droplets, max_steps, waves, cells) -> PgeTape``
+    -- the pass then runs as the float64 wave apply, recorded for the
+    adjoint (``pge_trace_apply_tape``); the spawns, parameters and tape are
+    returned under ``stats["adjoint"]``."""
     ep = erosion_group(params)
     check_plain(ep)
     key = iteration_key if isinstance(iteration_key, (tuple, list)) else (int(iteration_key),)
@@ -416,13 +424,23 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     if float(ep.slope_limit_deposit) > 0.0:
         iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     w = default_wave(ep, Ptot) if wave is None else int(wave)
+    if tape is not None:
+        apply, precision, w = _lib.APPLY_WAVE, _lib.PREC_F64, min(w, Ptot)
     prm = make_params(state, ep, volume0, Ptot, w, precision, mom_scale, disc_sat, iter_deposit, threads_per_block, blocks_per_sm,
                       apply, trace_lanes, apply_lanes)
     ecap = _erode_cap(state, ep, prm)
     if events is not None:
         events[0].record()
-    check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), ecap, _ptr(stats_d),
-                            _ptr(ws), ws.numel(), st), "pge_trace_apply")
+    if tape is not None:
+        if ecap is not None:
+            raise ValueError("the adjoint's tape does not cover erosion.slope_limit_erode")
+        tp = tape(Ptot, max_steps, -(-Ptot // w), state.height.numel())
+        check(L.pge_trace_apply_tape(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), ctypes.byref(tp),
+                                     _ptr(stats_d), _ptr(ws), ws.numel(), st), "pge_trace_apply_tape")
+        stats["adjoint"] = {"spawns": PgeSpawns.from_buffer_copy(spawns), "params": PgeParams.from_buffer_copy(prm), "tape": tp}
+    else:
+        check(L.pge_trace_apply(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), ecap, _ptr(stats_d),
+                                _ptr(ws), ws.numel(), st), "pge_trace_apply")
     if events is not None:
         events[1].record()
     hst = sp["host_stats"]
@@ -620,7 +638,7 @@ def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, s
 
 
 def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0: float, n_rain: int | None = None,
-                 wave: int | None = None, precision: int = _lib.PREC_F64, apply: int = _lib.APPLY_ORDERED) -> dict:
+                 wave: int | None = None, precision: int = _lib.PREC_F64, apply: int = _lib.APPLY_ORDERED, tape=None) -> dict:
     """One droplet pass over explicitly given spawns (no random draws): pack,
     waves, apply, fold and EMA, exactly as :func:`run_iteration` does after
     spawning.  ``n_rain`` is the rain count the concurrency divisor is
@@ -646,12 +664,22 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     stats_d = sp["stats"]
     stats_d.zero_()
     ws = state.workspace
-    check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns), ctypes.byref(prm),
-                            ecap, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
+    out = {}
+    if tape is not None:  # the pass recorded for the adjoint (float64 wave apply; see run_iteration)
+        tp = tape(P, max_steps, -(-P // w), state.height.numel())
+        check(L.pge_trace_apply_tape(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns),
+                                     ctypes.byref(prm), ctypes.byref(tp), _ptr(stats_d), _ptr(ws), ws.numel(), _stream()),
+              "pge_trace_apply_tape")
+        out["adjoint"] = {"spawns": PgeSpawns.from_buffer_copy(spawns), "params": PgeParams.from_buffer_copy(prm), "tape": tp}
+    else:
+        check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns),
+                                ctypes.byref(prm), ecap, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
     r = PgeStats.from_buffer_copy(stats_d.cpu().numpy().tobytes())
     if r.errors:
         raise _lib.PgeError("ordered apply: a cell hand-off wait gave up; the pass is invalid")
     fx = _lib.FX_MASS
-    return {"droplets": int(r.droplets), "droplet_steps": int(r.droplet_steps), "entries": int(r.entries), "clamped": int(r.clamped),
-            "deaths": [int(v) for v in r.deaths], "to_pending": r.to_pending_fx / fx, "lost_offshore": r.lost_offshore_fx / fx,
-            "deficit_out": r.deficit_out_fx / fx, "eroded": r.eroded_fx / fx, "deposited": r.deposited_fx / fx}
+    out.update({"droplets": int(r.droplets), "droplet_steps": int(r.droplet_steps), "entries": int(r.entries),
+                "clamped": int(r.clamped), "deaths": [int(v) for v in r.deaths], "to_pending": r.to_pending_fx / fx,
+                "lost_offshore": r.lost_offshore_fx / fx, "deficit_out": r.deficit_out_fx / fx, "eroded": r.eroded_fx / fx,
+                "deposited": r.deposited_fx / fx})
+    return out
