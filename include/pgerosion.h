@@ -27,6 +27,10 @@
  *   pge_uplift            apply_uplift             globe/erosion/maps.py:1088-1147
  *   pge_hold_datum        hold_datum               globe/erosion/maps.py:1446-1508
  *   pge_halo_gather       FaceField.exchange_halos globe/field.py:104-125
+ *   pge_route_flood       ErosionState.refresh_route: the epsilon-filled routing
+ *                         surface (priority_flood_eps)
+ *                                                  globe/erosion/maps.py:351-358,
+ *                                                  globe/erosion/route.py:31-125
  *   pge_trace_apply_tape  pge_trace_apply (wave apply, one wave) recording each
  *                         droplet's steps and ledger branches for the adjoint
  *   pge_adjoint_pass      reverse of one taped droplet pass: gradients of the
@@ -335,6 +339,20 @@ PGE_API int pge_hold_datum(const PgeGrid *g, PgeState *s, double land_fraction, 
 /* Fills the halo rows of one field from its interior: a scalar (F,NE,NE)
  * field, or with vector = 1 a (F,NE,NE,2) field rotated per source. */
 PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, void *stream);
+
+/* The routing surface (route.py:31-125): the surface filled so that every
+ * cell reached from a seed drains by at least eps per cell, as the reference's
+ * priority flood computes it (value for value), with halo cells left at their
+ * surface (refresh them with the linear halo exchange).  Seeds: interior cells
+ * with surface < 0 and surface <= s->base, and (windows) cells next to an
+ * outside or halo cell; s->mask (may be NULL) excludes outside cells; owner is
+ * the (F,NE,NE) int32 owner table (cubesphere.py:664-674; the identity for a
+ * window).  Surface = s->height + s->sediment.  Runs a relaxation to its fixed
+ * point, synchronising the stream every 32 sweeps to test it; *sweeps (host,
+ * may be NULL) gets the sweeps run; PGE_E_UNSUPPORTED if max_sweeps did not
+ * reach the fixed point. */
+PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *owner, double eps, double *route, int64_t max_sweeps,
+                            int64_t *sweeps, void *ws, size_t ws_bytes, void *stream);
 
 /* No counterpart in the reference: the adjoint of the particle pass.
  *

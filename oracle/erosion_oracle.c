@@ -21,7 +21,8 @@
  *   particle.ema_update                  particle.py:1230-1242
  *   particle.spawn_cells                 particle.py:1245-1260
  *
- * Scope: the plain path (no routing surface, no lake parks, no lateral bank
+ * Scope: the plain path with or without the routing surface (particles steer
+ * on it where it stands above the terrain; no lake parks, no lateral bank
  * cut, no roots); masks 0/1/2, windows (spherical = 0) and deposit-on-exit
  * are supported.  Numba types the packed samples as float32 and so computes
  * the stencil differences of _sbilin_grad in float32; the change list keeps
@@ -185,14 +186,14 @@ void orc_transfer_velocity_batch(int64_t n, const int32_t *face, const double *u
 /* ------------------------------------------------------------------------ */
 void orc_pack(int64_t ncell, float *samp, const double *height, const double *sediment, const double *discharge,
               const double *momentum, const float *evap, const float *hardness, const float *metric,
-              const float *metric_inv, const double *base)
+              const float *metric_inv, const double *base, const double *route)
 {
     for (int64_t c = 0; c < ncell; c++) {
         float *s = samp + NS * c;
         double sd = sediment[c];
         double surf = height[c] + sd;
         s[S_SURF] = (float)surf;
-        s[S_ROUTE] = (float)surf;
+        s[S_ROUTE] = (float)(route ? route[c] : surf);
         s[S_DISCH] = (float)discharge[c];
         s[S_MOMA] = (float)momentum[2 * c];
         s[S_MOMB] = (float)momentum[2 * c + 1];
@@ -203,7 +204,8 @@ void orc_pack(int64_t ncell, float *samp, const double *height, const double *se
             s[S_G + k] = metric[3 * c + k];
             s[S_GINV + k] = metric_inv[3 * c + k];
         }
-        s[S_RFLAG] = 0.0f;
+        /* 1 where the routing surface differs from the terrain (particle.py:186-190, no lakes) */
+        s[S_RFLAG] = (route && s[S_ROUTE] != s[S_SURF]) ? 1.0f : 0.0f;
         s[S_BASE] = (float)base[c];
     }
 }
@@ -258,6 +260,18 @@ static inline void sbilin_grad(const Samp *S, int f, double fi, double fj, int c
     *gj = (double)d01 * (1.0 - wi) + (double)d1110 * wi;
 }
 
+/* the routing surface differs from the terrain somewhere in the stencil (particle.py:228-233) */
+static inline int rflag(const Samp *S, int f, double fi, double fj)
+{
+    int i0, j0;
+    double wi, wj;
+    clamp_ij(fi, fj, S->NE, &i0, &j0, &wi, &wj);
+    float sum = cellp(S, f, i0, j0)[S_RFLAG] + cellp(S, f, i0 + 1, j0)[S_RFLAG];
+    sum = sum + cellp(S, f, i0, j0 + 1)[S_RFLAG];
+    sum = sum + cellp(S, f, i0 + 1, j0 + 1)[S_RFLAG];
+    return sum != 0.0f;
+}
+
 static inline double snorm(const float *cp, double a, double b)
 {
     double g0 = cp[S_G], g1 = cp[S_G + 1], g2 = cp[S_G + 2];
@@ -293,6 +307,7 @@ typedef struct {
         disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
         ocean_rate, fan_room, dep_floor;
     int32_t max_steps, pit_steps, ocean_steps, deposit_on_exit, N, H, spherical, F;
+    int32_t use_route, pad;
 } OrcTraceParams;
 
 static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mask, int f, double x, double y,
@@ -346,6 +361,16 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
         double h0, gi, gj;
         sbilin_grad(S, f, fi, fj, S_SURF, &h0, &gi, &gj);
         double h0r = h0;
+        if (P->use_route && rflag(S, f, fi, fj)) {
+            /* steer on the routing surface where it is above the terrain (particle.py:453-460) */
+            double r0, rgi, rgj;
+            sbilin_grad(S, f, fi, fj, S_ROUTE, &r0, &rgi, &rgj);
+            if (r0 > h0) {
+                h0r = r0;
+                gi = rgi;
+                gj = rgj;
+            }
+        }
         double q0 = cp[S_GINV], q1 = cp[S_GINV + 1], q2 = cp[S_GINV + 2];
         double di = q0 * gi + q1 * gj;
         double dj = q1 * gi + q2 * gj;
@@ -405,7 +430,12 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
         double h1 = sbilin(S, nf, nfi, nfj, S_SURF);
         double b1 = np_[S_BASE];
         double dh = h0 - (h1 > b1 ? h1 : b1);
-        double dhr = h0r - h1;
+        double h1r = h1;
+        if (P->use_route && rflag(S, nf, nfi, nfj)) {
+            double r1 = sbilin(S, nf, nfi, nfj, S_ROUTE);
+            if (r1 > h1) h1r = r1;
+        }
+        double dhr = h0r - h1r;
         if (m == MASK_ACTIVE && in_sea) {
             double cdiff = -P->ocean_rate * sed;
             double room = h_prev > -1e300 ? h_prev - (double)h_here : P->fan_room;
@@ -569,7 +599,7 @@ void orc_trace(const OrcTraceParams *P, const float *samp, const uint8_t *mask, 
 /* ------------------------------------------------------------------------ */
 typedef struct {
     double iter_erode, iter_deposit, fan_slope, dep_floor, offshore_writeoff;
-    int32_t use_erode_cap, pad;
+    int32_t use_erode_cap, use_route;
 } OrcApplyParams;
 
 void orc_apply(const OrcApplyParams *A, const int32_t *cl_cell, const double *cl_delta, const float *cl_vol,
@@ -648,6 +678,8 @@ void orc_apply(const OrcApplyParams *A, const int32_t *cl_cell, const double *cl
             samp[c * NS + S_SURF] = (float)s_new;
             double sd = sediment[c] + a2;
             samp[c * NS + S_SED] = (float)(sd > 0.0 ? sd : 0.0);
+            if (A->use_route && samp[c * NS + S_RFLAG] < 1.5f)  /* the route flag follows the live surface */
+                samp[c * NS + S_RFLAG] = samp[c * NS + S_ROUTE] != samp[c * NS + S_SURF] ? 1.0f : 0.0f;
             if (is_step) {
                 if (v > 0.0f) {
                     disch_track[c] += (double)v;

@@ -15,7 +15,9 @@ this module; the product never does.  It drives the C restatement in
 * :func:`hold_datum` -- maps.py:1446-1508
 * :func:`apply_isostasy` -- maps.py:1331-1410 (the Laplace-Beltrami smoother
   of field.py:179-188, 372-404 restated in numpy)
-* :func:`step` -- maps.py:1516-1617, plain path (plus isostasy)
+* :func:`step` -- maps.py:1516-1617, plain path (plus isostasy and the
+  routing surface, :func:`refresh_route` / :func:`priority_flood_eps`,
+  maps.py:351-358 and route.py:31-125)
 
 Every random number comes from ``params.rng("erosion", iteration)`` exactly
 as in the reference, so a GPU run and this oracle see the same spawns.
@@ -79,12 +81,13 @@ class TraceParams(ctypes.Structure):
         "dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
         "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
         "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor")] + [
-        (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F")]
+        (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F",
+                                      "use_route", "pad")]
 
 
 class ApplyParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("iter_erode", "iter_deposit", "fan_slope", "dep_floor", "offshore_writeoff")] + [
-        ("use_erode_cap", ctypes.c_int32), ("pad", ctypes.c_int32)]
+        ("use_erode_cap", ctypes.c_int32), ("use_route", ctypes.c_int32)]
 
 
 def _p(a: np.ndarray):
@@ -156,6 +159,7 @@ class OracleState:
     base: np.ndarray = None
     pending: np.ndarray = None
     iteration: int = 0
+    route: np.ndarray = None  # the epsilon-filled routing surface (refresh_route) or None
     land_target: float | None = None
     deposit_on_exit: bool = False
     samp: np.ndarray = field(default=None, repr=False)
@@ -222,7 +226,7 @@ class OracleState:
         n = self.height.size
         lib().orc_pack(ctypes.c_int64(n), _p(self.samp), _p(self.height), _p(self.sediment), _p(self.discharge),
                        _p(self.momentum), _p(self.evap), _p(self.hardness), _p(self.metric), _p(self.metric_inv),
-                       _p(self.base))
+                       _p(self.base), None if getattr(self, "route", None) is None else _p(self.route))
 
     def exchange_halos(self):
         if not self.spherical:
@@ -293,14 +297,15 @@ def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -
         fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
         deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
-        F=int(state.F))
+        F=int(state.F), use_route=int(getattr(state, "route", None) is not None))
 
 
 def apply_params(state, ep, iter_deposit) -> ApplyParams:
     u = state.height_unit_m
     return ApplyParams(iter_erode=_cu(ep, "iter_erode", u), iter_deposit=float(iter_deposit), fan_slope=float(ep.fan_slope),
                        dep_floor=_cu(ep, "dep_floor_m", u), offshore_writeoff=float(ep.offshore_writeoff),
-                       use_erode_cap=int(float(ep.slope_limit_erode) > 0.0))
+                       use_erode_cap=int(float(ep.slope_limit_erode) > 0.0),
+                       use_route=int(getattr(state, "route", None) is not None))
 
 
 def trace(state, tp: TraceParams, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0):
@@ -506,7 +511,20 @@ def hold_datum(state, land_fraction, level=0.0):
     if q != 0.0:
         state.height -= q
         np.subtract(state.base, q, out=state.base, where=state.base < 0.0)
+        if state.route is not None:  # registered with the terrain (maps.py:1498-1499)
+            state.route -= q
     return q
+
+
+def refresh_route(state, eps):
+    """maps.py:351-358: the routing surface of the current terrain, then the
+    linear halo exchange."""
+    from pgerosion.geometry import exchange_halos as xh
+
+    state.route = priority_flood_eps(state.height + state.sediment, state.mask, state.grid.owner, state.H, state.N, float(eps),
+                                     state.base)
+    if state.spherical:
+        xh(state.grid, state.route, linear=True)
 
 
 def laplacian(state, d):
@@ -611,6 +629,8 @@ def apply_isostasy(state, params) -> dict:
 
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     ep = _ep(params)
+    if int(getattr(ep, "flood_every", 0)) > 0 and (state.route is None or state.iteration % int(ep.flood_every) == 0):
+        refresh_route(state, _cu(ep, "route_eps", state.height_unit_m))  # maps.py:1553-1554
     iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
     if iso:
         if getattr(state, "iso_acc", None) is None:
@@ -628,3 +648,67 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     state.exchange_halos()
     state.iteration += 1
     return st
+
+
+# --------------------------------------------------------------------------
+# routing surface (globe/erosion/route.py:31-125), for the refresh_route tests
+# --------------------------------------------------------------------------
+D8 = ((1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0), (-1, -1), (0, -1), (1, -1))
+
+
+def priority_flood_eps(surface, mask, owner, H, N, eps, base):
+    """The epsilon-filled surface by a heap priority flood, in the
+    reference's order (route.py:31-125): cells outside the mask and on the
+    array border are never entered; seeds are interior cells with
+    surface < 0 and surface <= base, or a D8 neighbour (through ``owner``)
+    outside the mask or not interior; popping the lowest (value, cell), each
+    unvisited neighbour takes max(its surface, value + eps)."""
+    import heapq
+
+    F, NE, _ = surface.shape
+    s = np.asarray(surface, np.float64).reshape(-1)
+    b = np.asarray(base, np.float64).reshape(-1)
+    m = np.asarray(mask).reshape(-1)
+    o = np.asarray(owner, np.int64).reshape(-1)
+    filled = s.copy()
+    visited = np.zeros(s.size, bool)
+    idx = np.arange(s.size).reshape(F, NE, NE)
+    border = np.zeros((F, NE, NE), bool)
+    border[:, 0, :] = border[:, -1, :] = border[:, :, 0] = border[:, :, -1] = True
+    visited[(m == MASK_OUTSIDE) | border.reshape(-1)] = True
+    heap = []
+    for f in range(F):
+        for ei in range(H, H + N):
+            for ej in range(H, H + N):
+                c = int(idx[f, ei, ej])
+                if visited[c]:
+                    continue
+                seed = s[c] < 0.0 and s[c] <= b[c]
+                if not seed:
+                    for di, dj in D8:
+                        n = int(o[idx[f, ei + di, ej + dj]])
+                        if m[n] == MASK_OUTSIDE:
+                            seed = True
+                            break
+                        rem = n % (NE * NE)
+                        if not (H <= rem // NE < H + N and H <= rem % NE < H + N):
+                            seed = True
+                            break
+                if seed:
+                    visited[c] = True
+                    heapq.heappush(heap, (s[c], c))
+    while heap:
+        h, c = heapq.heappop(heap)
+        f, rem = divmod(c, NE * NE)
+        ei, ej = divmod(rem, NE)
+        for di, dj in D8:
+            n = int(o[idx[f, ei + di, ej + dj]])
+            if visited[n]:
+                continue
+            visited[n] = True
+            v = s[n]
+            if v < h + eps:
+                v = h + eps
+            filled[n] = v
+            heapq.heappush(heap, (v, n))
+    return filled.reshape(F, NE, NE)

@@ -509,6 +509,22 @@ PGE_API int pge_adjoint_pass(const PgeGrid *g, const PgeState *s, const PgeSpawn
     return e == cudaSuccess ? PGE_OK : cuda_fail(e, "adjoint_pass");
 }
 
+PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *owner, double eps, double *route, int64_t max_sweeps,
+                            int64_t *sweeps, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay))) return r;
+    if (!s || !s->height || !s->sediment || !s->base || !owner || !route) return fail(PGE_E_ARG, "route_flood: NULL pointer");
+    if (!(eps >= 0.0) || max_sweeps < 1) return fail(PGE_E_ARG, "route_flood: eps must be >= 0 and max_sweeps >= 1");
+    long long done = 0;
+    cudaError_t e = route_flood(*g, *s, owner, eps, route, lay, ws, max_sweeps, &done, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "route_flood");
+    if (sweeps) *sweeps = done;
+    if (done < 0) return fail(PGE_E_UNSUPPORTED, "route_flood: not converged within %lld sweeps", (long long)max_sweeps);
+    return PGE_OK;
+}
+
 PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream)
 {
     if (!h || !zbar || (h->K > 0 && (!h->dst || !h->src || !h->w))) return fail(PGE_E_ARG, "halo_adjoint: NULL pointer");

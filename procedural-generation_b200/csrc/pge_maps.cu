@@ -842,3 +842,117 @@ void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, co
 }
 
 }  // namespace pge
+
+namespace pge {
+
+// ---------------------------------------------------------------------------
+// routing surface: the epsilon-filled surface of a priority flood
+// (globe/erosion/route.py:31-125), as the fixed point of a relaxation.  A cell
+// reached from the seeds takes max(its surface, lowest reaching neighbour + eps);
+// a heap flood reaches every cell first from its lowest reaching neighbour, so
+// the fixed point is the heap flood's result value for value.  Neighbours are
+// pushed to along the owner table (the reference's direction: from a popped cell
+// to owner[its D8 neighbour]); values live as the datum select's order-preserving
+// uint64 keys (okey) so a plain atomicMin keeps the lowest.
+// ---------------------------------------------------------------------------
+namespace {
+enum : unsigned char { RF_EXCLUDED = 0, RF_FREE = 1, RF_SEED = 2 };
+constexpr unsigned long long RF_UNREACHED = 0xFFFFFFFFFFFFFFFFull;
+__constant__ int kRouteD8[8][2] = {{1, 0}, {1, 1}, {0, 1}, {-1, 1}, {-1, 0}, {-1, -1}, {0, -1}, {1, -1}};
+
+}  // namespace
+
+__global__ void route_init_kernel(int F, int NE, int H, int N, const double *__restrict__ h, const double *__restrict__ s,
+                                  const double *__restrict__ base, const uint8_t *__restrict__ mask, const int32_t *__restrict__ owner,
+                                  unsigned long long *key, unsigned char *state)
+{
+    const long long total = (long long)F * NE * NE;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(c / ((long long)NE * NE));
+        const int ei = (int)((c / NE) % NE), ej = (int)(c % NE);
+        const double sv = h[c] + s[c];
+        const bool outside = mask && mask[c] == PGE_MASK_OUTSIDE;
+        if (outside || ei == 0 || ej == 0 || ei == NE - 1 || ej == NE - 1) {
+            state[c] = RF_EXCLUDED;
+            key[c] = okey(sv);
+            continue;
+        }
+        bool seed = false;
+        if (ei >= H && ei < H + N && ej >= H && ej < H + N) {
+            seed = sv < 0.0 && sv <= base[c];
+            for (int k = 0; k < 8 && !seed; k++) {
+                const long long n = owner[((long long)f * NE + ei + kRouteD8[k][0]) * NE + ej + kRouteD8[k][1]];
+                if (mask && mask[n] == PGE_MASK_OUTSIDE) {
+                    seed = true;
+                    break;
+                }
+                const long long rem = n % ((long long)NE * NE);
+                const int nei = (int)(rem / NE), nej = (int)(rem % NE);
+                if (nei < H || nei >= H + N || nej < H || nej >= H + N) seed = true;  // no real neighbour (window edge)
+            }
+        }
+        state[c] = seed ? RF_SEED : RF_FREE;
+        key[c] = seed ? okey(sv) : RF_UNREACHED;
+    }
+}
+
+__global__ void route_push_kernel(int F, int NE, const double *__restrict__ h, const double *__restrict__ s, const int32_t *__restrict__ owner,
+                                  double eps, unsigned long long *key, const unsigned char *__restrict__ state,
+                                  unsigned long long *changed)
+{
+    const long long total = (long long)F * NE * NE;
+    bool any = false;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
+        if (state[c] == RF_EXCLUDED) continue;
+        const unsigned long long kc = ((volatile unsigned long long *)key)[c];
+        if (kc == RF_UNREACHED) continue;
+        const double v = unokey(kc) + eps;
+        const int f = (int)(c / ((long long)NE * NE));
+        const int ei = (int)((c / NE) % NE), ej = (int)(c % NE);
+        for (int k = 0; k < 8; k++) {
+            const long long n = owner[((long long)f * NE + ei + kRouteD8[k][0]) * NE + ej + kRouteD8[k][1]];
+            if (state[n] != RF_FREE) continue;
+            const double sn = h[n] + s[n];
+            const unsigned long long kn = okey(sn > v ? sn : v);
+            if (kn < ((volatile unsigned long long *)key)[n] && atomicMin(key + n, kn) > kn) any = true;
+        }
+    }
+    if (any) *changed = 1ull;
+}
+
+__global__ void route_final_kernel(long long total, const double *__restrict__ h, const double *__restrict__ s,
+                                   const unsigned long long *__restrict__ key, const unsigned char *__restrict__ state, double *route)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total; c += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = key[c];
+        route[c] = (state[c] == RF_EXCLUDED || k == RF_UNREACHED) ? h[c] + s[c] : unokey(k);
+    }
+}
+
+cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *owner, double eps, double *route, const Layout &lay,
+                        void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s)
+{
+    const int NE = g.N + 2 * g.H;
+    const long long n = lay.ncell;
+    unsigned long long *key = ws_ptr<unsigned long long>(ws, lay.cdf);
+    unsigned char *state = ws_ptr<unsigned char>(ws, lay.flags);
+    unsigned long long *changed = ws_ptr<unsigned long long>(ws, lay.counters) + 8;
+    route_init_kernel<<<grid_for(n), 256, 0, s>>>(g.F, NE, g.H, g.N, st.height, st.sediment, st.base, st.mask, owner, key, state);
+    unsigned long long host_changed = 1;
+    long long sweeps = 0;
+    const int batch = 32;  // sweeps between convergence checks (the check synchronises the stream)
+    while (host_changed && sweeps < max_sweeps) {
+        cudaError_t e = cudaMemsetAsync(changed, 0, 8, s);
+        if (e != cudaSuccess) return e;
+        for (int k = 0; k < batch; k++)
+            route_push_kernel<<<grid_for(n), 256, 0, s>>>(g.F, NE, st.height, st.sediment, owner, eps, key, state, changed);
+        sweeps += batch;
+        if ((e = cudaMemcpyAsync(&host_changed, changed, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    }
+    if (sweeps_out) *sweeps_out = host_changed ? -sweeps : sweeps;
+    route_final_kernel<<<grid_for(n), 256, 0, s>>>(n, st.height, st.sediment, key, state, route);
+    return cudaPeekAtLastError();
+}
+
+}  // namespace pge

@@ -19,6 +19,9 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// routing surface (epsilon-filled priority flood); *sweeps_out < 0: not converged within max_sweeps
+cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *owner, double eps, double *route, const Layout &lay,
+                        void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s);
 // the adjoint (pge_adjoint.cu)
 cudaError_t adjoint_pass(const PgeGrid &g, const PgeState &s, const PgeSpawns &sp, const PgeParams &p, const PgeTape &tape,
                          int carry_path, const double *zbar_after, double *zbar_before, double *ebar, double *pbar,

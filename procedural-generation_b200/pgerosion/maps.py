@@ -86,6 +86,9 @@ class ErosionState:
     #: per-cell multiplier of erosion.erodibility (float32, (F, NE, NE)) or None: the calibrated field of the
     #: adjoint (pgerosion.adjoint); the wave apply only
     erodibility: torch.Tensor = field(default=None, repr=False)
+    #: the epsilon-filled routing surface (float64, (F, NE, NE), cell units) or None (refresh_route)
+    route: torch.Tensor = field(default=None, repr=False)
+    _owner: torch.Tensor = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -239,6 +242,29 @@ class ErosionState:
         for t in (self.height, self.sediment, self.discharge):
             check(L.pge_halo_gather(ctypes.byref(h), _ptr(t), 0, st), "pge_halo_gather")
         check(L.pge_halo_gather(ctypes.byref(h), _ptr(self.momentum), 1, st), "pge_halo_gather")
+
+    def owner_table(self) -> torch.Tensor:
+        """int32 flat index of the interior cell owning every extended cell
+        (cubesphere.py:664-674; the identity for a window), on the device."""
+        if self._owner is None:
+            F, NE = self.F, self.N + 2 * self.H
+            own = self.grid.owner if self.spherical else np.arange(F * NE * NE).reshape(F, NE, NE)
+            self._owner = torch.as_tensor(np.ascontiguousarray(own, dtype=np.int32), device=self.height.device)
+        return self._owner
+
+    def refresh_route(self, eps: float, max_sweeps: int = 1 << 22) -> int:
+        """Recompute the routing surface from the current terrain
+        (maps.py:351-358: route.priority_flood_eps, then the linear halo
+        exchange); returns the relaxation sweeps run."""
+        _ensure_workspace(self)
+        if self.route is None or self.route.shape != self.height.shape:
+            self.route = torch.empty_like(self.height)
+        n = ctypes.c_int64(0)
+        check(_lib.load().pge_route_flood(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), _ptr(self.owner_table()),
+                                          float(eps), _ptr(self.route), int(max_sweeps), ctypes.byref(n), _ptr(self.workspace),
+                                          self.workspace.numel(), _stream()), "pge_route_flood")
+        self.exchange_field(self.route, linear=True)
+        return int(n.value)
 
     def n_active_interior(self) -> int:
         if self.mask is None:
@@ -529,7 +555,10 @@ def hold_datum(state: ErosionState, land_fraction: float, level: float = 0.0) ->
     check(L.pge_hold_datum(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), float(land_fraction), float(level),
                            ctypes.c_void_p(scal.data_ptr() + 8), _ptr(state.workspace), state.workspace.numel(), _stream()),
           "pge_hold_datum")
-    return float(scal[1].item())
+    q = float(scal[1].item())
+    if state.route is not None and q != 0.0:  # the routing surface stays registered with the terrain (maps.py:1498-1499)
+        state.route -= q
+    return q
 
 
 def held_land_fraction(state: ErosionState, params) -> float:

@@ -29,6 +29,12 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
 * ``step_tiny.npz`` -- a six-face N=32 world run through the reference
   ``maps.step`` (plain knobs, uplift replay) for a few iterations: the
   initial state, the final state and the per-iteration stats.
+* ``route_flood.npz`` -- the reference's routing flood
+  (``route.priority_flood_eps``) on a six-face N=32 world after two
+  iterations (with one basin given its own base level) and on a one-face
+  window of it.
+* ``step_route.npz`` -- as ``step_tiny.npz`` with the routing surface on
+  (``erosion.flood_every = 2``): particles steer on the flood.
 
 The fixtures are small (well under a few MB) and committed; the tests never
 import the bake.
@@ -323,6 +329,34 @@ def gen_step(cs, maps, pk, WorldParams):
     print("step_tiny:", stats[-1])
 
 
+def gen_step_route(cs, maps, pk, WorldParams):
+    """gen_step with the routing surface on (erosion.flood_every = 2): the
+    reference's maps.step refreshes route.priority_flood_eps before the
+    particle pass and the kernel steers on it."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=7, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    iters = 5
+    p = _world_params(WorldParams, 32, 2, 50.0, 7, 0.45, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", flood_every=2)
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    stats = []
+    routes = []
+    for it in range(iters):
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "to_pending", "released", "pending_total",
+                                         "deficit_out", "lost_offshore", "deaths", "datum_shift")})
+        routes.append(int((st.route > st.height + st.sediment).sum()))
+    np.savez_compressed(HERE / "step_route.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=7, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h_start, height=st.height, sediment=st.sediment, discharge=st.discharge, momentum=st.momentum,
+                        pending=st.pending, route=st.route, stats=json.dumps(stats), **init)
+    print("step_route: cells under the route", routes, stats[-1])
+
+
 def gen_isostasy(cs, maps, pk, WorldParams):
     from pgerosion import synth
 
@@ -346,12 +380,45 @@ def gen_isostasy(cs, maps, pk, WorldParams):
     print("isostasy_tiny:", [x.get("isostasy") for x in stats])
 
 
+def gen_route(cs, maps, pk, WorldParams):
+    """The reference's routing flood (route.priority_flood_eps) on a
+    six-face N=32 world after two reference iterations, and on a window of
+    one of its faces (identity owner, a mask with an outside ring)."""
+    from globe.erosion import route as rt
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=13, N=32, H=2, cell_size_m=50.0, land_fraction=0.35)
+    p = _world_params(WorldParams, 32, 2, 50.0, 13, 0.35, iterations=10, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="stack")
+    st = _ref_state(cs, maps, world, p)
+    for it in range(2):
+        maps.step(st, p, it, n_particles=3000)
+    eps = 0.05 / 50.0
+    surf = st.height + st.sediment
+    base = np.zeros_like(surf)
+    base[:, 8:12, 8:12] = surf[:, 8:12, 8:12].min()  # a basin with its own base level: its low point seeds
+    mask = np.ones(surf.shape, np.uint8)
+    owner = np.ascontiguousarray(st.grid.owner, dtype=np.int64)
+    route = rt.priority_flood_eps(surf, mask, owner, st.H, st.N, eps, base)
+    NE = st.NE
+    wmask = np.zeros((1, NE, NE), np.uint8)
+    wmask[0, 3:NE - 3, 3:NE - 3] = 1
+    wsurf = np.ascontiguousarray(surf[2:3])
+    wowner = rt.window_owner(1, NE)
+    wroute = rt.priority_flood_eps(wsurf, wmask, wowner, st.H, st.N, eps, np.zeros_like(wsurf))
+    np.savez_compressed(HERE / "route_flood.npz", N=32, H=2, eps=eps, height=st.height, sediment=st.sediment, base=base, mask=mask,
+                        owner=owner, route=route, w_height=np.ascontiguousarray(st.height[2:3]),
+                        w_sediment=np.ascontiguousarray(st.sediment[2:3]), w_mask=wmask, w_owner=wowner, w_route=wroute)
+    print(f"route_flood: filled cells {(route > surf).sum()}, window filled {(wroute > wsurf).sum()}")
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
             "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
-            "step": lambda: gen_step(cs, maps, pk, WorldParams)}
+            "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
+            "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

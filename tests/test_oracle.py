@@ -127,3 +127,38 @@ def test_isostasy_steps_match_reference_bit_exact():
         assert s["datum_shift"] == r["datum_shift"], it
     for k in ("height", "sediment", "discharge", "momentum", "pending"):
         assert np.array_equal(getattr(st, k), t[k]), k
+
+
+def test_route_flood_matches_reference_bit_exact():
+    """The oracle's heap flood against the reference's (route.py:31-125),
+    on the sphere (with a basin that has its own base level) and on a window."""
+    fx = np.load(GOLDEN / "route_flood.npz")
+    surf = fx["height"] + fx["sediment"]
+    got = orc.priority_flood_eps(surf, fx["mask"], fx["owner"], int(fx["H"]), int(fx["N"]), float(fx["eps"]), fx["base"])
+    assert got.tobytes() == fx["route"].tobytes()
+    wsurf = fx["w_height"] + fx["w_sediment"]
+    got = orc.priority_flood_eps(wsurf, fx["w_mask"], fx["w_owner"], int(fx["H"]), int(fx["N"]), float(fx["eps"]), np.zeros_like(wsurf))
+    assert got.tobytes() == fx["w_route"].tobytes()
+
+
+def test_routed_steps_match_reference_bit_exact():
+    """Full steps with the routing surface on (erosion.flood_every = 2: the
+    flood refreshed before iterations 0, 2 and 4, particles steering on it,
+    maps.py:1553-1554 and particle.py:453-460, 556-559)."""
+    c = step_case(GOLDEN / "step_route.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(st, c["params"])
+    assert np.array_equal(st.height, t["h_start"])
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == r[k], (it, k)
+        assert s["datum_shift"] == r["datum_shift"]
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        assert np.array_equal(getattr(st, k), t[k]), k
+    # the route's interior bit for bit; its halos come from the linear halo gather, summed in another order (1 ulp)
+    inter = (slice(None), slice(st.H, st.H + st.N), slice(st.H, st.H + st.N))
+    assert np.array_equal(st.route[inter], t["route"][inter])
+    np.testing.assert_allclose(st.route, t["route"], rtol=0, atol=1e-12)
