@@ -138,6 +138,8 @@ typedef struct PgeState {
     const float *metric_inv; /* same shape: inverse metric */
     const float *erodibility; /* (F,NE,NE) per-cell multiplier of erosion.erodibility, or NULL (1 everywhere; the
                                  reference's model): the calibrated field of the adjoint; wave apply only */
+    const double *route;     /* (F,NE,NE) routing surface (pge_route_flood) or NULL: particles steer on it where it
+                                stands above the terrain (particle.py:453-460, 556-559); float64 trace only */
 } PgeState;
 
 /* droplet spawns of one iteration: rain first, then re-injected stockpiles */

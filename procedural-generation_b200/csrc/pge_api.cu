@@ -136,6 +136,7 @@ Layout layout(const PgeGrid &g)
     L.cellB = take(16 * L.ncell);
     L.live = take(16 * L.ncell);
     L.metric8 = take(32 * L.nmetric);
+    L.route2 = take(8 * L.ncell);
     L.acc4 = take(32 * L.ncell);
     L.pend = take(8 * L.ncell);
     if (!g.wave_tables) L.table_slots = 0;  // no own-change tables: ordered apply and map passes only
@@ -204,7 +205,10 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         const int threads = p->threads_per_block ? p->threads_per_block : 256;
         // blocks_per_sm >= 2 selects the kernel variant compiled for two resident blocks per SM
         const int minb = p->blocks_per_sm >= 2 ? 2 : 1;
+        if (s->route && (p->precision != PGE_PREC_F64 || tape))
+            return fail(PGE_E_UNSUPPORTED, "the routing surface needs the float64 trace and no tape");
         int bps = tape ? droplet_blocks_per_sm_f64_tape(threads)
+                  : s->route ? droplet_blocks_per_sm_f64_route(threads, true)
                   : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
         if (p->blocks_per_sm > 0 && p->blocks_per_sm < bps) bps = p->blocks_per_sm;
         long long maxblocks = (long long)sm_count() * bps;
@@ -230,6 +234,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.sp_dir = sp->dir;
         a.volume0 = sp->volume0;
         a.erod = s->erodibility;
+        a.R = s->route ? ws_ptr<float2>(ws, lay.route2) : nullptr;
         if (tape) a.tape = *tape;
         a.p = *p;
         a.acc4 = ws_ptr<long long>(ws, lay.acc4);
@@ -282,6 +287,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.sediment = s->sediment;
             oa.A = ws_ptr<float4>(ws, lay.cellA);
             oa.B = ws_ptr<float4>(ws, lay.cellB);
+            oa.R = s->route ? ws_ptr<float2>(ws, lay.route2) : nullptr;
             oa.mask = s->mask;
             oa.ecap = a.ecap;
             oa.acc4 = ws_ptr<double>(ws, lay.acc4);
@@ -312,7 +318,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);
             const long long rec_warps =
-                (long long)sm_count() * (p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
+                (long long)sm_count() * (s->route ? droplet_blocks_per_sm_f64_route(32, false)
+                                         : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
                                                                       : droplet_blocks_per_sm_f32(32, 1, false));
             int ebits = 1;
             while ((1LL << ebits) <= wave) ebits++;

@@ -233,6 +233,38 @@ __device__ __forceinline__ R bilin(const View &v, int c)
     return R(h00) * (R(1) - wi) * (R(1) - wj) + R(h10) * wi * (R(1) - wj) + R(h01) * (R(1) - wi) * wj + R(h11) * wi * wj;
 }
 
+// The routing surface's bilinear sample (and gradient) at (face, x, y), when
+// any of the stencil's four cells carries the route flag (particle.py:228-233,
+// 196-225); false: the route equals the terrain there and is not sampled.
+__device__ __forceinline__ bool route_sample(const DropArgs &a, int f, R x, R y, bool grad, R &val, R &gi, R &gj)
+{
+    const int NE = a.NE;
+    R fi = x - R(0.5) + R(a.H), fj = y - R(0.5) + R(a.H);
+    int i0 = (int)floor(fi), j0 = (int)floor(fj);
+    if (i0 < 0) i0 = 0;
+    if (i0 > NE - 2) i0 = NE - 2;
+    if (j0 < 0) j0 = 0;
+    if (j0 > NE - 2) j0 = NE - 2;
+    R wi = fi - R(i0), wj = fj - R(j0);
+    if (wi < R(0)) wi = R(0);
+    if (wi > R(1)) wi = R(1);
+    if (wj < R(0)) wj = R(0);
+    if (wj > R(1)) wj = R(1);
+    const long long c00 = ((long long)f * NE + i0) * NE + j0;
+    const float2 r00 = __ldg(a.R + c00), r01 = __ldg(a.R + c00 + 1), r10 = __ldg(a.R + c00 + NE), r11 = __ldg(a.R + c00 + NE + 1);
+    float flag = r00.y + r10.y;
+    flag = flag + r01.y;
+    flag = flag + r11.y;
+    if (flag == 0.0f) return false;
+    val = R(r00.x) * (R(1) - wi) * (R(1) - wj) + R(r10.x) * wi * (R(1) - wj) + R(r01.x) * (R(1) - wi) * wj + R(r11.x) * wi * wj;
+    if (grad) {
+        const float d10 = r10.x - r00.x, d11 = r11.x - r01.x, d01 = r01.x - r00.x, d1110 = r11.x - r10.x;
+        gi = R(d10) * (R(1) - wj) + R(d11) * wj;
+        gj = R(d01) * (R(1) - wi) + R(d1110) * wi;
+    }
+    return true;
+}
+
 __device__ __forceinline__ R snorm(const View &v, R a, R b)
 {
     R n2 = R(v.g0) * a * a + R(2) * R(v.g1) * a * b + R(v.g2) * b * b;
@@ -534,7 +566,8 @@ enum { ST_DROP, ST_STEPS, ST_ENTRIES, ST_CLAMPED, ST_OVER, ST_TOPEND, ST_DEFICIT
        ST_DEATH0, ST_N = ST_DEATH0 + PGE_N_DEATHS };
 
 // TAPE (with LEDGER): also record the adjoint's tape (a.tape, row = the droplet's index in the pass)
-template <int MINB, bool LEDGER, bool TAPE = false>
+// ROUTE: steer on the routing surface a.R where it stands above the terrain
+template <int MINB, bool LEDGER, bool TAPE = false, bool ROUTE = false>
 __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
 {
     const PgeParams &p = a.p;
@@ -675,6 +708,17 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 gi = R(d10) * (R(1) - wj) + R(d11) * wj;
                 gj = R(d01) * (R(1) - wi) + R(d1110) * wi;
             }
+            R h0r = h0;
+            if (ROUTE) {
+                // a lake or pit: steer on the epsilon-filled routing surface where it is above the terrain;
+                // erode on the terrain (particle.py:453-460)
+                R r0, rgi, rgj;
+                if (route_sample(a, f, x, y, true, r0, rgi, rgj) && r0 > h0) {
+                    h0r = r0;
+                    gi = rgi;
+                    gj = rgj;
+                }
+            }
             const R di = R(cv.q0) * gi + R(cv.q1) * gj;
             const R dj = R(cv.q1) * gi + R(cv.q2) * gj;
             R s2 = gi * di + gj * dj;
@@ -754,7 +798,12 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             const R h1 = bilin(nv, 0);
             const R b1 = R(nv.base);
             const R dh = h0 - (h1 > b1 ? h1 : b1);
-            const R dhr = h0 - h1;
+            R h1r = h1;
+            if (ROUTE) {  // particle.py:556-559
+                R r1, unused_i, unused_j;
+                if (route_sample(a, nf, nx, ny, false, r1, unused_i, unused_j) && r1 > h1) h1r = r1;
+            }
+            const R dhr = h0r - h1r;
             if (TAPE && h1 > b1) tb |= PGE_TB_H1_ABOVE;
             // mass transfer at the cell we leave (particle.py:562-671)
             if (m == PGE_MASK_ACTIVE && in_sea) {

@@ -7,6 +7,7 @@
 namespace pge {
 cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st)
 {
+    if (a.R) return launch_droplets_f64_route(a, blocks, threads, st);
     if (!a.ledger)
         f64::droplet_kernel<1, false><<<blocks, threads, 0, st>>>(a);
     else if (a.minb >= 2)
@@ -14,6 +15,22 @@ cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cuda
     else
         f64::droplet_kernel<1, true><<<blocks, threads, 0, st>>>(a);
     return cudaPeekAtLastError();
+}
+cudaError_t launch_droplets_f64_route(const DropArgs &a, int blocks, int threads, cudaStream_t st)
+{
+    if (a.ledger)
+        f64::droplet_kernel<1, true, false, true><<<blocks, threads, 0, st>>>(a);
+    else
+        f64::droplet_kernel<1, false, false, true><<<blocks, threads, 0, st>>>(a);
+    return cudaPeekAtLastError();
+}
+int droplet_blocks_per_sm_f64_route(int threads, bool ledger)
+{
+    int n = 0;
+    const cudaError_t e = ledger ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, true, false, true>, threads, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, false, false, true>, threads, 0);
+    if (e != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
 }
 cudaError_t launch_droplets_f64_tape(const DropArgs &a, int blocks, int threads, cudaStream_t st)
 {

@@ -10,6 +10,8 @@
 //              float64 terrain the ledger applies against
 //   metric8  = two float4 per (face-shared) cell: (g_ii, g_ij, g_jj, ginv_ii),
 //              (ginv_ij, ginv_jj, 0, 0)
+//   route2[c] = float2(routing surface, flag: 1 where it differs from the
+//              cell's packed surface) -- only when the state has a route
 // These are the channels of the reference's packed float32 sample array
 // (bake/globe/erosion/particle.py:146-191) split by access pattern.
 //
@@ -54,7 +56,7 @@ __device__ __forceinline__ void red_add(long long *p, long long v)
 // workspace layout
 // ---------------------------------------------------------------------------
 struct Layout {
-    size_t cellA, cellB, live, metric8, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
+    size_t cellA, cellB, live, metric8, route2, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
         partial, thermal, flags, total;
     // ordered apply (exact mode): one wave's change lists and ranks
     size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_desc, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
@@ -106,6 +108,7 @@ struct DropArgs {
     int rec_cap;
     long long rec_base;  // recorded droplet index = d - rec_base
     const float *erod;   // per-cell erodibility multiplier, or nullptr (1); read by the ledger variants
+    const float2 *R;     // packed routing surface (route, flag) or nullptr: the ROUTE variants steer on it
     PgeTape tape;        // the adjoint's record (the taped kernel variant only)
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
@@ -116,6 +119,8 @@ struct DropArgs {
 // one is compiled without FMA contraction so it rounds like the reference)
 cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 cudaError_t launch_droplets_f64_tape(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+cudaError_t launch_droplets_f64_route(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+int droplet_blocks_per_sm_f64_route(int threads, bool ledger);
 int droplet_blocks_per_sm_f64_tape(int threads);
 cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger = true);

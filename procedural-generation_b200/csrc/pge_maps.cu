@@ -61,7 +61,7 @@ __global__ void pack_metric_kernel(long long n, const float *__restrict__ g, con
 // between waves: the packed surface / sediment and the ledger's wave-start
 // change follow the net change so far (apply_changes' samp sync, particle.py:1005-1009)
 __global__ void refresh_kernel(long long ncell, const double *__restrict__ s, const long long *__restrict__ acc4, float4 *A,
-                               float4 *B, double2 *L)
+                               float4 *B, double2 *L, float2 *R)
 {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
         const double a = (double)acc4[4 * c] * INV_FX_MASS;
@@ -69,9 +69,21 @@ __global__ void refresh_kernel(long long ncell, const double *__restrict__ s, co
         if (l.y == a) continue;  // unchanged since the last refresh
         l.y = a;
         L[c] = l;
-        A[c].x = (float)(l.x + a);
+        const float surf = (float)(l.x + a);
+        A[c].x = surf;
         const double sd = s[c] + a;
         B[c].z = (float)(sd > 0.0 ? sd : 0.0);
+        if (R) R[c].y = R[c].x != surf ? 1.0f : 0.0f;  // the route flag follows the live surface (particle.py:1010-1012)
+    }
+}
+
+// the routing surface and its flag, beside the packed surface (particle.py:165-190, no lakes)
+__global__ void pack_route_kernel(long long ncell, const double *__restrict__ h, const double *__restrict__ s,
+                                  const double *__restrict__ route, float2 *R)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const float r = (float)route[c], surf = (float)(h[c] + s[c]);
+        R[c] = make_float2(r, r != surf ? 1.0f : 0.0f);
     }
 }
 
@@ -149,13 +161,14 @@ void pack(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, cuda
                                              ws_ptr<float4>(ws, lay.cellA), ws_ptr<float4>(ws, lay.cellB),
                                              ws_ptr<double2>(ws, lay.live));
     pack_metric_kernel<<<grid_for(lay.nmetric), 256, 0, st>>>(lay.nmetric, s.metric, s.metric_inv, ws_ptr<float4>(ws, lay.metric8));
+    if (s.route) pack_route_kernel<<<grid_for(n), 256, 0, st>>>(n, s.height, s.sediment, s.route, ws_ptr<float2>(ws, lay.route2));
 }
 
 void refresh(const PgeState &s, const Layout &lay, void *ws, cudaStream_t st)
 {
     refresh_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.sediment, ws_ptr<long long>(ws, lay.acc4),
                                                        ws_ptr<float4>(ws, lay.cellA), ws_ptr<float4>(ws, lay.cellB),
-                                                       ws_ptr<double2>(ws, lay.live));
+                                                       ws_ptr<double2>(ws, lay.live), s.route ? ws_ptr<float2>(ws, lay.route2) : nullptr);
 }
 
 void fold_ema(PgeState &s, const Layout &lay, void *ws, double ema, int exact, cudaStream_t st)

@@ -566,9 +566,11 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
         const double acc = hand_acc(hw[0], hw[1]);
         accp[0] = acc;
         if (active) {
-            a.A[c].x = (float)(a.L[c].x + acc);
+            const float surf = (float)(a.L[c].x + acc);
+            a.A[c].x = surf;
             const double sd = a.sediment[c] + acc;
             a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
+            if (a.R) a.R[c].y = a.R[c].x != surf ? 1.0f : 0.0f;  // the route flag follows the live surface
         }
     }
     if (eroded) atomicAdd(&sfx[0], (unsigned long long)eroded);

@@ -38,6 +38,7 @@ struct OrderedArgs {
     const double *sediment;
     float4 *A;
     float4 *B;
+    float2 *R;  // packed routing surface (route, flag) or nullptr: flags follow the live surface
     const uint8_t *mask;
     const double *ecap;
     // per cell: the live net change and the hand-off counter, one 16-byte word

@@ -121,6 +121,8 @@ def calib_step(state: ErosionState, params, iteration_key, n_particles: int, tap
     check_plain(ep)
     if state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0:
         raise ValueError("the calibration path has no isostasy (erosion.isostasy = 0)")
+    if int(getattr(ep, "flood_every", 0)) > 0 or state.route is not None:
+        raise ValueError("the calibration path has no routing surface (erosion.flood_every = 0)")
     st = run_iteration(state, params, iteration_key, n_particles=n_particles, apply=_lib.APPLY_WAVE, wave=wave, tape=tape)
     thermal_erosion(state, params)
     apply_uplift(state, uplift_cap(state, ep))

@@ -170,7 +170,8 @@ class ErosionState:
         return PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
                         momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
                         hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
-                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility))
+                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility),
+                        route=_ptr(self.route))
 
     def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to
@@ -592,6 +593,11 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     exchange; increments ``state.iteration``."""
     ep = erosion_group(params)
     t0 = time.time()
+    flood = int(getattr(ep, "flood_every", 0))
+    if flood > 0 and (state.route is None or state.iteration % flood == 0):
+        # the routing surface the particles steer on (maps.py:1553-1554)
+        state.refresh_route(cell_units(ep, "route_eps", state.height_unit_m))
+    t_route = time.time()
     iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
     if iso:
         if state.iso_acc is None:
@@ -612,8 +618,8 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
         st["datum_shift"] = hold_datum(state, held_land_fraction(state, params))
     state.exchange_halos()
     state.iteration += 1
-    st["seconds_route"] = 0.0
-    st["seconds_particles"] = t1 - t0
+    st["seconds_route"] = t_route - t0
+    st["seconds_particles"] = t1 - t_route
     st["seconds_total"] = time.time() - t0
     return st
 

@@ -190,11 +190,9 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (routing surface, lakes, glacial pass, ice, lateral cut).  Isostasy
-    is supported (on the sphere)."""
+    path (sea mask, lakes, glacial pass, ice, lateral cut, basin fill).
+    Isostasy and the routing surface (``flood_every``) are supported."""
     bad = []
-    if int(getattr(ep, "flood_every", 0)) > 0:
-        bad.append("flood_every")
     if int(getattr(ep, "sea_mask_every", 0)) > 0:
         bad.append("sea_mask_every")
     if bool(getattr(ep, "lake_balance", False)):

@@ -80,3 +80,100 @@ def test_refresh_route_on_a_state(cuda):
     q = gm.hold_datum(st, 0.5)
     assert q != 0.0
     torch.testing.assert_close(st.route, r0 - q, rtol=0, atol=0)
+
+
+def test_routed_ordered_pass_matches_oracle(cuda):
+    """One exact (ordered) pass with particles steering on the routing
+    surface (particle.py:453-460, 556-559; the route flags following the live
+    surface, particle.py:1010-1012) against the oracle's chunked serial pass
+    on the same spawns, start terrain and route -- to the tolerance of the
+    plain pass's parity test -- and the route changes the pass."""
+    import torch
+
+    from oracle import oracle as orc
+    from pgerosion import maps as gm
+    from tests.parity_cases import GOLDEN, step_case
+
+    c = step_case(GOLDEN / "step_route.npz")
+    ep = c["params"].erosion
+    o = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(o, c["params"])
+    eps = float(ep.route_eps) / o.height_unit_m
+    orc.refresh_route(o, eps)
+    f, x, y, v0 = orc.spawn_particles(o, c["n_particles"], c["params"].rng("erosion", 0))
+    P = len(f)
+    z = np.zeros(P)
+    g = gm.ErosionState.from_world(c["world"])
+    g.height.copy_(torch.as_tensor(o.height))
+    g.route = torch.as_tensor(o.route.copy(), device="cuda")
+    s = gm.apply_spawns(g, c["params"], f, x, y, z, z, v0)
+    chunk = orc.chunk_size(ep, P)
+    o.pack()
+    o.acc[...] = 0.0
+    tp = orc.trace_params(o, ep, v0, chunk / (v0 * P))
+    ap = orc.apply_params(o, ep, ep.iter_deposit / o.height_unit_m)
+    cap = orc.change_list_cap(tp.max_steps)
+    clamped = 0
+    for c0 in range(0, P, chunk):
+        cl = orc.trace(o, tp, f[c0:c0 + chunk], x[c0:c0 + chunk], y[c0:c0 + chunk], z[c0:c0 + chunk], z[c0:c0 + chunk], v0)
+        clamped += orc.apply(o, ap, cl, cap)[0]
+    import ctypes
+
+    lib = orc.lib()
+    lib.orc_fold(ctypes.c_int64(o.height.size), orc._p(o.height), orc._p(o.sediment), orc._p(o.acc), orc._p(o.mask))
+    lib.orc_ema(ctypes.c_int64(o.height.size), orc._p(o.discharge), orc._p(o.momentum), orc._p(o.disch_track), orc._p(o.mom_track),
+                orc._p(o.mask), ctypes.c_double(float(ep.ema)))
+    a = g.to_numpy()
+    # a few trajectories differ in their last bits (libm: the face transfer, the discharge power), which
+    # can flip a branch downstream; every other cell within the plain pass's tolerance
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        off = ~np.isclose(a[k], getattr(o, k), rtol=1e-5, atol=1e-8)
+        assert off.mean() <= 1e-3 and np.abs(a[k] - getattr(o, k)).max() <= 1e-3, (k, int(off.sum()))
+    assert np.mean(a["height"] == o.height) > 0.99
+    assert abs(s["clamped"] - clamped) <= 1e-3 * clamped, (s["clamped"], clamped)
+    # without the route the same pass ends elsewhere
+    g2 = gm.ErosionState.from_world(c["world"])
+    o2 = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(o2, c["params"])
+    g2.height.copy_(torch.as_tensor(o2.height))
+    gm.apply_spawns(g2, c["params"], f, x, y, z, z, v0)
+    assert not np.array_equal(g2.to_numpy()["height"], a["height"])
+
+
+def test_routed_steps_follow_the_reference(cuda):
+    """maps.step with erosion.flood_every = 2 (the flood refreshed before
+    iterations 0, 2 and 4): the hypsometry within the chaotic bound of the
+    reference's own routed run, the routing surface of the final terrain
+    bit-identical to the oracle's flood of it, and the mass balance of a
+    routed pass."""
+    from oracle import oracle as orc
+    from pgerosion import maps as gm
+    from tests.parity_cases import GOLDEN, hypsometry, step_case
+    from tests.test_gpu_parity import HYPS_TOL_MANY, _mass_balance
+
+    c = step_case(GOLDEN / "step_route.npz")
+    t = c["t"]
+    ep = c["params"].erosion
+    g = gm.ErosionState.from_world(c["world"])
+    gm.start_replay(g, c["params"])
+    inter = g.interior
+    for it in range(c["iterations"]):
+        refresh = it % int(ep.flood_every) == 0
+        s = gm.step(g, c["params"], it, n_particles=c["n_particles"])
+        if refresh:
+            assert s["seconds_route"] > 0.0
+        assert g.route is not None
+    a = g.to_numpy()
+    hg = hypsometry(a["height"], a["sediment"], inter, 50.0)
+    hr = hypsometry(t["height"], t["sediment"], inter, 50.0)
+    assert np.abs(hg - hr).max() <= HYPS_TOL_MANY, (hg, hr)
+    # the route of the final terrain against the oracle's flood of it
+    g.refresh_route(float(ep.route_eps) / g.height_unit_m)
+    surf = a["height"] + a["sediment"]
+    want = orc.priority_flood_eps(surf, np.ones(surf.shape, np.uint8), g.grid.owner, g.H, g.N, float(ep.route_eps) / g.height_unit_m,
+                                  g.base.cpu().numpy())
+    assert g.route.cpu().numpy()[inter].tobytes() == want[inter].tobytes()
+    # mass balance of one more routed pass
+    m0 = g.total_mass()
+    s = gm.run_iteration(g, c["params"], c["iterations"], n_particles=c["n_particles"])
+    _mass_balance(s, m0, g.total_mass())
