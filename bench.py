@@ -380,6 +380,16 @@ def run_b200(args, rank, world_size, dist):
         batched = run_batched(args, rank, world_size, dist, dev)
     if rank != 0:
         return None
+    # the routing surface of the evolved N_c = 1024 terrain (erosion.flood_every's refresh), CUDA-event timed
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sweeps = st.refresh_route(float(params.erosion.route_eps) / st.height_unit_m)
+    e1.record()
+    e1.synchronize()
+    surf = st.height + st.sediment
+    route_flood = {"what": "epsilon-filled routing surface (pge_route_flood + linear halo exchange) of the evolved world",
+                   "ms": e0.elapsed_time(e1), "sweeps": sweeps, "filled_cells": int((st.route > surf).sum().item())}
+    st.route = None
     adjoint = None
     if not args.no_adjoint:
         adjoint = run_adjoint(args, dev)
@@ -417,6 +427,7 @@ def run_b200(args, rank, world_size, dist):
         out["batched_worlds"] = batched
     if adjoint is not None:
         out["adjoint"] = adjoint
+    out["route_flood"] = route_flood
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
