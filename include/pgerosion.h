@@ -31,6 +31,11 @@
  *                         surface (priority_flood_eps)
  *                                                  globe/erosion/maps.py:351-358,
  *                                                  globe/erosion/route.py:31-125
+ *   pge_sea_base          ErosionState.refresh_base: the base level of closed
+ *                         below-sea basins (the sea mask)
+ *                                                  globe/erosion/maps.py:360-420,
+ *                                                  globe/hydro/run.py:64-83,
+ *                                                  globe/hydro/lakes.py:19-46
  *   pge_trace_apply_tape  pge_trace_apply (wave apply, one wave) recording each
  *                         droplet's steps and ledger branches for the adjoint
  *   pge_adjoint_pass      reverse of one taped droplet pass: gradients of the
@@ -355,6 +360,24 @@ PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, voi
  * reach the fixed point. */
 PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *owner, double eps, double *route, int64_t max_sweeps,
                             int64_t *sweeps, void *ws, size_t ws_bytes, void *stream);
+
+/* The sea mask (maps.py:360-420): interior cells whose float32 surface
+ * (s->height + s->sediment) is below 0 are joined into 8-connected
+ * components through the owner table (int32, (F,NE,NE)); a component whose
+ * area (area: (F,N,N) float32 interior cell areas, summed in float64)
+ * reaches min_area is open ocean, and so is the largest; every other one is
+ * a closed basin, whose cells get the basin's lowest surface as their base
+ * level.  Writes base (F,NE,NE): that floor on closed-basin cells, 0 on the
+ * rest of the interior and on the halos (copy each halo cell from its
+ * nearest interior source afterwards, as the reference does); labels (may be
+ * NULL) gets (F,N,N) int32 component ids (the lowest cell id of the
+ * component, -1 above the waterline).  Components are joined along the
+ * owner relation taken both ways (the reference walks it one way from each
+ * component's lowest cell; they differ only where a cube corner's halo
+ * mapping is one-sided).  Synchronises the stream every 16 sweeps; spherical
+ * grids only. */
+PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
+                         int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream);
 
 /* No counterpart in the reference: the adjoint of the particle pass.
  *

@@ -15,9 +15,10 @@ this module; the product never does.  It drives the C restatement in
 * :func:`hold_datum` -- maps.py:1446-1508
 * :func:`apply_isostasy` -- maps.py:1331-1410 (the Laplace-Beltrami smoother
   of field.py:179-188, 372-404 restated in numpy)
-* :func:`step` -- maps.py:1516-1617, plain path (plus isostasy and the
+* :func:`step` -- maps.py:1516-1617, plain path (plus isostasy, the
   routing surface, :func:`refresh_route` / :func:`priority_flood_eps`,
-  maps.py:351-358 and route.py:31-125)
+  maps.py:351-358 and route.py:31-125, and the sea mask,
+  :func:`refresh_base`, maps.py:360-420 with hydro/run.py:64-83)
 
 Every random number comes from ``params.rng("erosion", iteration)`` exactly
 as in the reference, so a GPU run and this oracle see the same spawns.
@@ -160,6 +161,7 @@ class OracleState:
     pending: np.ndarray = None
     iteration: int = 0
     route: np.ndarray = None  # the epsilon-filled routing surface (refresh_route) or None
+    base_at: int = None  # iteration of the last sea-mask refresh (refresh_base)
     land_target: float | None = None
     deposit_on_exit: bool = False
     samp: np.ndarray = field(default=None, repr=False)
@@ -627,8 +629,91 @@ def apply_isostasy(state, params) -> dict:
             "rebound_max": float((f[state.interior] - mean).max()), "rebound_min": float((f[state.interior] - mean).min())}
 
 
+def interior_cell_area(grid) -> np.ndarray:
+    """(6, N, N) float32 cell areas in m^2 (cubesphere.py:505-517: the
+    float32 sqrt det g times the cell size squared, rounded to float32)."""
+    g = grid.metric_face.astype(np.float64)
+    sq = np.sqrt(g[..., 0] * g[..., 2] - g[..., 1] ** 2).astype(np.float32)
+    a = (sq.astype(np.float64) * float(grid.cell_size_m) ** 2).astype(np.float32)
+    H, N = grid.H, grid.N
+    return np.broadcast_to(a[H:H + N, H:H + N], (6, N, N)).copy()
+
+
+def below_sea_components(surf32, grid, min_fraction):
+    """hydro/run.py:64-83 with hydro/lakes.py:19-46: the interior cells
+    under the waterline, their 8-connected components (a walk from the
+    lowest unlabelled cell along the owner table's D8 neighbours), and which
+    components are open ocean (area >= min_fraction of the globe, and the
+    largest)."""
+    N, H = grid.N, grid.H
+    NE = N + 2 * H
+    below = (np.asarray(surf32) < 0.0).reshape(-1)
+    if not below.any():
+        return below, None, None
+    owner = grid.owner.reshape(-1)
+    labels = np.full(below.size, -1, np.int32)
+    n = 0
+    for s0 in range(below.size):
+        if not below[s0] or labels[s0] >= 0:
+            continue
+        labels[s0] = n
+        stack = [s0]
+        while stack:
+            c = stack.pop()
+            f, rem = divmod(c, N * N)
+            i, j = divmod(rem, N)
+            for di, dj in D8:
+                o = int(owner[(f * NE + i + H + di) * NE + j + H + dj])
+                f2, r2 = divmod(o, NE * NE)
+                q = (f2 * N + r2 // NE - H) * N + r2 % NE - H
+                if below[q] and labels[q] < 0:
+                    labels[q] = n
+                    stack.append(q)
+        n += 1
+    area = interior_cell_area(grid).reshape(-1).astype(np.float64)
+    per = np.bincount(labels[below], weights=area[below], minlength=max(n, 1))
+    keep = per >= float(min_fraction) * float(area.sum())
+    keep[int(np.argmax(per))] = True
+    return below, labels, keep
+
+
+def refresh_base(state, min_fraction) -> dict:
+    """maps.py:360-420: the base level -- 0 on the open ocean and on land,
+    a closed below-sea basin's deepest surface on its cells; halos copied
+    from their nearest interior source."""
+    base = np.zeros_like(state.height)
+    info = {"closed_cells": 0, "closed_basins": 0, "sea_cells": 0, "deepest_basin_floor": 0.0}
+    inter = state.interior
+    surf = (state.height[inter] + state.sediment[inter]).astype(np.float64)
+    below, labels, keep = below_sea_components(surf.astype(np.float32), state.grid, float(min_fraction))
+    if labels is not None:
+        sea = below & keep[np.maximum(labels, 0)]
+        closed = below & ~sea
+        info["sea_cells"] = int(sea.sum())
+        info["closed_cells"] = int(closed.sum())
+        if closed.any():
+            lab = labels[closed]
+            floor = np.zeros(keep.size, dtype=np.float64)
+            np.minimum.at(floor, lab, surf.reshape(-1)[closed])
+            inner = np.zeros(surf.size, dtype=np.float64)
+            inner[closed] = floor[lab]
+            base[inter] = inner.reshape(surf.shape)
+            info["closed_basins"] = int(np.unique(lab).size)
+            info["deepest_basin_floor"] = float(floor.min())
+    hm = state.grid.halo
+    flat = base.reshape(-1, 1)
+    flat[hm.dst] = flat[hm.nearest]
+    state.base = base
+    state.base_at = state.iteration
+    return info
+
+
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     ep = _ep(params)
+    sea_every = int(getattr(ep, "sea_mask_every", 0))
+    st_base = None
+    if state.spherical and sea_every > 0 and (state.base_at is None or state.iteration % sea_every == 0):
+        st_base = refresh_base(state, OCEAN_MIN_FRACTION)  # maps.py:1546-1551, before the route
     if int(getattr(ep, "flood_every", 0)) > 0 and (state.route is None or state.iteration % int(ep.flood_every) == 0):
         refresh_route(state, _cu(ep, "route_eps", state.height_unit_m))  # maps.py:1553-1554
     iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
@@ -647,7 +732,13 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
         st["datum_shift"] = hold_datum(state, state.land_target)
     state.exchange_halos()
     state.iteration += 1
+    if st_base is not None:
+        st["sea"] = st_base
     return st
+
+
+#: hydro.ocean_min_fraction, the bake's default (the share of the globe a below-sea body needs to be open ocean)
+OCEAN_MIN_FRACTION = 0.02
 
 
 # --------------------------------------------------------------------------

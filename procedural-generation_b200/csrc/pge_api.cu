@@ -532,6 +532,23 @@ PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *
     return PGE_OK;
 }
 
+PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
+                         int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay))) return r;
+    if (!g->spherical) return fail(PGE_E_UNSUPPORTED, "sea_base: the sea mask is a global (spherical) pass");
+    if (!s || !s->height || !s->sediment || !owner || !area || !base) return fail(PGE_E_ARG, "sea_base: NULL pointer");
+    if (max_sweeps < 1) return fail(PGE_E_ARG, "sea_base: max_sweeps must be >= 1");
+    long long done = 0;
+    cudaError_t e = sea_base(*g, *s, owner, area, min_area, base, labels, lay, ws, max_sweeps, &done, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "sea_base");
+    if (sweeps) *sweeps = done;
+    if (done < 0) return fail(PGE_E_UNSUPPORTED, "sea_base: labelling not converged within %lld sweeps", (long long)max_sweeps);
+    return PGE_OK;
+}
+
 PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream)
 {
     if (!h || !zbar || (h->K > 0 && (!h->dst || !h->src || !h->w))) return fail(PGE_E_ARG, "halo_adjoint: NULL pointer");

@@ -968,4 +968,136 @@ cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *own
     return cudaPeekAtLastError();
 }
 
+// ---------------------------------------------------------------------------
+// sea mask: the base level (maps.py:360-420, hydro/run.py:64-83).  Interior
+// cells under the waterline (float32 surface < 0) are joined into
+// 8-connected components along the owner table (labels: the component's
+// lowest cell id, by min-label propagation with pointer jumping); a component
+// is open ocean when its area reaches min_area, and the largest always is;
+// the others are closed basins, whose cells take the basin's lowest surface.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ long long sea_ext(long long c, int N, int H, int NE)
+{
+    const long long f = c / ((long long)N * N), rem = c % ((long long)N * N);
+    return (f * NE + rem / N + H) * NE + rem % N + H;
+}
+__device__ __forceinline__ long long sea_nb(const int32_t *owner, long long c, int k, int N, int H, int NE)
+{
+    const long long f = c / ((long long)N * N), rem = c % ((long long)N * N);
+    const long long o = owner[(f * NE + rem / N + H + kRouteD8[k][0]) * NE + rem % N + H + kRouteD8[k][1]];
+    const long long f2 = o / ((long long)NE * NE), r2 = o % ((long long)NE * NE);
+    return (f2 * N + r2 / NE - H) * N + r2 % NE - H;
+}
+}  // namespace
+
+__global__ void sea_init_kernel(long long M, int N, int H, int NE, const double *__restrict__ h, const double *__restrict__ s,
+                                int32_t *label, double *per, unsigned long long *floorkey)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+        const long long e = sea_ext(c, N, H, NE);
+        label[c] = (float)(h[e] + s[e]) < 0.0f ? (int32_t)c : -1;
+        per[c] = 0.0;
+        floorkey[c] = okey(0.0);  // the basin floor starts at 0 (maps.py: np.zeros, then np.minimum.at)
+    }
+}
+
+__global__ void sea_join_kernel(long long M, int N, int H, int NE, const int32_t *__restrict__ owner, int32_t *label,
+                                unsigned long long *changed)
+{
+    bool any = false;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+        const int l = ((volatile int32_t *)label)[c];
+        if (l < 0) continue;
+        int m = l;
+        const int ll = ((volatile int32_t *)label)[l];  // pointer jumping: the label of the label
+        if (ll >= 0 && ll < m) m = ll;
+        long long nb[8];
+        for (int k = 0; k < 8; k++) {
+            nb[k] = sea_nb(owner, c, k, N, H, NE);
+            const int lq = ((volatile int32_t *)label)[nb[k]];
+            if (lq >= 0 && lq < m) m = lq;
+        }
+        if (m < l && atomicMin(label + c, m) > m) any = true;
+        for (int k = 0; k < 8; k++) {
+            const int lq = ((volatile int32_t *)label)[nb[k]];
+            if (lq > m && atomicMin(label + nb[k], m) > m) any = true;
+        }
+    }
+    if (any) *changed = 1ull;
+}
+
+__global__ void sea_stats_kernel(long long M, int N, int H, int NE, const double *__restrict__ h, const double *__restrict__ s,
+                                 const float *__restrict__ area, const int32_t *__restrict__ label, double *per,
+                                 unsigned long long *floorkey)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+        const int l = label[c];
+        if (l < 0) continue;
+        const long long e = sea_ext(c, N, H, NE);
+        atomicAdd(per + l, (double)area[c]);
+        atomicMin(floorkey + l, okey(h[e] + s[e]));
+    }
+}
+
+__global__ void sea_largest_kernel(long long M, const int32_t *__restrict__ label, const double *__restrict__ per,
+                                   unsigned long long *maxkey, unsigned long long *largest, int pass)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < M; c += (long long)gridDim.x * blockDim.x) {
+        if (label[c] != (int32_t)c) continue;  // one root per component
+        const unsigned long long k = okey(per[c]);
+        if (pass == 0) atomicMax(maxkey, k);
+        else if (k == *maxkey) atomicMin(largest, (unsigned long long)c);  // np.argmax: the first (lowest) component
+    }
+}
+
+__global__ void sea_base_kernel(long long total, int N, int H, int NE, const int32_t *__restrict__ label, const double *__restrict__ per,
+                                const unsigned long long *__restrict__ floorkey, const unsigned long long *__restrict__ largest,
+                                double min_area, double *base)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total; e += (long long)gridDim.x * blockDim.x) {
+        const long long f = e / ((long long)NE * NE), rem = e % ((long long)NE * NE);
+        const int ei = (int)(rem / NE), ej = (int)(rem % NE);
+        double b = 0.0;
+        if (ei >= H && ei < H + N && ej >= H && ej < H + N) {
+            const long long c = (f * N + ei - H) * N + ej - H;
+            const int l = label[c];
+            if (l >= 0 && (unsigned long long)l != *largest && !(per[l] >= min_area)) b = unokey(floorkey[l]);
+        }
+        base[e] = b;
+    }
+}
+
+cudaError_t sea_base(const PgeGrid &g, const PgeState &st, const int32_t *owner, const float *area, double min_area, double *base,
+                     int32_t *label_out, const Layout &lay, void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s)
+{
+    const int N = g.N, H = g.H, NE = N + 2 * H;
+    const long long M = (long long)g.F * N * N;
+    int32_t *label = label_out ? label_out : ws_ptr<int32_t>(ws, lay.flags);
+    double *per = ws_ptr<double>(ws, lay.cdf);
+    unsigned long long *floorkey = reinterpret_cast<unsigned long long *>(per + M);
+    unsigned long long *cnt = ws_ptr<unsigned long long>(ws, lay.counters);
+    unsigned long long *changed = cnt + 9, *maxkey = cnt + 10, *largest = cnt + 11;
+    sea_init_kernel<<<grid_for(M), 256, 0, s>>>(M, N, H, NE, st.height, st.sediment, label, per, floorkey);
+    unsigned long long host_changed = 1;
+    long long sweeps = 0;
+    cudaError_t e;
+    while (host_changed && sweeps < max_sweeps) {
+        if ((e = cudaMemsetAsync(changed, 0, 8, s)) != cudaSuccess) return e;
+        for (int k = 0; k < 16; k++) sea_join_kernel<<<grid_for(M), 256, 0, s>>>(M, N, H, NE, owner, label, changed);
+        sweeps += 16;
+        if ((e = cudaMemcpyAsync(&host_changed, changed, 8, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    }
+    if (sweeps_out) *sweeps_out = host_changed ? -sweeps : sweeps;
+    sea_stats_kernel<<<grid_for(M), 256, 0, s>>>(M, N, H, NE, st.height, st.sediment, area, label, per, floorkey);
+    if ((e = cudaMemsetAsync(maxkey, 0, 8, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(largest, 0xFF, 8, s)) != cudaSuccess) return e;
+    sea_largest_kernel<<<grid_for(M), 256, 0, s>>>(M, label, per, maxkey, largest, 0);
+    sea_largest_kernel<<<grid_for(M), 256, 0, s>>>(M, label, per, maxkey, largest, 1);
+    sea_base_kernel<<<grid_for(lay.ncell), 256, 0, s>>>(lay.ncell, N, H, NE, label, per, floorkey, largest, min_area, base);
+    return cudaPeekAtLastError();
+}
+
 }  // namespace pge
+

@@ -22,6 +22,9 @@ size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
 // routing surface (epsilon-filled priority flood); *sweeps_out < 0: not converged within max_sweeps
 cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *owner, double eps, double *route, const Layout &lay,
                         void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s);
+// sea mask: base level of closed below-sea basins; *sweeps_out < 0: the labelling did not converge
+cudaError_t sea_base(const PgeGrid &g, const PgeState &st, const int32_t *owner, const float *area, double min_area, double *base,
+                     int32_t *label_out, const Layout &lay, void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s);
 // the adjoint (pge_adjoint.cu)
 cudaError_t adjoint_pass(const PgeGrid &g, const PgeState &s, const PgeSpawns &sp, const PgeParams &p, const PgeTape &tape,
                          int carry_path, const double *zbar_after, double *zbar_before, double *ebar, double *pbar,

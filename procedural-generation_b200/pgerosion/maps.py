@@ -88,7 +88,10 @@ class ErosionState:
     erodibility: torch.Tensor = field(default=None, repr=False)
     #: the epsilon-filled routing surface (float64, (F, NE, NE), cell units) or None (refresh_route)
     route: torch.Tensor = field(default=None, repr=False)
+    #: iteration of the last sea-mask refresh (refresh_base), None before the first
+    base_at: int = None
     _owner: torch.Tensor = field(default=None, repr=False)
+    _sea: tuple = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
 
     def __post_init__(self):
@@ -266,6 +269,51 @@ class ErosionState:
                                           self.workspace.numel(), _stream()), "pge_route_flood")
         self.exchange_field(self.route, linear=True)
         return int(n.value)
+
+    def refresh_base(self, min_fraction: float = 0.02, max_sweeps: int = 1 << 22) -> dict:
+        """Recompute the base level (maps.py:360-420): 0 on the open ocean
+        and on land, a closed below-sea basin's deepest surface on its cells
+        (hydro/run.py:64-83: a below-sea body is open ocean when it covers
+        ``min_fraction`` of the globe, and the largest always is); halos
+        copied from their nearest interior source.  Returns the reference's
+        statistics."""
+        info = {"closed_cells": 0, "closed_basins": 0, "sea_cells": 0, "deepest_basin_floor": 0.0}
+        if not self.spherical:
+            self.base = torch.zeros_like(self.height)
+            self.base_at = self.iteration
+            return info
+        _ensure_workspace(self)
+        dev = self.height.device
+        if self._sea is None:
+            from .isostasy import sqrt_det_metric
+
+            H, N = self.H, self.N
+            sq = sqrt_det_metric(self.grid)[H:H + N, H:H + N]
+            area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * float(self.grid.cell_size_m) ** 2)
+                                                        .astype(np.float32), (self.F, N, N)))
+            hm = self.grid.halo
+            self._sea = (torch.as_tensor(area, device=dev), float(area.reshape(-1).astype(np.float64).sum()),
+                         torch.as_tensor(hm.dst.astype(np.int64), device=dev), torch.as_tensor(hm.nearest.astype(np.int64), device=dev))
+        area, total, dst, nearest = self._sea
+        base = torch.empty_like(self.height)
+        labels = torch.empty((self.F, self.N, self.N), dtype=torch.int32, device=dev)
+        n = ctypes.c_int64(0)
+        check(_lib.load().pge_sea_base(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), _ptr(self.owner_table()),
+                                       _ptr(area), float(min_fraction) * total, _ptr(base), _ptr(labels), int(max_sweeps),
+                                       ctypes.byref(n), _ptr(self.workspace), self.workspace.numel(), _stream()), "pge_sea_base")
+        flat = base.view(-1)
+        flat[dst] = flat[nearest]  # the halo is an exact copy of the cell it mirrors (a jump at a basin rim)
+        b = base[self.interior]
+        below = labels >= 0
+        closed = below & (b < 0.0)
+        info["sea_cells"] = int((below & ~closed).sum().item())
+        info["closed_cells"] = int(closed.sum().item())
+        if info["closed_cells"]:
+            info["closed_basins"] = int(torch.unique(labels[closed]).numel())
+            info["deepest_basin_floor"] = float(b[closed].min().item())
+        self.base = base
+        self.base_at = self.iteration
+        return info
 
     def n_active_interior(self) -> int:
         if self.mask is None:
@@ -562,6 +610,13 @@ def hold_datum(state: ErosionState, land_fraction: float, level: float = 0.0) ->
     return q
 
 
+def ocean_min_fraction(params) -> float:
+    """``hydro.ocean_min_fraction`` when the params carry a hydro group, else
+    the bake's default 0.02 (maps.py:770-774)."""
+    hydro = getattr(params, "hydro", None)
+    return float(getattr(hydro, "ocean_min_fraction", 0.02)) if hydro is not None else 0.02
+
+
 def held_land_fraction(state: ErosionState, params) -> float:
     if state.land_target is not None:
         return float(state.land_target)
@@ -593,6 +648,11 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     exchange; increments ``state.iteration``."""
     ep = erosion_group(params)
     t0 = time.time()
+    sea_every = int(getattr(ep, "sea_mask_every", 0))
+    st_base = None
+    if state.spherical and sea_every > 0 and (state.base_at is None or state.iteration % sea_every == 0):
+        # the sea mask before the route: the flood seeds on the sea (maps.py:1546-1551)
+        st_base = state.refresh_base(ocean_min_fraction(params))
     flood = int(getattr(ep, "flood_every", 0))
     if flood > 0 and (state.route is None or state.iteration % flood == 0):
         # the routing surface the particles steer on (maps.py:1553-1554)
@@ -618,6 +678,8 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
         st["datum_shift"] = hold_datum(state, held_land_fraction(state, params))
     state.exchange_halos()
     state.iteration += 1
+    if st_base is not None:
+        st["sea"] = st_base
     st["seconds_route"] = t_route - t0
     st["seconds_particles"] = t1 - t_route
     st["seconds_total"] = time.time() - t0

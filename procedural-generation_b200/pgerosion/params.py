@@ -190,11 +190,10 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (sea mask, lakes, glacial pass, ice, lateral cut, basin fill).
-    Isostasy and the routing surface (``flood_every``) are supported."""
+    path (lakes, glacial pass, ice, lateral cut, basin fill).  Isostasy, the
+    routing surface (``flood_every``) and the sea mask (``sea_mask_every``)
+    are supported."""
     bad = []
-    if int(getattr(ep, "sea_mask_every", 0)) > 0:
-        bad.append("sea_mask_every")
     if bool(getattr(ep, "lake_balance", False)):
         bad.append("lake_balance")
     if int(getattr(ep, "glacial_every", 0)) > 0:

@@ -35,6 +35,9 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
   window of it.
 * ``step_route.npz`` -- as ``step_tiny.npz`` with the routing surface on
   (``erosion.flood_every = 2``): particles steer on the flood.
+* ``step_sea.npz`` -- a world with closed below-sea basins: the reference's
+  sea mask (``refresh_base``) of its start, and steps with the sea mask and
+  the routing flood on (``sea_mask_every = flood_every = 2``).
 
 The fixtures are small (well under a few MB) and committed; the tests never
 import the bake.
@@ -357,6 +360,40 @@ def gen_step_route(cs, maps, pk, WorldParams):
     print("step_route: cells under the route", routes, stats[-1])
 
 
+def gen_sea(cs, maps, pk, WorldParams):
+    """The reference's sea mask (ErosionState.refresh_base: below-sea
+    components, open ocean by area, closed basins at their floor) on a
+    six-face N=32 world with closed basins, and steps with the sea mask and
+    the routing flood on (sea_mask_every = flood_every = 2)."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=7, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    iters = 5
+    p = _world_params(WorldParams, 32, 2, 50.0, 7, 0.45, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", flood_every=2, sea_mask_every=2)
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    mf = float(p.hydro.ocean_min_fraction)
+    b_height, b_sediment = st.height.copy(), st.sediment.copy()
+    info0 = st.refresh_base(mf)
+    base0 = st.base.copy()
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    stats = []
+    for it in range(iters):
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "deaths", "datum_shift")})
+        if "sea" in s:
+            stats[-1]["sea"] = s["sea"]
+    np.savez_compressed(HERE / "step_sea.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=7, iterations=iters,
+                        n_particles=4096, ocean_min_fraction=mf,
+                        params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        b_height=b_height, b_sediment=b_sediment, b_base=base0, b_info=json.dumps(info0),
+                        h_start=h_start, height=st.height, sediment=st.sediment, discharge=st.discharge, momentum=st.momentum,
+                        pending=st.pending, base=st.base, route=st.route, stats=json.dumps(stats), **init)
+    print("step_sea: first refresh", info0, "last", stats[-1])
+
+
 def gen_isostasy(cs, maps, pk, WorldParams):
     from pgerosion import synth
 
@@ -418,7 +455,7 @@ def main(bake: str, only: str | None = None):
             "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
-            "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams)}
+            "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

@@ -162,3 +162,30 @@ def test_routed_steps_match_reference_bit_exact():
     inter = (slice(None), slice(st.H, st.H + st.N), slice(st.H, st.H + st.N))
     assert np.array_equal(st.route[inter], t["route"][inter])
     np.testing.assert_allclose(st.route, t["route"], rtol=0, atol=1e-12)
+
+
+def test_sea_mask_matches_reference_bit_exact():
+    """The oracle's sea mask (maps.py:360-420, hydro/run.py:64-83) on the
+    reference fixture's world, and full steps with the sea mask and the
+    routing flood on (sea_mask_every = flood_every = 2)."""
+    c = step_case(GOLDEN / "step_sea.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    st.height[...] = t["b_height"]
+    st.sediment[...] = t["b_sediment"]
+    info = orc.refresh_base(st, float(t["ocean_min_fraction"]))
+    assert info == json.loads(str(t["b_info"]))
+    assert info["closed_basins"] > 0
+    assert np.array_equal(st.base, t["b_base"])
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.refresh_base(st, float(t["ocean_min_fraction"]))
+    orc.start_replay(st, c["params"])
+    assert np.array_equal(st.height, t["h_start"])
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        for k in ("particles", "entries", "clamped", "deaths", "datum_shift"):
+            assert s[k] == r[k], (it, k)
+        assert s.get("sea") == r.get("sea"), it
+    for k in ("height", "sediment", "discharge", "momentum", "pending", "base"):
+        assert np.array_equal(getattr(st, k), t[k]), k
