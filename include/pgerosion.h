@@ -36,6 +36,9 @@
  *                                                  globe/erosion/maps.py:360-420,
  *                                                  globe/hydro/run.py:64-83,
  *                                                  globe/hydro/lakes.py:19-46
+ *   pge_glacial           glacial.carve (the ice line of the evaporation field)
+ *                                                  globe/erosion/glacial.py:100-257,
+ *                                                  globe/erosion/maps.py:1580-1590
  *   pge_trace_apply_tape  pge_trace_apply (wave apply, one wave) recording each
  *                         droplet's steps and ledger branches for the adjoint
  *   pge_adjoint_pass      reverse of one taped droplet pass: gradients of the
@@ -378,6 +381,23 @@ PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *
  * grids only. */
 PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
                          int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream);
+
+/* The glacial pass (glacial.py:162-257), the ice line read from the
+ * evaporation field: ice on active cells with evap <= ice_evap and surface
+ * > 0 (or, with ice_prev non-NULL -- erosion.glacial_sticky -- ice there
+ * before and still cold; ice_prev (F,NE,NE) uint8 is then updated); the bed
+ * lowered by glacial_rate sqrt(max(discharge, 0) / disc_saturation)
+ * (1 - 0.5 hardness) times the taper (glacial_ramp rings in from the
+ * margin), capped at glacial_max and at the cell's base level (less 0.02);
+ * the carved rock spread over the ice margin by discharge as sediment,
+ * capped per cell at iter_deposit, the rest added to pending.  Lengths in
+ * cell units.  Every rule runs on the extended arrays with neighbours
+ * wrapping at each face array's edges (the reference's numpy rolls); refresh
+ * the halos afterwards.  stats (host): ice cells, carved, moraine cells,
+ * largest carve, outwash (parked).  Synchronises the stream. */
+PGE_API int pge_glacial(const PgeGrid *g, PgeState *s, uint8_t *ice_prev, double glacial_rate, double glacial_max, int32_t glacial_ramp,
+                        double ice_evap, double disc_saturation, double moraine_frac, double iter_deposit, double *stats, void *ws,
+                        size_t ws_bytes, void *stream);
 
 /* No counterpart in the reference: the adjoint of the particle pass.
  *

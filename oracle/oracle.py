@@ -18,7 +18,8 @@ this module; the product never does.  It drives the C restatement in
 * :func:`step` -- maps.py:1516-1617, plain path (plus isostasy, the
   routing surface, :func:`refresh_route` / :func:`priority_flood_eps`,
   maps.py:351-358 and route.py:31-125, and the sea mask,
-  :func:`refresh_base`, maps.py:360-420 with hydro/run.py:64-83)
+  :func:`refresh_base`, maps.py:360-420 with hydro/run.py:64-83, and the
+  glacial pass, :func:`glacial_carve`, erosion/glacial.py:162-257)
 
 Every random number comes from ``params.rng("erosion", iteration)`` exactly
 as in the reference, so a GPU run and this oracle see the same spawns.
@@ -162,6 +163,7 @@ class OracleState:
     iteration: int = 0
     route: np.ndarray = None  # the epsilon-filled routing surface (refresh_route) or None
     base_at: int = None  # iteration of the last sea-mask refresh (refresh_base)
+    ice_prev: np.ndarray = None  # the last glacial pass's ice (erosion.glacial_sticky)
     land_target: float | None = None
     deposit_on_exit: bool = False
     samp: np.ndarray = field(default=None, repr=False)
@@ -726,6 +728,14 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     if iso:
         state.iso_acc += (state.height + state.sediment) - s0
     apply_uplift(state, None)
+    ge = int(getattr(ep, "glacial_every", 0))
+    if state.spherical and ge > 0 and (state.iteration + 1) % ge == 0 and \
+            (state.iteration + 1) >= float(ep.glacial_from) * int(ep.iterations):
+        if iso:
+            s1 = state.height + state.sediment
+        st["glacial"] = glacial_carve(state, params)  # maps.py:1580-1590
+        if iso:
+            state.iso_acc += (state.height + state.sediment) - s1
     if iso and (state.iteration + 1) % max(int(getattr(ep, "isostasy_every", 10)), 1) == 0:
         st["isostasy"] = apply_isostasy(state, params)
     if state.spherical:
@@ -735,6 +745,94 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     if st_base is not None:
         st["sea"] = st_base
     return st
+
+
+#: the deposit floor of the glacial pass's room (particle.py:99), cell units
+GLACIAL_DEP_FLOOR = 0.02
+
+
+def _ring(a: np.ndarray) -> np.ndarray:
+    """The eight D8 neighbours of every cell of each face's extended array,
+    wrapping at the array's edges (np.roll, as the reference's passes do)."""
+    out = []
+    for di in (-1, 0, 1):
+        for dj in (-1, 0, 1):
+            if di or dj:
+                out.append(np.roll(np.roll(a, di, axis=1), dj, axis=2))
+    return out
+
+
+def glacial_carve(state, params) -> dict:
+    """erosion/glacial.py:162-257 (the ice line of the evaporation field:
+    no ice sheet, no surface temperature): the bed under ice lowered by
+    glacial_rate sqrt(discharge / disc_saturation) (1 - 0.5 hardness) times
+    the taper of :func:`_ice_depth`, capped, down to the cell's base level;
+    the spoil spread over the ice margin by discharge, capped per cell at
+    iter_deposit, the rest parked as stockpile."""
+    ep = _ep(params)
+    u = state.height_unit_m
+    rate = _cu(ep, "glacial_rate", u)
+    cap = _cu(ep, "glacial_max", u)
+    stats = {"ice_cells": 0, "carved": 0.0, "moraine_cells": 0, "max_carve": 0.0, "outwash": 0.0}
+    if rate <= 0.0:
+        return stats
+    active = state.mask == MASK_ACTIVE
+    cold = state.evap <= float(ep.ice_evap)
+    ice = active & cold & (state.height + state.sediment > 0.0)
+    sticky = bool(getattr(ep, "glacial_sticky", False))
+    if sticky and state.ice_prev is not None:
+        ice = ice | (state.ice_prev & active & cold)
+    if not ice.any():
+        return stats
+    state.exchange_halos()
+    if sticky:
+        state.ice_prev = ice.copy()
+    sat = max(float(ep.disc_saturation), 1e-9)
+    q = np.maximum(state.discharge, 0.0) / sat
+    ramp = int(ep.glacial_ramp)
+    if ramp <= 0:
+        taper = ice.astype(np.float64)
+    else:
+        inner = ice.copy()
+        depth = ice.astype(np.float64)
+        for _ in range(ramp):
+            shrunk = inner.copy()
+            for nb in _ring(inner):
+                shrunk &= nb
+            state.exchange_halos()
+            inner = shrunk
+            depth += inner
+        state.exchange_halos()
+        taper = np.clip(depth / float(ramp + 1), 0.0, 1.0)
+    dz = rate * np.sqrt(q) * (1.0 - 0.5 * state.hardness) * taper
+    np.clip(dz, 0.0, cap, out=dz)
+    dz = np.where(ice, dz, 0.0)
+    room = np.maximum(state.height + state.sediment + GLACIAL_DEP_FLOOR - state.base, 0.0)
+    dz = np.minimum(dz, room)
+    inter = state.interior
+    carved = float(dz[inter].sum())
+    if carved <= 0.0:
+        return stats
+    state.height -= dz
+    near = np.zeros_like(ice)
+    for nb in _ring(ice):
+        near |= nb
+    margin = near & ~ice & active & (state.height + state.sediment > state.base)
+    frac = float(ep.moraine_frac)
+    parked = 0.0
+    if margin.any() and frac > 0.0:
+        w = np.where(margin, np.maximum(state.discharge, 0.0) + 1e-6, 0.0)
+        wsum = float(w[inter].sum())
+        if wsum > 0.0:
+            add = (w / wsum) * (carved * frac)
+            placed = np.minimum(add, _cu(ep, "iter_deposit", u))
+            state.sediment += placed
+            state.pending += add - placed
+            parked = float((add - placed)[inter].sum())
+    state.exchange_halos()
+    stats.update(ice_cells=int(ice[inter].sum()), carved=carved, moraine_cells=int(margin[inter].sum()),
+                 max_carve=float(dz[inter].max()), outwash=parked)
+    return stats
 
 
 #: hydro.ocean_min_fraction, the bake's default (the share of the globe a below-sea body needs to be open ocean)

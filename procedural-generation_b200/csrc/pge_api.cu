@@ -549,6 +549,27 @@ PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *own
     return PGE_OK;
 }
 
+PGE_API int pge_glacial(const PgeGrid *g, PgeState *s, uint8_t *ice_prev, double glacial_rate, double glacial_max, int32_t glacial_ramp,
+                        double ice_evap, double disc_saturation, double moraine_frac, double iter_deposit, double *stats, void *ws,
+                        size_t ws_bytes, void *stream)
+{
+    int r;
+    Layout lay;
+    if ((r = check_grid(g)) || (r = check_ws(g, ws, ws_bytes, lay)) || (r = check_state(s))) return r;
+    if (!stats) return fail(PGE_E_ARG, "glacial: NULL stats");
+    GlacialArgs ga;
+    ga.rate = glacial_rate;
+    ga.cap = glacial_max;
+    ga.ramp = glacial_ramp;
+    ga.ice_evap = (float)ice_evap;
+    ga.sat = disc_saturation > 1e-9 ? disc_saturation : 1e-9;
+    ga.dep_floor = 0.02;
+    ga.moraine_frac = moraine_frac;
+    ga.iter_deposit = iter_deposit;
+    const int e = glacial(*g, *s, ice_prev, ga, stats, lay, ws, (cudaStream_t)stream);
+    return e == 0 ? PGE_OK : cuda_fail((cudaError_t)(-e), "glacial");
+}
+
 PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream)
 {
     if (!h || !zbar || (h->K > 0 && (!h->dst || !h->src || !h->w))) return fail(PGE_E_ARG, "halo_adjoint: NULL pointer");

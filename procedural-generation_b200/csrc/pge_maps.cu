@@ -9,6 +9,8 @@
 //   datum order statistic       maps.py:1446-1508 (radix select instead of np.partition)
 //   halo gather                 field.py:104-125
 //   spawn weights / inverse CDF maps.py:793-833, particle.py:1245-1260
+#include <cstring>
+
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
@@ -1097,6 +1099,184 @@ cudaError_t sea_base(const PgeGrid &g, const PgeState &st, const int32_t *owner,
     sea_largest_kernel<<<grid_for(M), 256, 0, s>>>(M, label, per, maxkey, largest, 1);
     sea_base_kernel<<<grid_for(lay.ncell), 256, 0, s>>>(lay.ncell, N, H, NE, label, per, floorkey, largest, min_area, base);
     return cudaPeekAtLastError();
+}
+
+// ---------------------------------------------------------------------------
+// glacial pass (erosion/glacial.py:162-257; the ice line of the evaporation
+// field).  Every per-cell rule runs on the whole extended array, neighbours
+// wrapping at each face array's edges as numpy's roll does, so the interior
+// comes out as the reference's; the sums are float64 atomics.
+// ---------------------------------------------------------------------------
+namespace {
+__device__ __forceinline__ long long glac_nb(long long e, int NE, int k)
+{
+    const long long f = e / ((long long)NE * NE), rem = e % ((long long)NE * NE);
+    int i = (int)(rem / NE) + kRouteD8[k][0], j = (int)(rem % NE) + kRouteD8[k][1];
+    i = i < 0 ? i + NE : (i >= NE ? i - NE : i);
+    j = j < 0 ? j + NE : (j >= NE ? j - NE : j);
+    return (f * NE + i) * NE + j;
+}
+__device__ __forceinline__ bool glac_interior(long long e, int NE, int H, int N)
+{
+    const long long rem = e % ((long long)NE * NE);
+    const int i = (int)(rem / NE), j = (int)(rem % NE);
+    return i >= H && i < H + N && j >= H && j < H + N;
+}
+struct GlacSums {
+    unsigned long long ice_any, ice_interior, margin_any, margin_interior, max_key;
+    double carved, wsum, parked;
+};
+}  // namespace
+
+__global__ void glac_ice_kernel(long long n, int NE, int H, int N, const double *__restrict__ h, const double *__restrict__ s,
+                                const float *__restrict__ evap, const uint8_t *__restrict__ mask, const uint8_t *__restrict__ prev,
+                                float ice_evap, uint8_t *ice, double *depth, GlacSums *sums)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const bool active = mask ? mask[e] == PGE_MASK_ACTIVE : true;
+        const bool cold = evap[e] <= ice_evap;
+        bool v = active && cold && (h[e] + s[e] > 0.0);
+        if (prev && prev[e] && active && cold) v = true;
+        ice[e] = v;
+        depth[e] = v ? 1.0 : 0.0;
+        if (v) {
+            atomicAdd(&sums->ice_any, 1ull);
+            if (glac_interior(e, NE, H, N)) atomicAdd(&sums->ice_interior, 1ull);
+        }
+    }
+}
+
+// one ring: a cell stays inside while it and its eight neighbours are
+__global__ void glac_ring_kernel(long long n, int NE, const uint8_t *__restrict__ inner, uint8_t *shrunk, double *depth)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        bool v = inner[e];
+        for (int k = 0; k < 8 && v; k++) v = inner[glac_nb(e, NE, k)];
+        shrunk[e] = v;
+        if (v) depth[e] += 1.0;
+    }
+}
+
+__global__ void glac_dz_kernel(long long n, int NE, int H, int N, const double *__restrict__ h, const double *__restrict__ s,
+                               const double *__restrict__ q, const float *__restrict__ hard, const double *__restrict__ base,
+                               const uint8_t *__restrict__ ice, const double *__restrict__ depth, int ramp, double rate, double cap,
+                               double sat, double dep_floor, double *dz, GlacSums *sums)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        double taper = depth[e];
+        if (ramp > 0) {
+            taper = taper / (double)(ramp + 1);
+            taper = taper < 0.0 ? 0.0 : (taper > 1.0 ? 1.0 : taper);
+        }
+        const double qq = (q[e] > 0.0 ? q[e] : 0.0) / sat;
+        const float hf = __fsub_rn(1.0f, __fmul_rn(0.5f, hard[e]));  // float32, as the reference's array arithmetic
+        double d = rate * sqrt(qq) * (double)hf * taper;
+        d = d < 0.0 ? 0.0 : (d > cap ? cap : d);
+        if (!ice[e]) d = 0.0;
+        double room = h[e] + s[e] + dep_floor - base[e];
+        if (room < 0.0) room = 0.0;
+        if (room < d) d = room;
+        dz[e] = d;
+        if (d != 0.0 && glac_interior(e, NE, H, N)) {
+            atomicAdd(&sums->carved, d);
+            atomicMax(&sums->max_key, okey(d));
+        }
+    }
+}
+
+__global__ void glac_carve_kernel(long long n, double *h, const double *__restrict__ dz)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        h[e] -= dz[e];
+}
+
+__global__ void glac_margin_kernel(long long n, int NE, int H, int N, const double *__restrict__ h, const double *__restrict__ s,
+                                   const double *__restrict__ q, const double *__restrict__ base, const uint8_t *__restrict__ mask,
+                                   const uint8_t *__restrict__ ice, double *w, GlacSums *sums)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        bool near = false;
+        for (int k = 0; k < 8 && !near; k++) near = ice[glac_nb(e, NE, k)];
+        const bool active = mask ? mask[e] == PGE_MASK_ACTIVE : true;
+        const bool margin = near && !ice[e] && active && (h[e] + s[e] > base[e]);
+        w[e] = margin ? (q[e] > 0.0 ? q[e] : 0.0) + 1e-6 : 0.0;
+        if (margin) {
+            atomicAdd(&sums->margin_any, 1ull);
+            if (glac_interior(e, NE, H, N)) {
+                atomicAdd(&sums->margin_interior, 1ull);
+                atomicAdd(&sums->wsum, w[e]);
+            }
+        }
+    }
+}
+
+__global__ void glac_moraine_kernel(long long n, int NE, int H, int N, const double *__restrict__ w, double wsum, double load, double cap,
+                                    double *s, double *pending, GlacSums *sums)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double add = (w[e] / wsum) * load;
+        const double placed = add < cap ? add : cap;
+        s[e] += placed;
+        pending[e] += add - placed;
+        const double parked = add - placed;
+        if (parked != 0.0 && glac_interior(e, NE, H, N)) atomicAdd(&sums->parked, parked);
+    }
+}
+
+int glacial(const PgeGrid &g, PgeState &st, uint8_t *ice_prev, const GlacialArgs &ga, double stats[5], const Layout &lay, void *ws,
+            cudaStream_t s)
+{
+    const int N = g.N, H = g.H, NE = N + 2 * H;
+    const long long n = lay.ncell;
+    stats[0] = stats[1] = stats[2] = stats[3] = stats[4] = 0.0;
+    if (ga.rate <= 0.0) return 0;
+    uint8_t *ice = ws_ptr<uint8_t>(ws, lay.flags), *ping = ice + n, *pong = ice + 2 * n;
+    double *depth = ws_ptr<double>(ws, lay.thermal), *dz = depth + n, *w = depth + 2 * n;
+    GlacSums *sums = reinterpret_cast<GlacSums *>(ws_ptr<unsigned long long>(ws, lay.counters) + 12);
+    GlacSums hs;
+    cudaError_t e;
+    auto read = [&]() -> cudaError_t {
+        cudaError_t r = cudaMemcpyAsync(&hs, sums, sizeof(GlacSums), cudaMemcpyDeviceToHost, s);
+        return r == cudaSuccess ? cudaStreamSynchronize(s) : r;
+    };
+    if ((e = cudaMemsetAsync(sums, 0, sizeof(GlacSums), s)) != cudaSuccess) return -(int)e;
+    glac_ice_kernel<<<grid_for(n), 256, 0, s>>>(n, NE, H, N, st.height, st.sediment, st.evap, st.mask, ice_prev, ga.ice_evap, ice,
+                                                depth, sums);
+    if ((e = read()) != cudaSuccess) return -(int)e;
+    if (!hs.ice_any) return 0;  // no ice: nothing changes (and the last ice stays as it was)
+    if (ice_prev && (e = cudaMemcpyAsync(ice_prev, ice, n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return -(int)e;
+    if (ga.ramp > 0) {
+        const uint8_t *inner = ice;
+        for (int r = 0; r < ga.ramp; r++) {
+            uint8_t *out = (r & 1) ? pong : ping;
+            glac_ring_kernel<<<grid_for(n), 256, 0, s>>>(n, NE, inner, out, depth);
+            inner = out;
+        }
+    }
+    glac_dz_kernel<<<grid_for(n), 256, 0, s>>>(n, NE, H, N, st.height, st.sediment, st.discharge, st.hardness, st.base, ice, depth,
+                                               ga.ramp, ga.rate, ga.cap, ga.sat, ga.dep_floor, dz, sums);
+    if ((e = read()) != cudaSuccess) return -(int)e;
+    if (!(hs.carved > 0.0)) return 0;  // nothing carved: the reference returns before any change (and empty statistics)
+    glac_carve_kernel<<<grid_for(n), 256, 0, s>>>(n, st.height, dz);
+    glac_margin_kernel<<<grid_for(n), 256, 0, s>>>(n, NE, H, N, st.height, st.sediment, st.discharge, st.base, st.mask, ice, w, sums);
+    if ((e = read()) != cudaSuccess) return -(int)e;
+    if (hs.margin_any && ga.moraine_frac > 0.0 && hs.wsum > 0.0) {
+        glac_moraine_kernel<<<grid_for(n), 256, 0, s>>>(n, NE, H, N, w, hs.wsum, hs.carved * ga.moraine_frac, ga.iter_deposit,
+                                                        st.sediment, st.pending, sums);
+        if ((e = read()) != cudaSuccess) return -(int)e;
+    }
+    stats[0] = (double)hs.ice_interior;
+    stats[1] = hs.carved;
+    stats[2] = (double)hs.margin_interior;
+    {  // the order-preserving key back to its double (host side of unokey)
+        const unsigned long long k = hs.max_key;
+        const unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+        double v;
+        memcpy(&v, &b, sizeof v);
+        stats[3] = v;
+    }
+    stats[4] = hs.parked;
+    return 0;
 }
 
 }  // namespace pge

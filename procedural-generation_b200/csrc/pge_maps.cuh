@@ -25,6 +25,14 @@ cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *own
 // sea mask: base level of closed below-sea basins; *sweeps_out < 0: the labelling did not converge
 cudaError_t sea_base(const PgeGrid &g, const PgeState &st, const int32_t *owner, const float *area, double min_area, double *base,
                      int32_t *label_out, const Layout &lay, void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s);
+// glacial pass (erosion/glacial.py:162-257), lengths in cell units; returns 0 or -cudaError
+struct GlacialArgs {
+    double rate, cap, sat, dep_floor, moraine_frac, iter_deposit;
+    float ice_evap;
+    int ramp;
+};
+int glacial(const PgeGrid &g, PgeState &st, uint8_t *ice_prev, const GlacialArgs &ga, double stats[5], const Layout &lay, void *ws,
+            cudaStream_t s);
 // the adjoint (pge_adjoint.cu)
 cudaError_t adjoint_pass(const PgeGrid &g, const PgeState &s, const PgeSpawns &sp, const PgeParams &p, const PgeTape &tape,
                          int carry_path, const double *zbar_after, double *zbar_before, double *ebar, double *pbar,

@@ -26,7 +26,7 @@ EXPORTS = (
     "pge_version", "pge_last_error", "pge_workspace_bytes", "pge_spawn_rain", "pge_count_pending",
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
-    "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base",
+    "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base", "pge_glacial",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -127,6 +127,8 @@ def load(path: str | os.PathLike | None = None):
                                    c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_halo_adjoint.argtypes = [P(PgeHalo), c_vp, c_vp]
     L.pge_route_flood.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]
+    L.pge_glacial.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_f64, c_i32, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp,
+                              ctypes.c_size_t, c_vp]
     L.pge_sea_base.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_vp, c_f64, c_vp, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]
     for n in EXPORTS:
         if n not in ("pge_version", "pge_last_error", "pge_workspace_bytes"):

@@ -90,6 +90,8 @@ class ErosionState:
     route: torch.Tensor = field(default=None, repr=False)
     #: iteration of the last sea-mask refresh (refresh_base), None before the first
     base_at: int = None
+    #: the last glacial pass's ice (uint8, (F, NE, NE)) for erosion.glacial_sticky, None before the first
+    ice_prev: torch.Tensor = field(default=None, repr=False)
     _owner: torch.Tensor = field(default=None, repr=False)
     _sea: tuple = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
@@ -610,6 +612,30 @@ def hold_datum(state: ErosionState, land_fraction: float, level: float = 0.0) ->
     return q
 
 
+def glacial_carve(state: ErosionState, params) -> dict:
+    """One glacial pass (erosion/glacial.py:162-257) with the ice line read
+    from the evaporation field (``evap <= erosion.ice_evap``; the state
+    carries no temperature): the bed under ice lowered, the spoil put on the
+    ice margin as moraine, the excess parked as stockpile; the halos
+    refreshed.  Returns the reference's statistics."""
+    ep = erosion_group(params)
+    _ensure_workspace(state, ep)
+    u = state.height_unit_m
+    sticky = bool(getattr(ep, "glacial_sticky", False))
+    if sticky and state.ice_prev is None:
+        state.ice_prev = torch.zeros(state.height.shape, dtype=torch.uint8, device=state.height.device)
+    out = (ctypes.c_double * 5)()
+    check(_lib.load().pge_glacial(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()),
+                                  _ptr(state.ice_prev) if sticky else None, cell_units(ep, "glacial_rate", u),
+                                  cell_units(ep, "glacial_max", u), int(ep.glacial_ramp), float(ep.ice_evap),
+                                  float(ep.disc_saturation), float(getattr(ep, "moraine_frac", 1.0)), cell_units(ep, "iter_deposit", u),
+                                  out, _ptr(state.workspace), state.workspace.numel(), _stream()), "pge_glacial")
+    if out[1] > 0.0:
+        state.exchange_halos()
+    return {"ice_cells": int(out[0]), "carved": float(out[1]), "moraine_cells": int(out[2]), "max_carve": float(out[3]),
+            "outwash": float(out[4])}
+
+
 def ocean_min_fraction(params) -> float:
     """``hydro.ocean_min_fraction`` when the params carry a hydro group, else
     the bake's default 0.02 (maps.py:770-774)."""
@@ -670,6 +696,15 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
         # only what surface processes moved: uplift and the datum shift are not loads
         state.iso_acc += (state.height + state.sediment) - s0
     apply_uplift(state, uplift_cap(state, ep))
+    ge = int(getattr(ep, "glacial_every", 0))
+    if state.spherical and ge > 0 and (state.iteration + 1) % ge == 0 and \
+            (state.iteration + 1) >= float(ep.glacial_from) * int(ep.iterations):
+        # glacial carving: the one pass that may leave a closed depression (maps.py:1580-1590)
+        if iso:
+            s1 = state.height + state.sediment
+        st["glacial"] = glacial_carve(state, params)
+        if iso:
+            state.iso_acc += (state.height + state.sediment) - s1
     if iso and (state.iteration + 1) % max(int(getattr(ep, "isostasy_every", 10)), 1) == 0:
         from .isostasy import apply_isostasy
 

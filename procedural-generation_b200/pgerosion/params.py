@@ -92,6 +92,8 @@ class ErosionParams:
     glacial_rate: float = 6.0
     glacial_ramp: int = 4
     glacial_max: float = 20.0
+    glacial_sticky: bool = True
+    moraine_frac: float = 1.0
     climate_at_surface: bool = True
     ice_age_c: float = 8.0
     ice_history: bool = True
@@ -190,14 +192,13 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (lakes, glacial pass, ice, lateral cut, basin fill).  Isostasy, the
-    routing surface (``flood_every``) and the sea mask (``sea_mask_every``)
+    path (lakes, ice sheet, lateral cut, basin fill).  Isostasy, the routing
+    surface (``flood_every``), the sea mask (``sea_mask_every``) and the
+    glacial pass (``glacial_every``, the ice line of the evaporation field)
     are supported."""
     bad = []
     if bool(getattr(ep, "lake_balance", False)):
         bad.append("lake_balance")
-    if int(getattr(ep, "glacial_every", 0)) > 0:
-        bad.append("glacial_every")
     if float(getattr(ep, "lateral_rate", 0.0)) > 0.0:
         bad.append("lateral_rate")
     if bool(getattr(ep, "ice_sheet", False)):

@@ -38,6 +38,8 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
 * ``step_sea.npz`` -- a world with closed below-sea basins: the reference's
   sea mask (``refresh_base``) of its start, and steps with the sea mask and
   the routing flood on (``sea_mask_every = flood_every = 2``).
+* ``step_glacial.npz`` -- steps with the glacial pass on (every 2
+  iterations from the start) on a world frozen poleward of 50 degrees.
 
 The fixtures are small (well under a few MB) and committed; the tests never
 import the bake.
@@ -394,6 +396,38 @@ def gen_sea(cs, maps, pk, WorldParams):
     print("step_sea: first refresh", info0, "last", stats[-1])
 
 
+def gen_glacial(cs, maps, pk, WorldParams):
+    """Steps with the glacial pass on (glacial_every = 2 from the start,
+    erosion/glacial.py carve): a world whose high latitudes are frozen
+    (evaporation multiplier 0 poleward of 50 degrees, the reference's ice line
+    at ice_evap = 0), run through the reference's maps.step."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=17, N=32, H=2, cell_size_m=50.0, land_fraction=0.4)
+    world.evap[...] = np.where(np.abs(world.grid.latitude()) > np.radians(50.0), 0.0, 1.0).astype(np.float32)
+    iters = 4
+    p = _world_params(WorldParams, 32, 2, 50.0, 17, 0.4, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", glacial_every=2, glacial_from=0.0)
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    stats = []
+    pre = None
+    for it in range(iters):
+        if (it + 1) % 2 == 0 and pre is None:
+            pre = {k: getattr(st, k).copy() for k in ("height", "sediment", "discharge", "momentum", "pending", "base")}
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "deaths", "datum_shift")})
+        if "glacial" in s:
+            stats[-1]["glacial"] = s["glacial"]
+    np.savez_compressed(HERE / "step_glacial.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.4, seed=17, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h_start, height=st.height, sediment=st.sediment, discharge=st.discharge, momentum=st.momentum,
+                        pending=st.pending, stats=json.dumps(stats), **init)
+    print("step_glacial:", [x.get("glacial") for x in stats])
+
+
 def gen_isostasy(cs, maps, pk, WorldParams):
     from pgerosion import synth
 
@@ -455,7 +489,8 @@ def main(bake: str, only: str | None = None):
             "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
-            "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams)}
+            "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams),
+            "glacial": lambda: gen_glacial(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

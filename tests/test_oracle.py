@@ -189,3 +189,26 @@ def test_sea_mask_matches_reference_bit_exact():
         assert s.get("sea") == r.get("sea"), it
     for k in ("height", "sediment", "discharge", "momentum", "pending", "base"):
         assert np.array_equal(getattr(st, k), t[k]), k
+
+
+def test_glacial_steps_match_reference_bit_exact():
+    """Steps with the glacial pass on (erosion/glacial.py: every 2 iterations
+    on a world frozen poleward of 50 degrees): its statistics and the state."""
+    c = step_case(GOLDEN / "step_glacial.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(st, c["params"])
+    assert np.array_equal(st.height, t["h_start"])
+    n_carves = 0
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        for k in ("particles", "entries", "clamped", "deaths", "datum_shift"):
+            assert s[k] == r[k], (it, k)
+        assert s.get("glacial") == r.get("glacial"), it
+        n_carves += "glacial" in s
+    assert n_carves == 2
+    inter = st.interior
+    for k in ("height", "sediment", "discharge", "momentum"):
+        assert np.array_equal(getattr(st, k), t[k]), k
+    assert np.array_equal(st.pending[inter], t["pending"][inter])
