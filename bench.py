@@ -117,13 +117,14 @@ def run_adjoint(args, dev):
 
     from pgerosion import adjoint as adj
 
-    params = adj.calibration_params(seed=0)
+    N, P, iters = args.adjoint_n, args.adjoint_droplets, args.adjoint_iterations
+    params = adj.calibration_params(seed=0, N=N, iterations=iters)
     st = adj.calibration_state(params, device=dev)
-    calib = adj.Calibration(st, params, adj.CALIB_ITERATIONS, adj.CALIB_DROPLETS, checkpoint_every=adj.CALIB_CHECKPOINT)
-    target = calib.run(None, adj.rates_of(adj.calibration_params(seed=0, jitter=0.3, jitter_seed=1)).tolist())
+    calib = adj.Calibration(st, params, iters, P, checkpoint_every=adj.CALIB_CHECKPOINT)
+    target = calib.run(None, adj.rates_of(adj.calibration_params(seed=0, N=N, iterations=iters, jitter=0.3, jitter_seed=1)).tolist())
     land = torch.zeros_like(target, dtype=torch.bool)
     land[st.interior] = target[st.interior] > 0.0
-    out = {"workload": f"calibration: N_c={adj.CALIB_N}, {adj.CALIB_DROPLETS} droplets/iteration, {adj.CALIB_ITERATIONS} "
+    out = {"workload": f"calibration: N_c={N}, {P} droplets/iteration, {iters} "
                        f"iterations, checkpoint every {adj.CALIB_CHECKPOINT}, wave apply (one wave per iteration), loss = "
                        "mean squared land height difference (m^2) to a target from rates +-30 %",
            "metric": "adjoint/forward time ratio", "higher_is_better": False, "modes": {}}
@@ -492,6 +493,10 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true", help="skip the calibration (adjoint) measurement")
     ap.add_argument("--adjoint-reps", type=int, default=2)
+    ap.add_argument("--adjoint-only", action="store_true", help="run the calibration (adjoint) measurement alone")
+    ap.add_argument("--adjoint-n", type=int, default=256, help="calibration world N_c (the workload: 256)")
+    ap.add_argument("--adjoint-droplets", type=int, default=1 << 17, help="calibration droplets per iteration (the workload: 2^17)")
+    ap.add_argument("--adjoint-iterations", type=int, default=50, help="calibration iterations (the workload: 50)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3
@@ -502,6 +507,12 @@ def main():
     dist = None
     if args.impl == "reference":
         out = run_reference(args, rank)
+    elif args.adjoint_only:
+        import torch
+
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        torch.cuda.set_device(dev)
+        out = {"adjoint": run_adjoint(args, dev)} if rank == 0 else None
     else:
         if world_size > 1:
             import datetime

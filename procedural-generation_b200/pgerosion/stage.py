@@ -94,6 +94,23 @@ def ckpt_hash(params, apply: int) -> str:
 CKPT_FIELDS = ("height", "sediment", "discharge", "momentum", "pending")
 
 
+def _state_fields(state) -> list:
+    """The arrays a checkpoint holds beyond CKPT_FIELDS, as the reference's
+    (run.py:104-116): the routing surface (refreshed every flood_every), the
+    base level once the sea mask has run, an isostatic load not yet applied,
+    and the sticky glacial ice."""
+    out = []
+    if state.route is not None:
+        out.append("route")
+    if state.base_at is not None:
+        out.append("base")
+    if state.iso_acc is not None:
+        out.append("iso_acc")
+    if state.ice_prev is not None:
+        out.append("ice_prev")
+    return out
+
+
 def _write_checkpoint(d: Path, it: int, arrays: dict, meta: dict) -> Path:
     """npz to ``.tmp``, renamed, then the ``.json`` (a crash in between leaves
     the previous checkpoint for :func:`find_checkpoint`), then pruning."""
@@ -119,8 +136,8 @@ def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
     a = state.to_numpy()
     arrays = {k: a[k] for k in CKPT_FIELDS}
     arrays["lake_load"] = np.zeros_like(a["height"])
-    if state.iso_acc is not None:  # a rebound not yet applied is part of the state
-        arrays["iso_acc"] = state.iso_acc.detach().cpu().numpy()
+    for k in _state_fields(state):
+        arrays[k] = getattr(state, k).detach().cpu().numpy()
     return _write_checkpoint(d, state.iteration, arrays, _ckpt_meta(state, params, apply))
 
 
@@ -150,7 +167,8 @@ class CheckpointWriter:
 
         self.wait()
         self.dir.mkdir(parents=True, exist_ok=True)
-        names = list(CKPT_FIELDS) + (["iso_acc"] if state.iso_acc is not None else [])
+        extra = _state_fields(state)
+        names = list(CKPT_FIELDS) + extra
         for k in names:  # the snapshot, on the stream the iterations run on
             src = getattr(state, k)
             if k not in self._snap or self._snap[k].shape != src.shape:
@@ -172,8 +190,8 @@ class CheckpointWriter:
             copied.synchronize()
             arrays = {k: self._host[k].numpy() for k in CKPT_FIELDS}
             arrays["lake_load"] = np.zeros_like(arrays["height"])
-            if "iso_acc" in names:
-                arrays["iso_acc"] = self._host["iso_acc"].numpy()
+            for k in extra:
+                arrays[k] = self._host[k].numpy()
             # the writer reads the pinned buffers only until np.savez returns
             return _write_checkpoint(self.dir, it, arrays, meta)
 
@@ -245,7 +263,15 @@ def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
         for k in ("height", "sediment", "discharge", "momentum"):
             getattr(state, k).copy_(torch.as_tensor(z[k]))
         state.pending.copy_(torch.as_tensor(z["pending"]) if "pending" in z.files else torch.zeros_like(state.pending))
-        state.iso_acc = torch.as_tensor(z["iso_acc"], device=state.height.device) if "iso_acc" in z.files else None
+        dev = state.height.device
+        state.iso_acc = torch.as_tensor(z["iso_acc"], device=dev) if "iso_acc" in z.files else None
+        state.route = torch.as_tensor(z["route"], device=dev) if "route" in z.files else None
+        if "base" in z.files:  # a resume sees the sea mask the continuous run had
+            state.base = torch.as_tensor(z["base"], device=dev)
+            state.base_at = int(meta["iteration"])
+        else:
+            state.base_at = None
+        state.ice_prev = torch.as_tensor(np.asarray(z["ice_prev"], np.uint8), device=dev) if "ice_prev" in z.files else None
     state.iteration = int(meta["iteration"])
 
 

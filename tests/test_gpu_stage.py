@@ -79,3 +79,31 @@ def test_isostasy_state_is_checkpointed_and_resumed(cuda, tmp_path):
     for n in stage.OUTPUTS:
         again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
         assert again.tobytes() == out[n].tobytes(), n
+
+
+def test_host_refreshes_are_checkpointed_and_resumed(cuda, tmp_path):
+    """With the routing flood, the sea mask and the glacial pass on (every 2
+    iterations, ice poleward of 50 degrees), the route, the base level and
+    the sticky ice are part of the checkpoint (run.py:104-116, 200-210) and a
+    resumed run lands on the continuous run's outputs byte for byte."""
+    import dataclasses
+
+    w = synth.earth_world(seed=4, N=32, H=2, cell_size_m=50.0, land_fraction=0.3)
+    w.evap[...] = np.where(np.abs(w.grid.latitude()) > np.radians(50.0), 0.0, 1.0).astype(np.float32)
+    st = stage.LocalStore(tmp_path)
+    for name in ("bedrock", "hardness", "precip", "evap", "uplift"):
+        st.save_field(name, getattr(w, name), w.grid.H)
+    _, p = _world_store(tmp_path / "unused")
+    p = dataclasses.replace(p, erosion=dataclasses.replace(p.erosion, flood_every=2, sea_mask_every=2, glacial_every=2,
+                                                           glacial_from=0.0))
+    stage.run(st, p, log=lambda m: None)
+    with np.load(st.checkpoint_dir / "erosion_iter0003.npz") as z:
+        assert {"route", "base", "ice_prev"} <= set(z.files)
+        assert z["ice_prev"].dtype == np.uint8 and z["ice_prev"].any()
+    out = {n: np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)]) for n in stage.OUTPUTS}
+    for suf in (".npz", ".json"):
+        (st.checkpoint_dir / f"erosion_iter0006{suf}").unlink()
+    stage.run(st, p, log=lambda m: None)
+    for n in stage.OUTPUTS:
+        again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
+        assert again.tobytes() == out[n].tobytes(), n
