@@ -22,9 +22,11 @@
  *   particle.spawn_cells                 particle.py:1245-1260
  *
  * Scope: the plain path with or without the routing surface (particles steer
- * on it where it stands above the terrain; no lake parks, no lateral bank
- * cut, no roots); masks 0/1/2, windows (spherical = 0) and deposit-on-exit
- * are supported.  Numba types the packed samples as float32 and so computes
+ * on it where it stands above the terrain) and with or without overflowing
+ * lakes flagged by the caller (crossing without exchange, the load dropped at
+ * the shore, the bed kept at the water level; no lake parks), no lateral
+ * bank cut, no roots; masks 0/1/2, windows (spherical = 0) and
+ * deposit-on-exit are supported.  Numba types the packed samples as float32 and so computes
  * the stencil differences of _sbilin_grad in float32; the change list keeps
  * volumes and momenta as float32.  Both are mirrored here.
  *
@@ -186,7 +188,7 @@ void orc_transfer_velocity_batch(int64_t n, const int32_t *face, const double *u
 /* ------------------------------------------------------------------------ */
 void orc_pack(int64_t ncell, float *samp, const double *height, const double *sediment, const double *discharge,
               const double *momentum, const float *evap, const float *hardness, const float *metric,
-              const float *metric_inv, const double *base, const double *route)
+              const float *metric_inv, const double *base, const double *route, const uint8_t *lake_flag)
 {
     for (int64_t c = 0; c < ncell; c++) {
         float *s = samp + NS * c;
@@ -204,8 +206,12 @@ void orc_pack(int64_t ncell, float *samp, const double *height, const double *se
             s[S_G + k] = metric[3 * c + k];
             s[S_GINV + k] = metric_inv[3 * c + k];
         }
-        /* 1 where the routing surface differs from the terrain (particle.py:186-190, no lakes) */
-        s[S_RFLAG] = (route && s[S_ROUTE] != s[S_SURF]) ? 1.0f : 0.0f;
+        /* 2 on an overflowing lake, 3 on one with room for its rivers' load, else 1 where the routing
+           surface differs from the terrain (particle.py:186-190) */
+        if (route && lake_flag && lake_flag[c] > 0)
+            s[S_RFLAG] = lake_flag[c] > 1 ? 3.0f : 2.0f;
+        else
+            s[S_RFLAG] = (route && s[S_ROUTE] != s[S_SURF]) ? 1.0f : 0.0f;
         s[S_BASE] = (float)base[c];
     }
 }
@@ -305,7 +311,7 @@ int orc_change_list_cap(int max_steps, int lateral)
 typedef struct {
     double dt, density, friction, deposition_rate, evap_rate, k_mom, mom_scale, k_disc, disc_saturation,
         disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
-        ocean_rate, fan_room, dep_floor;
+        ocean_rate, fan_room, dep_floor, lake_trap;
     int32_t max_steps, pit_steps, ocean_steps, deposit_on_exit, N, H, spherical, F;
     int32_t use_route, pad;
 } OrcTraceParams;
@@ -328,6 +334,7 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
     int32_t *ring = cl_cell + cap - SPREAD;
     double h_prev = -1e300;
     int exited = 0, in_sea = 0, cause = DEATH_AGE;
+    int in_lake = 0; /* on an overflowing lake: crossing, no exchange with the bed (particle.py:417) */
 #define RECORD(CELL, DELTA, VOL, MA, MB)                                   \
     do {                                                                   \
         cl_cell[n] = (int32_t)(CELL);                                      \
@@ -469,6 +476,12 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
                 k_e = P->deposition_rate;
             }
             double cdiff = k_e * (c_eq - sed);
+            if (in_lake) {
+                cdiff = 0.0; /* crossing a lake: the bed sees nothing (particle.py:626-629) */
+            } else if (sed > 0.0 && np_[S_RFLAG] >= 1.5f) {
+                double trap = -P->lake_trap * sed; /* entering a lake: the load drops at the shore (630-634) */
+                if (trap < cdiff) cdiff = trap;
+            }
             double kexp = 1.0 + q * P->conc_scale;
             if (cdiff > 0.0) {
                 double ecap = dh / kexp;
@@ -492,12 +505,13 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
         y = ny;
         f = nf;
         h_prev = h_here;
+        in_lake = np_[S_RFLAG] >= 1.5f;
         if (np_[S_SURF] < np_[S_BASE] && !in_sea) {
             in_sea = 1;
             if (sed <= 0.0) { cause = DEATH_OCEAN; break; }
         }
         if (vol < P->min_volume) { cause = in_sea ? DEATH_OCEAN : DEATH_EVAP; break; }
-        if (dhr < 0.0) {
+        if (dhr < 0.0 && !in_lake) {
             uphill++;
             if (uphill > P->pit_steps) { cause = in_sea ? DEATH_OCEAN : DEATH_PIT; break; }
         } else {
@@ -631,6 +645,10 @@ void orc_apply(const OrcApplyParams *A, const int32_t *cl_cell, const double *cl
                 }
                 if (e_act > room) e_act = room;
                 double floor_ = s_c >= b_c ? (double)b_c : s_c;
+                if (A->use_route && samp[c * NS + S_RFLAG] >= 1.5f) {
+                    double r_c = samp[c * NS + S_ROUTE]; /* a lake bed is never eroded below its water level */
+                    if (r_c > floor_) floor_ = r_c;
+                }
                 if (k + 1 < cnt) {
                     int64_t nc = cl_cell[base + k + 1];
                     double ns = height[nc] + sediment[nc] + acc[nc];

@@ -43,7 +43,7 @@ MASK_OUTSIDE, MASK_ACTIVE, MASK_FROZEN = 0, 1, 2
 DEATH_NAMES = ("age", "ocean", "exit", "pit", "evap", "stop")
 SPREAD, LAKE_PARKS = 8, 8
 NS = 16
-S_SURF, S_SED, S_BASE = 0, 7, 15
+S_SURF, S_ROUTE, S_SED, S_RFLAG, S_BASE = 0, 1, 7, 14, 15
 
 
 def build() -> Path:
@@ -82,7 +82,7 @@ class TraceParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
         "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
-        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor")] + [
+        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap")] + [
         (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F",
                                       "use_route", "pad")]
 
@@ -162,6 +162,9 @@ class OracleState:
     pending: np.ndarray = None
     iteration: int = 0
     route: np.ndarray = None  # the epsilon-filled routing surface (refresh_route) or None
+    #: overflowing lakes (uint8, 1 a lake, 2 a lake with room for its rivers' load; maps.py:87), set by the caller or
+    #: by refresh_lakes_window; read with the routing surface only
+    lake_flag: np.ndarray = None
     base_at: int = None  # iteration of the last sea-mask refresh (refresh_base)
     ice_prev: np.ndarray = None  # the last glacial pass's ice (erosion.glacial_sticky)
     land_target: float | None = None
@@ -230,7 +233,8 @@ class OracleState:
         n = self.height.size
         lib().orc_pack(ctypes.c_int64(n), _p(self.samp), _p(self.height), _p(self.sediment), _p(self.discharge),
                        _p(self.momentum), _p(self.evap), _p(self.hardness), _p(self.metric), _p(self.metric_inv),
-                       _p(self.base), None if getattr(self, "route", None) is None else _p(self.route))
+                       _p(self.base), None if getattr(self, "route", None) is None else _p(self.route),
+                       None if getattr(self, "lake_flag", None) is None else _p(self.lake_flag))
 
     def exchange_halos(self):
         if not self.spherical:
@@ -298,7 +302,7 @@ def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -
         slope_gain=float(ep.slope_gain), slope_sat=float(ep.slope_saturation), erodibility=float(ep.erodibility),
         cover_depth=_cu(ep, "cover_depth", u), min_volume=float(ep.min_volume_frac) * float(volume0),
         max_erode=_cu(ep, "max_erode", u), conc_scale=float(conc_scale), ocean_rate=float(ep.ocean_deposition_rate),
-        fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u),
+        fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u), lake_trap=float(getattr(ep, "lake_trap", 0.9)),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
         deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
         F=int(state.F), use_route=int(getattr(state, "route", None) is not None))
@@ -525,10 +529,31 @@ def refresh_route(state, eps):
     linear halo exchange."""
     from pgerosion.geometry import exchange_halos as xh
 
-    state.route = priority_flood_eps(state.height + state.sediment, state.mask, state.grid.owner, state.H, state.N, float(eps),
-                                     state.base)
+    owner = state.grid.owner if state.spherical else np.arange(state.height.size, dtype=np.int64).reshape(state.height.shape)
+    state.route = priority_flood_eps(state.height + state.sediment, state.mask, owner, state.H, state.N, float(eps), state.base)
     if state.spherical:
         xh(state.grid, state.route, linear=True)
+
+
+#: hydro.lake_min_depth's default (m): the depth a window lake must reach to be one
+LAKE_MIN_DEPTH_M = 0.5
+
+
+def refresh_lakes_window(state, min_depth, lake_evap=0.0) -> dict:
+    """maps.py:629-673 with lake_evap = 0: every depression the routing flood
+    fills more than ``min_depth`` (cell units) deep is an overflowing lake,
+    flagged on the interior's active cells (the halos stay 0)."""
+    if float(lake_evap) > 0.0:
+        raise NotImplementedError("the evaporation balance of window lakes (erosion.window_lake_evap > 0)")
+    flag = np.zeros(state.height.shape, np.uint8)
+    if state.route is None:
+        state.lake_flag = flag
+        return {"lake_cells": 0}
+    lake = ((state.route - (state.height + state.sediment)) > float(min_depth)) & (state.mask == MASK_ACTIVE)
+    inter = state.interior
+    flag[inter] = lake[inter]
+    state.lake_flag = flag
+    return {"lake_cells": int(lake[inter].sum())}
 
 
 def laplacian(state, d):
@@ -718,6 +743,13 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
         st_base = refresh_base(state, OCEAN_MIN_FRACTION)  # maps.py:1546-1551, before the route
     if int(getattr(ep, "flood_every", 0)) > 0 and (state.route is None or state.iteration % int(ep.flood_every) == 0):
         refresh_route(state, _cu(ep, "route_eps", state.height_unit_m))  # maps.py:1553-1554
+    st_lake = None
+    if not state.spherical and bool(getattr(ep, "window_lakes", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
+            (state.lake_flag is None or state.iteration % int(ep.flood_every) == 0):
+        hydro = getattr(params, "hydro", None)
+        depth_m = float(getattr(hydro, "lake_min_depth", LAKE_MIN_DEPTH_M)) if hydro is not None else LAKE_MIN_DEPTH_M
+        st_lake = refresh_lakes_window(state, depth_m / state.height_unit_m,
+                                       float(getattr(ep, "window_lake_evap", 0.0)))  # maps.py:1563-1566
     iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
     if iso:
         if getattr(state, "iso_acc", None) is None:
@@ -744,6 +776,8 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     state.iteration += 1
     if st_base is not None:
         st["sea"] = st_base
+    if st_lake is not None:
+        st["lakes"] = st_lake
     return st
 
 

@@ -234,13 +234,14 @@ def gen_trace(cs, maps, pk, WorldParams):
     print(f"trace_isolated: {keep.size} isolated droplets of {P}; deaths {np.bincount(res['sp_death'], minlength=6)}")
 
 
-def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit):
+def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit,
+               use_route=False):
     n = f.size
     out = dict(cl_cell=np.zeros(n * cap, np.int32), cl_delta=np.zeros(n * cap), cl_vol=np.zeros(n * cap, np.float32),
                cl_mom=np.zeros((n * cap, 2), np.float32), cl_count=np.zeros(n, np.int64), cl_lo=np.zeros(n, np.int64),
                cl_hi=np.zeros(n, np.int64), sp_death=np.zeros(n, np.int8))
     cu = lambda k: float(getattr(ep, k)) / unit
-    pk.trace_particles(f.astype(np.int64), x, y, sed, dirs, volume0, st_samp, False, mask, N, H, spherical,
+    pk.trace_particles(f.astype(np.int64), x, y, sed, dirs, volume0, st_samp, bool(use_route), mask, N, H, spherical,
                        float(ep.dt), float(ep.density), float(ep.friction), float(ep.deposition_rate), float(ep.evap_rate),
                        float(ep.k_mom), 1.0, float(ep.k_disc), float(ep.disc_saturation), float(ep.disc_exponent),
                        float(ep.slope_gain), float(ep.slope_saturation), float(ep.erodibility), cu("cover_depth"),
@@ -483,6 +484,133 @@ def gen_route(cs, maps, pk, WorldParams):
     print(f"route_flood: filled cells {(route > surf).sum()}, window filled {(wroute > wsurf).sum()}")
 
 
+def _window_of_evolved(cs, maps, pk, WorldParams):
+    """One face (with land and sea) of the N=48 world after three reference
+    iterations, as a window: an outside ring of 2 cells, a frozen margin of
+    3, the active basin inside."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=3, N=48, H=2, cell_size_m=50.0, land_fraction=0.35)
+    p = _world_params(WorldParams, 48, 2, 50.0, 3, 0.35, iterations=10, max_steps=64, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="stack")
+    st = _ref_state(cs, maps, world, p)
+    for it in range(3):
+        maps.step(st, p, it)
+    NE, H, N = st.NE, st.H, st.N
+    land = [(st.height[k][H:H + N, H:H + N] + st.sediment[k][H:H + N, H:H + N] >= 0).mean() for k in range(6)]
+    fw = int(np.argsort(land)[3])
+    sl = slice(fw, fw + 1)
+    w = {k: np.ascontiguousarray(getattr(st, k)[sl]) for k in ("height", "sediment", "discharge", "momentum", "evap", "hardness",
+                                                                "base", "metric", "metric_inv")}
+    mask = np.zeros((1, NE, NE), np.uint8)
+    mask[0, 2:NE - 2, 2:NE - 2] = 2
+    mask[0, 5:NE - 5, 5:NE - 5] = 1
+    return st, p, fw, w, mask
+
+
+def gen_lake_trace(cs, maps, pk, WorldParams):
+    """Lakes on a window (erosion.window_lakes): the reference's
+    ErosionState.refresh_route and refresh_lakes_window (maps.py:629-673) on
+    a window of the evolved N=48 world, then one trace + serial apply with
+    the routing surface and the lake flags packed (particle.py:186-190: flag
+    2 on a lake cell; 626-636: no exchange while crossing, the load dropped
+    at the shore; 763: no pit count on a lake; 952-956: the bed never eroded
+    below the water; 1010-1012: lake flags kept)."""
+    st, p, fw, w, mask = _window_of_evolved(cs, maps, pk, WorldParams)
+    ep = p.erosion
+    NE, H, N = st.NE, st.H, st.N
+    unit = st.height_unit_m
+    ws = maps.ErosionState(height=w["height"].copy(), sediment=w["sediment"].copy(), discharge=w["discharge"].copy(),
+                           momentum=w["momentum"].copy(), hardness=w["hardness"], precip=np.ones((1, NE, NE), np.float32),
+                           evap=w["evap"], uplift=np.zeros((1, NE, NE)), mask=mask, metric=w["metric"], metric_inv=w["metric_inv"],
+                           N=N, H=H, spherical=False, height_unit_m=unit, base=w["base"].copy(), deposit_on_exit=True)
+    eps = float(ep.route_eps) / unit
+    min_depth = float(p.hydro.lake_min_depth) / unit
+    ws.refresh_route(eps)
+    info = ws.refresh_lakes_window(min_depth, 0.0)
+    samp = np.zeros((1, NE, NE, pk.NS), np.float32)
+    pk.pack_samples(samp, w["height"], w["sediment"], ws.route, True, w["discharge"], w["momentum"], w["evap"], w["hardness"],
+                    w["metric"], w["metric_inv"], w["base"], ws.lake_flag)
+    rng = np.random.default_rng(93)
+    act = np.flatnonzero(mask.reshape(-1) == 1)
+    lakec = np.flatnonzero((ws.lake_flag.reshape(-1) > 0) & (mask.reshape(-1) == 1))
+    n_rain, n_load, n_lake = 1200, 250, 300
+    pick = np.concatenate([act[rng.integers(0, act.size, n_rain + n_load)], lakec[rng.integers(0, lakec.size, n_lake)]])
+    ei, ej = pick // NE, pick % NE
+    x = (ei - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5), rng.random(n_lake)])
+    y = (ej - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5), rng.random(n_lake)])
+    sed = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 0.5 + 1e-3, rng.random(n_lake) * 0.2])
+    dirs = np.concatenate([np.zeros(n_rain), rng.random(n_load + n_lake) * 2 * np.pi])
+    f = np.zeros(x.size, np.int64)
+    volume0 = 0.02
+    conc = 1.0 / (volume0 * x.size)
+    max_steps = maps.max_steps_of(ep, N)
+    cap = int(pk.change_list_cap(max_steps, False))
+    res = _ref_trace(pk, ep, samp, mask, N, H, False, True, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit, use_route=True)
+    acc = np.zeros_like(w["height"])
+    pending = np.zeros_like(w["height"])
+    dtr = np.zeros_like(w["height"])
+    mtr = np.zeros_like(w["momentum"])
+    samp_after = samp.copy()
+    cu = lambda k: float(getattr(ep, k)) / unit
+    ap = pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                          w["height"], w["sediment"], acc, pending, samp_after, dtr, mtr, mask, cu("iter_erode"), cu("iter_deposit"),
+                          float(ep.fan_slope), True, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                          np.zeros((1, NE, NE)), np.zeros((1, NE, NE), np.int32), np.zeros(1))
+    np.savez_compressed(
+        HERE / "lake_trace.npz", N=N, H=H, face=fw, **w, mask=mask, route=ws.route, lake_flag=ws.lake_flag, eps=eps,
+        min_depth=min_depth, sp_face=f, sp_x=x, sp_y=y, sp_sed=sed, sp_dir=dirs, volume0=volume0, conc_scale=conc, cap=cap,
+        max_steps=max_steps, deposit_on_exit=True, params=json.dumps({k: getattr(ep, k) for k in ep.__dataclass_fields__}),
+        cell_size_m=unit, **res, acc=acc, pending=pending, disch_track=dtr, mom_track=mtr,
+        rflag_after=samp_after[..., pk.S_RFLAG], apply_out=np.array([float(a) for a in ap]))
+    print(f"lake_trace: face {fw}, lakes {info}, {x.size} droplets, entries {int(res['cl_count'].sum())}, deaths "
+          f"{np.bincount(res['sp_death'], minlength=6)}, clamped {ap[0]}")
+
+
+def gen_step_lake(cs, maps, pk, WorldParams):
+    """Full steps on the sphere with lake flags set by the caller (the
+    kernel side of erosion.lake_balance, whose hydro-stage balance is not
+    run here: ErosionState.lake_flag = 1 where the routing surface stands
+    more than hydro.lake_min_depth over the terrain of the first refresh, 2
+    on faces 0-2 (a lake with room, packed as 3), halos copied from the
+    nearest interior cell as refresh_lakes does, maps.py:471-479); the
+    routing flood refreshed every 2 iterations (flood_every = 2)."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=7, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    iters = 5
+    p = _world_params(WorldParams, 32, 2, 50.0, 7, 0.45, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", flood_every=2)
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    unit = st.height_unit_m
+    st.refresh_route(float(p.erosion.route_eps) / unit)
+    H, N = st.H, st.N
+    inter = (slice(None), slice(H, H + N), slice(H, H + N))
+    lake = (st.route - (st.height + st.sediment)) > float(p.hydro.lake_min_depth) / unit
+    flag = np.zeros(st.height.shape, np.uint8)
+    flag[inter] = lake[inter]
+    flag[:3][flag[:3] > 0] = 2
+    hm = st.grid.halo
+    flat = flag.reshape(-1, 1)
+    flat[hm.dst] = flat[hm.nearest]
+    st.lake_flag = flag
+    planted = flag.copy()
+    stats = []
+    for it in range(iters):
+        s = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "to_pending", "released", "pending_total",
+                                         "deficit_out", "lost_offshore", "deaths", "datum_shift")})
+    np.savez_compressed(HERE / "step_lake.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=7, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h_start, lake_flag=planted, height=st.height, sediment=st.sediment, discharge=st.discharge,
+                        momentum=st.momentum, pending=st.pending, route=st.route, stats=json.dumps(stats), **init)
+    print("step_lake: lake cells", int((planted[inter] > 0).sum()), "of which with room", int((planted[inter] > 1).sum()),
+          "last", stats[-1])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -490,7 +618,9 @@ def main(bake: str, only: str | None = None):
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
             "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams),
-            "glacial": lambda: gen_glacial(cs, maps, pk, WorldParams)}
+            "glacial": lambda: gen_glacial(cs, maps, pk, WorldParams),
+            "lake_trace": lambda: gen_lake_trace(cs, maps, pk, WorldParams),
+            "step_lake": lambda: gen_step_lake(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

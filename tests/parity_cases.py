@@ -96,6 +96,49 @@ def window_case(path=GOLDEN / "window_trace.npz") -> dict:
     return case
 
 
+def lake_case(path=GOLDEN / "lake_trace.npz") -> dict:
+    """The window of window_case with the routing surface and the lakes of
+    the reference's refresh_lakes_window packed, droplets spawned on the
+    lakes too, and the reference's change lists and serial apply."""
+    t = np.load(path)
+    N, H = int(t["N"]), int(t["H"])
+    cs = float(t["cell_size_m"])
+    ep = erosion_params(str(t["params"]))
+    case = {k: t[k] for k in t.files if k not in ("params",)}
+    case.update(params=ep, N=N, H=H, cell_size_m=cs, volume0=float(t["volume0"]), conc_scale=float(t["conc_scale"]),
+                cap=int(t["cap"]), eps=float(t["eps"]), min_depth=float(t["min_depth"]))
+
+    def oracle_state():
+        from oracle import oracle as orc
+
+        NE = N + 2 * H
+        return orc.OracleState(height=t["height"].copy(), sediment=t["sediment"].copy(), discharge=t["discharge"].copy(),
+                               momentum=t["momentum"].copy(), hardness=t["hardness"], precip=np.ones((1, NE, NE), np.float32),
+                               evap=t["evap"], uplift=np.zeros((1, NE, NE)), mask=t["mask"], metric=t["metric"],
+                               metric_inv=t["metric_inv"], N=N, H=H, spherical=False, height_unit_m=cs, base=t["base"].copy(),
+                               deposit_on_exit=bool(t["deposit_on_exit"]))
+
+    def oracle():
+        from oracle import oracle as orc
+
+        st = oracle_state()
+        orc.refresh_route(st, case["eps"])
+        lakes = orc.refresh_lakes_window(st, case["min_depth"])
+        st.pack()
+        tp = orc.trace_params(st, ep, case["volume0"], case["conc_scale"])
+        cl = orc.trace(st, tp, t["sp_face"], t["sp_x"], t["sp_y"], t["sp_sed"], t["sp_dir"], case["volume0"])
+        out = orc.apply(st, orc.apply_params(st, ep, ep.iter_deposit / cs), cl, case["cap"])
+        names = ("cl_cell", "cl_delta", "cl_vol", "cl_mom", "cl_count", "cl_lo", "cl_hi", "sp_death")
+        r = dict(zip(names, cl))
+        r.update(acc=st.acc, pending=st.pending, disch_track=st.disch_track, mom_track=st.mom_track, apply_out=np.array(out, float),
+                 route=st.route, lake_flag=st.lake_flag, rflag_after=st.samp[..., orc.S_RFLAG].copy(), lakes=lakes)
+        return r
+
+    case["oracle"] = oracle
+    case["oracle_state"] = oracle_state
+    return case
+
+
 def step_case(path=GOLDEN / "step_tiny.npz") -> dict:
     """A six-face N=32 world and the reference's state after a few steps."""
     from pgerosion.synth import World

@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as orc
-from tests.parity_cases import GOLDEN, changelist_rows, isolated_case, step_case, window_case
+from tests.parity_cases import GOLDEN, changelist_rows, isolated_case, lake_case, step_case, window_case
 
 
 def test_cubesphere_vectors_bit_exact():
@@ -212,3 +212,76 @@ def test_glacial_steps_match_reference_bit_exact():
     for k in ("height", "sediment", "discharge", "momentum"):
         assert np.array_equal(getattr(st, k), t[k]), k
     assert np.array_equal(st.pending[inter], t["pending"][inter])
+
+
+def test_window_lakes_trace_and_apply_match_reference_bit_exact():
+    """Lakes on a window (erosion.window_lakes, maps.py:629-673): the
+    oracle's routing flood and lake flags equal the reference's, and with
+    them packed (flag 2 on a lake) the trace and serial apply equal the
+    reference's bit for bit: no exchange while crossing a lake, the load
+    dropped at the shore, no pit count on the water, the bed never eroded
+    below the water level, lake flags kept by the apply."""
+    case = lake_case()
+    res = case["oracle"]()
+    assert res["route"].tobytes() == case["route"].tobytes()
+    assert np.array_equal(res["lake_flag"], case["lake_flag"])
+    assert res["lakes"]["lake_cells"] > 10
+    cap = case["cap"]
+    for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
+        assert np.array_equal(res[k], case[k]), k
+    rows_ref = changelist_rows(case, cap)
+    for a, b in zip(changelist_rows(res, cap), rows_ref):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    # the lake branches are exercised: entries with no exchange on lake cells
+    lake = case["lake_flag"].reshape(-1) > 0
+    crossing = sum(int(((lake[c]) & (d == 0.0)).sum()) for c, d, _, _ in rows_ref)
+    assert crossing > 1000
+    for k in ("acc", "pending", "disch_track", "mom_track", "rflag_after"):
+        assert np.array_equal(res[k], case[k]), k
+    assert np.array_equal(res["apply_out"], case["apply_out"])
+
+
+def test_lake_flag_changes_the_pass():
+    """Planting mistakes in the oracle shows the fixture can tell: without
+    the lake flags, or with another shore trap, the change lists differ."""
+    case = lake_case()
+    from oracle import oracle as orc
+
+    def run(flags, trap):
+        st = case["oracle_state"]()
+        orc.refresh_route(st, case["eps"])
+        st.lake_flag = flags
+        st.pack()
+        ep = case["params"]
+        ep_t = type(ep)(**{**{k: getattr(ep, k) for k in ep.__dataclass_fields__}, "lake_trap": trap})
+        tp = orc.trace_params(st, ep_t, case["volume0"], case["conc_scale"])
+        return orc.trace(st, tp, case["sp_face"], case["sp_x"], case["sp_y"], case["sp_sed"], case["sp_dir"], case["volume0"])
+
+    ep = case["params"]
+    base = run(case["lake_flag"], float(ep.lake_trap))
+    assert np.array_equal(base[1], case["cl_delta"])
+    assert not np.array_equal(run(None, float(ep.lake_trap))[1], case["cl_delta"])
+    assert not np.array_equal(run(case["lake_flag"], 0.5)[1], case["cl_delta"])
+
+
+def test_lake_steps_match_reference_bit_exact():
+    """Full steps on the sphere with caller-set lake flags (1 and 2, halos
+    from the nearest interior cell) and the routing flood every 2
+    iterations: the oracle's state equals the reference's bit for bit."""
+    c = step_case(GOLDEN / "step_lake.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(st, c["params"])
+    assert np.array_equal(st.height, t["h_start"])
+    st.lake_flag = t["lake_flag"].copy()
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == r[k], (it, k)
+        assert s["datum_shift"] == r["datum_shift"]
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        assert np.array_equal(getattr(st, k), t[k]), k
+    inter = (slice(None), slice(st.H, st.H + st.N), slice(st.H, st.H + st.N))
+    assert np.array_equal(st.route[inter], t["route"][inter])
