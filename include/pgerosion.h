@@ -36,6 +36,9 @@
  *                                                  globe/erosion/maps.py:360-420,
  *                                                  globe/hydro/run.py:64-83,
  *                                                  globe/hydro/lakes.py:19-46
+ *   pge_window_lakes      ErosionState.refresh_lakes_window (lake_evap = 0): the
+ *                         overflowing lakes of a window
+ *                                                  globe/erosion/maps.py:629-673
  *   pge_glacial           glacial.carve (the ice line of the evaporation field)
  *                                                  globe/erosion/glacial.py:100-257,
  *                                                  globe/erosion/maps.py:1580-1590
@@ -148,6 +151,12 @@ typedef struct PgeState {
                                  reference's model): the calibrated field of the adjoint; wave apply only */
     const double *route;     /* (F,NE,NE) routing surface (pge_route_flood) or NULL: particles steer on it where it
                                 stands above the terrain (particle.py:453-460, 556-559); float64 trace only */
+    const uint8_t *lake_flag; /* (F,NE,NE) overflowing lakes (ErosionState.lake_flag, maps.py:87) or NULL; read only
+                                 with `route`: 1 a lake, 2 a lake with room for its rivers' load (the same to this
+                                 library, which parks no loads: erosion.lake_fill off).  A droplet entering a lake
+                                 drops lake_trap of its load at the shore, crosses it without touching the bed and
+                                 counts no pit steps on it; the bed is never eroded below the lake's routing surface
+                                 (particle.py:186-190, 626-636, 751-763, 952-956) */
 } PgeState;
 
 /* droplet spawns of one iteration: rain first, then re-injected stockpiles */
@@ -165,6 +174,8 @@ typedef struct PgeParams {
     double dt, density, friction, deposition_rate, evap_rate, k_mom, mom_scale, k_disc, disc_saturation,
         disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
         ocean_rate, fan_room, dep_floor, iter_erode, iter_deposit, fan_slope, offshore_writeoff, ema;
+    double lake_trap;        /* share of the load dropped at the shore on entering a lake (erosion.lake_trap);
+                                read only with s->lake_flag */
     int32_t max_steps, pit_steps, ocean_steps;
     int32_t wave;            /* droplets traced against one frozen terrain (the reference's chunk) */
     int32_t precision;       /* PGE_PREC_* */
@@ -381,6 +392,16 @@ PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *
  * grids only. */
 PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
                          int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream);
+
+/* The lakes of a window (maps.py:629-673, erosion.window_lakes with
+ * window_lake_evap = 0): lake_flag (F,NE,NE) = 1 on interior cells whose
+ * mask is active (every cell when s->mask is NULL) and whose routing surface
+ * s->route stands more than min_depth (cell units) above the surface
+ * s->height + s->sediment (float64), 0 on the rest and on the halos.
+ * lake_cells (device, may be NULL) gets their count.  Any grid; the planet's
+ * lakes (maps.py:422-479) come from the hydro stage's balance instead. */
+PGE_API int pge_window_lakes(const PgeGrid *g, const PgeState *s, double min_depth, uint8_t *lake_flag, int64_t *lake_cells,
+                             void *stream);
 
 /* The glacial pass (glacial.py:162-257), the ice line read from the
  * evaporation field: ice on active cells with evap <= ice_evap and surface

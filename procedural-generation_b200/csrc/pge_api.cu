@@ -235,6 +235,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.volume0 = sp->volume0;
         a.erod = s->erodibility;
         a.R = s->route ? ws_ptr<float2>(ws, lay.route2) : nullptr;
+        a.lakes = s->route && s->lake_flag ? 1 : 0;
         if (tape) a.tape = *tape;
         a.p = *p;
         a.acc4 = ws_ptr<long long>(ws, lay.acc4);
@@ -288,6 +289,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.A = ws_ptr<float4>(ws, lay.cellA);
             oa.B = ws_ptr<float4>(ws, lay.cellB);
             oa.R = s->route ? ws_ptr<float2>(ws, lay.route2) : nullptr;
+            oa.lakes = a.lakes;
             oa.mask = s->mask;
             oa.ecap = a.ecap;
             oa.acc4 = ws_ptr<double>(ws, lay.acc4);
@@ -529,6 +531,18 @@ PGE_API int pge_route_flood(const PgeGrid *g, const PgeState *s, const int32_t *
     if (e != cudaSuccess) return cuda_fail(e, "route_flood");
     if (sweeps) *sweeps = done;
     if (done < 0) return fail(PGE_E_UNSUPPORTED, "route_flood: not converged within %lld sweeps", (long long)max_sweeps);
+    return PGE_OK;
+}
+
+PGE_API int pge_window_lakes(const PgeGrid *g, const PgeState *s, double min_depth, uint8_t *lake_flag, int64_t *lake_cells,
+                             void *stream)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (!s || !s->height || !s->sediment || !s->route || !lake_flag) return fail(PGE_E_ARG, "window_lakes: NULL pointer");
+    if (!(min_depth >= 0.0)) return fail(PGE_E_ARG, "window_lakes: min_depth must be >= 0");
+    cudaError_t e = window_lakes(*g, *s, min_depth, lake_flag, lake_cells, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "window_lakes");
     return PGE_OK;
 }
 

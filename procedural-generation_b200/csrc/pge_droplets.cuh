@@ -418,7 +418,7 @@ __device__ __forceinline__ void tape_entry(const DropArgs &a, Ledger &L, long lo
     L.tap_n++;
 }
 
-template <bool TAPE = false>
+template <bool TAPE = false, bool ROUTE = false>
 __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger &L, const Entry &e, LCell &c, bool has_next,
                                             const LCell &nx, long long row = 0)
 {
@@ -449,6 +449,11 @@ __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger 
             src = 1;
         }
         double floor_ = s_c >= (double)b_c ? (double)b_c : s_c;
+        if (ROUTE && a.lakes) {
+            // a lake bed is never eroded below its water level (particle.py:952-956)
+            const float2 rc = __ldg(a.R + c.cell);
+            if (rc.y >= 1.5f && (double)rc.x > floor_) floor_ = (double)rc.x;
+        }
         if (has_next) {
             const double ns = nx.live();
             if (ns > floor_) {
@@ -601,6 +606,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
     int f = 0, step = 0, uphill = 0, sea_steps = 0, nring = 0;
     R x = R(0), y = R(0), sa = R(0), sb = R(0), vol = R(0), sed = R(0);
     bool in_sea = false, has_hprev = false;
+    bool in_lake = false;  // on an overflowing lake: crossing, no exchange with the bed (particle.py:417)
     float h_prev = 0.0f;
     int r0 = -1, r1 = -1, r2 = -1, r3 = -1, r4 = -1, r5 = -1, r6 = -1, r7 = -1;  // ring, newest first
     View cv;
@@ -638,7 +644,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                         sb = sin(dir);
                     }
                     step = uphill = sea_steps = nring = 0;
-                    in_sea = has_hprev = false;
+                    in_sea = has_hprev = in_lake = false;
                     r0 = r1 = r2 = r3 = r4 = r5 = r6 = r7 = -1;
                     has_pe = false;
                     L.deficit = L.surplus = 0.0;
@@ -804,6 +810,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 if (route_sample(a, nf, nx, ny, false, r1, unused_i, unused_j) && r1 > h1) h1r = r1;
             }
             const R dhr = h0r - h1r;
+            // the next cell's lake flag (2 or 3 on an overflowing lake)
+            const float nflag = ROUTE && a.lakes ? __ldg(&a.R[nv.cell].y) : 0.0f;
             if (TAPE && h1 > b1) tb |= PGE_TB_H1_ABOVE;
             // mass transfer at the cell we leave (particle.py:562-671)
             if (m == PGE_MASK_ACTIVE && in_sea) {
@@ -867,6 +875,14 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     k_e = k_depr;
                 }
                 R cdiff = k_e * (c_eq - sed);
+                if (ROUTE) {
+                    if (in_lake) {
+                        cdiff = R(0);  // crossing a lake: the bed sees nothing (particle.py:626-629)
+                    } else if (sed > R(0) && nflag >= 1.5f) {
+                        const R trap = -R(p.lake_trap) * sed;  // entering a lake: the load drops at the shore (630-634)
+                        if (trap < cdiff) cdiff = trap;
+                    }
+                }
                 const R kexp = R(1) + q * k_conc;
                 if (cdiff > R(0)) {
                     R ecap = dh / kexp;
@@ -919,6 +935,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             f = nf;
             h_prev = h_here;
             has_hprev = true;
+            if (ROUTE) in_lake = nflag >= 1.5f;
             cv = nv;
             moved = true;
             if (TAPE) a.tape.bits[trow * (a.tape.steps + 1) + step] = tb;
@@ -929,7 +946,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 if (sed <= R(0)) { cause = PGE_DEATH_OCEAN; break; }
             }
             if (vol < k_minvol) { cause = in_sea ? PGE_DEATH_OCEAN : PGE_DEATH_EVAP; break; }
-            if (dhr < R(0)) {
+            if (dhr < R(0) && !in_lake) {
                 uphill++;
                 if (uphill > p.pit_steps) { cause = in_sea ? PGE_DEATH_OCEAN : PGE_DEATH_PIT; break; }
             } else {
@@ -941,7 +958,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         if (have_entry) {
             // `cur` still describes the cell the entry was made at
             if (has_pe && LEDGER) {
-                apply_entry<TAPE>(a, t, L, pe, pend, true, cur, trow);
+                apply_entry<TAPE, ROUTE>(a, t, L, pe, pend, true, cur, trow);
                 sync_own(cur, pend);
                 sync_own(nxt, pend);
             }
@@ -1017,7 +1034,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         }
         if (nout > 0) load_lcell(a, t, ring[0], nxt);
         if (has_pe) {
-            apply_entry<TAPE>(a, t, L, pe, pend, nout > 0, nxt, trow);
+            apply_entry<TAPE, ROUTE>(a, t, L, pe, pend, nout > 0, nxt, trow);
             if (nout > 0) sync_own(nxt, pend);
         }
         for (int r = 0; r < nout; r++) {
@@ -1030,7 +1047,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             fe.vol = -1.0f;
             fe.ma = fe.mb = 0.0f;
             fe.sidx = -1;
-            apply_entry<TAPE>(a, t, L, fe, c, more, nxt, trow);
+            apply_entry<TAPE, ROUTE>(a, t, L, fe, c, more, nxt, trow);
             if (more) sync_own(nxt, c);
             if (a.rec_cell && rec_n < a.rec_cap) {
                 const long long o = (d - a.rec_base) * a.rec_cap + rec_n;

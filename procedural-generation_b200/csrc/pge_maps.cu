@@ -75,17 +75,37 @@ __global__ void refresh_kernel(long long ncell, const double *__restrict__ s, co
         A[c].x = surf;
         const double sd = s[c] + a;
         B[c].z = (float)(sd > 0.0 ? sd : 0.0);
-        if (R) R[c].y = R[c].x != surf ? 1.0f : 0.0f;  // the route flag follows the live surface (particle.py:1010-1012)
+        // the route flag follows the live surface; a lake cell stays a lake cell (particle.py:1010-1012)
+        if (R && R[c].y < 1.5f) R[c].y = R[c].x != surf ? 1.0f : 0.0f;
     }
 }
 
-// the routing surface and its flag, beside the packed surface (particle.py:165-190, no lakes)
+// the routing surface and its flag, beside the packed surface (particle.py:165-190): 2 on an
+// overflowing lake, 3 on one with room for its rivers' load, else 1 where the route is not the surface
 __global__ void pack_route_kernel(long long ncell, const double *__restrict__ h, const double *__restrict__ s,
-                                  const double *__restrict__ route, float2 *R)
+                                  const double *__restrict__ route, const uint8_t *__restrict__ lake, float2 *R)
 {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
         const float r = (float)route[c], surf = (float)(h[c] + s[c]);
-        R[c] = make_float2(r, r != surf ? 1.0f : 0.0f);
+        const uint8_t lk = lake ? lake[c] : (uint8_t)0;
+        R[c] = make_float2(r, lk > 0 ? (lk > 1 ? 3.0f : 2.0f) : (r != surf ? 1.0f : 0.0f));
+    }
+}
+
+// the lakes of a window (maps.py:662-672): interior active cells the routing surface covers more
+// than min_depth deep
+__global__ void window_lakes_kernel(long long ncell, int N, int H, const double *__restrict__ h, const double *__restrict__ s,
+                                    const double *__restrict__ route, const uint8_t *__restrict__ mask, double min_depth,
+                                    uint8_t *flag, unsigned long long *count)
+{
+    const int NE = N + 2 * H;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(c % NE), i = (int)((c / NE) % NE);
+        const bool inner = i >= H && i < H + N && j >= H && j < H + N;
+        const bool lake = inner && (!mask || mask[c] == PGE_MASK_ACTIVE) && route[c] - (h[c] + s[c]) > min_depth;
+        flag[c] = lake ? 1 : 0;
+        const unsigned ballot = __ballot_sync(__activemask(), lake);
+        if (count && ballot && (threadIdx.x & 31) == __ffs(ballot) - 1) atomicAdd(count, (unsigned long long)__popc(ballot));
     }
 }
 
@@ -163,7 +183,8 @@ void pack(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, cuda
                                              ws_ptr<float4>(ws, lay.cellA), ws_ptr<float4>(ws, lay.cellB),
                                              ws_ptr<double2>(ws, lay.live));
     pack_metric_kernel<<<grid_for(lay.nmetric), 256, 0, st>>>(lay.nmetric, s.metric, s.metric_inv, ws_ptr<float4>(ws, lay.metric8));
-    if (s.route) pack_route_kernel<<<grid_for(n), 256, 0, st>>>(n, s.height, s.sediment, s.route, ws_ptr<float2>(ws, lay.route2));
+    if (s.route)
+        pack_route_kernel<<<grid_for(n), 256, 0, st>>>(n, s.height, s.sediment, s.route, s.lake_flag, ws_ptr<float2>(ws, lay.route2));
 }
 
 void refresh(const PgeState &s, const Layout &lay, void *ws, cudaStream_t st)
@@ -1277,6 +1298,18 @@ int glacial(const PgeGrid &g, PgeState &st, uint8_t *ice_prev, const GlacialArgs
     }
     stats[4] = hs.parked;
     return 0;
+}
+
+cudaError_t window_lakes(const PgeGrid &g, const PgeState &st, double min_depth, uint8_t *flag, int64_t *count, cudaStream_t stream)
+{
+    const long long NE = g.N + 2LL * g.H, n = (long long)g.F * NE * NE;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(count);
+    if (cnt) {
+        const cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), stream);
+        if (e != cudaSuccess) return e;
+    }
+    window_lakes_kernel<<<grid_for(n), 256, 0, stream>>>(n, g.N, g.H, st.height, st.sediment, st.route, st.mask, min_depth, flag, cnt);
+    return cudaGetLastError();
 }
 
 }  // namespace pge

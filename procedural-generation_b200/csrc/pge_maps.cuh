@@ -19,6 +19,8 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// the lakes of a window (route deeper than min_depth over the surface on active interior cells)
+cudaError_t window_lakes(const PgeGrid &g, const PgeState &st, double min_depth, uint8_t *flag, int64_t *count, cudaStream_t stream);
 // routing surface (epsilon-filled priority flood); *sweeps_out < 0: not converged within max_sweeps
 cudaError_t route_flood(const PgeGrid &g, const PgeState &st, const int32_t *owner, double eps, double *route, const Layout &lay,
                         void *ws, long long max_sweeps, long long *sweeps_out, cudaStream_t s);

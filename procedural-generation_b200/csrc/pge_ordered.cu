@@ -235,19 +235,20 @@ struct alignas(16) Slot {
     unsigned long long h0, h1;  // the cell's hand-off word as prefetched
     CellTerr t;                 // the cell's read-only terrain
     double cap;                 // the slope erode cap (when on)
-    double pad;
+    float2 route;               // the cell's packed routing surface and flag (with lakes)
 };
 static_assert(sizeof(Slot) == 64, "slot layout");
 
 __device__ __forceinline__ void stage_desc(const OrderedArgs &a, Slot &s, long long e) { cp_cg16(&s.d, a.desc + e); }
 
-template <bool ECAP>
+template <bool ECAP, bool LAKE>
 __device__ __forceinline__ void stage_cell(const OrderedArgs &a, Slot &s)
 {
     const long long c = s.d.cell;
     cp_cg16(&s.h0, a.hand + c);
     cp_cg16(&s.t, a.terr + c);
     if (ECAP) cp_ca8(&s.cap, a.ecap + c);
+    if (LAKE) cp_ca8(&s.route, a.R + c);
 }
 
 // per droplet state carried from entry to entry
@@ -292,7 +293,7 @@ __device__ __forceinline__ bool cell_value(const OrderedArgs &a, const Walk &w, 
 }
 }  // namespace
 
-template <bool ECAP>
+template <bool ECAP, bool LAKE>
 __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const OrderedArgs a)
 {
     __shared__ unsigned long long sstat[OS_N];
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
         for (int j = 0; j < 5 && j < K; j++) stage_desc(a, R[j], b0 + j);
         cp_commit();
         cp_wait<0>();
-        for (int j = 0; j < 3 && j < K; j++) stage_cell<ECAP>(a, R[j]);
+        for (int j = 0; j < 3 && j < K; j++) stage_cell<ECAP, LAKE>(a, R[j]);
         cp_commit();
         cp_wait<0>();
         Walk w;
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
             // the copies issued two or more entries ago have landed: the descriptor of entry k+3
             // and the cell data of entries k and k+1
             cp_wait<1>();
-            if (k + 3 < K) stage_cell<ECAP>(a, R[(k + 3) & (RING - 1)]);
+            if (k + 3 < K) stage_cell<ECAP, LAKE>(a, R[(k + 3) & (RING - 1)]);
             if (k + 5 < K) stage_desc(a, R[(k + 5) & (RING - 1)], b0 + k + 5);
             cp_commit();
             const Slot &cur = R[k & (RING - 1)];
@@ -375,6 +376,8 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
                     }
                     if (e_act > room) e_act = room;
                     double floor_ = s_c >= b_c ? b_c : s_c;
+                    // a lake bed is never eroded below its water level (particle.py:952-956)
+                    if (LAKE && cur.route.y >= 1.5f && (double)cur.route.x > floor_) floor_ = (double)cur.route.x;
                     if (has_next && nlive > floor_) floor_ = nlive;
                     if (e_act > s_c - floor_) e_act = s_c - floor_;
                     if (e_act < 0.0) e_act = 0.0;
@@ -570,7 +573,8 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
             a.A[c].x = surf;
             const double sd = a.sediment[c] + acc;
             a.B[c].z = (float)(sd > 0.0 ? sd : 0.0);
-            if (a.R) a.R[c].y = a.R[c].x != surf ? 1.0f : 0.0f;  // the route flag follows the live surface
+            // the route flag follows the live surface; a lake cell stays a lake cell (particle.py:1010-1012)
+            if (a.R && a.R[c].y < 1.5f) a.R[c].y = a.R[c].x != surf ? 1.0f : 0.0f;
         }
     }
     if (eroded) atomicAdd(&sfx[0], (unsigned long long)eroded);
@@ -606,7 +610,7 @@ int ordered_blocks_per_sm(int lanes)
 {
     int n = 0;
     const size_t smem = (size_t)(APPLY_THREADS / 32) * lanes * RING * sizeof(Slot);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false>, APPLY_THREADS, smem) != cudaSuccess) return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false, false>, APPLY_THREADS, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
 }
 
@@ -629,10 +633,15 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     long long blocks = (warps * 32 + APPLY_THREADS - 1) / APPLY_THREADS;
     if (blocks > w.max_blocks) blocks = w.max_blocks;
     const size_t smem = (size_t)(APPLY_THREADS / 32) * w.a.lanes * RING * sizeof(Slot);
-    if (w.a.ecap)
-        ordered_apply_kernel<true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
+    const bool lake = w.a.lakes && w.a.R;
+    if (w.a.ecap && lake)
+        ordered_apply_kernel<true, true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
+    else if (w.a.ecap)
+        ordered_apply_kernel<true, false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
+    else if (lake)
+        ordered_apply_kernel<false, true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     else
-        ordered_apply_kernel<false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
+        ordered_apply_kernel<false, false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
     return cudaPeekAtLastError();
 }

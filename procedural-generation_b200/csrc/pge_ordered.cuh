@@ -39,6 +39,7 @@ struct OrderedArgs {
     float4 *A;
     float4 *B;
     float2 *R;  // packed routing surface (route, flag) or nullptr: flags follow the live surface
+    int lakes;  // R's flags mark overflowing lakes: a lake bed is not eroded below its routing surface
     const uint8_t *mask;
     const double *ecap;
     // per cell: the live net change and the hand-off counter, one 16-byte word

@@ -27,6 +27,7 @@ EXPORTS = (
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
     "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base", "pge_glacial",
+    "pge_window_lakes",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -42,7 +43,8 @@ class PgeGrid(ctypes.Structure):
 
 class PgeState(ctypes.Structure):
     _fields_ = [(n, c_vp) for n in ("height", "sediment", "discharge", "momentum", "pending", "base", "uplift",
-                                    "hardness", "precip", "evap", "mask", "metric", "metric_inv", "erodibility", "route")]
+                                    "hardness", "precip", "evap", "mask", "metric", "metric_inv", "erodibility", "route",
+                                    "lake_flag")]
 
 
 class PgeSpawns(ctypes.Structure):
@@ -52,7 +54,7 @@ class PgeSpawns(ctypes.Structure):
 PARAM_DOUBLES = ("dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
                  "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
                  "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "iter_erode",
-                 "iter_deposit", "fan_slope", "offshore_writeoff", "ema")
+                 "iter_deposit", "fan_slope", "offshore_writeoff", "ema", "lake_trap")
 PARAM_INTS = ("max_steps", "pit_steps", "ocean_steps", "wave", "precision", "apply", "use_erode_cap", "threads_per_block",
               "blocks_per_sm", "trace_lanes", "apply_lanes")
 
@@ -127,6 +129,7 @@ def load(path: str | os.PathLike | None = None):
                                    c_vp, c_vp, c_vp, ctypes.c_size_t, c_vp]
     L.pge_halo_adjoint.argtypes = [P(PgeHalo), c_vp, c_vp]
     L.pge_route_flood.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]
+    L.pge_window_lakes.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_vp, c_vp, c_vp]
     L.pge_glacial.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_f64, c_i32, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp,
                               ctypes.c_size_t, c_vp]
     L.pge_sea_base.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_vp, c_f64, c_vp, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]

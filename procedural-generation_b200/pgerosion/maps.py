@@ -88,6 +88,9 @@ class ErosionState:
     erodibility: torch.Tensor = field(default=None, repr=False)
     #: the epsilon-filled routing surface (float64, (F, NE, NE), cell units) or None (refresh_route)
     route: torch.Tensor = field(default=None, repr=False)
+    #: overflowing lakes (uint8, (F, NE, NE): 1 a lake, 2 a lake with room for its rivers' load; maps.py:87) or None:
+    #: set by the caller (the hydro stage's balance) or by refresh_lakes_window; read with the routing surface only
+    lake_flag: torch.Tensor = field(default=None, repr=False)
     #: iteration of the last sea-mask refresh (refresh_base), None before the first
     base_at: int = None
     #: the last glacial pass's ice (uint8, (F, NE, NE)) for erosion.glacial_sticky, None before the first
@@ -176,7 +179,7 @@ class ErosionState:
                         momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
                         hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
                         metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility),
-                        route=_ptr(self.route))
+                        route=_ptr(self.route), lake_flag=_ptr(self.lake_flag))
 
     def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to
@@ -272,6 +275,26 @@ class ErosionState:
         self.exchange_field(self.route, linear=True)
         return int(n.value)
 
+    def refresh_lakes_window(self, min_depth: float, lake_evap: float = 0.0) -> dict:
+        """The lakes of a window (maps.py:629-673, erosion.window_lakes): every
+        depression the routing surface fills more than ``min_depth`` (cell
+        units) deep is an overflowing lake, flagged on the interior's active
+        cells; particles cross it without touching the bed, drop their load at
+        its shore and are not counted as climbing inside it.  Must run after
+        :meth:`refresh_route`.  The evaporation balance of ``lake_evap > 0``
+        (erosion.window_lake_evap) is not supported."""
+        if float(lake_evap) > 0.0:
+            raise ValueError("the b200 erosion backend has no window lake balance: erosion.window_lake_evap must be 0")
+        if self.lake_flag is None or self.lake_flag.shape != self.height.shape:
+            self.lake_flag = torch.zeros(self.height.shape, dtype=torch.uint8, device=self.height.device)
+        if self.route is None:
+            self.lake_flag.zero_()
+            return {"lake_cells": 0}
+        n = torch.zeros(1, dtype=torch.int64, device=self.height.device)
+        check(_lib.load().pge_window_lakes(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), float(min_depth),
+                                           _ptr(self.lake_flag), _ptr(n), _stream()), "pge_window_lakes")
+        return {"lake_cells": int(n.item())}
+
     def refresh_base(self, min_fraction: float = 0.02, max_sweeps: int = 1 << 22) -> dict:
         """Recompute the base level (maps.py:360-420): 0 on the open ocean
         and on land, a closed below-sea basin's deepest surface on its cells
@@ -345,7 +368,7 @@ def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, prec
         fan_room=cell_units(ep, "fan_room", u), dep_floor=cell_units(ep, "dep_floor_m", u), iter_erode=cell_units(ep, "iter_erode", u),
         iter_deposit=float(cell_units(ep, "iter_deposit", u) if iter_deposit is None else iter_deposit),
         fan_slope=float(ep.fan_slope), offshore_writeoff=float(ep.offshore_writeoff), ema=float(ep.ema),
-        max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
+        lake_trap=float(getattr(ep, "lake_trap", 0.9)), max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
         precision=int(precision), apply=int(apply), use_erode_cap=0, threads_per_block=int(threads_per_block),
         blocks_per_sm=int(blocks_per_sm), trace_lanes=int(trace_lanes), apply_lanes=int(apply_lanes))
 
@@ -643,6 +666,13 @@ def ocean_min_fraction(params) -> float:
     return float(getattr(hydro, "ocean_min_fraction", 0.02)) if hydro is not None else 0.02
 
 
+def lake_min_depth(params) -> float:
+    """``hydro.lake_min_depth`` (m) when the params carry a hydro group, else
+    the bake's 0.5 (maps.py:1564)."""
+    hydro = getattr(params, "hydro", None)
+    return float(getattr(hydro, "lake_min_depth", 0.5)) if hydro is not None else 0.5
+
+
 def held_land_fraction(state: ErosionState, params) -> float:
     if state.land_target is not None:
         return float(state.land_target)
@@ -683,6 +713,12 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     if flood > 0 and (state.route is None or state.iteration % flood == 0):
         # the routing surface the particles steer on (maps.py:1553-1554)
         state.refresh_route(cell_units(ep, "route_eps", state.height_unit_m))
+    st_lake = None
+    if not state.spherical and bool(getattr(ep, "window_lakes", False)) and flood > 0 and \
+            (state.lake_flag is None or state.iteration % flood == 0):
+        # a window's lakes, after the route they are read off (maps.py:1563-1566)
+        st_lake = state.refresh_lakes_window(lake_min_depth(params) / state.height_unit_m,
+                                             float(getattr(ep, "window_lake_evap", 0.0)))
     t_route = time.time()
     iso = state.spherical and float(getattr(ep, "isostasy", 0.0)) > 0.0
     if iso:
@@ -715,6 +751,8 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     state.iteration += 1
     if st_base is not None:
         st["sea"] = st_base
+    if st_lake is not None:
+        st["lakes"] = st_lake
     st["seconds_route"] = t_route - t0
     st["seconds_particles"] = t1 - t_route
     st["seconds_total"] = time.time() - t0

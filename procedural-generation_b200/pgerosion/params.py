@@ -111,6 +111,7 @@ class ErosionParams:
     lake_balance: bool = True
     lateral_rate: float = 0.0
     window_lakes: bool = False
+    window_lake_evap: float = 0.0
     lake_fill: bool = True
     lake_trap: float = 0.9
     dep_floor_m: float = 1.0
@@ -192,10 +193,13 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (lakes, ice sheet, lateral cut, basin fill).  Isostasy, the routing
-    surface (``flood_every``), the sea mask (``sea_mask_every``) and the
-    glacial pass (``glacial_every``, the ice line of the evaporation field)
-    are supported."""
+    path (the planet's lake balance, the window lake balance, ice sheet,
+    lateral cut, basin fill).  Isostasy, the routing surface
+    (``flood_every``), the sea mask (``sea_mask_every``), the glacial pass
+    (``glacial_every``, the ice line of the evaporation field) and the lakes
+    of a window (``window_lakes`` with ``window_lake_evap = 0``) are
+    supported; lake flags set on the state by the caller are read on the
+    planet too."""
     bad = []
     if bool(getattr(ep, "lake_balance", False)):
         bad.append("lake_balance")
@@ -205,5 +209,7 @@ def check_plain(ep) -> None:
         bad.append("ice_sheet")
     if float(getattr(ep, "basin_fill_grade", 0.0)) > 0.0:
         bad.append("basin_fill_grade")
+    if bool(getattr(ep, "window_lakes", False)) and float(getattr(ep, "window_lake_evap", 0.0)) > 0.0:
+        bad.append("window_lake_evap")
     if bad:
         raise ValueError("the b200 erosion backend runs the plain particle path only; switch off: " + ", ".join(bad))

@@ -7,7 +7,9 @@ Same contract: ``OUTPUTS`` and ``run(store, params, log) -> info``
 ``sediment``, ``discharge``, ``momentum`` as float32 metres (maps.py:738-752).
 Checkpoints keep the bake's format (run.py:100-225): ``erosion_iterNNNN.npz``
 with the float64 cell-unit arrays ``height, sediment, discharge, momentum,
-pending, lake_load``, written to ``.tmp`` then renamed, then a ``.json`` with
+pending, lake_load`` (plus the refreshed state: routing surface, base level,
+isostatic load, sticky ice, and the lake flags with ``lake_id, lake_room``),
+written to ``.tmp`` then renamed, then a ``.json`` with
 the iteration and the parameter hash; the two newest checkpoints of a hash
 family are kept; a run resumes from the newest matching checkpoint at or
 below its end.  The hash adds this backend's token and apply mode, because
@@ -108,7 +110,20 @@ def _state_fields(state) -> list:
         out.append("iso_acc")
     if state.ice_prev is not None:
         out.append("ice_prev")
+    if state.lake_flag is not None:
+        out.append("lake_flag")
     return out
+
+
+def _lake_arrays(arrays: dict) -> None:
+    """The lake arrays the reference's checkpoints always hold (run.py:125-128;
+    its state has lake flags from the first pack on): the flags (zeros when
+    the state has none), and the parked-load bookkeeping this library keeps
+    at its initial values (lake_id -1, lake_room 0: no loads are parked)."""
+    if "lake_flag" not in arrays:
+        arrays["lake_flag"] = np.zeros(arrays["height"].shape, np.uint8)
+    arrays["lake_id"] = np.full(arrays["height"].shape, -1, np.int32)
+    arrays["lake_room"] = np.zeros(1, np.float64)
 
 
 def _write_checkpoint(d: Path, it: int, arrays: dict, meta: dict) -> Path:
@@ -138,6 +153,7 @@ def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
     arrays["lake_load"] = np.zeros_like(a["height"])
     for k in _state_fields(state):
         arrays[k] = getattr(state, k).detach().cpu().numpy()
+    _lake_arrays(arrays)
     return _write_checkpoint(d, state.iteration, arrays, _ckpt_meta(state, params, apply))
 
 
@@ -192,6 +208,7 @@ class CheckpointWriter:
             arrays["lake_load"] = np.zeros_like(arrays["height"])
             for k in extra:
                 arrays[k] = self._host[k].numpy()
+            _lake_arrays(arrays)
             # the writer reads the pinned buffers only until np.savez returns
             return _write_checkpoint(self.dir, it, arrays, meta)
 
@@ -272,6 +289,7 @@ def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
         else:
             state.base_at = None
         state.ice_prev = torch.as_tensor(np.asarray(z["ice_prev"], np.uint8), device=dev) if "ice_prev" in z.files else None
+        state.lake_flag = torch.as_tensor(np.asarray(z["lake_flag"], np.uint8), device=dev) if "lake_flag" in z.files else None
     state.iteration = int(meta["iteration"])
 
 
