@@ -39,6 +39,13 @@
  *   pge_window_lakes      ErosionState.refresh_lakes_window (lake_evap = 0): the
  *                         overflowing lakes of a window
  *                                                  globe/erosion/maps.py:629-673
+ *   pge_lake_balance      ErosionState.refresh_lakes without erosion.lake_fill: the
+ *                         planet's lakes by the hydro stage's flood, D8 routing and
+ *                         evaporation balance (HOST code, host pointers)
+ *                                                  globe/erosion/maps.py:422-479,
+ *                                                  globe/hydro/priority_flood.py:127-191,
+ *                                                  globe/hydro/routing.py:28-90,
+ *                                                  globe/hydro/balance.py:63-284
  *   pge_glacial           glacial.carve (the ice line of the evaporation field)
  *                                                  globe/erosion/glacial.py:100-257,
  *                                                  globe/erosion/maps.py:1580-1590
@@ -402,6 +409,41 @@ PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *own
  * lakes (maps.py:422-479) come from the hydro stage's balance instead. */
 PGE_API int pge_window_lakes(const PgeGrid *g, const PgeState *s, double min_depth, uint8_t *lake_flag, int64_t *lake_cells,
                              void *stream);
+
+/* counts of one lake refresh (maps.py:481-483 and the balance's, balance.py:270-279) */
+typedef struct PgeLakeInfo {
+    int64_t lake_cells;        /* cells deeper than min_depth under water, off the ocean */
+    int64_t lake_cells_closed; /* of those, cells of lakes drawn below their rim */
+    int64_t depressions, overflowing, closed, dry;
+} PgeLakeInfo;
+
+/* The planet's lakes (maps.py:422-479 with erosion.lake_fill off), on the
+ * HOST: every pointer is a host pointer and no CUDA call is made.  The
+ * reference's sequence is serial by construction -- every later step follows
+ * the priority flood's pop order -- so it runs as one host pass between
+ * iterations, as the reference's does.  Inputs, interior (6,N,N) arrays in
+ * cell-id order (f*N + i)*N + j: surface (float32 height + sediment), ocean
+ * (1 on the open sea: the flood's drains), precip (the spawn weight), pet (the
+ * balance's potential evaporation: the state's evap, or lake_pet), cell_area
+ * (float32 m^2); owner (6,NE,NE) int32 the extended flat index of the
+ * interior cell owning each extended cell; metric (NE,NE,3) float32, shared
+ * by the faces.  The flood fills every depression from the drains (a FIFO for
+ * cells at or below the current level, a (level, push order) heap for the
+ * rest; the lowest cell drains when there is no ocean), D8 descends the
+ * filled surface by physical slope (flats to their flood parent), and one
+ * upstream-first accumulation of the runoff (Budyko's curve with land_evap >
+ * 0, else all of precip) solves each depression's level where its
+ * evaporation (lake_evap x pet, or pet less the land's evaporation with
+ * land_evap > 0) meets its inflow.  Outputs (6,N,N): lake_flag 1 on cells
+ * of overflowing lakes deeper than min_depth (cell units); closed_level (may
+ * be NULL) the water level (cell units) on cells of lakes drawn more than
+ * 1e-4 below their rim (the caller's base level there), NaN elsewhere; water
+ * (may be NULL) the water surface.  PGE_E_UNSUPPORTED if a land cell gets no
+ * flow direction (the flood did not reach it). */
+PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
+                             const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
+                             double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
+                             PgeLakeInfo *info);
 
 /* The glacial pass (glacial.py:162-257), the ice line read from the
  * evaporation field: ice on active cells with evap <= ice_evap and surface

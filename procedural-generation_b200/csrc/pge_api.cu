@@ -546,6 +546,24 @@ PGE_API int pge_window_lakes(const PgeGrid *g, const PgeState *s, double min_dep
     return PGE_OK;
 }
 
+PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
+                             const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
+                             double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
+                             PgeLakeInfo *info)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (!g->spherical) return fail(PGE_E_UNSUPPORTED, "lake_balance: the planet's lakes (a window's come from pge_window_lakes)");
+    if (!owner || !metric || !cell_area || !surface || !ocean || !precip || !pet || !lake_flag)
+        return fail(PGE_E_ARG, "lake_balance: NULL pointer");
+    if (!(cell_size_m > 0.0) || !(min_depth >= 0.0) || !(lake_evap >= 0.0) || !(land_evap >= 0.0))
+        return fail(PGE_E_ARG, "lake_balance: cell_size_m must be > 0 and min_depth, lake_evap, land_evap >= 0");
+    if (lake_balance_host(g->N, g->H, owner, metric, cell_area, cell_size_m, surface, ocean, precip, pet, lake_evap, land_evap,
+                          min_depth, lake_flag, water, closed_level, info) != 0)
+        return fail(PGE_E_UNSUPPORTED, "lake_balance: a land cell has no flow direction (unreached by the flood)");
+    return PGE_OK;
+}
+
 PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
                          int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream)
 {

@@ -1,0 +1,367 @@
+// The planet's lake balance on the host: ErosionState.refresh_lakes
+// (globe/erosion/maps.py:422-479) with erosion.lake_fill off.
+//
+// The reference runs the hydro stage's own sequence on the eroding surface:
+// the priority flood of the whole sphere with a FIFO for depression cells
+// (globe/hydro/priority_flood.py:127-191, 294-318), D8 on the filled surface
+// with flats draining to their flood parent (globe/hydro/routing.py:28-90,
+// globe/hydro/d8.py:123-136), then the evaporation balance of every
+// depression in one upstream-first accumulation (globe/hydro/balance.py:63-108,
+// 159-284, depressions labelled by globe/hydro/lakes.py:18-46).  Every step
+// after the flood follows the flood's pop order, which is a strictly serial
+// quantity (each pop depends on every earlier one), so this runs as one host
+// pass between iterations, as the reference's does, every erosion.flood_every
+// iterations; the device hands it the float32 surface and the sea mask and
+// takes back the lake flags and the closed lakes' levels.
+//
+// The arithmetic mirrors the reference's types: surfaces and the filled
+// surface in float32, slopes from float32 height differences over a float64
+// step length, the balance in float64, the water surface and the depth tests
+// in float32.  Compiled without floating-point contraction.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <queue>
+#include <vector>
+
+#include "../../include/pgerosion.h"
+
+namespace pge {
+namespace {
+
+constexpr int D8_DI[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+constexpr int D8_DJ[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+constexpr uint8_t FD_OCEAN = 255;
+
+// cell ids are interior flat indices (f * N + i) * N + j; `owner` maps an extended cell to the
+// extended flat index of the interior cell that owns it
+struct Sphere {
+    int N, H, NE;
+    const int32_t *owner;
+
+    int64_t neighbor(int64_t c, int k) const
+    {
+        const int64_t NN = (int64_t)N * N;
+        const int f = (int)(c / NN);
+        const int64_t rem = c - f * NN;
+        const int i = (int)(rem / N), j = (int)(rem - (int64_t)i * N);
+        const int64_t o = owner[((int64_t)f * NE + i + H + D8_DI[k]) * NE + j + H + D8_DJ[k]];
+        const int64_t NE2 = (int64_t)NE * NE;
+        const int f2 = (int)(o / NE2);
+        const int64_t r2 = o - f2 * NE2;
+        const int ei = (int)(r2 / NE), ej = (int)(r2 - (int64_t)ei * NE);
+        return ((int64_t)f2 * N + (ei - H)) * N + (ej - H);
+    }
+    int code_towards(int64_t c, int64_t target) const
+    {
+        for (int k = 0; k < 8; k++)
+            if (neighbor(c, k) == target) return k;
+        return -1;
+    }
+};
+
+struct HeapItem {
+    double key;
+    int64_t seq, cell;
+};
+struct HeapAfter {
+    bool operator()(const HeapItem &a, const HeapItem &b) const { return a.key > b.key || (a.key == b.key && a.seq > b.seq); }
+};
+
+// priority flood: the filled surface, each cell's flood parent and the pop sequence; drains are
+// the ocean cells (or the lowest cell when there is no ocean)
+void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, std::vector<float> &filled,
+           std::vector<int64_t> &parent, std::vector<int64_t> &order, std::vector<int64_t> &pop_seq)
+{
+    const int64_t M = (int64_t)6 * S.N * S.N;
+    bool any = false;
+    for (int64_t c = 0; c < M && !any; c++) any = drain[c] != 0;
+    if (!any) {
+        int64_t lo = 0;
+        for (int64_t c = 1; c < M; c++)
+            if (surface[c] < surface[lo]) lo = c;
+        drain[lo] = 1;
+    }
+    filled.assign(surface, surface + M);
+    parent.assign(M, -1);
+    order.assign(M, -1);
+    pop_seq.clear();
+    pop_seq.reserve(M);
+    std::vector<uint8_t> visited(M, 0);
+    std::priority_queue<HeapItem, std::vector<HeapItem>, HeapAfter> heap;
+    std::vector<int64_t> fifo;
+    fifo.reserve(1024);
+    int64_t seq = 0;
+    for (int64_t c = 0; c < M; c++) {
+        if (!drain[c]) continue;
+        visited[c] = 1;
+        bool push = false;
+        for (int k = 0; k < 8 && !push; k++) push = !drain[S.neighbor(c, k)];
+        if (push) heap.push({(double)surface[c], seq++, c});
+    }
+    size_t head = 0;
+    const int64_t NN = (int64_t)S.N * S.N;
+    while (head < fifo.size() || !heap.empty()) {
+        int64_t c;
+        if (head < fifo.size()) {
+            c = fifo[head++];
+            if (head == fifo.size()) {
+                fifo.clear();
+                head = 0;
+            }
+        } else {
+            c = heap.top().cell;
+            heap.pop();
+        }
+        const float lvl = filled[c];
+        order[c] = (int64_t)pop_seq.size();
+        pop_seq.push_back(c);
+        const int64_t f = c / NN;
+        for (int k = 0; k < 8; k++) {
+            const int64_t n = S.neighbor(c, k);
+            if (visited[n]) continue;
+            // across a face edge the nearest-cell mapping can be one-sided: only reversible links
+            if (n / NN != f && S.code_towards(n, c) < 0) continue;
+            visited[n] = 1;
+            parent[n] = c;
+            if (surface[n] <= lvl) {
+                filled[n] = lvl;
+                fifo.push_back(n);
+            } else {
+                filled[n] = surface[n];
+                heap.push({(double)surface[n], seq++, n});
+            }
+        }
+    }
+}
+
+// D8 on the filled surface: steepest physical descent among strictly lower neighbours, else the
+// flood parent; returns false when a land cell has no direction (the flood never reached it)
+bool flow_down(const Sphere &S, const float *metric, const std::vector<float> &filled, const uint8_t *ocean,
+               const std::vector<int64_t> &parent, std::vector<int64_t> &down)
+{
+    const int64_t M = (int64_t)6 * S.N * S.N, NN = (int64_t)S.N * S.N;
+    down.assign(M, -1);
+    for (int64_t c = 0; c < M; c++) {
+        if (ocean[c]) continue;
+        const int64_t rem = c % NN;
+        const int i = (int)(rem / S.N), j = (int)(rem % S.N);
+        const float *g = metric + 3 * ((int64_t)(i + S.H) * S.NE + (j + S.H));
+        const float hc = filled[c];
+        int best = -1;
+        double best_s = 0.0;
+        for (int k = 0; k < 8; k++) {
+            const int64_t n = S.neighbor(c, k);
+            const float hn = filled[n];
+            if (hn < hc) {
+                const double di = D8_DI[k], dj = D8_DJ[k];
+                const double d2 = (double)g[0] * di * di + 2.0 * (double)g[1] * di * dj + (double)g[2] * dj * dj;
+                const float dh = hc - hn;
+                const double s = (double)dh / std::sqrt(d2);
+                if (s > best_s) {
+                    best_s = s;
+                    best = k;
+                }
+            }
+        }
+        if (best < 0 && parent[c] >= 0) best = S.code_towards(c, parent[c]);
+        if (best < 0) return false;
+        down[c] = S.neighbor(c, best);
+    }
+    return true;
+}
+
+// 8-connected components of `mask` joining only cells of identical level, numbered by their lowest
+// cell id
+int64_t label_components(const Sphere &S, const std::vector<uint8_t> &mask, const std::vector<float> &level,
+                         std::vector<int64_t> &labels)
+{
+    const int64_t M = (int64_t)mask.size();
+    labels.assign(M, -1);
+    std::vector<int64_t> stack;
+    int64_t n = 0;
+    for (int64_t s = 0; s < M; s++) {
+        if (!mask[s] || labels[s] >= 0) continue;
+        labels[s] = n;
+        stack.push_back(s);
+        while (!stack.empty()) {
+            const int64_t c = stack.back();
+            stack.pop_back();
+            for (int k = 0; k < 8; k++) {
+                const int64_t q = S.neighbor(c, k);
+                if (mask[q] && labels[q] < 0 && level[q] == level[c]) {
+                    labels[q] = n;
+                    stack.push_back(q);
+                }
+            }
+        }
+        n++;
+    }
+    return n;
+}
+
+double budyko(double aridity)
+{
+    const double a = aridity > 1e-9 ? aridity : 1e-9;
+    return std::sqrt(a * std::tanh(1.0 / a) * (1.0 - std::exp(-a)));
+}
+
+}  // namespace
+
+// returns 0, or -1 when a land cell got no flow direction
+int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
+                      const float *surface, const uint8_t *ocean_in, const float *precip, const float *pet, double lake_evap,
+                      double land_evap, double min_depth, uint8_t *lake_flag, float *water_out, float *closed_level,
+                      PgeLakeInfo *info)
+{
+    Sphere S{N, H, N + 2 * H, owner};
+    const int64_t M = (int64_t)6 * N * N;
+    std::vector<uint8_t> drain(ocean_in, ocean_in + M);
+    std::vector<float> filled;
+    std::vector<int64_t> parent, order, pop_seq, down;
+    flood(S, surface, drain, filled, parent, order, pop_seq);
+    if (!flow_down(S, metric, filled, ocean_in, parent, down)) return -1;
+    // upstream first: the pop sequence reversed, without the ocean
+    std::vector<int64_t> topo;
+    topo.reserve(pop_seq.size());
+    for (size_t t = pop_seq.size(); t-- > 0;)
+        if (!ocean_in[pop_seq[t]]) topo.push_back(pop_seq[t]);
+
+    PgeLakeInfo inf{};
+    std::vector<float> water(filled);
+    std::vector<uint8_t> dep(M, 0);
+    bool any_dep = false;
+    for (int64_t c = 0; c < M; c++) {
+        dep[c] = filled[c] > surface[c] && !ocean_in[c];
+        any_dep |= dep[c] != 0;
+    }
+    if ((lake_evap > 0.0 || land_evap > 0.0) && any_dep) {
+        std::vector<int64_t> lab;
+        const int64_t n = label_components(S, dep, filled, lab);
+        // a depression's cells by depth (ties in cell order)
+        std::vector<int64_t> cells;
+        for (int64_t c = 0; c < M; c++)
+            if (lab[c] >= 0) cells.push_back(c);
+        std::stable_sort(cells.begin(), cells.end(), [&](int64_t a, int64_t b) {
+            if (lab[a] != lab[b]) return lab[a] < lab[b];
+            return surface[a] < surface[b];
+        });
+        const int64_t K = (int64_t)cells.size();
+        std::vector<int64_t> ptr(n + 1, K);
+        for (int64_t t = K; t-- > 0;) ptr[lab[cells[t]]] = t;
+        std::vector<double> w(M), wr(M), af(M);
+        const double cs2 = cell_size_m * cell_size_m;
+        for (int64_t c = 0; c < M; c++) {
+            w[c] = (double)precip[c];
+            af[c] = (double)cell_area[c] / cs2;
+        }
+        std::vector<double> per(K);
+        double k_lake = lake_evap;
+        const bool runoff = land_evap > 0.0;
+        if (runoff) {
+            // the land evaporates too: a cell's rain runs off in the share Budyko's curve leaves, and
+            // open water loses the potential evaporation less what the land under it would have
+            std::vector<double> et(M), pe(M);
+            for (int64_t c = 0; c < M; c++) {
+                const double rain = w[c] / af[c];
+                pe[c] = land_evap * (double)pet[c];
+                et[c] = rain * budyko(pe[c] / (rain > 1e-9 ? rain : 1e-9));
+                wr[c] = (rain - et[c]) * af[c];
+            }
+            for (int64_t t = 0; t < K; t++) per[t] = (pe[cells[t]] - et[cells[t]]) * af[cells[t]];
+            k_lake = 1.0;
+        } else {
+            wr = w;
+            for (int64_t t = 0; t < K; t++) per[t] = (double)pet[cells[t]] * af[cells[t]];
+        }
+        // cumulative loss of each depression with the water at each cell's level
+        std::vector<double> csum(K), cum(K), z(K);
+        double run_sum = 0.0;
+        for (int64_t t = 0; t < K; t++) {
+            run_sum += per[t];
+            csum[t] = run_sum;
+            z[t] = (double)surface[cells[t]];
+        }
+        for (int64_t L = 0; L < n; L++) {
+            const double before = L > 0 ? csum[ptr[L] - 1] : 0.0;
+            for (int64_t t = ptr[L]; t < ptr[L + 1]; t++) cum[t] = csum[t] - before;
+        }
+        // the outlet: the depression's first popped cell
+        std::vector<int64_t> outlet(n, -1), outlet_lake(M, -1);
+        for (int64_t t = 0; t < K; t++) {
+            const int64_t c = cells[t], L = lab[c];
+            if (outlet[L] < 0 || order[c] < order[outlet[L]]) outlet[L] = c;
+        }
+        std::vector<double> spill(n), level(n, 0.0), outflow(n, 0.0);
+        for (int64_t L = 0; L < n; L++) {
+            outlet_lake[outlet[L]] = L;
+            spill[L] = (double)filled[outlet[L]];
+        }
+        // one accumulation, upstream first, solving each depression as it passes its outlet
+        std::vector<double> acc(w), run(wr);
+        for (const int64_t c : topo) {
+            const int64_t L = outlet_lake[c];
+            if (L >= 0) {
+                const double inflow = run[c];
+                const int64_t lo = ptr[L], hi = ptr[L + 1];
+                if (inflow <= 0.0) {
+                    level[L] = z[lo];
+                    outflow[L] = 0.0;
+                } else {
+                    const double need = inflow / k_lake;
+                    const int64_t i = std::lower_bound(cum.begin() + lo, cum.begin() + hi, need) - (cum.begin() + lo);
+                    if (i >= hi - lo) {
+                        level[L] = spill[L];
+                        outflow[L] = inflow - k_lake * cum[hi - 1];
+                    } else {
+                        level[L] = z[lo + i];
+                        outflow[L] = 0.0;
+                    }
+                }
+                if (runoff)
+                    acc[c] = inflow > 0.0 ? acc[c] * (outflow[L] / inflow) : 0.0;
+                else
+                    acc[c] = outflow[L];
+                run[c] = outflow[L];
+            }
+            const int64_t d = down[c];
+            if (d >= 0) {
+                acc[d] += acc[c];
+                run[d] += run[c];
+            }
+        }
+        // a cell above its depression's balance level dries out
+        water.assign(surface, surface + M);
+        for (int64_t t = 0; t < K; t++) {
+            const int64_t c = cells[t];
+            const float lv = (float)level[lab[c]];
+            if (lv > water[c]) water[c] = lv;
+        }
+        for (int64_t c = 0; c < M; c++)
+            if (ocean_in[c]) water[c] = filled[c];
+        inf.depressions = n;
+        for (int64_t L = 0; L < n; L++) {
+            const bool closed = outflow[L] <= 0.0;
+            const bool wet = level[L] > z[ptr[L]];
+            inf.overflowing += !closed;
+            inf.closed += closed && wet;
+            inf.dry += closed && !wet;
+        }
+    }
+    // overflowing lakes are flagged; a lake drawn below its rim is a closed sea at its level
+    const float depth = (float)min_depth, rim = 1e-4f;
+    for (int64_t c = 0; c < M; c++) {
+        const bool lake = (float)(water[c] - surface[c]) > depth && !ocean_in[c];
+        const bool closed = lake && water[c] < (float)(filled[c] - rim);
+        lake_flag[c] = lake && !closed ? 1 : 0;
+        if (closed_level) closed_level[c] = closed ? water[c] : NAN;
+        inf.lake_cells += lake;
+        inf.lake_cells_closed += closed;
+    }
+    if (water_out) std::memcpy(water_out, water.data(), sizeof(float) * M);
+    if (info) *info = inf;
+    return 0;
+}
+
+}  // namespace pge

@@ -19,6 +19,11 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// the planet's lake balance on the host (pge_lakes.cpp); 0, or -1 when a land cell has no flow direction
+int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
+                      const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
+                      double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
+                      PgeLakeInfo *info);
 // the lakes of a window (route deeper than min_depth over the surface on active interior cells)
 cudaError_t window_lakes(const PgeGrid &g, const PgeState &st, double min_depth, uint8_t *flag, int64_t *count, cudaStream_t stream);
 // routing surface (epsilon-filled priority flood); *sweeps_out < 0: not converged within max_sweeps

@@ -91,6 +91,10 @@ class ErosionState:
     #: overflowing lakes (uint8, (F, NE, NE): 1 a lake, 2 a lake with room for its rivers' load; maps.py:87) or None:
     #: set by the caller (the hydro stage's balance) or by refresh_lakes_window; read with the routing surface only
     lake_flag: torch.Tensor = field(default=None, repr=False)
+    #: the potential evaporation the planet's lake balance runs on (float32, (F, NE, NE)) in place of evap, or None
+    lake_pet: torch.Tensor = field(default=None, repr=False)
+    #: the open sea of the last sea-mask refresh (bool, (F, N, N)), the lake balance's drains; None before the first
+    sea_mask: torch.Tensor = field(default=None, repr=False)
     #: iteration of the last sea-mask refresh (refresh_base), None before the first
     base_at: int = None
     #: the last glacial pass's ice (uint8, (F, NE, NE)) for erosion.glacial_sticky, None before the first
@@ -98,6 +102,7 @@ class ErosionState:
     _owner: torch.Tensor = field(default=None, repr=False)
     _sea: tuple = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
+    _lake_inputs: tuple = field(default=None, repr=False)
 
     def __post_init__(self):
         dev = self.height.device
@@ -307,31 +312,12 @@ class ErosionState:
             self.base = torch.zeros_like(self.height)
             self.base_at = self.iteration
             return info
-        _ensure_workspace(self)
-        dev = self.height.device
-        if self._sea is None:
-            from .isostasy import sqrt_det_metric
-
-            H, N = self.H, self.N
-            sq = sqrt_det_metric(self.grid)[H:H + N, H:H + N]
-            area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * float(self.grid.cell_size_m) ** 2)
-                                                        .astype(np.float32), (self.F, N, N)))
-            hm = self.grid.halo
-            self._sea = (torch.as_tensor(area, device=dev), float(area.reshape(-1).astype(np.float64).sum()),
-                         torch.as_tensor(hm.dst.astype(np.int64), device=dev), torch.as_tensor(hm.nearest.astype(np.int64), device=dev))
-        area, total, dst, nearest = self._sea
-        base = torch.empty_like(self.height)
-        labels = torch.empty((self.F, self.N, self.N), dtype=torch.int32, device=dev)
-        n = ctypes.c_int64(0)
-        check(_lib.load().pge_sea_base(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), _ptr(self.owner_table()),
-                                       _ptr(area), float(min_fraction) * total, _ptr(base), _ptr(labels), int(max_sweeps),
-                                       ctypes.byref(n), _ptr(self.workspace), self.workspace.numel(), _stream()), "pge_sea_base")
-        flat = base.view(-1)
-        flat[dst] = flat[nearest]  # the halo is an exact copy of the cell it mirrors (a jump at a basin rim)
+        base, labels = self._sea_base(min_fraction, max_sweeps)
         b = base[self.interior]
         below = labels >= 0
         closed = below & (b < 0.0)
-        info["sea_cells"] = int((below & ~closed).sum().item())
+        self.sea_mask = below & ~closed
+        info["sea_cells"] = int(self.sea_mask.sum().item())
         info["closed_cells"] = int(closed.sum().item())
         if info["closed_cells"]:
             info["closed_basins"] = int(torch.unique(labels[closed]).numel())
@@ -339,6 +325,92 @@ class ErosionState:
         self.base = base
         self.base_at = self.iteration
         return info
+
+    def _sea_tables(self):
+        """(interior cell areas float32 (F, N, N), their float64 sum, halo dst, halo nearest) on the device."""
+        if self._sea is None:
+            from .isostasy import sqrt_det_metric
+
+            dev = self.height.device
+            H, N = self.H, self.N
+            sq = sqrt_det_metric(self.grid)[H:H + N, H:H + N]
+            area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * float(self.grid.cell_size_m) ** 2)
+                                                        .astype(np.float32), (self.F, N, N)))
+            hm = self.grid.halo
+            self._sea = (torch.as_tensor(area, device=dev), float(area.reshape(-1).astype(np.float64).sum()),
+                         torch.as_tensor(hm.dst.astype(np.int64), device=dev), torch.as_tensor(hm.nearest.astype(np.int64), device=dev))
+        return self._sea
+
+    def _sea_base(self, min_fraction: float, max_sweeps: int = 1 << 22):
+        """pge_sea_base of the current surface: (base (F, NE, NE) with its halos copied from their nearest
+        interior cells, component labels (F, N, N))."""
+        _ensure_workspace(self)
+        area, total, dst, nearest = self._sea_tables()
+        base = torch.empty_like(self.height)
+        labels = torch.empty((self.F, self.N, self.N), dtype=torch.int32, device=self.height.device)
+        n = ctypes.c_int64(0)
+        check(_lib.load().pge_sea_base(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), _ptr(self.owner_table()),
+                                       _ptr(area), float(min_fraction) * total, _ptr(base), _ptr(labels), int(max_sweeps),
+                                       ctypes.byref(n), _ptr(self.workspace), self.workspace.numel(), _stream()), "pge_sea_base")
+        flat = base.view(-1)
+        flat[dst] = flat[nearest]  # the halo is an exact copy of the cell it mirrors (a jump at a basin rim)
+        return base, labels
+
+    def refresh_lakes(self, lake_evap: float, min_depth: float, min_fraction: float = 0.02, land_evap: float = 0.0) -> dict:
+        """The planet's lakes (maps.py:422-479, erosion.lake_balance with
+        erosion.lake_fill off): the hydro stage's flood, D8 routing and
+        evaporation balance on the eroding surface (``pge_lake_balance``, a
+        host pass: its every step follows the flood's serial pop order).
+        Overflowing lakes deeper than ``min_depth`` (cell units) are flagged
+        (``lake_flag``); a lake drawn below its rim is a closed sea, its level
+        written into ``base``.  The drains are the sea of the last
+        :meth:`refresh_base`, else the open ocean of the current surface;
+        the balance runs on ``lake_pet`` when set, else ``evap``.  Must run
+        after :meth:`refresh_base` and :meth:`refresh_route`."""
+        if not self.spherical:
+            raise ValueError("refresh_lakes is the planet's lake balance; a window's lakes come from refresh_lakes_window")
+        inter = self.interior
+        if self.sea_mask is not None:
+            sea = self.sea_mask
+        else:
+            sb, labels = self._sea_base(min_fraction)
+            sea = (labels >= 0) & (sb[inter] == 0.0)
+        area, _, dst, nearest = self._sea_tables()
+        pet = self.lake_pet if self.lake_pet is not None else self.evap
+        host = lambda t: np.ascontiguousarray(t.detach().cpu().numpy())
+        # every array handed to the host pass is held by a name until it returns
+        surf = host((self.height + self.sediment)[inter].float())
+        ocean = host(sea.to(torch.uint8))
+        precip = host(self.precip[inter])
+        pet_h = host(pet[inter].float())
+        if self._lake_inputs is None:
+            self._lake_inputs = (host(self.owner_table()), host(self.metric), host(area))
+        owner, metric, area_h = self._lake_inputs
+        F, N = self.F, self.N
+        flag = np.empty((F, N, N), np.uint8)
+        level = np.empty((F, N, N), np.float32)
+        info = _lib.PgeLakeInfo()
+        check(_lib.load().pge_lake_balance(ctypes.byref(self.pge_grid()), owner.ctypes.data, metric.ctypes.data, area_h.ctypes.data,
+                                           float(self.grid.cell_size_m), surf.ctypes.data, ocean.ctypes.data,
+                                           precip.ctypes.data, pet_h.ctypes.data,
+                                           float(lake_evap), float(land_evap), float(min_depth), flag.ctypes.data, None,
+                                           level.ctypes.data, ctypes.byref(info)), "pge_lake_balance")
+        dev = self.height.device
+        lf = torch.zeros(self.height.shape, dtype=torch.uint8, device=dev)
+        lf[inter] = torch.as_tensor(flag, device=dev)
+        closed = ~np.isnan(level)
+        if closed.any():
+            b = self.base[inter]
+            cl = torch.as_tensor(closed, device=dev)
+            b[cl] = torch.as_tensor(level, device=dev)[cl].double()
+            self.base[inter] = b
+        for t in (lf, self.base):  # exact copies of the cells they mirror (maps.py:476-479)
+            flat = t.view(-1)
+            flat[dst] = flat[nearest]
+        self.lake_flag = lf
+        return {"lake_cells": int(info.lake_cells), "lake_cells_closed": int(info.lake_cells_closed),
+                "depressions": int(info.depressions), "overflowing": int(info.overflowing), "closed": int(info.closed),
+                "dry": int(info.dry)}
 
     def n_active_interior(self) -> int:
         if self.mask is None:
@@ -714,7 +786,13 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
         # the routing surface the particles steer on (maps.py:1553-1554)
         state.refresh_route(cell_units(ep, "route_eps", state.height_unit_m))
     st_lake = None
-    if not state.spherical and bool(getattr(ep, "window_lakes", False)) and flood > 0 and \
+    if state.spherical and bool(getattr(ep, "lake_balance", False)) and flood > 0 and \
+            (state.lake_flag is None or state.iteration % flood == 0):
+        # the planet's lakes, after the base (rebuilt from scratch) and the route (maps.py:1555-1562)
+        hydro = getattr(params, "hydro", None)
+        st_lake = state.refresh_lakes(float(getattr(hydro, "lake_evap", 6.0)), lake_min_depth(params) / state.height_unit_m,
+                                      ocean_min_fraction(params), float(getattr(hydro, "land_evap", 3.0)))
+    elif not state.spherical and bool(getattr(ep, "window_lakes", False)) and flood > 0 and \
             (state.lake_flag is None or state.iteration % flood == 0):
         # a window's lakes, after the route they are read off (maps.py:1563-1566)
         st_lake = state.refresh_lakes_window(lake_min_depth(params) / state.height_unit_m,

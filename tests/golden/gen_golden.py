@@ -611,6 +611,65 @@ def gen_step_lake(cs, maps, pk, WorldParams):
           "last", stats[-1])
 
 
+def gen_lake_balance(cs, maps, pk, WorldParams):
+    """The planet's lake refresh (ErosionState.refresh_lakes, maps.py:422-479,
+    erosion.lake_fill off): on a six-face N=32 world after two reference
+    iterations, the refresh with the land's evaporation (hydro.land_evap = 3,
+    Budyko's curve) and without it (lake_evap alone), recording the flags, the
+    base level and the water surface; then full steps with lake_balance on,
+    the sea mask and the routing flood every 2 iterations."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=11, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    iters = 5
+    p = _world_params(WorldParams, 32, 2, 50.0, 11, 0.45, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", flood_every=2, sea_mask_every=2,
+                      lake_balance=True, lake_fill=False)
+    p = p.with_overrides(hydro={"land_evap": 3.0, "lake_evap": 6.0, "pet_t0": 0.0})
+    st = _ref_state(cs, maps, world, p)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    mf = float(p.hydro.ocean_min_fraction)
+    unit = st.height_unit_m
+    depth = float(p.hydro.lake_min_depth) / unit
+    # two plain iterations first (no refreshes) so the surface has the pits erosion makes
+    q = p.with_overrides(erosion={"flood_every": 0, "sea_mask_every": 0, "lake_balance": False})
+    for it in range(2):
+        maps.step(st, q, it, n_particles=4096)
+    st.iteration = 0
+    u_height, u_sediment = st.height.copy(), st.sediment.copy()
+    st.refresh_base(mf)
+    st.refresh_route(float(p.erosion.route_eps) / unit)
+    sea = st.sea.copy()
+    base_before = st.base.copy()
+    unit_out = {}
+    for tag, le in (("budyko", 3.0), ("plain", 0.0)):
+        st.base = base_before.copy()
+        st.lake_flag = None
+        info = st.refresh_lakes(float(p.hydro.lake_evap), depth, mf, None, le)
+        unit_out[f"{tag}_flag"] = st.lake_flag.copy()
+        unit_out[f"{tag}_base"] = st.base.copy()
+        unit_out[f"{tag}_water"] = np.asarray(st.lake_level, np.float32).copy()
+        unit_out[f"{tag}_info"] = json.dumps(info)
+        print("lake_balance", tag, info)
+    st2 = _ref_state(cs, maps, world, p)
+    maps.start_replay(st2, p)
+    h_start = st2.height.copy()
+    stats = []
+    for it in range(iters):
+        s = maps.step(st2, p, it, n_particles=4096)
+        stats.append({k: s[k] for k in ("particles", "entries", "clamped", "deaths", "datum_shift")})
+        if s.get("lakes") is not None:
+            stats[-1]["lakes"] = s["lakes"]
+    np.savez_compressed(HERE / "lake_balance.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=11, iterations=iters,
+                        n_particles=4096, ocean_min_fraction=mf, min_depth=depth, lake_evap=float(p.hydro.lake_evap),
+                        params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        u_height=u_height, u_sediment=u_sediment, u_sea=sea, u_base=base_before, u_route=st.route, **unit_out,
+                        h_start=h_start, height=st2.height, sediment=st2.sediment, discharge=st2.discharge, momentum=st2.momentum,
+                        pending=st2.pending, base=st2.base, lake_flag=st2.lake_flag, route=st2.route, stats=json.dumps(stats),
+                        **init)
+    print("lake_balance steps:", stats[-1])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -620,7 +679,8 @@ def main(bake: str, only: str | None = None):
             "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams),
             "glacial": lambda: gen_glacial(cs, maps, pk, WorldParams),
             "lake_trace": lambda: gen_lake_trace(cs, maps, pk, WorldParams),
-            "step_lake": lambda: gen_step_lake(cs, maps, pk, WorldParams)}
+            "step_lake": lambda: gen_step_lake(cs, maps, pk, WorldParams),
+            "lake_balance": lambda: gen_lake_balance(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

@@ -17,6 +17,7 @@ a pass's fields follow the routed pass's bound (at most 0.5 % of values off
 bit-identical); steps follow the hypsometry bound of the plain steps.
 """
 import ctypes
+import json
 
 import numpy as np
 import pytest
@@ -193,3 +194,71 @@ def test_lake_steps_follow_the_reference(cuda):
     gm.step(g1, c["params"], 0, n_particles=c["n_particles"])
     gm.step(g2, c["params"], 0, n_particles=c["n_particles"])
     assert not np.array_equal(g1.to_numpy()["height"], g2.to_numpy()["height"])
+
+
+def _balance_world():
+    from pgerosion.params import WorldGroup, WorldParams
+    from pgerosion.synth import World
+    from pgerosion.geometry import get_grid
+    from tests.parity_cases import erosion_params
+    import json
+
+    fx = np.load(GOLDEN / "lake_balance.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    ep = erosion_params(str(fx["params"]))
+    params = WorldParams(world=WorldGroup(seed=int(fx["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(fx["land_fraction"]),
+                                          halo=H), erosion=ep)
+    world = World(get_grid(N, H, cs), fx["bedrock"], fx["hardness"], fx["precip"], fx["evap"], fx["uplift"],
+                  float(fx["land_fraction"]))
+    return fx, params, world, json.loads(str(fx["stats"]))
+
+
+@pytest.mark.parametrize("tag,land_evap", [("budyko", 3.0), ("plain", 0.0)])
+def test_planet_lake_refresh_equals_the_reference(cuda, tag, land_evap):
+    """ErosionState.refresh_lakes on the device state (surface and sea mask
+    copied off the device, the host balance, flags and closed levels copied
+    back with halos from the nearest interior cell): the reference's flags
+    and base level, halos included, bit for bit."""
+    fx, params, world, _ = _balance_world()
+    g = gm.ErosionState.from_world(world)
+    g.height.copy_(torch.as_tensor(fx["u_height"]))
+    g.sediment.copy_(torch.as_tensor(fx["u_sediment"]))
+    mf = float(fx["ocean_min_fraction"])
+    g.refresh_base(mf)
+    assert np.array_equal(g.sea_mask.cpu().numpy(), fx["u_sea"].reshape(g.sea_mask.shape))
+    assert g.base.cpu().numpy().tobytes() == np.ascontiguousarray(fx["u_base"]).tobytes()
+    g.refresh_route(float(params.erosion.route_eps) / g.height_unit_m)
+    info = g.refresh_lakes(float(fx["lake_evap"]), float(fx["min_depth"]), mf, land_evap)
+    want = json.loads(str(fx[f"{tag}_info"]))
+    assert {k: info[k] for k in info} == {k: want[k] for k in info}
+    assert np.array_equal(g.lake_flag.cpu().numpy(), fx[f"{tag}_flag"])
+    assert g.base.cpu().numpy().tobytes() == np.ascontiguousarray(fx[f"{tag}_base"]).tobytes()
+
+
+def test_planet_lake_steps_follow_the_reference(cuda):
+    """maps.step with erosion.lake_balance (lake_fill off), the sea mask and
+    the routing flood every 2 iterations: the lakes refreshed on the same
+    iterations as the reference's, the hypsometry within the chaotic bound of
+    the plain steps, and the mass balance of one more pass with the lakes."""
+    from tests.test_gpu_parity import _mass_balance
+
+    fx, params, world, stats = _balance_world()
+    g = gm.ErosionState.from_world(world)
+    gm.start_replay(g, params)
+    got = []
+    for it in range(int(fx["iterations"])):
+        s = gm.step(g, params, it, n_particles=int(fx["n_particles"]))
+        assert ("lakes" in s) == ("lakes" in stats[it]), it
+        got.append(s.get("lakes"))
+    want = [st.get("lakes") for st in stats]
+    # the first refresh sees the same surface as the reference's: the same lakes
+    assert got[0] == want[0], (got, want)
+    assert all(x is None or x["depressions"] > 0 for x in got), (got, want)
+    a = g.to_numpy()
+    inter = g.interior
+    hg = hypsometry(a["height"], a["sediment"], inter, 50.0)
+    hr = hypsometry(fx["height"], fx["sediment"], inter, 50.0)
+    assert np.abs(hg - hr).max() <= HYPS_TOL_MANY, (hg, hr)
+    m0 = g.total_mass()
+    s = gm.run_iteration(g, params, int(fx["iterations"]), n_particles=int(fx["n_particles"]))
+    _mass_balance(s, m0, g.total_mass())

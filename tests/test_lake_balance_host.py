@@ -1,0 +1,88 @@
+"""The planet's lake balance (``pge_lake_balance``: ErosionState.refresh_lakes,
+globe/erosion/maps.py:422-479, with erosion.lake_fill off) against the
+reference's own refresh on the same surface (tests/golden/lake_balance.npz,
+made by tests/golden/gen_golden.py).
+
+``pge_lake_balance`` is the library's host code (the reference's sequence
+follows the flood's serial pop order), so it runs here without a GPU; the
+arrays it takes are what ``ErosionState.refresh_lakes`` copies off the
+device.  Flags, closed levels and the water surface are comparison and
+float32 work on the reference's own operation order: identical."""
+import ctypes
+import json
+
+import numpy as np
+import pytest
+
+from pgerosion import _lib
+from pgerosion.geometry import get_grid
+from pgerosion.isostasy import sqrt_det_metric
+from tests.parity_cases import GOLDEN
+
+
+def _inputs():
+    fx = np.load(GOLDEN / "lake_balance.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    grid = get_grid(N, H, cs)
+    inter = (slice(None), slice(H, H + N), slice(H, H + N))
+    c = lambda a, t: np.ascontiguousarray(np.asarray(a)[inter], dtype=t)
+    surf = c(fx["u_height"] + fx["u_sediment"], np.float32)
+    sq = sqrt_det_metric(grid)[H:H + N, H:H + N]
+    area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * cs ** 2).astype(np.float32), (6, N, N)))
+    return dict(fx=fx, grid=grid, N=N, H=H, cs=cs, inter=inter, surf=surf, ocean=np.ascontiguousarray(fx["u_sea"], np.uint8),
+                precip=c(fx["precip"], np.float32), pet=c(fx["evap"], np.float32), area=area,
+                owner=np.ascontiguousarray(grid.owner, np.int32), metric=np.ascontiguousarray(grid.metric_face, np.float32))
+
+
+def _balance(d, land_evap):
+    N = d["N"]
+    g = _lib.PgeGrid(F=6, N=N, H=d["H"], spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    flag = np.empty((6, N, N), np.uint8)
+    water = np.empty((6, N, N), np.float32)
+    level = np.empty((6, N, N), np.float32)
+    info = _lib.PgeLakeInfo()
+    _lib.check(_lib.load().pge_lake_balance(ctypes.byref(g), d["owner"].ctypes.data, d["metric"].ctypes.data, d["area"].ctypes.data,
+                                            d["cs"], d["surf"].ctypes.data, d["ocean"].ctypes.data, d["precip"].ctypes.data,
+                                            d["pet"].ctypes.data, float(d["fx"]["lake_evap"]), float(land_evap),
+                                            float(d["fx"]["min_depth"]), flag.ctypes.data, water.ctypes.data, level.ctypes.data,
+                                            ctypes.byref(info)), "pge_lake_balance")
+    return flag, water, level, info
+
+
+@pytest.mark.parametrize("tag,land_evap", [("budyko", 3.0), ("plain", 0.0)])
+def test_lake_balance_equals_the_reference(tag, land_evap):
+    d = _inputs()
+    fx, inter = d["fx"], d["inter"]
+    flag, water, level, info = _balance(d, land_evap)
+    want = json.loads(str(fx[f"{tag}_info"]))
+    got = {k: int(getattr(info, k)) for k in ("lake_cells", "lake_cells_closed", "depressions", "overflowing", "closed", "dry")}
+    assert got == {k: want[k] for k in got}, (got, want)
+    assert np.array_equal(flag, fx[f"{tag}_flag"][inter])
+    assert water.tobytes() == np.ascontiguousarray(fx[f"{tag}_water"], np.float32).tobytes()
+    # the closed lakes' levels are the base level there, the rest of the base is untouched
+    base = np.array(fx["u_base"][inter])
+    closed = ~np.isnan(level)
+    base[closed] = level[closed]
+    assert base.tobytes() == np.ascontiguousarray(fx[f"{tag}_base"][inter]).tobytes()
+    assert got["lake_cells"] > 0 and got["closed"] > 0 and got["overflowing"] > 0
+
+
+def test_lake_balance_without_evaporation_is_the_spill_fill():
+    """lake_evap = land_evap = 0: every depression stands at its spill
+    point, overflowing, and no lake is closed."""
+    d = _inputs()
+    d["fx"] = dict(d["fx"])
+    d["fx"]["lake_evap"] = np.float64(0.0)
+    flag, water, level, info = _balance(d, 0.0)
+    assert info.lake_cells_closed == 0 and np.isnan(level).all()
+    assert (water >= d["surf"]).all()
+    assert int(flag.sum()) == int(info.lake_cells) > 0
+
+
+def test_lake_balance_rejects_a_window():
+    N = 8
+    g = _lib.PgeGrid(F=1, N=N, H=2, spherical=0, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    a = np.zeros((1, N, N), np.float32)
+    r = _lib.load().pge_lake_balance(ctypes.byref(g), a.ctypes.data, a.ctypes.data, a.ctypes.data, 1.0, a.ctypes.data, a.ctypes.data,
+                                     a.ctypes.data, a.ctypes.data, 1.0, 0.0, 0.0, a.ctypes.data, None, None, None)
+    assert r == _lib.PGE_E_UNSUPPORTED
