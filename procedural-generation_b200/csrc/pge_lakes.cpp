@@ -17,7 +17,9 @@
 // The arithmetic mirrors the reference's types: surfaces and the filled
 // surface in float32, slopes from float32 height differences over a float64
 // step length, the balance in float64, the water surface and the depth tests
-// in float32.  Compiled without floating-point contraction.
+// in float32.  Compiled without floating-point contraction.  The flood is
+// serial; the per-cell passes (D8, the runoff, the flags) run on the host's
+// cores with OpenMP, each cell's result independent of the split.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -53,10 +55,24 @@ struct Sphere {
         const int ei = (int)(r2 / NE), ej = (int)(r2 - (int64_t)ei * NE);
         return ((int64_t)f2 * N + (ei - H)) * N + (ej - H);
     }
+    // all eight neighbours; a cell off the face's edge ring has them on its own face
+    void neighbors(int64_t c, int64_t *out) const
+    {
+        const int64_t NN = (int64_t)N * N;
+        const int64_t rem = c % NN;
+        const int i = (int)(rem / N), j = (int)(rem % N);
+        if (i >= 1 && i <= N - 2 && j >= 1 && j <= N - 2) {
+            for (int k = 0; k < 8; k++) out[k] = c + (int64_t)D8_DI[k] * N + D8_DJ[k];
+        } else {
+            for (int k = 0; k < 8; k++) out[k] = neighbor(c, k);
+        }
+    }
     int code_towards(int64_t c, int64_t target) const
     {
+        int64_t nb[8];
+        neighbors(c, nb);
         for (int k = 0; k < 8; k++)
-            if (neighbor(c, k) == target) return k;
+            if (nb[k] == target) return k;
         return -1;
     }
 };
@@ -96,8 +112,10 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
     for (int64_t c = 0; c < M; c++) {
         if (!drain[c]) continue;
         visited[c] = 1;
+        int64_t nb[8];
+        S.neighbors(c, nb);
         bool push = false;
-        for (int k = 0; k < 8 && !push; k++) push = !drain[S.neighbor(c, k)];
+        for (int k = 0; k < 8 && !push; k++) push = !drain[nb[k]];
         if (push) heap.push({(double)surface[c], seq++, c});
     }
     size_t head = 0;
@@ -118,8 +136,10 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
         order[c] = (int64_t)pop_seq.size();
         pop_seq.push_back(c);
         const int64_t f = c / NN;
+        int64_t nb[8];
+        S.neighbors(c, nb);
         for (int k = 0; k < 8; k++) {
-            const int64_t n = S.neighbor(c, k);
+            const int64_t n = nb[k];
             if (visited[n]) continue;
             // across a face edge the nearest-cell mapping can be one-sided: only reversible links
             if (n / NN != f && S.code_towards(n, c) < 0) continue;
@@ -143,16 +163,20 @@ bool flow_down(const Sphere &S, const float *metric, const std::vector<float> &f
 {
     const int64_t M = (int64_t)6 * S.N * S.N, NN = (int64_t)S.N * S.N;
     down.assign(M, -1);
+    int64_t unreached = 0;
+#pragma omp parallel for schedule(static) reduction(+ : unreached)
     for (int64_t c = 0; c < M; c++) {
         if (ocean[c]) continue;
         const int64_t rem = c % NN;
         const int i = (int)(rem / S.N), j = (int)(rem % S.N);
         const float *g = metric + 3 * ((int64_t)(i + S.H) * S.NE + (j + S.H));
         const float hc = filled[c];
+        int64_t nb[8];
+        S.neighbors(c, nb);
         int best = -1;
         double best_s = 0.0;
         for (int k = 0; k < 8; k++) {
-            const int64_t n = S.neighbor(c, k);
+            const int64_t n = nb[k];
             const float hn = filled[n];
             if (hn < hc) {
                 const double di = D8_DI[k], dj = D8_DJ[k];
@@ -166,10 +190,12 @@ bool flow_down(const Sphere &S, const float *metric, const std::vector<float> &f
             }
         }
         if (best < 0 && parent[c] >= 0) best = S.code_towards(c, parent[c]);
-        if (best < 0) return false;
-        down[c] = S.neighbor(c, best);
+        if (best < 0)
+            unreached++;
+        else
+            down[c] = nb[best];
     }
-    return true;
+    return unreached == 0;
 }
 
 // 8-connected components of `mask` joining only cells of identical level, numbered by their lowest
@@ -188,8 +214,10 @@ int64_t label_components(const Sphere &S, const std::vector<uint8_t> &mask, cons
         while (!stack.empty()) {
             const int64_t c = stack.back();
             stack.pop_back();
+            int64_t nb[8];
+            S.neighbors(c, nb);
             for (int k = 0; k < 8; k++) {
-                const int64_t q = S.neighbor(c, k);
+                const int64_t q = nb[k];
                 if (mask[q] && labels[q] < 0 && level[q] == level[c]) {
                     labels[q] = n;
                     stack.push_back(q);
@@ -231,11 +259,13 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
     PgeLakeInfo inf{};
     std::vector<float> water(filled);
     std::vector<uint8_t> dep(M, 0);
-    bool any_dep = false;
+    int64_t ndep = 0;
+#pragma omp parallel for schedule(static) reduction(+ : ndep)
     for (int64_t c = 0; c < M; c++) {
         dep[c] = filled[c] > surface[c] && !ocean_in[c];
-        any_dep |= dep[c] != 0;
+        ndep += dep[c];
     }
+    const bool any_dep = ndep > 0;
     if ((lake_evap > 0.0 || land_evap > 0.0) && any_dep) {
         std::vector<int64_t> lab;
         const int64_t n = label_components(S, dep, filled, lab);
@@ -252,6 +282,7 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
         for (int64_t t = K; t-- > 0;) ptr[lab[cells[t]]] = t;
         std::vector<double> w(M), wr(M), af(M);
         const double cs2 = cell_size_m * cell_size_m;
+#pragma omp parallel for schedule(static)
         for (int64_t c = 0; c < M; c++) {
             w[c] = (double)precip[c];
             af[c] = (double)cell_area[c] / cs2;
@@ -263,6 +294,7 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
             // the land evaporates too: a cell's rain runs off in the share Budyko's curve leaves, and
             // open water loses the potential evaporation less what the land under it would have
             std::vector<double> et(M), pe(M);
+#pragma omp parallel for schedule(static)
             for (int64_t c = 0; c < M; c++) {
                 const double rain = w[c] / af[c];
                 pe[c] = land_evap * (double)pet[c];
@@ -351,14 +383,18 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
     }
     // overflowing lakes are flagged; a lake drawn below its rim is a closed sea at its level
     const float depth = (float)min_depth, rim = 1e-4f;
+    int64_t nlake = 0, nclosed = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nlake, nclosed)
     for (int64_t c = 0; c < M; c++) {
         const bool lake = (float)(water[c] - surface[c]) > depth && !ocean_in[c];
         const bool closed = lake && water[c] < (float)(filled[c] - rim);
         lake_flag[c] = lake && !closed ? 1 : 0;
         if (closed_level) closed_level[c] = closed ? water[c] : NAN;
-        inf.lake_cells += lake;
-        inf.lake_cells_closed += closed;
+        nlake += lake;
+        nclosed += closed;
     }
+    inf.lake_cells = nlake;
+    inf.lake_cells_closed = nclosed;
     if (water_out) std::memcpy(water_out, water.data(), sizeof(float) * M);
     if (info) *info = inf;
     return 0;
