@@ -390,7 +390,20 @@ def run_b200(args, rank, world_size, dist):
     surf = st.height + st.sediment
     route_flood = {"what": "epsilon-filled routing surface (pge_route_flood + linear halo exchange) of the evolved world",
                    "ms": e0.elapsed_time(e1), "sweeps": sweeps, "filled_cells": int((st.route > surf).sum().item())}
-    st.route = None
+    # the planet's lake refresh of the same terrain (erosion.lake_balance: the sea mask on the device, then the
+    # host pass -- surface and sea off the device, flood, D8, evaporation balance, flags and levels back), wall clock
+    # around synchronised calls: the host pass is not a kernel
+    base0 = st.base.clone()
+    st.refresh_base(0.02)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lk = st.refresh_lakes(6.0, 0.5 / st.height_unit_m, 0.02, 3.0)
+    torch.cuda.synchronize()
+    lake_balance = {"what": "planet lake refresh (refresh_lakes: D2H of surface and sea, the host flood + D8 + "
+                            "evaporation balance of pge_lake_balance, H2D of flags and closed levels), lake_evap 6, land_evap 3",
+                    "ms": (time.perf_counter() - t0) * 1e3, "host_threads": torch.get_num_threads(), **lk}
+    st.route = st.lake_flag = st.sea_mask = st.base_at = None
+    st.base = base0
     adjoint = None
     if not args.no_adjoint:
         adjoint = run_adjoint(args, dev)
@@ -429,6 +442,7 @@ def run_b200(args, rank, world_size, dist):
     if adjoint is not None:
         out["adjoint"] = adjoint
     out["route_flood"] = route_flood
+    out["lake_balance"] = lake_balance
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
