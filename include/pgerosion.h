@@ -46,6 +46,9 @@
  *                                                  globe/hydro/priority_flood.py:127-191,
  *                                                  globe/hydro/routing.py:28-90,
  *                                                  globe/hydro/balance.py:63-284
+ *   pge_basin_fill        fill_basins: sediment graded into the closed basins of a
+ *                         fresh state (HOST code, host pointers)
+ *                                                  globe/erosion/maps.py:1216-1229, 1278-1326
  *   pge_glacial           glacial.carve (the ice line of the evaporation field)
  *                                                  globe/erosion/glacial.py:100-257,
  *                                                  globe/erosion/maps.py:1580-1590
@@ -444,6 +447,19 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
                              const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                              double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
                              PgeLakeInfo *info);
+
+/* The basin fill of a fresh state (maps.py:1278-1326, erosion.basin_fill_grade),
+ * on the HOST (host pointers, no CUDA call): the same priority flood as
+ * pge_lake_balance from the ocean drains (surface, ocean: interior (6,N,N)
+ * float32 / uint8; owner as there), then every cell raised to at least
+ * `step` (cell units per cell: basin_fill_grade x cell km / height unit)
+ * above the cell that flooded it, in pop order; add (6,N,N) float64 gets
+ * that plain less the surface (>= 0) on cells the flood left more than
+ * min_depth (cell units, float32 test) under its fill and off the ocean, 0
+ * elsewhere -- the sediment the caller adds.  basin (6,N,N) uint8 (may be
+ * NULL) gets 1 on those cells, basin_cells (host, may be NULL) their count. */
+PGE_API int pge_basin_fill(const PgeGrid *g, const int32_t *owner, const float *surface, const uint8_t *ocean, double step,
+                           double min_depth, double *add, uint8_t *basin, int64_t *basin_cells);
 
 /* The glacial pass (glacial.py:162-257), the ice line read from the
  * evaporation field: ice on active cells with evap <= ice_evap and surface

@@ -564,6 +564,18 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
     return PGE_OK;
 }
 
+PGE_API int pge_basin_fill(const PgeGrid *g, const int32_t *owner, const float *surface, const uint8_t *ocean, double step,
+                           double min_depth, double *add, uint8_t *basin, int64_t *basin_cells)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (!g->spherical) return fail(PGE_E_UNSUPPORTED, "basin_fill: a global (spherical) pass");
+    if (!owner || !surface || !ocean || !add) return fail(PGE_E_ARG, "basin_fill: NULL pointer");
+    if (!(step >= 0.0) || !(min_depth >= 0.0)) return fail(PGE_E_ARG, "basin_fill: step and min_depth must be >= 0");
+    basin_fill_host(g->N, g->H, owner, surface, ocean, step, min_depth, add, basin, basin_cells);
+    return PGE_OK;
+}
+
 PGE_API int pge_sea_base(const PgeGrid *g, const PgeState *s, const int32_t *owner, const float *area, double min_area, double *base,
                          int32_t *labels, int64_t max_sweeps, int64_t *sweeps, void *ws, size_t ws_bytes, void *stream)
 {

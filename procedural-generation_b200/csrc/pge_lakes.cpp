@@ -400,4 +400,38 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
     return 0;
 }
 
+// the sediment fill_basins lays into the closed basins of a fresh state (maps.py:1278-1326): the flood's
+// surface graded `step` (cell units per cell) up from each basin's outlet along the flood tree, where the
+// flood found a basin deeper than min_depth off the ocean
+void basin_fill_host(int N, int H, const int32_t *owner, const float *surface, const uint8_t *ocean_in, double step, double min_depth,
+                     double *add, uint8_t *basin_out, int64_t *basin_cells)
+{
+    Sphere S{N, H, N + 2 * H, owner};
+    const int64_t M = (int64_t)6 * N * N;
+    std::vector<uint8_t> drain(ocean_in, ocean_in + M);
+    std::vector<float> filled;
+    std::vector<int64_t> parent, order, pop_seq;
+    flood(S, surface, drain, filled, parent, order, pop_seq);
+    // every cell at least `step` above the cell that flooded it, parents before children (pop order)
+    std::vector<double> g(surface, surface + M);
+    for (const int64_t c : pop_seq) {
+        const int64_t q = parent[c];
+        if (q >= 0) {
+            const double v = g[q] + step;
+            if (v > g[c]) g[c] = v;
+        }
+    }
+    const float depth = (float)min_depth;
+    int64_t nb = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nb)
+    for (int64_t c = 0; c < M; c++) {
+        const bool basin = (float)(filled[c] - surface[c]) > depth && !ocean_in[c];
+        const double a = g[c] - (double)surface[c];
+        add[c] = basin ? (a > 0.0 ? a : 0.0) : 0.0;
+        if (basin_out) basin_out[c] = basin ? 1 : 0;
+        nb += basin;
+    }
+    if (basin_cells) *basin_cells = nb;
+}
+
 }  // namespace pge

@@ -24,6 +24,9 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
                       const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                       double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
                       PgeLakeInfo *info);
+// the basin fill of a fresh state on the host (pge_lakes.cpp)
+void basin_fill_host(int N, int H, const int32_t *owner, const float *surface, const uint8_t *ocean, double step, double min_depth,
+                     double *add, uint8_t *basin, int64_t *basin_cells);
 // the lakes of a window (route deeper than min_depth over the surface on active interior cells)
 cudaError_t window_lakes(const PgeGrid &g, const PgeState &st, double min_depth, uint8_t *flag, int64_t *count, cudaStream_t stream);
 // routing surface (epsilon-filled priority flood); *sweeps_out < 0: not converged within max_sweeps

@@ -738,6 +738,44 @@ def ocean_min_fraction(params) -> float:
     return float(getattr(hydro, "ocean_min_fraction", 0.02)) if hydro is not None else 0.02
 
 
+def fill_basins(state: ErosionState, params) -> dict | None:
+    """``erosion.basin_fill_grade`` > 0 (maps.py:1278-1326): lay sediment into
+    the closed basins the bedrock arrives with, up to a plain rising
+    ``basin_fill_grade`` (m per km) from each basin's outlet along the flood
+    tree, on cells the flood leaves more than ``basin_fill_min_m`` under its
+    fill and off the open ocean (``pge_basin_fill``, a host pass: the flood's
+    pop order is serial).  Call once on a fresh state after
+    :func:`start_replay`; returns the reference's statistics, or None when
+    off, on a window or without a world group."""
+    ep = erosion_group(params)
+    grade = float(getattr(ep, "basin_fill_grade", 0.0))
+    if grade <= 0.0 or not state.spherical or getattr(params, "world", None) is None:
+        return None
+    inter = state.interior
+    sb, labels = state._sea_base(ocean_min_fraction(params))
+    sea = (labels >= 0) & (sb[inter] == 0.0)  # the open ocean of the current surface
+    host = lambda t: np.ascontiguousarray(t.detach().cpu().numpy())
+    surf = host((state.height + state.sediment)[inter].float())
+    ocean = host(sea.to(torch.uint8))
+    owner = host(state.owner_table())
+    F, N = state.F, state.N
+    add = np.empty((F, N, N), np.float64)
+    basin = np.empty((F, N, N), np.uint8)
+    nb = ctypes.c_int64(0)
+    unit = state.height_unit_m
+    step = grade * (float(state.grid.cell_size_m) / 1000.0) / unit  # cell units per cell
+    check(_lib.load().pge_basin_fill(ctypes.byref(state.pge_grid()), owner.ctypes.data, surf.ctypes.data, ocean.ctypes.data,
+                                     float(step), float(getattr(ep, "basin_fill_min_m", 1.0)) / unit, add.ctypes.data,
+                                     basin.ctypes.data, ctypes.byref(nb)), "pge_basin_fill")
+    state.sediment[inter] += torch.as_tensor(add, device=state.height.device)
+    state.exchange_halos()
+    area = host(state._sea_tables()[0])
+    b = basin.astype(bool)
+    return {"basin_cells": int(nb.value), "basin_area_km2": float(area[b].sum() / 1e6),
+            "fill_km3": float((add * unit * area).sum() / 1e9),
+            "fill_mean_m": float(add[b].mean() * unit) if b.any() else 0.0, "fill_max_m": float(add.max() * unit)}
+
+
 def lake_min_depth(params) -> float:
     """``hydro.lake_min_depth`` (m) when the params carry a hydro group, else
     the bake's 0.5 (maps.py:1564)."""

@@ -194,7 +194,7 @@ def plain_knobs() -> dict:
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
     path (the lake parks of ``lake_fill``, the window lake balance, ice
-    sheet, lateral cut, basin fill).  Isostasy, the routing surface
+    sheet, lateral cut).  The basin fill, isostasy, the routing surface
     (``flood_every``), the sea mask (``sea_mask_every``), the glacial pass
     (``glacial_every``, the ice line of the evaporation field), the planet's
     lake balance (``lake_balance`` with ``lake_fill`` off) and the lakes of
@@ -207,8 +207,6 @@ def check_plain(ep) -> None:
         bad.append("lateral_rate")
     if bool(getattr(ep, "ice_sheet", False)):
         bad.append("ice_sheet")
-    if float(getattr(ep, "basin_fill_grade", 0.0)) > 0.0:
-        bad.append("basin_fill_grade")
     if bool(getattr(ep, "window_lakes", False)) and float(getattr(ep, "window_lake_evap", 0.0)) > 0.0:
         bad.append("window_lake_evap")
     if bad:

@@ -326,6 +326,11 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
     state = build_state(store, params)
     land0 = float((state.surface()[state.interior] >= 0).float().mean().item())
     rep = gm.start_replay(state, params)
+    # the basins the bedrock arrives with become sedimentary plains (run.py:383-385); a resume
+    # overwrites this with the checkpoint's sediment, which already carries it
+    fill = gm.fill_basins(state, params)
+    if fill is not None:
+        log(f"[erosion] basin fill: {fill['basin_cells']} cells, {fill['fill_km3']:.1f} km3, mean {fill['fill_mean_m']:.1f} m")
     ck = find_checkpoint(store, params, apply, max_iteration=n_iter) if ep.resume else None
     if ck is not None:
         load_checkpoint(state, *ck)

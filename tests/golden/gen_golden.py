@@ -670,6 +670,25 @@ def gen_lake_balance(cs, maps, pk, WorldParams):
     print("lake_balance steps:", stats[-1])
 
 
+def gen_basin_fill(cs, maps, pk, WorldParams):
+    """The reference's fill_basins (maps.py:1278-1326) on a fresh six-face
+    N=32 world after start_replay: the sediment it lays and its statistics."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=11, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    p = _world_params(WorldParams, 32, 2, 50.0, 11, 0.45, iterations=5, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", basin_fill_grade=0.1, basin_fill_min_m=1.0)
+    st = _ref_state(cs, maps, world, p)
+    maps.start_replay(st, p)
+    h0, s0 = st.height.copy(), st.sediment.copy()
+    info = maps.fill_basins(st, p)
+    np.savez_compressed(HERE / "basin_fill.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=11,
+                        params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h0, s_start=s0, height=st.height, sediment=st.sediment, info=json.dumps(info),
+                        bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    print("basin_fill:", info)
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -680,7 +699,8 @@ def main(bake: str, only: str | None = None):
             "glacial": lambda: gen_glacial(cs, maps, pk, WorldParams),
             "lake_trace": lambda: gen_lake_trace(cs, maps, pk, WorldParams),
             "step_lake": lambda: gen_step_lake(cs, maps, pk, WorldParams),
-            "lake_balance": lambda: gen_lake_balance(cs, maps, pk, WorldParams)}
+            "lake_balance": lambda: gen_lake_balance(cs, maps, pk, WorldParams),
+            "basin_fill": lambda: gen_basin_fill(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

@@ -86,3 +86,34 @@ def test_lake_balance_rejects_a_window():
     r = _lib.load().pge_lake_balance(ctypes.byref(g), a.ctypes.data, a.ctypes.data, a.ctypes.data, 1.0, a.ctypes.data, a.ctypes.data,
                                      a.ctypes.data, a.ctypes.data, 1.0, 0.0, 0.0, a.ctypes.data, None, None, None)
     assert r == _lib.PGE_E_UNSUPPORTED
+
+
+def test_basin_fill_equals_the_reference():
+    """``pge_basin_fill`` (fill_basins, maps.py:1278-1326, on the host) on the
+    reference fixture's fresh world after start_replay, with the open ocean
+    of the oracle's sea mask (pinned to the reference): the sediment the
+    reference lays, bit for bit, and its basin count."""
+    from oracle import oracle as orc
+
+    fx = np.load(GOLDEN / "basin_fill.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    grid = get_grid(N, H, cs)
+    inter = (slice(None), slice(H, H + N), slice(H, H + N))
+    surf = np.ascontiguousarray((fx["h_start"] + fx["s_start"])[inter], np.float32)
+    below, labels, keep = orc.below_sea_components(surf, grid, 0.02)[:3]
+    ocean = np.ascontiguousarray((below & keep[np.maximum(labels, 0)]).reshape(surf.shape), np.uint8)
+    ep = json.loads(str(fx["params"]))
+    step = float(ep["basin_fill_grade"]) * (cs / 1000.0) / cs
+    add = np.empty((6, N, N))
+    basin = np.empty((6, N, N), np.uint8)
+    nb = ctypes.c_int64(0)
+    g = _lib.PgeGrid(F=6, N=N, H=H, spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    owner = np.ascontiguousarray(grid.owner, np.int32)
+    _lib.check(_lib.load().pge_basin_fill(ctypes.byref(g), owner.ctypes.data, surf.ctypes.data, ocean.ctypes.data, step,
+                                          float(ep["basin_fill_min_m"]) / cs, add.ctypes.data, basin.ctypes.data,
+                                          ctypes.byref(nb)), "pge_basin_fill")
+    info = json.loads(str(fx["info"]))
+    assert int(nb.value) == info["basin_cells"] > 0
+    sed = np.array(fx["s_start"])
+    sed[inter] += add
+    assert sed[inter].tobytes() == np.ascontiguousarray(fx["sediment"][inter]).tobytes()
