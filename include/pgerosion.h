@@ -167,6 +167,10 @@ typedef struct PgeState {
                                  drops lake_trap of its load at the shore, crosses it without touching the bed and
                                  counts no pit steps on it; the bed is never eroded below the lake's routing surface
                                  (particle.py:186-190, 626-636, 751-763, 952-956) */
+    const float *roots;       /* (F,NE,NE) the share of a droplet's exchange with the bed the plants hold back
+                                 (erosion.vegetation, maps.py:113; in [0, 1]) or NULL: bare ground.  The
+                                 exchange rate on land is scaled by 1 - roots (particle.py:615-618); not with
+                                 the adjoint's tape */
 } PgeState;
 
 /* droplet spawns of one iteration: rain first, then re-injected stockpiles */

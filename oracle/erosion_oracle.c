@@ -24,8 +24,8 @@
  * Scope: the plain path with or without the routing surface (particles steer
  * on it where it stands above the terrain) and with or without overflowing
  * lakes flagged by the caller (crossing without exchange, the load dropped at
- * the shore, the bed kept at the water level; no lake parks), no lateral
- * bank cut, no roots; masks 0/1/2, windows (spherical = 0) and
+ * the shore, the bed kept at the water level; no lake parks), with or
+ * without roots (the exchange scaled by 1 - roots), no lateral bank cut; masks 0/1/2, windows (spherical = 0) and
  * deposit-on-exit are supported.  Numba types the packed samples as float32 and so computes
  * the stencil differences of _sbilin_grad in float32; the change list keeps
  * volumes and momenta as float32.  Both are mirrored here.
@@ -314,6 +314,7 @@ typedef struct {
         ocean_rate, fan_room, dep_floor, lake_trap;
     int32_t max_steps, pit_steps, ocean_steps, deposit_on_exit, N, H, spherical, F;
     int32_t use_route, pad;
+    const float *roots; /* (F,NE,NE) the share of the exchange the plants hold back, or NULL */
 } OrcTraceParams;
 
 static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mask, int f, double x, double y,
@@ -475,6 +476,7 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
             } else {
                 k_e = P->deposition_rate;
             }
+            if (P->roots) k_e *= 1.0 - (double)P->roots[cidx]; /* roots hold the ground (particle.py:615-618) */
             double cdiff = k_e * (c_eq - sed);
             if (in_lake) {
                 cdiff = 0.0; /* crossing a lake: the bed sees nothing (particle.py:626-629) */

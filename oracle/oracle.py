@@ -84,7 +84,7 @@ class TraceParams(ctypes.Structure):
         "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
         "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap")] + [
         (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F",
-                                      "use_route", "pad")]
+                                      "use_route", "pad")] + [("roots", ctypes.c_void_p)]
 
 
 class ApplyParams(ctypes.Structure):
@@ -165,6 +165,8 @@ class OracleState:
     #: overflowing lakes (uint8, 1 a lake, 2 a lake with room for its rivers' load; maps.py:87), set by the caller or
     #: by refresh_lakes_window; read with the routing surface only
     lake_flag: np.ndarray = None
+    #: the share of the exchange the plants hold back (float32 (F, NE, NE), erosion.vegetation) or None
+    roots: np.ndarray = None
     base_at: int = None  # iteration of the last sea-mask refresh (refresh_base)
     ice_prev: np.ndarray = None  # the last glacial pass's ice (erosion.glacial_sticky)
     land_target: float | None = None
@@ -305,7 +307,8 @@ def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -
         fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u), lake_trap=float(getattr(ep, "lake_trap", 0.9)),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
         deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
-        F=int(state.F), use_route=int(getattr(state, "route", None) is not None))
+        F=int(state.F), use_route=int(getattr(state, "route", None) is not None),
+        roots=None if getattr(state, "roots", None) is None else _p(state.roots))
 
 
 def apply_params(state, ep, iter_deposit) -> ApplyParams:

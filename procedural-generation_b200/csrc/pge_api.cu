@@ -207,6 +207,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         const int minb = p->blocks_per_sm >= 2 ? 2 : 1;
         if (s->route && (p->precision != PGE_PREC_F64 || tape))
             return fail(PGE_E_UNSUPPORTED, "the routing surface needs the float64 trace and no tape");
+        if (s->roots && tape) return fail(PGE_E_UNSUPPORTED, "the adjoint's tape does not differentiate the roots");
         int bps = tape ? droplet_blocks_per_sm_f64_tape(threads)
                   : s->route ? droplet_blocks_per_sm_f64_route(threads, true)
                   : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
@@ -236,6 +237,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.erod = s->erodibility;
         a.R = s->route ? ws_ptr<float2>(ws, lay.route2) : nullptr;
         a.lakes = s->route && s->lake_flag ? 1 : 0;
+        a.roots = s->roots;
         if (tape) a.tape = *tape;
         a.p = *p;
         a.acc4 = ws_ptr<long long>(ws, lay.acc4);

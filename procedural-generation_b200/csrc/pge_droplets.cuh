@@ -874,6 +874,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 } else {
                     k_e = k_depr;
                 }
+                if (a.roots) k_e *= R(1) - R(__ldg(a.roots + cv.cell));  // roots hold the ground (particle.py:615-618)
                 R cdiff = k_e * (c_eq - sed);
                 if (ROUTE) {
                     if (in_lake) {

@@ -110,6 +110,7 @@ struct DropArgs {
     const float *erod;   // per-cell erodibility multiplier, or nullptr (1); read by the ledger variants
     const float2 *R;     // packed routing surface (route, flag) or nullptr: the ROUTE variants steer on it
     int lakes;           // the packed flags mark overflowing lakes (the ROUTE variants read the next cell's flag)
+    const float *roots;  // per-cell share of the exchange the plants hold back, or nullptr (bare ground)
     PgeTape tape;        // the adjoint's record (the taped kernel variant only)
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM

@@ -44,7 +44,7 @@ class PgeGrid(ctypes.Structure):
 class PgeState(ctypes.Structure):
     _fields_ = [(n, c_vp) for n in ("height", "sediment", "discharge", "momentum", "pending", "base", "uplift",
                                     "hardness", "precip", "evap", "mask", "metric", "metric_inv", "erodibility", "route",
-                                    "lake_flag")]
+                                    "lake_flag", "roots")]
 
 
 class PgeSpawns(ctypes.Structure):

@@ -91,6 +91,9 @@ class ErosionState:
     #: overflowing lakes (uint8, (F, NE, NE): 1 a lake, 2 a lake with room for its rivers' load; maps.py:87) or None:
     #: set by the caller (the hydro stage's balance) or by refresh_lakes_window; read with the routing surface only
     lake_flag: torch.Tensor = field(default=None, repr=False)
+    #: the share of a droplet's exchange with the bed the plants hold back (float32 (F, NE, NE) in [0, 1],
+    #: erosion.vegetation) or None: bare ground
+    roots: torch.Tensor = field(default=None, repr=False)
     #: the potential evaporation the planet's lake balance runs on (float32, (F, NE, NE)) in place of evap, or None
     lake_pet: torch.Tensor = field(default=None, repr=False)
     #: the open sea of the last sea-mask refresh (bool, (F, N, N)), the lake balance's drains; None before the first
@@ -184,7 +187,7 @@ class ErosionState:
                         momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
                         hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
                         metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility),
-                        route=_ptr(self.route), lake_flag=_ptr(self.lake_flag))
+                        route=_ptr(self.route), lake_flag=_ptr(self.lake_flag), roots=_ptr(self.roots))
 
     def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to

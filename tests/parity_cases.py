@@ -65,7 +65,8 @@ def isolated_case(path=GOLDEN / "trace_isolated.npz") -> dict:
 def window_case(path=GOLDEN / "window_trace.npz") -> dict:
     """One face of the N=48 world as a window (spherical=False, F = 1; mask:
     active basin, frozen margin, outside ring; deposit_on_exit) with droplets
-    that share cells, and the reference's change lists and serial apply."""
+    that share cells, and the reference's change lists and serial apply
+    (``roots_trace.npz``: the same with a roots field)."""
     t = np.load(path)
     N, H = int(t["N"]), int(t["H"])
     cs = float(t["cell_size_m"])
@@ -83,6 +84,8 @@ def window_case(path=GOLDEN / "window_trace.npz") -> dict:
                              evap=t["evap"], uplift=np.zeros((1, NE, NE)), mask=t["mask"], metric=t["metric"],
                              metric_inv=t["metric_inv"], N=N, H=H, spherical=False, height_unit_m=cs, base=t["base"].copy(),
                              deposit_on_exit=bool(t["deposit_on_exit"]))
+        if "roots" in t.files:
+            st.roots = np.ascontiguousarray(t["roots"], np.float32)
         st.pack()
         tp = orc.trace_params(st, ep, case["volume0"], case["conc_scale"])
         cl = orc.trace(st, tp, t["sp_face"], t["sp_x"], t["sp_y"], t["sp_sed"], t["sp_dir"], case["volume0"])

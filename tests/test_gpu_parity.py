@@ -346,6 +346,27 @@ def test_window_change_lists_match_reference(cuda):
         np.testing.assert_allclose(a[3], b[3], rtol=1e-5, atol=1e-7, err_msg=f"droplet {p} momentum")
 
 
+def test_window_roots_change_lists_match_reference(cuda):
+    """The window with a roots field (erosion.vegetation, particle.py:615-618;
+    the reference's fixture): every droplet's change list -- cells and death
+    causes identical, deltas / volumes / momenta within 1e-5 relative."""
+    from tests.parity_cases import GOLDEN
+
+    case = window_case(GOLDEN / "roots_trace.npz")
+    st = _gpu_window_state(case)
+    st.roots = torch.as_tensor(np.ascontiguousarray(case["roots"], np.float32), device="cuda")
+    res = gm.trace_changelist(st, case["params"], case["sp_face"], case["sp_x"], case["sp_y"], case["sp_sed"], case["sp_dir"],
+                              case["volume0"], case["conc_scale"], precision=_lib.PREC_F64)
+    cap = case["cap"]
+    assert np.array_equal(res["sp_death"], case["sp_death"])
+    assert np.array_equal(res["cl_count"], case["cl_count"])
+    for p, (a, b) in enumerate(zip(changelist_rows(res, cap), changelist_rows(case, cap))):
+        assert np.array_equal(a[0], b[0]), f"droplet {p}: cell path differs"
+        np.testing.assert_allclose(a[1], b[1], rtol=1e-5, atol=1e-12, err_msg=f"droplet {p} delta")
+        np.testing.assert_allclose(a[2], b[2], rtol=1e-5, atol=0, err_msg=f"droplet {p} volume")
+        np.testing.assert_allclose(a[3], b[3], rtol=1e-5, atol=1e-7, err_msg=f"droplet {p} momentum")
+
+
 def test_window_ordered_pass_matches_oracle(cuda):
     """The window's droplets (sharing cells) through the ordered apply in the
     reference's chunks against the oracle's chunked serial pass (trace,

@@ -285,3 +285,22 @@ def test_lake_steps_match_reference_bit_exact():
         assert np.array_equal(getattr(st, k), t[k]), k
     inter = (slice(None), slice(st.H, st.H + st.N), slice(st.H, st.H + st.N))
     assert np.array_equal(st.route[inter], t["route"][inter])
+
+
+def test_roots_trace_and_serial_apply_match_reference_bit_exact():
+    """Roots (erosion.vegetation: the exchange on land scaled by 1 - roots,
+    particle.py:615-618) on the window: the oracle's trace and serial apply
+    equal the reference's bit for bit, and the roots change the pass."""
+    case = window_case(GOLDEN / "roots_trace.npz")
+    res = case["oracle"]()
+    cap = case["cap"]
+    for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
+        assert np.array_equal(res[k], case[k]), k
+    for a, b in zip(changelist_rows(res, cap), changelist_rows(case, cap)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    for k in ("acc", "pending", "disch_track", "mom_track"):
+        assert np.array_equal(res[k], case[k]), k
+    assert np.array_equal(res["apply_out"], case["apply_out"])
+    bare = window_case(GOLDEN / "window_trace.npz")
+    assert not np.array_equal(case["cl_delta"][:1000], bare["cl_delta"][:1000])
