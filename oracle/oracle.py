@@ -171,6 +171,7 @@ class OracleState:
     ice_prev: np.ndarray = None  # the last glacial pass's ice (erosion.glacial_sticky)
     land_target: float | None = None
     deposit_on_exit: bool = False
+    inflow_volume: float = 0.0  # window mode: spawn weight flowing in across the edge, not rain on the window
     samp: np.ndarray = field(default=None, repr=False)
     acc: np.ndarray = field(default=None, repr=False)
     disch_track: np.ndarray = field(default=None, repr=False)
@@ -392,7 +393,8 @@ def run_iteration(state, params, iteration_key, n_particles=None, particles_per_
     if float(ep.disc_saturation_cells) > 0.0 or float(ep.momentum_saturation_cells) > 0.0:
         total = float(volume0) * float(n_particles)
         n_rain = max(int(spawn_weights(state)[0].size), 1)
-        rain_per_cell = total / n_rain
+        rain_per_cell = max(total - float(getattr(state, "inflow_volume", 0.0)), 0.0) / n_rain  # maps.py:913-917
+        rain_per_cell = rain_per_cell if rain_per_cell > 0.0 else total / n_rain
         if float(ep.disc_saturation_cells) > 0.0:
             disc_sat = float(ep.disc_saturation_cells) * rain_per_cell
         if float(ep.momentum_saturation_cells) > 0.0:

@@ -75,6 +75,9 @@ class ErosionState:
     iteration: int = 0
     land_target: float | None = None
     deposit_on_exit: bool = False
+    #: window mode: the part of the spawn weight that is water flowing in across the window's edge, not rain on it
+    #: (zoom tiles); excluded from the rain per cell the cell-count discharge scales use
+    inflow_volume: float = 0.0
     max_droplets: int = 0
     max_steps: int = 0
     max_wave: int = 0
@@ -590,7 +593,10 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     disc_sat = float(ep.disc_saturation)
     mom_scale = 1.0
     if float(ep.disc_saturation_cells) > 0.0 or float(ep.momentum_saturation_cells) > 0.0:
-        rain_per_cell = volume0 * P / max(n_spawnable, 1)
+        # the window's inflow across its edge is not rain on it (maps.py:913-917)
+        rain_total = volume0 * P
+        rain_per_cell = max(rain_total - float(state.inflow_volume), 0.0) / max(n_spawnable, 1)
+        rain_per_cell = rain_per_cell if rain_per_cell > 0.0 else rain_total / max(n_spawnable, 1)
         if float(ep.disc_saturation_cells) > 0.0:
             disc_sat = float(ep.disc_saturation_cells) * rain_per_cell
         if float(ep.momentum_saturation_cells) > 0.0:

@@ -735,6 +735,38 @@ def gen_roots_trace(cs, maps, pk, WorldParams):
     print(f"roots_trace: {x.size} droplets, entries {int(res['cl_count'].sum())}, clamped {ap[0]}")
 
 
+def gen_window_steps(cs, maps, pk, WorldParams):
+    """Full reference steps on a window (maps.step with spherical=False):
+    the window of the evolved N=48 world with its masks, the cell-count
+    discharge scales on (disc_saturation_cells, momentum_saturation_cells)
+    and part of the spawn weight declared as inflow across the window's edge
+    (ErosionState.inflow_volume, maps.py:913-917)."""
+    st, p, fw, w, mask = _window_of_evolved(cs, maps, pk, WorldParams)
+    NE, H, N = st.NE, st.H, st.N
+    unit = st.height_unit_m
+    rng = np.random.default_rng(101)
+    precip = (0.5 + rng.random((1, NE, NE))).astype(np.float32)
+    q = p.with_overrides(erosion={"disc_saturation_cells": 40.0, "momentum_saturation_cells": 15.0, "uplift_mode": "stack"})
+    ws = maps.ErosionState(height=w["height"].copy(), sediment=w["sediment"].copy(), discharge=w["discharge"].copy(),
+                           momentum=w["momentum"].copy(), hardness=w["hardness"], precip=precip, evap=w["evap"],
+                           uplift=np.zeros((1, NE, NE)), mask=mask, metric=w["metric"], metric_inv=w["metric_inv"], N=N, H=H,
+                           spherical=False, height_unit_m=unit, base=w["base"].copy(), deposit_on_exit=True)
+    ws.inflow_volume = float(0.3 * maps.spawn_weights(ws)[1].sum())  # 30 % of the spawn weight flows in
+    h0 = {k: getattr(ws, k).copy() for k in ("height", "sediment", "discharge", "momentum")}
+    stats = []
+    for it in range(3):
+        s_ = maps.step(ws, q, it, n_particles=1500)
+        stats.append({k: s_[k] for k in ("particles", "entries", "clamped", "deaths")})
+    np.savez_compressed(HERE / "window_steps.npz", N=N, H=H, cell_size_m=unit, seed=int(q.world.seed), land_fraction=0.35,
+                        mask=mask, precip=precip, evap=w["evap"],
+                        hardness=w["hardness"], base=w["base"], metric=w["metric"], metric_inv=w["metric_inv"],
+                        inflow_volume=ws.inflow_volume, n_particles=1500, iterations=3,
+                        params=json.dumps({k: getattr(q.erosion, k) for k in q.erosion.__dataclass_fields__}),
+                        **{f"start_{k}": v for k, v in h0.items()}, height=ws.height, sediment=ws.sediment,
+                        discharge=ws.discharge, momentum=ws.momentum, pending=ws.pending, stats=json.dumps(stats))
+    print("window_steps:", stats[-1])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -747,7 +779,8 @@ def main(bake: str, only: str | None = None):
             "step_lake": lambda: gen_step_lake(cs, maps, pk, WorldParams),
             "lake_balance": lambda: gen_lake_balance(cs, maps, pk, WorldParams),
             "basin_fill": lambda: gen_basin_fill(cs, maps, pk, WorldParams),
-            "roots_trace": lambda: gen_roots_trace(cs, maps, pk, WorldParams)}
+            "roots_trace": lambda: gen_roots_trace(cs, maps, pk, WorldParams),
+            "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

@@ -95,3 +95,44 @@ def test_seafloor_stockpile_is_bounded(cuda):
     assert pend_k.max() <= (1.0 - w) / w * fresh.max() * (1.0 + 1e-8)
     assert pend_k[-1] < 0.25 * np.sum((1.0 - w) * fresh), (pend_k[-1], np.sum((1.0 - w) * fresh))
     assert pend_k[3 * n // 4:].max() < 2.0 * pend_k[n // 4: n // 2].max(), pend_k
+
+
+def test_window_steps_with_inflow_follow_the_reference(cuda):
+    """maps.step on a window with the cell-count discharge scales and part of
+    the spawn weight declared as inflow across its edge (maps.py:913-917;
+    the reference's own steps in tests/golden/window_steps.npz, which the
+    oracle equals bit for bit): the hypsometry of the active interior within
+    the chaotic bound of the plain steps after three iterations."""
+    import json
+
+    import torch
+
+    from pgerosion.params import WorldGroup, WorldParams
+    from tests.parity_cases import GOLDEN, erosion_params
+    from tests.test_gpu_parity import HYPS_TOL_MANY
+
+    t = np.load(GOLDEN / "window_steps.npz")
+    ep = erosion_params(str(t["params"]))
+    params = WorldParams(world=WorldGroup(seed=int(t["seed"]), N_c=int(t["N"]), cell_size_m=float(t["cell_size_m"]),
+                                          land_fraction=float(t["land_fraction"]), halo=int(t["H"])), erosion=ep)
+    dev = torch.device("cuda")
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    NE = int(t["N"]) + 2 * int(t["H"])
+    st = gm.ErosionState(height=f64(t["start_height"]), sediment=f64(t["start_sediment"]), discharge=f64(t["start_discharge"]),
+                         momentum=f64(t["start_momentum"]), hardness=f32(t["hardness"]), precip=f32(t["precip"]),
+                         evap=f32(t["evap"]), uplift=f64(np.zeros((1, NE, NE))),
+                         mask=torch.as_tensor(np.ascontiguousarray(t["mask"], np.uint8), device=dev), metric=f32(t["metric"][0]),
+                         metric_inv=f32(t["metric_inv"][0]), N=int(t["N"]), H=int(t["H"]), spherical=False,
+                         height_unit_m=float(t["cell_size_m"]), base=f64(t["base"]), deposit_on_exit=True,
+                         inflow_volume=float(t["inflow_volume"]))
+    stats = json.loads(str(t["stats"]))
+    for it in range(int(t["iterations"])):
+        s = gm.step(st, params, it, n_particles=int(t["n_particles"]))
+        if it == 0:  # later iterations re-inject stockpiles the run itself made
+            assert s["particles"] == stats[it]["particles"]
+    a = st.to_numpy()
+    act = np.asarray(t["mask"]) == 1
+    hg = np.percentile((a["height"] + a["sediment"])[act] * float(t["cell_size_m"]), [1, 5, 10, 25, 50, 75, 90, 95, 99])
+    hr = np.percentile((t["height"] + t["sediment"])[act] * float(t["cell_size_m"]), [1, 5, 10, 25, 50, 75, 90, 95, 99])
+    assert np.abs(hg - hr).max() <= HYPS_TOL_MANY, (hg, hr)

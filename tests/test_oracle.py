@@ -304,3 +304,44 @@ def test_roots_trace_and_serial_apply_match_reference_bit_exact():
     assert np.array_equal(res["apply_out"], case["apply_out"])
     bare = window_case(GOLDEN / "window_trace.npz")
     assert not np.array_equal(case["cl_delta"][:1000], bare["cl_delta"][:1000])
+
+
+def _window_steps_state(t, ep):
+    NE = int(t["N"]) + 2 * int(t["H"])
+    st = orc.OracleState(height=t["start_height"].copy(), sediment=t["start_sediment"].copy(),
+                         discharge=t["start_discharge"].copy(), momentum=t["start_momentum"].copy(), hardness=t["hardness"],
+                         precip=t["precip"], evap=t["evap"], uplift=np.zeros((1, NE, NE)), mask=t["mask"], metric=t["metric"],
+                         metric_inv=t["metric_inv"], N=int(t["N"]), H=int(t["H"]), spherical=False,
+                         height_unit_m=float(t["cell_size_m"]), base=t["base"].copy(), deposit_on_exit=True)
+    st.inflow_volume = float(t["inflow_volume"])
+    return st
+
+
+def test_window_steps_with_inflow_match_reference_bit_exact():
+    """Full steps on a window (maps.step, spherical=False: masks, deposit on
+    exit, no halo exchange or datum hold) with the cell-count discharge
+    scales on and part of the spawn weight declared as inflow across the
+    window's edge (maps.py:913-917): the oracle's state equals the
+    reference's bit for bit, and the inflow changes the run."""
+    from tests.parity_cases import erosion_params
+
+    from pgerosion.params import WorldGroup, WorldParams
+
+    t = np.load(GOLDEN / "window_steps.npz")
+    ep = erosion_params(str(t["params"]))
+    params = WorldParams(world=WorldGroup(seed=int(t["seed"]), N_c=int(t["N"]), cell_size_m=float(t["cell_size_m"]),
+                                          land_fraction=float(t["land_fraction"]), halo=int(t["H"])), erosion=ep)
+    st = _window_steps_state(t, ep)
+    stats = json.loads(str(t["stats"]))
+    for it in range(int(t["iterations"])):
+        s = orc.step(st, params, it, n_particles=int(t["n_particles"]))
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == stats[it][k], (it, k)
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        assert np.array_equal(getattr(st, k), t[k]), k
+    st2 = _window_steps_state(t, ep)
+    st2.inflow_volume = 0.0
+    orc.step(st2, params, 0, n_particles=int(t["n_particles"]))
+    st1 = _window_steps_state(t, ep)
+    orc.step(st1, params, 0, n_particles=int(t["n_particles"]))
+    assert not (np.array_equal(st1.sediment, st2.sediment) and np.array_equal(st1.discharge, st2.discharge))
