@@ -190,6 +190,10 @@ typedef struct PgeParams {
         ocean_rate, fan_room, dep_floor, iter_erode, iter_deposit, fan_slope, offshore_writeoff, ema;
     double lake_trap;        /* share of the load dropped at the shore on entering a lake (erosion.lake_trap);
                                 read only with s->lake_flag */
+    double lateral_rate;     /* erosion.lateral_rate > 0: a droplet cutting its bed also cuts the bank one cell
+                                across the flow on the outside of its bend (particle.py:699-738), an extra
+                                change-list entry of volume -2; float64 trace only, not with the tape, and the
+                                workspace's max_steps must hold 2 x max_steps (two entries a step) */
     int32_t max_steps, pit_steps, ocean_steps;
     int32_t wave;            /* droplets traced against one frozen terrain (the reference's chunk) */
     int32_t precision;       /* PGE_PREC_* */

@@ -25,7 +25,8 @@
  * on it where it stands above the terrain) and with or without overflowing
  * lakes flagged by the caller (crossing without exchange, the load dropped at
  * the shore, the bed kept at the water level; no lake parks), with or
- * without roots (the exchange scaled by 1 - roots), no lateral bank cut; masks 0/1/2, windows (spherical = 0) and
+ * without roots (the exchange scaled by 1 - roots), with or without the
+ * bank cut on the outside of bends (erosion.lateral_rate); masks 0/1/2, windows (spherical = 0) and
  * deposit-on-exit are supported.  Numba types the packed samples as float32 and so computes
  * the stencil differences of _sbilin_grad in float32; the change list keeps
  * volumes and momenta as float32.  Both are mirrored here.
@@ -311,7 +312,7 @@ int orc_change_list_cap(int max_steps, int lateral)
 typedef struct {
     double dt, density, friction, deposition_rate, evap_rate, k_mom, mom_scale, k_disc, disc_saturation,
         disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
-        ocean_rate, fan_room, dep_floor, lake_trap;
+        ocean_rate, fan_room, dep_floor, lake_trap, lateral_rate;
     int32_t max_steps, pit_steps, ocean_steps, deposit_on_exit, N, H, spherical, F;
     int32_t use_route, pad;
     const float *roots; /* (F,NE,NE) the share of the exchange the plants hold back, or NULL */
@@ -392,6 +393,7 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
         double q = sbilin(S, f, fi, fj, S_DISCH);
         if (q < 0.0) q = 0.0;
         double vol_rel = vol / volume0;
+        const double psa = sa, psb = sb; /* the direction this step started with (the bend) */
         double fr = 1.0 - P->dt * P->friction;
         if (fr < 0.0) fr = 0.0;
         sa *= fr;
@@ -498,6 +500,32 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
             }
             sed += cdiff;
             RECORD(cidx, -cdiff * vol_rel, vol, vol * sa, vol * sb);
+            /* the outside of the bend (particle.py:699-738): the bank one cell across the flow */
+            if (P->lateral_rate > 0.0 && cdiff > 0.0 && n + 2 * SPREAD + 2 < cap) {
+                double cross = psa * sb - psb * sa;
+                double turn = cross > 0.0 ? cross : -cross;
+                if (turn > 1e-6) {
+                    double sgn = cross > 0.0 ? 1.0 : -1.0;
+                    double bx = x + sgn * sb, by = y - sgn * sa;
+                    int bei = (int)floor(bx) + H, bej = (int)floor(by) + H;
+                    if (bei >= 0 && bei < NE && bej >= 0 && bej < NE) {
+                        int64_t bcell = ((int64_t)f * NE + bei) * NE + bej;
+                        if (mask[bcell] == MASK_ACTIVE) {
+                            float bank = S->samp[bcell * NS + S_SURF] - h_here;
+                            if (bank > 0.0f) {
+                                double lat = P->lateral_rate * turn * cdiff;
+                                double lcap = (double)bank / kexp;
+                                if (lcap > P->max_erode) lcap = P->max_erode;
+                                if (lat * vol_rel > lcap) lat = lcap / vol_rel;
+                                if (lat > 0.0) {
+                                    sed += lat;
+                                    RECORD(bcell, -lat * vol_rel, -2.0, 0.0, 0.0);
+                                }
+                            }
+                        }
+                    }
+                }
+            }
         }
         double ev = 1.0 - P->dt * P->evap_rate * (double)cp[S_EVAP];
         if (ev < 0.01) ev = 0.01;
@@ -595,7 +623,7 @@ void orc_trace(const OrcTraceParams *P, const float *samp, const uint8_t *mask, 
                int64_t *cl_hi, int8_t *sp_death)
 {
     TraceJob J = {P, {samp, P->N + 2 * P->H}, mask, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0,
-                  orc_change_list_cap(P->max_steps, 0), cl_cell, cl_delta, cl_vol, cl_mom, cl_count, cl_lo, cl_hi,
+                  orc_change_list_cap(P->max_steps, P->lateral_rate > 0.0), cl_cell, cl_delta, cl_vol, cl_mom, cl_count, cl_lo, cl_hi,
                   sp_death, np, 0};
     int nt = g_threads;
     if (nt > 1 && np > 64) {

@@ -82,7 +82,7 @@ class TraceParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
         "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
-        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap")] + [
+        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap", "lateral_rate")] + [
         (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F",
                                       "use_route", "pad")] + [("roots", ctypes.c_void_p)]
 
@@ -97,8 +97,8 @@ def _p(a: np.ndarray):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def change_list_cap(max_steps: int) -> int:
-    return int(lib().orc_change_list_cap(int(max_steps), 0))
+def change_list_cap(max_steps: int, lateral: bool = False) -> int:
+    return int(lib().orc_change_list_cap(int(max_steps), int(bool(lateral))))
 
 
 # --------------------------------------------------------------------------
@@ -306,6 +306,7 @@ def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -
         cover_depth=_cu(ep, "cover_depth", u), min_volume=float(ep.min_volume_frac) * float(volume0),
         max_erode=_cu(ep, "max_erode", u), conc_scale=float(conc_scale), ocean_rate=float(ep.ocean_deposition_rate),
         fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u), lake_trap=float(getattr(ep, "lake_trap", 0.9)),
+        lateral_rate=float(getattr(ep, "lateral_rate", 0.0)),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
         deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
         F=int(state.F), use_route=int(getattr(state, "route", None) is not None),
@@ -324,7 +325,7 @@ def trace(state, tp: TraceParams, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0):
     """Trace particles on the current packed samples; returns the change list
     ``(cl_cell, cl_delta, cl_vol, cl_mom, cl_count, cl_lo, cl_hi, sp_death)``."""
     P = int(sp_face.shape[0])
-    cap = change_list_cap(tp.max_steps)
+    cap = change_list_cap(tp.max_steps, tp.lateral_rate > 0.0)
     cl_cell = np.zeros(P * cap, np.int32)
     cl_delta = np.zeros(P * cap)
     cl_vol = np.zeros(P * cap, np.float32)
@@ -410,7 +411,7 @@ def run_iteration(state, params, iteration_key, n_particles=None, particles_per_
     if float(ep.slope_limit_deposit) > 0.0:
         iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     max_steps = max_steps_of(ep, state.N)
-    cap = change_list_cap(max_steps)
+    cap = change_list_cap(max_steps, float(getattr(ep, "lateral_rate", 0.0)) > 0.0)
     P = sp_face.shape[0]
     chunk = chunk_size(ep, P) if chunk is None else int(chunk)
     tp = trace_params(state, ep, volume0, chunk / (volume0 * P), mom_scale, disc_sat)

@@ -81,6 +81,10 @@ int check_params(const PgeGrid *g, const PgeParams *p)
 {
     if (!p) return fail(PGE_E_ARG, "params is NULL");
     if (p->max_steps < 1 || p->max_steps > g->max_steps) return fail(PGE_E_ARG, "max_steps %d outside 1..%d", p->max_steps, g->max_steps);
+    if (!(p->lateral_rate >= 0.0)) return fail(PGE_E_ARG, "lateral_rate must be >= 0");
+    if (list_steps(*p) > g->max_steps)
+        return fail(PGE_E_ARG, "the bank cut needs a workspace for 2 x max_steps = %d steps (grid max_steps %d)", list_steps(*p),
+                    g->max_steps);
     if (p->wave < 1) return fail(PGE_E_ARG, "wave must be >= 1");
     if (p->apply != PGE_APPLY_ORDERED && p->apply != PGE_APPLY_WAVE) return fail(PGE_E_ARG, "unknown apply mode %d", p->apply);
     if (p->apply == PGE_APPLY_ORDERED && p->wave > g->max_wave)
@@ -208,7 +212,11 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         if (s->route && (p->precision != PGE_PREC_F64 || tape))
             return fail(PGE_E_UNSUPPORTED, "the routing surface needs the float64 trace and no tape");
         if (s->roots && tape) return fail(PGE_E_UNSUPPORTED, "the adjoint's tape does not differentiate the roots");
+        const bool lateral = p->lateral_rate > 0.0;
+        if (lateral && (p->precision != PGE_PREC_F64 || tape))
+            return fail(PGE_E_UNSUPPORTED, "the bank cut (lateral_rate) needs the float64 trace and no tape");
         int bps = tape ? droplet_blocks_per_sm_f64_tape(threads)
+                  : lateral ? droplet_blocks_per_sm_f64_lateral(threads, true, s->route != nullptr)
                   : s->route ? droplet_blocks_per_sm_f64_route(threads, true)
                   : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(threads, minb) : droplet_blocks_per_sm_f32(threads, minb);
         if (p->blocks_per_sm > 0 && p->blocks_per_sm < bps) bps = p->blocks_per_sm;
@@ -253,7 +261,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.rec_mom = rec_mom;
         a.rec_count = rec_count;
         a.rec_death = rec_death;
-        a.rec_cap = change_list_cap(p->max_steps);
+        a.rec_cap = change_list_cap(list_steps(*p));
         a.rec_base = 0;
         a.ledger = 1;
         a.minb = minb;
@@ -322,7 +330,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);
             const long long rec_warps =
-                (long long)sm_count() * (s->route ? droplet_blocks_per_sm_f64_route(32, false)
+                (long long)sm_count() * (lateral ? droplet_blocks_per_sm_f64_lateral(32, false, s->route != nullptr)
+                                         : s->route ? droplet_blocks_per_sm_f64_route(32, false)
                                          : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
                                                                       : droplet_blocks_per_sm_f32(32, 1, false));
             int ebits = 1;

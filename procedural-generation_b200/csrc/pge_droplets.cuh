@@ -572,7 +572,8 @@ enum { ST_DROP, ST_STEPS, ST_ENTRIES, ST_CLAMPED, ST_OVER, ST_TOPEND, ST_DEFICIT
 
 // TAPE (with LEDGER): also record the adjoint's tape (a.tape, row = the droplet's index in the pass)
 // ROUTE: steer on the routing surface a.R where it stands above the terrain
-template <int MINB, bool LEDGER, bool TAPE = false, bool ROUTE = false>
+// LATERAL: cut the bank on the outside of the bend (erosion.lateral_rate > 0)
+template <int MINB, bool LEDGER, bool TAPE = false, bool ROUTE = false, bool LATERAL = false>
 __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
 {
     const PgeParams &p = a.p;
@@ -615,6 +616,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
     bool has_pe = false;
     Ledger L;
     int rec_n = 0;
+    int nbank = 0;  // bank entries (volume -2) of this droplet: entries, not steps
 
     while (true) {
         // ---- refill: lanes without a droplet take the next indices of the wave
@@ -657,6 +659,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     L.eroded_fx = L.deposited_fx = 0;
                     t.reset(++gen);
                     rec_n = 0;
+                    nbank = 0;
                     const int ei = cell_of(x, N) + H, ej = cell_of(y, N) + H;
                     load_view(a, f, x, y, ei, ej, cv);
                     cur.cell = cv.cell;
@@ -688,6 +691,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         int cause = -1;
         bool exited = false;
         bool have_entry = false;
+        bool have_bank = false;
+        Entry bank_en;
         bool moved = false;
         Entry en;
         do {
@@ -741,6 +746,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 if (TAPE) tb |= PGE_TB_Q_ZERO;
             }
             const R vol_rel = vol / volume0;
+            [[maybe_unused]] const R psa = sa, psb = sb;  // the direction this step started with (the bend, particle.py:485-486)
             R fr = R(1) - k_dt * k_friction;
             if (fr < R(0)) {
                 fr = R(0);
@@ -922,6 +928,39 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 en.mb = (float)(vol * sb);
                 en.sidx = step;
                 have_entry = true;
+                if (LATERAL && cdiff > R(0)) {
+                    // the outside of the bend (particle.py:699-738): a droplet cutting and turning also cuts
+                    // the bank one cell across the flow, down towards the bed it just eroded; the change
+                    // list's room (two entries a step) always holds it
+                    const R cross = psa * sb - psb * sa;
+                    const R turn = cross > R(0) ? cross : -cross;
+                    if (turn > R(1e-6)) {
+                        const R sgn = cross > R(0) ? R(1) : R(-1);
+                        const R bx = x + sgn * sb, by = y - sgn * sa;
+                        const int bei = (int)floor(bx) + H, bej = (int)floor(by) + H;
+                        if (bei >= 0 && bei < NE && bej >= 0 && bej < NE) {
+                            const long long bc = ((long long)f * NE + bei) * NE + bej;
+                            const int bm = a.mask ? (int)__ldg(a.mask + bc) : PGE_MASK_ACTIVE;
+                            const float bank = bm == PGE_MASK_ACTIVE ? __ldg(&a.A[bc].x) - h_here : 0.0f;
+                            if (bank > 0.0f) {
+                                R lat = R(p.lateral_rate) * turn * cdiff;
+                                R lcap = R(bank) / kexp;
+                                if (lcap > k_maxe) lcap = k_maxe;
+                                if (lat * vol_rel > lcap) lat = lcap / vol_rel;
+                                if (lat > R(0)) {
+                                    sed += lat;
+                                    bank_en.cell = bc;
+                                    bank_en.delta = (double)(-lat * vol_rel);
+                                    bank_en.vol = -2.0f;
+                                    bank_en.ma = 0.0f;
+                                    bank_en.mb = 0.0f;
+                                    bank_en.sidx = step;
+                                    have_bank = true;
+                                }
+                            }
+                        }
+                    }
+                }
             }
             // evaporation (mass conserving)
             R ev = R(1) - k_dt * k_evap * R(cv.evap);
@@ -976,6 +1015,31 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             }
             rec_n++;
         }
+        if (LATERAL && have_bank) {
+            // the bank entry follows the step's own: the step entry is applied with the bank as its next
+            // cell, the bank entry with the next step's cell (the reference's list order)
+            LCell bk;
+            bk.cell = bank_en.cell;
+            if (LEDGER) {
+                load_lcell(a, t, bank_en.cell, bk);
+                apply_entry<TAPE, ROUTE>(a, t, L, pe, pend, true, bk, trow);
+                sync_own(bk, pend);
+                sync_own(cur, pend);
+                sync_own(nxt, pend);
+            }
+            pe = bank_en;
+            pend = bk;
+            if (a.rec_cell && rec_n < a.rec_cap) {
+                const long long o = (d - a.rec_base) * a.rec_cap + rec_n;
+                a.rec_cell[o] = (int32_t)bank_en.cell;
+                a.rec_delta[o] = bank_en.delta;
+                a.rec_vol[o] = -2.0f;
+                a.rec_mom[2 * o] = 0.0f;
+                a.rec_mom[2 * o + 1] = 0.0f;
+            }
+            rec_n++;
+            nbank++;
+        }
         if (moved) {
             // the new cell becomes current (its own change was probed above)
             cur.cell = cv.cell;
@@ -1023,7 +1087,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 rec_n++;
             }
             atomicAdd(&sstat[ST_DROP], 1ull);
-            atomicAdd(&sstat[ST_STEPS], (unsigned long long)step_entries(rec_n, nout));
+            atomicAdd(&sstat[ST_STEPS], (unsigned long long)step_entries(rec_n - nbank, nout));
             atomicAdd(&sstat[ST_ENTRIES], (unsigned long long)rec_n);
             atomicAdd(&sstat[ST_DEATH0 + cause], 1ull);
             if (a.rec_cell) {
@@ -1088,7 +1152,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             reinterpret_cast<int2 *>(a.tape.count)[trow] = make_int2(step + 1, L.tap_n);
         }
         atomicAdd(&sstat[ST_DROP], 1ull);
-        atomicAdd(&sstat[ST_STEPS], (unsigned long long)step_entries(rec_n, nout));
+        atomicAdd(&sstat[ST_STEPS], (unsigned long long)step_entries(rec_n - nbank, nout));
         atomicAdd(&sstat[ST_ENTRIES], (unsigned long long)rec_n);
         if (L.clamped) atomicAdd(&sstat[ST_CLAMPED], (unsigned long long)L.clamped);
         if (t.overflow) atomicAdd(&sstat[ST_OVER], 1ull);

@@ -35,6 +35,8 @@ constexpr double INV_FX_MASS = 1.0 / FX_MASS;
 constexpr double INV_FX_TRACK = 1.0 / FX_TRACK;
 
 __host__ __device__ inline int change_list_cap(int max_steps) { return max_steps + 2 * SPREAD + 1 + SPREAD + LAKE_PARKS; }
+// steps' worth of change-list room: two entries a step with the bank cut (particle.py:259-272)
+__host__ __device__ inline int list_steps(const PgeParams &p) { return p.lateral_rate > 0.0 ? 2 * p.max_steps : p.max_steps; }
 // distinct cells one droplet's ledger can change: one per step entry plus its final deposits
 __host__ __device__ inline int ledger_table_cap(int max_steps) { return max_steps + SPREAD + 2; }
 // hash slots per droplet thread: a power of two at least twice the table capacity
@@ -122,6 +124,8 @@ struct DropArgs {
 cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 cudaError_t launch_droplets_f64_tape(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 cudaError_t launch_droplets_f64_route(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+cudaError_t launch_droplets_f64_lateral(const DropArgs &a, int blocks, int threads, cudaStream_t st);
+int droplet_blocks_per_sm_f64_lateral(int threads, bool ledger, bool route);
 int droplet_blocks_per_sm_f64_route(int threads, bool ledger);
 int droplet_blocks_per_sm_f64_tape(int threads);
 cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);

@@ -54,7 +54,7 @@ class PgeSpawns(ctypes.Structure):
 PARAM_DOUBLES = ("dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
                  "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
                  "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "iter_erode",
-                 "iter_deposit", "fan_slope", "offshore_writeoff", "ema", "lake_trap")
+                 "iter_deposit", "fan_slope", "offshore_writeoff", "ema", "lake_trap", "lateral_rate")
 PARAM_INTS = ("max_steps", "pit_steps", "ocean_steps", "wave", "precision", "apply", "use_erode_cap", "threads_per_block",
               "blocks_per_sm", "trace_lanes", "apply_lanes")
 

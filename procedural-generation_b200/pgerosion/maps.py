@@ -427,6 +427,13 @@ class ErosionState:
 # --------------------------------------------------------------------------
 # one iteration
 # --------------------------------------------------------------------------
+def list_steps_of(ep, N) -> int:
+    """Steps' worth of change-list room a droplet needs: two entries a step
+    with the bank cut (erosion.lateral_rate, particle.py:259-272)."""
+    m = max_steps_of(ep, N)
+    return 2 * m if float(getattr(ep, "lateral_rate", 0.0)) > 0.0 else m
+
+
 def default_wave(ep, n_particles: int) -> int:
     """The reference's chunk size: the wave that reproduces its terrain freezes."""
     return chunk_size(ep, n_particles)
@@ -446,7 +453,8 @@ def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, prec
         fan_room=cell_units(ep, "fan_room", u), dep_floor=cell_units(ep, "dep_floor_m", u), iter_erode=cell_units(ep, "iter_erode", u),
         iter_deposit=float(cell_units(ep, "iter_deposit", u) if iter_deposit is None else iter_deposit),
         fan_slope=float(ep.fan_slope), offshore_writeoff=float(ep.offshore_writeoff), ema=float(ep.ema),
-        lake_trap=float(getattr(ep, "lake_trap", 0.9)), max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
+        lake_trap=float(getattr(ep, "lake_trap", 0.9)), lateral_rate=float(getattr(ep, "lateral_rate", 0.0)),
+        max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
         precision=int(precision), apply=int(apply), use_erode_cap=0, threads_per_block=int(threads_per_block),
         blocks_per_sm=int(blocks_per_sm), trace_lanes=int(trace_lanes), apply_lanes=int(apply_lanes))
 
@@ -549,7 +557,7 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     P = int(n_particles)
     max_steps = max_steps_of(ep, state.N)
     # stockpiles re-injected: at most one per interior cell; the reference's chunk is at most erosion.chunk
-    state.reserve(P + state.F * state.N * state.N, max_steps,
+    state.reserve(P + state.F * state.N * state.N, list_steps_of(ep, state.N),
                   (int(ep.chunk) if wave is None else int(wave)) if apply == _lib.APPLY_ORDERED else 1,
                   wave_tables=apply == _lib.APPLY_WAVE)
     rng, u, off = predrawn if predrawn is not None else draw_spawns(params, rng_stage, key, P)
@@ -672,7 +680,7 @@ def _erode_cap(state: ErosionState, ep, prm: PgeParams):
 
 def _ensure_workspace(state: ErosionState, ep=None) -> None:
     if state.workspace is None:
-        state.reserve(max(state.max_droplets, 1), max(state.max_steps, max_steps_of(ep, state.N) if ep is not None else 1))
+        state.reserve(max(state.max_droplets, 1), max(state.max_steps, list_steps_of(ep, state.N) if ep is not None else 1))
 
 
 def thermal_erosion(state: ErosionState, params) -> None:
@@ -893,10 +901,10 @@ def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, s
     ep = erosion_group(params)
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
-    state.reserve(P, max_steps, 1, wave_tables=True)
+    state.reserve(P, list_steps_of(ep, state.N), 1, wave_tables=True)
     L = _lib.load()
     dev = state.height.device
-    cap = max_steps + 2 * 8 + 1 + 8 + 8
+    cap = list_steps_of(ep, state.N) + 2 * 8 + 1 + 8 + 8  # change_list_cap: the reference's row width
     face = torch.as_tensor(np.asarray(sp_face, np.int32), device=dev)
     xs = [torch.as_tensor(np.asarray(a, np.float64), device=dev) for a in (sp_x, sp_y, sp_sed, sp_dir)]
     spawns = PgeSpawns(face=_ptr(face), x=_ptr(xs[0]), y=_ptr(xs[1]), sed=_ptr(xs[2]), dir=_ptr(xs[3]), count=P,
@@ -942,7 +950,7 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
     w = default_wave(ep, P) if wave is None else int(wave)
-    state.reserve(P, max_steps, w if apply == _lib.APPLY_ORDERED else 1, wave_tables=apply == _lib.APPLY_WAVE)
+    state.reserve(P, list_steps_of(ep, state.N), w if apply == _lib.APPLY_ORDERED else 1, wave_tables=apply == _lib.APPLY_WAVE)
     L = _lib.load()
     dev = state.height.device
     sp = state._spawn

@@ -193,18 +193,16 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (the lake parks of ``lake_fill``, the window lake balance, ice
-    sheet, lateral cut).  The basin fill, isostasy, the routing surface
-    (``flood_every``), the sea mask (``sea_mask_every``), the glacial pass
-    (``glacial_every``, the ice line of the evaporation field), the planet's
-    lake balance (``lake_balance`` with ``lake_fill`` off) and the lakes of
-    a window (``window_lakes`` with ``window_lake_evap = 0``) are
-    supported."""
+    path (the lake parks of ``lake_fill``, the window lake balance, the ice
+    sheet).  The bank cut (``lateral_rate``), the basin fill, isostasy, the
+    routing surface (``flood_every``), the sea mask (``sea_mask_every``),
+    the glacial pass (``glacial_every``, the ice line of the evaporation
+    field), the planet's lake balance (``lake_balance`` with ``lake_fill``
+    off) and the lakes of a window (``window_lakes`` with
+    ``window_lake_evap = 0``) are supported."""
     bad = []
     if bool(getattr(ep, "lake_balance", False)) and bool(getattr(ep, "lake_fill", False)):
         bad.append("lake_fill")
-    if float(getattr(ep, "lateral_rate", 0.0)) > 0.0:
-        bad.append("lateral_rate")
     if bool(getattr(ep, "ice_sheet", False)):
         bad.append("ice_sheet")
     if bool(getattr(ep, "window_lakes", False)) and float(getattr(ep, "window_lake_evap", 0.0)) > 0.0:

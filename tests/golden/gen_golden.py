@@ -235,7 +235,7 @@ def gen_trace(cs, maps, pk, WorldParams):
 
 
 def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit,
-               use_route=False, roots=None):
+               use_route=False, roots=None, lateral=0.0):
     n = f.size
     out = dict(cl_cell=np.zeros(n * cap, np.int32), cl_delta=np.zeros(n * cap), cl_vol=np.zeros(n * cap, np.float32),
                cl_mom=np.zeros((n * cap, 2), np.float32), cl_count=np.zeros(n, np.int64), cl_lo=np.zeros(n, np.int64),
@@ -247,7 +247,7 @@ def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y,
                        float(ep.slope_gain), float(ep.slope_saturation), float(ep.erodibility), cu("cover_depth"),
                        float(ep.min_volume_frac) * volume0, int(max_steps), cu("max_erode"), conc, int(ep.pit_steps),
                        bool(deposit_on_exit), float(ep.ocean_deposition_rate), int(ep.ocean_steps), cu("fan_room"),
-                       cu("dep_floor_m"), float(ep.lake_trap), 0.0, 0.0,
+                       cu("dep_floor_m"), float(ep.lake_trap), 0.0, float(lateral),
                        np.zeros((1, 1, 1), np.float32) if roots is None else roots, roots is not None,
                        out["cl_cell"], out["cl_delta"], out["cl_vol"], out["cl_mom"], out["cl_count"], out["cl_lo"],
                        out["cl_hi"], out["sp_death"])
@@ -767,6 +767,74 @@ def gen_window_steps(cs, maps, pk, WorldParams):
     print("window_steps:", stats[-1])
 
 
+def gen_lateral(cs, maps, pk, WorldParams):
+    """The bank cut on the outside of bends (erosion.lateral_rate,
+    particle.py:699-738; entries of volume -2 applied under the erosion caps,
+    particle.py:934-1018): one reference trace + serial apply on the window
+    of the evolved N=48 world, and full reference steps on a six-face N=32
+    world with lateral_rate = 0.5."""
+    st, p, fw, w, mask = _window_of_evolved(cs, maps, pk, WorldParams)
+    ep = p.erosion
+    NE, H, N = st.NE, st.H, st.N
+    unit = st.height_unit_m
+    rate = 0.5
+    samp = np.zeros((1, NE, NE, pk.NS), np.float32)
+    pk.pack_samples(samp, w["height"], w["sediment"], w["height"], False, w["discharge"], w["momentum"], w["evap"], w["hardness"],
+                    w["metric"], w["metric_inv"], w["base"], np.zeros((1, NE, NE), np.uint8))
+    rng = np.random.default_rng(103)
+    act = np.flatnonzero(mask.reshape(-1) == 1)
+    n_rain, n_load = 1200, 250
+    pick = act[rng.integers(0, act.size, n_rain + n_load)]
+    ei, ej = pick // NE, pick % NE
+    x = (ei - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    y = (ej - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    sed = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 0.5 + 1e-3])
+    dirs = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 2 * np.pi])
+    f = np.zeros(x.size, np.int64)
+    volume0 = 0.02
+    conc = 1.0 / (volume0 * x.size)
+    max_steps = maps.max_steps_of(ep, N)
+    cap = int(pk.change_list_cap(max_steps, True))
+    res = _ref_trace(pk, ep, samp, mask, N, H, False, True, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit, lateral=rate)
+    acc = np.zeros_like(w["height"])
+    pending = np.zeros_like(w["height"])
+    dtr = np.zeros_like(w["height"])
+    mtr = np.zeros_like(w["momentum"])
+    samp_after = samp.copy()
+    cu = lambda k: float(getattr(ep, k)) / unit
+    ap = pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                          w["height"], w["sediment"], acc, pending, samp_after, dtr, mtr, mask, cu("iter_erode"), cu("iter_deposit"),
+                          float(ep.fan_slope), False, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                          np.zeros((1, NE, NE)), np.zeros((1, NE, NE), np.int32), np.zeros(1))
+    banks = int((res["cl_vol"] == -2.0).sum())
+    np.savez_compressed(
+        HERE / "lateral_trace.npz", N=N, H=H, face=fw, **w, mask=mask, lateral_rate=rate, sp_face=f, sp_x=x, sp_y=y, sp_sed=sed,
+        sp_dir=dirs, volume0=volume0, conc_scale=conc, cap=cap, max_steps=max_steps, deposit_on_exit=True,
+        params=json.dumps({**{k: getattr(ep, k) for k in ep.__dataclass_fields__}, "lateral_rate": rate}), cell_size_m=unit,
+        **res, acc=acc, pending=pending, disch_track=dtr, mom_track=mtr, apply_out=np.array([float(a) for a in ap]))
+    print(f"lateral_trace: {x.size} droplets, entries {int(res['cl_count'].sum())}, bank entries {banks}, clamped {ap[0]}")
+
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=5, N=32, H=2, cell_size_m=50.0, land_fraction=0.3)
+    iters = 4
+    p2 = _world_params(WorldParams, 32, 2, 50.0, 5, 0.3, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                       deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", lateral_rate=rate)
+    st2 = _ref_state(cs, maps, world, p2)
+    init = dict(bedrock=world.bedrock, hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    maps.start_replay(st2, p2)
+    h_start = st2.height.copy()
+    stats = []
+    for it in range(iters):
+        s_ = maps.step(st2, p2, it, n_particles=4096)
+        stats.append({k: s_[k] for k in ("particles", "entries", "clamped", "deaths", "datum_shift")})
+    np.savez_compressed(HERE / "step_lateral.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.3, seed=5, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p2.erosion, k) for k in p2.erosion.__dataclass_fields__}),
+                        h_start=h_start, height=st2.height, sediment=st2.sediment, discharge=st2.discharge,
+                        momentum=st2.momentum, pending=st2.pending, stats=json.dumps(stats), **init)
+    print("step_lateral:", stats[-1])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -780,7 +848,8 @@ def main(bake: str, only: str | None = None):
             "lake_balance": lambda: gen_lake_balance(cs, maps, pk, WorldParams),
             "basin_fill": lambda: gen_basin_fill(cs, maps, pk, WorldParams),
             "roots_trace": lambda: gen_roots_trace(cs, maps, pk, WorldParams),
-            "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams)}
+            "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams),
+            "lateral": lambda: gen_lateral(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

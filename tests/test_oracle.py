@@ -345,3 +345,41 @@ def test_window_steps_with_inflow_match_reference_bit_exact():
     st1 = _window_steps_state(t, ep)
     orc.step(st1, params, 0, n_particles=int(t["n_particles"]))
     assert not (np.array_equal(st1.sediment, st2.sediment) and np.array_equal(st1.discharge, st2.discharge))
+
+
+def test_bank_cut_trace_and_serial_apply_match_reference_bit_exact():
+    """The bank cut on the outside of bends (erosion.lateral_rate,
+    particle.py:699-738: an entry of volume -2 after the step's own, applied
+    under the erosion caps, no discharge, the path unchanged) on the window:
+    the oracle's trace and serial apply equal the reference's bit for bit."""
+    case = window_case(GOLDEN / "lateral_trace.npz")
+    res = case["oracle"]()
+    cap = case["cap"]
+    assert cap == orc.change_list_cap(int(case["max_steps"]), True)
+    for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
+        assert np.array_equal(res[k], case[k]), k
+    for a, b in zip(changelist_rows(res, cap), changelist_rows(case, cap)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    assert int(sum((r[2] == -2.0).sum() for r in changelist_rows(case, cap))) > 1000
+    for k in ("acc", "pending", "disch_track", "mom_track"):
+        assert np.array_equal(res[k], case[k]), k
+    assert np.array_equal(res["apply_out"], case["apply_out"])
+
+
+def test_bank_cut_steps_match_reference_bit_exact():
+    """Full steps on the sphere with lateral_rate = 0.5: the oracle's state
+    equals the reference's bit for bit."""
+    c = step_case(GOLDEN / "step_lateral.npz")
+    t = c["t"]
+    st = orc.OracleState.from_world(c["world"], c["params"])
+    orc.start_replay(st, c["params"])
+    assert np.array_equal(st.height, t["h_start"])
+    for it in range(c["iterations"]):
+        s = orc.step(st, c["params"], it, n_particles=c["n_particles"])
+        r = c["stats"][it]
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == r[k], (it, k)
+        assert s["datum_shift"] == r["datum_shift"]
+    for k in ("height", "sediment", "discharge", "momentum", "pending"):
+        assert np.array_equal(getattr(st, k), t[k]), k
