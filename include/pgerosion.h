@@ -46,6 +46,9 @@
  *                                                  globe/hydro/priority_flood.py:127-191,
  *                                                  globe/hydro/routing.py:28-90,
  *                                                  globe/hydro/balance.py:63-284
+ *   pge_window_lake_balance  ErosionState._balance_window_lakes (window_lake_evap > 0):
+ *                         a window's lakes settled against evaporation (HOST code)
+ *                                                  globe/erosion/maps.py:675-736
  *   pge_basin_fill        fill_basins: sediment graded into the closed basins of a
  *                         fresh state (HOST code, host pointers)
  *                                                  globe/erosion/maps.py:1216-1229, 1278-1326
@@ -455,6 +458,23 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
                              const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                              double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
                              PgeLakeInfo *info);
+
+/* The lakes of a window balanced against evaporation (maps.py:675-736,
+ * erosion.window_lakes with window_lake_evap > 0), on the HOST (host
+ * pointers, no CUDA call), over the whole (NE,NE) window array: the flat
+ * priority flood draining to the cells not active and the array's border,
+ * precip (the spawn weight) accumulated down the flood tree, every
+ * depression (8-connected active cells the flood fills more than 1e-6 above
+ * the float32 surface, numbered in raster order) settled where the inflow
+ * reaching it meets lake_evap x max(evap, 0) summed over its cells under the
+ * water (a dry one drops below its floor, one that cannot evaporate its
+ * inflow spills).  lake (NE,NE) gets 1 on active cells more than min_depth
+ * (cell units) under water; route (NE,NE, in/out) is lowered to the water on
+ * them; counts (5 int64, may be NULL): depressions, overflowing, closed,
+ * dry, lake cells.  The caller flags the interior. */
+PGE_API int pge_window_lake_balance(const PgeGrid *g, const float *surface, const uint8_t *active, const float *precip,
+                                    const float *evap, double lake_evap, double min_depth, double *route, uint8_t *lake,
+                                    int64_t *counts);
 
 /* The basin fill of a fresh state (maps.py:1278-1326, erosion.basin_fill_grade),
  * on the HOST (host pointers, no CUDA call): the same priority flood as

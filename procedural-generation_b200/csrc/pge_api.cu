@@ -575,6 +575,19 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
     return PGE_OK;
 }
 
+PGE_API int pge_window_lake_balance(const PgeGrid *g, const float *surface, const uint8_t *active, const float *precip,
+                                    const float *evap, double lake_evap, double min_depth, double *route, uint8_t *lake,
+                                    int64_t *counts)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (g->spherical || g->F != 1) return fail(PGE_E_UNSUPPORTED, "window_lake_balance: a window (F = 1, not spherical)");
+    if (!surface || !active || !precip || !evap || !route || !lake) return fail(PGE_E_ARG, "window_lake_balance: NULL pointer");
+    if (!(lake_evap > 0.0) || !(min_depth >= 0.0)) return fail(PGE_E_ARG, "window_lake_balance: lake_evap must be > 0, min_depth >= 0");
+    window_lake_balance_host(g->N + 2 * g->H, surface, active, precip, evap, lake_evap, min_depth, route, lake, counts);
+    return PGE_OK;
+}
+
 PGE_API int pge_basin_fill(const PgeGrid *g, const int32_t *owner, const float *surface, const uint8_t *ocean, double step,
                            double min_depth, double *add, uint8_t *basin, int64_t *basin_cells)
 {

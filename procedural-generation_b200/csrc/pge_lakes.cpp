@@ -434,4 +434,168 @@ void basin_fill_host(int N, int H, const int32_t *owner, const float *surface, c
     if (basin_cells) *basin_cells = nb;
 }
 
+// the lakes of a window balanced against evaporation (maps.py:675-736, erosion.window_lake_evap > 0) on a
+// W x W array: the flat flood (globe/hydro/priority_flood.py:193-270) from the inactive cells and the
+// array's border, the window's rain accumulated down the flood tree (globe/zoom/bake.py:323-330), each
+// depression (8-connected cells the flood fills more than 1e-6 above the surface, active) settled where
+// its inflow meets lake_evap x evap summed over the water at each level; returns the flags (deeper than
+// min_depth, active) and lowers the routing surface to the water on them
+void window_lake_balance_host(int W, const float *surface, const uint8_t *active, const float *precip, const float *evap,
+                              double lake_evap, double min_depth, double *route, uint8_t *lake, int64_t *counts)
+{
+    const int64_t M = (int64_t)W * W;
+    std::vector<uint8_t> drain(M);
+    for (int64_t c = 0; c < M; c++) {
+        const int i = (int)(c / W), j = (int)(c % W);
+        drain[c] = !active[c] || i == 0 || i == W - 1 || j == 0 || j == W - 1;
+    }
+    // the flat flood: the same FIFO + (level, push order) heap, neighbours inside the array
+    std::vector<float> filled(surface, surface + M);
+    std::vector<int64_t> parent(M, -1), pop_seq;
+    pop_seq.reserve(M);
+    std::vector<uint8_t> visited(M, 0);
+    std::priority_queue<HeapItem, std::vector<HeapItem>, HeapAfter> heap;
+    std::vector<int64_t> fifo;
+    int64_t seq = 0;
+    auto nbr = [&](int64_t c, int k, int64_t &n) {
+        const int i2 = (int)(c / W) + D8_DI[k], j2 = (int)(c % W) + D8_DJ[k];
+        if (i2 < 0 || i2 >= W || j2 < 0 || j2 >= W) return false;
+        n = (int64_t)i2 * W + j2;
+        return true;
+    };
+    for (int64_t c = 0; c < M; c++) {
+        if (!drain[c]) continue;
+        visited[c] = 1;
+        bool push = false;
+        for (int k = 0; k < 8 && !push; k++) {
+            int64_t n;
+            if (nbr(c, k, n)) push = !drain[n];
+        }
+        if (push) heap.push({(double)surface[c], seq++, c});
+    }
+    size_t head = 0;
+    while (head < fifo.size() || !heap.empty()) {
+        int64_t c;
+        if (head < fifo.size()) {
+            c = fifo[head++];
+            if (head == fifo.size()) {
+                fifo.clear();
+                head = 0;
+            }
+        } else {
+            c = heap.top().cell;
+            heap.pop();
+        }
+        const float lvl = filled[c];
+        pop_seq.push_back(c);
+        for (int k = 0; k < 8; k++) {
+            int64_t n;
+            if (!nbr(c, k, n) || visited[n]) continue;
+            visited[n] = 1;
+            parent[n] = c;
+            if (surface[n] <= lvl) {
+                filled[n] = lvl;
+                fifo.push_back(n);
+            } else {
+                filled[n] = surface[n];
+                heap.push({(double)surface[n], seq++, n});
+            }
+        }
+    }
+    // the rain accumulated down the flood tree, children before parents
+    std::vector<double> acc(M);
+    for (int64_t c = 0; c < M; c++) acc[c] = (double)precip[c];
+    for (size_t k = pop_seq.size(); k-- > 0;) {
+        const int64_t c = pop_seq[k], q = parent[c];
+        if (q >= 0) acc[q] += acc[c];
+    }
+    // depressions: 8-connected, labelled 1.. in raster order of their first cell
+    std::vector<int64_t> lab(M, 0), stack;
+    int64_t n = 0;
+    for (int64_t c = 0; c < M; c++) {
+        const bool dep = filled[c] > (float)(surface[c] + 1e-6f) && active[c];
+        lab[c] = dep ? -1 : 0;
+    }
+    for (int64_t s0 = 0; s0 < M; s0++) {
+        if (lab[s0] != -1) continue;
+        lab[s0] = ++n;
+        stack.push_back(s0);
+        while (!stack.empty()) {
+            const int64_t c = stack.back();
+            stack.pop_back();
+            for (int k = 0; k < 8; k++) {
+                int64_t q;
+                if (nbr(c, k, q) && lab[q] == -1) {
+                    lab[q] = n;
+                    stack.push_back(q);
+                }
+            }
+        }
+    }
+    int64_t nover = 0, nclosed = 0, ndry = 0;
+    std::vector<double> water(M);
+    for (int64_t c = 0; c < M; c++) water[c] = (double)surface[c];
+    if (n > 0) {
+        std::vector<int64_t> cells;
+        for (int64_t c = 0; c < M; c++)
+            if (lab[c] > 0) cells.push_back(c);
+        std::stable_sort(cells.begin(), cells.end(), [&](int64_t a, int64_t b) {
+            if (lab[a] != lab[b]) return lab[a] < lab[b];
+            return surface[a] < surface[b];
+        });
+        const int64_t K = (int64_t)cells.size();
+        std::vector<int64_t> ptr(n + 2, K);
+        for (int64_t t = K; t-- > 0;) ptr[lab[cells[t]]] = t;
+        ptr[0] = 0;
+        // the evaporative demand with the water at each cell's level, cumulated over every depression in turn
+        std::vector<double> demand(K), z(K);
+        double run_sum = 0.0;
+        for (int64_t t = 0; t < K; t++) {
+            const double e = (double)evap[cells[t]];
+            run_sum += lake_evap * (e > 0.0 ? e : 0.0);
+            demand[t] = run_sum;
+            z[t] = (double)surface[cells[t]];
+        }
+        std::vector<double> spill(n + 1, -INFINITY), inflow(n + 1, -INFINITY), level(n + 1, 0.0);
+        for (int64_t t = 0; t < K; t++) {
+            const int64_t c = cells[t], L = lab[c];
+            if ((double)filled[c] > spill[L]) spill[L] = (double)filled[c];
+            if (acc[c] > inflow[L]) inflow[L] = acc[c];
+        }
+        for (int64_t L = 1; L <= n; L++) {
+            const int64_t a = ptr[L], b = ptr[L + 1];
+            if (b <= a) continue;
+            const double need = inflow[L], before = a > 0 ? demand[a - 1] : 0.0;
+            if (need <= 0.0) {
+                level[L] = z[a] - 1.0;
+                ndry++;
+            } else if (demand[b - 1] - before <= need) {
+                level[L] = spill[L];  // cannot evaporate what arrives: still spills
+                nover++;
+            } else {
+                int64_t i = 0;
+                while (i < b - a && demand[a + i] - before < need) i++;  // the first level whose loss reaches the inflow
+                level[L] = z[a + (i < b - a - 1 ? i : b - a - 1)];
+                nclosed++;
+            }
+        }
+        for (int64_t c = 0; c < M; c++)
+            if (lab[c] > 0) water[c] = level[lab[c]];
+    }
+    int64_t nlake = 0;
+    for (int64_t c = 0; c < M; c++) {
+        const bool l = water[c] - (double)surface[c] > min_depth && active[c];
+        lake[c] = l ? 1 : 0;
+        nlake += l;
+        if (l && water[c] < route[c]) route[c] = water[c];
+    }
+    if (counts) {
+        counts[0] = n;
+        counts[1] = nover;
+        counts[2] = nclosed;
+        counts[3] = ndry;
+        counts[4] = nlake;
+    }
+}
+
 }  // namespace pge

@@ -24,6 +24,9 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
                       const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                       double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
                       PgeLakeInfo *info);
+// the evaporation balance of a window's lakes on the host (pge_lakes.cpp)
+void window_lake_balance_host(int W, const float *surface, const uint8_t *active, const float *precip, const float *evap,
+                              double lake_evap, double min_depth, double *route, uint8_t *lake, int64_t *counts);
 // the basin fill of a fresh state on the host (pge_lakes.cpp)
 void basin_fill_host(int N, int H, const int32_t *owner, const float *surface, const uint8_t *ocean, double step, double min_depth,
                      double *add, uint8_t *basin, int64_t *basin_cells);

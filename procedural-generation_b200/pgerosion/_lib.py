@@ -28,6 +28,7 @@ EXPORTS = (
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
     "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base", "pge_glacial",
     "pge_window_lakes", "pge_lake_balance", "pge_basin_fill",
+    "pge_window_lake_balance",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -134,6 +135,7 @@ def load(path: str | os.PathLike | None = None):
     L.pge_halo_adjoint.argtypes = [P(PgeHalo), c_vp, c_vp]
     L.pge_route_flood.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]
     L.pge_window_lakes.argtypes = [P(PgeGrid), P(PgeState), c_f64, c_vp, c_vp, c_vp]
+    L.pge_window_lake_balance.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_vp, c_vp, c_vp]
     L.pge_basin_fill.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_f64, c_f64, c_vp, c_vp, P(c_i64)]
     L.pge_lake_balance.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_f64, c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_f64, c_vp, c_vp, c_vp,
                                    P(PgeLakeInfo)]

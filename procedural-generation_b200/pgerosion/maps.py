@@ -287,20 +287,44 @@ class ErosionState:
         return int(n.value)
 
     def refresh_lakes_window(self, min_depth: float, lake_evap: float = 0.0) -> dict:
-        """The lakes of a window (maps.py:629-673, erosion.window_lakes): every
+        """The lakes of a window (maps.py:629-736, erosion.window_lakes): every
         depression the routing surface fills more than ``min_depth`` (cell
         units) deep is an overflowing lake, flagged on the interior's active
         cells; particles cross it without touching the bed, drop their load at
-        its shore and are not counted as climbing inside it.  Must run after
-        :meth:`refresh_route`.  The evaporation balance of ``lake_evap > 0``
-        (erosion.window_lake_evap) is not supported."""
-        if float(lake_evap) > 0.0:
-            raise ValueError("the b200 erosion backend has no window lake balance: erosion.window_lake_evap must be 0")
+        its shore and are not counted as climbing inside it.  With
+        ``lake_evap > 0`` (erosion.window_lake_evap) each depression settles
+        where the rain reaching it meets its evaporation instead
+        (``pge_window_lake_balance``, a host pass over the flat flood), and the
+        routing surface is lowered to the water on its lake cells.  Must run
+        after :meth:`refresh_route`."""
         if self.lake_flag is None or self.lake_flag.shape != self.height.shape:
             self.lake_flag = torch.zeros(self.height.shape, dtype=torch.uint8, device=self.height.device)
         if self.route is None:
             self.lake_flag.zero_()
             return {"lake_cells": 0}
+        if float(lake_evap) > 0.0:
+            if self.spherical or self.F != 1:
+                raise ValueError("the evaporation balance of window lakes runs on a window (F = 1)")
+            host = lambda t: np.ascontiguousarray(t.detach().cpu().numpy())
+            surf = host((self.height + self.sediment)[0].float())
+            active = host(self.mask[0] == MASK_ACTIVE) if self.mask is not None else np.ones(surf.shape, bool)
+            active = np.ascontiguousarray(active, np.uint8)
+            precip = host(self.precip[0])
+            evap = host(self.evap[0])
+            route = host(self.route[0]).copy()
+            lake = np.empty(surf.shape, np.uint8)
+            counts = np.zeros(5, np.int64)
+            check(_lib.load().pge_window_lake_balance(ctypes.byref(self.pge_grid()), surf.ctypes.data, active.ctypes.data,
+                                                      precip.ctypes.data, evap.ctypes.data, float(lake_evap), float(min_depth),
+                                                      route.ctypes.data, lake.ctypes.data, counts.ctypes.data),
+                  "pge_window_lake_balance")
+            dev = self.height.device
+            self.route[0] = torch.as_tensor(route, device=dev)
+            H, N = self.H, self.N
+            self.lake_flag.zero_()
+            self.lake_flag[0, H:H + N, H:H + N] = torch.as_tensor(lake[H:H + N, H:H + N], device=dev)
+            return {"lake_cells": int(lake[H:H + N, H:H + N].sum()), "depressions": int(counts[0]), "overflowing": int(counts[1]),
+                    "closed": int(counts[2]), "dry": int(counts[3])}
         n = torch.zeros(1, dtype=torch.int64, device=self.height.device)
         check(_lib.load().pge_window_lakes(ctypes.byref(self.pge_grid()), ctypes.byref(self.pge_state()), float(min_depth),
                                            _ptr(self.lake_flag), _ptr(n), _stream()), "pge_window_lakes")

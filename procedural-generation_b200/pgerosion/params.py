@@ -192,20 +192,18 @@ def plain_knobs() -> dict:
 
 
 def check_plain(ep) -> None:
-    """Raise ``ValueError`` when a knob asks for a process outside the plain
-    path (the lake parks of ``lake_fill``, the window lake balance, the ice
-    sheet).  The bank cut (``lateral_rate``), the basin fill, isostasy, the
-    routing surface (``flood_every``), the sea mask (``sea_mask_every``),
-    the glacial pass (``glacial_every``, the ice line of the evaporation
-    field), the planet's lake balance (``lake_balance`` with ``lake_fill``
-    off) and the lakes of a window (``window_lakes`` with
-    ``window_lake_evap = 0``) are supported."""
+    """Raise ``ValueError`` when a knob asks for a process this library does
+    not run: the lake parks of ``lake_fill`` and the ice sheet.  The bank
+    cut (``lateral_rate``), the basin fill, isostasy, the routing surface
+    (``flood_every``), the sea mask (``sea_mask_every``), the glacial pass
+    (``glacial_every``, the ice line of the evaporation field), the planet's
+    lake balance (``lake_balance`` with ``lake_fill`` off) and the lakes of
+    a window (``window_lakes``, balanced with ``window_lake_evap > 0``) are
+    supported."""
     bad = []
     if bool(getattr(ep, "lake_balance", False)) and bool(getattr(ep, "lake_fill", False)):
         bad.append("lake_fill")
     if bool(getattr(ep, "ice_sheet", False)):
         bad.append("ice_sheet")
-    if bool(getattr(ep, "window_lakes", False)) and float(getattr(ep, "window_lake_evap", 0.0)) > 0.0:
-        bad.append("window_lake_evap")
     if bad:
         raise ValueError("the b200 erosion backend runs the plain particle path only; switch off: " + ", ".join(bad))

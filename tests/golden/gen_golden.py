@@ -835,6 +835,37 @@ def gen_lateral(cs, maps, pk, WorldParams):
     print("step_lateral:", stats[-1])
 
 
+def gen_window_lake_balance(cs, maps, pk, WorldParams):
+    """A window's lakes settled against evaporation (ErosionState.
+    refresh_lakes_window with window_lake_evap > 0, maps.py:629-736) on the
+    window of the evolved N=48 world with a seeded rain field: the flags, the
+    lowered routing surface and the counts, for two evaporation rates."""
+    st, p, fw, w, mask = _window_of_evolved(cs, maps, pk, WorldParams)
+    NE, H, N = st.NE, st.H, st.N
+    unit = st.height_unit_m
+    rng = np.random.default_rng(107)
+    precip = (0.2 + rng.random((1, NE, NE))).astype(np.float32)
+    out = {}
+    for tag, le in (("a", 5.0), ("b", 60.0)):
+        ws = maps.ErosionState(height=w["height"].copy(), sediment=w["sediment"].copy(), discharge=w["discharge"].copy(),
+                               momentum=w["momentum"].copy(), hardness=w["hardness"], precip=precip, evap=w["evap"],
+                               uplift=np.zeros((1, NE, NE)), mask=mask, metric=w["metric"], metric_inv=w["metric_inv"], N=N, H=H,
+                               spherical=False, height_unit_m=unit, base=w["base"].copy(), deposit_on_exit=True)
+        eps = float(p.erosion.route_eps) / unit
+        depth = float(p.hydro.lake_min_depth) / unit
+        ws.refresh_route(eps)
+        route0 = ws.route.copy()
+        info = ws.refresh_lakes_window(depth, le)
+        out[f"{tag}_route0"] = route0
+        out[f"{tag}_route"] = ws.route.copy()
+        out[f"{tag}_flag"] = ws.lake_flag.copy()
+        out[f"{tag}_info"] = json.dumps(info)
+        out[f"{tag}_lake_evap"] = le
+        print("window_lake_balance", tag, le, info)
+    np.savez_compressed(HERE / "window_lake_balance.npz", N=N, H=H, cell_size_m=unit, height=w["height"], sediment=w["sediment"],
+                        mask=mask, precip=precip, evap=w["evap"], min_depth=float(p.hydro.lake_min_depth) / unit, **out)
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -849,7 +880,8 @@ def main(bake: str, only: str | None = None):
             "basin_fill": lambda: gen_basin_fill(cs, maps, pk, WorldParams),
             "roots_trace": lambda: gen_roots_trace(cs, maps, pk, WorldParams),
             "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams),
-            "lateral": lambda: gen_lateral(cs, maps, pk, WorldParams)}
+            "lateral": lambda: gen_lateral(cs, maps, pk, WorldParams),
+            "window_lake_balance": lambda: gen_window_lake_balance(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

@@ -297,3 +297,32 @@ def test_basin_fill_equals_the_reference(cuda):
     # off, or on a window: nothing
     ep0 = type(ep)(**{**{k: getattr(ep, k) for k in ep.__dataclass_fields__}, "basin_fill_grade": 0.0})
     assert gm.fill_basins(g, WorldParams(world=params.world, erosion=ep0)) is None
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_window_lake_balance_on_the_state_equals_the_reference(cuda, tag):
+    """ErosionState.refresh_lakes_window with window_lake_evap > 0 on the
+    device window state (the routing flood on the device, the balance on the
+    host, flags and the lowered route back): the reference's flags, route
+    and counts, bit for bit."""
+    fx = np.load(GOLDEN / "window_lake_balance.npz")
+    N, H = int(fx["N"]), int(fx["H"])
+    NE = N + 2 * H
+    dev = torch.device("cuda")
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=dev)
+    from pgerosion.geometry import get_grid
+
+    grid = get_grid(N, H, float(fx["cell_size_m"]))
+    g = gm.ErosionState(height=f64(fx["height"]), sediment=f64(fx["sediment"]), discharge=f64(np.zeros((1, NE, NE))),
+                        momentum=f64(np.zeros((1, NE, NE, 2))), hardness=f32(np.full((1, NE, NE), 0.5)), precip=f32(fx["precip"]),
+                        evap=f32(fx["evap"]), uplift=f64(np.zeros((1, NE, NE))),
+                        mask=torch.as_tensor(np.ascontiguousarray(fx["mask"], np.uint8), device=dev),
+                        metric=f32(grid.metric_face), metric_inv=f32(grid.metric_inv_face), N=N, H=H, spherical=False,
+                        height_unit_m=float(fx["cell_size_m"]), deposit_on_exit=True)
+    g.route = f64(fx[f"{tag}_route0"])
+    info = g.refresh_lakes_window(float(fx["min_depth"]), float(fx[f"{tag}_lake_evap"]))
+    want = json.loads(str(fx[f"{tag}_info"]))
+    assert info == want, (info, want)
+    assert np.array_equal(g.lake_flag.cpu().numpy(), fx[f"{tag}_flag"])
+    assert g.route.cpu().numpy().tobytes() == np.ascontiguousarray(fx[f"{tag}_route"]).tobytes()

@@ -117,3 +117,36 @@ def test_basin_fill_equals_the_reference():
     sed = np.array(fx["s_start"])
     sed[inter] += add
     assert sed[inter].tobytes() == np.ascontiguousarray(fx["sediment"][inter]).tobytes()
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_window_lake_balance_equals_the_reference(tag):
+    """``pge_window_lake_balance`` (ErosionState._balance_window_lakes,
+    maps.py:675-736, on the host) on the reference fixture's window after
+    its routing flood: the reference's lake flags, lowered routing surface
+    and counts, bit for bit, at two evaporation rates (overflowing and closed
+    lakes)."""
+    fx = np.load(GOLDEN / "window_lake_balance.npz")
+    N, H = int(fx["N"]), int(fx["H"])
+    NE = N + 2 * H
+    surf = np.ascontiguousarray((fx["height"] + fx["sediment"])[0], np.float32)
+    active = np.ascontiguousarray(fx["mask"][0] == 1, np.uint8)
+    precip = np.ascontiguousarray(fx["precip"][0], np.float32)
+    evap = np.ascontiguousarray(fx["evap"][0], np.float32)
+    route = np.ascontiguousarray(fx[f"{tag}_route0"][0], np.float64).copy()
+    lake = np.empty((NE, NE), np.uint8)
+    counts = np.zeros(5, np.int64)
+    g = _lib.PgeGrid(F=1, N=N, H=H, spherical=0, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    _lib.check(_lib.load().pge_window_lake_balance(ctypes.byref(g), surf.ctypes.data, active.ctypes.data, precip.ctypes.data,
+                                                   evap.ctypes.data, float(fx[f"{tag}_lake_evap"]), float(fx["min_depth"]),
+                                                   route.ctypes.data, lake.ctypes.data, counts.ctypes.data),
+               "pge_window_lake_balance")
+    info = json.loads(str(fx[f"{tag}_info"]))
+    assert {"depressions": int(counts[0]), "overflowing": int(counts[1]), "closed": int(counts[2]), "dry": int(counts[3])} == \
+        {k: info[k] for k in ("depressions", "overflowing", "closed", "dry")}
+    flag = np.zeros((NE, NE), np.uint8)
+    flag[H:H + N, H:H + N] = lake[H:H + N, H:H + N]
+    assert np.array_equal(flag, fx[f"{tag}_flag"][0])
+    assert int(flag.sum()) == info["lake_cells"]
+    assert route.tobytes() == np.ascontiguousarray(fx[f"{tag}_route"][0]).tobytes()
+    assert info["closed"] > 0
