@@ -34,7 +34,6 @@ namespace {
 
 constexpr int D8_DI[8] = {1, 1, 0, -1, -1, -1, 0, 1};
 constexpr int D8_DJ[8] = {0, 1, 1, 1, 0, -1, -1, -1};
-constexpr uint8_t FD_OCEAN = 255;
 
 // cell ids are interior flat indices (f * N + i) * N + j; `owner` maps an extended cell to the
 // extended flat index of the interior cell that owns it
