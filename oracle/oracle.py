@@ -738,7 +738,286 @@ def refresh_base(state, min_fraction) -> dict:
     flat[hm.dst] = flat[hm.nearest]
     state.base = base
     state.base_at = state.iteration
+    state.sea = None if labels is None else (below & keep[np.maximum(labels, 0)]).reshape(surf.shape)
     return info
+
+
+# --------------------------------------------------------------------------
+# the planet's lake refresh (maps.py:422-479 with erosion.lake_fill off), restated
+# --------------------------------------------------------------------------
+_D8_DI = np.array([1, 1, 0, -1, -1, -1, 0, 1])
+_D8_DJ = np.array([0, 1, 1, 1, 0, -1, -1, -1])
+
+
+def _cell_neighbors(grid) -> np.ndarray:
+    """(M, 8) cell ids of every interior cell's D8 neighbours through the
+    owner table (hydro/d8.py:70-77)."""
+    N, H, NE = grid.N, grid.H, grid.NE
+    f, i, j = np.meshgrid(np.arange(6), np.arange(N), np.arange(N), indexing="ij")
+    out = np.empty((6 * N * N, 8), np.int64)
+    for k in range(8):
+        o = grid.owner[f, i + H + _D8_DI[k], j + H + _D8_DJ[k]].reshape(-1).astype(np.int64)
+        f2, r = o // (NE * NE), o % (NE * NE)
+        out[:, k] = (f2 * N + r // NE - H) * N + r % NE - H
+    return out
+
+
+def hydro_flood(surf32, ocean, nbr, N):
+    """hydro/priority_flood.py:127-191, 294-318: the whole-sphere priority
+    flood from the ocean drains (the lowest cell when there is none), a FIFO
+    for cells at or below the current level and a (level, push order) heap
+    for the rest; returns (filled float32, parent, order, pop_seq)."""
+    import heapq
+
+    M = surf32.size
+    drain = np.asarray(ocean, bool).reshape(-1).copy()
+    if not drain.any():
+        drain[int(np.argmin(surf32))] = True
+    filled = surf32.copy()
+    visited = np.zeros(M, bool)
+    parent = np.full(M, -1, np.int64)
+    order = np.full(M, -1, np.int64)
+    pop_seq = []
+    heap, fifo, seq = [], [], 0
+    for c in range(M):
+        if drain[c]:
+            visited[c] = True
+            if (~drain[nbr[c]]).any():
+                heapq.heappush(heap, (float(surf32[c]), seq, c))
+                seq += 1
+    head = 0
+    NN = N * N
+    while head < len(fifo) or heap:
+        if head < len(fifo):
+            c = fifo[head]
+            head += 1
+        else:
+            c = heapq.heappop(heap)[2]
+        lvl = filled[c]
+        order[c] = len(pop_seq)
+        pop_seq.append(c)
+        for n in nbr[c]:
+            if visited[n]:
+                continue
+            if n // NN != c // NN and c not in nbr[n]:
+                continue  # a one-sided link across a face edge
+            visited[n] = True
+            parent[n] = c
+            if surf32[n] <= lvl:
+                filled[n] = lvl
+                fifo.append(n)
+            else:
+                filled[n] = surf32[n]
+                heapq.heappush(heap, (float(surf32[n]), seq, n))
+                seq += 1
+    return filled, parent, order, np.array(pop_seq, np.int64)
+
+
+def flow_down(filled, ocean, parent, nbr, metric_face, N, H):
+    """hydro/routing.py:28-90 + d8.py:123-136: each land cell's downstream
+    cell, by the steepest physical descent on the filled surface (the float32
+    height difference over the float64 step length), flats to their flood
+    parent."""
+    M = filled.size
+    down = np.full(M, -1, np.int64)
+    oc = np.asarray(ocean, bool).reshape(-1)
+    for c in range(M):
+        if oc[c]:
+            continue
+        i, j = (c % (N * N)) // N, c % N
+        g = metric_face[i + H, j + H]
+        best, best_s = -1, 0.0
+        for k in range(8):
+            hn = filled[nbr[c, k]]
+            if hn < filled[c]:
+                di, dj = float(_D8_DI[k]), float(_D8_DJ[k])
+                d2 = float(g[0]) * di * di + 2.0 * float(g[1]) * di * dj + float(g[2]) * dj * dj
+                sl = float(np.float32(filled[c] - hn)) / math.sqrt(d2)
+                if sl > best_s:
+                    best, best_s = k, sl
+        if best < 0 and parent[c] >= 0:
+            hit = np.flatnonzero(nbr[c] == parent[c])
+            best = int(hit[0]) if hit.size else -1
+        if best < 0:
+            raise RuntimeError("a land cell has no D8 direction")
+        down[c] = nbr[c, best]
+    return down
+
+
+def _label_level(mask, level, nbr):
+    """hydro/lakes.py:18-46: 8-connected components joining only cells of
+    one level, numbered by their lowest cell id."""
+    M = mask.size
+    lab = np.full(M, -1, np.int64)
+    n = 0
+    for s0 in range(M):
+        if not mask[s0] or lab[s0] >= 0:
+            continue
+        lab[s0] = n
+        stack = [s0]
+        while stack:
+            c = stack.pop()
+            for q in nbr[c]:
+                if mask[q] and lab[q] < 0 and level[q] == level[c]:
+                    lab[q] = n
+                    stack.append(q)
+        n += 1
+    return lab, n
+
+
+def balance_lakes(surf32, filled, ocean, order, down, topo, precip, pet, area, cell_size_m, nbr, lake_evap, land_evap):
+    """hydro/balance.py:63-108, 159-284: every depression lowered to the level
+    where its inflow meets its evaporation, in one upstream-first pass;
+    returns (water float32 (M,), info)."""
+    M = surf32.size
+    oc = np.asarray(ocean, bool).reshape(-1)
+    w = np.asarray(precip, np.float64).reshape(-1)
+    dep = (filled > surf32) & ~oc
+    info = {"depressions": 0, "overflowing": 0, "closed": 0, "dry": 0}
+    if (float(lake_evap) <= 0.0 and float(land_evap) <= 0.0) or not dep.any():
+        return filled.copy(), info
+    lab, n = _label_level(dep, filled, nbr)
+    cells = np.flatnonzero(lab >= 0)
+    cells = cells[np.lexsort((surf32[cells], lab[cells]))]
+    lab_s = lab[cells]
+    ptr = np.searchsorted(lab_s, np.arange(n + 1))
+    z = surf32[cells].astype(np.float64)
+    af = np.asarray(area, np.float64).reshape(-1) / (float(cell_size_m) ** 2)
+    ev = np.asarray(pet, np.float64).reshape(-1)
+    wr = w
+    k_lake = float(lake_evap)
+    if float(land_evap) > 0.0:
+        rain = w / af
+        pe = float(land_evap) * ev
+        a = np.maximum(pe / np.maximum(rain, 1e-9), 1e-9)
+        et = rain * np.sqrt(a * np.tanh(1.0 / a) * (1.0 - np.exp(-a)))
+        wr = (rain - et) * af
+        per = (pe[cells] - et[cells]) * af[cells]
+        k_lake = 1.0
+    else:
+        per = ev[cells] * af[cells]
+    csum = np.cumsum(per)
+    before = np.zeros(n)
+    before[1:] = csum[ptr[1:n] - 1]
+    cum = csum - before[lab_s]
+    ordv = order[cells]
+    best = np.full(n, np.iinfo(np.int64).max)
+    np.minimum.at(best, lab_s, ordv)
+    sel = ordv == best[lab_s]
+    outlet = np.zeros(n, np.int64)
+    outlet[lab_s[sel]] = cells[sel]
+    outlet_lake = np.full(M, -1, np.int64)
+    outlet_lake[outlet] = np.arange(n)
+    spill = filled[outlet].astype(np.float64)
+    level = np.zeros(n)
+    outflow = np.zeros(n)
+    acc = w.copy()
+    run = wr.copy()
+    for c in topo:
+        L = outlet_lake[c]
+        if L >= 0:
+            inflow = run[c]
+            lo, hi = ptr[L], ptr[L + 1]
+            if inflow <= 0.0:
+                level[L], outflow[L] = z[lo], 0.0
+            else:
+                i = int(np.searchsorted(cum[lo:hi], inflow / k_lake))
+                if i >= hi - lo:
+                    level[L], outflow[L] = spill[L], inflow - k_lake * cum[hi - 1]
+                else:
+                    level[L], outflow[L] = z[lo + i], 0.0
+            if float(land_evap) > 0.0:
+                acc[c] = acc[c] * (outflow[L] / inflow) if inflow > 0.0 else 0.0
+            else:
+                acc[c] = outflow[L]
+            run[c] = outflow[L]
+        d = down[c]
+        if d >= 0:
+            acc[d] += acc[c]
+            run[d] += run[c]
+    water = surf32.copy()
+    np.maximum.at(water, cells, level[lab_s].astype(np.float32))
+    water[oc] = filled[oc]
+    closed = outflow <= 0.0
+    wet = level > z[ptr[:n]]
+    info.update(depressions=int(n), overflowing=int((~closed).sum()), closed=int((closed & wet).sum()),
+                dry=int((closed & ~wet).sum()))
+    return water, info
+
+
+def fill_basins(state, params) -> dict | None:
+    """maps.py:1216-1229, 1278-1326: sediment into the closed basins of a
+    fresh state, up to the flood's surface graded ``basin_fill_grade`` (m per
+    km) up from each basin's outlet along the flood tree, where the flood
+    leaves more than ``basin_fill_min_m`` off the open ocean."""
+    ep = _ep(params)
+    grade = float(getattr(ep, "basin_fill_grade", 0.0))
+    if grade <= 0.0 or not state.spherical or not hasattr(params, "world"):
+        return None
+    grid = state.grid
+    N = grid.N
+    inter = state.interior
+    surf = np.ascontiguousarray((state.height + state.sediment)[inter], np.float32)
+    below, labels, keep = below_sea_components(surf, grid, OCEAN_MIN_FRACTION)
+    ocean = np.zeros(surf.size, bool) if labels is None else (below & keep[np.maximum(labels, 0)]).reshape(-1)
+    if getattr(state, "_nbr", None) is None:
+        state._nbr = _cell_neighbors(grid)
+    s32 = surf.reshape(-1)
+    filled, parent, order, pop_seq = hydro_flood(s32, ocean, state._nbr, N)
+    step = grade * (float(grid.cell_size_m) / 1000.0) / state.height_unit_m
+    g = s32.astype(np.float64)
+    for c in pop_seq:
+        q = parent[c]
+        if q >= 0 and g[q] + step > g[c]:
+            g[c] = g[q] + step
+    basin = ((filled - s32) > np.float32(float(ep.basin_fill_min_m) / state.height_unit_m)) & ~ocean
+    add = np.where(basin, np.maximum(g - s32, 0.0), 0.0)
+    sed = state.sediment[inter].reshape(-1) + add
+    state.sediment[inter] = sed.reshape(surf.shape)
+    state.exchange_halos()
+    return {"basin_cells": int(basin.sum())}
+
+
+def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0) -> dict:
+    """maps.py:422-479 (erosion.lake_fill off): the planet's lakes on the
+    current surface -- overflowing lakes deeper than ``min_depth`` flagged,
+    a lake drawn below its rim a closed sea at its level in ``base``; flags
+    and base halos copied from their nearest interior cell."""
+    grid = state.grid
+    N, H = grid.N, grid.H
+    inter = state.interior
+    surf = np.ascontiguousarray((state.height + state.sediment)[inter], np.float32)
+    sea = getattr(state, "sea", None)
+    if sea is None:
+        below, labels, keep = below_sea_components(surf, grid, float(min_fraction))
+        sea = np.zeros(surf.shape, bool) if labels is None else (below & keep[np.maximum(labels, 0)]).reshape(surf.shape)
+    ocean = np.asarray(sea, bool).reshape(-1)
+    if getattr(state, "_nbr", None) is None:
+        state._nbr = _cell_neighbors(grid)
+    nbr = state._nbr
+    s32 = surf.reshape(-1)
+    filled, parent, order, pop_seq = hydro_flood(s32, ocean, nbr, N)
+    down = flow_down(filled, ocean, parent, nbr, grid.metric_face, N, H)
+    topo = pop_seq[::-1]
+    topo = topo[~ocean[topo]]
+    pet = getattr(state, "lake_pet", None)
+    pet = (state.evap if pet is None else pet)[inter]
+    water, bal = balance_lakes(s32, filled, ocean, order, down, topo, state.precip[inter], pet, interior_cell_area(grid),
+                               grid.cell_size_m, nbr, lake_evap, land_evap)
+    lake = ((water - s32) > np.float32(min_depth)) & ~ocean
+    closed = lake & (water < filled - np.float32(1e-4))
+    flag = np.zeros(state.height.shape, np.uint8)
+    flag[inter] = (lake & ~closed).reshape(surf.shape)
+    if closed.any():
+        b = state.base[inter].reshape(-1).copy()
+        b[closed] = water[closed]
+        state.base[inter] = b.reshape(surf.shape)
+    hm = grid.halo
+    for arr in (flag, state.base):
+        flat = arr.reshape(-1, 1)
+        flat[hm.dst] = flat[hm.nearest]
+    state.lake_flag = flag
+    return {"lake_cells": int(lake.sum()), "lake_cells_closed": int((closed & lake).sum()), **bal}
 
 
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
@@ -750,7 +1029,13 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     if int(getattr(ep, "flood_every", 0)) > 0 and (state.route is None or state.iteration % int(ep.flood_every) == 0):
         refresh_route(state, _cu(ep, "route_eps", state.height_unit_m))  # maps.py:1553-1554
     st_lake = None
-    if not state.spherical and bool(getattr(ep, "window_lakes", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
+    if state.spherical and bool(getattr(ep, "lake_balance", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
+            (getattr(state, "lake_flag", None) is None or state.iteration % int(ep.flood_every) == 0):
+        hydro = getattr(params, "hydro", None)
+        depth_m = float(getattr(hydro, "lake_min_depth", LAKE_MIN_DEPTH_M)) if hydro is not None else LAKE_MIN_DEPTH_M
+        st_lake = refresh_lakes(state, float(getattr(hydro, "lake_evap", 6.0)), depth_m / state.height_unit_m,
+                                OCEAN_MIN_FRACTION, float(getattr(hydro, "land_evap", 3.0)))  # maps.py:1555-1562
+    elif not state.spherical and bool(getattr(ep, "window_lakes", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
             (state.lake_flag is None or state.iteration % int(ep.flood_every) == 0):
         hydro = getattr(params, "hydro", None)
         depth_m = float(getattr(hydro, "lake_min_depth", LAKE_MIN_DEPTH_M)) if hydro is not None else LAKE_MIN_DEPTH_M

@@ -383,3 +383,74 @@ def test_bank_cut_steps_match_reference_bit_exact():
         assert s["datum_shift"] == r["datum_shift"]
     for k in ("height", "sediment", "discharge", "momentum", "pending"):
         assert np.array_equal(getattr(st, k), t[k]), k
+
+
+def test_planet_lake_refresh_and_steps_match_reference_bit_exact():
+    """The oracle's restatement of the planet's lake refresh (maps.py:422-479
+    with lake_fill off: the hydro flood, D8, the evaporation balance) on the
+    reference fixture's surface, for both balance branches, and full steps
+    with lake_balance, the sea mask and the routing flood every 2
+    iterations: flags, base level and state equal the reference's bit for
+    bit."""
+    import json as _json
+
+    from pgerosion.params import WorldGroup, WorldParams
+    from tests.parity_cases import erosion_params
+
+    fx = np.load(GOLDEN / "lake_balance.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    ep = erosion_params(str(fx["params"]))
+    params = WorldParams(world=WorldGroup(seed=int(fx["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(fx["land_fraction"]),
+                                          halo=H), erosion=ep)
+    from pgerosion.synth import World
+    from pgerosion.geometry import get_grid
+
+    world = World(get_grid(N, H, cs), fx["bedrock"], fx["hardness"], fx["precip"], fx["evap"], fx["uplift"],
+                  float(fx["land_fraction"]))
+    for tag, le in (("budyko", 3.0), ("plain", 0.0)):
+        st = orc.OracleState.from_world(world, params)
+        st.height[...] = fx["u_height"]
+        st.sediment[...] = fx["u_sediment"]
+        orc.refresh_base(st, float(fx["ocean_min_fraction"]))
+        assert np.array_equal(st.sea.reshape(-1), fx["u_sea"].reshape(-1))
+        info = orc.refresh_lakes(st, float(fx["lake_evap"]), float(fx["min_depth"]), float(fx["ocean_min_fraction"]), le)
+        want = _json.loads(str(fx[f"{tag}_info"]))
+        assert info == {k: want[k] for k in info}, (info, want)
+        assert np.array_equal(st.lake_flag, fx[f"{tag}_flag"])
+        assert st.base.tobytes() == np.ascontiguousarray(fx[f"{tag}_base"]).tobytes()
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    assert np.array_equal(st.height, fx["h_start"])
+    stats = _json.loads(str(fx["stats"]))
+    for it in range(int(fx["iterations"])):
+        s = orc.step(st, params, it, n_particles=int(fx["n_particles"]))
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == stats[it][k], (it, k)
+        if "lakes" in stats[it]:
+            assert s["lakes"] == {k: stats[it]["lakes"][k] for k in s["lakes"]}, it
+    for k in ("height", "sediment", "discharge", "momentum", "pending", "base", "lake_flag"):
+        assert np.array_equal(getattr(st, k), fx[k]), k
+
+
+def test_basin_fill_matches_reference_bit_exact():
+    """The oracle's fill_basins (maps.py:1278-1326) on the reference's fresh
+    world after start_replay: the reference's sediment bit for bit."""
+    import json as _json
+
+    from pgerosion.geometry import get_grid
+    from pgerosion.params import WorldGroup, WorldParams
+    from pgerosion.synth import World
+    from tests.parity_cases import erosion_params
+
+    fx = np.load(GOLDEN / "basin_fill.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    params = WorldParams(world=WorldGroup(seed=int(fx["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(fx["land_fraction"]),
+                                          halo=H), erosion=erosion_params(str(fx["params"])))
+    world = World(get_grid(N, H, cs), fx["bedrock"], fx["hardness"], fx["precip"], fx["evap"], fx["uplift"],
+                  float(fx["land_fraction"]))
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    assert np.array_equal(st.height, fx["h_start"]) and np.array_equal(st.sediment, fx["s_start"])
+    info = orc.fill_basins(st, params)
+    assert info["basin_cells"] == _json.loads(str(fx["info"]))["basin_cells"]
+    assert np.array_equal(st.sediment, fx["sediment"])
