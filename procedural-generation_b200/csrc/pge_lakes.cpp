@@ -24,7 +24,6 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
-#include <queue>
 #include <vector>
 
 #include "../../include/pgerosion.h"
@@ -76,12 +75,73 @@ struct Sphere {
     }
 };
 
-struct HeapItem {
-    double key;
-    int64_t seq, cell;
-};
-struct HeapAfter {
-    bool operator()(const HeapItem &a, const HeapItem &b) const { return a.key > b.key || (a.key == b.key && a.seq > b.seq); }
+// The flood's heap orders cells by (level, push order).  Levels are float32 surfaces and fewer than 2^32 cells
+// are ever pushed, so the pair packs into one unsigned 64-bit key: the level's bits mapped to an order-preserving
+// unsigned integer (negative zero taken as zero, so equal levels tie as the float compare has them) over the push
+// count.  A 4-ary min-heap of (key, cell) pops exactly the sequence a (level, push order) heap does.
+inline uint64_t level_key(float level, int64_t seq)
+{
+    if (level == 0.0f) level = 0.0f;
+    uint32_t u;
+    std::memcpy(&u, &level, 4);
+    u = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return ((uint64_t)u << 32) | (uint64_t)(uint32_t)seq;
+}
+
+class LevelHeap {
+  public:
+    bool empty() const { return k_.empty(); }
+    void push(uint64_t key, int64_t cell)
+    {
+        k_.push_back(key);
+        c_.push_back(cell);
+        size_t i = k_.size() - 1;
+        while (i > 0) {
+            const size_t p = (i - 1) >> 2;
+            if (k_[p] <= key) break;
+            k_[i] = k_[p];
+            c_[i] = c_[p];
+            i = p;
+        }
+        k_[i] = key;
+        c_[i] = cell;
+    }
+    int64_t pop()
+    {
+        const int64_t top = c_[0];
+        const uint64_t key = k_.back();
+        const int64_t cell = c_.back();
+        k_.pop_back();
+        c_.pop_back();
+        const size_t n = k_.size();
+        if (n > 0) {
+            size_t i = 0;
+            while (true) {
+                const size_t first = 4 * i + 1;
+                if (first >= n) break;
+                size_t m = first;
+                const size_t last = first + 4 < n ? first + 4 : n;
+                for (size_t j = first + 1; j < last; j++)
+                    if (k_[j] < k_[m]) m = j;
+                if (k_[m] >= key) break;
+                k_[i] = k_[m];
+                c_[i] = c_[m];
+                i = m;
+            }
+            k_[i] = key;
+            c_[i] = cell;
+        }
+        return top;
+    }
+    void reserve(size_t n)
+    {
+        k_.reserve(n);
+        c_.reserve(n);
+    }
+
+  private:
+    std::vector<uint64_t> k_;
+    std::vector<int64_t> c_;
 };
 
 // priority flood: the filled surface, each cell's flood parent and the pop sequence; drains are
@@ -104,7 +164,8 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
     pop_seq.clear();
     pop_seq.reserve(M);
     std::vector<uint8_t> visited(M, 0);
-    std::priority_queue<HeapItem, std::vector<HeapItem>, HeapAfter> heap;
+    LevelHeap heap;
+    heap.reserve(1 << 16);
     std::vector<int64_t> fifo;
     fifo.reserve(1024);
     int64_t seq = 0;
@@ -115,7 +176,7 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
         S.neighbors(c, nb);
         bool push = false;
         for (int k = 0; k < 8 && !push; k++) push = !drain[nb[k]];
-        if (push) heap.push({(double)surface[c], seq++, c});
+        if (push) heap.push(level_key(surface[c], seq++), c);
     }
     size_t head = 0;
     const int64_t NN = (int64_t)S.N * S.N;
@@ -128,8 +189,7 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
                 head = 0;
             }
         } else {
-            c = heap.top().cell;
-            heap.pop();
+            c = heap.pop();
         }
         const float lvl = filled[c];
         order[c] = (int64_t)pop_seq.size();
@@ -149,7 +209,7 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
                 fifo.push_back(n);
             } else {
                 filled[n] = surface[n];
-                heap.push({(double)surface[n], seq++, n});
+                heap.push(level_key(surface[n], seq++), n);
             }
         }
     }
@@ -453,7 +513,7 @@ void window_lake_balance_host(int W, const float *surface, const uint8_t *active
     std::vector<int64_t> parent(M, -1), pop_seq;
     pop_seq.reserve(M);
     std::vector<uint8_t> visited(M, 0);
-    std::priority_queue<HeapItem, std::vector<HeapItem>, HeapAfter> heap;
+    LevelHeap heap;
     std::vector<int64_t> fifo;
     int64_t seq = 0;
     auto nbr = [&](int64_t c, int k, int64_t &n) {
@@ -470,7 +530,7 @@ void window_lake_balance_host(int W, const float *surface, const uint8_t *active
             int64_t n;
             if (nbr(c, k, n)) push = !drain[n];
         }
-        if (push) heap.push({(double)surface[c], seq++, c});
+        if (push) heap.push(level_key(surface[c], seq++), c);
     }
     size_t head = 0;
     while (head < fifo.size() || !heap.empty()) {
@@ -482,8 +542,7 @@ void window_lake_balance_host(int W, const float *surface, const uint8_t *active
                 head = 0;
             }
         } else {
-            c = heap.top().cell;
-            heap.pop();
+            c = heap.pop();
         }
         const float lvl = filled[c];
         pop_seq.push_back(c);
@@ -497,7 +556,7 @@ void window_lake_balance_host(int W, const float *surface, const uint8_t *active
                 fifo.push_back(n);
             } else {
                 filled[n] = surface[n];
-                heap.push({(double)surface[n], seq++, n});
+                heap.push(level_key(surface[n], seq++), n);
             }
         }
     }
