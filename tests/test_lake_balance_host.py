@@ -150,3 +150,110 @@ def test_window_lake_balance_equals_the_reference(tag):
     assert int(flag.sum()) == info["lake_cells"]
     assert route.tobytes() == np.ascontiguousarray(fx[f"{tag}_route"][0]).tobytes()
     assert info["closed"] > 0
+
+
+def _oracle_lakes(surf, ocean, precip, pet, grid, lake_evap, land_evap, min_depth):
+    """The oracle's restatement of the planet lake refresh (pinned to the
+    reference above) on raw interior arrays: flags, water, closed levels."""
+    from oracle import oracle as orc
+
+    N, H = grid.N, grid.H
+    nbr = orc._cell_neighbors(grid)
+    s32 = surf.reshape(-1)
+    oc = ocean.reshape(-1).astype(bool)
+    filled, parent, order, pop_seq = orc.hydro_flood(s32, oc, nbr, N)
+    down = orc.flow_down(filled, oc, parent, nbr, grid.metric_face, N, H)
+    topo = pop_seq[::-1]
+    topo = topo[~oc[topo]]
+    water, bal = orc.balance_lakes(s32, filled, oc, order, down, topo, precip, pet, orc.interior_cell_area(grid), grid.cell_size_m,
+                                   nbr, lake_evap, land_evap)
+    lake = ((water - s32) > np.float32(min_depth)) & ~oc
+    closed = lake & (water < filled - np.float32(1e-4))
+    return (lake & ~closed).astype(np.uint8), water, closed, bal
+
+
+@pytest.mark.parametrize("case", ["noise", "no_ocean", "plateau", "all_ocean_but_one"])
+@pytest.mark.parametrize("land_evap", [0.0, 3.0])
+def test_lake_balance_equals_the_oracle_on_edge_cases(case, land_evap):
+    """Seeded small worlds the fixtures do not cover -- rough noise with a
+    sea, no ocean at all (an error, as in the reference), a flat plateau with
+    pits (flats drain to their flood parent), a world that is ocean but for
+    one cell -- checked against the oracle's restatement of the reference."""
+    N, H, cs = 12, 2, 1000.0
+    grid = get_grid(N, H, cs)
+    rng = np.random.default_rng(hash((case, land_evap)) % 2**32)
+    if case == "noise":
+        surf = rng.normal(0.5, 1.0, (6, N, N)).astype(np.float32)
+    elif case == "no_ocean":
+        surf = (2.0 + rng.random((6, N, N))).astype(np.float32)
+    elif case == "plateau":
+        surf = np.full((6, N, N), 3.0, np.float32)
+        surf[:, 3:5, 3:5] = 2.0
+        surf[0, :2, :] = -1.0
+    else:
+        surf = np.full((6, N, N), -5.0, np.float32)
+        surf[2, 6, 6] = 1.0
+    ocean = np.zeros((6, N, N), np.uint8)
+    if case != "no_ocean":
+        from oracle import oracle as orc
+
+        below, labels, keep = orc.below_sea_components(surf, grid, 0.02)[:3]
+        if labels is not None:
+            ocean = np.ascontiguousarray((below & keep[np.maximum(labels, 0)]).reshape(surf.shape), np.uint8)
+    precip = (0.2 + rng.random((6, N, N))).astype(np.float32)
+    pet = rng.random((6, N, N)).astype(np.float32)
+    sq = sqrt_det_metric(grid)[H:H + N, H:H + N]
+    area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * cs ** 2).astype(np.float32), (6, N, N)))
+    d = dict(fx={"lake_evap": np.float64(2.0), "min_depth": np.float64(1e-3)}, N=N, H=H, cs=cs, surf=np.ascontiguousarray(surf),
+             ocean=ocean, precip=precip, pet=pet, area=area, owner=np.ascontiguousarray(grid.owner, np.int32),
+             metric=np.ascontiguousarray(grid.metric_face, np.float32))
+    if case == "no_ocean":
+        # the flood drains the lowest cell, but D8 holds it to be land with nowhere to go: the reference's
+        # flow_directions raises (hydro/routing.py:86-89), and so do the oracle and the library
+        with pytest.raises(RuntimeError):
+            _oracle_lakes(surf, ocean, precip, pet, grid, 2.0, land_evap, 1e-3)
+        with pytest.raises(_lib.PgeError, match="no flow direction"):
+            _balance(d, land_evap)
+        return
+    flag, water, level, info = _balance(d, land_evap)
+    want_flag, want_water, closed, bal = _oracle_lakes(surf, ocean, precip, pet, grid, 2.0, land_evap, 1e-3)
+    assert np.array_equal(flag.reshape(-1), want_flag)
+    assert water.reshape(-1).tobytes() == want_water.tobytes()
+    assert np.array_equal(~np.isnan(level.reshape(-1)), closed)
+    assert {k: int(getattr(info, k)) for k in bal} == bal
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_basin_fill_equals_the_oracle_on_noise_worlds(seed):
+    """``pge_basin_fill`` against the oracle's restatement (pinned to the
+    reference above) on seeded rough worlds with a sea and many closed
+    basins, at a steep grade so the plain's slope shows."""
+    from oracle import oracle as orc
+
+    N, H, cs = 12, 2, 1000.0
+    grid = get_grid(N, H, cs)
+    rng = np.random.default_rng(seed)
+    surf = rng.normal(0.3, 1.0, (6, N, N)).astype(np.float32)
+    below, labels, keep = orc.below_sea_components(surf, grid, 0.02)[:3]
+    ocean = np.ascontiguousarray((below & keep[np.maximum(labels, 0)]).reshape(surf.shape), np.uint8)
+    step, depth = 0.05, 0.01
+    add = np.empty((6, N, N))
+    basin = np.empty((6, N, N), np.uint8)
+    nb = ctypes.c_int64(0)
+    g = _lib.PgeGrid(F=6, N=N, H=H, spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    owner = np.ascontiguousarray(grid.owner, np.int32)
+    _lib.check(_lib.load().pge_basin_fill(ctypes.byref(g), owner.ctypes.data, surf.ctypes.data, ocean.ctypes.data, step, depth,
+                                          add.ctypes.data, basin.ctypes.data, ctypes.byref(nb)), "pge_basin_fill")
+    s32 = surf.reshape(-1)
+    oc = ocean.reshape(-1).astype(bool)
+    filled, parent, order, pop_seq = orc.hydro_flood(s32, oc, orc._cell_neighbors(grid), N)
+    gr = s32.astype(np.float64)
+    for c in pop_seq:
+        q = parent[c]
+        if q >= 0 and gr[q] + step > gr[c]:
+            gr[c] = gr[q] + step
+    want_basin = ((filled - s32) > np.float32(depth)) & ~oc
+    want = np.where(want_basin, np.maximum(gr - s32, 0.0), 0.0)
+    assert np.array_equal(basin.reshape(-1).astype(bool), want_basin) and want_basin.any()
+    assert add.reshape(-1).tobytes() == want.tobytes()
+    assert int(nb.value) == int(want_basin.sum())
