@@ -545,21 +545,129 @@ def refresh_route(state, eps):
 LAKE_MIN_DEPTH_M = 0.5
 
 
+def _window_lake_balance(state, surf, min_depth, lake_evap):
+    """maps.py:675-736: a window's depressions settled against evaporation --
+    the flat flood (hydro/priority_flood.py:193-270) draining to the inactive
+    cells and the array's border, the rain accumulated down the flood tree
+    (zoom/bake.py:323-330), each depression (scipy's 8-connected labels)
+    where its inflow meets lake_evap x evap over the water; returns (lake
+    (NE, NE) bool, counts) and lowers the route to the water on the lakes."""
+    import heapq
+
+    from scipy import ndimage
+
+    s = np.ascontiguousarray(surf[0], np.float32)
+    W = s.shape[0]
+    active = state.mask[0] == MASK_ACTIVE
+    drain = ~active
+    drain[0, :] = drain[-1, :] = drain[:, 0] = drain[:, -1] = True
+    sf, df = s.reshape(-1), drain.reshape(-1)
+    M = sf.size
+    filled = sf.copy()
+    visited = np.zeros(M, bool)
+    parent = np.full(M, -1, np.int64)
+    pop_seq, heap, fifo, seq = [], [], [], 0
+
+    def nbrs(c):
+        i, j = divmod(c, W)
+        for k in range(8):
+            i2, j2 = i + _D8_DI[k], j + _D8_DJ[k]
+            if 0 <= i2 < W and 0 <= j2 < W:
+                yield i2 * W + j2
+
+    for c in range(M):
+        if df[c]:
+            visited[c] = True
+            if any(not df[n] for n in nbrs(c)):
+                heapq.heappush(heap, (float(sf[c]), seq, c))
+                seq += 1
+    head = 0
+    while head < len(fifo) or heap:
+        if head < len(fifo):
+            c = fifo[head]
+            head += 1
+        else:
+            c = heapq.heappop(heap)[2]
+        lvl = filled[c]
+        pop_seq.append(c)
+        for n in nbrs(c):
+            if visited[n]:
+                continue
+            visited[n] = True
+            parent[n] = c
+            if sf[n] <= lvl:
+                filled[n] = lvl
+                fifo.append(n)
+            else:
+                filled[n] = sf[n]
+                heapq.heappush(heap, (float(sf[n]), seq, n))
+                seq += 1
+    acc = np.ascontiguousarray(state.precip[0], np.float64).ravel().copy()
+    for c in reversed(pop_seq):
+        if parent[c] >= 0:
+            acc[parent[c]] += acc[c]
+    filled = filled.reshape(s.shape)
+    acc = acc.reshape(s.shape)
+    dep = (filled > s + np.float32(1e-6)) & active
+    lab, n = ndimage.label(dep, structure=np.ones((3, 3), bool))
+    counts = {"depressions": int(n), "overflowing": 0, "closed": 0, "dry": 0}
+    out = np.zeros(s.shape, bool)
+    if n == 0:
+        return out, counts
+    cells = np.flatnonzero(lab.ravel() > 0)
+    cells = cells[np.lexsort((s.ravel()[cells], lab.ravel()[cells]))]
+    lab_s = lab.ravel()[cells].astype(np.int64)
+    ptr = np.searchsorted(lab_s, np.arange(1, n + 2))
+    demand = np.cumsum(lake_evap * np.maximum(state.evap[0].ravel()[cells].astype(np.float64), 0.0))
+    z = s.ravel()[cells].astype(np.float64)
+    spill = np.atleast_1d(ndimage.maximum(filled, lab, np.arange(1, n + 1)))
+    inflow = np.atleast_1d(ndimage.maximum(acc, lab, np.arange(1, n + 1)))
+    level = np.zeros(n)
+    for k in range(n):
+        a, b = ptr[k], ptr[k + 1]
+        if b <= a:
+            continue
+        need, before = float(inflow[k]), (demand[a - 1] if a > 0 else 0.0)
+        loss = demand[a:b] - before
+        if need <= 0.0:
+            level[k] = z[a] - 1.0
+            counts["dry"] += 1
+        elif loss[-1] <= need:
+            level[k] = float(spill[k])
+            counts["overflowing"] += 1
+        else:
+            i = int(np.searchsorted(loss, need))
+            level[k] = float(z[a + min(i, b - a - 1)])
+            counts["closed"] += 1
+    lv = np.zeros(n + 1)
+    lv[1:] = level
+    water = np.where(lab > 0, lv[lab], s)
+    out = (water - s > min_depth) & active
+    r = state.route[0]
+    r[out] = np.minimum(r[out], water[out])
+    return out, counts
+
+
 def refresh_lakes_window(state, min_depth, lake_evap=0.0) -> dict:
-    """maps.py:629-673 with lake_evap = 0: every depression the routing flood
-    fills more than ``min_depth`` (cell units) deep is an overflowing lake,
-    flagged on the interior's active cells (the halos stay 0)."""
-    if float(lake_evap) > 0.0:
-        raise NotImplementedError("the evaporation balance of window lakes (erosion.window_lake_evap > 0)")
+    """maps.py:629-673: every depression the routing flood fills more than
+    ``min_depth`` (cell units) deep is an overflowing lake, flagged on the
+    interior's active cells (the halos stay 0); with ``lake_evap > 0`` each
+    settles where its inflow meets its evaporation instead (and the route is
+    lowered to the water on the lakes)."""
     flag = np.zeros(state.height.shape, np.uint8)
     if state.route is None:
         state.lake_flag = flag
         return {"lake_cells": 0}
-    lake = ((state.route - (state.height + state.sediment)) > float(min_depth)) & (state.mask == MASK_ACTIVE)
+    surf = state.height + state.sediment
+    lake = ((state.route - surf) > float(min_depth)) & (state.mask == MASK_ACTIVE)
+    st = {}
+    if float(lake_evap) > 0.0:
+        out, st = _window_lake_balance(state, surf, float(min_depth), float(lake_evap))
+        lake = out[None]
     inter = state.interior
     flag[inter] = lake[inter]
     state.lake_flag = flag
-    return {"lake_cells": int(lake[inter].sum())}
+    return {"lake_cells": int(lake[inter].sum()), **st}
 
 
 def laplacian(state, d):

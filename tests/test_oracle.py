@@ -454,3 +454,26 @@ def test_basin_fill_matches_reference_bit_exact():
     info = orc.fill_basins(st, params)
     assert info["basin_cells"] == _json.loads(str(fx["info"]))["basin_cells"]
     assert np.array_equal(st.sediment, fx["sediment"])
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_window_lake_balance_matches_reference_bit_exact(tag):
+    """The oracle's restatement of a window's lake balance (maps.py:675-736,
+    window_lake_evap > 0) on the reference fixture's window and route: the
+    flags, the lowered route and the counts, bit for bit."""
+    fx = np.load(GOLDEN / "window_lake_balance.npz")
+    N, H = int(fx["N"]), int(fx["H"])
+    NE = N + 2 * H
+    from pgerosion.geometry import get_grid
+
+    grid = get_grid(N, H, float(fx["cell_size_m"]))
+    st = orc.OracleState(height=fx["height"].copy(), sediment=fx["sediment"].copy(), discharge=np.zeros((1, NE, NE)),
+                         momentum=np.zeros((1, NE, NE, 2)), hardness=np.full((1, NE, NE), 0.5, np.float32), precip=fx["precip"],
+                         evap=fx["evap"], uplift=np.zeros((1, NE, NE)), mask=fx["mask"],
+                         metric=np.ascontiguousarray(grid.metric_face[None]), metric_inv=np.ascontiguousarray(grid.metric_inv_face[None]),
+                         N=N, H=H, spherical=False, height_unit_m=float(fx["cell_size_m"]), deposit_on_exit=True)
+    st.route = fx[f"{tag}_route0"].copy()
+    info = orc.refresh_lakes_window(st, float(fx["min_depth"]), float(fx[f"{tag}_lake_evap"]))
+    assert info == json.loads(str(fx[f"{tag}_info"]))
+    assert np.array_equal(st.lake_flag, fx[f"{tag}_flag"])
+    assert st.route.tobytes() == np.ascontiguousarray(fx[f"{tag}_route"]).tobytes()
