@@ -82,9 +82,10 @@ def test_isostasy_state_is_checkpointed_and_resumed(cuda, tmp_path):
 
 
 def test_host_refreshes_are_checkpointed_and_resumed(cuda, tmp_path):
-    """With the routing flood, the sea mask and the glacial pass on (every 2
-    iterations, ice poleward of 50 degrees), the route, the base level and
-    the sticky ice are part of the checkpoint (run.py:104-116, 200-210) and a
+    """With the routing flood, the sea mask, the planet's lake balance and the
+    glacial pass on (every 2 iterations, ice poleward of 50 degrees) and the
+    basin fill at the start, the route, the base level, the lake flags and the
+    sticky ice are part of the checkpoint (run.py:104-128, 200-223) and a
     resumed run lands on the continuous run's outputs byte for byte."""
     import dataclasses
 
@@ -95,10 +96,11 @@ def test_host_refreshes_are_checkpointed_and_resumed(cuda, tmp_path):
         st.save_field(name, getattr(w, name), w.grid.H)
     _, p = _world_store(tmp_path / "unused")
     p = dataclasses.replace(p, erosion=dataclasses.replace(p.erosion, flood_every=2, sea_mask_every=2, glacial_every=2,
-                                                           glacial_from=0.0))
+                                                           glacial_from=0.0, lake_balance=True, lake_fill=False,
+                                                           basin_fill_grade=0.1))
     stage.run(st, p, log=lambda m: None)
     with np.load(st.checkpoint_dir / "erosion_iter0003.npz") as z:
-        assert {"route", "base", "ice_prev"} <= set(z.files)
+        assert {"route", "base", "ice_prev", "lake_flag", "lake_id", "lake_room"} <= set(z.files)
         assert z["ice_prev"].dtype == np.uint8 and z["ice_prev"].any()
     out = {n: np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)]) for n in stage.OUTPUTS}
     for suf in (".npz", ".json"):
