@@ -430,10 +430,9 @@ class ErosionState:
         lf[inter] = torch.as_tensor(flag, device=dev)
         closed = ~np.isnan(level)
         if closed.any():
-            b = self.base[inter]
+            b = self.base[inter]  # a view: the closed lakes' levels land in the base itself
             cl = torch.as_tensor(closed, device=dev)
             b[cl] = torch.as_tensor(level, device=dev)[cl].double()
-            self.base[inter] = b
         for t in (lf, self.base):  # exact copies of the cells they mirror (maps.py:476-479)
             flat = t.view(-1)
             flat[dst] = flat[nearest]
