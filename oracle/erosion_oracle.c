@@ -312,7 +312,7 @@ int orc_change_list_cap(int max_steps, int lateral)
 typedef struct {
     double dt, density, friction, deposition_rate, evap_rate, k_mom, mom_scale, k_disc, disc_saturation,
         disc_exponent, slope_gain, slope_sat, erodibility, cover_depth, min_volume, max_erode, conc_scale,
-        ocean_rate, fan_room, dep_floor, lake_trap, lateral_rate;
+        ocean_rate, fan_room, dep_floor, lake_trap, lateral_rate, lake_park;
     int32_t max_steps, pit_steps, ocean_steps, deposit_on_exit, N, H, spherical, F;
     int32_t use_route, pad;
     const float *roots; /* (F,NE,NE) the share of the exchange the plants hold back, or NULL */
@@ -337,6 +337,7 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
     double h_prev = -1e300;
     int exited = 0, in_sea = 0, cause = DEATH_AGE;
     int in_lake = 0; /* on an overflowing lake: crossing, no exchange with the bed (particle.py:417) */
+    int parks = 0;   /* loads this droplet has left in lakes (at most LAKE_PARKS, particle.py:418) */
 #define RECORD(CELL, DELTA, VOL, MA, MB)                                   \
     do {                                                                   \
         cl_cell[n] = (int32_t)(CELL);                                      \
@@ -480,11 +481,13 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
             }
             if (P->roots) k_e *= 1.0 - (double)P->roots[cidx]; /* roots hold the ground (particle.py:615-618) */
             double cdiff = k_e * (c_eq - sed);
+            double trapped = 0.0;
             if (in_lake) {
                 cdiff = 0.0; /* crossing a lake: the bed sees nothing (particle.py:626-629) */
             } else if (sed > 0.0 && np_[S_RFLAG] >= 1.5f) {
                 double trap = -P->lake_trap * sed; /* entering a lake: the load drops at the shore (630-634) */
                 if (trap < cdiff) cdiff = trap;
+                if (np_[S_RFLAG] >= 2.5f) trapped = P->lake_trap * sed; /* ...and a lake with room keeps the rest */
             }
             double kexp = 1.0 + q * P->conc_scale;
             if (cdiff > 0.0) {
@@ -500,6 +503,16 @@ static void trace_one(const OrcTraceParams *P, const Samp *S, const uint8_t *mas
             }
             sed += cdiff;
             RECORD(cidx, -cdiff * vol_rel, vol, vol * sa, vol * sb);
+            /* a lake keeps what its shore had no room for (particle.py:672-696): parked on the lake cell
+               entered, an entry of volume -3 */
+            if (P->lake_park > 0.0 && trapped > 0.0 && parks < LAKE_PARKS) {
+                double rest = trapped + cdiff;
+                if (rest > 0.0) {
+                    parks++;
+                    sed -= rest;
+                    RECORD(nidx, rest * vol_rel, -3.0, 0.0, 0.0);
+                }
+            }
             /* the outside of the bend (particle.py:699-738): the bank one cell across the flow */
             if (P->lateral_rate > 0.0 && cdiff > 0.0 && n + 2 * SPREAD + 2 < cap) {
                 double cross = psa * sb - psb * sa;
@@ -649,17 +662,37 @@ typedef struct {
 void orc_apply(const OrcApplyParams *A, const int32_t *cl_cell, const double *cl_delta, const float *cl_vol,
                const float *cl_mom, int64_t np, const int64_t *cl_count, int cap, const double *height,
                const double *sediment, double *acc, double *pending, float *samp, double *disch_track,
-               double *mom_track, const uint8_t *mask, const double *erode_cap, double *out4)
+               double *mom_track, const uint8_t *mask, const double *erode_cap, double *out4, double *lake_load,
+               const int32_t *lake_id, double *lake_room)
 {
     int64_t n_clamp = 0;
     double to_pending = 0.0, lost = 0.0, lost_offshore = 0.0;
     for (int64_t p = 0; p < np; p++) {
         int64_t base = p * cap;
         int64_t cnt = cl_count[p];
-        double deficit = 0.0, surplus = 0.0;
+        double deficit = 0.0, surplus = 0.0, refused = 0.0;
         int64_t prev = -1, death = -1;
         for (int64_t k = 0; k < cnt; k++) {
             int64_t c = cl_cell[base + k];
+            if (cl_vol[base + k] == -3.0f) {
+                /* a load for a lake to keep (particle.py:912-933): the lake takes what it still has room for,
+                   counted down in particle order; the rest goes where the particle ends */
+                double take = cl_delta[base + k], rest = 0.0;
+                int32_t lk = lake_id ? lake_id[c] : -1;
+                if (lk < 0) {
+                    rest = take;
+                    take = 0.0;
+                } else if (take > lake_room[lk]) {
+                    rest = take - lake_room[lk];
+                    take = lake_room[lk];
+                }
+                if (take > 0.0) {
+                    lake_load[c] += take;
+                    lake_room[lk] -= take;
+                }
+                refused += rest;
+                continue;
+            }
             if (mask[c] != MASK_ACTIVE) continue;
             double d = cl_delta[base + k];
             float v = cl_vol[base + k];
@@ -737,6 +770,7 @@ void orc_apply(const OrcApplyParams *A, const int32_t *cl_cell, const double *cl
                 prev = c;
             }
         }
+        surplus += refused;
         if (surplus > 0.0 && death >= 0) {
             if (height[death] + sediment[death] + acc[death] < samp[death * NS + S_BASE]) {
                 double keep = surplus * (1.0 - A->offshore_writeoff);

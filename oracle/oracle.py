@@ -82,7 +82,8 @@ class TraceParams(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "dt", "density", "friction", "deposition_rate", "evap_rate", "k_mom", "mom_scale", "k_disc",
         "disc_saturation", "disc_exponent", "slope_gain", "slope_sat", "erodibility", "cover_depth",
-        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap", "lateral_rate")] + [
+        "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "lake_trap", "lateral_rate",
+        "lake_park")] + [
         (n, ctypes.c_int32) for n in ("max_steps", "pit_steps", "ocean_steps", "deposit_on_exit", "N", "H", "spherical", "F",
                                       "use_route", "pad")] + [("roots", ctypes.c_void_p)]
 
@@ -167,6 +168,11 @@ class OracleState:
     lake_flag: np.ndarray = None
     #: the share of the exchange the plants hold back (float32 (F, NE, NE), erosion.vegetation) or None
     roots: np.ndarray = None
+    #: the lake parks' bookkeeping (erosion.lake_fill, maps.py:105-107): float64 load parked per cell, int32 lake of
+    #: each cell (-1: none), float64 room left per lake; None: no lake keeps a load
+    lake_load: np.ndarray = None
+    lake_id: np.ndarray = None
+    lake_room: np.ndarray = None
     base_at: int = None  # iteration of the last sea-mask refresh (refresh_base)
     ice_prev: np.ndarray = None  # the last glacial pass's ice (erosion.glacial_sticky)
     land_target: float | None = None
@@ -307,6 +313,8 @@ def trace_params(state, ep, volume0, conc_scale, mom_scale=1.0, disc_sat=None) -
         max_erode=_cu(ep, "max_erode", u), conc_scale=float(conc_scale), ocean_rate=float(ep.ocean_deposition_rate),
         fan_room=_cu(ep, "fan_room", u), dep_floor=_cu(ep, "dep_floor_m", u), lake_trap=float(getattr(ep, "lake_trap", 0.9)),
         lateral_rate=float(getattr(ep, "lateral_rate", 0.0)),
+        lake_park=1.0 if (state.spherical and bool(getattr(ep, "lake_fill", False)) and bool(getattr(ep, "lake_balance", False)))
+        else 0.0,
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps),
         deposit_on_exit=int(bool(state.deposit_on_exit)), N=int(state.N), H=int(state.H), spherical=int(bool(state.spherical)),
         F=int(state.F), use_route=int(getattr(state, "route", None) is not None),
@@ -349,7 +357,8 @@ def apply(state, ap: ApplyParams, cl, cap, ecap=None):
     lib().orc_apply(ctypes.byref(ap), _p(cl_cell), _p(cl_delta), _p(cl_vol), _p(cl_mom), ctypes.c_int64(cnt.size),
                     _p(np.ascontiguousarray(cnt)), ctypes.c_int(cap), _p(state.height), _p(state.sediment), _p(state.acc),
                     _p(state.pending), _p(state.samp), _p(state.disch_track), _p(state.mom_track), _p(state.mask), _p(ecap),
-                    _p(out4))
+                    _p(out4), *((None, None, None) if getattr(state, "lake_id", None) is None else
+                                (_p(state.lake_load), _p(state.lake_id), _p(state.lake_room))))
     return int(out4[0]), float(out4[1]), float(out4[2]), float(out4[3])
 
 

@@ -235,7 +235,7 @@ def gen_trace(cs, maps, pk, WorldParams):
 
 
 def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit,
-               use_route=False, roots=None, lateral=0.0):
+               use_route=False, roots=None, lateral=0.0, lake_park=0.0):
     n = f.size
     out = dict(cl_cell=np.zeros(n * cap, np.int32), cl_delta=np.zeros(n * cap), cl_vol=np.zeros(n * cap, np.float32),
                cl_mom=np.zeros((n * cap, 2), np.float32), cl_count=np.zeros(n, np.int64), cl_lo=np.zeros(n, np.int64),
@@ -247,7 +247,7 @@ def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y,
                        float(ep.slope_gain), float(ep.slope_saturation), float(ep.erodibility), cu("cover_depth"),
                        float(ep.min_volume_frac) * volume0, int(max_steps), cu("max_erode"), conc, int(ep.pit_steps),
                        bool(deposit_on_exit), float(ep.ocean_deposition_rate), int(ep.ocean_steps), cu("fan_room"),
-                       cu("dep_floor_m"), float(ep.lake_trap), 0.0, float(lateral),
+                       cu("dep_floor_m"), float(ep.lake_trap), float(lake_park), float(lateral),
                        np.zeros((1, 1, 1), np.float32) if roots is None else roots, roots is not None,
                        out["cl_cell"], out["cl_delta"], out["cl_vol"], out["cl_mom"], out["cl_count"], out["cl_lo"],
                        out["cl_hi"], out["sp_death"])
@@ -866,6 +866,71 @@ def gen_window_lake_balance(cs, maps, pk, WorldParams):
                         mask=mask, precip=precip, evap=w["evap"], min_depth=float(p.hydro.lake_min_depth) / unit, **out)
 
 
+def gen_lake_parks(cs, maps, pk, WorldParams):
+    """Lake parks (erosion.lake_fill: particle.py:626-636, 672-696 in the
+    trace, 912-933 and 1019 in the apply): the lake window of
+    gen_lake_trace with every lake flagged 2 (room for its rivers' load),
+    each lake numbered (lake_id) with a small room (lake_room) so that the
+    serial countdown refuses some loads; one reference trace with lake_park
+    on and one serial apply, recording the parked loads and the rooms left."""
+    from scipy import ndimage
+
+    st, p, fw, w, mask = _window_of_evolved(cs, maps, pk, WorldParams)
+    ep = p.erosion
+    NE, H, N = st.NE, st.H, st.N
+    unit = st.height_unit_m
+    ws = maps.ErosionState(height=w["height"].copy(), sediment=w["sediment"].copy(), discharge=w["discharge"].copy(),
+                           momentum=w["momentum"].copy(), hardness=w["hardness"], precip=np.ones((1, NE, NE), np.float32),
+                           evap=w["evap"], uplift=np.zeros((1, NE, NE)), mask=mask, metric=w["metric"], metric_inv=w["metric_inv"],
+                           N=N, H=H, spherical=False, height_unit_m=unit, base=w["base"].copy(), deposit_on_exit=True)
+    ws.refresh_route(float(ep.route_eps) / unit)
+    ws.refresh_lakes_window(float(p.hydro.lake_min_depth) / unit, 0.0)
+    lab, n = ndimage.label(ws.lake_flag[0] > 0, structure=np.ones((3, 3), bool))
+    flag = (ws.lake_flag > 0).astype(np.uint8) * 2
+    lake_id = np.full((1, NE, NE), -1, np.int32)
+    lake_id[0][lab > 0] = lab[lab > 0] - 1
+    lake_room = np.full(max(n, 1), 0.02, np.float64)
+    samp = np.zeros((1, NE, NE, pk.NS), np.float32)
+    pk.pack_samples(samp, w["height"], w["sediment"], ws.route, True, w["discharge"], w["momentum"], w["evap"], w["hardness"],
+                    w["metric"], w["metric_inv"], w["base"], flag)
+    rng = np.random.default_rng(109)
+    act = np.flatnonzero(mask.reshape(-1) == 1)
+    n_rain, n_load = 1500, 400
+    pick = act[rng.integers(0, act.size, n_rain + n_load)]
+    ei, ej = pick // NE, pick % NE
+    x = (ei - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    y = (ej - H) + np.concatenate([rng.random(n_rain), np.full(n_load, 0.5)])
+    sed = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 0.5 + 1e-3])
+    dirs = np.concatenate([np.zeros(n_rain), rng.random(n_load) * 2 * np.pi])
+    f = np.zeros(x.size, np.int64)
+    volume0 = 0.02
+    conc = 1.0 / (volume0 * x.size)
+    max_steps = maps.max_steps_of(ep, N)
+    cap = int(pk.change_list_cap(max_steps, False))
+    res = _ref_trace(pk, ep, samp, mask, N, H, False, True, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit,
+                     use_route=True, lake_park=1.0)
+    acc = np.zeros_like(w["height"])
+    pending = np.zeros_like(w["height"])
+    dtr = np.zeros_like(w["height"])
+    mtr = np.zeros_like(w["momentum"])
+    samp_after = samp.copy()
+    lake_load = np.zeros((1, NE, NE))
+    room_after = lake_room.copy()
+    cu = lambda k: float(getattr(ep, k)) / unit
+    ap = pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                          w["height"], w["sediment"], acc, pending, samp_after, dtr, mtr, mask, cu("iter_erode"), cu("iter_deposit"),
+                          float(ep.fan_slope), True, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                          lake_load, lake_id, room_after)
+    parks = int((res["cl_vol"] == -3.0).sum())
+    np.savez_compressed(
+        HERE / "lake_parks.npz", N=N, H=H, face=fw, **w, mask=mask, route=ws.route, lake_flag=flag, lake_id=lake_id,
+        lake_room=lake_room, sp_face=f, sp_x=x, sp_y=y, sp_sed=sed, sp_dir=dirs, volume0=volume0, conc_scale=conc, cap=cap,
+        max_steps=max_steps, deposit_on_exit=True, params=json.dumps({k: getattr(ep, k) for k in ep.__dataclass_fields__}),
+        cell_size_m=unit, **res, acc=acc, pending=pending, disch_track=dtr, mom_track=mtr, lake_load=lake_load,
+        room_after=room_after, apply_out=np.array([float(a) for a in ap]))
+    print(f"lake_parks: {n} lakes, {x.size} droplets, park entries {parks}, parked {lake_load.sum():.4f}, rooms left {room_after}")
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -881,7 +946,8 @@ def main(bake: str, only: str | None = None):
             "roots_trace": lambda: gen_roots_trace(cs, maps, pk, WorldParams),
             "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams),
             "lateral": lambda: gen_lateral(cs, maps, pk, WorldParams),
-            "window_lake_balance": lambda: gen_window_lake_balance(cs, maps, pk, WorldParams)}
+            "window_lake_balance": lambda: gen_window_lake_balance(cs, maps, pk, WorldParams),
+            "lake_parks": lambda: gen_lake_parks(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

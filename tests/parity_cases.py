@@ -86,13 +86,23 @@ def window_case(path=GOLDEN / "window_trace.npz") -> dict:
                              deposit_on_exit=bool(t["deposit_on_exit"]))
         if "roots" in t.files:
             st.roots = np.ascontiguousarray(t["roots"], np.float32)
+        if "lake_id" in t.files:  # the lake parks' window: route, lakes with room, their ids and rooms
+            st.route = t["route"].copy()
+            st.lake_flag = t["lake_flag"].copy()
+            st.lake_load = np.zeros_like(st.height)
+            st.lake_id = np.ascontiguousarray(t["lake_id"], np.int32)
+            st.lake_room = t["lake_room"].copy()
         st.pack()
         tp = orc.trace_params(st, ep, case["volume0"], case["conc_scale"])
+        if "lake_id" in t.files:
+            tp.lake_park = 1.0
         cl = orc.trace(st, tp, t["sp_face"], t["sp_x"], t["sp_y"], t["sp_sed"], t["sp_dir"], case["volume0"])
         out = orc.apply(st, orc.apply_params(st, ep, ep.iter_deposit / cs), cl, case["cap"])
         names = ("cl_cell", "cl_delta", "cl_vol", "cl_mom", "cl_count", "cl_lo", "cl_hi", "sp_death")
         r = dict(zip(names, cl))
         r.update(acc=st.acc, pending=st.pending, disch_track=st.disch_track, mom_track=st.mom_track, apply_out=np.array(out, float))
+        if "lake_id" in t.files:
+            r.update(lake_load=st.lake_load, room_after=st.lake_room)
         return r
 
     case["oracle"] = oracle

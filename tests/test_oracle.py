@@ -477,3 +477,25 @@ def test_window_lake_balance_matches_reference_bit_exact(tag):
     assert info == json.loads(str(fx[f"{tag}_info"]))
     assert np.array_equal(st.lake_flag, fx[f"{tag}_flag"])
     assert st.route.tobytes() == np.ascontiguousarray(fx[f"{tag}_route"]).tobytes()
+
+
+def test_lake_parks_trace_and_serial_apply_match_reference_bit_exact():
+    """Lake parks (erosion.lake_fill; particle.py:626-636, 672-696 in the
+    trace, 912-933 and 1019 in the apply) on the lake window with every lake
+    flagged as having room and small rooms: the park entries (volume -3 on
+    the lake cell entered), the serial room countdown, the parked loads and
+    the refused rest added to the particle's surplus equal the reference's
+    bit for bit."""
+    case = window_case(GOLDEN / "lake_parks.npz")
+    res = case["oracle"]()
+    cap = case["cap"]
+    for k in ("cl_count", "cl_lo", "cl_hi", "sp_death"):
+        assert np.array_equal(res[k], case[k]), k
+    for a, b in zip(changelist_rows(res, cap), changelist_rows(case, cap)):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    assert int((case["cl_vol"] == -3.0).sum()) > 50
+    for k in ("acc", "pending", "disch_track", "mom_track", "lake_load", "room_after"):
+        assert np.array_equal(res[k], case[k]), k
+    assert np.array_equal(res["apply_out"], case["apply_out"])
+    assert float(case["lake_load"].sum()) > 0.0 and (case["room_after"] == 0.0).all()  # rooms ran out: loads refused
