@@ -1095,7 +1095,125 @@ def fill_basins(state, params) -> dict | None:
     return {"basin_cells": int(basin.sum())}
 
 
-def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0) -> dict:
+def _lake_plain(water, lab, parent, pop_seq, grade):
+    """maps.py:1232-1245: the plain a lake fills towards -- its water level at
+    the outlet, ``grade`` higher with every flood step inside the same lake
+    (pop order: a parent is done before its children)."""
+    g = water.copy()
+    for c in pop_seq:
+        if lab[c] >= 0:
+            q = parent[c]
+            if q >= 0 and lab[q] == lab[c]:
+                g[c] = g[q] + grade
+    return g
+
+
+def settle_lake_loads(state, lake, water, surf, flood, grade, ice_evap, rise=0.0, load_share=1.0):
+    """maps.py:490-628: lay what the lakes kept (``lake_load``) over their
+    floors and give every lake its room until the next refresh.  A load goes
+    to the lake of this refresh that holds its cell, else to the heir of the
+    lake it was parked in (the new lake covering most of it), else on as a
+    stockpile; each lake fills towards a plain graded from its outlet, at
+    most ``rise`` above the water, farthest cells from the outlet first; its
+    room left is what that plain would still take (0 for a frozen lake).
+    Returns (volumes, takes)."""
+    grid = state.grid
+    N, H = grid.N, grid.H
+    inter = state.interior
+    filled, parent, order, pop_seq = flood
+    load = state.lake_load[inter]
+    out = {"parked": float(load.sum()), "laid": 0.0, "stray": 0.0, "room": 0.0, "lakes": 0}
+    takes = np.zeros(lake.size, bool)
+    lake_id = np.full(lake.size, -1, np.int32)
+    state.lake_room = np.zeros(1)
+
+    def add(arr, flat_cells, values):
+        f, i, j = np.unravel_index(flat_cells, (6, N, N))
+        arr[f, i + H, j + H] += values  # distinct cells
+
+    lab, n = _label_level(lake.reshape(-1), np.asarray(water, np.float32).reshape(-1), state._nbr)
+    lflat = load.reshape(-1)
+    held = np.flatnonzero(lflat > 0.0)
+    have = np.zeros(max(n, 1))
+    if held.size:
+        was = state.lake_id[inter].reshape(-1)
+        n_was = int(was.max()) + 1 if was.size else 0
+        heir = np.full(max(n_was, 1), -1, np.int64)
+        both = np.flatnonzero((was >= 0) & (lab >= 0))
+        if both.size and n > 0:
+            key, cnt = np.unique(was[both].astype(np.int64) * n + lab[both], return_counts=True)
+            o = np.lexsort((cnt, key // n))
+            k_old = (key // n)[o]
+            last = np.r_[k_old[1:] != k_old[:-1], True]
+            heir[k_old[last]] = (key % n)[o][last]
+        to = np.where(lab[held] >= 0, lab[held], np.where(was[held] >= 0, heir[np.maximum(was[held], 0)], -1))
+        ok = to >= 0
+        np.add.at(have, to[ok], lflat[held[ok]])
+        if (~ok).any():
+            add(state.pending, held[~ok], lflat[held[~ok]])
+            out["stray"] = float(lflat[held[~ok]].sum())
+    cells = np.flatnonzero(lab >= 0)
+    if cells.size:
+        s64 = np.asarray(surf, np.float64).reshape(-1)
+        w64 = np.asarray(water, np.float64).reshape(-1)
+        plain = _lake_plain(w64, lab, parent, pop_seq, float(grade))
+        room = np.maximum(np.minimum(plain[cells], w64[cells] + float(rise)) - s64[cells], 0.0)
+        order_f = order[cells]
+        first = np.full(n, np.iinfo(np.int64).max)
+        np.minimum.at(first, lab[cells], order_f)
+        outlet = np.zeros(n, np.int64)
+        at = order_f == first[lab[cells]]
+        outlet[lab[cells][at]] = cells[at]
+        if getattr(state, "_centres", None) is None:
+            state._centres = np.ascontiguousarray(grid.centers()[:, H:H + N, H:H + N].reshape(-1, 3))
+        centres = state._centres
+        far = np.linalg.norm(centres[cells] - centres[outlet[lab[cells]]], axis=1)
+        o = np.lexsort((-far, lab[cells]))
+        cells, room = cells[o], room[o]
+        L = lab[cells].astype(np.int64)
+        ptr = np.searchsorted(L, np.arange(n))
+        csum = np.cumsum(room)
+        before = csum - room - (csum[ptr] - room[ptr])[L]
+        lay = np.clip(have[L] - before, 0.0, room)
+        add(state.sediment, cells, lay)
+        if getattr(state, "iso_acc", None) is not None:
+            add(state.iso_acc, cells, float(load_share) * lay)
+        left = np.bincount(L, weights=room - lay, minlength=n)
+        over = have - np.bincount(L, weights=lay, minlength=n)
+        spill = over > 1e-9
+        if spill.any():
+            add(state.pending, cells[ptr[spill]], over[spill])
+            out["stray"] += float(over[spill].sum())
+        warm = np.ones(n, bool)
+        cold = (state.evap[inter] <= float(ice_evap)).reshape(-1)[cells]
+        warm[np.unique(L[cold])] = False
+        open_ = warm & (left > 0.0)
+        takes[cells[open_[L]]] = True
+        ids = np.cumsum(open_) - 1
+        lake_id[cells[open_[L]]] = ids[L[open_[L]]].astype(np.int32)
+        if open_.any():
+            state.lake_room = np.ascontiguousarray(left[open_], np.float64)
+        out.update(laid=float(lay.sum()), room=float(left[open_].sum()), lakes=int(open_.sum()))
+    state.lake_load[inter] = 0.0
+    full = np.full(state.height.shape, -1, np.int32)
+    full[inter] = lake_id.reshape(6, N, N)
+    state.lake_id = full
+    return out, takes
+
+
+def lake_fill_args(state, params):
+    """maps.py:1248-1258: refresh_lakes' ``fill`` -- (grade in cell units per
+    cell, ice_evap, the plain's rise above the water in cell units, the load
+    share) with erosion.lake_fill and lake_balance on the planet, else None."""
+    ep = _ep(params)
+    if not (state.spherical and bool(getattr(ep, "lake_fill", False)) and bool(getattr(ep, "lake_balance", False))):
+        return None
+    cell_km = float(state.grid.cell_size_m) / 1000.0
+    return (float(getattr(ep, "basin_fill_grade", 0.0)) * cell_km / state.height_unit_m, float(getattr(ep, "ice_evap", 0.0)),
+            float(getattr(ep, "lake_fill_rise_m", 1.0)) / state.height_unit_m, float(getattr(ep, "lake_fill_load", 0.55)))
+
+
+def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0, fill=None) -> dict:
     """maps.py:422-479 (erosion.lake_fill off): the planet's lakes on the
     current surface -- overflowing lakes deeper than ``min_depth`` flagged,
     a lake drawn below its rim a closed sea at its level in ``base``; flags
@@ -1124,7 +1242,18 @@ def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0) -> d
     lake = ((water - s32) > np.float32(min_depth)) & ~ocean
     closed = lake & (water < filled - np.float32(1e-4))
     flag = np.zeros(state.height.shape, np.uint8)
-    flag[inter] = (lake & ~closed).reshape(surf.shape)
+    settled = {}
+    if fill is not None:
+        if state.lake_load is None:
+            state.lake_load = np.zeros_like(state.height)
+            state.lake_id = np.full(state.height.shape, -1, np.int32)
+            state.lake_room = np.zeros(1)
+        settled, takes = settle_lake_loads(state, lake & ~closed, water, s32, (filled, parent, order, pop_seq), *fill)
+        s32 = np.ascontiguousarray((state.height + state.sediment)[inter], np.float32).reshape(-1)
+        lake &= (water - s32) > np.float32(min_depth)  # what the load raised to its plain is ground again
+        flag[inter] = ((lake & ~closed).astype(np.uint8) + (takes & lake & ~closed)).reshape(surf.shape)
+    else:
+        flag[inter] = (lake & ~closed).reshape(surf.shape)
     if closed.any():
         b = state.base[inter].reshape(-1).copy()
         b[closed] = water[closed]
@@ -1134,7 +1263,8 @@ def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0) -> d
         flat = arr.reshape(-1, 1)
         flat[hm.dst] = flat[hm.nearest]
     state.lake_flag = flag
-    return {"lake_cells": int(lake.sum()), "lake_cells_closed": int((closed & lake).sum()), **bal}
+    return {"lake_cells": int(lake.sum()), "lake_cells_closed": int((closed & lake).sum()), **bal,
+            **{f"load_{k}": v for k, v in settled.items()}}
 
 
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
@@ -1151,7 +1281,8 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
         hydro = getattr(params, "hydro", None)
         depth_m = float(getattr(hydro, "lake_min_depth", LAKE_MIN_DEPTH_M)) if hydro is not None else LAKE_MIN_DEPTH_M
         st_lake = refresh_lakes(state, float(getattr(hydro, "lake_evap", 6.0)), depth_m / state.height_unit_m,
-                                OCEAN_MIN_FRACTION, float(getattr(hydro, "land_evap", 3.0)))  # maps.py:1555-1562
+                                OCEAN_MIN_FRACTION, float(getattr(hydro, "land_evap", 3.0)),
+                                lake_fill_args(state, params))  # maps.py:1555-1562
     elif not state.spherical and bool(getattr(ep, "window_lakes", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
             (state.lake_flag is None or state.iteration % int(ep.flood_every) == 0):
         hydro = getattr(params, "hydro", None)

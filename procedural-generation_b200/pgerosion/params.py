@@ -114,6 +114,8 @@ class ErosionParams:
     window_lake_evap: float = 0.0
     lake_fill: bool = True
     lake_trap: float = 0.9
+    lake_fill_rise_m: float = 1.0
+    lake_fill_load: float = 0.55
     dep_floor_m: float = 1.0
     flood_every: int = 10
     route_eps: float = 0.05

@@ -931,6 +931,37 @@ def gen_lake_parks(cs, maps, pk, WorldParams):
     print(f"lake_parks: {n} lakes, {x.size} droplets, park entries {parks}, parked {lake_load.sum():.4f}, rooms left {room_after}")
 
 
+def gen_lake_fill_steps(cs, maps, pk, WorldParams):
+    """Full reference steps with the bake's default lakes: lake_balance and
+    lake_fill on (the loads rivers bring a lake parked in it and laid over
+    its floor at each refresh, maps.py:490-628), the sea mask and the routing
+    flood every 2 iterations, on the six-face N=32 world of gen_lake_balance."""
+    from pgerosion import synth
+
+    world = synth.earth_world(seed=11, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    iters = 7
+    p = _world_params(WorldParams, 32, 2, 50.0, 11, 0.45, iterations=iters, max_steps=48, friction=0.05, erodibility=0.3,
+                      deposition_rate=0.3, evap_rate=0.01, uplift_mode="replay", flood_every=2, sea_mask_every=2,
+                      lake_balance=True, lake_fill=True, basin_fill_grade=0.1)
+    p = p.with_overrides(hydro={"land_evap": 3.0, "lake_evap": 6.0, "pet_t0": 0.0})
+    st = _ref_state(cs, maps, world, p)
+    maps.start_replay(st, p)
+    h_start = st.height.copy()
+    stats = []
+    for it in range(iters):
+        s_ = maps.step(st, p, it, n_particles=4096)
+        stats.append({k: s_[k] for k in ("particles", "entries", "clamped", "deaths", "datum_shift")})
+        if s_.get("lakes") is not None:
+            stats[-1]["lakes"] = s_["lakes"]
+    np.savez_compressed(HERE / "lake_fill_steps.npz", N=32, H=2, cell_size_m=50.0, land_fraction=0.45, seed=11, iterations=iters,
+                        n_particles=4096, params=json.dumps({k: getattr(p.erosion, k) for k in p.erosion.__dataclass_fields__}),
+                        h_start=h_start, height=st.height, sediment=st.sediment, discharge=st.discharge, momentum=st.momentum,
+                        pending=st.pending, base=st.base, lake_flag=st.lake_flag, lake_load=st.lake_load, lake_id=st.lake_id,
+                        lake_room=st.lake_room, route=st.route, stats=json.dumps(stats), bedrock=world.bedrock,
+                        hardness=world.hardness, precip=world.precip, evap=world.evap, uplift=world.uplift)
+    print("lake_fill_steps:", [s_.get("lakes") for s_ in stats])
+
+
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
@@ -947,7 +978,8 @@ def main(bake: str, only: str | None = None):
             "window_steps": lambda: gen_window_steps(cs, maps, pk, WorldParams),
             "lateral": lambda: gen_lateral(cs, maps, pk, WorldParams),
             "window_lake_balance": lambda: gen_window_lake_balance(cs, maps, pk, WorldParams),
-            "lake_parks": lambda: gen_lake_parks(cs, maps, pk, WorldParams)}
+            "lake_parks": lambda: gen_lake_parks(cs, maps, pk, WorldParams),
+            "lake_fill_steps": lambda: gen_lake_fill_steps(cs, maps, pk, WorldParams)}
     for name, g in gens.items():
         if only is None or name == only:
             g()

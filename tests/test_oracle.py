@@ -499,3 +499,36 @@ def test_lake_parks_trace_and_serial_apply_match_reference_bit_exact():
         assert np.array_equal(res[k], case[k]), k
     assert np.array_equal(res["apply_out"], case["apply_out"])
     assert float(case["lake_load"].sum()) > 0.0 and (case["room_after"] == 0.0).all()  # rooms ran out: loads refused
+
+
+def test_lake_fill_steps_match_reference_bit_exact():
+    """Full steps with the bake's default lakes (lake_balance and lake_fill:
+    park entries, the serial room countdown, the loads laid over the lake
+    floors and the rooms given at each refresh, maps.py:490-628), the sea
+    mask and the routing flood every 2 iterations: the oracle's state, lake
+    loads, ids, rooms and flags equal the reference's bit for bit."""
+    import json as _json
+
+    from pgerosion.geometry import get_grid
+    from pgerosion.params import WorldGroup, WorldParams
+    from pgerosion.synth import World
+    from tests.parity_cases import erosion_params
+
+    fx = np.load(GOLDEN / "lake_fill_steps.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    params = WorldParams(world=WorldGroup(seed=int(fx["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(fx["land_fraction"]),
+                                          halo=H), erosion=erosion_params(str(fx["params"])))
+    world = World(get_grid(N, H, cs), fx["bedrock"], fx["hardness"], fx["precip"], fx["evap"], fx["uplift"],
+                  float(fx["land_fraction"]))
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    assert np.array_equal(st.height, fx["h_start"])
+    stats = _json.loads(str(fx["stats"]))
+    for it in range(int(fx["iterations"])):
+        s = orc.step(st, params, it, n_particles=int(fx["n_particles"]))
+        for k in ("particles", "entries", "clamped", "deaths"):
+            assert s[k] == stats[it][k], (it, k)
+        if "lakes" in stats[it]:
+            assert s["lakes"] == stats[it]["lakes"], it
+    for k in ("height", "sediment", "discharge", "momentum", "pending", "base", "lake_flag", "lake_load", "lake_id", "lake_room"):
+        assert np.array_equal(getattr(st, k), fx[k]), k
