@@ -1075,7 +1075,7 @@ def fill_basins(state, params) -> dict | None:
     N = grid.N
     inter = state.interior
     surf = np.ascontiguousarray((state.height + state.sediment)[inter], np.float32)
-    below, labels, keep = below_sea_components(surf, grid, OCEAN_MIN_FRACTION)
+    below, labels, keep = below_sea_components(surf, grid, _ocean_min_fraction(params))
     ocean = np.zeros(surf.size, bool) if labels is None else (below & keep[np.maximum(labels, 0)]).reshape(-1)
     if getattr(state, "_nbr", None) is None:
         state._nbr = _cell_neighbors(grid)
@@ -1267,12 +1267,18 @@ def refresh_lakes(state, lake_evap, min_depth, min_fraction, land_evap=0.0, fill
             **{f"load_{k}": v for k, v in settled.items()}}
 
 
+def _ocean_min_fraction(params) -> float:
+    """hydro.ocean_min_fraction when the params carry a hydro group, else the bake's 0.02 (maps.py:770-774)."""
+    hydro = getattr(params, "hydro", None)
+    return float(getattr(hydro, "ocean_min_fraction", OCEAN_MIN_FRACTION)) if hydro is not None else OCEAN_MIN_FRACTION
+
+
 def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
     ep = _ep(params)
     sea_every = int(getattr(ep, "sea_mask_every", 0))
     st_base = None
     if state.spherical and sea_every > 0 and (state.base_at is None or state.iteration % sea_every == 0):
-        st_base = refresh_base(state, OCEAN_MIN_FRACTION)  # maps.py:1546-1551, before the route
+        st_base = refresh_base(state, _ocean_min_fraction(params))  # maps.py:1546-1551, before the route
     if int(getattr(ep, "flood_every", 0)) > 0 and (state.route is None or state.iteration % int(ep.flood_every) == 0):
         refresh_route(state, _cu(ep, "route_eps", state.height_unit_m))  # maps.py:1553-1554
     st_lake = None
@@ -1281,7 +1287,7 @@ def step(state, params, iteration_key, n_particles=None, chunk=None) -> dict:
         hydro = getattr(params, "hydro", None)
         depth_m = float(getattr(hydro, "lake_min_depth", LAKE_MIN_DEPTH_M)) if hydro is not None else LAKE_MIN_DEPTH_M
         st_lake = refresh_lakes(state, float(getattr(hydro, "lake_evap", 6.0)), depth_m / state.height_unit_m,
-                                OCEAN_MIN_FRACTION, float(getattr(hydro, "land_evap", 3.0)),
+                                _ocean_min_fraction(params), float(getattr(hydro, "land_evap", 3.0)),
                                 lake_fill_args(state, params))  # maps.py:1555-1562
     elif not state.spherical and bool(getattr(ep, "window_lakes", False)) and int(getattr(ep, "flood_every", 0)) > 0 and \
             (state.lake_flag is None or state.iteration % int(ep.flood_every) == 0):

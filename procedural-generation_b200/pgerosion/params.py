@@ -139,13 +139,27 @@ class TectonicsGroup:
 
 
 @dataclass
+class HydroGroup:
+    """The hydro knobs the erosion stage reads (the bake's ``hydro`` group,
+    defaults as there): the lakes' open-water evaporation and the land's
+    (the evaporation balance), the depth a lake must reach, and the share of
+    the globe a below-sea body needs to count as open ocean."""
+
+    lake_evap: float = 6.0
+    land_evap: float = 3.0
+    lake_min_depth: float = 0.5
+    ocean_min_fraction: float = 0.02
+
+
+@dataclass
 class WorldParams:
-    """Minimal stand-in for the bake's ``WorldParams``: the world and erosion
-    groups plus the deterministic random streams."""
+    """Minimal stand-in for the bake's ``WorldParams``: the world, erosion
+    and hydro groups plus the deterministic random streams."""
 
     world: WorldGroup = field(default_factory=WorldGroup)
     erosion: ErosionParams = field(default_factory=ErosionParams)
     tectonics: TectonicsGroup = field(default_factory=TectonicsGroup)
+    hydro: HydroGroup = field(default_factory=HydroGroup)
 
     def rng(self, stage: str, *extra: int) -> np.random.Generator:
         if stage not in STAGE_SEED_OFFSETS:
