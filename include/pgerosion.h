@@ -453,7 +453,10 @@ typedef struct PgeLakeInfo {
  * be NULL) the water level (cell units) on cells of lakes drawn more than
  * 1e-4 below their rim (the caller's base level there), NaN elsewhere; water
  * (may be NULL) the water surface.  PGE_E_UNSUPPORTED if a land cell gets no
- * flow direction (the flood did not reach it). */
+ * flow direction (the flood did not reach it).  The pass keeps its
+ * full-size scratch (about 120 bytes a cell: 0.8 GB at N = 1024) on the
+ * calling thread between calls, so that a refresh every few iterations
+ * reuses its pages. */
 PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
                              const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                              double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,

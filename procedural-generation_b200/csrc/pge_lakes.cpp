@@ -138,6 +138,11 @@ class LevelHeap {
         k_.reserve(n);
         c_.reserve(n);
     }
+    void clear()
+    {
+        k_.clear();
+        c_.clear();
+    }
 
   private:
     std::vector<uint64_t> k_;
@@ -163,11 +168,16 @@ void flood(const Sphere &S, const float *surface, std::vector<uint8_t> &drain, s
     order.assign(M, -1);
     pop_seq.clear();
     pop_seq.reserve(M);
-    std::vector<uint8_t> visited(M, 0);
-    LevelHeap heap;
-    heap.reserve(1 << 16);
-    std::vector<int64_t> fifo;
-    fifo.reserve(1024);
+    // per-thread scratch kept between calls (a refresh every few iterations reuses its pages)
+    static thread_local std::vector<uint8_t> visited_s;
+    static thread_local LevelHeap heap_s;
+    static thread_local std::vector<int64_t> fifo_s;
+    std::vector<uint8_t> &visited = visited_s;
+    LevelHeap &heap = heap_s;
+    std::vector<int64_t> &fifo = fifo_s;
+    visited.assign(M, 0);
+    heap.clear();
+    fifo.clear();
     int64_t seq = 0;
     for (int64_t c = 0; c < M; c++) {
         if (!drain[c]) continue;
@@ -264,7 +274,9 @@ int64_t label_components(const Sphere &S, const std::vector<uint8_t> &mask, cons
 {
     const int64_t M = (int64_t)mask.size();
     labels.assign(M, -1);
-    std::vector<int64_t> stack;
+    static thread_local std::vector<int64_t> stack_s;
+    std::vector<int64_t> &stack = stack_s;
+    stack.clear();
     int64_t n = 0;
     for (int64_t s = 0; s < M; s++) {
         if (!mask[s] || labels[s] >= 0) continue;
@@ -294,6 +306,20 @@ double budyko(double aridity)
     return std::sqrt(a * std::tanh(1.0 / a) * (1.0 - std::exp(-a)));
 }
 
+// the planet pass's full-size scratch, one per calling thread, kept between refreshes: every array is
+// reassigned before it is read, and the OpenMP loops reach it through references taken on the calling thread
+struct LakeScratch {
+    std::vector<uint8_t> drain, dep;
+    std::vector<float> filled, water;
+    std::vector<int64_t> parent, order, pop_seq, down, topo, lab, cells, outlet_lake;
+    std::vector<double> w, wr, af, et, pe, acc, run;
+};
+LakeScratch &lake_scratch()
+{
+    static thread_local LakeScratch s;
+    return s;
+}
+
 }  // namespace
 
 // returns 0, or -1 when a land cell got no flow direction
@@ -304,20 +330,21 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
 {
     Sphere S{N, H, N + 2 * H, owner};
     const int64_t M = (int64_t)6 * N * N;
-    std::vector<uint8_t> drain(ocean_in, ocean_in + M);
-    std::vector<float> filled;
-    std::vector<int64_t> parent, order, pop_seq, down;
+    LakeScratch &X = lake_scratch();
+    std::vector<uint8_t> &drain = X.drain, &dep = X.dep;
+    std::vector<float> &filled = X.filled, &water = X.water;
+    std::vector<int64_t> &parent = X.parent, &order = X.order, &pop_seq = X.pop_seq, &down = X.down, &topo = X.topo;
+    drain.assign(ocean_in, ocean_in + M);
     flood(S, surface, drain, filled, parent, order, pop_seq);
     if (!flow_down(S, metric, filled, ocean_in, parent, down)) return -1;
     // upstream first: the pop sequence reversed, without the ocean
-    std::vector<int64_t> topo;
-    topo.reserve(pop_seq.size());
+    topo.clear();
     for (size_t t = pop_seq.size(); t-- > 0;)
         if (!ocean_in[pop_seq[t]]) topo.push_back(pop_seq[t]);
 
     PgeLakeInfo inf{};
-    std::vector<float> water(filled);
-    std::vector<uint8_t> dep(M, 0);
+    water.assign(filled.begin(), filled.end());
+    dep.assign(M, 0);
     int64_t ndep = 0;
 #pragma omp parallel for schedule(static) reduction(+ : ndep)
     for (int64_t c = 0; c < M; c++) {
@@ -326,10 +353,10 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
     }
     const bool any_dep = ndep > 0;
     if ((lake_evap > 0.0 || land_evap > 0.0) && any_dep) {
-        std::vector<int64_t> lab;
+        std::vector<int64_t> &lab = X.lab, &cells = X.cells;
         const int64_t n = label_components(S, dep, filled, lab);
         // a depression's cells by depth (ties in cell order)
-        std::vector<int64_t> cells;
+        cells.clear();
         for (int64_t c = 0; c < M; c++)
             if (lab[c] >= 0) cells.push_back(c);
         std::stable_sort(cells.begin(), cells.end(), [&](int64_t a, int64_t b) {
@@ -339,7 +366,10 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
         const int64_t K = (int64_t)cells.size();
         std::vector<int64_t> ptr(n + 1, K);
         for (int64_t t = K; t-- > 0;) ptr[lab[cells[t]]] = t;
-        std::vector<double> w(M), wr(M), af(M);
+        std::vector<double> &w = X.w, &wr = X.wr, &af = X.af;
+        w.resize(M);
+        wr.resize(M);
+        af.resize(M);
         const double cs2 = cell_size_m * cell_size_m;
 #pragma omp parallel for schedule(static)
         for (int64_t c = 0; c < M; c++) {
@@ -352,7 +382,9 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
         if (runoff) {
             // the land evaporates too: a cell's rain runs off in the share Budyko's curve leaves, and
             // open water loses the potential evaporation less what the land under it would have
-            std::vector<double> et(M), pe(M);
+            std::vector<double> &et = X.et, &pe = X.pe;
+            et.resize(M);
+            pe.resize(M);
 #pragma omp parallel for schedule(static)
             for (int64_t c = 0; c < M; c++) {
                 const double rain = w[c] / af[c];
@@ -363,7 +395,7 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
             for (int64_t t = 0; t < K; t++) per[t] = (pe[cells[t]] - et[cells[t]]) * af[cells[t]];
             k_lake = 1.0;
         } else {
-            wr = w;
+            wr.assign(w.begin(), w.end());
             for (int64_t t = 0; t < K; t++) per[t] = (double)pet[cells[t]] * af[cells[t]];
         }
         // cumulative loss of each depression with the water at each cell's level
@@ -379,7 +411,9 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
             for (int64_t t = ptr[L]; t < ptr[L + 1]; t++) cum[t] = csum[t] - before;
         }
         // the outlet: the depression's first popped cell
-        std::vector<int64_t> outlet(n, -1), outlet_lake(M, -1);
+        std::vector<int64_t> outlet(n, -1);
+        std::vector<int64_t> &outlet_lake = X.outlet_lake;
+        outlet_lake.assign(M, -1);
         for (int64_t t = 0; t < K; t++) {
             const int64_t c = cells[t], L = lab[c];
             if (outlet[L] < 0 || order[c] < order[outlet[L]]) outlet[L] = c;
@@ -390,7 +424,9 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
             spill[L] = (double)filled[outlet[L]];
         }
         // one accumulation, upstream first, solving each depression as it passes its outlet
-        std::vector<double> acc(w), run(wr);
+        std::vector<double> &acc = X.acc, &run = X.run;
+        acc.assign(w.begin(), w.end());
+        run.assign(wr.begin(), wr.end());
         for (const int64_t c : topo) {
             const int64_t L = outlet_lake[c];
             if (L >= 0) {
