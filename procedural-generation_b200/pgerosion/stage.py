@@ -293,15 +293,58 @@ def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
     state.iteration = int(meta["iteration"])
 
 
+#: the active volcanic edifices tectonics hands over (run.py:229)
+VOLCANO_FIELD = "volcano_active"
+
+
+def active_volcanoes(store, grid) -> np.ndarray | None:
+    """The cones (m, extended) of the edifices active at the end of tectonics,
+    or None when the store has none (run.py:232-234)."""
+    has = getattr(store, "has_field", None)
+    return _field(store, VOLCANO_FIELD, grid) if has is not None and has(VOLCANO_FIELD) else None
+
+
+def datum_land_fraction(params, bedrock_interior) -> float:
+    """The land fraction the datum hold keeps (maps.py:1413-1430):
+    ``world.land_fraction``, or in shelf mode (``tectonics.shelf_fraction``
+    > 0, where the land area is an output of tectonics) the share of cells
+    whose bedrock stands at or above 0."""
+    if float(getattr(getattr(params, "tectonics", None), "shelf_fraction", 0.0) or 0.0) > 0.0:
+        return float(np.mean(np.asarray(bedrock_interior) >= 0))
+    return float(params.world.land_fraction)
+
+
 def build_state(store, params, device="cuda") -> gm.ErosionState:
-    """The iteration-0 state from the stage inputs (run.py:237-296, plain path)."""
+    """The iteration-0 state from the stage inputs (run.py:237-296): the
+    bedrock with the active volcanic cones taken off (the stage erodes the
+    ground under them; :func:`run` puts them back at its end), the held land
+    fraction of :func:`datum_land_fraction`."""
     w = params.world
     grid = get_grid(int(w.N_c), int(w.halo), float(w.cell_size_m))
-    st = gm.ErosionState.from_grid(grid, _field(store, "bedrock", grid), _field(store, "hardness", grid),
-                                   _field(store, "precip", grid), _field(store, "evap", grid), _field(store, "uplift", grid),
-                                   device=device)
-    st.land_target = float(w.land_fraction)
+    bed = _field(store, "bedrock", grid)
+    cone = active_volcanoes(store, grid)
+    if cone is not None:
+        bed = bed - cone
+    st = gm.ErosionState.from_grid(grid, bed, _field(store, "hardness", grid), _field(store, "precip", grid),
+                                   _field(store, "evap", grid), _field(store, "uplift", grid), device=device)
+    H, N = grid.H, grid.N
+    st.land_target = datum_land_fraction(params, np.asarray(bed)[:, H:H + N, H:H + N])
     return st
+
+
+def restore_volcanoes(state: gm.ErosionState, cone) -> dict:
+    """Put the active edifices back on top of the eroded surface (run.py:299-311)."""
+    import torch
+
+    if cone is None:
+        return {}
+    add = np.asarray(cone).astype(np.float64) / state.height_unit_m
+    state.height += torch.as_tensor(add, device=state.height.device)
+    c = np.asarray(cone)[state.interior]
+    surf = (state.height + state.sediment)[state.interior].cpu().numpy()
+    on = c > 0.0
+    return {"volcano_cells": int(on.sum()), "volcano_max_m": float(c.max()) if on.any() else 0.0,
+            "volcano_land_cells": int((on & (surf >= 0.0)).sum())}
 
 
 def write_outputs(store, state: gm.ErosionState) -> None:
@@ -359,6 +402,11 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
                 log(f"[erosion] checkpoint -> {p.name}")
     if writer is not None:
         writer.close()
+    # the active volcanic edifices go back on top of what the stage made of the ground under them (run.py:495-499)
+    volc = restore_volcanoes(state, active_volcanoes(store, state.grid))
+    if volc:
+        log(f"[erosion] active volcanoes back on top: {volc['volcano_cells']} cells, max {volc['volcano_max_m']:.0f} m, "
+            f"{volc['volcano_land_cells']} of them land")
     write_outputs(store, state)
     a = state.to_numpy()
     inter = state.interior
@@ -372,4 +420,7 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
             "backend": "b200", "apply": "ordered" if apply == _lib.APPLY_ORDERED else "wave"}
     if rep is not None:
         info["replay_datum_start_m"] = rep["datum_shift"] * u
+    if fill is not None:
+        info["basin_fill"] = fill
+    info.update(volc)
     return info

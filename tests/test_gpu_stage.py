@@ -109,3 +109,34 @@ def test_host_refreshes_are_checkpointed_and_resumed(cuda, tmp_path):
     for n in stage.OUTPUTS:
         again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
         assert again.tobytes() == out[n].tobytes(), n
+
+
+def test_active_volcanoes_are_taken_off_and_put_back(cuda, tmp_path):
+    """A store with active volcanic cones (volcano_active, run.py:229-311):
+    the stage erodes the ground under them and puts them back on top at its
+    end, so its outputs are those of the same run on the bedrock without the
+    cones, with the cones added to the height (float32 metres); the other
+    outputs are untouched."""
+    import dataclasses
+
+    sa, p = _world_store(tmp_path / "a")
+    p = dataclasses.replace(p, erosion=dataclasses.replace(p.erosion, checkpoint_every=0, resume=False))
+    from pgerosion.geometry import get_grid
+
+    grid = get_grid(32, 2, 50.0)
+    bed = stage._field(sa, "bedrock", grid)
+    cone = np.zeros_like(bed)
+    cone[2, 10:13, 14:17] = 900.0
+    cone[4, 20, 8] = 2500.0
+    sa.save_field(stage.VOLCANO_FIELD, cone, grid.H)
+    info = stage.run(sa, p, log=lambda m: None)
+    assert info["volcano_cells"] == 10 and info["volcano_max_m"] == 2500.0
+    sb, _ = _world_store(tmp_path / "b")
+    sb.save_field("bedrock", (bed - cone).astype(np.float32), grid.H)
+    stage.run(sb, p, log=lambda m: None)
+    out = lambda s_, n: np.stack([np.load(s_.coarse / f"{n}.f{k}.npy") for k in range(6)])
+    H, N = grid.H, grid.N
+    ha, hb = out(sa, "height"), out(sb, "height")
+    np.testing.assert_allclose(ha, hb + cone[:, H:H + N, H:H + N], rtol=0, atol=1e-3)
+    for n in ("sediment", "discharge", "momentum"):
+        assert out(sa, n).tobytes() == out(sb, n).tobytes(), n

@@ -39,3 +39,29 @@ def test_small_world_inputs():
     assert w.bedrock.dtype == np.float32 and w.precip.min() == 1.0
     p, P = synth.config_params("small")
     assert P == 65536 and p.erosion.max_steps == 64 and p.world.N_c == 128
+
+
+def test_stage_land_target_and_volcano_field_without_gpu(tmp_path):
+    """The stage driver's host logic (run.py:229-261, maps.py:1413-1430):
+    the held land fraction is world.land_fraction, or in shelf mode the
+    bedrock's own share of cells at or above 0; the active volcanic cones
+    are read from the store only when it has them."""
+    import dataclasses
+
+    from pgerosion import stage
+    from pgerosion.geometry import get_grid
+    from pgerosion.params import TectonicsGroup, WorldGroup, WorldParams
+
+    p = WorldParams(world=WorldGroup(N_c=8, halo=2, land_fraction=0.3))
+    bed = np.array([-1.0, 0.0, 2.0, 3.0])
+    assert stage.datum_land_fraction(p, bed) == 0.3
+    ps = dataclasses.replace(p, tectonics=TectonicsGroup(shelf_fraction=0.1))
+    assert stage.datum_land_fraction(ps, bed) == 0.75
+    store = stage.LocalStore(tmp_path)
+    grid = get_grid(8, 2, 50.0)
+    assert stage.active_volcanoes(store, grid) is None
+    cone = np.zeros((6, grid.NE, grid.NE), np.float32)
+    cone[1, 4, 5] = 1200.0
+    store.save_field(stage.VOLCANO_FIELD, cone, grid.H)
+    got = stage.active_volcanoes(store, grid)
+    assert got is not None and float(got[1, 4, 5]) == 1200.0
