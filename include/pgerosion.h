@@ -552,10 +552,12 @@ PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream);
  * cudaMalloc's latency and implicit synchronisation: no workspace, the
  * scratch is a static device array of PGE_NOALLOC_MAX_CELLS cells (10 MiB,
  * held by every GPU that loads the library until exit).  Grids with more
- * cells than that (F * NE * NE) are rejected with PGE_E_ARG.  The first call
- * on a device looks up the array's device address (make it before any
- * stream capture).  All calls share the array: calls that overlap on the
- * GPU race, so order them. */
+ * cells than that (F * NE * NE) are rejected with PGE_E_ARG, and so is any
+ * grid pge_thermal rejects.  The first call on a device looks up the array's
+ * device address (make it before any stream capture) and keeps it; the kept
+ * address does not survive cudaDeviceReset, so do not call this entry point
+ * again on a device the process has reset.  All calls share the array: calls
+ * that overlap on the GPU race, so order them. */
 #define PGE_NOALLOC_MAX_CELLS 262144
 PGE_API int pge_thermal_noalloc(const PgeGrid *g, PgeState *s, double thermal_rate, double creep_rate, double thermal_max,
                                 double talus_soft, double talus_hard, double dep_floor, void *stream);

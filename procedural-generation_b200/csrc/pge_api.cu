@@ -40,7 +40,9 @@ int cuda_fail(cudaError_t e, const char *where)
     return fail(PGE_E_CUDA, "%s: %s", where, cudaGetErrorString(e));
 }
 
-// the geometry alone (calls that use no workspace)
+}  // namespace
+
+// the geometry alone (calls that use no workspace); shared with pge_static.cu
 int check_shape(const PgeGrid *g)
 {
     if (!g) return fail(PGE_E_ARG, "grid is NULL");
@@ -50,6 +52,8 @@ int check_shape(const PgeGrid *g)
     if ((long long)g->F * NE * NE >= (1LL << 31)) return fail(PGE_E_ARG, "grid too large for int32 cell indices");
     return PGE_OK;
 }
+
+namespace {
 
 int check_grid(const PgeGrid *g)
 {

@@ -68,6 +68,8 @@ struct Layout {
 
 // records the calling thread's error message (read back with pge_last_error) and returns code
 int pge_set_error(int code, const char *fmt, ...);
+// the grid's own shape rules (faces, sizes, halo, int32 cell indices): PGE_OK or PGE_E_ARG with the message set
+int check_shape(const PgeGrid *g);
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 

@@ -13,7 +13,11 @@
 // name is only a host-side stand-in, not a device address.  So the first
 // call on each device, with that device current, looks its device address
 // up with cudaGetSymbolAddress (checked) and keeps it for later calls on the
-// same device.  That first call should come before any stream capture.
+// same device.  That first call should come before any stream capture.  The
+// kept address belongs to the device's primary context: after
+// cudaDeviceReset (or anything else that destroys that context) the module
+// is loaded again and the array may move, so a process that resets a device
+// must not call this entry point on it again.
 //
 // Every call shares the one array and it keeps the last call's contents;
 // nothing in it needs to start at zero (each pass writes every scratch value
@@ -58,7 +62,8 @@ extern "C" PGE_API int pge_thermal_noalloc(const PgeGrid *g, PgeState *s, double
                                            double thermal_max, double talus_soft, double talus_hard, double dep_floor, void *stream)
 {
     using namespace pge;
-    if (!g || g->F < 1 || g->N < 2 || g->H < 1) return pge_set_error(PGE_E_ARG, "thermal_noalloc: bad grid");
+    int r;
+    if ((r = check_shape(g))) return r;  // the same grid rules as pge_thermal
     const long long NE = g->N + 2LL * g->H;
     const long long n = (long long)g->F * NE * NE;
     if (n > PGE_NOALLOC_MAX_CELLS)

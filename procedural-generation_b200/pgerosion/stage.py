@@ -60,6 +60,18 @@ class LocalStore:
     def has_field(self, name: str) -> bool:
         return (self.coarse / f"{name}.f0.npy").exists()
 
+    def stage_info(self, stage: str) -> dict | None:
+        """The stage's entry in ``manifest.json`` (``{"stages": {stage: {...,
+        "hash": ...}}}``, the bake's WorldStore.stage_info,
+        world_store.py:93-94), or None without one."""
+        m = self.root / "manifest.json"
+        if not m.exists():
+            return None
+        try:
+            return json.loads(m.read_text()).get("stages", {}).get(stage)
+        except json.JSONDecodeError:
+            return None
+
     def load_field(self, name: str, grid, vector: bool = False) -> np.ndarray:
         """The six faces with their halos filled by the grid's cubic exchange
         (FaceField.load, bake/globe/field.py:327-338)."""
@@ -76,20 +88,43 @@ def _field(store, name, grid):
     return np.asarray(getattr(v, "data", v))
 
 
-def ckpt_hash(params, apply: int) -> str:
-    """World and erosion parameters (run-control knobs normalised out, as
-    run.py:68-97 does), the backend token, its version and the apply mode."""
+def _group_dict(g) -> dict:
+    return dataclasses.asdict(g) if dataclasses.is_dataclass(g) else dict(vars(g))
+
+
+def _short_hash(obj) -> str:
+    return hashlib.sha256(json.dumps(obj, sort_keys=True, default=str).encode()).hexdigest()[:16]
+
+
+#: the upstream stages whose parameters and outputs a checkpoint depends on (run.py:89-96)
+UPSTREAM_STAGES = ("tectonics", "climate")
+
+
+def ckpt_hash(params, apply: int, store=None) -> str:
+    """Everything a checkpoint depends on, as run.py:68-97 hashes it: the
+    world and erosion groups (run-control knobs normalised out; the iteration
+    count kept in replay mode, where the start state depends on it), the
+    tectonics and climate groups, and -- with a ``store`` that answers
+    ``stage_info(stage)`` (the bake's ``WorldStore``, world_store.py:93-94)
+    -- the manifest hashes of the tectonics and climate outputs, so that a
+    re-baked upstream stage with unchanged parameters invalidates the
+    checkpoint.  Then this backend's token, its version (the counterpart of
+    ``particle.KERNEL_VERSION``) and the apply mode."""
     ep = erosion_group(params)
-    e = dataclasses.asdict(ep) if dataclasses.is_dataclass(ep) else dict(vars(ep))
+    e = _group_dict(ep)
     replay = str(e.get("uplift_mode", "stack")) == "replay"
     for k in ("checkpoint_every", "quicklook_every", "resume"):
         e.pop(k, None)
     if not replay:
         e["iterations"] = 0
-    w = params.world
-    wd = dataclasses.asdict(w) if dataclasses.is_dataclass(w) else dict(vars(w))
-    s = json.dumps({"world": wd, "erosion": e}, sort_keys=True, default=str)
-    return hashlib.sha256(s.encode()).hexdigest()[:16] + f":b200v{BACKEND_VERSION}:apply{apply}"
+    own = _short_hash({"world": _group_dict(params.world), "erosion": e})
+    groups = {s: _group_dict(getattr(params, s)) for s in UPSTREAM_STAGES if getattr(params, s, None) is not None}
+    up = ""
+    info_of = getattr(store, "stage_info", None) if store is not None else None
+    if info_of is not None:
+        for s in UPSTREAM_STAGES:
+            up += ":" + str((info_of(s) or {}).get("hash", ""))
+    return own + ":" + _short_hash(groups) + up + f":b200v{BACKEND_VERSION}:apply{apply}"
 
 
 #: the evolving arrays a checkpoint holds (run.py:100-139); iso_acc only while isostasy is on
@@ -140,8 +175,8 @@ def _write_checkpoint(d: Path, it: int, arrays: dict, meta: dict) -> Path:
     return p
 
 
-def _ckpt_meta(state, params, apply) -> dict:
-    return {"iteration": state.iteration, "params_hash": ckpt_hash(params, apply), "height_unit_m": state.height_unit_m,
+def _ckpt_meta(state, params, apply, store=None) -> dict:
+    return {"iteration": state.iteration, "params_hash": ckpt_hash(params, apply, store), "height_unit_m": state.height_unit_m,
             "time": time.strftime("%Y-%m-%dT%H:%M:%S")}
 
 
@@ -154,7 +189,7 @@ def save_checkpoint(store, state: gm.ErosionState, params, apply: int) -> Path:
     for k in _state_fields(state):
         arrays[k] = getattr(state, k).detach().cpu().numpy()
     _lake_arrays(arrays)
-    return _write_checkpoint(d, state.iteration, arrays, _ckpt_meta(state, params, apply))
+    return _write_checkpoint(d, state.iteration, arrays, _ckpt_meta(state, params, apply, store))
 
 
 class CheckpointWriter:
@@ -172,6 +207,7 @@ class CheckpointWriter:
         from concurrent.futures import ThreadPoolExecutor
 
         self.dir = Path(store.checkpoint_dir)
+        self.store = store
         self._ex = ThreadPoolExecutor(max_workers=1)
         self._pending = None
         self._snap: dict = {}
@@ -199,7 +235,7 @@ class CheckpointWriter:
                 self._host[k].copy_(self._snap[k], non_blocking=True)
             copied = torch.cuda.Event()
             copied.record()
-        meta = _ckpt_meta(state, params, apply)
+        meta = _ckpt_meta(state, params, apply, self.store)
         it = state.iteration
 
         def write():
@@ -251,7 +287,7 @@ def find_checkpoint(store, params, apply: int, max_iteration: int | None = None)
     d = Path(store.checkpoint_dir)
     if not d.exists():
         return None
-    want = ckpt_hash(params, apply)
+    want = ckpt_hash(params, apply, store)
     best = None
     for p in d.glob("erosion_iter*.npz"):
         if not _CKPT_RE.search(p.name):

@@ -986,4 +986,9 @@ def main(bake: str, only: str | None = None):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/bake", sys.argv[2] if len(sys.argv) > 2 else None)
+    import os
+
+    bake = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PGE_BAKE_DIR")
+    if not bake:
+        sys.exit("usage: gen_golden.py <bake checkout> [fixture]   (or set PGE_BAKE_DIR)")
+    main(bake, sys.argv[2] if len(sys.argv) > 2 else None)

@@ -22,13 +22,17 @@ def test_cubesphere_vectors_bit_exact():
 
 def test_reference_vector_file_if_present():
     """The bake's own checked-in vector file (tests/data/cubesphere_vectors.bin),
-    read when the bake is mounted next to this build."""
+    read when the environment variable PGE_BAKE_DIR names a bake checkout."""
+    import os
     import struct
     from pathlib import Path
 
-    path = Path("/root/reference/bake/tests/data/cubesphere_vectors.bin")
+    bake = os.environ.get("PGE_BAKE_DIR")
+    if not bake:
+        pytest.skip("PGE_BAKE_DIR not set (a bake checkout with tests/data/cubesphere_vectors.bin)")
+    path = Path(bake) / "tests" / "data" / "cubesphere_vectors.bin"
     if not path.exists():
-        pytest.skip("bake project not mounted")
+        pytest.skip(f"{path} not found")
     rec_t = np.dtype([("face", "<i4"), ("u", "<f8"), ("v", "<f8"), ("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("face2", "<i4"),
                       ("u2", "<f8"), ("v2", "<f8")])
     with open(path, "rb") as fh:

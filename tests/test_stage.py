@@ -25,6 +25,34 @@ def test_hash_normalises_run_control_knobs():
     assert stage.ckpt_hash(a, 0) != stage.ckpt_hash(a, 1)  # the apply mode is part of the identity
 
 
+def test_hash_covers_upstream_groups_and_outputs(tmp_path):
+    """A re-baked tectonics or climate output (same parameters, new manifest
+    hash) and a changed tectonics group both refuse the old checkpoint, as
+    run.py:68-97's hash does."""
+    st = stage.LocalStore(tmp_path)
+    d = st.checkpoint_dir
+    d.mkdir(parents=True)
+    p = _params(uplift_mode="stack")
+
+    def manifest(tect, clim):
+        (tmp_path / "manifest.json").write_text(json.dumps(
+            {"stages": {"tectonics": {"done": True, "hash": tect}, "climate": {"done": True, "hash": clim}}}))
+
+    manifest("t1", "c1")
+    h = stage.ckpt_hash(p, 0, st)
+    assert h != stage.ckpt_hash(p, 0)  # the upstream output hashes are part of it
+    _fake_ckpt(d, 4, h)
+    assert stage.find_checkpoint(st, p, 0)[1]["iteration"] == 4
+    manifest("t2", "c1")  # tectonics re-baked with the same parameters
+    assert stage.find_checkpoint(st, p, 0) is None
+    manifest("t1", "c2")  # climate re-baked
+    assert stage.find_checkpoint(st, p, 0) is None
+    manifest("t1", "c1")
+    assert stage.find_checkpoint(st, p, 0)[1]["iteration"] == 4
+    q = dataclasses.replace(p, tectonics=dataclasses.replace(p.tectonics, shelf_fraction=0.25))
+    assert stage.find_checkpoint(st, q, 0) is None  # a changed tectonics group
+
+
 def _fake_ckpt(d, it, h):
     p = d / f"erosion_iter{it:04d}.npz"
     np.savez(p, height=np.zeros(1))
@@ -36,7 +64,7 @@ def test_prune_and_find(tmp_path):
     d = st.checkpoint_dir
     d.mkdir(parents=True)
     p = _params(uplift_mode="stack")
-    h = stage.ckpt_hash(p, 0)
+    h = stage.ckpt_hash(p, 0, st)
     for it in (3, 6, 9):
         _fake_ckpt(d, it, h)
     _fake_ckpt(d, 1, "other")

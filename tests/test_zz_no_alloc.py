@@ -68,3 +68,9 @@ def test_thermal_noalloc_refuses_grids_beyond_its_scratch(cuda):
                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == _lib.PGE_E_ARG
     assert "exceed the static scratch" in _lib.last_error()
+    # the same grid rules as pge_thermal: a sphere has six faces, the halo fits the face
+    for bad in (_lib.PgeGrid(F=1, N=64, H=2, spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1),
+                _lib.PgeGrid(F=6, N=4, H=3, spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)):
+        rc = L.pge_thermal_noalloc(ctypes.byref(bad), ctypes.byref(st.pge_state()), 0.5, 0.02, 1.0, 0.6, 1.2, 0.02,
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == _lib.PGE_E_ARG, "a grid pge_thermal refuses must be refused here too"
