@@ -546,6 +546,27 @@ PGE_API int pge_adjoint_pass(const PgeGrid *g, const PgeState *s, const PgeSpawn
                              double *ebar, double *pbar, PgeStats *stats, void *ws, size_t ws_bytes, void *stream);
 PGE_API int pge_halo_adjoint(const PgeHalo *h, double *zbar, void *stream);
 
+/* Parity hooks of the float64 trace's own face-crossing code.
+ *
+ * pge_cubesphere_map runs, on the device, the functions the float64 droplet
+ * kernel crosses cube faces with, over n records (device arrays):
+ *   op 0: to_sphere(face[i], uv[2i], uv[2i+1]) -> xyz[3i..3i+2]
+ *         (cubesphere.to_sphere, globe/cubesphere.py:71-88)
+ *   op 1: from_sphere(xyz[3i..3i+2]) -> face[i], uv[2i..2i+1]
+ *         (cubesphere.from_sphere, globe/cubesphere.py:97-111)
+ *   op 2: transfer_velocity(face[i], uv[2i..], ab[2i..]) in place
+ *         (cubesphere.transfer_velocity, globe/cubesphere.py:204-220)
+ * pge_crmath (device arrays) and pge_crmath_host (host arrays) evaluate the
+ * kernel's float64 tan, atan, sin, cos (op 0..3): double-double evaluations
+ * rounded once, so that they give the C library's results that the
+ * reference's math.tan / math.atan (cubesphere.py:73-74, 110-111) and
+ * math.cos / math.sin (erosion/particle.py:400-401) return wherever those
+ * are correctly rounded.  pge_crmath's op 4..7 evaluate CUDA's own tan,
+ * atan, sin, cos instead, for comparison (the trace does not use them). */
+PGE_API int pge_cubesphere_map(int32_t op, int64_t n, int32_t *face, double *uv, double *ab, double *xyz, void *stream);
+PGE_API int pge_crmath(int32_t op, int64_t n, const double *x, double *y, void *stream);
+PGE_API int pge_crmath_host(int32_t op, int64_t n, const double *x, double *y);
+
 /* No counterpart in the reference.  pge_thermal for callers that cannot
  * allocate device memory -- a host that owns the whole device heap through
  * its own pool and forbids other allocations, or a loop that must not pay

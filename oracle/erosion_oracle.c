@@ -955,3 +955,12 @@ void orc_spawn_cells(int64_t M, const double *cdf, int64_t P, const double *u, i
         out[p] = k;
     }
 }
+
+/* The C library's tan / atan / sin / cos (op 0..3) over an array: the values
+ * the reference's numba code and this oracle's crossing compute, for checking
+ * the library's own double-double versions against them. */
+void orc_libm(int op, int64_t n, const double *x, double *y)
+{
+    for (int64_t i = 0; i < n; i++)
+        y[i] = op == 0 ? tan(x[i]) : op == 1 ? atan(x[i]) : op == 2 ? sin(x[i]) : cos(x[i]);
+}

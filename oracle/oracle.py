@@ -98,6 +98,14 @@ def _p(a: np.ndarray):
     return ctypes.c_void_p(a.ctypes.data)
 
 
+def libm(op: int, x) -> np.ndarray:
+    """The C library's tan / atan / sin / cos (op 0..3) of a float64 array."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.empty_like(x)
+    lib().orc_libm(ctypes.c_int(int(op)), ctypes.c_int64(x.size), _p(x), _p(y))
+    return y
+
+
 def change_list_cap(max_steps: int, lateral: bool = False) -> int:
     return int(lib().orc_change_list_cap(int(max_steps), int(bool(lateral))))
 

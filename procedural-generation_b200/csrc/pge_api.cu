@@ -749,4 +749,26 @@ PGE_API int pge_halo_gather(const PgeHalo *h, double *field, int32_t vector, voi
     return e == cudaSuccess ? PGE_OK : cuda_fail(e, "halo_gather");
 }
 
+PGE_API int pge_crmath(int32_t op, int64_t n, const double *x, double *y, void *stream)
+{
+    if (op < 0 || op > 7 || n < 0 || (n > 0 && (!x || !y))) return fail(PGE_E_ARG, "crmath: bad op, size or pointer");
+    cudaError_t e = launch_crmath(op, n, x, y, (cudaStream_t)stream);
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "crmath");
+}
+
+PGE_API int pge_crmath_host(int32_t op, int64_t n, const double *x, double *y)
+{
+    if (op < 0 || op > 3 || n < 0 || (n > 0 && (!x || !y))) return fail(PGE_E_ARG, "crmath_host: bad op, size or pointer");
+    crmath_host(op, n, x, y);
+    return PGE_OK;
+}
+
+PGE_API int pge_cubesphere_map(int32_t op, int64_t n, int32_t *face, double *uv, double *ab, double *xyz, void *stream)
+{
+    if (op < 0 || op > 2 || n < 0) return fail(PGE_E_ARG, "cubesphere_map: bad op or size");
+    if (n > 0 && (!face || !uv || (op == 2 && !ab) || (op < 2 && !xyz))) return fail(PGE_E_ARG, "cubesphere_map: NULL pointer");
+    cudaError_t e = launch_cubesphere(op, n, face, uv, ab, xyz, (cudaStream_t)stream);
+    return e == cudaSuccess ? PGE_OK : cuda_fail(e, "cubesphere_map");
+}
+
 }  // extern "C"

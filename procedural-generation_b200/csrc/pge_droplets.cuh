@@ -31,6 +31,7 @@
 #pragma once
 #include <cstdint>
 
+#include "pge_crmath.cuh"
 #include "pge_internal.cuh"
 
 #if !defined(PGE_REAL) || !defined(PGE_VARIANT)
@@ -57,6 +58,17 @@ constexpr double kPi = 3.14159265358979323846;
 __device__ __forceinline__ R half_pi() { return R(kPi / 2.0); }
 __device__ __forceinline__ R two_over_pi() { return R(2.0 / kPi); }
 
+// tan / atan / sin / cos of the droplet precision: float64 rounds like the C library the reference
+// calls (correctly rounded double-double evaluations, pge_crmath.cuh); float32 takes the builtins
+__device__ __forceinline__ double m_tan(double x) { return cr::d_tan(x); }
+__device__ __forceinline__ double m_atan(double x) { return cr::d_atan(x); }
+__device__ __forceinline__ double m_sin(double x) { return cr::d_sin(x); }
+__device__ __forceinline__ double m_cos(double x) { return cr::d_cos(x); }
+__device__ __forceinline__ float m_tan(float x) { return tanf(x); }
+__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
+__device__ __forceinline__ float m_sin(float x) { return sinf(x); }
+__device__ __forceinline__ float m_cos(float x) { return cosf(x); }
+
 // ---------------------------------------------------------------------------
 // cube-sphere mapping in droplet precision (cubesphere.py:70-220)
 // ---------------------------------------------------------------------------
@@ -74,8 +86,8 @@ __device__ void to_sphere(int face, R u, R v, R &x, R &y, R &z)
 {
     R r[3], up[3], n[3];
     face_axes(face, r, up, n);
-    R s = tan((u - R(0.5)) * half_pi());
-    R t = tan((v - R(0.5)) * half_pi());
+    R s = m_tan((u - R(0.5)) * half_pi());
+    R t = m_tan((v - R(0.5)) * half_pi());
     R qx = n[0] + s * r[0] + t * up[0];
     R qy = n[1] + s * r[1] + t * up[1];
     R qz = n[2] + s * r[2] + t * up[2];
@@ -97,8 +109,8 @@ __device__ int from_sphere(R x, R y, R z, R &u, R &v)
     R d = x * n[0] + y * n[1] + z * n[2];
     R s = (x * r[0] + y * r[1] + z * r[2]) / d;
     R t = (x * up[0] + y * up[1] + z * up[2]) / d;
-    u = atan(s) * two_over_pi() + R(0.5);
-    v = atan(t) * two_over_pi() + R(0.5);
+    u = m_atan(s) * two_over_pi() + R(0.5);
+    v = m_atan(t) * two_over_pi() + R(0.5);
     return face;
 }
 
@@ -106,7 +118,7 @@ __device__ void jacobian(int face, R u, R v, R J[6])
 {
     R r[3], up[3], n[3];
     face_axes(face, r, up, n);
-    R s = tan((u - R(0.5)) * half_pi()), t = tan((v - R(0.5)) * half_pi());
+    R s = m_tan((u - R(0.5)) * half_pi()), t = m_tan((v - R(0.5)) * half_pi());
     R dsdu = half_pi() * (R(1) + s * s);
     R dtdv = half_pi() * (R(1) + t * t);
     R qx = n[0] + s * r[0] + t * up[0];
@@ -642,8 +654,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     sb = R(0);
                     if (sed > R(0)) {
                         const R dir = R(a.sp_dir[d]);
-                        sa = cos(dir);
-                        sb = sin(dir);
+                        sa = m_cos(dir);
+                        sb = m_sin(dir);
                     }
                     step = uphill = sea_steps = nring = 0;
                     in_sea = has_hprev = in_lake = false;

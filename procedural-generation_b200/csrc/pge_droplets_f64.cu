@@ -78,3 +78,79 @@ int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger)
     return n > 0 ? n : 1;
 }
 }  // namespace pge
+
+// ---------------------------------------------------------------------------
+// parity hooks: the float64 droplet kernel's own face-crossing and trig code,
+// run over arrays (pge_cubesphere_map, pge_crmath)
+// ---------------------------------------------------------------------------
+namespace pge {
+namespace {
+__global__ void crmath_kernel(int op, long long n, const double *x, double *y)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        switch (op) {
+        case 0: y[i] = cr::d_tan(v); break;
+        case 1: y[i] = cr::d_atan(v); break;
+        case 2: y[i] = cr::d_sin(v); break;
+        case 3: y[i] = cr::d_cos(v); break;
+        // CUDA's own functions, for comparison only (the trace does not use them)
+        case 4: y[i] = tan(v); break;
+        case 5: y[i] = atan(v); break;
+        case 6: y[i] = sin(v); break;
+        default: y[i] = cos(v); break;
+        }
+    }
+}
+
+__global__ void cubesphere_kernel(int op, long long n, int32_t *face, double *uv, double *ab, double *xyz)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (op == 0) {
+            double x, y, z;
+            f64::to_sphere(face[i], uv[2 * i], uv[2 * i + 1], x, y, z);
+            xyz[3 * i] = x;
+            xyz[3 * i + 1] = y;
+            xyz[3 * i + 2] = z;
+        } else if (op == 1) {
+            double u, v;
+            face[i] = f64::from_sphere(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], u, v);
+            uv[2 * i] = u;
+            uv[2 * i + 1] = v;
+        } else {
+            double u = uv[2 * i], v = uv[2 * i + 1], a = ab[2 * i], b = ab[2 * i + 1];
+            face[i] = f64::transfer_velocity(face[i], u, v, a, b);
+            uv[2 * i] = u;
+            uv[2 * i + 1] = v;
+            ab[2 * i] = a;
+            ab[2 * i + 1] = b;
+        }
+    }
+}
+}  // namespace
+
+cudaError_t launch_crmath(int op, long long n, const double *x, double *y, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+    crmath_kernel<<<(int)blocks, 256, 0, st>>>(op, n, x, y);
+    return cudaPeekAtLastError();
+}
+
+cudaError_t launch_cubesphere(int op, long long n, int32_t *face, double *uv, double *ab, double *xyz, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096;
+    cubesphere_kernel<<<(int)blocks, 256, 0, st>>>(op, n, face, uv, ab, xyz);
+    return cudaPeekAtLastError();
+}
+
+// the same evaluations on the host (this file's host code is compiled without contraction)
+void crmath_host(int op, long long n, const double *x, double *y)
+{
+    for (long long i = 0; i < n; i++) {
+        const double v = x[i];
+        y[i] = op == 0 ? cr::cr_tan(v) : op == 1 ? cr::cr_atan(v) : op == 2 ? cr::cr_sin(v) : cr::cr_cos(v);
+    }
+}
+}  // namespace pge

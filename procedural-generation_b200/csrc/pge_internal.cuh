@@ -133,5 +133,10 @@ int droplet_blocks_per_sm_f64_tape(int threads);
 cudaError_t launch_droplets_f32(const DropArgs &a, int blocks, int threads, cudaStream_t st);
 int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger = true);
 int droplet_blocks_per_sm_f32(int threads, int minb, bool ledger = true);
+// parity hooks of the float64 trace's own code (pge_droplets_f64.cu): op 0..3 = tan, atan, sin, cos
+// (4..7: CUDA's own, device only); the cube-sphere op 0 = to_sphere, 1 = from_sphere, 2 = transfer_velocity
+cudaError_t launch_crmath(int op, long long n, const double *x, double *y, cudaStream_t st);
+void crmath_host(int op, long long n, const double *x, double *y);
+cudaError_t launch_cubesphere(int op, long long n, int32_t *face, double *uv, double *ab, double *xyz, cudaStream_t st);
 
 }  // namespace pge

@@ -28,7 +28,7 @@ EXPORTS = (
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
     "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base", "pge_glacial",
     "pge_window_lakes", "pge_lake_balance", "pge_basin_fill",
-    "pge_window_lake_balance",
+    "pge_window_lake_balance", "pge_cubesphere_map", "pge_crmath", "pge_crmath_host",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
@@ -142,6 +142,9 @@ def load(path: str | os.PathLike | None = None):
     L.pge_glacial.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_f64, c_i32, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp,
                               ctypes.c_size_t, c_vp]
     L.pge_sea_base.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_vp, c_f64, c_vp, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]
+    L.pge_cubesphere_map.argtypes = [c_i32, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp]
+    L.pge_crmath.argtypes = [c_i32, c_i64, c_vp, c_vp, c_vp]
+    L.pge_crmath_host.argtypes = [c_i32, c_i64, c_vp, c_vp]
     for n in EXPORTS:
         if n not in ("pge_version", "pge_last_error", "pge_workspace_bytes"):
             getattr(L, n).restype = ctypes.c_int

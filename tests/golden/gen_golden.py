@@ -11,6 +11,9 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
 * ``cubesphere_vectors.npz`` -- to_sphere / from_sphere / transfer_velocity
   of the scalar functions the particle kernel uses (cubesphere.py:70-220),
   on uniform points plus points within 1e-4 of face edges and corners.
+* ``cubesphere_ref_vectors.npz`` -- the bake's own vector file
+  (tests/data/cubesphere_vectors.bin: to_sphere / from_sphere records its
+  scalar functions reproduce bit for bit), copied into an npz.
 * ``halo_N8_H2.npz`` -- the Grid's halo tables, owner and metric at N=8, H=2,
   and SHA-256 digests of the tables at two larger grids.
 * ``trace_isolated.npz`` -- a six-face N=48 world after three reference
@@ -98,6 +101,26 @@ def gen_vectors(cs):
     np.savez_compressed(HERE / "cubesphere_vectors.npz", face=face.astype(np.int32), u=u, v=v, xyz=xyz, face2=f2, u2=u2, v2=v2,
                         t_face=tf.astype(np.int32), t_u=tu, t_v=tv, t_a=ta, t_b=tb, t_face2=tr[:, 0].astype(np.int32),
                         t_out=tr[:, 1:].astype(np.float64))
+
+
+def gen_ref_vectors(bake: str):
+    """The bake's own checked-in vector file (tests/data/cubesphere_vectors.bin:
+    "CSV2", a count, then records of face, u, v, x, y, z, face2, u2, v2 that
+    its scalar to_sphere / from_sphere reproduce bit for bit,
+    bake/tests/test_cubesphere.py:376-402), kept as an npz so the device
+    tests can read it where the bake is not mounted."""
+    import struct
+
+    rec_t = np.dtype([("face", "<i4"), ("u", "<f8"), ("v", "<f8"), ("x", "<f8"), ("y", "<f8"), ("z", "<f8"), ("face2", "<i4"),
+                      ("u2", "<f8"), ("v2", "<f8")])
+    with open(Path(bake) / "tests" / "data" / "cubesphere_vectors.bin", "rb") as fh:
+        assert fh.read(4) == b"CSV2"
+        (K,) = struct.unpack("<i", fh.read(4))
+        rec = np.frombuffer(fh.read(), dtype=rec_t)
+    assert rec.shape[0] == K
+    np.savez_compressed(HERE / "cubesphere_ref_vectors.npz", face=rec["face"].astype(np.int32), u=rec["u"], v=rec["v"],
+                        xyz=np.stack([rec["x"], rec["y"], rec["z"]], 1), face2=rec["face2"].astype(np.int32), u2=rec["u2"],
+                        v2=rec["v2"])
 
 
 def gen_halo(cs):
@@ -964,7 +987,7 @@ def gen_lake_fill_steps(cs, maps, pk, WorldParams):
 
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
-    gens = {"vectors": lambda: gen_vectors(cs), "halo": lambda: gen_halo(cs),
+    gens = {"vectors": lambda: gen_vectors(cs), "ref_vectors": lambda: gen_ref_vectors(bake), "halo": lambda: gen_halo(cs),
             "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
