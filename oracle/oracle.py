@@ -106,6 +106,60 @@ def libm(op: int, x) -> np.ndarray:
     return y
 
 
+def brush_weights(r: int) -> np.ndarray:
+    """The brush's integer weights (2r+1, 2r+1): 1024 x max(0, r + 1 - |(di, dj)|), rounded."""
+    d = np.arange(-r, r + 1, dtype=np.float64)
+    v = (r + 1) - np.sqrt(d[:, None] ** 2 + d[None, :] ** 2)
+    return np.where(v > 0.0, np.floor(1024.0 * v + 0.5), 0.0).astype(np.int64)
+
+
+def brush_spread(acc, mask, N, H, r, spherical=True):
+    """A net change field (F, NE, NE) spread by the erode / deposit brush of the
+    library's wave apply (no reference counterpart): every cell's change goes
+    to the active cells of its face within distance < r + 1 (the interior ones
+    on the sphere), in proportion to the weights; float64, no rounding to
+    fixed point.  Linear, so spreading each entry's change or each cell's sum
+    is the same up to the library's 2^-40 truncation."""
+    if r <= 0:
+        return acc.copy()
+    NE = acc.shape[1]
+    q = brush_weights(r)
+    lo, hi = (H, H + N) if spherical else (0, NE)
+    act = mask == MASK_ACTIVE
+    valid = np.zeros_like(act)
+    valid[:, lo:hi, lo:hi] = act[:, lo:hi, lo:hi]
+    Q = np.zeros(acc.shape)  # each cell's total weight over its valid footprint (the cell itself always counts)
+    for di in range(-r, r + 1):
+        for dj in range(-r, r + 1):
+            w = q[di + r, dj + r]
+            if w == 0:
+                continue
+            if di == 0 and dj == 0:
+                Q += w
+                continue
+            sh = np.zeros_like(valid)
+            i0, i1 = max(0, -di), min(NE, NE - di)
+            j0, j1 = max(0, -dj), min(NE, NE - dj)
+            sh[:, i0:i1, j0:j1] = valid[:, i0 + di:i1 + di, j0 + dj:j1 + dj]
+            Q += w * sh
+    out = np.zeros_like(acc)
+    src = np.where(acc != 0.0, acc / np.where(Q > 0, Q, 1.0), 0.0)
+    for di in range(-r, r + 1):
+        for dj in range(-r, r + 1):
+            w = q[di + r, dj + r]
+            if w == 0:
+                continue
+            if di == 0 and dj == 0:
+                out += w * src
+                continue
+            i0, i1 = max(0, -di), min(NE, NE - di)
+            j0, j1 = max(0, -dj), min(NE, NE - dj)
+            part = np.zeros_like(acc)
+            part[:, i0 + di:i1 + di, j0 + dj:j1 + dj] = w * src[:, i0:i1, j0:j1]
+            out += np.where(valid, part, 0.0)
+    return out
+
+
 def change_list_cap(max_steps: int, lateral: bool = False) -> int:
     return int(lib().orc_change_list_cap(int(max_steps), int(bool(lateral))))
 

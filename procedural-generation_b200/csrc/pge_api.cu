@@ -98,6 +98,10 @@ int check_params(const PgeGrid *g, const PgeParams *p)
         return fail(PGE_E_ARG, "threads_per_block must be a multiple of 32 in 32..256");
     if (p->trace_lanes < 0 || p->trace_lanes > 32) return fail(PGE_E_ARG, "trace_lanes %d outside 0..32", p->trace_lanes);
     if (p->apply_lanes < 0 || p->apply_lanes > 32) return fail(PGE_E_ARG, "apply_lanes %d outside 0..32", p->apply_lanes);
+    if (p->brush_radius < 0 || p->brush_radius > PGE_BRUSH_MAX_RADIUS)
+        return fail(PGE_E_ARG, "brush_radius %d outside 0..%d", p->brush_radius, PGE_BRUSH_MAX_RADIUS);
+    if (p->brush_radius > 0 && p->apply != PGE_APPLY_WAVE)
+        return fail(PGE_E_UNSUPPORTED, "the brush (brush_radius > 0) spreads changes with the wave apply's integer sums");
     return PGE_OK;
 }
 
@@ -159,6 +163,8 @@ Layout layout(const PgeGrid &g)
     L.partial = take(64 * 1024);
     L.thermal = take(40 * L.ncell);
     L.flags = take(8 * L.ncell);
+    L.pwv = take(8 * L.ncell);                  // compacted values of a pairwise sum / the spawn weights' integers
+    L.pwnode = take(pairwise_scratch_bytes());  // the pairwise sum's tree
     // ordered apply
     L.cap = change_list_cap(g.max_steps);
     L.max_wave = g.max_wave;
@@ -270,6 +276,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.ledger = 1;
         a.minb = minb;
         a.lanes = 32;
+        a.brush_r = p->brush_radius;
+        if (a.brush_r > 0) brush_weights(a.brush_r, a.brush_q);
         unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
         const long long wave = p->wave;
         const long long nw = (P + wave - 1) / wave;
@@ -331,7 +339,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.segscan = ws_ptr<int32_t>(ws, lay.w_segscan);
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
-            oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
+            oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 0;  // 0: the fed apply
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);
             const long long rec_warps =
                 (long long)sm_count() * (lateral ? droplet_blocks_per_sm_f64_lateral(32, false, s->route != nullptr)
@@ -499,6 +507,7 @@ PGE_API int pge_trace_apply_tape(const PgeGrid *g, PgeState *s, const PgeSpawns 
     if (p->apply != PGE_APPLY_WAVE || p->precision != PGE_PREC_F64 || p->use_erode_cap)
         return fail(PGE_E_UNSUPPORTED, "the tape records a float64 wave-apply pass without the erode cap");
     if (!tape->state || !tape->bits || !tape->entry || !tape->count || !tape->wave_acc) return fail(PGE_E_ARG, "tape has a NULL array");
+    if (p->brush_radius > 0) return fail(PGE_E_UNSUPPORTED, "the adjoint's tape does not differentiate the brush");
     const long long nw = (sp->count + p->wave - 1) / p->wave;
     if (tape->droplets < sp->count || tape->steps < p->max_steps || tape->entries < p->max_steps + SPREAD || tape->waves < nw)
         return fail(PGE_E_ARG, "tape too small: %lld rows x %d steps x %d entries x %lld waves for %lld droplets, max_steps %d, "

@@ -20,6 +20,7 @@
 //   acc4[c] = (terrain change 2^-40, discharge track 2^-32, momentum a, b 2^-32)
 //   pend[c] = stockpile 2^-40
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -59,7 +60,7 @@ __device__ __forceinline__ void red_add(long long *p, long long v)
 // ---------------------------------------------------------------------------
 struct Layout {
     size_t cellA, cellB, live, metric8, route2, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
-        partial, thermal, flags, total;
+        partial, thermal, flags, pwv, pwnode, total;
     // ordered apply (exact mode): one wave's change lists and ranks
     size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_desc, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
         w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, w_act, hand, terr, error;
@@ -119,7 +120,20 @@ struct DropArgs {
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
+    int brush_r;                      // the erode / deposit brush's radius (0: one cell)
+    short brush_q[(2 * PGE_BRUSH_MAX_RADIUS + 1) * (2 * PGE_BRUSH_MAX_RADIUS + 1)];  // its weights, row-major
 };
+
+// the brush's integer weights: PGE_BRUSH_SCALE x max(0, r + 1 - |(di, dj)|) rounded, (2r+1)^2 of them
+inline void brush_weights(int r, short *q)
+{
+    const int w = 2 * r + 1;
+    for (int di = -r; di <= r; di++)
+        for (int dj = -r; dj <= r; dj++) {
+            const double v = (double)(r + 1) - sqrt((double)(di * di + dj * dj));
+            q[(di + r) * w + dj + r] = (short)(v > 0.0 ? llround(PGE_BRUSH_SCALE * v) : 0);
+        }
+}
 
 // launchers of the two precisions (separate translation units: the float64
 // one is compiled without FMA contraction so it rounds like the reference)

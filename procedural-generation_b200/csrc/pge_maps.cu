@@ -13,6 +13,7 @@
 
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include "pge_internal.cuh"
 #include "pge_maps.cuh"
@@ -416,59 +417,190 @@ void thermal_on_scratch(const PgeGrid &g, PgeState &s, double *tb, long long n, 
     }
 }
 
-// ---------------------------------------------------------------------------
-// deterministic reductions (fixed block count, fixed tree order)
-// ---------------------------------------------------------------------------
-constexpr int RED_BLOCKS = 1024;
+struct UpliftValue {
+    const double *u;
+    double cap;
+    int use_cap;
+    __device__ __forceinline__ double operator()(const long long c) const
+    {
+        const double v = u[c];
+        return use_cap && v > cap ? cap : v;
+    }
+};
 
-__global__ void uplift_sum_kernel(long long ncell, int NE, int H, int N, const double *u, const uint8_t *mask, double cap,
-                                  int use_cap, double *partial, long long *pcount)
+struct InteriorActive {
+    int NE, H, N;
+    const uint8_t *mask;
+    __device__ __forceinline__ bool operator()(const long long c) const
+    {
+        return interior(c, NE, H, N) && (!mask || mask[c] == PGE_MASK_ACTIVE);
+    }
+};
+
+struct Positive {
+    __device__ __forceinline__ bool operator()(const double x) const { return x > 0.0; }
+};
+
+// ---------------------------------------------------------------------------
+// numpy's pairwise summation, so that a float64 sum the reference takes with
+// numpy (ndarray.sum / mean of a contiguous float64 array) is reproduced bit for
+// bit: n < 8 values are added one by one to 0; up to 128 values are added as
+// eight running sums over the leading multiple of 8, combined as
+// ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), and the rest added one by
+// one; a longer range is split at n2 = n/2 rounded down to a multiple of 8 and
+// the two halves' sums added.  (numpy's pairwise_sum, the reduction loop of
+// np.add; checked against np.sum on ranges of 1..5000 values of mixed
+// magnitudes.)  The top of the tree is expanded breadth-first into at most
+// PW_MAX_LEVEL_NODES nodes a level; the bottom nodes are summed one per thread
+// and the tree is folded back up in order.
+// ---------------------------------------------------------------------------
+constexpr int PW_LEAF = 128;
+constexpr int PW_MAX_LEVELS = 16;
+constexpr int PW_MAX_LEVEL_NODES = 2048;
+
+struct PwNode {
+    long long lo, n;
+    int child, nchild;  // children in the next level
+    double sum;
+};
+
+__device__ double pw_leaf(const double *a, long long n)
 {
-    __shared__ double sh[256];
-    __shared__ long long shc[256];
-    double acc = 0.0;
-    long long cnt = 0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
-        if (!interior(c, NE, H, N) || (mask && mask[c] != PGE_MASK_ACTIVE)) continue;
-        double v = u[c];
-        if (use_cap && v > cap) v = cap;
-        acc += v;
-        cnt++;
+    if (n < 8) {
+        double res = 0.0;
+        for (long long i = 0; i < n; i++) res += a[i];
+        return res;
     }
-    sh[threadIdx.x] = acc;
-    shc[threadIdx.x] = cnt;
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if (threadIdx.x < o) {
-            sh[threadIdx.x] += sh[threadIdx.x + o];
-            shc[threadIdx.x] += shc[threadIdx.x + o];
+    double r0 = a[0], r1 = a[1], r2 = a[2], r3 = a[3], r4 = a[4], r5 = a[5], r6 = a[6], r7 = a[7];
+    long long i = 8;
+    for (; i < n - (n % 8); i += 8) {
+        r0 += a[i];
+        r1 += a[i + 1];
+        r2 += a[i + 2];
+        r3 += a[i + 3];
+        r4 += a[i + 4];
+        r5 += a[i + 5];
+        r6 += a[i + 6];
+        r7 += a[i + 7];
+    }
+    double res = ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7));
+    for (; i < n; i++) res += a[i];
+    return res;
+}
+
+__device__ __forceinline__ long long pw_split(long long n)
+{
+    const long long n2 = n / 2;
+    return n2 - n2 % 8;
+}
+
+// the pairwise sum of a[0, n) by an explicit post-order walk (depth <= 40 for any n < 2^40)
+__device__ double pw_sum(const double *a, long long n)
+{
+    if (n <= PW_LEAF) return pw_leaf(a, n);
+    long long lo[40], len[40];
+    double left[40];
+    int stage[40];
+    int sp = 0;
+    lo[0] = 0;
+    len[0] = n;
+    stage[0] = 0;
+    double v = 0.0;
+    while (true) {
+        const int t = sp;
+        if (len[t] <= PW_LEAF || stage[t] == 2) {
+            // a finished node: a leaf, or both halves done (v holds the right half)
+            v = len[t] <= PW_LEAF ? pw_leaf(a + lo[t], len[t]) : left[t] + v;
+            if (sp == 0) return v;
+            sp--;
+            if (stage[sp] == 1) {  // the left half just finished: keep it, descend into the right half
+                left[sp] = v;
+                const long long n2 = pw_split(len[sp]);
+                stage[sp] = 2;
+                sp++;
+                lo[sp] = lo[sp - 1] + n2;
+                len[sp] = len[sp - 1] - n2;
+                stage[sp] = 0;
+            }
+            continue;
         }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        partial[blockIdx.x] = sh[0];
-        pcount[blockIdx.x] = shc[0];
+        stage[t] = 1;  // descend into the left half
+        sp++;
+        lo[sp] = lo[t];
+        len[sp] = pw_split(len[t]);
+        stage[sp] = 0;
     }
 }
 
-__global__ void mean_final_kernel(const double *partial, const long long *pcount, int n, double *mean_out)
+__global__ void pw_plan_kernel(const long long *count, PwNode *nodes, int *level_start)
 {
-    __shared__ double sh[RED_BLOCKS];
-    __shared__ long long shc[RED_BLOCKS];
-    for (int i = threadIdx.x; i < RED_BLOCKS; i += blockDim.x) {
-        sh[i] = i < n ? partial[i] : 0.0;
-        shc[i] = i < n ? pcount[i] : 0;
-    }
-    __syncthreads();
-    for (int o = RED_BLOCKS / 2; o > 0; o >>= 1) {
-        for (int i = threadIdx.x; i < o; i += blockDim.x) {
-            sh[i] += sh[i + o];
-            shc[i] += shc[i + o];
+    const long long M = *count;
+    nodes[0] = PwNode{0, M, -1, 0, 0.0};
+    int nl = 0, begin = 0, end = 1;
+    level_start[0] = 0;
+    while (nl + 1 < PW_MAX_LEVELS) {
+        long long biggest = 0;
+        for (int k = begin; k < end; k++) biggest = nodes[k].n > biggest ? nodes[k].n : biggest;
+        if (biggest <= 8 * PW_LEAF || 2 * (end - begin) > PW_MAX_LEVEL_NODES) break;
+        int next = end;
+        for (int k = begin; k < end; k++) {
+            PwNode &nd = nodes[k];
+            nd.child = next;
+            if (nd.n > PW_LEAF) {
+                const long long n2 = pw_split(nd.n);
+                nodes[next++] = PwNode{nd.lo, n2, -1, 0, 0.0};
+                nodes[next++] = PwNode{nd.lo + n2, nd.n - n2, -1, 0, 0.0};
+                nd.nchild = 2;
+            } else {
+                nodes[next++] = PwNode{nd.lo, nd.n, -1, 0, 0.0};  // a leaf passes down unchanged
+                nd.nchild = 1;
+            }
         }
-        __syncthreads();
+        begin = end;
+        end = next;
+        level_start[++nl] = begin;
     }
-    if (threadIdx.x == 0) *mean_out = shc[0] > 0 ? sh[0] / (double)shc[0] : 0.0;
+    level_start[nl + 1] = end;
+    level_start[PW_MAX_LEVELS + 1] = nl;  // the bottom level's index
 }
+
+__global__ void pw_bottom_kernel(const double *a, PwNode *nodes, const int *level_start)
+{
+    const int nl = level_start[PW_MAX_LEVELS + 1];
+    const int begin = level_start[nl], end = level_start[nl + 1];
+    for (int k = begin + blockIdx.x * blockDim.x + threadIdx.x; k < end; k += gridDim.x * blockDim.x)
+        nodes[k].sum = pw_sum(a + nodes[k].lo, nodes[k].n);
+}
+
+// folds the levels back up; out = the sum, or with mean_out the sum / count
+__global__ void pw_fold_kernel(PwNode *nodes, const int *level_start, const long long *count, double *out, int mean_out)
+{
+    const int nl = level_start[PW_MAX_LEVELS + 1];
+    for (int l = nl - 1; l >= 0; l--)
+        for (int k = level_start[l]; k < level_start[l + 1]; k++) {
+            PwNode &nd = nodes[k];
+            nd.sum = nd.nchild == 2 ? nodes[nd.child].sum + nodes[nd.child + 1].sum : nodes[nd.child].sum;
+        }
+    const long long M = *count;
+    *out = mean_out ? (M > 0 ? nodes[0].sum / (double)M : 0.0) : nodes[0].sum;
+}
+
+size_t pairwise_scratch_bytes() { return sizeof(PwNode) * (size_t)PW_MAX_LEVELS * PW_MAX_LEVEL_NODES + 256; }
+
+// sum (or mean) of a[0, *count) in numpy's pairwise order, written to *out on the stream
+void pairwise_sum(const double *a, const long long *count, void *scratch, double *out, int mean, cudaStream_t st)
+{
+    PwNode *nodes = static_cast<PwNode *>(scratch);
+    int *level_start = reinterpret_cast<int *>(nodes + (size_t)PW_MAX_LEVELS * PW_MAX_LEVEL_NODES);
+    pw_plan_kernel<<<1, 1, 0, st>>>(count, nodes, level_start);
+    pw_bottom_kernel<<<(PW_MAX_LEVEL_NODES + 127) / 128, 128, 0, st>>>(a, nodes, level_start);
+    pw_fold_kernel<<<1, 1, 0, st>>>(nodes, level_start, count, out, mean);
+}
+
+// ---------------------------------------------------------------------------
+// uplift and the datum's order statistic
+// ---------------------------------------------------------------------------
+constexpr int RED_BLOCKS = 1024;  // the partial-result area of the workspace: scalars of the uplift and the select
 
 __global__ void uplift_add_kernel(long long ncell, double *h, const double *u, const uint8_t *mask, double cap, int use_cap,
                                   const double *mean, double scale)
@@ -484,14 +616,22 @@ __global__ void uplift_add_kernel(long long ncell, double *h, const double *u, c
 
 void uplift(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, double cap, double scale, cudaStream_t st)
 {
+    // maps._applied_uplift (maps.py:1136-1147): the mean of the (capped) field over the interior active
+    // cells, u[interior][active].mean() -- their values in cell order, summed in numpy's pairwise order
     const int NE = g.N + 2 * g.H;
     const int use_cap = cap >= 0.0;
     double *partial = ws_ptr<double>(ws, lay.partial);
     long long *pcount = reinterpret_cast<long long *>(partial + RED_BLOCKS);
     double *mean = partial + 2 * RED_BLOCKS;
     if (g.spherical) {
-        uplift_sum_kernel<<<RED_BLOCKS, 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.uplift, s.mask, cap, use_cap, partial, pcount);
-        mean_final_kernel<<<1, 1024, 0, st>>>(partial, pcount, RED_BLOCKS, mean);
+        double *vals = ws_ptr<double>(ws, lay.pwv);
+        size_t tb = lay.cubtmp_bytes;
+        const thrust::counting_iterator<long long> c0(0);
+        cub::DeviceSelect::Flagged(ws_ptr<void>(ws, lay.cubtmp), tb,
+                                   thrust::make_transform_iterator(c0, UpliftValue{s.uplift, cap, use_cap}),
+                                   thrust::make_transform_iterator(c0, InteriorActive{NE, g.H, g.N, s.mask}), vals, pcount,
+                                   (int)lay.ncell, st);
+        pairwise_sum(vals, pcount, ws_ptr<void>(ws, lay.pwnode), mean, 1, st);
     }
     uplift_add_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.height, s.uplift, s.mask, cap, use_cap,
                                                            g.spherical ? mean : nullptr, scale);
@@ -647,16 +787,74 @@ void halo_gather(const PgeHalo &h, double *field, int vector, cudaStream_t st)
 // ---------------------------------------------------------------------------
 // spawns
 // ---------------------------------------------------------------------------
+// a float32 x > 0 is m * 2^(e - 150) with m a 24-bit integer (e the biased exponent, 1 for subnormals)
+__device__ __forceinline__ void f32_parts(float x, long long &m, int &e)
+{
+    const unsigned b = __float_as_uint(x);
+    const unsigned E = (b >> 23) & 0xffu;
+    m = (long long)((b & 0x7fffffu) | (E ? 0x800000u : 0u));
+    e = E ? (int)E : 1;
+}
+
 __global__ void spawn_weight_kernel(long long ncell, int NE, int H, int N, const double *h, const double *s, const double *base,
-                                    const uint8_t *mask, const float *precip, double *w, long long *lastc)
+                                    const uint8_t *mask, const float *precip, double *w, long long *lastc, long long *erange)
 {
     long long last = -1;
+    int emin = 1 << 20, emax = -1;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
         const bool ok = interior(c, NE, H, N) && (!mask || mask[c] == PGE_MASK_ACTIVE) && (h[c] + s[c] >= base[c]) && precip[c] > 0.0f;
         w[c] = ok ? (double)precip[c] : 0.0;
-        if (ok && c > last) last = c;
+        if (ok) {
+            if (c > last) last = c;
+            long long m;
+            int e;
+            f32_parts(precip[c], m, e);
+            emin = e < emin ? e : emin;
+            emax = e > emax ? e : emax;
+        }
     }
     if (last >= 0) atomicMax(reinterpret_cast<unsigned long long *>(lastc), (unsigned long long)last);
+    if (emax >= 0) {
+        atomicMin(erange, (long long)emin);
+        atomicMax(erange + 1, (long long)emax);
+    }
+}
+
+// The fixed-point unit of the weights' integer scan: 2^(base - 150), the smallest weight's
+// last bit (so every weight is an integer of it and every prefix sum exact) unless the spread
+// of exponents would overflow 62 bits over ncell weights.
+__device__ __forceinline__ int spawn_fx_base(const long long *erange, long long ncell)
+{
+    int lg = 0;
+    while ((1LL << lg) < ncell) lg++;
+    const int emin = (int)erange[0], emax = (int)erange[1];
+    const int need = emax + 24 + lg - 62;
+    return emin > need ? emin : need;
+}
+
+__global__ void spawn_quant_kernel(long long ncell, const double *w, const long long *erange, long long *wq)
+{
+    const int base = spawn_fx_base(erange, ncell);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        long long q = 0;
+        if (w[c] > 0.0) {
+            long long m;
+            int e;
+            f32_parts((float)w[c], m, e);
+            const int sh = e - base;
+            q = sh >= 0 ? m << sh : (sh > -40 ? (m + (1LL << (-sh - 1))) >> (-sh) : 0);
+        }
+        wq[c] = q;
+    }
+}
+
+// the integer prefix sums back to float64, in place
+__global__ void spawn_cdf_kernel(long long ncell, const long long *erange, double *cdf)
+{
+    const int base = spawn_fx_base(erange, ncell);
+    long long *S = reinterpret_cast<long long *>(cdf);
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
+        cdf[c] = ldexp((double)S[c], base - 150);
 }
 
 __global__ void spawn_count_kernel(long long ncell, const double *w, long long *count)
@@ -669,11 +867,9 @@ __global__ void spawn_count_kernel(long long ncell, const double *w, long long *
 }
 
 __global__ void spawn_search_kernel(long long ncell, int NE, int H, const double *cdf, const long long *lastc, const double *u,
-                                    const double *off, long long P, int32_t *face, double *x, double *y, double *sed, double *dir,
-                                    double *total_out)
+                                    const double *off, long long P, int32_t *face, double *x, double *y, double *sed, double *dir)
 {
     const double total = cdf[ncell - 1];
-    if (blockIdx.x == 0 && threadIdx.x == 0 && total_out) *total_out = total;
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
         const double target = u[p] * total;
         // first index with cdf > target (the reference walks its compacted cdf the same way)
@@ -728,32 +924,59 @@ size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets)
     cub::DeviceRadixSort::SortKeys(nullptr, b, (double *)nullptr, (double *)nullptr, (int)(max_droplets > 0 ? max_droplets : 1));
     cub::DeviceSelect::If(nullptr, c, thrust::counting_iterator<long long>(0), (long long *)nullptr, (long long *)nullptr,
                           (int)ncell, PendFlag{nullptr});
+    size_t d = 0, f = 0, h = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, d, (long long *)nullptr, (long long *)nullptr, (int)ncell);
+    cub::DeviceSelect::If(nullptr, f, (double *)nullptr, (double *)nullptr, (long long *)nullptr, (int)ncell, Positive{});
+    cub::DeviceSelect::Flagged(nullptr, h, thrust::make_transform_iterator(thrust::counting_iterator<long long>(0), UpliftValue{}),
+                               thrust::make_transform_iterator(thrust::counting_iterator<long long>(0), InteriorActive{}),
+                               (double *)nullptr, (long long *)nullptr, (int)ncell);
     size_t m = a > b ? a : b;
-    return m > c ? m : c;
+    m = m > c ? m : c;
+    m = m > d ? m : d;
+    m = m > f ? m : f;
+    return m > h ? m : h;
 }
 
 cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, const double *u, const double *off,
                        long long P, PgeSpawns &sp, double *total_dev, long long *nspawn_dev, cudaStream_t st)
 {
+    // maps.spawn_weights / spawn_particles (maps.py:793-833): w = precip on spawnable cells, their
+    // cumulative sum (np.cumsum: sequential), total = w.sum() (numpy's pairwise order) and the inverse
+    // CDF of the sorted uniforms (particle.spawn_cells).  The cumulative sum is an integer scan of the
+    // weights in fixed point (their float32 bits), so it is order-free and equals the sequential float64
+    // sum bit for bit whenever that sum is exact -- every prefix below 2^53 units of the smallest
+    // weight's last bit (any float32 precip of 0.1 .. 3 over 6.3 M cells, or uniform rain).
     const int NE = g.N + 2 * g.H;
     double *w = ws_ptr<double>(ws, lay.cdf);
     double *cdf = w + lay.ncell;
     double *keys = ws_ptr<double>(ws, lay.sortkeys);
-    long long *lastc = ws_ptr<long long>(ws, lay.counters) + 2;
+    long long *ctr = ws_ptr<long long>(ws, lay.counters);
+    long long *lastc = ctr + 2, *erange = ctr + 4, *nsel = ctr + 6;
+    long long *wq = ws_ptr<long long>(ws, lay.pwv);
     cudaError_t e = cudaMemsetAsync(lastc, 0, sizeof(long long), st);
     if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(erange, 0x7f, sizeof(long long), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(erange + 1, 0, sizeof(long long), st)) != cudaSuccess) return e;
     if (nspawn_dev && (e = cudaMemsetAsync(nspawn_dev, 0, sizeof(long long), st)) != cudaSuccess) return e;
     spawn_weight_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, s.base, s.mask,
-                                                             s.precip, w, lastc);
+                                                             s.precip, w, lastc, erange);
     if (nspawn_dev) spawn_count_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, w, nspawn_dev);
+    spawn_quant_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, w, erange, wq);
     size_t tb = lay.cubtmp_bytes;
-    e = cub::DeviceScan::InclusiveSum(ws_ptr<void>(ws, lay.cubtmp), tb, w, cdf, (int)lay.ncell, st);
+    e = cub::DeviceScan::InclusiveSum(ws_ptr<void>(ws, lay.cubtmp), tb, wq, reinterpret_cast<long long *>(cdf), (int)lay.ncell, st);
     if (e != cudaSuccess) return e;
+    spawn_cdf_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, erange, cdf);
+    // the total weight in numpy's order: the spawnable weights compacted in cell order, summed pairwise
+    double *wc = ws_ptr<double>(ws, lay.pwv);
+    tb = lay.cubtmp_bytes;
+    e = cub::DeviceSelect::If(ws_ptr<void>(ws, lay.cubtmp), tb, w, wc, nsel, (int)lay.ncell, Positive{}, st);
+    if (e != cudaSuccess) return e;
+    if (total_dev) pairwise_sum(wc, nsel, ws_ptr<void>(ws, lay.pwnode), total_dev, 0, st);
     tb = lay.cubtmp_bytes;
     e = cub::DeviceRadixSort::SortKeys(ws_ptr<void>(ws, lay.cubtmp), tb, u, keys, (int)P, 0, 64, st);
     if (e != cudaSuccess) return e;
     spawn_search_kernel<<<grid_for(P), 256, 0, st>>>(lay.ncell, NE, g.H, cdf, lastc, keys, off, P, sp.face, sp.x, sp.y, sp.sed,
-                                                     sp.dir, total_dev);
+                                                     sp.dir);
     return cudaPeekAtLastError();
 }
 

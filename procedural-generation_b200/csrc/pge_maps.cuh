@@ -19,6 +19,9 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// numpy's pairwise float64 sum (mean = 1: divided by the count) of a[0, *count), on the stream
+size_t pairwise_scratch_bytes();
+void pairwise_sum(const double *a, const long long *count, void *scratch, double *out, int mean, cudaStream_t st);
 // the planet's lake balance on the host (pge_lakes.cpp); 0, or -1 when a land cell has no flow direction
 int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
                       const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,

@@ -293,6 +293,127 @@ __device__ __forceinline__ bool cell_value(const OrderedArgs &a, const Walk &w, 
 }
 }  // namespace
 
+// One change-list entry against the live terrain (particle.py:934-1002): the erosion floor (the
+// base level or the cell itself, the next path cell's live surface nlive), the deposit ceilings (the
+// previous step's live surface, or for a final deposit the next, older path cell), the deficit and
+// surplus carried along the droplet's list.  acc is the cell's live net change; writes the new one
+// and the amount actually moved.
+template <bool ECAP, bool LAKE>
+__device__ __forceinline__ void entry_arith(const PgeParams &p, Walk &w, int32_t c, double dlt, bool is_step, bool act, double hs,
+                                            double b_c, double acc, bool has_next, double nlive, double capv, float2 route,
+                                            double &acc_new, double &amount)
+{
+    if (act) {
+        const double s_c = hs + acc;
+        if (dlt < 0.0) {
+            const double ew = -dlt;
+            double e_act = ew;
+            double room = p.iter_erode + acc;
+            if (ECAP) {
+                const double r2 = capv + acc;
+                if (r2 < room) room = r2;
+            }
+            if (e_act > room) e_act = room;
+            double floor_ = s_c >= b_c ? b_c : s_c;
+            // a lake bed is never eroded below its water level (particle.py:952-956)
+            if (LAKE && route.y >= 1.5f && (double)route.x > floor_) floor_ = (double)route.x;
+            if (has_next && nlive > floor_) floor_ = nlive;
+            if (e_act > s_c - floor_) e_act = s_c - floor_;
+            if (e_act < 0.0) e_act = 0.0;
+            if (e_act < ew) {
+                w.clamped++;
+                w.deficit += ew - e_act;
+            }
+            acc_new = acc - e_act;
+            amount = e_act;
+        } else {
+            double want = dlt + w.surplus;
+            w.surplus = 0.0;
+            if (w.deficit > 0.0) {
+                const double t = want < w.deficit ? want : w.deficit;
+                want -= t;
+                w.deficit -= t;
+            }
+            double d_act = want;
+            const double room = p.iter_deposit - acc;
+            if (d_act > room) d_act = room;
+            bool has_ref = false;
+            double ref_live = 0.0;
+            if (is_step) {
+                has_ref = w.has_prev;
+                ref_live = w.prev_live;
+            } else if (has_next) {
+                has_ref = true;
+                ref_live = nlive;
+            }
+            if (has_ref) {
+                double ceil_ = ref_live + p.dep_floor;
+                if (s_c < b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
+                const double lim = ceil_ - s_c;
+                if (d_act > lim) d_act = lim;
+            }
+            if (s_c < b_c) {
+                const double lim = b_c - p.dep_floor - s_c;
+                if (d_act > lim) d_act = lim;
+            }
+            if (d_act < 0.0) d_act = 0.0;
+            if (d_act < want) w.clamped++;
+            w.surplus = want - d_act;
+            acc_new = acc + d_act;
+            amount = d_act;
+            if (!is_step && w.death < 0) w.death = c;
+        }
+        if (c == w.death) w.sub_death = hs + acc_new < b_c;
+        if (is_step) {
+            w.has_prev = true;
+            w.prev_live = hs + acc_new;
+        }
+    }
+}
+
+// a droplet's stockpile (particle.py:1019-1041) and its statistics, once its list is applied
+__device__ __forceinline__ void droplet_end(const OrderedArgs &a, const Walk &w, long long q, unsigned long long *sstat)
+{
+    const PgeParams &p = a.p;
+    long long topend = 0, lostoff = 0;
+    int32_t dth = -1;
+    double add = 0.0;
+    if (w.death >= 0 && w.surplus > 0.0) {
+        if (w.sub_death) {
+            double keep = w.surplus * (1.0 - p.offshore_writeoff);
+            if (keep < 1e-4) keep = 0.0;
+            add = keep;
+            topend = fx_mass(keep);
+            lostoff = fx_mass(w.surplus) - topend;
+        } else {
+            add = w.surplus;
+            topend = fx_mass(w.surplus);
+        }
+        dth = w.death;
+    }
+    a.dth[q] = dth;
+    a.keep[q] = add;
+    if (w.clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)w.clamped);
+    if (topend) atomicAdd(&sstat[OS_TOPEND], (unsigned long long)topend);
+    if (w.deficit > 0.0) atomicAdd(&sstat[OS_DEFICIT], (unsigned long long)fx_mass(w.deficit));
+    if (lostoff) atomicAdd(&sstat[OS_LOSTOFF], (unsigned long long)lostoff);
+}
+
+// the block's statistics to the pass totals (after a __syncthreads)
+__device__ __forceinline__ void flush_stats(const OrderedArgs &a, const unsigned long long *sstat)
+{
+    if (threadIdx.x < OS_N && sstat[threadIdx.x]) {
+        PgeStats *st = a.stats;
+        int64_t *dst = threadIdx.x == OS_CLAMPED ? &st->clamped
+                     : threadIdx.x == OS_TOPEND ? &st->to_pending_fx
+                     : threadIdx.x == OS_DEFICIT ? &st->deficit_out_fx
+                     : threadIdx.x == OS_LOSTOFF ? &st->lost_offshore_fx
+                     : threadIdx.x == OS_ERODED ? &st->eroded_fx
+                                                : &st->deposited_fx;
+        red_add(reinterpret_cast<long long *>(dst), (long long)sstat[threadIdx.x]);
+    }
+}
+
 template <bool ECAP, bool LAKE>
 __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const OrderedArgs a)
 {
@@ -363,73 +484,8 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
             }
             const double acc = w.acc_c;
             double acc_new = acc, amount = 0.0;
-            if (act) {
-                const double s_c = hs + acc;
-                const double nlive = hs_n + acc_n;
-                if (dlt < 0.0) {
-                    const double ew = -dlt;
-                    double e_act = ew;
-                    double room = p.iter_erode + acc;
-                    if (ECAP) {
-                        const double r2 = cur.cap + acc;
-                        if (r2 < room) room = r2;
-                    }
-                    if (e_act > room) e_act = room;
-                    double floor_ = s_c >= b_c ? b_c : s_c;
-                    // a lake bed is never eroded below its water level (particle.py:952-956)
-                    if (LAKE && cur.route.y >= 1.5f && (double)cur.route.x > floor_) floor_ = (double)cur.route.x;
-                    if (has_next && nlive > floor_) floor_ = nlive;
-                    if (e_act > s_c - floor_) e_act = s_c - floor_;
-                    if (e_act < 0.0) e_act = 0.0;
-                    if (e_act < ew) {
-                        w.clamped++;
-                        w.deficit += ew - e_act;
-                    }
-                    acc_new = acc - e_act;
-                    amount = e_act;
-                } else {
-                    double want = dlt + w.surplus;
-                    w.surplus = 0.0;
-                    if (w.deficit > 0.0) {
-                        const double t = want < w.deficit ? want : w.deficit;
-                        want -= t;
-                        w.deficit -= t;
-                    }
-                    double d_act = want;
-                    const double room = p.iter_deposit - acc;
-                    if (d_act > room) d_act = room;
-                    bool has_ref = false;
-                    double ref_live = 0.0;
-                    if (is_step) {
-                        has_ref = w.has_prev;
-                        ref_live = w.prev_live;
-                    } else if (has_next) {
-                        has_ref = true;
-                        ref_live = nlive;
-                    }
-                    if (has_ref) {
-                        double ceil_ = ref_live + p.dep_floor;
-                        if (s_c < b_c && is_step) ceil_ -= p.dep_floor + p.fan_slope;
-                        const double lim = ceil_ - s_c;
-                        if (d_act > lim) d_act = lim;
-                    }
-                    if (s_c < b_c) {
-                        const double lim = b_c - p.dep_floor - s_c;
-                        if (d_act > lim) d_act = lim;
-                    }
-                    if (d_act < 0.0) d_act = 0.0;
-                    if (d_act < want) w.clamped++;
-                    w.surplus = want - d_act;
-                    acc_new = acc + d_act;
-                    amount = d_act;
-                    if (!is_step && w.death < 0) w.death = c;
-                }
-                if (c == w.death) w.sub_death = hs + acc_new < b_c;
-                if (is_step) {
-                    w.has_prev = true;
-                    w.prev_live = hs + acc_new;
-                }
-            }
+            entry_arith<ECAP, LAKE>(p, w, c, dlt, is_step, act, hs, b_c, acc, has_next, hs_n + acc_n, cur.cap, cur.route, acc_new,
+                                    amount);
             // publish the net change; a droplet's last write at a cell also hands the cell on
             const bool lastv = (df & ENTRY_LAST) != 0;
             if (act || lastv) hand_store(a.hand + c, acc_new, a.epoch + (df & ENTRY_D_MASK) + (lastv ? 1u : 0u));
@@ -455,40 +511,271 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
             failed = true;
             break;
         }
-        long long topend = 0, lostoff = 0;
-        int32_t dth = -1;
-        double add = 0.0;
-        if (w.death >= 0 && w.surplus > 0.0) {
-            if (w.sub_death) {
-                double keep = w.surplus * (1.0 - p.offshore_writeoff);
-                if (keep < 1e-4) keep = 0.0;
-                add = keep;
-                topend = fx_mass(keep);
-                lostoff = fx_mass(w.surplus) - topend;
-            } else {
-                add = w.surplus;
-                topend = fx_mass(w.surplus);
-            }
-            dth = w.death;
-        }
-        a.dth[q] = dth;
-        a.keep[q] = add;
-        if (w.clamped) atomicAdd(&sstat[OS_CLAMPED], (unsigned long long)w.clamped);
-        if (topend) atomicAdd(&sstat[OS_TOPEND], (unsigned long long)topend);
-        if (w.deficit > 0.0) atomicAdd(&sstat[OS_DEFICIT], (unsigned long long)fx_mass(w.deficit));
-        if (lostoff) atomicAdd(&sstat[OS_LOSTOFF], (unsigned long long)lostoff);
+        droplet_end(a, w, q, sstat);
     }
     __syncthreads();
-    if (threadIdx.x < OS_N && sstat[threadIdx.x]) {
-        PgeStats *st = a.stats;
-        int64_t *dst = threadIdx.x == OS_CLAMPED ? &st->clamped
-                     : threadIdx.x == OS_TOPEND ? &st->to_pending_fx
-                     : threadIdx.x == OS_DEFICIT ? &st->deficit_out_fx
-                     : threadIdx.x == OS_LOSTOFF ? &st->lost_offshore_fx
-                     : threadIdx.x == OS_ERODED ? &st->eroded_fx
-                                                : &st->deposited_fx;
-        red_add(reinterpret_cast<long long *>(dst), (long long)sstat[threadIdx.x]);
+    flush_stats(a, sstat);
+}
+
+// ---------------------------------------------------------------------------
+// The fed apply: one droplet per block of two warps.  Warp 1, the feeder, streams the droplet's
+// entries into a ring in shared memory -- the descriptor, the cell's pass-start terrain, its hand-off
+// word (and the erode cap / routing surface) -- FED_CHUNK entries at a time (a lane each), and keeps
+// re-polling the hand-off words of upcoming first visits whose cell the earlier droplets have not yet
+// handed on.  Lane 0 of warp 0, the applier, walks the list reading only shared memory: its serial
+// chain is the arithmetic of the entries, not the latency of their loads.  The feeder overwrites an
+// entry's slot only once the applier is more than FED_LOOKBACK entries past it, so the applier finds
+// its own recent writes to a cell it revisits (the final deposits over the last path cells) in the ring.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int FED_THREADS = 64;
+constexpr int FED_RING = 128;
+constexpr int FED_CHUNK = 32;
+constexpr int FED_LOOKBACK = 32;
+constexpr long long kFedSpin = 1LL << 26;  // polls of one wait (~ a second or more): far beyond any hand-off
+
+struct alignas(16) FedSlot {
+    EntryDesc d;                         // descriptor
+    volatile unsigned long long h0, h1;  // the cell's hand-off word, refreshed by the feeder until it is ready
+    CellTerr t;                          // the cell's pass-start terrain
+    double cap;                          // the slope erode cap (when on)
+    float2 route;                        // the packed routing surface and flag (with lakes)
+};
+static_assert(sizeof(FedSlot) == 64, "fed slot layout");
+
+// the droplet's own latest value at cell c among its entries k - FED_LOOKBACK .. k - 1
+__device__ __forceinline__ bool own_lookback(const FedSlot *ring, const double *ownv, int k, int32_t c, double &acc)
+{
+    const int lim = k < FED_LOOKBACK ? k : FED_LOOKBACK;
+    for (int i = 1; i <= lim; i++) {
+        const int sl = (k - i) & (FED_RING - 1);
+        if (ring[sl].d.cell == c) {
+            acc = ownv[sl];
+            return true;
+        }
     }
+    return false;
+}
+
+// the net change of cell c for entry k (its slot sl): the droplet's own earlier write (a revisit), or
+// once the D earlier droplets have handed the cell on, the hand-off word the feeder keeps fresh
+__device__ __forceinline__ bool fed_value(const OrderedArgs &a, const FedSlot *ring, const double *ownv, int k, int sl, int32_t c,
+                                          uint32_t df, const volatile int *quit, double &acc)
+{
+    if (!(df & ENTRY_FIRST)) {
+        if (own_lookback(ring, ownv, k, c, acc)) return true;
+        acc = own_value(a.hand, c);
+        return true;
+    }
+    const uint32_t D = df & ENTRY_D_MASK;
+    const uint32_t want = a.epoch + D;
+    const FedSlot &s = ring[sl];
+    for (long long i = 0; i < kFedSpin; i++) {
+        const unsigned long long w0 = s.h0, w1 = s.h1;
+        if (D == 0 || hand_ready(w0, w1, want)) {
+            acc = hand_acc(w0, w1);
+            return true;
+        }
+        if ((i & 1023) == 1023 && (*quit || *(volatile int *)a.error)) return false;
+    }
+    atomicExch(a.error, 1);
+    return false;
+}
+
+template <bool ECAP, bool LAKE>
+__device__ __forceinline__ void feed_entry(const OrderedArgs &a, FedSlot &s, long long e)
+{
+    // both arrays are read-only while the apply runs: 16-byte read-only loads
+    const int4 dv = __ldg(reinterpret_cast<const int4 *>(a.desc + e));
+    EntryDesc d;
+    memcpy(&d, &dv, sizeof(d));
+    s.d = d;
+    const long long c = d.cell;
+    const int4 tv = __ldg(reinterpret_cast<const int4 *>(a.terr + c));
+    CellTerr t;
+    memcpy(&t, &tv, sizeof(t));
+    s.t = t;
+    unsigned long long w0, w1;
+    hand_load(a.hand + c, w0, w1);
+    s.h0 = w0;
+    s.h1 = w1;
+    if (ECAP) s.cap = __ldg(a.ecap + c);
+    if (LAKE) s.route = __ldg(a.R + c);
+}
+
+// warp 1: keep the ring filled ahead of the applier and the pending hand-off words fresh
+template <bool ECAP, bool LAKE>
+__device__ void feeder(const OrderedArgs &a, FedSlot *ring, long long b0, int K, volatile int *loaded_s, volatile int *done_s,
+                       volatile int *quit)
+{
+    const int lane = threadIdx.x & 31;
+    int loaded = 0, last_done = -1;
+    long long idle = 0;
+    while (true) {
+        // every decision of the loop is the warp's: lane 0 reads the shared counters for all
+        int done = 0, stop = 0;
+        if (lane == 0) {
+            done = *done_s;
+            stop = *quit;
+        }
+        done = __shfl_sync(0xffffffffu, done, 0);
+        stop = __shfl_sync(0xffffffffu, stop, 0);
+        if (done >= K || stop) return;
+        if (done != last_done) {
+            last_done = done;
+            idle = 0;
+        } else if (++idle > kFedSpin) {  // the applier made no progress for seconds
+            if (lane == 0) {
+                atomicExch(a.error, 1);
+                *quit = 1;
+            }
+            return;
+        }
+        // a chunk [loaded, loaded + 32) overwrites entries loaded - FED_RING ..; they must be older than
+        // done - FED_LOOKBACK (done never runs ahead of the applier)
+        if (loaded < K && loaded <= done - FED_LOOKBACK + FED_RING - FED_CHUNK) {
+            const int j = loaded + lane;
+            if (j < K) feed_entry<ECAP, LAKE>(a, ring[j & (FED_RING - 1)], b0 + j);
+            loaded = loaded + FED_CHUNK < K ? loaded + FED_CHUNK : K;
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                *loaded_s = loaded;
+            }
+            continue;
+        }
+        bool polled = false;
+        for (int j = done + lane; j < loaded; j += 32) {
+            FedSlot &s = ring[j & (FED_RING - 1)];
+            const uint32_t df = s.d.dflags;
+            const uint32_t D = df & ENTRY_D_MASK;
+            if (!(df & ENTRY_FIRST) || D == 0) continue;
+            const uint32_t want = a.epoch + D;
+            if (hand_ready(s.h0, s.h1, want)) continue;
+            unsigned long long w0, w1;
+            hand_load(a.hand + s.d.cell, w0, w1);
+            polled = true;
+            if (hand_ready(w0, w1, want)) {
+                s.h0 = w0;
+                s.h1 = w1;
+            }
+        }
+        if (!__any_sync(0xffffffffu, polled)) __nanosleep(64);
+    }
+}
+}  // namespace
+
+template <bool ECAP, bool LAKE>
+__global__ void __launch_bounds__(FED_THREADS) ordered_apply_fed_kernel(const OrderedArgs a)
+{
+    __shared__ FedSlot ring[FED_RING];
+    __shared__ double ownv[FED_RING];
+    __shared__ unsigned long long sstat[OS_N];
+    __shared__ int s_loaded, s_done, s_quit;
+    for (int k = threadIdx.x; k < OS_N; k += blockDim.x) sstat[k] = 0ull;
+    if (threadIdx.x == 0) s_quit = 0;
+    __syncthreads();
+    volatile int *loaded_s = &s_loaded, *done_s = &s_done, *quit = &s_quit;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (long long q = blockIdx.x; q < a.nw; q += gridDim.x) {
+        const int K = (int)a.count[q];
+        if (K <= 0) {
+            if (threadIdx.x == 0) a.dth[q] = -1;
+            continue;
+        }
+        const long long b0 = q * a.cap;
+        if (threadIdx.x == 0) {
+            s_loaded = 0;
+            s_done = 0;
+        }
+        __syncthreads();
+        if (warp == 1) {
+            feeder<ECAP, LAKE>(a, ring, b0, K, loaded_s, done_s, quit);
+        } else if (lane == 0) {
+            Walk w;
+            w.deficit = w.surplus = w.prev_live = w.acc_c = 0.0;
+            w.clamped = 0;
+            w.death = -1;
+            w.sub_death = w.has_prev = w.have_c = false;
+            w.ok = true;
+            int seen = 0;
+            for (int k = 0; k < K; k++) {
+                // entries k and k + 1 in the ring
+                const int need = k + 1 < K ? k + 2 : k + 1;
+                if (seen < need) {
+                    for (long long i = 0; seen < need; i++) {
+                        seen = *loaded_s;
+                        if (seen >= need) break;
+                        if (*quit) {
+                            w.ok = false;
+                            break;
+                        }
+                        if (i > kFedSpin) {
+                            atomicExch(a.error, 1);
+                            w.ok = false;
+                            break;
+                        }
+                    }
+                    if (!w.ok) break;
+                    __threadfence_block();  // the slots the feeder published before its count
+                }
+                const int sl = k & (FED_RING - 1), nsl = (k + 1) & (FED_RING - 1);
+                const FedSlot &cur = ring[sl];
+                const FedSlot &nx = ring[nsl];
+                const bool has_next = k + 1 < K;
+                const int32_t c = cur.d.cell;
+                const uint32_t df = cur.d.dflags;
+                const double dlt = cur.d.delta;
+                const double hs = cur.t.hs;
+                const double b_c = (double)cur.t.base;
+                const bool act = cur.t.active != 0;
+                if (!w.have_c && !(w.ok = fed_value(a, ring, ownv, k, sl, c, df, quit, w.acc_c))) break;
+                // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
+                // acquire it now; a step deposit does not, and acquires it only before writing it
+                const bool is_step = (df & ENTRY_STEP) != 0;
+                const bool reads_next = has_next && (dlt < 0.0 || !is_step);
+                const int32_t ncell = has_next ? nx.d.cell : -1;
+                double acc_n = 0.0, hs_n = 0.0;
+                if (reads_next) {
+                    hs_n = nx.t.hs;
+                    if (ncell == c)
+                        acc_n = w.acc_c;
+                    else if (!(w.ok = fed_value(a, ring, ownv, k, nsl, ncell, nx.d.dflags, quit, acc_n)))
+                        break;
+                }
+                const double acc = w.acc_c;
+                double acc_new = acc, amount = 0.0;
+                entry_arith<ECAP, LAKE>(a.p, w, c, dlt, is_step, act, hs, b_c, acc, has_next, hs_n + acc_n, cur.cap, cur.route,
+                                        acc_new, amount);
+                // publish the net change; a droplet's last write at a cell also hands the cell on
+                const bool lastv = (df & ENTRY_LAST) != 0;
+                if (act || lastv) hand_store(a.hand + c, acc_new, a.epoch + (df & ENTRY_D_MASK) + (lastv ? 1u : 0u));
+                a.act[b0 + k] = amount;
+                ownv[sl] = acc_new;
+                // the next entry's cell: acquired (with its net change) if this entry read it; the same
+                // cell again keeps its acquisition and its updated net change
+                if (has_next && ncell == c) {
+                    w.have_c = true;
+                    w.acc_c = acc_new;
+                } else {
+                    w.have_c = reads_next;
+                    w.acc_c = acc_n;
+                }
+                *done_s = k + 1;
+            }
+            if (w.ok) {
+                droplet_end(a, w, q, sstat);
+            } else {
+                *quit = 1;
+            }
+            *done_s = K;  // releases the feeder
+        }
+        __syncwarp();  // warp 0's idle lanes wait for lane 0 here, so the warp meets the barrier converged
+        __syncthreads();
+        if (s_quit) break;
+    }
+    __syncthreads();
+    flush_stats(a, sstat);
 }
 
 // ---------------------------------------------------------------------------
@@ -609,6 +896,11 @@ cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, 
 int ordered_blocks_per_sm(int lanes)
 {
     int n = 0;
+    if (lanes <= 0) {  // the fed apply: one droplet per block, static shared memory
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_fed_kernel<true, true>, FED_THREADS, 0) != cudaSuccess)
+            return 1;
+        return n > 0 ? n : 1;
+    }
     const size_t smem = (size_t)(APPLY_THREADS / 32) * lanes * RING * sizeof(Slot);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false, false>, APPLY_THREADS, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
@@ -629,11 +921,27 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, w.segpos, w.segscan, MaxOp{}, (int)nslots, st)) != cudaSuccess) return e;
     ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
                                                           w.a.delta, w.a.vol, const_cast<EntryDesc *>(w.a.desc));
+    const bool lake = w.a.lakes && w.a.R;
+    if (w.a.lanes <= 0) {
+        // the fed apply: a block per droplet while they last (every block resident: a droplet waits only
+        // on earlier droplets, which blocks already running hold)
+        long long blocks = w.nw < w.max_blocks ? w.nw : w.max_blocks;
+        if (blocks < 1) blocks = 1;
+        if (w.a.ecap && lake)
+            ordered_apply_fed_kernel<true, true><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
+        else if (w.a.ecap)
+            ordered_apply_fed_kernel<true, false><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
+        else if (lake)
+            ordered_apply_fed_kernel<false, true><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
+        else
+            ordered_apply_fed_kernel<false, false><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
+        ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
+        return cudaPeekAtLastError();
+    }
     const long long warps = (w.nw + w.a.lanes - 1) / w.a.lanes;  // a lane per droplet
     long long blocks = (warps * 32 + APPLY_THREADS - 1) / APPLY_THREADS;
     if (blocks > w.max_blocks) blocks = w.max_blocks;
     const size_t smem = (size_t)(APPLY_THREADS / 32) * w.a.lanes * RING * sizeof(Slot);
-    const bool lake = w.a.lakes && w.a.R;
     if (w.a.ecap && lake)
         ordered_apply_kernel<true, true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     else if (w.a.ecap)

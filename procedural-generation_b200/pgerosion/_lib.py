@@ -32,6 +32,9 @@ EXPORTS = (
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
 NOALLOC_MAX_CELLS = 262144
+#: the erode / deposit brush (PgeParams.brush_radius, include/pgerosion.h)
+BRUSH_MAX_RADIUS = 4
+BRUSH_SCALE = 1024
 
 c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
 
@@ -57,7 +60,7 @@ PARAM_DOUBLES = ("dt", "density", "friction", "deposition_rate", "evap_rate", "k
                  "min_volume", "max_erode", "conc_scale", "ocean_rate", "fan_room", "dep_floor", "iter_erode",
                  "iter_deposit", "fan_slope", "offshore_writeoff", "ema", "lake_trap", "lateral_rate")
 PARAM_INTS = ("max_steps", "pit_steps", "ocean_steps", "wave", "precision", "apply", "use_erode_cap", "threads_per_block",
-              "blocks_per_sm", "trace_lanes", "apply_lanes")
+              "blocks_per_sm", "trace_lanes", "apply_lanes", "brush_radius")
 
 
 class PgeParams(ctypes.Structure):

@@ -465,6 +465,9 @@ def default_wave(ep, n_particles: int) -> int:
 def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, precision: int, mom_scale=1.0, disc_sat=None,
                 iter_deposit=None, threads_per_block=0, blocks_per_sm=0, apply=_lib.APPLY_ORDERED, trace_lanes=0,
                 apply_lanes=0) -> PgeParams:
+    """The kernel's parameters in cell units.  ``erosion.brush_radius`` (no
+    counterpart in the reference; 0 when the group has no such knob) spreads
+    the wave apply's changes over a brush (PgeParams.brush_radius)."""
     u = state.height_unit_m
     return PgeParams(
         dt=float(ep.dt), density=float(ep.density), friction=float(ep.friction), deposition_rate=float(ep.deposition_rate),
@@ -479,7 +482,8 @@ def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, prec
         lake_trap=float(getattr(ep, "lake_trap", 0.9)), lateral_rate=float(getattr(ep, "lateral_rate", 0.0)),
         max_steps=max_steps_of(ep, state.N), pit_steps=int(ep.pit_steps), ocean_steps=int(ep.ocean_steps), wave=int(wave),
         precision=int(precision), apply=int(apply), use_erode_cap=0, threads_per_block=int(threads_per_block),
-        blocks_per_sm=int(blocks_per_sm), trace_lanes=int(trace_lanes), apply_lanes=int(apply_lanes))
+        blocks_per_sm=int(blocks_per_sm), trace_lanes=int(trace_lanes), apply_lanes=int(apply_lanes),
+        brush_radius=int(getattr(ep, "brush_radius", 0)))
 
 
 def draw_spawns(params, rng_stage: str, key, P: int):
@@ -490,6 +494,31 @@ def draw_spawns(params, rng_stage: str, key, P: int):
     u = rng.random(P)
     off = rng.random((P, 2))
     return rng, u, off
+
+
+def spawn_rain(state: ErosionState, u, off) -> dict:
+    """The rain spawns of ``u`` (P uniforms, unsorted) and ``off`` ((P, 2)
+    offsets) on the device (``pge_spawn_rain``: maps.spawn_particles,
+    maps.py:809-833): ``face``, ``x``, ``y`` (host arrays), the total spawn
+    weight (``w.sum()``, so ``volume0 = total / P``) and the count of
+    spawnable cells."""
+    P = int(np.asarray(u).shape[0])
+    state.reserve(P, 1, 1)
+    L = _lib.load()
+    dev = state.height.device
+    u_d = torch.as_tensor(u, dtype=torch.float64, device=dev)
+    off_d = torch.as_tensor(off, dtype=torch.float64, device=dev).contiguous()
+    face = torch.zeros(P, dtype=torch.int32, device=dev)
+    xs, ys, sed, dirs = (torch.zeros(P, dtype=torch.float64, device=dev) for _ in range(4))
+    scal = torch.zeros(1, dtype=torch.float64, device=dev)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    spawns = PgeSpawns(face=_ptr(face), x=_ptr(xs), y=_ptr(ys), sed=_ptr(sed), dir=_ptr(dirs), count=P, volume0=0.0)
+    check(L.pge_spawn_rain(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), _ptr(u_d), _ptr(off_d), P,
+                           ctypes.byref(spawns), _ptr(scal), _ptr(cnt), _ptr(state.workspace), state.workspace.numel(), _stream()),
+          "pge_spawn_rain")
+    torch.cuda.synchronize()
+    return {"face": face.cpu().numpy(), "x": xs.cpu().numpy(), "y": ys.cpu().numpy(), "total": float(scal.item()),
+            "n_spawnable": int(cnt.item())}
 
 
 class SpawnFeeder:

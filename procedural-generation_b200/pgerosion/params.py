@@ -122,6 +122,9 @@ class ErosionParams:
     pit_steps: int = 16
     chunk: int = 2048
     backend: str = "cpu"
+    #: no counterpart in the reference (its particles write one cell a step): the wave apply's
+    #: erode / deposit brush radius in cells, 0..4 (PgeParams.brush_radius)
+    brush_radius: int = 0
 
 
 @dataclass

@@ -20,6 +20,10 @@ computes on seeded synthetic inputs built by ``pgerosion.synth``:
   iterations, a set of droplets whose touched cells (plus a one-cell ring)
   are pairwise disjoint, and the reference ``trace_particles`` change lists
   and ``apply_changes`` results for them (particle.py:275-1042).
+* ``trace_isolated_c1.npz``, ``trace_isolated_n1024.npz`` -- isolated
+  droplets on the fresh N_c = 128 small world and N_c = 1024 Earth-default
+  world (rebuilt from seed 0 by the tests), with the reference's change
+  lists and accumulators for them under those workloads' knobs.
 * ``window_trace.npz`` -- one face of that N=48 world cut out as a window
   (``spherical=False``, F = 1; mask: an active basin inside a frozen
   margin inside an outside ring; ``deposit_on_exit``), loaded and unloaded
@@ -255,6 +259,105 @@ def gen_trace(cs, maps, pk, WorldParams):
         cell_size_m=st.height_unit_m, **res, acc=acc, pending=pending, disch_track=dtr, mom_track=mtr,
         apply_out=np.array([float(a) for a in ap]))
     print(f"trace_isolated: {keep.size} isolated droplets of {P}; deaths {np.bincount(res['sp_death'], minlength=6)}")
+
+
+def gen_isolated_configs(cs, maps, pk, WorldParams, which=("c1", "n1024")):
+    """Gate 1 on the benchmarked worlds: isolated droplets (paths plus a
+    one-cell ring pairwise disjoint) on the fresh N_c = 128 small world and
+    the fresh N_c = 1024 Earth-default world (the ones ``synth`` builds from
+    seed 0), traced by the reference's ``trace_particles`` and applied by its
+    ``apply_changes`` with those workloads' knobs, volume and concurrency
+    divisor.  The worlds are rebuilt by the tests from their seed and checked
+    against the bedrock digest stored here; the change lists are stored
+    compacted (``cl_count`` entries per droplet) and the accumulators as
+    their nonzero cells."""
+    from pgerosion import synth
+
+    for name in which:
+        if name == "c1":
+            world = synth.plain_small_world(0)
+            ours, P = synth.config_params("small")
+        else:
+            world = synth.earth_world(seed=0, N=1024, device="cpu")
+            ours, P = synth.config_params("earth")
+        N, H, cell = world.grid.N, world.grid.H, world.grid.cell_size_m
+        eo = ours.erosion
+        p = _world_params(WorldParams, N, H, cell, 0, world.land_fraction, iterations=int(eo.iterations),
+                          max_steps=int(eo.max_steps), friction=float(eo.friction), erodibility=float(eo.erodibility),
+                          deposition_rate=float(eo.deposition_rate), evap_rate=float(eo.evap_rate), uplift_mode=str(eo.uplift_mode))
+        st = _ref_state(cs, maps, world, p)
+        st.pack()
+        ep = p.erosion
+        NE = st.NE
+        rng = np.random.default_rng(4242 + N)
+        idx, w = maps.spawn_weights(st)
+        total = float(w.sum())
+        volume0 = total / P
+        chunk = maps.chunk_size(ep, P)
+        conc = chunk / (volume0 * P)
+        nc, nl = 1400, 200
+        pick = idx[np.searchsorted(np.cumsum(w), rng.random(nc) * total, side="right").clip(0, idx.size - 1)]
+        f = pick // (NE * NE)
+        rem = pick - f * NE * NE
+        x = (rem // NE - H) + rng.random(nc)
+        y = (rem % NE - H) + rng.random(nc)
+        inter = np.flatnonzero(np.pad(np.ones((6, N, N), bool), ((0, 0), (H, H), (H, H))).reshape(-1))
+        lp = inter[rng.integers(0, inter.size, nl)]
+        lf = lp // (NE * NE)
+        lrem = lp - lf * NE * NE
+        f = np.concatenate([f, lf])
+        x = np.concatenate([x, (lrem // NE - H) + 0.5])
+        y = np.concatenate([y, (lrem % NE - H) + 0.5])
+        sed = np.concatenate([np.zeros(nc), rng.random(nl) * 0.02 + 1e-4])
+        dirs = np.concatenate([np.zeros(nc), rng.random(nl) * 2 * np.pi])
+        max_steps = maps.max_steps_of(ep, N)
+        cap = int(pk.change_list_cap(max_steps, False))
+        allt = _ref_trace(pk, ep, st.samp, st.mask, N, H, True, False, f, x, y, sed, dirs, volume0, conc, max_steps, cap,
+                          st.height_unit_m)
+        own = st.grid.owner.reshape(-1)
+        taken = np.zeros(st.height.size, bool)
+        keep = []
+        for q in range(f.size):
+            cells = allt["cl_cell"][q * cap: q * cap + allt["cl_count"][q]].astype(np.int64)
+            c0 = (int(f[q]) * NE + int(np.floor(x[q])) + H) * NE + int(np.floor(y[q])) + H
+            cells = np.unique(np.concatenate([cells, [c0]]))
+            cf = cells // (NE * NE)
+            cr = cells - cf * NE * NE
+            ci, cj = cr // NE, cr % NE
+            ring = np.unique(np.concatenate([own[(cf * NE + np.clip(ci + di, 0, NE - 1)) * NE + np.clip(cj + dj, 0, NE - 1)]
+                                             for di in (-1, 0, 1) for dj in (-1, 0, 1)]))
+            if taken[ring].any():
+                continue
+            taken[ring] = True
+            keep.append(q)
+        keep = np.array(keep)
+        f, x, y, sed, dirs = f[keep], x[keep], y[keep], sed[keep], dirs[keep]
+        res = _ref_trace(pk, ep, st.samp, st.mask, N, H, True, False, f, x, y, sed, dirs, volume0, conc, max_steps, cap,
+                         st.height_unit_m)
+        acc = np.zeros_like(st.height)
+        pending = np.zeros_like(st.height)
+        dtr = np.zeros_like(st.height)
+        mtr = np.zeros_like(st.momentum)
+        samp = st.samp.copy()
+        cu = lambda k: float(getattr(ep, k)) / st.height_unit_m
+        pk.apply_changes(res["cl_cell"], res["cl_delta"], res["cl_vol"], res["cl_mom"], res["cl_count"], cap,
+                         st.height, st.sediment, acc, pending, samp, dtr, mtr, st.mask, cu("iter_erode"), cu("iter_deposit"),
+                         float(ep.fan_slope), False, cu("dep_floor_m"), float(ep.offshore_writeoff), np.zeros(1), False,
+                         st.lake_load, st.lake_id, st.lake_room)
+        n = keep.size
+        sel = np.concatenate([np.arange(q * cap, q * cap + res["cl_count"][q]) for q in range(n)])
+        touched = np.flatnonzero((acc != 0) | (pending != 0) | (dtr != 0) | (mtr[..., 0] != 0) | (mtr[..., 1] != 0))
+        np.savez_compressed(
+            HERE / f"trace_isolated_{name}.npz", world=name, N=N, H=H, cell_size_m=cell, P=P,
+            bedrock_sha=hashlib.sha256(np.ascontiguousarray(world.bedrock).tobytes()).hexdigest(),
+            sp_face=f.astype(np.int64), sp_x=x, sp_y=y, sp_sed=sed, sp_dir=dirs, volume0=volume0, conc_scale=conc, cap=cap,
+            max_steps=max_steps, params=json.dumps({k: getattr(ep, k) for k in ep.__dataclass_fields__}),
+            cl_count=res["cl_count"], sp_death=res["sp_death"], cl_cell=res["cl_cell"][sel], cl_delta=res["cl_delta"][sel],
+            cl_vol=res["cl_vol"][sel], cl_mom=res["cl_mom"][sel], touched=touched, acc=acc.reshape(-1)[touched],
+            pending=pending.reshape(-1)[touched], disch_track=dtr.reshape(-1)[touched],
+            mom_track=mtr.reshape(-1, 2)[touched])
+        print(f"trace_isolated_{name}: {n} isolated droplets of {nc + nl} candidates; deaths "
+              f"{np.bincount(res['sp_death'], minlength=6)}; entries {sel.size}")
 
 
 def _ref_trace(pk, ep, st_samp, mask, N, H, spherical, deposit_on_exit, f, x, y, sed, dirs, volume0, conc, max_steps, cap, unit,
@@ -988,7 +1091,8 @@ def gen_lake_fill_steps(cs, maps, pk, WorldParams):
 def main(bake: str, only: str | None = None):
     cs, maps, pk, WorldParams = _ref(bake)
     gens = {"vectors": lambda: gen_vectors(cs), "ref_vectors": lambda: gen_ref_vectors(bake), "halo": lambda: gen_halo(cs),
-            "trace": lambda: gen_trace(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
+            "trace": lambda: gen_trace(cs, maps, pk, WorldParams),
+            "isolated_configs": lambda: gen_isolated_configs(cs, maps, pk, WorldParams), "window": lambda: gen_window(cs, maps, pk, WorldParams),
             "isostasy": lambda: gen_isostasy(cs, maps, pk, WorldParams),
             "step": lambda: gen_step(cs, maps, pk, WorldParams), "route": lambda: gen_route(cs, maps, pk, WorldParams),
             "step_route": lambda: gen_step_route(cs, maps, pk, WorldParams), "sea": lambda: gen_sea(cs, maps, pk, WorldParams),

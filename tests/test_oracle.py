@@ -536,3 +536,22 @@ def test_lake_fill_steps_match_reference_bit_exact():
             assert s["lakes"] == stats[it]["lakes"], it
     for k in ("height", "sediment", "discharge", "momentum", "pending", "base", "lake_flag", "lake_load", "lake_id", "lake_room"):
         assert np.array_equal(getattr(st, k), fx[k]), k
+
+
+def test_brush_restatement_conserves_and_spreads():
+    """oracle.brush_spread (the library's brush, no reference counterpart): a unit
+    change in the middle of a face spreads over the footprint in proportion to
+    the weights; next to a face edge the weights renormalise over the interior;
+    the total is kept."""
+    N, H, r = 16, 2, 3
+    NE = N + 2 * H
+    acc = np.zeros((6, NE, NE))
+    acc[2, 10, 10] = 1.0
+    acc[4, H, H + 5] = -2.0  # on the interior's first row: the footprint is cut by the edge
+    out = orc.brush_spread(acc, np.ones(acc.shape, np.uint8), N, H, r)
+    assert abs(out.sum() - acc.sum()) < 1e-12
+    q = orc.brush_weights(r)
+    assert q[r, r] == 1024 * (r + 1) and q[0, 0] == 0  # corners beyond r + 1
+    np.testing.assert_allclose(out[2, 10 - r:10 + r + 1, 10 - r:10 + r + 1], q / q.sum(), rtol=1e-14)
+    assert np.all(out[4, :H] == 0.0) and np.all(out[4, :, :H] == 0.0)  # nothing on the halo
+    assert abs(out[4].sum() + 2.0) < 1e-12
