@@ -40,6 +40,14 @@ for p in (ROOT, ROOT / "procedural-generation_b200"):
 #: metric (24 B), base / evap / hardness / sediment (16 B), mask (1 B);
 #: scattered int64 terrain change, discharge and two momentum tracks (32 B)
 BYTES_PER_STEP = 137
+#: the brush measurement (radius 3, BASELINE's c1 / c2 brush): the same gathers (105 B), the
+#: int64 terrain change scattered over the footprint (45 cells within distance < 4: 360 B) and the
+#: discharge and two momentum tracks on the step's own cell (24 B)
+BRUSH_RADIUS = 3
+BRUSH_CELLS = 45
+BRUSH_BYTES_PER_STEP = 105 + 8 * BRUSH_CELLS + 24
+#: the planet level's brush (radius 2): 25 cells within distance < 3
+PLANET_BRUSH_CELLS = 25
 
 
 def run_batched(args, rank, world_size, dist, dev):
@@ -265,6 +273,46 @@ def launches_per_iteration(nw: int, pending: bool, creep: bool, ordered: bool) -
     return spawn + droplets + thermal + uplift + datum + halo
 
 
+def _side_leg(st, params, P, kw, it0, nsteps, dev, dist, bytes_per_step):
+    """A secondary measurement on the evolved world: 3 untimed iterations with
+    ``kw``, then ``nsteps`` timed ones (CUDA events around the whole steps and
+    around each droplet pass); returns its result and the next iteration key."""
+    import torch
+
+    from pgerosion import maps as gm
+
+    for k in range(3):
+        rng, u, off = gm.draw_spawns(params, "erosion", (it0 + k,), P)
+        gm.step(st, params, it0 + k, predrawn=(rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)), **kw)
+    pre = []
+    for k in range(nsteps):
+        rng, u, off = gm.draw_spawns(params, "erosion", (it0 + 3 + k,), P)
+        pre.append((rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)))
+    ta = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e2[0].record()
+    steps = 0
+    for k in range(nsteps):
+        s2 = gm.step(st, params, it0 + 3 + k, predrawn=pre[k], events=ta[k], **kw)
+        steps += s2["droplet_steps"]
+    e2[1].record()
+    torch.cuda.synchronize()
+    t2 = torch.tensor([steps, e2[0].elapsed_time(e2[1])], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t2[:1])
+        dist.all_reduce(t2[1:], op=dist.ReduceOp.MAX)
+    avg = float(np.mean([a.elapsed_time(b) for a, b in ta]))
+    ach = steps / max(nsteps, 1) * bytes_per_step / (avg * 1e-3) / 1e9
+    peak, _ = _peaks()
+    res = {"value": float(t2[0]) / (float(t2[1]) * 1e-3), "unit": "droplet-steps/s", "steps": nsteps,
+           "ms_per_step": float(t2[1]) / nsteps,
+           "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "ms_per_launch": avg}}
+    return res, it0 + 3 + nsteps
+
+
 def run_b200(args, rank, world_size, dist):
     import torch
 
@@ -338,44 +386,22 @@ def run_b200(args, rank, world_size, dist):
     e2e_ms = ee[0].elapsed_time(ee[1])
     feeder.close()
     (steps_all, e2e_all), (ms_max, e2e_ms_max) = reduce_totals(dist, [steps_done, e2e_steps], [ms, e2e_ms], device=dev)
-    alt = None
+    alt = brush = None
+    it_next = n_total + args.steps
     if apply == _lib.APPLY_ORDERED and not args.no_alt:
         # the order-free wave apply on the same world (one wave per iteration): faster, not the
         # reference's serial apply
         kw_alt = dict(kw, apply=_lib.APPLY_WAVE, wave=max(P + P // 8, 1))
-        it0 = n_total + args.steps
-        for k in range(3):
-            rng, u, off = gm.draw_spawns(params, "erosion", (it0 + k,), P)
-            gm.step(st, params, it0 + k, predrawn=(rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)), **kw_alt)
-        pre_alt = []
-        for k in range(args.alt_steps):
-            rng, u, off = gm.draw_spawns(params, "erosion", (it0 + 3 + k,), P)
-            pre_alt.append((rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev)))
-        ta2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.alt_steps)]
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        e2 = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        e2[0].record()
-        alt_steps = 0
-        for k in range(args.alt_steps):
-            s2 = gm.step(st, params, it0 + 3 + k, predrawn=pre_alt[k], events=ta2[k], **kw_alt)
-            alt_steps += s2["droplet_steps"]
-        e2[1].record()
-        torch.cuda.synchronize()
-        alt_ms = e2[0].elapsed_time(e2[1])
-        t2 = torch.tensor([alt_steps, alt_ms], dtype=torch.float64, device=dev)
-        if dist:
-            dist.all_reduce(t2[:1])
-            dist.all_reduce(t2[1:], op=dist.ReduceOp.MAX)
-        avg2 = float(np.mean([a.elapsed_time(b) for a, b in ta2]))
-        ach2 = alt_steps / max(args.alt_steps, 1) * BYTES_PER_STEP / (avg2 * 1e-3) / 1e9
-        peak, _ = _peaks()
-        alt = {"apply": "wave (order-free, int64 fixed point; not the reference's serial apply)",
-               "value": float(t2[0]) / (float(t2[1]) * 1e-3), "unit": "droplet-steps/s", "steps": args.alt_steps,
-               "ms_per_step": float(t2[1]) / args.alt_steps,
-               "roofline": {"bound": "hbm", "achieved": ach2, "peak": peak, "unit": "GB/s", "frac": ach2 / peak,
-                            "ms_per_launch": avg2}}
+        alt, it_next = _side_leg(st, params, P, kw_alt, it_next, args.alt_steps, dev, dist, BYTES_PER_STEP)
+        alt["apply"] = "wave (order-free, int64 fixed point; not the reference's serial apply)"
+        if not args.no_brush:
+            # the same with the erode / deposit brush of radius 3 (BASELINE's c2 brush; no reference counterpart)
+            import dataclasses
+
+            pb = dataclasses.replace(params, erosion=dataclasses.replace(params.erosion, brush_radius=BRUSH_RADIUS))
+            brush, it_next = _side_leg(st, pb, P, kw_alt, it_next, args.alt_steps, dev, dist, BRUSH_BYTES_PER_STEP)
+            brush["apply"] = f"wave apply with the erode / deposit brush, radius {BRUSH_RADIUS} ({BRUSH_CELLS} cells)"
+            brush["bytes_per_step"] = BRUSH_BYTES_PER_STEP
     batched = None
     if not args.no_batch:
         batched = run_batched(args, rank, world_size, dist, dev)
@@ -437,6 +463,8 @@ def run_b200(args, rank, world_size, dist):
     }
     if alt is not None:
         out["alt_wave_apply"] = alt
+    if brush is not None:
+        out["brush"] = brush
     if batched is not None:
         out["batched_worlds"] = batched
     if adjoint is not None:
@@ -446,6 +474,68 @@ def run_b200(args, rank, world_size, dist):
     if world_size == 1 and not args.no_cpu:
         w_host = world
         out["cpu_baseline"] = cpu_baseline(params, P, w_host, seconds=args.cpu_seconds)
+    return out
+
+
+def run_planet(args, dev):
+    """Config c5: the planet-wide N_c = 8192 level on one GPU (pgerosion.planet): 2^24 droplets an
+    iteration, max_steps 128, the wave apply with the brush of radius 2, heights to pinned host memory
+    every 20 iterations.  Prints its own JSON line."""
+    import torch
+
+    from pgerosion import _lib
+    from pgerosion import maps as gm
+    from pgerosion import planet
+
+    N = args.n or planet.PLANET_N
+    params = planet.planet_params(N=N)
+    P = planet.PLANET_DROPLETS if N == planet.PLANET_N else max(1, (6 * N * N) // 24)
+    t0 = time.time()
+    st = planet.planet_state(N=N, device=dev)
+    build_s = time.time() - t0
+    kw = dict(n_particles=P, apply=_lib.APPLY_WAVE, wave=P + P // 8)
+    timeline = planet.Timeline(st, every=20)
+    total = args.warmup + args.steps if args.planet_iterations <= 0 else args.planet_iterations
+    for it in range(args.warmup if args.planet_iterations <= 0 else 0):
+        gm.step(st, params, it, **kw)
+        timeline.maybe(it)
+    torch.cuda.synchronize()
+    first = args.warmup if args.planet_iterations <= 0 else 0
+    ta = []
+    steps = 0
+    with ClockSampler(dev.index) as clk:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        w0 = time.perf_counter()
+        ev[0].record()
+        for it in range(first, total):
+            e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            s = gm.step(st, params, it, events=e, **kw)
+            timeline.maybe(it + 1)
+            steps += s["droplet_steps"]
+            ta.append(e)
+        ev[1].record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+    timeline.wait()
+    ms = ev[0].elapsed_time(ev[1])
+    n = total - first
+    avg = float(np.mean([a.elapsed_time(b) for a, b in ta]))
+    bytes_step = 105 + 8 * PLANET_BRUSH_CELLS + 24
+    ach = steps / n * bytes_step / (avg * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    a = st.to_numpy() if N <= 2048 else None
+    out = {"metric": "droplet-steps/s", "value": steps / (ms * 1e-3), "unit": "droplet-steps/s", "n_gpus": 1, "steps": n,
+           "warmup": first, "ms_per_step": ms / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded N_c=1024 fBm + ridge base, bicubic to N_c=8192, + 3 detail octaves; built on the device)",
+           "config": {"workload": f"planet level: cube-sphere N_c={N}, H=2, {P} droplets/iteration, max_steps 128, wave apply, "
+                                  f"brush radius 2, timeline every 20 iterations", "N_c": N, "droplets_per_iteration": P},
+           "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                        "kernel": "droplet pass (pge_trace_apply, one wave)", "ms_per_launch": avg, "bytes_per_step": bytes_step},
+           "stage": {"iterations": n, "wall_s": wall, "build_s": build_s, "timeline_frames": [f for f, _ in timeline.frames],
+                     "device_gb_peak": torch.cuda.max_memory_allocated(dev) / 1e9},
+           "clocks": clk.summary()}
+    if a is not None:
+        out["stage"]["land_fraction"] = float(np.mean((a["height"] + a["sediment"])[st.interior] >= 0))
     return out
 
 
@@ -501,6 +591,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)
+    ap.add_argument("--no-brush", action="store_true", help="skip the brush (radius 3) measurement")
+    ap.add_argument("--config", default="c2", choices=("c2", "c5"),
+                    help="c2: the Earth-default N_c=1024 line (default); c5: the N_c=8192 planet level on one GPU")
+    ap.add_argument("--planet-iterations", type=int, default=0, help="c5: run this many iterations as the timed stage")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     ap.add_argument("--batch-worlds", type=int, default=64)
@@ -521,6 +615,12 @@ def main():
     dist = None
     if args.impl == "reference":
         out = run_reference(args, rank)
+    elif args.config == "c5":
+        import torch
+
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+        torch.cuda.set_device(dev)
+        out = run_planet(args, dev) if rank == 0 else None
     elif args.adjoint_only:
         import torch
 
