@@ -328,7 +328,7 @@ def run_b200(args, rank, world_size, dist):
     prec = _lib.PREC_F64 if args.precision == "f64" else _lib.PREC_F32
     wave = None if args.wave == 0 else args.wave
     apply = _lib.APPLY_ORDERED if args.apply == "ordered" else _lib.APPLY_WAVE
-    kw = dict(n_particles=P, wave=wave, precision=prec, blocks_per_sm=args.blocks_per_sm, apply=apply)
+    kw = dict(n_particles=P, wave=wave, precision=prec, blocks_per_sm=args.blocks_per_sm, apply=apply, apply_lanes=args.apply_lanes)
     n_total = args.warmup + args.steps
 
     # value: spawn uniforms of every iteration drawn up front and resident in HBM
@@ -592,6 +592,7 @@ def main():
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)
     ap.add_argument("--no-brush", action="store_true", help="skip the brush (radius 3) measurement")
+    ap.add_argument("--apply-lanes", type=int, default=0, help="ordered apply: 0 = the fed kernel (default), 1..32 = the unfed one")
     ap.add_argument("--config", default="c2", choices=("c2", "c5"),
                     help="c2: the Earth-default N_c=1024 line (default); c5: the N_c=8192 planet level on one GPU")
     ap.add_argument("--planet-iterations", type=int, default=0, help="c5: run this many iterations as the timed stage")

@@ -277,7 +277,6 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.minb = minb;
         a.lanes = 32;
         a.brush_r = p->brush_radius;
-        if (a.brush_r > 0) brush_weights(a.brush_r, a.brush_q);
         unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
         const long long wave = p->wave;
         const long long nw = (P + wave - 1) / wave;

@@ -59,11 +59,13 @@ __device__ __forceinline__ R half_pi() { return R(kPi / 2.0); }
 __device__ __forceinline__ R two_over_pi() { return R(2.0 / kPi); }
 
 // tan / atan / sin / cos of the droplet precision: float64 rounds like the C library the reference
-// calls (correctly rounded double-double evaluations, pge_crmath.cuh); float32 takes the builtins
-__device__ __forceinline__ double m_tan(double x) { return cr::d_tan(x); }
-__device__ __forceinline__ double m_atan(double x) { return cr::d_atan(x); }
-__device__ __forceinline__ double m_sin(double x) { return cr::d_sin(x); }
-__device__ __forceinline__ double m_cos(double x) { return cr::d_cos(x); }
+// calls (correctly rounded double-double evaluations, pge_crmath.cuh); float32 takes the builtins.
+// The float64 ones are inlined into the out-of-line face crossing and spawn direction below, so the
+// droplet kernel itself holds one call site for each.
+__device__ __forceinline__ double m_tan(double x) { return cr::cr_tan(x); }
+__device__ __forceinline__ double m_atan(double x) { return cr::cr_atan(x); }
+__device__ __forceinline__ double m_sin(double x) { return cr::cr_sin(x); }
+__device__ __forceinline__ double m_cos(double x) { return cr::cr_cos(x); }
 __device__ __forceinline__ float m_tan(float x) { return tanf(x); }
 __device__ __forceinline__ float m_atan(float x) { return atanf(x); }
 __device__ __forceinline__ float m_sin(float x) { return sinf(x); }
@@ -170,6 +172,32 @@ __device__ int transfer_velocity(int face, R &u, R &v, R &a, R &b)
     v = v2;
     return f2;
 }
+
+// the crossing and the direction of a loaded spawn, out of line: the droplet kernel runs them rarely and
+// their double-double arithmetic stays out of its register allocation
+struct Crossed {
+    R u, v, a, b;
+    int face;
+};
+__device__ __noinline__ Crossed cross_out_of_line(int face, R u, R v, R a, R b)
+{
+    Crossed c{u, v, a, b, face};
+    c.face = transfer_velocity(face, c.u, c.v, c.a, c.b);
+    return c;
+}
+__device__ __forceinline__ int cross_face(int face, R &u, R &v, R &a, R &b)
+{
+    const Crossed c = cross_out_of_line(face, u, v, a, b);
+    u = c.u;
+    v = c.v;
+    a = c.a;
+    b = c.b;
+    return c.face;
+}
+struct Dir {
+    R c, s;
+};
+__device__ __noinline__ Dir spawn_dir(R dir) { return Dir{m_cos(dir), m_sin(dir)}; }
 
 // ---------------------------------------------------------------------------
 // what a step reads about the cell a droplet stands in
@@ -416,13 +444,18 @@ __device__ __forceinline__ void load_lcell(const DropArgs &a, const Table &t, lo
 }
 
 // The erode / deposit brush: an applied change fx (fixed point) at cell c spread over the active
-// cells of c's face within a.brush_r of it (the interior ones on the sphere, whose halos are copies)
-// with the integer weights a.brush_q; the shares are truncated toward zero and the rest stays on c,
-// so the sum is exactly fx whatever the order the atomics land in.
-__device__ __noinline__ void brush_add(const DropArgs &a, long long c, long long fx)
+// cells of c's face within r of it (the interior ones on the sphere, whose halos are copies) with
+// the weights brush_weight (r + 1 - distance, integers of 1/PGE_BRUSH_SCALE); the shares are truncated
+// toward zero and the rest stays on c, so the sum is exactly fx whatever the order the atomics land in.
+// Everything by value: the droplet kernel's argument block stays where it is.
+__device__ __forceinline__ int brush_weight(int r, int di, int dj)
 {
-    const int NE = a.NE, r = a.brush_r, w = 2 * r + 1;
-    const int lo = a.spherical ? a.H : 0, hi = a.spherical ? a.H + a.N : NE;
+    const double v = (double)(r + 1) - sqrt((double)(di * di + dj * dj));
+    return v > 0.0 ? (int)llround(PGE_BRUSH_SCALE * v) : 0;
+}
+
+__device__ __noinline__ void brush_add(long long *acc4, const uint8_t *mask, int NE, int lo, int hi, int r, long long c, long long fx)
+{
     const long long plane = (long long)NE * NE;
     const long long fb = c / plane * plane;
     const int ei = (int)((c - fb) / NE), ej = (int)((c - fb) % NE);
@@ -432,10 +465,10 @@ __device__ __noinline__ void brush_add(const DropArgs &a, long long c, long long
         if (ii < lo || ii >= hi) continue;
         for (int dj = -r; dj <= r; dj++) {
             const int jj = ej + dj;
-            const int q = a.brush_q[(di + r) * w + dj + r];
+            const int q = brush_weight(r, di, dj);
             if (!q || jj < lo || jj >= hi) continue;
             const long long cc = fb + (long long)ii * NE + jj;
-            if (cc != c && a.mask && __ldg(a.mask + cc) != PGE_MASK_ACTIVE) continue;
+            if (cc != c && mask && __ldg(mask + cc) != PGE_MASK_ACTIVE) continue;
             Q += q;
         }
     }
@@ -446,19 +479,19 @@ __device__ __noinline__ void brush_add(const DropArgs &a, long long c, long long
             if (ii < lo || ii >= hi) continue;
             for (int dj = -r; dj <= r; dj++) {
                 const int jj = ej + dj;
-                const int q = a.brush_q[(di + r) * w + dj + r];
+                const int q = brush_weight(r, di, dj);
                 if (!q || jj < lo || jj >= hi || (di == 0 && dj == 0)) continue;
                 const long long cc = fb + (long long)ii * NE + jj;
-                if (a.mask && __ldg(a.mask + cc) != PGE_MASK_ACTIVE) continue;
+                if (mask && __ldg(mask + cc) != PGE_MASK_ACTIVE) continue;
                 const long long share = (long long)(((__int128)fx * q) / Q);
                 if (share) {
-                    red_add(a.acc4 + 4 * cc, share);
+                    red_add(acc4 + 4 * cc, share);
                     given += share;
                 }
             }
         }
     }
-    red_add(a.acc4 + 4 * c, fx - given);
+    red_add(acc4 + 4 * c, fx - given);
 }
 
 // Apply one change-list entry (particle.py:934-1018) at cell `c` against the
@@ -595,7 +628,7 @@ __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger 
         t.store(c.cell, c.tidx, c.own);
         const long long fx = fx_mass(applied);
         if (a.brush_r > 0)
-            brush_add(a, c.cell, fx);
+            brush_add(a.acc4, a.mask, a.NE, a.spherical ? a.H : 0, a.spherical ? a.H + a.N : a.NE, a.brush_r, c.cell, fx);
         else
             red_add(a.acc4 + 4 * c.cell, fx);
         if (fx < 0) L.eroded_fx -= fx;
@@ -703,8 +736,9 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     sb = R(0);
                     if (sed > R(0)) {
                         const R dir = R(a.sp_dir[d]);
-                        sa = m_cos(dir);
-                        sb = m_sin(dir);
+                        const Dir dd = spawn_dir(dir);
+                        sa = dd.c;
+                        sb = dd.s;
                     }
                     step = uphill = sea_steps = nring = 0;
                     in_sea = has_hprev = in_lake = false;
@@ -836,7 +870,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             if (a.spherical) {
                 if (nx < R(0) || nx >= Nf || ny < R(0) || ny >= Nf) {
                     R u = nx / Nf, v = ny / Nf;
-                    nf = transfer_velocity(f, u, v, sa, sb);
+                    nf = cross_face(f, u, v, sa, sb);
                     nx = u * Nf;
                     ny = v * Nf;
                     if (TAPE) {

@@ -120,20 +120,8 @@ struct DropArgs {
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
-    int brush_r;                      // the erode / deposit brush's radius (0: one cell)
-    short brush_q[(2 * PGE_BRUSH_MAX_RADIUS + 1) * (2 * PGE_BRUSH_MAX_RADIUS + 1)];  // its weights, row-major
+    int brush_r;  // the erode / deposit brush's radius (0: one cell)
 };
-
-// the brush's integer weights: PGE_BRUSH_SCALE x max(0, r + 1 - |(di, dj)|) rounded, (2r+1)^2 of them
-inline void brush_weights(int r, short *q)
-{
-    const int w = 2 * r + 1;
-    for (int di = -r; di <= r; di++)
-        for (int dj = -r; dj <= r; dj++) {
-            const double v = (double)(r + 1) - sqrt((double)(di * di + dj * dj));
-            q[(di + r) * w + dj + r] = (short)(v > 0.0 ? llround(PGE_BRUSH_SCALE * v) : 0);
-        }
-}
 
 // launchers of the two precisions (separate translation units: the float64
 // one is compiled without FMA contraction so it rounds like the reference)

@@ -81,7 +81,11 @@ def test_device_mapping_against_the_reference_vector_file(cuda):
     print(f"reference vector file, {n} records: to_sphere bit-exact in {np.mean(u_xyz.max(1) == 0):.2%} (max {u_xyz.max()} ulp), "
           f"from_sphere bit-exact in {np.mean(u_uv.max(1) == 0):.2%} (max {u_uv.max()} ulp)")
     assert np.array_equal(f2, g["face2"])
-    assert u_xyz.max() <= 2 and u_uv.max() <= 2  # the reference's bar for code other than its scalar functions
+    # the reference's bar for code other than its scalar functions: within 2 eps absolute
+    # (bake/tests/test_cubesphere.py:396-402); a last-bit difference of u near 0 is many ulps of u
+    eps = np.finfo(np.float64).eps
+    assert np.abs(xyz - g["xyz"]).max() <= 2 * eps
+    assert np.abs(uv2 - np.stack([g["u2"], g["v2"]], 1)).max() <= 2 * eps
     assert np.mean(u_xyz.max(1) == 0) > 0.99 and np.mean(u_uv.max(1) == 0) > 0.99
 
 
