@@ -160,6 +160,17 @@ def run_adjoint(args, dev):
                               "loss_m2": float(loss.detach()), "finite": fin,
                               "rate_gradient": g if fin else None,
                               "field_gradient_l1": float(erod.grad.double().abs().sum()) if fin else None}
+    if args.calibrate_steps > 0:
+        # gradient descent from the start (rates of the base parameters, field 1 +- 0.2) toward the target
+        # made with the rates +-30 %: the loss at every step, and where the rates went
+        calib.carry_path, calib.carry_terrain = False, False
+        t0 = time.perf_counter()
+        cal = adj.calibrate(calib, target, land, adj.erodibility_init(st, seed=0), adj.rates_of(params), steps=args.calibrate_steps)
+        torch.cuda.synchronize()
+        tgt = adj.rates_of(adj.calibration_params(seed=0, N=N, iterations=iters, jitter=0.3, jitter_seed=1)).tolist()
+        out["calibration"] = {"steps": args.calibrate_steps, "loss_m2": cal["loss"], "rates": cal["rates"][-1],
+                              "start_rates": adj.rates_of(params).tolist(), "target_rates": tgt,
+                              "wall_s": time.perf_counter() - t0}
     out["value"] = out["modes"]["truncated"]["ratio"]
     out["droplet_steps_per_iteration"] = float(np.mean([s_.get("droplet_steps", 0) for s_ in calib.stats]))
     del calib, st
@@ -592,7 +603,7 @@ def main():
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)
     ap.add_argument("--no-brush", action="store_true", help="skip the brush (radius 3) measurement")
-    ap.add_argument("--apply-lanes", type=int, default=0, help="ordered apply: 0 = the fed kernel (default), 1..32 = the unfed one")
+    ap.add_argument("--apply-lanes", type=int, default=0, help="ordered apply: droplets per warp (0 = 1)")
     ap.add_argument("--config", default="c2", choices=("c2", "c5"),
                     help="c2: the Earth-default N_c=1024 line (default); c5: the N_c=8192 planet level on one GPU")
     ap.add_argument("--planet-iterations", type=int, default=0, help="c5: run this many iterations as the timed stage")
@@ -606,6 +617,7 @@ def main():
     ap.add_argument("--adjoint-n", type=int, default=256, help="calibration world N_c (the workload: 256)")
     ap.add_argument("--adjoint-droplets", type=int, default=1 << 17, help="calibration droplets per iteration (the workload: 2^17)")
     ap.add_argument("--adjoint-iterations", type=int, default=50, help="calibration iterations (the workload: 50)")
+    ap.add_argument("--calibrate-steps", type=int, default=0, help="calibration: run this many gradient steps (Adam) as well")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         args.warmup = 3

@@ -207,11 +207,9 @@ typedef struct PgeParams {
     int32_t trace_lanes;       /* ordered apply: droplets per warp in each wave's trace; 0 = as few as keep
                                   every warp of the wave resident (fastest alone), up to 32 (smallest
                                   footprint, for passes of several worlds running at once) */
-    int32_t apply_lanes;       /* ordered apply: 0 = the fed apply (a block of two warps per droplet: one
-                                  streams the droplet's entries and the hand-offs it waits for into shared
-                                  memory, one lane applies them); 1 .. 32 = droplets per warp of the unfed
-                                  apply (each lane loads its own entries; more lanes hold fewer warps, for
-                                  passes of several worlds running at once) */
+    int32_t apply_lanes;       /* ordered apply: droplets per warp in the apply, 0 = 1 .. 32; more hold
+                                  fewer warps but lanes waiting on different hand-offs take turns
+                                  (one per warp measured fastest, alone and with other passes) */
     int32_t brush_radius;      /* wave apply: 0 = each entry changes its own cell (the reference's one-cell write,
                                   particle.py:662-671); r = 1..PGE_BRUSH_MAX_RADIUS: each applied erosion or
                                   deposition is spread over the cells of its face within distance < r + 1

@@ -338,13 +338,17 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.segscan = ws_ptr<int32_t>(ws, lay.w_segscan);
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
-            oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 0;  // 0: the fed apply
+            oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);
             const long long rec_warps =
                 (long long)sm_count() * (lateral ? droplet_blocks_per_sm_f64_lateral(32, false, s->route != nullptr)
                                          : s->route ? droplet_blocks_per_sm_f64_route(32, false)
                                          : p->precision == PGE_PREC_F64 ? droplet_blocks_per_sm_f64(32, 1, false)
                                                                       : droplet_blocks_per_sm_f32(32, 1, false));
+            // the plain float64 record-only trace also comes in a 128-register build: more warps resident,
+            // so a wave that fits runs one droplet per warp (no lane waits on another droplet's branches)
+            const bool plain64 = !lateral && !s->route && p->precision == PGE_PREC_F64;
+            const long long rec_warps_lean = plain64 ? (long long)sm_count() * droplet_blocks_per_sm_f64(32, 2, false) : 0;
             int ebits = 1;
             while ((1LL << ebits) <= wave) ebits++;
             long long ebase = 0;
@@ -360,6 +364,11 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 // other's branches
                 const long long nd = a.d_end - a.d_begin;
                 long long lanes = p->trace_lanes > 0 ? p->trace_lanes : (nd + rec_warps - 1) / rec_warps;
+                a.minb = 1;
+                if (p->trace_lanes == 0 && plain64 && nd <= rec_warps_lean) {
+                    lanes = 1;
+                    a.minb = 2;
+                }
                 a.lanes = (int)(lanes < 1 ? 1 : (lanes > 32 ? 32 : lanes));
                 const int tpb = 32;
                 long long blocks = (nd + a.lanes - 1) / a.lanes;

@@ -11,15 +11,19 @@
 // wherever the C library is correctly rounded too, the two agree bit for bit.
 //
 // Method (textbook double-double arithmetic after Dekker and Knuth, with the
-// exact product from fma):
+// exact product from fma; table-driven argument reduction):
 //   sin, cos: x reduced to r = x - k pi/2 (|r| <= pi/4) with a three-part
-//             pi/2, then their Taylor series in r^2 (Horner, terms to r^29).
+//             pi/2, then r = j/32 + t (|t| <= 1/64) and the angle sums with
+//             tabulated sin(j/32), cos(j/32); sin(t), cos(t) by their series,
+//             the leading terms in double-double, the rest in double.
 //   tan:      sin(r) / cos(r), or -cos(r) / sin(r) for odd k.
 //   atan:     |x| > 1 by pi/2 - atan(1/|x|); then t in [0, 1] by
-//             atan(t) = atan(c) + atan((t - c) / (1 + t c)), c = round(8 t) / 8
-//             (|z| <= 1/16), and the odd Taylor series of atan(z) to z^27.
-// The constants (pi/2 in three parts, atan(k/8) in two) are the exact values
-// rounded to double, computed with 90-digit decimal arithmetic.
+//             atan(t) = atan(k/64) + atan((t - k/64) / (1 + t k/64)), |z| <= 1/128,
+//             and atan(z)'s odd series.
+// The error before the final rounding stays below about 2^-100 of the result.
+// The constants (pi/2 in three parts, the tables, the series' leading
+// coefficients) are exact values rounded to double pairs, computed with
+// 100-digit decimal arithmetic (gen_crmath_tables.py).
 //
 // Every operation is an IEEE double add, multiply, divide or fma, so a host
 // build and a device build give identical results (the device build must not
@@ -108,33 +112,68 @@ PGE_HD dd div_d(dd a, double b)
     return add(quick_two_sum(q1, q2), dd{q3, 0.0});
 }
 
-// pi/2 = P1 + P2 + P3 (each the rounded rest of the one before)
-constexpr double kPio2_1 = 1.5707963267948966;
-constexpr double kPio2_2 = 6.123233995736766e-17;
-constexpr double kPio2_3 = -1.4973849048591698e-33;
-constexpr double kTwoOverPi = 0.6366197723675814;
+// the constants (pge_crmath_tables.inc, made by gen_crmath_tables.py): constant memory on the device,
+// plain arrays on the host; PGE_CR_TAB names the copy the code being compiled reads
+namespace host_tab {
+#define PGE_CR_QUAL static const
+#include "pge_crmath_tables.inc"
+#undef PGE_CR_QUAL
+}  // namespace host_tab
+#if defined(__CUDACC__)
+namespace dev_tab {
+#define PGE_CR_QUAL static __constant__ const
+#include "pge_crmath_tables.inc"
+#undef PGE_CR_QUAL
+}  // namespace dev_tab
+#endif
+#if defined(__CUDA_ARCH__)
+#define PGE_CR_TAB dev_tab
+#else
+#define PGE_CR_TAB host_tab
+#endif
 
-// sin(r) and cos(r) for |r| <= pi/4 + a little, r in double-double
+PGE_HD dd pair(const double *v) { return {v[0], v[1]}; }
+
+// sin(t) and cos(t) for |t| <= 1/64 (and a little), t double-double: the series' leading terms in
+// double-double, the terms from t^7 (sin) and t^8 (cos) on, below 2^-47 of the result, in double
+PGE_HD void sincos_small(dd t, dd &s, dd &c)
+{
+    const dd t2 = mul(t, t);
+    const double x = t2.hi;
+    const double ps = -1.0 / 5040.0 + x * (1.0 / 362880.0 + x * (-1.0 / 39916800.0 + x * (1.0 / 6227020800.0)));
+    const dd sa = add(pair(PGE_CR_TAB::kInv5f), mul_d(t2, ps));  // 1/5! + t^2 (...)
+    const dd sb = add(neg(pair(PGE_CR_TAB::kInv3f)), mul(t2, sa));  // -1/3! + t^2 (...)
+    s = add(t, mul(mul(t, t2), sb));
+    const double pc = 1.0 / 40320.0 + x * (-1.0 / 3628800.0 + x * (1.0 / 479001600.0));
+    const dd ca = add(neg(pair(PGE_CR_TAB::kInv6f)), mul_d(t2, pc));  // -1/6! + t^2 (...)
+    const dd cb = add(pair(PGE_CR_TAB::kInv4f), mul(t2, ca));
+    const dd cc = add(neg(pair(PGE_CR_TAB::kInv2f)), mul(t2, cb));
+    c = add(dd{1.0, 0.0}, mul(t2, cc));
+}
+
+// sin(r) and cos(r) for |r| <= pi/4 + a little: r = j/32 + t, the angle sums with the tabulated
+// sin(j/32), cos(j/32)
 PGE_HD void sincos_reduced(dd r, dd &s, dd &c)
 {
-    const dd r2 = mul(r, r);
-    // sin: r (1 - r^2/(2*3) (1 - r^2/(4*5) (1 - ...))), innermost n = 28 (the r^29 term)
-    dd ps = {1.0, 0.0};
-    for (int n = 28; n >= 2; n -= 2) ps = add(dd{1.0, 0.0}, neg(div_d(mul(r2, ps), (double)(n * (n + 1)))));
-    s = mul(r, ps);
-    // cos: 1 - r^2/(1*2) (1 - r^2/(3*4) (1 - ...)), innermost n = 27 (the r^28 term)
-    dd pc = {1.0, 0.0};
-    for (int n = 27; n >= 1; n -= 2) pc = add(dd{1.0, 0.0}, neg(div_d(mul(r2, pc), (double)(n * (n + 1)))));
-    c = pc;
+    const int j = (int)rint(r.hi * 32.0);
+    const int aj = j < 0 ? -j : j;
+    const dd t = add(r, dd{-(double)j * 0.03125, 0.0});  // j/32 is exact
+    dd st, ct;
+    sincos_small(t, st, ct);
+    dd sj = pair(PGE_CR_TAB::kSinJ[aj]);
+    if (j < 0) sj = neg(sj);
+    const dd cj = pair(PGE_CR_TAB::kCosJ[aj]);
+    s = add(mul(sj, ct), mul(cj, st));
+    c = add(mul(cj, ct), neg(mul(sj, st)));
 }
 
 // x = k pi/2 + r; returns k mod 4.  |x| up to a few thousand keeps k pi/2 exact enough
 PGE_HD int reduce(double x, dd &r)
 {
-    const double k = rint(x * kTwoOverPi);
-    dd t = add(dd{x, 0.0}, neg(two_prod(k, kPio2_1)));  // x - k P1 exactly, then the smaller parts
-    t = add(t, neg(two_prod(k, kPio2_2)));
-    t = add(t, dd{-k * kPio2_3, 0.0});
+    const double k = rint(x * 0.6366197723675814);  // x * 2/pi, any rounding of it will do
+    dd t = add(dd{x, 0.0}, neg(two_prod(k, PGE_CR_TAB::kPio2[0])));  // x - k P1 exactly, then the smaller parts
+    t = add(t, neg(two_prod(k, PGE_CR_TAB::kPio2[1])));
+    t = add(t, dd{-k * PGE_CR_TAB::kPio2[2], 0.0});
     r = t;
     const long long ki = (long long)k;
     return (int)(((ki % 4) + 4) % 4);
@@ -170,33 +209,20 @@ PGE_HD double cr_tan(double x)
     return v.hi + v.lo;
 }
 
-// atan(k/8), k = 0..8, each as hi + lo
-PGE_HD dd atan_k8(int k)
-{
-    switch (k) {
-    case 1: return {0.12435499454676144, -3.1253241424539383e-18};
-    case 2: return {0.24497866312686414, 1.0698755618734451e-17};
-    case 3: return {0.35877067027057225, -2.4623815582638635e-17};
-    case 4: return {0.4636476090008061, 2.2698777452961687e-17};
-    case 5: return {0.5585993153435624, -5.4556305485916264e-18};
-    case 6: return {0.6435011087932844, 1.5834785051444286e-17};
-    case 7: return {0.7188299996216245, -2.1478388444456983e-17};
-    case 8: return {0.7853981633974483, 3.061616997868383e-17};
-    default: return {0.0, 0.0};
-    }
-}
-
-// atan(t) for t in [0, 1] (double-double)
+// atan(t) for t in [0, 1] (double-double): t = k/64 + ..., atan(t) = atan(k/64) + atan(z),
+// z = (t - k/64) / (1 + t k/64), |z| <= 1/128; atan(z)'s terms to z^7 in double-double, from z^9 on in double
 PGE_HD dd atan01(dd t)
 {
-    const int k = (int)rint(t.hi * 8.0);
-    const double c = (double)k * 0.125;
-    const dd z = div(add(t, dd{-c, 0.0}), add(dd{1.0, 0.0}, mul_d(t, c)));  // (t - c) / (1 + t c)
+    const int k = (int)rint(t.hi * 64.0);
+    const double c = (double)k * 0.015625;
+    const dd z = div(add(t, dd{-c, 0.0}), add(dd{1.0, 0.0}, mul_d(t, c)));
     const dd z2 = mul(z, z);
-    // atan(z) = z (1 - z^2/3 + z^4/5 - ...), terms to z^27
-    dd p = div_d(dd{1.0, 0.0}, 27.0);
-    for (int n = 25; n >= 1; n -= 2) p = add(div_d(dd{1.0, 0.0}, (double)n), neg(mul(z2, p)));
-    return add(atan_k8(k), mul(z, p));
+    const double x = z2.hi;
+    const double pa = 1.0 / 9.0 + x * (-1.0 / 11.0 + x * (1.0 / 13.0 + x * (-1.0 / 15.0)));
+    const dd a7 = add(neg(pair(PGE_CR_TAB::kInv7)), mul_d(z2, pa));  // -1/7 + z^2 (...)
+    const dd a5 = add(pair(PGE_CR_TAB::kInv5), mul(z2, a7));
+    const dd a3 = add(neg(pair(PGE_CR_TAB::kInv3)), mul(z2, a5));
+    return add(pair(PGE_CR_TAB::kAtanK[k]), add(z, mul(mul(z, z2), a3)));
 }
 
 PGE_HD double cr_atan(double x)
@@ -208,10 +234,10 @@ PGE_HD double cr_atan(double x)
     if (ax <= 1.0) {
         v = atan01(dd{ax, 0.0});
     } else if (ax == INFINITY) {
-        v = dd{kPio2_1, kPio2_2};
+        v = dd{PGE_CR_TAB::kPio2[0], PGE_CR_TAB::kPio2[1]};
     } else {  // pi/2 - atan(1/ax)
         const dd inv = div(dd{1.0, 0.0}, dd{ax, 0.0});
-        v = add(add(dd{kPio2_1, kPio2_2}, dd{kPio2_3, 0.0}), neg(atan01(inv)));
+        v = add(add(dd{PGE_CR_TAB::kPio2[0], PGE_CR_TAB::kPio2[1]}, dd{PGE_CR_TAB::kPio2[2], 0.0}), neg(atan01(inv)));
     }
     const double y = v.hi + v.lo;
     return neg_x ? -y : y;

@@ -9,7 +9,9 @@ cudaError_t launch_droplets_f64(const DropArgs &a, int blocks, int threads, cuda
 {
     if (a.p.lateral_rate > 0.0) return launch_droplets_f64_lateral(a, blocks, threads, st);
     if (a.R) return launch_droplets_f64_route(a, blocks, threads, st);
-    if (!a.ledger)
+    if (!a.ledger && a.minb >= 2)  // record only, at most 128 registers: a wave's droplets one per warp
+        f64::droplet_kernel<2, false><<<blocks, threads, 0, st>>>(a);
+    else if (!a.ledger)
         f64::droplet_kernel<1, false><<<blocks, threads, 0, st>>>(a);
     else if (a.minb >= 2)
         f64::droplet_kernel<2, true><<<blocks, threads, 0, st>>>(a);
@@ -71,7 +73,8 @@ int droplet_blocks_per_sm_f64_tape(int threads)
 int droplet_blocks_per_sm_f64(int threads, int minb, bool ledger)
 {
     int n = 0;
-    cudaError_t e = !ledger     ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, false>, threads, 0)
+    cudaError_t e = !ledger     ? (minb >= 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<2, false>, threads, 0)
+                                             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, false>, threads, 0))
                     : minb >= 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<2, true>, threads, 0)
                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f64::droplet_kernel<1, true>, threads, 0);
     if (e != cudaSuccess) return 1;

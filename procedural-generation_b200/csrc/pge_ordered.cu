@@ -518,267 +518,6 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
 }
 
 // ---------------------------------------------------------------------------
-// The fed apply: one droplet per block of two warps.  Warp 1, the feeder, streams the droplet's
-// entries into a ring in shared memory -- the descriptor, the cell's pass-start terrain, its hand-off
-// word (and the erode cap / routing surface) -- FED_CHUNK entries at a time (a lane each), and keeps
-// re-polling the hand-off words of upcoming first visits whose cell the earlier droplets have not yet
-// handed on.  Lane 0 of warp 0, the applier, walks the list reading only shared memory: its serial
-// chain is the arithmetic of the entries, not the latency of their loads.  The feeder overwrites an
-// entry's slot only once the applier is more than FED_LOOKBACK entries past it, so the applier finds
-// its own recent writes to a cell it revisits (the final deposits over the last path cells) in the ring.
-// ---------------------------------------------------------------------------
-namespace {
-constexpr int FED_THREADS = 64;
-constexpr int FED_RING = 128;
-constexpr int FED_CHUNK = 32;
-constexpr int FED_LOOKBACK = 32;
-constexpr long long kFedSpin = 1LL << 26;  // polls of one wait (~ a second or more): far beyond any hand-off
-
-struct alignas(16) FedSlot {
-    EntryDesc d;                         // descriptor
-    volatile unsigned long long h0, h1;  // the cell's hand-off word, refreshed by the feeder until it is ready
-    CellTerr t;                          // the cell's pass-start terrain
-    double cap;                          // the slope erode cap (when on)
-    float2 route;                        // the packed routing surface and flag (with lakes)
-};
-static_assert(sizeof(FedSlot) == 64, "fed slot layout");
-
-// the droplet's own latest value at cell c among its entries k - FED_LOOKBACK .. k - 1
-__device__ __forceinline__ bool own_lookback(const FedSlot *ring, const double *ownv, int k, int32_t c, double &acc)
-{
-    const int lim = k < FED_LOOKBACK ? k : FED_LOOKBACK;
-    for (int i = 1; i <= lim; i++) {
-        const int sl = (k - i) & (FED_RING - 1);
-        if (ring[sl].d.cell == c) {
-            acc = ownv[sl];
-            return true;
-        }
-    }
-    return false;
-}
-
-// the net change of cell c for entry k (its slot sl): the droplet's own earlier write (a revisit), or
-// once the D earlier droplets have handed the cell on, the hand-off word the feeder keeps fresh
-__device__ __forceinline__ bool fed_value(const OrderedArgs &a, const FedSlot *ring, const double *ownv, int k, int sl, int32_t c,
-                                          uint32_t df, const volatile int *quit, double &acc)
-{
-    if (!(df & ENTRY_FIRST)) {
-        if (own_lookback(ring, ownv, k, c, acc)) return true;
-        acc = own_value(a.hand, c);
-        return true;
-    }
-    const uint32_t D = df & ENTRY_D_MASK;
-    const uint32_t want = a.epoch + D;
-    const FedSlot &s = ring[sl];
-    for (long long i = 0; i < kFedSpin; i++) {
-        const unsigned long long w0 = s.h0, w1 = s.h1;
-        if (D == 0 || hand_ready(w0, w1, want)) {
-            acc = hand_acc(w0, w1);
-            return true;
-        }
-        if ((i & 1023) == 1023 && (*quit || *(volatile int *)a.error)) return false;
-    }
-    atomicExch(a.error, 1);
-    return false;
-}
-
-template <bool ECAP, bool LAKE>
-__device__ __forceinline__ void feed_entry(const OrderedArgs &a, FedSlot &s, long long e)
-{
-    // both arrays are read-only while the apply runs: 16-byte read-only loads
-    const int4 dv = __ldg(reinterpret_cast<const int4 *>(a.desc + e));
-    EntryDesc d;
-    memcpy(&d, &dv, sizeof(d));
-    s.d = d;
-    const long long c = d.cell;
-    const int4 tv = __ldg(reinterpret_cast<const int4 *>(a.terr + c));
-    CellTerr t;
-    memcpy(&t, &tv, sizeof(t));
-    s.t = t;
-    unsigned long long w0, w1;
-    hand_load(a.hand + c, w0, w1);
-    s.h0 = w0;
-    s.h1 = w1;
-    if (ECAP) s.cap = __ldg(a.ecap + c);
-    if (LAKE) s.route = __ldg(a.R + c);
-}
-
-// warp 1: keep the ring filled ahead of the applier and the pending hand-off words fresh
-template <bool ECAP, bool LAKE>
-__device__ void feeder(const OrderedArgs &a, FedSlot *ring, long long b0, int K, volatile int *loaded_s, volatile int *done_s,
-                       volatile int *quit)
-{
-    const int lane = threadIdx.x & 31;
-    int loaded = 0, last_done = -1;
-    long long idle = 0;
-    while (true) {
-        // every decision of the loop is the warp's: lane 0 reads the shared counters for all
-        int done = 0, stop = 0;
-        if (lane == 0) {
-            done = *done_s;
-            stop = *quit;
-        }
-        done = __shfl_sync(0xffffffffu, done, 0);
-        stop = __shfl_sync(0xffffffffu, stop, 0);
-        if (done >= K || stop) return;
-        if (done != last_done) {
-            last_done = done;
-            idle = 0;
-        } else if (++idle > kFedSpin) {  // the applier made no progress for seconds
-            if (lane == 0) {
-                atomicExch(a.error, 1);
-                *quit = 1;
-            }
-            return;
-        }
-        // a chunk [loaded, loaded + 32) overwrites entries loaded - FED_RING ..; they must be older than
-        // done - FED_LOOKBACK (done never runs ahead of the applier)
-        if (loaded < K && loaded <= done - FED_LOOKBACK + FED_RING - FED_CHUNK) {
-            const int j = loaded + lane;
-            if (j < K) feed_entry<ECAP, LAKE>(a, ring[j & (FED_RING - 1)], b0 + j);
-            loaded = loaded + FED_CHUNK < K ? loaded + FED_CHUNK : K;
-            __syncwarp();
-            if (lane == 0) {
-                __threadfence_block();
-                *loaded_s = loaded;
-            }
-            continue;
-        }
-        bool polled = false;
-        for (int j = done + lane; j < loaded; j += 32) {
-            FedSlot &s = ring[j & (FED_RING - 1)];
-            const uint32_t df = s.d.dflags;
-            const uint32_t D = df & ENTRY_D_MASK;
-            if (!(df & ENTRY_FIRST) || D == 0) continue;
-            const uint32_t want = a.epoch + D;
-            if (hand_ready(s.h0, s.h1, want)) continue;
-            unsigned long long w0, w1;
-            hand_load(a.hand + s.d.cell, w0, w1);
-            polled = true;
-            if (hand_ready(w0, w1, want)) {
-                s.h0 = w0;
-                s.h1 = w1;
-            }
-        }
-        if (!__any_sync(0xffffffffu, polled)) __nanosleep(64);
-    }
-}
-}  // namespace
-
-template <bool ECAP, bool LAKE>
-__global__ void __launch_bounds__(FED_THREADS) ordered_apply_fed_kernel(const OrderedArgs a)
-{
-    __shared__ FedSlot ring[FED_RING];
-    __shared__ double ownv[FED_RING];
-    __shared__ unsigned long long sstat[OS_N];
-    __shared__ int s_loaded, s_done, s_quit;
-    for (int k = threadIdx.x; k < OS_N; k += blockDim.x) sstat[k] = 0ull;
-    if (threadIdx.x == 0) s_quit = 0;
-    __syncthreads();
-    volatile int *loaded_s = &s_loaded, *done_s = &s_done, *quit = &s_quit;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (long long q = blockIdx.x; q < a.nw; q += gridDim.x) {
-        const int K = (int)a.count[q];
-        if (K <= 0) {
-            if (threadIdx.x == 0) a.dth[q] = -1;
-            continue;
-        }
-        const long long b0 = q * a.cap;
-        if (threadIdx.x == 0) {
-            s_loaded = 0;
-            s_done = 0;
-        }
-        __syncthreads();
-        if (warp == 1) {
-            feeder<ECAP, LAKE>(a, ring, b0, K, loaded_s, done_s, quit);
-        } else if (lane == 0) {
-            Walk w;
-            w.deficit = w.surplus = w.prev_live = w.acc_c = 0.0;
-            w.clamped = 0;
-            w.death = -1;
-            w.sub_death = w.has_prev = w.have_c = false;
-            w.ok = true;
-            int seen = 0;
-            for (int k = 0; k < K; k++) {
-                // entries k and k + 1 in the ring
-                const int need = k + 1 < K ? k + 2 : k + 1;
-                if (seen < need) {
-                    for (long long i = 0; seen < need; i++) {
-                        seen = *loaded_s;
-                        if (seen >= need) break;
-                        if (*quit) {
-                            w.ok = false;
-                            break;
-                        }
-                        if (i > kFedSpin) {
-                            atomicExch(a.error, 1);
-                            w.ok = false;
-                            break;
-                        }
-                    }
-                    if (!w.ok) break;
-                    __threadfence_block();  // the slots the feeder published before its count
-                }
-                const int sl = k & (FED_RING - 1), nsl = (k + 1) & (FED_RING - 1);
-                const FedSlot &cur = ring[sl];
-                const FedSlot &nx = ring[nsl];
-                const bool has_next = k + 1 < K;
-                const int32_t c = cur.d.cell;
-                const uint32_t df = cur.d.dflags;
-                const double dlt = cur.d.delta;
-                const double hs = cur.t.hs;
-                const double b_c = (double)cur.t.base;
-                const bool act = cur.t.active != 0;
-                if (!w.have_c && !(w.ok = fed_value(a, ring, ownv, k, sl, c, df, quit, w.acc_c))) break;
-                // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
-                // acquire it now; a step deposit does not, and acquires it only before writing it
-                const bool is_step = (df & ENTRY_STEP) != 0;
-                const bool reads_next = has_next && (dlt < 0.0 || !is_step);
-                const int32_t ncell = has_next ? nx.d.cell : -1;
-                double acc_n = 0.0, hs_n = 0.0;
-                if (reads_next) {
-                    hs_n = nx.t.hs;
-                    if (ncell == c)
-                        acc_n = w.acc_c;
-                    else if (!(w.ok = fed_value(a, ring, ownv, k, nsl, ncell, nx.d.dflags, quit, acc_n)))
-                        break;
-                }
-                const double acc = w.acc_c;
-                double acc_new = acc, amount = 0.0;
-                entry_arith<ECAP, LAKE>(a.p, w, c, dlt, is_step, act, hs, b_c, acc, has_next, hs_n + acc_n, cur.cap, cur.route,
-                                        acc_new, amount);
-                // publish the net change; a droplet's last write at a cell also hands the cell on
-                const bool lastv = (df & ENTRY_LAST) != 0;
-                if (act || lastv) hand_store(a.hand + c, acc_new, a.epoch + (df & ENTRY_D_MASK) + (lastv ? 1u : 0u));
-                a.act[b0 + k] = amount;
-                ownv[sl] = acc_new;
-                // the next entry's cell: acquired (with its net change) if this entry read it; the same
-                // cell again keeps its acquisition and its updated net change
-                if (has_next && ncell == c) {
-                    w.have_c = true;
-                    w.acc_c = acc_new;
-                } else {
-                    w.have_c = reads_next;
-                    w.acc_c = acc_n;
-                }
-                *done_s = k + 1;
-            }
-            if (w.ok) {
-                droplet_end(a, w, q, sstat);
-            } else {
-                *quit = 1;
-            }
-            *done_s = K;  // releases the feeder
-        }
-        __syncwarp();  // warp 0's idle lanes wait for lane 0 here, so the warp meets the barrier converged
-        __syncthreads();
-        if (s_quit) break;
-    }
-    __syncthreads();
-    flush_stats(a, sstat);
-}
-
-// ---------------------------------------------------------------------------
 // after the apply: per touched cell, in the serial (droplet, entry) order, the discharge and
 // momentum tracks (particle.py:1013-1018) and the stockpile (:1019-1041); then the cell's net
 // change to the accumulators and its packed samples (:1005-1009); and the wave's eroded and
@@ -896,11 +635,6 @@ cudaError_t ordered_terrain(long long ncell, const double2 *L, const float4 *B, 
 int ordered_blocks_per_sm(int lanes)
 {
     int n = 0;
-    if (lanes <= 0) {  // the fed apply: one droplet per block, static shared memory
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_fed_kernel<true, true>, FED_THREADS, 0) != cudaSuccess)
-            return 1;
-        return n > 0 ? n : 1;
-    }
     const size_t smem = (size_t)(APPLY_THREADS / 32) * lanes * RING * sizeof(Slot);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ordered_apply_kernel<false, false>, APPLY_THREADS, smem) != cudaSuccess) return 1;
     return n > 0 ? n : 1;
@@ -922,22 +656,6 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
                                                           w.a.delta, w.a.vol, const_cast<EntryDesc *>(w.a.desc));
     const bool lake = w.a.lakes && w.a.R;
-    if (w.a.lanes <= 0) {
-        // the fed apply: a block per droplet while they last (every block resident: a droplet waits only
-        // on earlier droplets, which blocks already running hold)
-        long long blocks = w.nw < w.max_blocks ? w.nw : w.max_blocks;
-        if (blocks < 1) blocks = 1;
-        if (w.a.ecap && lake)
-            ordered_apply_fed_kernel<true, true><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
-        else if (w.a.ecap)
-            ordered_apply_fed_kernel<true, false><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
-        else if (lake)
-            ordered_apply_fed_kernel<false, true><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
-        else
-            ordered_apply_fed_kernel<false, false><<<(int)blocks, FED_THREADS, 0, st>>>(w.a);
-        ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
-        return cudaPeekAtLastError();
-    }
     const long long warps = (w.nw + w.a.lanes - 1) / w.a.lanes;  // a lane per droplet
     long long blocks = (warps * 32 + APPLY_THREADS - 1) / APPLY_THREADS;
     if (blocks > w.max_blocks) blocks = w.max_blocks;

@@ -313,3 +313,33 @@ def erodibility_init(state: ErosionState, seed: int = 0, spread: float = 0.2) ->
 def rates_of(params) -> torch.Tensor:
     ep = erosion_group(params)
     return torch.tensor([float(getattr(ep, k)) for k in RATES], dtype=torch.float64)
+
+
+def calibrate(calib: Calibration, target: torch.Tensor, land: torch.Tensor, erod0: torch.Tensor, rates0: torch.Tensor,
+              steps: int = 10, lr_rates: float = 0.05, lr_field: float = 0.02, field: bool = True) -> dict:
+    """Gradient-based calibration in place of the grid sweep of the rates
+    (docs/erosion-tuning.md's procedure): Adam on the log of the four rates
+    and (``field``) on the per-cell erodibility field, each step one forward
+    run of ``calib`` and its adjoint.  Returns the loss before every step and
+    after the last, and the rates and field after each step."""
+    dev = calib.state.height.device
+    logr = torch.log(rates0.detach().to(dev, torch.float64)).clone().requires_grad_(True)
+    erod = erod0.detach().clone().requires_grad_(field)
+    groups = [{"params": [logr], "lr": lr_rates}]
+    if field:
+        groups.append({"params": [erod], "lr": lr_field})
+    opt = torch.optim.Adam(groups)
+    losses, rates_hist = [], []
+    for _ in range(int(steps)):
+        opt.zero_grad()
+        loss = land_loss(erode(erod, torch.exp(logr), calib), target, land, calib.state.height_unit_m)
+        loss.backward()
+        losses.append(float(loss.detach()))
+        opt.step()
+        with torch.no_grad():
+            erod.clamp_(0.05, 5.0)
+        rates_hist.append(torch.exp(logr).detach().cpu().tolist())
+    with torch.no_grad():
+        final = land_loss(erode(erod, torch.exp(logr), calib), target, land, calib.state.height_unit_m)
+    losses.append(float(final))
+    return {"loss": losses, "rates": rates_hist, "field": erod.detach()}

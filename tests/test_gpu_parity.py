@@ -425,28 +425,3 @@ def test_spawn_feeder_gives_the_reference_draws(cuda):
     finally:
         feeder.close()
 
-
-@pytest.mark.parametrize("world", ["tiny", "small"])
-def test_fed_apply_equals_unfed_apply(cuda, world):
-    """The ordered apply's two kernels -- the fed one (a feeder warp streams each droplet's entries
-    and the hand-offs it waits for into shared memory; apply_lanes = 0, the default) and the unfed
-    one (each droplet's lane loads its own entries; apply_lanes = 1) -- do the same float64
-    operations in the same serial order, so a pass from the same state is bit for bit the same."""
-    from pgerosion import synth
-
-    if world == "tiny":
-        c = step_case()
-        w, params, P = c["world"], c["params"], c["n_particles"]
-    else:
-        w = synth.plain_small_world(0)
-        params, P = synth.config_params("small")
-    out = []
-    for lanes in (0, 1):
-        g = gm.ErosionState.from_world(w)
-        for it in range(2):
-            s = gm.run_iteration(g, params, it, n_particles=P, apply_lanes=lanes)
-        out.append((g.to_numpy(), s))
-    (a, sa), (b, sb) = out
-    for k in ("height", "sediment", "discharge", "momentum", "pending"):
-        assert a[k].tobytes() == b[k].tobytes(), k
-    assert sa["clamped"] == sb["clamped"] and sa["entries"] == sb["entries"]
