@@ -397,7 +397,7 @@ def run_b200(args, rank, world_size, dist):
     e2e_ms = ee[0].elapsed_time(ee[1])
     feeder.close()
     (steps_all, e2e_all), (ms_max, e2e_ms_max) = reduce_totals(dist, [steps_done, e2e_steps], [ms, e2e_ms], device=dev)
-    alt = brush = None
+    alt = brush = f32 = None
     it_next = n_total + args.steps
     if apply == _lib.APPLY_ORDERED and not args.no_alt:
         # the order-free wave apply on the same world (one wave per iteration): faster, not the
@@ -413,6 +413,12 @@ def run_b200(args, rank, world_size, dist):
             brush, it_next = _side_leg(st, pb, P, kw_alt, it_next, args.alt_steps, dev, dist, BRUSH_BYTES_PER_STEP)
             brush["apply"] = f"wave apply with the erode / deposit brush, radius {BRUSH_RADIUS} ({BRUSH_CELLS} cells)"
             brush["bytes_per_step"] = BRUSH_BYTES_PER_STEP
+        if not args.no_f32 and prec == _lib.PREC_F64:
+            # the exact pass with the trace in float32 (the ledger and the apply stay float64): what float64
+            # arithmetic costs the trace; its paths are not the reference's (tests: >= 90 % identical)
+            kw32 = dict(kw, precision=_lib.PREC_F32)
+            f32, it_next = _side_leg(st, params, P, kw32, it_next, min(args.alt_steps, 3), dev, dist, BYTES_PER_STEP)
+            f32["trace"] = "float32 trace, float64 ordered apply (reference chunk waves)"
     batched = None
     if not args.no_batch:
         batched = run_batched(args, rank, world_size, dist, dev)
@@ -476,6 +482,8 @@ def run_b200(args, rank, world_size, dist):
         out["alt_wave_apply"] = alt
     if brush is not None:
         out["brush"] = brush
+    if f32 is not None:
+        out["f32_trace"] = f32
     if batched is not None:
         out["batched_worlds"] = batched
     if adjoint is not None:
@@ -603,6 +611,7 @@ def main():
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)
     ap.add_argument("--no-brush", action="store_true", help="skip the brush (radius 3) measurement")
+    ap.add_argument("--no-f32", action="store_true", help="skip the float32-trace measurement")
     ap.add_argument("--apply-lanes", type=int, default=0, help="ordered apply: droplets per warp (0 = 1)")
     ap.add_argument("--config", default="c2", choices=("c2", "c5"),
                     help="c2: the Earth-default N_c=1024 line (default); c5: the N_c=8192 planet level on one GPU")
