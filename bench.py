@@ -96,6 +96,8 @@ def run_batched(args, rank, world_size, dist, dev):
     res = runner.step(k, n_particles=counts, spawns=lambda i, it: pre[(i, it)]) if runner else []
     ev[3].record()
     torch.cuda.synchronize()
+    if runner:
+        runner.close()
     together = sum(s["droplet_steps"] for r in res for s in r)
     (one_all, tog_all), (ms_one, ms_tog, worst) = batch.reduce_totals(
         dist, [one, together], [ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), worst], device=dev)

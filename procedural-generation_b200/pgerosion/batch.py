@@ -140,6 +140,13 @@ class Runner:
         self.step_kw = dict(step_kw)
         if len(self.states) > 1:
             self.step_kw.setdefault("trace_lanes", int(trace_lanes))
+        # one long-lived pool: a world's host passes (the lake balance keeps its scratch per thread) run on
+        # threads that stay, so later refreshes reuse their pages
+        self._pool = ThreadPoolExecutor(max_workers=len(self.streams))
+
+    def close(self) -> None:
+        """Stop the runner's host threads (their per-thread scratch goes with them)."""
+        self._pool.shutdown(wait=True)
 
     def _run(self, i: int, iterations: int, first: int | None, kw: dict, spawns) -> list[dict]:
         import torch
@@ -175,9 +182,8 @@ class Runner:
             kws.append(kw)
         # the costliest worlds first, so their threads start their passes first
         order = sorted(range(len(self.states)), key=lambda i: -self.states[i].N)
-        with ThreadPoolExecutor(max_workers=len(self.streams)) as ex:
-            futs = {i: ex.submit(self._run, i, iterations, first, kws[i], spawns) for i in order}
-            res = [futs[i].result() for i in range(len(self.states))]
+        futs = {i: self._pool.submit(self._run, i, iterations, first, kws[i], spawns) for i in order}
+        res = [futs[i].result() for i in range(len(self.states))]
         torch.cuda.synchronize()
         return res
 
