@@ -25,7 +25,6 @@
 // direction are constants; its own move is still differentiated).
 #include <cmath>
 
-#include "pge_crmath.cuh"
 #include "pge_internal.cuh"
 #include "pge_maps.cuh"
 
@@ -105,7 +104,7 @@ __device__ __forceinline__ D4 dsqrt(const D4 &a)
 __device__ __forceinline__ D4 dtan(const D4 &a)
 {
     D4 r;
-    r.v = cr::d_tan(a.v);  // the forward trace's rounding (pge_crmath.cuh)
+    r.v = tan(a.v);  // as the taped wave-apply pass crosses faces (CUDA's own)
     const double g = 1.0 + r.v * r.v;
 #pragma unroll
     for (int k = 0; k < 4; k++) r.d[k] = a.d[k] * g;
@@ -114,7 +113,7 @@ __device__ __forceinline__ D4 dtan(const D4 &a)
 __device__ __forceinline__ D4 datan(const D4 &a)
 {
     D4 r;
-    r.v = cr::d_atan(a.v);
+    r.v = atan(a.v);
     const double g = 1.0 / (1.0 + a.v * a.v);
 #pragma unroll
     for (int k = 0; k < 4; k++) r.d[k] = a.d[k] * g;

@@ -277,6 +277,9 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.minb = minb;
         a.lanes = 32;
         a.brush_r = p->brush_radius;
+        // the exact pass and the change-list hook follow the reference's arithmetic; the order-free wave apply
+        // (and its tape, which the adjoint reverses with the same functions) takes CUDA's own trig
+        a.cr_trig = (p->apply == PGE_APPLY_ORDERED || rec_cell != nullptr) ? 1 : 0;
         unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
         const long long wave = p->wave;
         const long long nw = (P + wave - 1) / wave;

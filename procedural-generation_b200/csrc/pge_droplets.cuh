@@ -58,18 +58,20 @@ constexpr double kPi = 3.14159265358979323846;
 __device__ __forceinline__ R half_pi() { return R(kPi / 2.0); }
 __device__ __forceinline__ R two_over_pi() { return R(2.0 / kPi); }
 
-// tan / atan / sin / cos of the droplet precision: float64 rounds like the C library the reference
-// calls (correctly rounded double-double evaluations, pge_crmath.cuh); float32 takes the builtins.
-// The float64 ones are inlined into the out-of-line face crossing and spawn direction below, so the
-// droplet kernel itself holds one call site for each.
-__device__ __forceinline__ double m_tan(double x) { return cr::cr_tan(x); }
-__device__ __forceinline__ double m_atan(double x) { return cr::cr_atan(x); }
-__device__ __forceinline__ double m_sin(double x) { return cr::cr_sin(x); }
-__device__ __forceinline__ double m_cos(double x) { return cr::cr_cos(x); }
-__device__ __forceinline__ float m_tan(float x) { return tanf(x); }
-__device__ __forceinline__ float m_atan(float x) { return atanf(x); }
-__device__ __forceinline__ float m_sin(float x) { return sinf(x); }
-__device__ __forceinline__ float m_cos(float x) { return cosf(x); }
+// tan / atan / sin / cos of the droplet precision.  CR (float64 only): correctly rounded double-double
+// evaluations (pge_crmath.cuh), which give the C library's results the reference computes with
+// wherever those are correctly rounded -- the exact (ordered) pass and the change-list hook use them;
+// otherwise CUDA's own functions, for the order-free wave apply, whose results are not the
+// reference's anyway.  They run inside the out-of-line face crossing and spawn direction below, so
+// the droplet kernel itself holds one call site for each.
+template <bool CR> __device__ __forceinline__ double m_tan(double x) { return CR ? cr::cr_tan(x) : tan(x); }
+template <bool CR> __device__ __forceinline__ double m_atan(double x) { return CR ? cr::cr_atan(x) : atan(x); }
+template <bool CR> __device__ __forceinline__ double m_sin(double x) { return CR ? cr::cr_sin(x) : sin(x); }
+template <bool CR> __device__ __forceinline__ double m_cos(double x) { return CR ? cr::cr_cos(x) : cos(x); }
+template <bool CR> __device__ __forceinline__ float m_tan(float x) { return tanf(x); }
+template <bool CR> __device__ __forceinline__ float m_atan(float x) { return atanf(x); }
+template <bool CR> __device__ __forceinline__ float m_sin(float x) { return sinf(x); }
+template <bool CR> __device__ __forceinline__ float m_cos(float x) { return cosf(x); }
 
 // ---------------------------------------------------------------------------
 // cube-sphere mapping in droplet precision (cubesphere.py:70-220)
@@ -84,12 +86,13 @@ __device__ __forceinline__ void face_axes(int f, R r[3], R u[3], R n[3])
     }
 }
 
+template <bool CR = true>
 __device__ void to_sphere(int face, R u, R v, R &x, R &y, R &z)
 {
     R r[3], up[3], n[3];
     face_axes(face, r, up, n);
-    R s = m_tan((u - R(0.5)) * half_pi());
-    R t = m_tan((v - R(0.5)) * half_pi());
+    R s = m_tan<CR>((u - R(0.5)) * half_pi());
+    R t = m_tan<CR>((v - R(0.5)) * half_pi());
     R qx = n[0] + s * r[0] + t * up[0];
     R qy = n[1] + s * r[1] + t * up[1];
     R qz = n[2] + s * r[2] + t * up[2];
@@ -99,6 +102,7 @@ __device__ void to_sphere(int face, R u, R v, R &x, R &y, R &z)
     z = qz * inv;
 }
 
+template <bool CR = true>
 __device__ int from_sphere(R x, R y, R z, R &u, R &v)
 {
     R ax = fabs(x), ay = fabs(y), az = fabs(z);
@@ -111,16 +115,17 @@ __device__ int from_sphere(R x, R y, R z, R &u, R &v)
     R d = x * n[0] + y * n[1] + z * n[2];
     R s = (x * r[0] + y * r[1] + z * r[2]) / d;
     R t = (x * up[0] + y * up[1] + z * up[2]) / d;
-    u = m_atan(s) * two_over_pi() + R(0.5);
-    v = m_atan(t) * two_over_pi() + R(0.5);
+    u = m_atan<CR>(s) * two_over_pi() + R(0.5);
+    v = m_atan<CR>(t) * two_over_pi() + R(0.5);
     return face;
 }
 
+template <bool CR = true>
 __device__ void jacobian(int face, R u, R v, R J[6])
 {
     R r[3], up[3], n[3];
     face_axes(face, r, up, n);
-    R s = m_tan((u - R(0.5)) * half_pi()), t = m_tan((v - R(0.5)) * half_pi());
+    R s = m_tan<CR>((u - R(0.5)) * half_pi()), t = m_tan<CR>((v - R(0.5)) * half_pi());
     R dsdu = half_pi() * (R(1) + s * s);
     R dtdv = half_pi() * (R(1) + t * t);
     R qx = n[0] + s * r[0] + t * up[0];
@@ -141,12 +146,13 @@ __device__ void jacobian(int face, R u, R v, R J[6])
 }
 
 // particle face transition; returns the new face, (u, v, a, b) updated in place
+template <bool CR = true>
 __device__ int transfer_velocity(int face, R &u, R &v, R &a, R &b)
 {
     if (u >= R(0) && u < R(1) && v >= R(0) && v < R(1)) return face;
     R x, y, z, u2, v2;
-    to_sphere(face, u, v, x, y, z);
-    int f2 = from_sphere(x, y, z, u2, v2);
+    to_sphere<CR>(face, u, v, x, y, z);
+    int f2 = from_sphere<CR>(x, y, z, u2, v2);
     if (f2 == face) {
         R m = u2 < R(0) ? R(0) : u2;
         u = R(0.999999999) < m ? R(0.999999999) : m;
@@ -155,11 +161,11 @@ __device__ int transfer_velocity(int face, R &u, R &v, R &a, R &b)
         return face;
     }
     R J[6], K[6];
-    jacobian(face, u, v, J);
+    jacobian<CR>(face, u, v, J);
     R wx = a * J[0] + b * J[3];
     R wy = a * J[1] + b * J[4];
     R wz = a * J[2] + b * J[5];
-    jacobian(f2, u2, v2, K);
+    jacobian<CR>(f2, u2, v2, K);
     R guu = K[0] * K[0] + K[1] * K[1] + K[2] * K[2];
     R guv = K[0] * K[3] + K[1] * K[4] + K[2] * K[5];
     R gvv = K[3] * K[3] + K[4] * K[4] + K[5] * K[5];
@@ -179,15 +185,16 @@ struct Crossed {
     R u, v, a, b;
     int face;
 };
+template <bool CR>
 __device__ __noinline__ Crossed cross_out_of_line(int face, R u, R v, R a, R b)
 {
     Crossed c{u, v, a, b, face};
-    c.face = transfer_velocity(face, c.u, c.v, c.a, c.b);
+    c.face = transfer_velocity<CR>(face, c.u, c.v, c.a, c.b);
     return c;
 }
-__device__ __forceinline__ int cross_face(int face, R &u, R &v, R &a, R &b)
+__device__ __forceinline__ int cross_face(bool cr, int face, R &u, R &v, R &a, R &b)
 {
-    const Crossed c = cross_out_of_line(face, u, v, a, b);
+    const Crossed c = cr ? cross_out_of_line<true>(face, u, v, a, b) : cross_out_of_line<false>(face, u, v, a, b);
     u = c.u;
     v = c.v;
     a = c.a;
@@ -197,7 +204,8 @@ __device__ __forceinline__ int cross_face(int face, R &u, R &v, R &a, R &b)
 struct Dir {
     R c, s;
 };
-__device__ __noinline__ Dir spawn_dir(R dir) { return Dir{m_cos(dir), m_sin(dir)}; }
+template <bool CR>
+__device__ __noinline__ Dir spawn_dir(R dir) { return Dir{m_cos<CR>(dir), m_sin<CR>(dir)}; }
 
 // ---------------------------------------------------------------------------
 // what a step reads about the cell a droplet stands in
@@ -736,7 +744,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     sb = R(0);
                     if (sed > R(0)) {
                         const R dir = R(a.sp_dir[d]);
-                        const Dir dd = spawn_dir(dir);
+                        const Dir dd = a.cr_trig ? spawn_dir<true>(dir) : spawn_dir<false>(dir);
                         sa = dd.c;
                         sb = dd.s;
                     }
@@ -870,7 +878,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             if (a.spherical) {
                 if (nx < R(0) || nx >= Nf || ny < R(0) || ny >= Nf) {
                     R u = nx / Nf, v = ny / Nf;
-                    nf = cross_face(f, u, v, sa, sb);
+                    nf = cross_face(a.cr_trig != 0, f, u, v, sa, sb);
                     nx = u * Nf;
                     ny = v * Nf;
                     if (TAPE) {

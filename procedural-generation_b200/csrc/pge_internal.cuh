@@ -121,6 +121,7 @@ struct DropArgs {
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
     int brush_r;  // the erode / deposit brush's radius (0: one cell)
+    int cr_trig;  // 1: the face crossing's trig correctly rounded (the exact pass, the change-list hook); 0: CUDA's
 };
 
 // launchers of the two precisions (separate translation units: the float64
