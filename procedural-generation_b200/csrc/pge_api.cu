@@ -165,6 +165,7 @@ Layout layout(const PgeGrid &g)
     L.flags = take(8 * L.ncell);
     L.pwv = take(8 * L.ncell);                  // compacted values of a pairwise sum / the spawn weights' integers
     L.pwnode = take(pairwise_scratch_bytes());  // the pairwise sum's tree
+    L.spread = take(8 * L.ncell);               // the brush: each cell's net change as last spread
     // ordered apply
     L.cap = change_list_cap(g.max_steps);
     L.max_wave = g.max_wave;
@@ -205,6 +206,8 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
     cudaError_t e;
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.acc4), 0, 32 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset acc");
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.pend), 0, 8 * lay.ncell, st)) != cudaSuccess) return cuda_fail(e, "memset pending");
+    if (p->brush_radius > 0 && (e = cudaMemsetAsync(ws_ptr<void>(ws, lay.spread), 0, 8 * lay.ncell, st)) != cudaSuccess)
+        return cuda_fail(e, "memset spread");
     if ((e = cudaMemsetAsync(ws_ptr<void>(ws, lay.counters), 0, 16, st)) != cudaSuccess) return cuda_fail(e, "memset counters");
     // own-change tables: generation 0 everywhere (free); waves then use generations (w + 1) << 24 onwards
     const bool ledger_pass = p->apply == PGE_APPLY_WAVE || rec_cell != nullptr;
@@ -276,7 +279,6 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         a.ledger = 1;
         a.minb = minb;
         a.lanes = 32;
-        a.brush_r = p->brush_radius;
         // the exact pass and the change-list hook follow the reference's arithmetic; the order-free wave apply
         // (and its tape, which the adjoint reverses with the same functions) takes CUDA's own trig
         a.cr_trig = (p->apply == PGE_APPLY_ORDERED || rec_cell != nullptr) ? 1 : 0;
@@ -416,6 +418,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                      : p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, threads, st)
                                                     : launch_droplets_f32(a, (int)blocks, threads, st);
             if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
+            if (p->brush_radius > 0) brush_spread(*g, *s, lay, ws, p->brush_radius, st);
             if (w + 1 < nw) refresh(*s, lay, ws, st);
         }
     }

@@ -451,57 +451,6 @@ __device__ __forceinline__ void load_lcell(const DropArgs &a, const Table &t, lo
     lc.own = t.lookup(c, lc.tidx);
 }
 
-// The erode / deposit brush: an applied change fx (fixed point) at cell c spread over the active
-// cells of c's face within r of it (the interior ones on the sphere, whose halos are copies) with
-// the weights brush_weight (r + 1 - distance, integers of 1/PGE_BRUSH_SCALE); the shares are truncated
-// toward zero and the rest stays on c, so the sum is exactly fx whatever the order the atomics land in.
-// Everything by value: the droplet kernel's argument block stays where it is.
-__device__ __forceinline__ int brush_weight(int r, int di, int dj)
-{
-    const double v = (double)(r + 1) - sqrt((double)(di * di + dj * dj));
-    return v > 0.0 ? (int)llround(PGE_BRUSH_SCALE * v) : 0;
-}
-
-__device__ __noinline__ void brush_add(long long *acc4, const uint8_t *mask, int NE, int lo, int hi, int r, long long c, long long fx)
-{
-    const long long plane = (long long)NE * NE;
-    const long long fb = c / plane * plane;
-    const int ei = (int)((c - fb) / NE), ej = (int)((c - fb) % NE);
-    long long Q = 0;
-    for (int di = -r; di <= r; di++) {
-        const int ii = ei + di;
-        if (ii < lo || ii >= hi) continue;
-        for (int dj = -r; dj <= r; dj++) {
-            const int jj = ej + dj;
-            const int q = brush_weight(r, di, dj);
-            if (!q || jj < lo || jj >= hi) continue;
-            const long long cc = fb + (long long)ii * NE + jj;
-            if (cc != c && mask && __ldg(mask + cc) != PGE_MASK_ACTIVE) continue;
-            Q += q;
-        }
-    }
-    long long given = 0;
-    if (Q > 0) {
-        for (int di = -r; di <= r; di++) {
-            const int ii = ei + di;
-            if (ii < lo || ii >= hi) continue;
-            for (int dj = -r; dj <= r; dj++) {
-                const int jj = ej + dj;
-                const int q = brush_weight(r, di, dj);
-                if (!q || jj < lo || jj >= hi || (di == 0 && dj == 0)) continue;
-                const long long cc = fb + (long long)ii * NE + jj;
-                if (mask && __ldg(mask + cc) != PGE_MASK_ACTIVE) continue;
-                const long long share = (long long)(((__int128)fx * q) / Q);
-                if (share) {
-                    red_add(acc4 + 4 * cc, share);
-                    given += share;
-                }
-            }
-        }
-    }
-    red_add(acc4 + 4 * c, fx - given);
-}
-
 // Apply one change-list entry (particle.py:934-1018) at cell `c` against the
 // droplet's view of the terrain.  `nx` is the next entry's cell (has_next).
 // Updates c.own (and the table), emits the atomics and returns the applied
@@ -635,10 +584,7 @@ __device__ __forceinline__ void apply_entry(const DropArgs &a, Table &t, Ledger 
         c.own = c.own + applied;
         t.store(c.cell, c.tidx, c.own);
         const long long fx = fx_mass(applied);
-        if (a.brush_r > 0)
-            brush_add(a.acc4, a.mask, a.NE, a.spherical ? a.H : 0, a.spherical ? a.H + a.N : a.NE, a.brush_r, c.cell, fx);
-        else
-            red_add(a.acc4 + 4 * c.cell, fx);
+        red_add(a.acc4 + 4 * c.cell, fx);
         if (fx < 0) L.eroded_fx -= fx;
         else L.deposited_fx += fx;
     }

@@ -60,7 +60,7 @@ __device__ __forceinline__ void red_add(long long *p, long long v)
 // ---------------------------------------------------------------------------
 struct Layout {
     size_t cellA, cellB, live, metric8, route2, acc4, pend, tkey, town, counters, sortkeys, sortvals, cdf, cubtmp, cubtmp_bytes,
-        partial, thermal, flags, pwv, pwnode, total;
+        partial, thermal, flags, pwv, pwnode, spread, total;
     // ordered apply (exact mode): one wave's change lists and ranks
     size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_desc, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
         w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, w_act, hand, terr, error;
@@ -120,7 +120,6 @@ struct DropArgs {
     int ledger;          // 1: apply each droplet's ledger inline; 0: record the change lists only
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
-    int brush_r;  // the erode / deposit brush's radius (0: one cell)
     int cr_trig;  // 1: the face crossing's trig correctly rounded (the exact pass, the change-list hook); 0: CUDA's
 };
 

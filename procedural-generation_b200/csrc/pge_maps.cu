@@ -210,6 +210,107 @@ void read_accumulators(const Layout &lay, void *ws, double *acc, double *dtr, do
 }
 
 // ---------------------------------------------------------------------------
+// the erode / deposit brush: the change each cell received since the last spread (the wave apply adds
+// every entry's applied change to its own cell) is shared out over the active cells of its face within
+// distance < r + 1 (the interior ones on the sphere), weights r + 1 - distance in integers of
+// 1/PGE_BRUSH_SCALE renormalised over the footprint; each share is truncated toward zero and the rest
+// stays on the cell, so the total is kept exactly.  A gather: each cell adds the shares its neighbours
+// send it, computed by the same expression the sender uses for its rest, so no atomics are needed and the
+// result is the same whatever the order.
+// ---------------------------------------------------------------------------
+struct BrushGeo {
+    int NE, lo, hi, r;
+    const uint8_t *mask;
+};
+
+__device__ __forceinline__ int brush_weight(int r, int di, int dj)
+{
+    const double v = (double)(r + 1) - sqrt((double)(di * di + dj * dj));
+    return v > 0.0 ? (int)llround(PGE_BRUSH_SCALE * v) : 0;
+}
+
+__device__ __forceinline__ bool brush_valid(const BrushGeo &g, long long fb, int i, int j)
+{
+    if (i < g.lo || i >= g.hi || j < g.lo || j >= g.hi) return false;
+    return !g.mask || g.mask[fb + (long long)i * g.NE + j] == PGE_MASK_ACTIVE;
+}
+
+__device__ __forceinline__ long long brush_share(long long d, int q, int Q) { return (long long)((double)d * (double)q / (double)Q); }
+
+// pass 1: each cell's change since the last spread and, where it has one, its footprint's total weight
+__global__ void brush_delta_kernel(long long ncell, BrushGeo g, const long long *acc4, const long long *prev, long long *delta, int *Q)
+{
+    const long long plane = (long long)g.NE * g.NE;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const long long d = acc4[4 * c] - prev[c];
+        delta[c] = d;
+        int q = 0;
+        if (d != 0) {
+            const long long fb = c / plane * plane;
+            const int ei = (int)((c - fb) / g.NE), ej = (int)((c - fb) % g.NE);
+            for (int di = -g.r; di <= g.r; di++)
+                for (int dj = -g.r; dj <= g.r; dj++) {
+                    const int w = brush_weight(g.r, di, dj);
+                    if (w && ((di == 0 && dj == 0) || brush_valid(g, fb, ei + di, ej + dj))) q += w;
+                }
+        }
+        Q[c] = q;
+    }
+}
+
+// pass 2: the shares the footprint sends each cell, plus the rest of its own change; net change = the last spread + that
+__global__ void brush_gather_kernel(long long ncell, BrushGeo g, const long long *delta, const int *Q, long long *acc4, long long *prev)
+{
+    const long long plane = (long long)g.NE * g.NE;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x) {
+        const long long fb = c / plane * plane;
+        const int ei = (int)((c - fb) / g.NE), ej = (int)((c - fb) % g.NE);
+        long long sum = 0;
+        if (brush_valid(g, fb, ei, ej))
+            for (int di = -g.r; di <= g.r; di++) {
+                const int i = ei + di;
+                if (i < 0 || i >= g.NE) continue;
+                for (int dj = -g.r; dj <= g.r; dj++) {
+                    const int j = ej + dj;
+                    const int w = brush_weight(g.r, di, dj);
+                    if (!w || (di == 0 && dj == 0) || j < 0 || j >= g.NE) continue;
+                    const long long s = fb + (long long)i * g.NE + j;
+                    const long long d = delta[s];
+                    if (d != 0) sum += brush_share(d, w, Q[s]);
+                }
+            }
+        const long long d = delta[c];
+        if (d != 0) {
+            long long kept = d;
+            for (int di = -g.r; di <= g.r; di++)
+                for (int dj = -g.r; dj <= g.r; dj++) {
+                    const int w = brush_weight(g.r, di, dj);
+                    if (!w || (di == 0 && dj == 0) || !brush_valid(g, fb, ei + di, ej + dj)) continue;
+                    kept -= brush_share(d, w, Q[c]);
+                }
+            sum += kept;
+        }
+        if (sum != 0 || d != 0) {
+            const long long v = prev[c] + sum;
+            acc4[4 * c] = v;
+            prev[c] = v;
+        }
+    }
+}
+
+void brush_spread(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, int r, cudaStream_t st)
+{
+    const int NE = g.N + 2 * g.H;
+    BrushGeo bg{NE, g.spherical ? g.H : 0, g.spherical ? g.H + g.N : NE, r, s.mask};
+    long long *acc4 = ws_ptr<long long>(ws, lay.acc4);
+    long long *prev = ws_ptr<long long>(ws, lay.spread);
+    long long *delta = ws_ptr<long long>(ws, lay.pwv);
+    int *Q = ws_ptr<int>(ws, lay.flags);
+    brush_delta_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, bg, acc4, prev, delta, Q);
+    brush_gather_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, bg, delta, Q, acc4, prev);
+}
+
+// ---------------------------------------------------------------------------
 // thermal erosion (talus / creep mass wasting)
 // ---------------------------------------------------------------------------
 struct ThermalArgs {
@@ -951,7 +1052,7 @@ cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, v
     double *cdf = w + lay.ncell;
     double *keys = ws_ptr<double>(ws, lay.sortkeys);
     long long *ctr = ws_ptr<long long>(ws, lay.counters);
-    long long *lastc = ctr + 2, *erange = ctr + 4, *nsel = ctr + 6;
+    long long *lastc = ctr + 2, *erange = ctr + 24, *nsel = ctr + 26;  // slots 4 (the pass mode), 8, 12.. are taken
     long long *wq = ws_ptr<long long>(ws, lay.pwv);
     cudaError_t e = cudaMemsetAsync(lastc, 0, sizeof(long long), st);
     if (e != cudaSuccess) return e;

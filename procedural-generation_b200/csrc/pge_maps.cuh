@@ -19,6 +19,9 @@ void slope_erode_cap(const PgeGrid &g, const PgeState &s, double k, double exit_
 void smooth_step(const PgeGrid &g, const double *in, const float *metric_inv, const float *sqrt_det, double kappa, int keep,
                  double cell_m, double *out, cudaStream_t st);
 size_t cub_temp_bytes(int64_t ncell, int64_t max_droplets);
+// the erode / deposit brush (PgeParams.brush_radius): the net change the wave apply accumulated since the last call,
+// spread over each cell's footprint in integer shares, added to the accumulators' net-change column
+void brush_spread(const PgeGrid &g, const PgeState &s, const Layout &lay, void *ws, int r, cudaStream_t st);
 // numpy's pairwise float64 sum (mean = 1: divided by the count) of a[0, *count), on the stream
 size_t pairwise_scratch_bytes();
 void pairwise_sum(const double *a, const long long *count, void *scratch, double *out, int mean, cudaStream_t st);
