@@ -72,7 +72,10 @@ def run_batched(args, rank, world_size, dist, dev):
         for it in range(1, 2 + k):
             rng, u, off = gm.draw_spawns(w.params, "erosion", (it,), counts[i])
             pre[(i, it)] = (rng, torch.as_tensor(u, device=dev), torch.as_tensor(off, device=dev))
-    runner = batch.Runner(states, [w.params for w in sub], costs=[w.cost for w in sub]) if sub else None
+    from pgerosion import _lib
+
+    wave_kw = {} if args.batch_apply == "ordered" else {"apply": _lib.APPLY_WAVE, "wave": max(counts) * 2 if counts else 1}
+    runner = batch.Runner(states, [w.params for w in sub], costs=[w.cost for w in sub], **wave_kw) if sub else None
     if runner:
         runner.step(1, n_particles=counts)  # warm-up: workspaces, first pass of every world
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -84,7 +87,7 @@ def run_batched(args, rank, world_size, dist, dev):
     for i, (st, w) in enumerate(zip(states, sub)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        one += gm.step(st, w.params, st.iteration, n_particles=counts[i], predrawn=pre[(i, st.iteration)])["droplet_steps"]
+        one += gm.step(st, w.params, st.iteration, n_particles=counts[i], predrawn=pre[(i, st.iteration)], **wave_kw)["droplet_steps"]
         e1.record()
         e1.synchronize()
         worst = max(worst, e0.elapsed_time(e1))
@@ -106,7 +109,7 @@ def run_batched(args, rank, world_size, dist, dev):
     del runner, states
     torch.cuda.empty_cache()
     return {"workload": f"{len(worlds)} worlds, N_c {sizes[0]}..{sizes[-1]} (mean N_c^2 {np.mean(np.square(sizes)):.0f}), "
-                        "6 N^2/8 droplets, max_steps 2N, rates +-30 %, ordered apply",
+                        f"6 N^2/8 droplets, max_steps 2N, rates +-30 %, {args.batch_apply} apply",
             "one_by_one": {"value": v_one, "unit": "droplet-steps/s", "ms_per_step": ms_one},
             "concurrent": {"value": v_tog, "unit": "droplet-steps/s", "ms_per_step": ms_tog / k, "steps": k},
             "speedup": v_tog / v_one,
@@ -622,6 +625,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-worlds measurement")
     ap.add_argument("--batch-worlds", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--batch-apply", default="ordered", choices=("ordered", "wave"), help="the batched worlds' apply")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the calibration (adjoint) measurement")
     ap.add_argument("--adjoint-reps", type=int, default=2)
     ap.add_argument("--adjoint-only", action="store_true", help="run the calibration (adjoint) measurement alone")
