@@ -132,8 +132,8 @@ HYPS_TOL_MANY = 25.0
 def test_full_iterations_reference_waves_match_oracle(cuda):
     """The tiny world's steps, ordered apply with the reference's chunk as
     the wave: mass balance every iteration; hypsometry within 0.5 m of the
-    oracle after the first iteration and within the chaotic bound of the
-    reference's own state after all of them."""
+    oracle after the first iteration and of the reference's own state after
+    all of them."""
     c = step_case()
     t = c["t"]
     g = gm.ErosionState.from_world(c["world"])
@@ -161,7 +161,10 @@ def test_full_iterations_reference_waves_match_oracle(cuda):
     a = g.to_numpy()
     hg = hypsometry(a["height"], a["sediment"], inter, 50.0)
     hr = hypsometry(t["height"], t["sediment"], inter, 50.0)
-    assert np.abs(hg - hr).max() <= HYPS_TOL_MANY, (hg, hr)
+    # with the correctly rounded crossing and numpy's order for the spawn total and the uplift mean,
+    # this world's run follows the reference's to the north star's literal bound over every iteration
+    print(f"tiny world, {c['iterations']} iterations: largest hypsometry difference {np.abs(hg - hr).max():.4f} m")
+    assert np.abs(hg - hr).max() <= HYPS_TOL_FIRST, (hg, hr)
 
 
 @pytest.mark.parametrize("apply,wave", [(_lib.APPLY_ORDERED, None), (_lib.APPLY_WAVE, 65536)])
