@@ -267,6 +267,19 @@ def land_loss(z: torch.Tensor, target: torch.Tensor, land: torch.Tensor, unit_m:
     return (d[land] ** 2).mean()
 
 
+def block_loss(z: torch.Tensor, target: torch.Tensor, land: torch.Tensor, unit_m: float, N: int, H: int,
+               block: int = 8) -> torch.Tensor:
+    """Mean squared difference in metres of the surface's and the target's
+    means over ``block`` x ``block`` cell blocks of each face's interior,
+    over the blocks that are land in the majority: the shape of the valleys
+    and ranges without the cell-scale placement of single channels, which
+    moves chaotically with any change of the rates."""
+    pool = lambda a: torch.nn.functional.avg_pool2d(a[:, None, H:H + N, H:H + N], block)[:, 0]
+    d = (pool(z) - pool(target)) * float(unit_m)
+    keep = pool(land.to(z.dtype)) > 0.5
+    return (d[keep] ** 2).mean()
+
+
 # --------------------------------------------------------------------------
 # the calibration workload
 # --------------------------------------------------------------------------
@@ -316,23 +329,79 @@ def rates_of(params) -> torch.Tensor:
 
 
 def calibrate(calib: Calibration, target: torch.Tensor, land: torch.Tensor, erod0: torch.Tensor, rates0: torch.Tensor,
-              steps: int = 10, lr_rates: float = 0.05, lr_field: float = 0.02, field: bool = True) -> dict:
+              steps: int = 10, lr_rates: float = 0.05, lr_field: float = 0.02, field: bool = True, method: str = "line",
+              loss_fn=None, eta0: float = 0.1, eta_min: float = 1e-3) -> dict:
     """Gradient-based calibration in place of the grid sweep of the rates
-    (docs/erosion-tuning.md's procedure): Adam on the log of the four rates
-    and (``field``) on the per-cell erodibility field, each step one forward
-    run of ``calib`` and its adjoint.  Returns the loss before every step and
-    after the last, and the rates and field after each step."""
+    (docs/erosion-tuning.md's procedure), each step one forward run of
+    ``calib`` and its adjoint.
+
+    ``method`` "line" (the default): the four rates in log space move along
+    the normalised negative gradient by a backtracking line search (step
+    ``eta0``, halved until the loss falls, down to ``eta_min``; the next step
+    starts from twice the accepted one); the field stays at ``erod0``.  The
+    loss falls or the run stops, whatever the roughness of the loss surface
+    (the gradient is the truncated one along the recorded paths: a descent
+    direction for small steps, not a model of the loss at large ones).
+    ``method`` "adam": Adam on the log-rates (``lr_rates``) and, with
+    ``field``, on the per-cell erodibility field (``lr_field``).
+
+    ``loss_fn(z)`` is the loss of a final surface (default: ``land_loss``
+    against ``target`` over ``land``).  Returns the loss before every step
+    and after the last (for "line", the steps taken), the rates after each step (for "line" also the
+    accepted step sizes and the numbers of forward and adjoint runs), and the
+    field."""
     dev = calib.state.height.device
+    unit = calib.state.height_unit_m
+    if loss_fn is None:
+        loss_fn = lambda z: land_loss(z, target, land, unit)
     logr = torch.log(rates0.detach().to(dev, torch.float64)).clone().requires_grad_(True)
+    losses, rates_hist = [], []
+    if method == "line":
+        erod = erod0.detach().clone()
+        etas, forwards, adjoints = [], 1, 0
+        eta = float(eta0)
+        loss = loss_fn(erode(erod, torch.exp(logr), calib))
+        for _ in range(int(steps)):
+            logr.grad = None
+            loss.backward()
+            adjoints += 1
+            cur = float(loss.detach())
+            losses.append(cur)
+            g = logr.grad.detach()
+            gn = float(g.norm())
+            if not np.isfinite(gn) or gn == 0.0:
+                losses.pop()
+                break
+            accepted = None
+            while eta >= eta_min:
+                with torch.no_grad():
+                    trial = (logr - eta * g / gn).detach()
+                trial.requires_grad_(True)
+                tl = loss_fn(erode(erod, torch.exp(trial), calib))
+                forwards += 1
+                if float(tl.detach()) < cur:
+                    accepted = (trial, tl)
+                    break
+                eta *= 0.5
+            if accepted is None:  # no step lowered the loss: the run ends where it is
+                losses.pop()
+                break
+            logr, loss = accepted
+            etas.append(eta)
+            rates_hist.append(torch.exp(logr).detach().cpu().tolist())
+            eta = min(2.0 * eta, float(eta0))
+        losses.append(float(loss.detach()))
+        return {"loss": losses, "rates": rates_hist, "field": erod, "eta": etas, "forwards": forwards, "adjoints": adjoints}
+    if method != "adam":
+        raise ValueError(f"calibrate: method {method!r} is neither 'line' nor 'adam'")
     erod = erod0.detach().clone().requires_grad_(field)
     groups = [{"params": [logr], "lr": lr_rates}]
     if field:
         groups.append({"params": [erod], "lr": lr_field})
     opt = torch.optim.Adam(groups)
-    losses, rates_hist = [], []
     for _ in range(int(steps)):
         opt.zero_grad()
-        loss = land_loss(erode(erod, torch.exp(logr), calib), target, land, calib.state.height_unit_m)
+        loss = loss_fn(erode(erod, torch.exp(logr), calib))
         loss.backward()
         losses.append(float(loss.detach()))
         opt.step()
@@ -340,6 +409,6 @@ def calibrate(calib: Calibration, target: torch.Tensor, land: torch.Tensor, erod
             erod.clamp_(0.05, 5.0)
         rates_hist.append(torch.exp(logr).detach().cpu().tolist())
     with torch.no_grad():
-        final = land_loss(erode(erod, torch.exp(logr), calib), target, land, calib.state.height_unit_m)
+        final = loss_fn(erode(erod, torch.exp(logr), calib))
     losses.append(float(final))
     return {"loss": losses, "rates": rates_hist, "field": erod.detach()}

@@ -341,3 +341,22 @@ def test_autograd_function_matches_the_reverse(cuda):
         print(f"carry_path {carry_path} carry_terrain {carry_terrain}: loss {float(loss):.6e} rate gradient {pb.tolist()}")
         grads[carry_path] = pb.cpu().numpy()
     assert np.all(np.sign(grads[False][:3]) == np.sign(grads[True][:3])), grads
+
+
+def test_line_search_calibration_lowers_the_loss(cuda):
+    """Three steps of the line-search calibration from the base rates toward
+    the target of rates x (1.25, 0.8, 1.2, 0.85): the truncated gradient is a
+    descent direction (at least one step accepted, the loss lower at the end
+    than at the start, never higher after a step), for the land loss and the
+    4 x 4-block loss."""
+    from pgerosion import adjoint as adj
+
+    st, params, calib, target, land = _calibration_case()
+    unit, N, H = st.height_unit_m, st.N, st.H
+    for name, fn in (("land", None), ("block4", lambda z: adj.block_loss(z, target, land, unit, N, H, block=4))):
+        cal = adj.calibrate(calib, target, land, adj.erodibility_init(st, seed=0), adj.rates_of(params), steps=3,
+                            method="line", loss_fn=fn, eta0=0.2, eta_min=1e-3)
+        L = cal["loss"]
+        print(f"{name}: loss {L} steps {cal['eta']} forwards {cal['forwards']} rates {cal['rates'][-1] if cal['rates'] else None}")
+        assert len(cal["eta"]) >= 1, "no step lowered the loss"
+        assert all(b < a for a, b in zip(L[:-1], L[1:])), L
