@@ -46,6 +46,10 @@
  *                                                  globe/hydro/priority_flood.py:127-191,
  *                                                  globe/hydro/routing.py:28-90,
  *                                                  globe/hydro/balance.py:63-284
+ *   pge_lake_balance_fill pge_lake_balance with erosion.lake_fill: the loads the
+ *                         lakes kept laid over their floors, the lakes numbered and
+ *                         given their room (HOST code, host pointers)
+ *                                                  globe/erosion/maps.py:422-479, 490-628
  *   pge_window_lake_balance  ErosionState._balance_window_lakes (window_lake_evap > 0):
  *                         a window's lakes settled against evaporation (HOST code)
  *                                                  globe/erosion/maps.py:675-736
@@ -165,15 +169,25 @@ typedef struct PgeState {
     const double *route;     /* (F,NE,NE) routing surface (pge_route_flood) or NULL: particles steer on it where it
                                 stands above the terrain (particle.py:453-460, 556-559); float64 trace only */
     const uint8_t *lake_flag; /* (F,NE,NE) overflowing lakes (ErosionState.lake_flag, maps.py:87) or NULL; read only
-                                 with `route`: 1 a lake, 2 a lake with room for its rivers' load (the same to this
-                                 library, which parks no loads: erosion.lake_fill off).  A droplet entering a lake
-                                 drops lake_trap of its load at the shore, crosses it without touching the bed and
-                                 counts no pit steps on it; the bed is never eroded below the lake's routing surface
-                                 (particle.py:186-190, 626-636, 751-763, 952-956) */
+                                 with `route`: 1 a lake, 2 a lake with room for its rivers' load (the same as 1
+                                 unless lake_load is set).  A droplet entering a lake drops lake_trap of its load
+                                 at the shore, crosses it without touching the bed and counts no pit steps on it;
+                                 the bed is never eroded below the lake's routing surface (particle.py:186-190,
+                                 626-636, 751-763, 952-956) */
     const float *roots;       /* (F,NE,NE) the share of a droplet's exchange with the bed the plants hold back
                                  (erosion.vegetation, maps.py:113; in [0, 1]) or NULL: bare ground.  The
                                  exchange rate on land is scaled by 1 - roots (particle.py:615-618); not with
                                  the adjoint's tape */
+    double *lake_load;        /* (F,NE,NE) the lake parks (erosion.lake_fill, maps.py:105-107) or NULL: off.  With
+                                 `route` and `lake_flag`, a droplet entering a lake flagged 2 that its shore had no
+                                 room to take the trapped load for parks the rest on the lake cell it steps onto
+                                 (a change-list entry of volume -3, at most 8 a droplet, particle.py:672-696);
+                                 the ordered apply counts each lake's room down in droplet order, adds what it
+                                 takes here and adds the rest to the droplet's leftover load (particle.py:
+                                 912-933, 1019).  Ordered apply (and the change-list hook) only */
+    const int32_t *lake_id;   /* (F,NE,NE) the lake of lake_room each cell belongs to, -1 none (read with lake_load) */
+    double *lake_room;        /* (lakes) the room each lake has left (cell units), counted down in place */
+    int64_t lakes;            /* entries of lake_room */
 } PgeState;
 
 /* droplet spawns of one iteration: rain first, then re-injected stockpiles */
@@ -472,6 +486,43 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
                              const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                              double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
                              PgeLakeInfo *info);
+
+/* erosion.lake_fill's side of a lake refresh (maps.py:490-628), host arrays,
+ * interior (6,N,N) in cell-id order unless noted */
+typedef struct PgeLakeFill {
+    double grade;          /* the lake plain's rise per cell from the outlet (cell units: basin_fill_grade x cell km) */
+    double ice_evap;       /* a lake with a cell of evap <= ice_evap is frozen: it takes no load */
+    double rise;           /* the plain stands at most this much above the water (cell units) */
+    const float *evap;     /* evaporation field */
+    const double *centres; /* (6,N,N,3) unit-sphere cell centres (the outlet distance) */
+    const double *height;  /* bedrock and sediment (the surface after laying) */
+    const double *sediment;
+    double *lake_load;     /* in: the loads parked since the last refresh; out: zero */
+    int32_t *lake_id;      /* in: the last refresh's lake of each cell (-1 none); out: this refresh's */
+    double *lay;           /* out: sediment laid on each cell (the caller adds it to sediment; with the
+                              isostasy, load_share x lay to its load) */
+    double *pending;       /* out: loads that go on as stockpiles (their lake drained, or rounding), 0 elsewhere */
+    double *lake_room;     /* out: the room each numbered lake has left, lake_room_cap entries at most */
+    int64_t lake_room_cap;
+    int64_t lakes;         /* out: lakes numbered (open, warm, with room left) */
+    double parked, laid, stray, room; /* out: totals (cell units) */
+} PgeLakeFill;
+
+/* pge_lake_balance with erosion.lake_fill (maps.py:422-479 with `fill`, and
+ * settle_lake_loads, maps.py:490-628), on the HOST.  After the balance, the
+ * overflowing lakes (cells joined at one water level) receive the loads
+ * parked on their cells since the last refresh (a load whose cell is no
+ * longer under a lake goes to the lake of this refresh covering most of its
+ * old lake, else on as a stockpile); each lake fills towards a plain graded
+ * `grade` per flood step from its outlet and at most `rise` above its water,
+ * the cells farthest from the outlet first; a lake with room left and no
+ * frozen cell is numbered (lake_id, lake_room) and its cells flagged 2.
+ * lake_flag then marks the lakes still deeper than min_depth over the
+ * surface with the laid sediment.  Other arguments as pge_lake_balance. */
+PGE_API int pge_lake_balance_fill(const PgeGrid *g, const int32_t *owner, const float *metric, const float *cell_area,
+                                  double cell_size_m, const float *surface, const uint8_t *ocean, const float *precip,
+                                  const float *pet, double lake_evap, double land_evap, double min_depth, uint8_t *lake_flag,
+                                  float *water, float *closed_level, PgeLakeFill *fill, PgeLakeInfo *info);
 
 /* The lakes of a window balanced against evaporation (maps.py:675-736,
  * erosion.window_lakes with window_lake_evap > 0), on the HOST (host

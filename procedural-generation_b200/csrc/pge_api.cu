@@ -186,11 +186,14 @@ Layout layout(const PgeGrid &g)
     L.w_segpos = take(4 * ws);
     L.w_runscan = take(4 * ws);
     L.w_segscan = take(4 * ws);
-    L.w_temp_bytes = ordered_temp_bytes(ws);
+    L.w_temp_bytes = ordered_temp_bytes(ws, L.max_wave);
     L.w_temp = take(L.w_temp_bytes);
     L.w_dth = take(4 * L.max_wave);
     L.w_keep = take(8 * L.max_wave);
     L.w_act = take(8 * ws);
+    L.w_park_n = take(4 * L.max_wave);
+    L.w_park_k = take(4 * LAKE_PARKS * L.max_wave);
+    L.w_park_rest = take(8 * LAKE_PARKS * L.max_wave);
     L.hand = take(16 * L.ncell);
     L.terr = take(16 * L.ncell);
     L.error = take(256);
@@ -228,6 +231,13 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         const bool lateral = p->lateral_rate > 0.0;
         if (lateral && (p->precision != PGE_PREC_F64 || tape))
             return fail(PGE_E_UNSUPPORTED, "the bank cut (lateral_rate) needs the float64 trace and no tape");
+        const bool parks = s->lake_load != nullptr;
+        if (parks) {
+            if (!s->route || !s->lake_flag || !s->lake_id || !s->lake_room || s->lakes < 1)
+                return fail(PGE_E_ARG, "lake parks (lake_load) need route, lake_flag, lake_id and lake_room (lakes >= 1)");
+            if (p->apply != PGE_APPLY_ORDERED && !rec_cell)
+                return fail(PGE_E_UNSUPPORTED, "lake parks count each lake's room down in droplet order: ordered apply only");
+        }
         int bps = tape ? droplet_blocks_per_sm_f64_tape(threads)
                   : lateral ? droplet_blocks_per_sm_f64_lateral(threads, true, s->route != nullptr)
                   : s->route ? droplet_blocks_per_sm_f64_route(threads, true)
@@ -282,6 +292,10 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
         // the exact pass and the change-list hook follow the reference's arithmetic; the order-free wave apply
         // (and its tape, which the adjoint reverses with the same functions) takes CUDA's own trig
         a.cr_trig = (p->apply == PGE_APPLY_ORDERED || rec_cell != nullptr) ? 1 : 0;
+        a.parks = parks ? 1 : 0;
+        a.park_n = a.park_k = nullptr;
+        // the change-list hook with lake parks records the lists only: the rooms are counted by the ordered apply
+        if (parks && rec_cell) a.ledger = 0;
         unsigned long long *ctr = ws_ptr<unsigned long long>(ws, lay.counters);
         const long long wave = p->wave;
         const long long nw = (P + wave - 1) / wave;
@@ -327,6 +341,30 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             oa.p = *p;
             oa.stats = stats;
             oa.error = ws_ptr<int>(ws, lay.error);
+            ParkWave pw{};
+            if (parks) {
+                a.park_n = ws_ptr<int32_t>(ws, lay.w_park_n);
+                a.park_k = ws_ptr<int32_t>(ws, lay.w_park_k);
+                oa.park_n = a.park_n;
+                oa.park_rest = ws_ptr<double>(ws, lay.w_park_rest);
+                pw.cap = (int)lay.cap;
+                pw.cell = a.rec_cell;
+                pw.delta = a.rec_delta;
+                pw.park_n = a.park_n;
+                pw.park_k = a.park_k;
+                pw.lake_id = s->lake_id;
+                pw.lake_room = s->lake_room;
+                pw.lakes = s->lakes;
+                pw.lake_load = s->lake_load;
+                pw.rest = ws_ptr<double>(ws, lay.w_park_rest);
+                // the cell sort's scan buffers are free until the wave's own ranks
+                pw.keys_in = ws_ptr<uint32_t>(ws, lay.w_runstart);
+                pw.keys_out = ws_ptr<uint32_t>(ws, lay.w_segpos);
+                pw.vals_in = ws_ptr<int32_t>(ws, lay.w_runscan);
+                pw.vals_out = ws_ptr<int32_t>(ws, lay.w_segscan);
+                pw.temp = ws_ptr<void>(ws, lay.w_temp);
+                pw.temp_bytes = lay.w_temp_bytes;
+            }
             ow.cap = (int)lay.cap;
             // sort keys: the cell, cbits wide; all ones marks a slot past its list's end
             int cbits = 0;
@@ -383,6 +421,10 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");
                 ow.nw = nd;
                 oa.nw = ow.nw;
+                if (parks) {
+                    pw.nw = nd;
+                    if ((e = park_wave(pw, st)) != cudaSuccess) return cuda_fail(e, "lake parks");
+                }
                 // epochs step by 2^ebits > wave, so a counter never reaches the next wave's values;
                 // they are 32-bit, and start over (counters zeroed) before they would wrap
                 if (((unsigned long long)(w - ebase + 2) << ebits) >= (1ull << 32)) {
@@ -597,8 +639,31 @@ PGE_API int pge_lake_balance(const PgeGrid *g, const int32_t *owner, const float
     if (!(cell_size_m > 0.0) || !(min_depth >= 0.0) || !(lake_evap >= 0.0) || !(land_evap >= 0.0))
         return fail(PGE_E_ARG, "lake_balance: cell_size_m must be > 0 and min_depth, lake_evap, land_evap >= 0");
     if (lake_balance_host(g->N, g->H, owner, metric, cell_area, cell_size_m, surface, ocean, precip, pet, lake_evap, land_evap,
-                          min_depth, lake_flag, water, closed_level, info) != 0)
+                          min_depth, lake_flag, water, closed_level, nullptr, info) != 0)
         return fail(PGE_E_UNSUPPORTED, "lake_balance: a land cell has no flow direction (unreached by the flood)");
+    return PGE_OK;
+}
+
+PGE_API int pge_lake_balance_fill(const PgeGrid *g, const int32_t *owner, const float *metric, const float *cell_area,
+                                  double cell_size_m, const float *surface, const uint8_t *ocean, const float *precip,
+                                  const float *pet, double lake_evap, double land_evap, double min_depth, uint8_t *lake_flag,
+                                  float *water, float *closed_level, PgeLakeFill *fill, PgeLakeInfo *info)
+{
+    int r;
+    if ((r = check_shape(g))) return r;
+    if (!g->spherical) return fail(PGE_E_UNSUPPORTED, "lake_balance_fill: the planet's lakes");
+    if (!owner || !metric || !cell_area || !surface || !ocean || !precip || !pet || !lake_flag || !fill)
+        return fail(PGE_E_ARG, "lake_balance_fill: NULL pointer");
+    if (!fill->evap || !fill->centres || !fill->height || !fill->sediment || !fill->lake_load || !fill->lake_id || !fill->lay ||
+        !fill->pending || !fill->lake_room || fill->lake_room_cap < 1)
+        return fail(PGE_E_ARG, "lake_balance_fill: a NULL fill array or no lake_room entry");
+    if (!(cell_size_m > 0.0) || !(min_depth >= 0.0) || !(lake_evap >= 0.0) || !(land_evap >= 0.0) || !(fill->grade >= 0.0) ||
+        !(fill->rise >= 0.0))
+        return fail(PGE_E_ARG, "lake_balance_fill: cell_size_m must be > 0 and min_depth, lake_evap, land_evap, grade, rise >= 0");
+    const int rc = lake_balance_host(g->N, g->H, owner, metric, cell_area, cell_size_m, surface, ocean, precip, pet, lake_evap,
+                                     land_evap, min_depth, lake_flag, water, closed_level, fill, info);
+    if (rc == -1) return fail(PGE_E_UNSUPPORTED, "lake_balance_fill: a land cell has no flow direction (unreached by the flood)");
+    if (rc == -2) return fail(PGE_E_ARG, "lake_balance_fill: more lakes take load than lake_room_cap (%lld)", (long long)fill->lake_room_cap);
     return PGE_OK;
 }
 

@@ -664,7 +664,8 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
     bool has_pe = false;
     Ledger L;
     int rec_n = 0;
-    int nbank = 0;  // bank entries (volume -2) of this droplet: entries, not steps
+    int nbank = 0;  // bank entries (volume -2) and lake parks (volume -3) of this droplet: entries, not steps
+    int parks = 0;  // loads this droplet has left in lakes (at most LAKE_PARKS, particle.py:418)
 
     while (true) {
         // ---- refill: lanes without a droplet take the next indices of the wave
@@ -709,6 +710,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                     t.reset(++gen);
                     rec_n = 0;
                     nbank = 0;
+                    parks = 0;
                     const int ei = cell_of(x, N) + H, ej = cell_of(y, N) + H;
                     load_view(a, f, x, y, ei, ej, cv);
                     cur.cell = cv.cell;
@@ -742,6 +744,9 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
         bool have_entry = false;
         bool have_bank = false;
         Entry bank_en;
+        [[maybe_unused]] bool have_park = false;
+        [[maybe_unused]] long long park_cell = 0;
+        [[maybe_unused]] double park_delta = 0.0;
         bool moved = false;
         Entry en;
         do {
@@ -931,12 +936,14 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 }
                 if (a.roots) k_e *= R(1) - R(__ldg(a.roots + cv.cell));  // roots hold the ground (particle.py:615-618)
                 R cdiff = k_e * (c_eq - sed);
+                [[maybe_unused]] R trapped = R(0);
                 if (ROUTE) {
                     if (in_lake) {
                         cdiff = R(0);  // crossing a lake: the bed sees nothing (particle.py:626-629)
                     } else if (sed > R(0) && nflag >= 1.5f) {
                         const R trap = -R(p.lake_trap) * sed;  // entering a lake: the load drops at the shore (630-634)
                         if (trap < cdiff) cdiff = trap;
+                        if (nflag >= 2.5f) trapped = R(p.lake_trap) * sed;  // ...and this lake has room for the rest (636)
                     }
                 }
                 const R kexp = R(1) + q * k_conc;
@@ -977,6 +984,19 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 en.mb = (float)(vol * sb);
                 en.sidx = step;
                 have_entry = true;
+                if (!LEDGER && ROUTE && a.parks && trapped > R(0) && parks < LAKE_PARKS) {
+                    // a lake with room keeps what its shore did not take (particle.py:672-696): parked on the lake
+                    // cell stepped onto, an entry of volume -3 after the step's own, for the apply to count
+                    // against the lake's room
+                    const R rest = trapped + cdiff;  // cdiff <= 0: what the shore took
+                    if (rest > R(0)) {
+                        parks++;
+                        sed -= rest;
+                        park_cell = nv.cell;
+                        park_delta = (double)(rest * vol_rel);
+                        have_park = true;
+                    }
+                }
                 if (LATERAL && cdiff > R(0)) {
                     // the outside of the bend (particle.py:699-738): a droplet cutting and turning also cuts
                     // the bank one cell across the flow, down towards the bed it just eroded; the change
@@ -1064,6 +1084,19 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
             }
             rec_n++;
         }
+        if (!LEDGER && ROUTE && have_park) {
+            if (a.rec_cell && rec_n < a.rec_cap) {
+                const long long o = (d - a.rec_base) * a.rec_cap + rec_n;
+                a.rec_cell[o] = (int32_t)park_cell;
+                a.rec_delta[o] = park_delta;
+                a.rec_vol[o] = -3.0f;
+                a.rec_mom[2 * o] = 0.0f;
+                a.rec_mom[2 * o + 1] = 0.0f;
+            }
+            if (a.park_k) a.park_k[(d - a.rec_base) * LAKE_PARKS + parks - 1] = rec_n;
+            rec_n++;
+            nbank++;
+        }
         if (LATERAL && have_bank) {
             // the bank entry follows the step's own: the step entry is applied with the bank as its next
             // cell, the bank entry with the next step's cell (the reference's list order)
@@ -1143,6 +1176,7 @@ __global__ void __launch_bounds__(256, MINB) droplet_kernel(const DropArgs a)
                 a.rec_count[d - a.rec_base] = rec_n;
                 a.rec_death[d - a.rec_base] = (int8_t)cause;
             }
+            if (a.park_n) a.park_n[d - a.rec_base] = parks;
             alive = false;
             continue;
         }

@@ -64,6 +64,8 @@ struct Layout {
     // ordered apply (exact mode): one wave's change lists and ranks
     size_t w_cell, w_delta, w_vol, w_mom, w_count, w_death, w_desc, w_keys0, w_keys1, w_vals0, w_vals1, w_runstart,
         w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, w_act, hand, terr, error;
+    // the lake parks of one wave: per droplet its park count and entry indices, per park the refused rest
+    size_t w_park_n, w_park_k, w_park_rest;
     int64_t ncell, nmetric, nslots, table_cap, table_slots, max_droplets, max_wave, wave_slots, cap;
 };
 
@@ -121,6 +123,12 @@ struct DropArgs {
     int minb;  // kernel variant: registers for 1 or 2 resident blocks of 256 per SM
     int lanes; // droplets in flight per warp (1..32): fewer spread a latency-bound wave over more warps
     int cr_trig;  // 1: the face crossing's trig correctly rounded (the exact pass, the change-list hook); 0: CUDA's
+    // lake parks (erosion.lake_fill, record-only variants): a droplet entering a lake with room parks the load its
+    // shore did not take on the lake cell (an entry of volume -3); park_n[d - rec_base] counts them and
+    // park_k[(d - rec_base) * LAKE_PARKS + j] is the j-th one's entry index (both may be nullptr with parks on:
+    // the change-list hook)
+    int parks;
+    int32_t *park_n, *park_k;
 };
 
 // launchers of the two precisions (separate translation units: the float64

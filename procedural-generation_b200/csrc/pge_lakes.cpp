@@ -313,11 +313,178 @@ struct LakeScratch {
     std::vector<float> filled, water;
     std::vector<int64_t> parent, order, pop_seq, down, topo, lab, cells, outlet_lake;
     std::vector<double> w, wr, af, et, pe, acc, run;
+    std::vector<uint8_t> olake, takes;
+    std::vector<float> surf_after;
 };
 LakeScratch &lake_scratch()
 {
     static thread_local LakeScratch s;
     return s;
+}
+
+// numpy's clip(x, lo, hi) for float64: max then min, each a plain compare (so -0.0 clipped at 0.0 is 0.0)
+inline double clip(double x, double lo, double hi)
+{
+    const double m = x > lo ? x : lo;
+    return m < hi ? m : hi;
+}
+
+// settle_lake_loads (maps.py:490-628): the loads the lakes kept laid over their floors, the lakes numbered
+// for the kernel.  olake: the overflowing lakes of this refresh (interior cell ids); water / surf their level
+// and the ground under them (float32); parent / order / pop_seq the flood they came from.  Writes F.lay,
+// F.pending (dense), F.lake_id, F.lake_room, the totals; takes[c] = 1 on the cells of numbered lakes.
+// Returns 0, or -1 when more lakes take load than F.lake_room_cap holds.
+int settle_lake_loads(const Sphere &S, const std::vector<uint8_t> &olake, const std::vector<float> &water, const float *surf,
+                      const std::vector<int64_t> &parent, const std::vector<int64_t> &order, const std::vector<int64_t> &pop_seq,
+                      PgeLakeFill &F, std::vector<uint8_t> &takes)
+{
+    const int64_t M = (int64_t)6 * S.N * S.N;
+    double *load = F.lake_load;
+    int32_t *lake_id = F.lake_id;
+    std::memset(F.lay, 0, sizeof(double) * M);
+    std::memset(F.pending, 0, sizeof(double) * M);
+    takes.assign(M, 0);
+    F.parked = F.laid = F.stray = F.room = 0.0;
+    F.lakes = 0;
+    for (int64_t c = 0; c < M; c++) F.parked += load[c];
+    // the lakes: cells joined at one water level, numbered by their lowest cell id
+    std::vector<int64_t> lab;
+    const int64_t n = label_components(S, olake, water, lab);
+    // a load belongs to the lake it was parked in: this refresh's lake over its cell, else the heir of its
+    // old lake (the lake of this refresh covering most of it; ties to the higher number), else a stockpile
+    std::vector<double> have(n > 0 ? n : 1, 0.0);
+    bool any_held = false;
+    for (int64_t c = 0; c < M && !any_held; c++) any_held = load[c] > 0.0;
+    if (any_held) {
+        int32_t was_max = -1;
+        for (int64_t c = 0; c < M; c++) was_max = lake_id[c] > was_max ? lake_id[c] : was_max;
+        const int64_t n_was = (int64_t)was_max + 1;
+        std::vector<int64_t> heir(n_was > 0 ? n_was : 1, -1);
+        if (n > 0) {
+            std::vector<int64_t> keys;
+            for (int64_t c = 0; c < M; c++)
+                if (lake_id[c] >= 0 && lab[c] >= 0) keys.push_back((int64_t)lake_id[c] * n + lab[c]);
+            std::sort(keys.begin(), keys.end());
+            // per old lake the (count, new lake) largest in that order
+            std::vector<int64_t> best_cnt(n_was > 0 ? n_was : 1, -1);
+            for (size_t t = 0; t < keys.size();) {
+                size_t u = t;
+                while (u < keys.size() && keys[u] == keys[t]) u++;
+                const int64_t cnt = (int64_t)(u - t), old = keys[t] / n, nl = keys[t] % n;
+                if (cnt >= best_cnt[old]) {  // keys ascend, so an equal count goes to the higher new lake
+                    best_cnt[old] = cnt;
+                    heir[old] = nl;
+                }
+                t = u;
+            }
+        }
+        for (int64_t c = 0; c < M; c++) {
+            if (!(load[c] > 0.0)) continue;
+            const int64_t to = lab[c] >= 0 ? lab[c] : (lake_id[c] >= 0 ? heir[lake_id[c]] : -1);
+            if (to >= 0) {
+                have[to] += load[c];
+            } else {  // its lake has drained altogether: on downstream as a stockpile
+                F.pending[c] += load[c];
+                F.stray += load[c];
+            }
+        }
+    }
+    for (int64_t c = 0; c < M; c++) lake_id[c] = -1;
+    std::vector<int64_t> cells;
+    for (int64_t c = 0; c < M; c++)
+        if (lab[c] >= 0) cells.push_back(c);
+    const int64_t K = (int64_t)cells.size();
+    if (K > 0) {
+        // the plain each lake fills towards: its water at the outlet, `grade` higher per flood step inside it
+        std::vector<double> plain(M);
+        for (int64_t c = 0; c < M; c++) plain[c] = (double)water[c];
+        for (const int64_t c : pop_seq) {
+            if (lab[c] < 0) continue;
+            const int64_t q = parent[c];
+            if (q >= 0 && lab[q] == lab[c]) plain[c] = plain[q] + F.grade;
+        }
+        std::vector<double> room(K), far(K);
+        for (int64_t t = 0; t < K; t++) {
+            const int64_t c = cells[t];
+            const double w = (double)water[c] + F.rise, g = plain[c];
+            const double r = (g <= w ? g : w) - (double)surf[c];
+            room[t] = r >= 0.0 ? r : 0.0;
+        }
+        // each lake's outlet: its first popped cell; distances from it as the crow flies
+        std::vector<int64_t> first(n, INT64_MAX), outlet(n, 0);
+        for (const int64_t c : cells) first[lab[c]] = order[c] < first[lab[c]] ? order[c] : first[lab[c]];
+        for (const int64_t c : cells)
+            if (order[c] == first[lab[c]]) outlet[lab[c]] = c;
+        for (int64_t t = 0; t < K; t++) {
+            const double *a = F.centres + 3 * cells[t], *b = F.centres + 3 * outlet[lab[cells[t]]];
+            const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+            far[t] = std::sqrt((dx * dx + dy * dy) + dz * dz);
+        }
+        // farthest from the outlet first within each lake (ties in cell order)
+        std::vector<int64_t> o(K);
+        for (int64_t t = 0; t < K; t++) o[t] = t;
+        std::stable_sort(o.begin(), o.end(), [&](int64_t x, int64_t y) {
+            const int64_t lx = lab[cells[x]], ly = lab[cells[y]];
+            if (lx != ly) return lx < ly;
+            return -far[x] < -far[y];
+        });
+        std::vector<int64_t> sc(K), L(K);
+        std::vector<double> sr(K);
+        for (int64_t t = 0; t < K; t++) {
+            sc[t] = cells[o[t]];
+            sr[t] = room[o[t]];
+            L[t] = lab[sc[t]];
+        }
+        std::vector<int64_t> ptr(n, K);
+        for (int64_t t = K; t-- > 0;) ptr[L[t]] = t;
+        std::vector<double> csum(K);
+        double run = 0.0;
+        for (int64_t t = 0; t < K; t++) {
+            run += sr[t];
+            csum[t] = run;
+        }
+        std::vector<double> left(n, 0.0), laid(n, 0.0);
+        for (int64_t t = 0; t < K; t++) {
+            const int64_t p = ptr[L[t]];
+            const double before = (csum[t] - sr[t]) - (csum[p] - sr[p]);  // room in the lake's cells laid first
+            const double lay = clip(have[L[t]] - before, 0.0, sr[t]);
+            F.lay[sc[t]] = lay;
+            F.laid += lay;
+            left[L[t]] += sr[t] - lay;
+            laid[L[t]] += lay;
+        }
+        for (int64_t l = 0; l < n; l++) {
+            const double over = have[l] - laid[l];  // rounding only: the apply holds a lake to its room
+            if (over > 1e-9) {
+                F.pending[sc[ptr[l]]] += over;
+                F.stray += over;
+            }
+        }
+        // a lake with a frozen cell takes nothing; the others with room left are numbered in order
+        std::vector<uint8_t> warm(n, 1);
+        const float ice = (float)F.ice_evap;
+        for (const int64_t c : cells)
+            if (F.evap[c] <= ice) warm[lab[c]] = 0;
+        std::vector<int64_t> id(n, -1);
+        int64_t nid = 0;
+        for (int64_t l = 0; l < n; l++)
+            if (warm[l] && left[l] > 0.0) id[l] = nid++;
+        if (nid > F.lake_room_cap) return -1;
+        for (int64_t l = 0; l < n; l++)
+            if (id[l] >= 0) {
+                F.lake_room[id[l]] = left[l];
+                F.room += left[l];
+            }
+        for (const int64_t c : cells)
+            if (id[lab[c]] >= 0) {
+                takes[c] = 1;
+                lake_id[c] = (int32_t)id[lab[c]];
+            }
+        F.lakes = nid;
+    }
+    if (F.lakes == 0 && F.lake_room_cap > 0) F.lake_room[0] = 0.0;  // the reference's one-entry zero room
+    std::memset(load, 0, sizeof(double) * M);
+    return 0;
 }
 
 }  // namespace
@@ -326,7 +493,7 @@ LakeScratch &lake_scratch()
 int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
                       const float *surface, const uint8_t *ocean_in, const float *precip, const float *pet, double lake_evap,
                       double land_evap, double min_depth, uint8_t *lake_flag, float *water_out, float *closed_level,
-                      PgeLakeInfo *info)
+                      PgeLakeFill *fill, PgeLakeInfo *info)
 {
     Sphere S{N, H, N + 2 * H, owner};
     const int64_t M = (int64_t)6 * N * N;
@@ -478,15 +645,33 @@ int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, c
     }
     // overflowing lakes are flagged; a lake drawn below its rim is a closed sea at its level
     const float depth = (float)min_depth, rim = 1e-4f;
+    std::vector<uint8_t> &takes = X.takes;
+    std::vector<float> &surf_after = X.surf_after;
+    if (fill) {
+        // erosion.lake_fill: the overflowing lakes take the loads parked on them, then only what stays deeper
+        // than min_depth over the laid sediment is still a lake (maps.py:466-470)
+        std::vector<uint8_t> &olake = X.olake;
+        olake.assign(M, 0);
+        for (int64_t c = 0; c < M; c++) {
+            const bool lake = (float)(water[c] - surface[c]) > depth && !ocean_in[c];
+            olake[c] = lake && !(water[c] < (float)(filled[c] - rim));
+        }
+        if (settle_lake_loads(S, olake, water, surface, parent, order, pop_seq, *fill, takes) != 0) return -2;
+        surf_after.assign(surface, surface + M);
+        for (int64_t c = 0; c < M; c++)
+            if (fill->lay[c] != 0.0) surf_after[c] = (float)(fill->height[c] + (fill->sediment[c] + fill->lay[c]));
+    }
+    const float *surf2 = fill ? surf_after.data() : surface;
     int64_t nlake = 0, nclosed = 0;
 #pragma omp parallel for schedule(static) reduction(+ : nlake, nclosed)
     for (int64_t c = 0; c < M; c++) {
-        const bool lake = (float)(water[c] - surface[c]) > depth && !ocean_in[c];
+        bool lake = (float)(water[c] - surface[c]) > depth && !ocean_in[c];
         const bool closed = lake && water[c] < (float)(filled[c] - rim);
-        lake_flag[c] = lake && !closed ? 1 : 0;
-        if (closed_level) closed_level[c] = closed ? water[c] : NAN;
+        if (fill) lake = lake && (float)(water[c] - surf2[c]) > depth;
+        lake_flag[c] = lake && !closed ? (fill && takes[c] ? 2 : 1) : 0;
+        if (closed_level) closed_level[c] = closed && lake ? water[c] : NAN;
         nlake += lake;
-        nclosed += closed;
+        nclosed += closed && lake;
     }
     inf.lake_cells = nlake;
     inf.lake_cells_closed = nclosed;

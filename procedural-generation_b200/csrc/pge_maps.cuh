@@ -25,11 +25,12 @@ void brush_spread(const PgeGrid &g, const PgeState &s, const Layout &lay, void *
 // numpy's pairwise float64 sum (mean = 1: divided by the count) of a[0, *count), on the stream
 size_t pairwise_scratch_bytes();
 void pairwise_sum(const double *a, const long long *count, void *scratch, double *out, int mean, cudaStream_t st);
-// the planet's lake balance on the host (pge_lakes.cpp); 0, or -1 when a land cell has no flow direction
+// the planet's lake balance on the host (pge_lakes.cpp), with erosion.lake_fill's settle when fill is set; 0,
+// -1 when a land cell has no flow direction, -2 when more lakes take load than fill->lake_room_cap
 int lake_balance_host(int N, int H, const int32_t *owner, const float *metric, const float *cell_area, double cell_size_m,
                       const float *surface, const uint8_t *ocean, const float *precip, const float *pet, double lake_evap,
                       double land_evap, double min_depth, uint8_t *lake_flag, float *water, float *closed_level,
-                      PgeLakeInfo *info);
+                      PgeLakeFill *fill, PgeLakeInfo *info);
 // the evaporation balance of a window's lakes on the host (pge_lakes.cpp)
 void window_lake_balance_host(int W, const float *surface, const uint8_t *active, const float *precip, const float *evap,
                               double lake_evap, double min_depth, double *route, uint8_t *lake, int64_t *counts);

@@ -187,7 +187,8 @@ __global__ void ordered_rank_kernel(long long nslots, const unsigned long long *
         const bool fst = i == 0 || keys[i - 1] != k || vals[i - 1] / cap != s / cap;
         EntryDesc d;
         d.cell = (int32_t)k;
-        d.dflags = D | (lst ? ENTRY_LAST : 0u) | (fst ? ENTRY_FIRST : 0u) | (vol[s] >= 0.0f ? ENTRY_STEP : 0u);
+        d.dflags = D | (lst ? ENTRY_LAST : 0u) | (fst ? ENTRY_FIRST : 0u) | (vol[s] >= 0.0f ? ENTRY_STEP : 0u) |
+                   (vol[s] == -3.0f ? ENTRY_PARK : 0u);
         d.delta = delta[s];
         desc[s] = d;
     }
@@ -209,15 +210,86 @@ struct MaxOp {
     __device__ __forceinline__ int32_t operator()(const int32_t a, const int32_t b) const { return a > b ? a : b; }
 };
 
-size_t ordered_temp_bytes(long long nslots)
+size_t ordered_temp_bytes(long long nslots, long long max_wave)
 {
-    size_t a = 0, b = 0, c = 0;
+    size_t a = 0, b = 0, c = 0, d = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long *)nullptr, (unsigned long long *)nullptr, (int32_t *)nullptr,
                                     (int32_t *)nullptr, (int)nslots);
     cub::DeviceScan::InclusiveSum(nullptr, b, (int32_t *)nullptr, (int32_t *)nullptr, (int)nslots);
     cub::DeviceScan::InclusiveScan(nullptr, c, (int32_t *)nullptr, (int32_t *)nullptr, MaxOp{}, (int)nslots);
+    cub::DeviceRadixSort::SortPairs(nullptr, d, (uint32_t *)nullptr, (uint32_t *)nullptr, (int32_t *)nullptr, (int32_t *)nullptr,
+                                    (int)(max_wave * LAKE_PARKS));
     size_t m = a > b ? a : b;
-    return m > c ? m : c;
+    m = m > c ? m : c;
+    return m > d ? m : d;
+}
+
+// ---------------------------------------------------------------------------
+// lake parks: each lake's room counted down in droplet order (particle.py:912-933)
+// ---------------------------------------------------------------------------
+// one item per (droplet, park slot): key = the lake of the park's cell (all ones: no lake, or past the
+// droplet's parks); the items enter the stable sort in (droplet, park) order, which is the serial order
+__global__ void park_keys_kernel(long long nitems, int cap, const int32_t *cell, const double *delta, const int32_t *park_n,
+                                 const int32_t *park_k, const int32_t *lake_id, long long lakes, uint32_t *keys, int32_t *vals,
+                                 double *rest)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nitems; i += (long long)gridDim.x * blockDim.x) {
+        const long long q = i / LAKE_PARKS;
+        const int j = (int)(i - q * LAKE_PARKS);
+        uint32_t key = 0xffffffffu;
+        double r = 0.0;
+        if (j < park_n[q] && park_k[i] >= 0 && park_k[i] < cap) {  // (an entry past the list's room was not recorded)
+            const long long s = q * cap + park_k[i];
+            const int32_t lk = lake_id[cell[s]];
+            if (lk >= 0 && lk < lakes)
+                key = (uint32_t)lk;
+            else
+                r = delta[s];  // no lake to take it: all of it is refused
+        }
+        keys[i] = key;
+        vals[i] = (int32_t)i;
+        rest[i] = r;
+    }
+}
+
+// the first item of each lake walks its lake's parks in the serial order: the lake takes what it still has
+// room for, the rest is refused
+__global__ void park_walk_kernel(long long nitems, int cap, const uint32_t *keys, const int32_t *vals, const int32_t *cell,
+                                 const double *delta, const int32_t *park_k, double *lake_room, double *lake_load, double *rest)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nitems; i += (long long)gridDim.x * blockDim.x) {
+        const uint32_t key = keys[i];
+        if (key == 0xffffffffu || (i > 0 && keys[i - 1] == key)) continue;
+        double room = lake_room[key];
+        for (long long t = i; t < nitems && keys[t] == key; t++) {
+            const int32_t v = vals[t];  // a park with a lake (its entry index checked by park_keys_kernel)
+            const long long s = (long long)(v / LAKE_PARKS) * cap + park_k[v];
+            double take = delta[s], r = 0.0;
+            if (take > room) {
+                r = take - room;
+                take = room;
+            }
+            if (take > 0.0) {
+                lake_load[cell[s]] += take;
+                room -= take;
+            }
+            rest[v] = r;
+        }
+        lake_room[key] = room;
+    }
+}
+
+cudaError_t park_wave(const ParkWave &pw, cudaStream_t st)
+{
+    const long long n = pw.nw * LAKE_PARKS;
+    park_keys_kernel<<<grid_for(n), 256, 0, st>>>(n, pw.cap, pw.cell, pw.delta, pw.park_n, pw.park_k, pw.lake_id, pw.lakes, pw.keys_in,
+                                                  pw.vals_in, pw.rest);
+    size_t tb = pw.temp_bytes;
+    cudaError_t e = cub::DeviceRadixSort::SortPairs(pw.temp, tb, pw.keys_in, pw.keys_out, pw.vals_in, pw.vals_out, (int)n, 0, 32, st);
+    if (e != cudaSuccess) return e;
+    park_walk_kernel<<<grid_for(n), 256, 0, st>>>(n, pw.cap, pw.keys_out, pw.vals_out, pw.cell, pw.delta, pw.park_k, pw.lake_room,
+                                                  pw.lake_load, pw.rest);
+    return cudaPeekAtLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -378,16 +450,23 @@ __device__ __forceinline__ void droplet_end(const OrderedArgs &a, const Walk &w,
     long long topend = 0, lostoff = 0;
     int32_t dth = -1;
     double add = 0.0;
-    if (w.death >= 0 && w.surplus > 0.0) {
+    double surplus = w.surplus;
+    if (a.park_n) {  // the loads its lakes had no room for join what it could not place (particle.py:1019)
+        double refused = 0.0;
+        const int np = a.park_n[q];
+        for (int j = 0; j < np; j++) refused += a.park_rest[q * LAKE_PARKS + j];
+        surplus += refused;
+    }
+    if (w.death >= 0 && surplus > 0.0) {
         if (w.sub_death) {
-            double keep = w.surplus * (1.0 - p.offshore_writeoff);
+            double keep = surplus * (1.0 - p.offshore_writeoff);
             if (keep < 1e-4) keep = 0.0;
             add = keep;
             topend = fx_mass(keep);
-            lostoff = fx_mass(w.surplus) - topend;
+            lostoff = fx_mass(surplus) - topend;
         } else {
-            add = w.surplus;
-            topend = fx_mass(w.surplus);
+            add = surplus;
+            topend = fx_mass(surplus);
         }
         dth = w.death;
     }
@@ -467,12 +546,13 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
             const double dlt = cur.d.delta;
             const double hs = cur.t.hs;
             const double b_c = (double)cur.t.base;
-            const bool act = cur.t.active != 0;
+            const bool park = (df & ENTRY_PARK) != 0;  // a lake park changes no terrain (particle.py:912-933)
+            const bool act = cur.t.active != 0 && !park;
             if (!w.have_c && !(w.ok = cell_value(a, w, c, df, cur.h0, cur.h1, w.acc_c))) break;
             // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
             // acquire it now; a step deposit does not, and acquires it only before writing it
             const bool is_step = (df & ENTRY_STEP) != 0;
-            const bool reads_next = has_next && (dlt < 0.0 || !is_step);
+            const bool reads_next = has_next && !park && (dlt < 0.0 || !is_step);
             const int32_t ncell = has_next ? nx.d.cell : -1;
             double acc_n = 0.0, hs_n = 0.0;
             if (reads_next) {

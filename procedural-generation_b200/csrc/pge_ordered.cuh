@@ -14,6 +14,7 @@ constexpr uint32_t ENTRY_D_MASK = 0xffffffu;
 constexpr uint32_t ENTRY_LAST = 1u << 24;   // its droplet's last visit to the cell
 constexpr uint32_t ENTRY_FIRST = 1u << 25;  // its droplet's first visit to the cell
 constexpr uint32_t ENTRY_STEP = 1u << 26;   // a step entry (vol >= 0), not a final deposit
+constexpr uint32_t ENTRY_PARK = 1u << 27;   // a lake park (vol -3): its cell is visited and handed on unchanged
 
 // a cell's read-only terrain for the ordered apply (built once per pass)
 struct alignas(16) CellTerr {
@@ -57,6 +58,29 @@ struct OrderedArgs {
     PgeParams p;
     PgeStats *stats;
     int *error;
+    // lake parks (nullptr: off): per droplet its park count, per park (LAKE_PARKS a droplet) the rest its lake
+    // had no room for, added to the droplet's leftover load in list order
+    const int32_t *park_n;
+    const double *park_rest;
+};
+
+// the lake parks of one wave (erosion.lake_fill): each lake's room counted down in droplet order
+struct ParkWave {
+    long long nw;  // droplets of the wave
+    int cap;
+    const int32_t *cell;
+    const double *delta;
+    const int32_t *park_n, *park_k;  // per droplet its parks and their entry indices
+    const int32_t *lake_id;          // per cell
+    double *lake_room;               // per lake, counted down in place
+    long long lakes;
+    double *lake_load;               // per cell, the loads the lakes took
+    double *rest;                    // out: per park the rest refused
+    uint32_t *keys_in, *keys_out;
+    int32_t *vals_in, *vals_out;
+    int end_bit;
+    void *temp;
+    size_t temp_bytes;
 };
 
 struct OrderedWave {
@@ -71,7 +95,8 @@ struct OrderedWave {
     long long max_blocks;
 };
 
-size_t ordered_temp_bytes(long long nslots);
+size_t ordered_temp_bytes(long long nslots, long long max_wave);
+cudaError_t park_wave(const ParkWave &pw, cudaStream_t st);
 int ordered_blocks_per_sm(int lanes);  // resident blocks of the apply kernel per SM
 cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st);
 cudaError_t hand_reset(long long ncell, double2 *hand, cudaStream_t st);

@@ -27,7 +27,7 @@ EXPORTS = (
     "pge_collect_pending", "pge_trace_apply", "pge_trace_changelist", "pge_read_accumulators", "pge_thermal",
     "pge_uplift", "pge_hold_datum", "pge_halo_gather", "pge_thermal_noalloc", "pge_slope_erode_cap",
     "pge_smooth_step", "pge_trace_apply_tape", "pge_adjoint_pass", "pge_halo_adjoint", "pge_route_flood", "pge_sea_base", "pge_glacial",
-    "pge_window_lakes", "pge_lake_balance", "pge_basin_fill",
+    "pge_window_lakes", "pge_lake_balance", "pge_lake_balance_fill", "pge_basin_fill",
     "pge_window_lake_balance", "pge_cubesphere_map", "pge_crmath", "pge_crmath_host",
 )
 #: cells the workspace-free thermal entry point accepts (include/pgerosion.h)
@@ -48,7 +48,7 @@ class PgeGrid(ctypes.Structure):
 class PgeState(ctypes.Structure):
     _fields_ = [(n, c_vp) for n in ("height", "sediment", "discharge", "momentum", "pending", "base", "uplift",
                                     "hardness", "precip", "evap", "mask", "metric", "metric_inv", "erodibility", "route",
-                                    "lake_flag", "roots")]
+                                    "lake_flag", "roots", "lake_load", "lake_id", "lake_room")] + [("lakes", c_i64)]
 
 
 class PgeSpawns(ctypes.Structure):
@@ -88,6 +88,12 @@ TAPE_EXTRA_ENTRIES = 8
 
 class PgeLakeInfo(ctypes.Structure):
     _fields_ = [(n, c_i64) for n in ("lake_cells", "lake_cells_closed", "depressions", "overflowing", "closed", "dry")]
+
+
+class PgeLakeFill(ctypes.Structure):
+    _fields_ = ([(n, c_f64) for n in ("grade", "ice_evap", "rise")]
+                + [(n, c_vp) for n in ("evap", "centres", "height", "sediment", "lake_load", "lake_id", "lay", "pending", "lake_room")]
+                + [("lake_room_cap", c_i64), ("lakes", c_i64)] + [(n, c_f64) for n in ("parked", "laid", "stray", "room")])
 
 
 class PgeHalo(ctypes.Structure):
@@ -142,6 +148,8 @@ def load(path: str | os.PathLike | None = None):
     L.pge_basin_fill.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_f64, c_f64, c_vp, c_vp, P(c_i64)]
     L.pge_lake_balance.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_f64, c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_f64, c_vp, c_vp, c_vp,
                                    P(PgeLakeInfo)]
+    L.pge_lake_balance_fill.argtypes = [P(PgeGrid), c_vp, c_vp, c_vp, c_f64, c_vp, c_vp, c_vp, c_vp, c_f64, c_f64, c_f64, c_vp, c_vp,
+                                        c_vp, P(PgeLakeFill), P(PgeLakeInfo)]
     L.pge_glacial.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_f64, c_f64, c_i32, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp,
                               ctypes.c_size_t, c_vp]
     L.pge_sea_base.argtypes = [P(PgeGrid), P(PgeState), c_vp, c_vp, c_f64, c_vp, c_vp, c_i64, P(c_i64), c_vp, ctypes.c_size_t, c_vp]

@@ -99,6 +99,12 @@ class ErosionState:
     roots: torch.Tensor = field(default=None, repr=False)
     #: the potential evaporation the planet's lake balance runs on (float32, (F, NE, NE)) in place of evap, or None
     lake_pet: torch.Tensor = field(default=None, repr=False)
+    #: the lake parks (erosion.lake_fill, maps.py:105-107): float64 load per cell that droplets parked in a lake with
+    #: room since the last refresh, the int32 lake of lake_room each cell belongs to (-1 none), and float64 room per
+    #: lake; None until the first pass with parks
+    lake_load: torch.Tensor = field(default=None, repr=False)
+    lake_id: torch.Tensor = field(default=None, repr=False)
+    lake_room: torch.Tensor = field(default=None, repr=False)
     #: the open sea of the last sea-mask refresh (bool, (F, N, N)), the lake balance's drains; None before the first
     sea_mask: torch.Tensor = field(default=None, repr=False)
     #: iteration of the last sea-mask refresh (refresh_base), None before the first
@@ -109,6 +115,7 @@ class ErosionState:
     _sea: tuple = field(default=None, repr=False)
     _spawn: dict = field(default=None, repr=False)
     _lake_inputs: tuple = field(default=None, repr=False)
+    _centres: np.ndarray = field(default=None, repr=False)
 
     def __post_init__(self):
         dev = self.height.device
@@ -170,8 +177,12 @@ class ErosionState:
         return self.height + self.sediment
 
     def total_mass(self) -> float:
-        """Sum of height + sediment + pending over the active interior (cell units)."""
-        t = (self.height + self.sediment + self.pending)[self.interior]
+        """Sum of height + sediment + pending (+ lake_load, the loads parked in
+        lakes) over the active interior (cell units), as maps.py:323-326."""
+        t = self.height + self.sediment + self.pending
+        if self.lake_load is not None:
+            t = t + self.lake_load
+        t = t[self.interior]
         if self.mask is not None:
             t = t[self.mask[self.interior] == MASK_ACTIVE]
         return float(t.sum().item())
@@ -185,12 +196,29 @@ class ErosionState:
                        deposit_on_exit=int(bool(self.deposit_on_exit)), metric_shared=1, max_steps=int(self.max_steps),
                        wave_tables=int(self.wave_tables), max_droplets=int(self.max_droplets), max_wave=int(self.max_wave))
 
-    def pge_state(self) -> PgeState:
-        return PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
-                        momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
-                        hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
-                        metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility),
-                        route=_ptr(self.route), lake_flag=_ptr(self.lake_flag), roots=_ptr(self.roots))
+    def pge_state(self, parks: bool = False) -> PgeState:
+        """The C view of the state; with ``parks`` the lake parks' arrays
+        (:meth:`ensure_lake_parks` first), else none (parks off)."""
+        ps = PgeState(height=_ptr(self.height), sediment=_ptr(self.sediment), discharge=_ptr(self.discharge),
+                      momentum=_ptr(self.momentum), pending=_ptr(self.pending), base=_ptr(self.base), uplift=_ptr(self.uplift),
+                      hardness=_ptr(self.hardness), precip=_ptr(self.precip), evap=_ptr(self.evap), mask=_ptr(self.mask),
+                      metric=_ptr(self.metric), metric_inv=_ptr(self.metric_inv), erodibility=_ptr(self.erodibility),
+                      route=_ptr(self.route), lake_flag=_ptr(self.lake_flag), roots=_ptr(self.roots))
+        if parks:
+            ps.lake_load, ps.lake_id, ps.lake_room = _ptr(self.lake_load), _ptr(self.lake_id), _ptr(self.lake_room)
+            ps.lakes = int(self.lake_room.numel())
+        return ps
+
+    def ensure_lake_parks(self) -> None:
+        """The lake parks' arrays at their initial values (maps.py:128-133):
+        no load parked, no lake numbered, one zero room."""
+        dev = self.height.device
+        if self.lake_load is None:
+            self.lake_load = torch.zeros_like(self.height)
+        if self.lake_id is None:
+            self.lake_id = torch.full(self.height.shape, -1, dtype=torch.int32, device=dev)
+        if self.lake_room is None:
+            self.lake_room = torch.zeros(1, dtype=torch.float64, device=dev)
 
     def reserve(self, max_droplets: int, max_steps: int, max_wave: int = 1, wave_tables: bool = False) -> None:
         """Size the library workspace and spawn buffers for up to
@@ -386,17 +414,22 @@ class ErosionState:
         flat[dst] = flat[nearest]  # the halo is an exact copy of the cell it mirrors (a jump at a basin rim)
         return base, labels
 
-    def refresh_lakes(self, lake_evap: float, min_depth: float, min_fraction: float = 0.02, land_evap: float = 0.0) -> dict:
-        """The planet's lakes (maps.py:422-479, erosion.lake_balance with
-        erosion.lake_fill off): the hydro stage's flood, D8 routing and
-        evaporation balance on the eroding surface (``pge_lake_balance``, a
-        host pass: its every step follows the flood's serial pop order).
-        Overflowing lakes deeper than ``min_depth`` (cell units) are flagged
-        (``lake_flag``); a lake drawn below its rim is a closed sea, its level
-        written into ``base``.  The drains are the sea of the last
-        :meth:`refresh_base`, else the open ocean of the current surface;
-        the balance runs on ``lake_pet`` when set, else ``evap``.  Must run
-        after :meth:`refresh_base` and :meth:`refresh_route`."""
+    def refresh_lakes(self, lake_evap: float, min_depth: float, min_fraction: float = 0.02, land_evap: float = 0.0,
+                      fill: tuple | None = None) -> dict:
+        """The planet's lakes (maps.py:422-479, erosion.lake_balance): the
+        hydro stage's flood, D8 routing and evaporation balance on the
+        eroding surface (``pge_lake_balance``, a host pass: its every step
+        follows the flood's serial pop order).  Overflowing lakes deeper than
+        ``min_depth`` (cell units) are flagged (``lake_flag``); a lake drawn
+        below its rim is a closed sea, its level written into ``base``.  The
+        drains are the sea of the last :meth:`refresh_base`, else the open
+        ocean of the current surface; the balance runs on ``lake_pet`` when
+        set, else ``evap``.  Must run after :meth:`refresh_base` and
+        :meth:`refresh_route`.  With ``fill`` (:func:`lake_fill_args`,
+        erosion.lake_fill) the lakes first take the loads parked on them
+        (``pge_lake_balance_fill``, maps.py:490-628): laid over their floors
+        as sediment (and isostatic load), the lakes with room numbered in
+        ``lake_id`` / ``lake_room`` and flagged 2."""
         if not self.spherical:
             raise ValueError("refresh_lakes is the planet's lake balance; a window's lakes come from refresh_lakes_window")
         inter = self.interior
@@ -420,12 +453,49 @@ class ErosionState:
         flag = np.empty((F, N, N), np.uint8)
         level = np.empty((F, N, N), np.float32)
         info = _lib.PgeLakeInfo()
-        check(_lib.load().pge_lake_balance(ctypes.byref(self.pge_grid()), owner.ctypes.data, metric.ctypes.data, area_h.ctypes.data,
-                                           float(self.grid.cell_size_m), surf.ctypes.data, ocean.ctypes.data,
-                                           precip.ctypes.data, pet_h.ctypes.data,
-                                           float(lake_evap), float(land_evap), float(min_depth), flag.ctypes.data, None,
-                                           level.ctypes.data, ctypes.byref(info)), "pge_lake_balance")
         dev = self.height.device
+        settled = {}
+        if fill is None:
+            check(_lib.load().pge_lake_balance(ctypes.byref(self.pge_grid()), owner.ctypes.data, metric.ctypes.data,
+                                               area_h.ctypes.data, float(self.grid.cell_size_m), surf.ctypes.data,
+                                               ocean.ctypes.data, precip.ctypes.data, pet_h.ctypes.data, float(lake_evap),
+                                               float(land_evap), float(min_depth), flag.ctypes.data, None, level.ctypes.data,
+                                               ctypes.byref(info)), "pge_lake_balance")
+        else:
+            grade, ice_evap, rise, load_share = (float(v) for v in fill)
+            self.ensure_lake_parks()
+            evap_h = host(self.evap[inter])
+            height_h, sed_h = host(self.height[inter]), host(self.sediment[inter])
+            load_h, id_h = host(self.lake_load[inter]), host(self.lake_id[inter])
+            H = self.H
+            if self._centres is None:
+                self._centres = np.ascontiguousarray(self.grid.centers()[:, H:H + N, H:H + N], dtype=np.float64)
+            lay = np.zeros((F, N, N))
+            pend_add = np.zeros((F, N, N))
+            room = np.zeros(F * N * N)  # at most one lake a cell
+            fl = _lib.PgeLakeFill(grade=grade, ice_evap=ice_evap, rise=rise, evap=evap_h.ctypes.data,
+                                  centres=self._centres.ctypes.data, height=height_h.ctypes.data, sediment=sed_h.ctypes.data,
+                                  lake_load=load_h.ctypes.data, lake_id=id_h.ctypes.data, lay=lay.ctypes.data,
+                                  pending=pend_add.ctypes.data, lake_room=room.ctypes.data, lake_room_cap=room.size)
+            check(_lib.load().pge_lake_balance_fill(ctypes.byref(self.pge_grid()), owner.ctypes.data, metric.ctypes.data,
+                                                    area_h.ctypes.data, float(self.grid.cell_size_m), surf.ctypes.data,
+                                                    ocean.ctypes.data, precip.ctypes.data, pet_h.ctypes.data, float(lake_evap),
+                                                    float(land_evap), float(min_depth), flag.ctypes.data, None,
+                                                    level.ctypes.data, ctypes.byref(fl), ctypes.byref(info)),
+                  "pge_lake_balance_fill")
+            lay_d = torch.as_tensor(lay, device=dev)
+            sed_i = self.sediment[inter]  # views: the laid sediment and stockpiles land in the state itself
+            sed_i += lay_d
+            if self.iso_acc is not None:
+                iso_i = self.iso_acc[inter]
+                iso_i += load_share * lay_d
+            pend_i = self.pending[inter]
+            pend_i += torch.as_tensor(pend_add, device=dev)
+            self.lake_load.zero_()
+            self.lake_id.fill_(-1)
+            self.lake_id[inter] = torch.as_tensor(id_h, device=dev)
+            self.lake_room = torch.as_tensor(room[:max(int(fl.lakes), 1)].copy(), device=dev)
+            settled = {"parked": fl.parked, "laid": fl.laid, "stray": fl.stray, "room": fl.room, "lakes": int(fl.lakes)}
         lf = torch.zeros(self.height.shape, dtype=torch.uint8, device=dev)
         lf[inter] = torch.as_tensor(flag, device=dev)
         closed = ~np.isnan(level)
@@ -439,7 +509,7 @@ class ErosionState:
         self.lake_flag = lf
         return {"lake_cells": int(info.lake_cells), "lake_cells_closed": int(info.lake_cells_closed),
                 "depressions": int(info.depressions), "overflowing": int(info.overflowing), "closed": int(info.closed),
-                "dry": int(info.dry)}
+                "dry": int(info.dry), **{f"load_{k}": v for k, v in settled.items()}}
 
     def n_active_interior(self) -> int:
         if self.mask is None:
@@ -590,9 +660,11 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
                   particles_per_cell: float | None = None, rng_stage: str = "erosion", log=None, wave: int | None = None,
                   precision: int = _lib.PREC_F64, predrawn=None, threads_per_block: int = 0, blocks_per_sm: int = 0,
                   events=None, apply: int = _lib.APPLY_ORDERED, trace_lanes: int = 0, apply_lanes: int = 0,
-                  tape=None) -> dict:
+                  tape=None, parks: bool | None = None) -> dict:
     """One particle pass (maps.py:839-1047) on the device; see the module
-    docstring.  ``predrawn`` may carry ``draw_spawns``' result for this
+    docstring.  ``parks``: the lake parks (erosion.lake_fill; default: on
+    where :func:`lake_fill_args` is, as the reference's pass has them,
+    maps.py:996).  ``predrawn`` may carry ``draw_spawns``' result for this
     iteration (drawn ahead, host or device arrays); ``events`` a pair of
     CUDA events recorded around the droplet pass (``pge_trace_apply``).
     ``tape``: a callable ``(n_droplets, max_steps, waves, cells) -> PgeTape``
@@ -615,7 +687,12 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     rng, u, off = predrawn if predrawn is not None else draw_spawns(params, rng_stage, key, P)
     L = _lib.load()
     g = state.pge_grid()
-    s = state.pge_state()
+    if parks is None:  # no lakes yet (no route or flags): nothing can be parked
+        parks = lake_fill_args(state, params) is not None and state.route is not None and state.lake_flag is not None
+    if parks:
+        state.ensure_lake_parks()
+        parked0 = state.lake_load.sum()
+    s = state.pge_state(parks)
     sp = state._spawn
     ws = state.workspace
     st = _stream()
@@ -706,6 +783,8 @@ def run_iteration(state: ErosionState, params, iteration_key, n_particles: int |
     stats["chunk"] = int(w)
     stats["apply"] = "ordered" if apply == _lib.APPLY_ORDERED else "wave"
     stats["n_pending"] = int(n_pend)
+    if parks:  # the loads the lakes took this pass (the rest of a park went on with its droplet)
+        stats["parked"] = float(state.lake_load.sum() - parked0)
     stats["disc_saturation"] = disc_sat
     stats["mom_scale"] = mom_scale
     if log is not None:
@@ -875,6 +954,37 @@ def start_replay(state: ErosionState, params) -> dict | None:
     return info
 
 
+def lake_fill_args(state: ErosionState, params):
+    """refresh_lakes' ``fill`` (maps.py:1248-1258): (the lake plain's grade in
+    cell units per cell, ice_evap, the plain's rise above the water in cell
+    units, the share of the fill that is isostatic load) with
+    erosion.lake_fill and lake_balance on the planet, else None."""
+    ep = erosion_group(params)
+    if not (state.spherical and bool(getattr(ep, "lake_fill", False)) and bool(getattr(ep, "lake_balance", False))):
+        return None
+    cell_km = float(state.grid.cell_size_m) / 1000.0
+    return (float(getattr(ep, "basin_fill_grade", 0.0)) * cell_km / state.height_unit_m, float(getattr(ep, "ice_evap", 0.0)),
+            float(getattr(ep, "lake_fill_rise_m", 1.0)) / state.height_unit_m, float(getattr(ep, "lake_fill_load", 0.55)))
+
+
+def settle_lakes(state: ErosionState, params) -> dict | None:
+    """The lakes lay what the last iterations parked on them (maps.py:1261-1275,
+    a run ends between two refreshes): the sea mask and the route refreshed,
+    one lake refresh with the fill, halos exchanged.  None without lake_fill."""
+    fill = lake_fill_args(state, params)
+    if fill is None or not hasattr(params, "world"):
+        return None
+    ep = erosion_group(params)
+    if int(getattr(ep, "sea_mask_every", 0)) > 0:
+        state.refresh_base(ocean_min_fraction(params))
+    state.refresh_route(cell_units(ep, "route_eps", state.height_unit_m))
+    hydro = getattr(params, "hydro", None)
+    st = state.refresh_lakes(float(getattr(hydro, "lake_evap", 6.0)), lake_min_depth(params) / state.height_unit_m,
+                             ocean_min_fraction(params), float(getattr(hydro, "land_evap", 3.0)), fill=fill)
+    state.exchange_halos()
+    return st
+
+
 def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
     """One plain iteration (maps.py:1516-1617): particles, thermal erosion,
     uplift, isostasy (when ``erosion.isostasy > 0``: the surface change of
@@ -898,7 +1008,8 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
         # the planet's lakes, after the base (rebuilt from scratch) and the route (maps.py:1555-1562)
         hydro = getattr(params, "hydro", None)
         st_lake = state.refresh_lakes(float(getattr(hydro, "lake_evap", 6.0)), lake_min_depth(params) / state.height_unit_m,
-                                      ocean_min_fraction(params), float(getattr(hydro, "land_evap", 3.0)))
+                                      ocean_min_fraction(params), float(getattr(hydro, "land_evap", 3.0)),
+                                      fill=lake_fill_args(state, params))
     elif not state.spherical and bool(getattr(ep, "window_lakes", False)) and flood > 0 and \
             (state.lake_flag is None or state.iteration % flood == 0):
         # a window's lakes, after the route they are read off (maps.py:1563-1566)
@@ -945,11 +1056,13 @@ def step(state: ErosionState, params, iteration_key, log=None, **kw) -> dict:
 
 
 def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0: float, conc_scale: float,
-                     precision: int = _lib.PREC_F64, wave: int | None = None) -> dict:
+                     precision: int = _lib.PREC_F64, wave: int | None = None, parks: bool = False) -> dict:
     """Parity hook: trace and apply the given droplets in one wave (or waves
     of ``wave``) on the current state, recording each droplet's change list
     in the reference layout (particle.py:275-818) and returning it with the
-    pass's accumulators.  The state's terrain is left unchanged."""
+    pass's accumulators.  The state's terrain is left unchanged.  With
+    ``parks`` (the lake parks, on the state's lake_id / lake_room) the lists
+    are recorded only: the accumulators stay zero."""
     ep = erosion_group(params)
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
@@ -970,7 +1083,9 @@ def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, s
     stats_d = torch.zeros(_lib.STATS_WORDS, dtype=torch.int64, device=dev)
     ws = state.workspace
     st = _stream()
-    g, s = state.pge_grid(), state.pge_state()
+    if parks:
+        state.ensure_lake_parks()
+    g, s = state.pge_grid(), state.pge_state(parks)
     check(L.pge_trace_changelist(ctypes.byref(g), ctypes.byref(s), ctypes.byref(spawns), ctypes.byref(prm), _ptr(out["cl_cell"]),
                                  _ptr(out["cl_delta"]), _ptr(out["cl_vol"]), _ptr(out["cl_mom"]), _ptr(out["cl_count"]),
                                  _ptr(out["sp_death"]), _ptr(stats_d), _ptr(ws), ws.numel(), st), "pge_trace_changelist")
@@ -993,11 +1108,14 @@ def trace_changelist(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, s
 
 
 def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_dir, volume0: float, n_rain: int | None = None,
-                 wave: int | None = None, precision: int = _lib.PREC_F64, apply: int = _lib.APPLY_ORDERED, tape=None) -> dict:
+                 wave: int | None = None, precision: int = _lib.PREC_F64, apply: int = _lib.APPLY_ORDERED, tape=None,
+                 parks: bool = False, conc_scale: float | None = None) -> dict:
     """One droplet pass over explicitly given spawns (no random draws): pack,
     waves, apply, fold and EMA, exactly as :func:`run_iteration` does after
     spawning.  ``n_rain`` is the rain count the concurrency divisor is
-    computed with (the reference divides by the whole spawn count)."""
+    computed with (the reference divides by the whole spawn count).
+    ``parks``: the lake parks on the state's lake_id / lake_room;
+    ``conc_scale``: the concurrency divisor's scale in place of the wave's."""
     ep = erosion_group(params)
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
@@ -1015,11 +1133,16 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     if float(ep.slope_limit_deposit) > 0.0:
         iter_deposit = min(iter_deposit, float(ep.slope_limit_deposit) * math.sqrt(2.0) * 0.3)
     prm = make_params(state, ep, volume0, P, w, precision, iter_deposit=iter_deposit, apply=apply)
+    if conc_scale is not None:
+        prm.conc_scale = float(conc_scale)
     ecap = _erode_cap(state, ep, prm)
     stats_d = sp["stats"]
     stats_d.zero_()
     ws = state.workspace
     out = {}
+    if parks:
+        state.ensure_lake_parks()
+    pst = state.pge_state(parks)
     if tape is not None:  # the pass recorded for the adjoint (float64 wave apply; see run_iteration)
         tp = tape(P, max_steps, -(-P // w), state.height.numel())
         check(L.pge_trace_apply_tape(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns),
@@ -1027,7 +1150,7 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
               "pge_trace_apply_tape")
         out["adjoint"] = {"spawns": PgeSpawns.from_buffer_copy(spawns), "params": PgeParams.from_buffer_copy(prm), "tape": tp}
     else:
-        check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(state.pge_state()), ctypes.byref(spawns),
+        check(L.pge_trace_apply(ctypes.byref(state.pge_grid()), ctypes.byref(pst), ctypes.byref(spawns),
                                 ctypes.byref(prm), ecap, _ptr(stats_d), _ptr(ws), ws.numel(), _stream()), "pge_trace_apply")
     r = PgeStats.from_buffer_copy(stats_d.cpu().numpy().tobytes())
     if r.errors:

@@ -212,16 +212,14 @@ def plain_knobs() -> dict:
 
 def check_plain(ep) -> None:
     """Raise ``ValueError`` when a knob asks for a process this library does
-    not run: the lake parks of ``lake_fill`` and the ice sheet.  The bank
-    cut (``lateral_rate``), the basin fill, isostasy, the routing surface
-    (``flood_every``), the sea mask (``sea_mask_every``), the glacial pass
-    (``glacial_every``, the ice line of the evaporation field), the planet's
-    lake balance (``lake_balance`` with ``lake_fill`` off) and the lakes of
-    a window (``window_lakes``, balanced with ``window_lake_evap > 0``) are
-    supported."""
+    not run: the ice sheet.  The bank cut (``lateral_rate``), the basin
+    fill, isostasy, the routing surface (``flood_every``), the sea mask
+    (``sea_mask_every``), the glacial pass (``glacial_every``, the ice line
+    of the evaporation field), the planet's lake balance (``lake_balance``)
+    with the lake parks (``lake_fill``, the exact apply only) and the lakes
+    of a window (``window_lakes``, balanced with ``window_lake_evap > 0``)
+    are supported."""
     bad = []
-    if bool(getattr(ep, "lake_balance", False)) and bool(getattr(ep, "lake_fill", False)):
-        bad.append("lake_fill")
     if bool(getattr(ep, "ice_sheet", False)):
         bad.append("ice_sheet")
     if bad:

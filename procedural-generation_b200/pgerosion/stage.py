@@ -147,18 +147,22 @@ def _state_fields(state) -> list:
         out.append("ice_prev")
     if state.lake_flag is not None:
         out.append("lake_flag")
+    if state.lake_load is not None:  # the lake parks' bookkeeping (run.py:107, 127-128)
+        out += ["lake_load", "lake_id", "lake_room"]
     return out
 
 
 def _lake_arrays(arrays: dict) -> None:
-    """The lake arrays the reference's checkpoints always hold (run.py:125-128;
+    """The lake arrays the reference's checkpoints always hold (run.py:104-128;
     its state has lake flags from the first pack on): the flags (zeros when
-    the state has none), and the parked-load bookkeeping this library keeps
-    at its initial values (lake_id -1, lake_room 0: no loads are parked)."""
+    the state has none) and the parked-load bookkeeping, at its initial
+    values (nothing parked, lake_id -1, one zero room) when the run has no
+    parks."""
     if "lake_flag" not in arrays:
         arrays["lake_flag"] = np.zeros(arrays["height"].shape, np.uint8)
-    arrays["lake_id"] = np.full(arrays["height"].shape, -1, np.int32)
-    arrays["lake_room"] = np.zeros(1, np.float64)
+    if "lake_id" not in arrays:
+        arrays["lake_id"] = np.full(arrays["height"].shape, -1, np.int32)
+        arrays["lake_room"] = np.zeros(1, np.float64)
 
 
 def _write_checkpoint(d: Path, it: int, arrays: dict, meta: dict) -> Path:
@@ -326,6 +330,11 @@ def load_checkpoint(state: gm.ErosionState, path: Path, meta: dict) -> None:
             state.base_at = None
         state.ice_prev = torch.as_tensor(np.asarray(z["ice_prev"], np.uint8), device=dev) if "ice_prev" in z.files else None
         state.lake_flag = torch.as_tensor(np.asarray(z["lake_flag"], np.uint8), device=dev) if "lake_flag" in z.files else None
+        if "lake_id" in z.files:  # the loads parked since the last refresh, the lakes' numbers and rooms (run.py:202, 222-224)
+            state.lake_load = torch.as_tensor(np.asarray(z["lake_load"], np.float64), device=dev) if "lake_load" in z.files \
+                else torch.zeros_like(state.height)
+            state.lake_id = torch.as_tensor(np.asarray(z["lake_id"], np.int32), device=dev)
+            state.lake_room = torch.as_tensor(np.asarray(z["lake_room"], np.float64), device=dev)
     state.iteration = int(meta["iteration"])
 
 
@@ -438,6 +447,12 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
                 log(f"[erosion] checkpoint -> {p.name}")
     if writer is not None:
         writer.close()
+    # the lakes lay what the last iterations brought them: a run ends between two lake refreshes (run.py:476-483)
+    lakes_end = gm.settle_lakes(state, params)
+    if lakes_end is not None:
+        log(f"[erosion] lakes at the end: {lakes_end['lake_cells']} cells, "
+            f"{lakes_end.get('load_laid', 0.0) * state.height_unit_m:,.0f} m-cells laid of "
+            f"{lakes_end.get('load_parked', 0.0) * state.height_unit_m:,.0f} their rivers left")
     # the active volcanic edifices go back on top of what the stage made of the ground under them (run.py:495-499)
     volc = restore_volcanoes(state, active_volcanoes(store, state.grid))
     if volc:
@@ -458,5 +473,7 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
         info["replay_datum_start_m"] = rep["datum_shift"] * u
     if fill is not None:
         info["basin_fill"] = fill
+    if lakes_end is not None:
+        info["lakes_end"] = lakes_end
     info.update(volc)
     return info

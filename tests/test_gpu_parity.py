@@ -120,7 +120,7 @@ def test_map_passes_match_oracle(cuda):
 
 def _mass_balance(stats, m0, m1):
     eroded = stats["eroded"]
-    exported = stats["to_pending"] - stats["released"] + stats["lost_offshore"] + stats["deficit_out"]
+    exported = stats["to_pending"] - stats["released"] + stats["lost_offshore"] + stats["deficit_out"] + stats.get("parked", 0.0)
     assert abs(eroded - (stats["deposited"] + exported)) <= 1e-6 * max(eroded, 1e-12), stats
     assert abs((m1 - m0) + stats["lost_offshore"] + stats["deficit_out"]) <= 1e-6 * max(eroded, 1e-12), (m0, m1, stats)
 

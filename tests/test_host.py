@@ -27,7 +27,9 @@ def test_chunk_and_steps():
 def test_plain_path_guard():
     pp.check_plain(pp.ErosionParams(**pp.plain_knobs()))
     with pytest.raises(ValueError):
-        pp.check_plain(pp.ErosionParams())
+        pp.check_plain(pp.ErosionParams())  # the ice sheet
+    # the bake's lakes with their parks run (the exact apply)
+    pp.check_plain(pp.ErosionParams(**{**pp.plain_knobs(), "lake_balance": True, "lake_fill": True, "flood_every": 10}))
 
 
 def test_small_world_inputs():

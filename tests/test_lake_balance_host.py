@@ -257,3 +257,99 @@ def test_basin_fill_equals_the_oracle_on_noise_worlds(seed):
     assert np.array_equal(basin.reshape(-1).astype(bool), want_basin) and want_basin.any()
     assert add.reshape(-1).tobytes() == want.tobytes()
     assert int(nb.value) == int(want_basin.sum())
+
+
+def test_lake_fill_refresh_equals_the_oracle(monkeypatch):
+    """``pge_lake_balance_fill`` (the lake refresh with erosion.lake_fill:
+    the parked loads laid over the lake floors, the lakes numbered and given
+    their room, maps.py:422-479, 490-628) against the oracle's refresh, which
+    reproduces the reference's steps on tests/golden/lake_fill_steps.npz bit
+    for bit: at every refresh of those steps, on the same state, the flags,
+    the sediment laid, the stockpiles, the lake numbers and rooms, the
+    isostatic load and the closed lakes' levels are identical."""
+    import json as _json
+
+    from oracle import oracle as orc
+    from pgerosion.params import WorldGroup, WorldParams
+    from pgerosion.synth import World
+    from tests.parity_cases import erosion_params
+
+    fx = np.load(GOLDEN / "lake_fill_steps.npz")
+    N, H, cs = int(fx["N"]), int(fx["H"]), float(fx["cell_size_m"])
+    params = WorldParams(world=WorldGroup(seed=int(fx["seed"]), N_c=N, cell_size_m=cs, land_fraction=float(fx["land_fraction"]),
+                                          halo=H), erosion=erosion_params(str(fx["params"])))
+    grid = get_grid(N, H, cs)
+    world = World(grid, fx["bedrock"], fx["hardness"], fx["precip"], fx["evap"], fx["uplift"], float(fx["land_fraction"]))
+    st = orc.OracleState.from_world(world, params)
+    orc.start_replay(st, params)
+    inter = (slice(None), slice(H, H + N), slice(H, H + N))
+    sq = sqrt_det_metric(grid)[H:H + N, H:H + N]
+    area = np.ascontiguousarray(np.broadcast_to((sq.astype(np.float64) * cs ** 2).astype(np.float32), (6, N, N)))
+    owner = np.ascontiguousarray(grid.owner, np.int32)
+    metric = np.ascontiguousarray(grid.metric_face, np.float32)
+    centres = np.ascontiguousarray(grid.centers()[:, H:H + N, H:H + N], np.float64)
+    g = _lib.PgeGrid(F=6, N=N, H=H, spherical=1, metric_shared=1, max_steps=1, max_droplets=1, max_wave=1)
+    original = orc.refresh_lakes
+    seen = []
+
+    def checked(state, lake_evap, min_depth, min_fraction, land_evap=0.0, fill=None):
+        if fill is None:
+            return original(state, lake_evap, min_depth, min_fraction, land_evap, fill)
+        c = lambda a, t: np.ascontiguousarray(np.asarray(a)[inter], dtype=t)
+        surf = c(state.height + state.sediment, np.float32)
+        sea = getattr(state, "sea", None)
+        if sea is None:
+            below, labels, keep = orc.below_sea_components(surf, grid, float(min_fraction))
+            sea = np.zeros(surf.shape, bool) if labels is None else (below & keep[np.maximum(labels, 0)]).reshape(surf.shape)
+        ocean = np.ascontiguousarray(np.asarray(sea, bool).reshape(surf.shape), np.uint8)
+        pet = getattr(state, "lake_pet", None)
+        pet = c(state.evap if pet is None else pet, np.float32)
+        if state.lake_load is None:
+            load, ids = np.zeros((6, N, N)), np.full((6, N, N), -1, np.int32)
+        else:
+            load, ids = c(state.lake_load, np.float64), c(state.lake_id, np.int32)
+        sed0, pend0 = c(state.sediment, np.float64), c(state.pending, np.float64)
+        iso0 = None if getattr(state, "iso_acc", None) is None else c(state.iso_acc, np.float64)
+        lay, padd, room = np.zeros((6, N, N)), np.zeros((6, N, N)), np.zeros(6 * N * N)
+        flag = np.empty((6, N, N), np.uint8)
+        water = np.empty((6, N, N), np.float32)
+        level = np.empty((6, N, N), np.float32)
+        evap = c(state.evap, np.float32)
+        height = c(state.height, np.float64)
+        precip = c(state.precip, np.float32)  # every array handed over is held by a name until the call returns
+        fl = _lib.PgeLakeFill(grade=fill[0], ice_evap=fill[1], rise=fill[2], evap=evap.ctypes.data, centres=centres.ctypes.data,
+                              height=height.ctypes.data, sediment=sed0.ctypes.data, lake_load=load.ctypes.data,
+                              lake_id=ids.ctypes.data, lay=lay.ctypes.data, pending=padd.ctypes.data, lake_room=room.ctypes.data,
+                              lake_room_cap=room.size)
+        info = _lib.PgeLakeInfo()
+        _lib.check(_lib.load().pge_lake_balance_fill(ctypes.byref(g), owner.ctypes.data, metric.ctypes.data, area.ctypes.data, cs,
+                                                     surf.ctypes.data, ocean.ctypes.data, precip.ctypes.data,
+                                                     pet.ctypes.data, float(lake_evap), float(land_evap), float(min_depth),
+                                                     flag.ctypes.data, water.ctypes.data, level.ctypes.data, ctypes.byref(fl),
+                                                     ctypes.byref(info)), "pge_lake_balance_fill")
+        base0 = c(state.base, np.float64)
+        out = original(state, lake_evap, min_depth, min_fraction, land_evap, fill)
+        assert np.array_equal(flag, np.asarray(state.lake_flag)[inter])
+        assert (sed0 + lay).tobytes() == c(state.sediment, np.float64).tobytes()
+        assert (pend0 + padd).tobytes() == c(state.pending, np.float64).tobytes()
+        assert np.array_equal(ids, c(state.lake_id, np.int32))
+        assert room[:max(int(fl.lakes), 1)].tobytes() == np.ascontiguousarray(state.lake_room, np.float64).tobytes()
+        if iso0 is not None:
+            assert (iso0 + fill[3] * lay).tobytes() == c(state.iso_acc, np.float64).tobytes()
+        closed = ~np.isnan(level)
+        base0[closed] = level[closed]
+        assert base0.tobytes() == c(state.base, np.float64).tobytes()
+        assert int(info.lake_cells) == out["lake_cells"] and int(info.lake_cells_closed) == out["lake_cells_closed"]
+        assert int(fl.lakes) == out["load_lakes"]
+        for k in ("parked", "laid", "stray", "room"):
+            assert abs(getattr(fl, k) - out[f"load_{k}"]) <= 1e-12 * max(abs(out[f"load_{k}"]), 1.0), k
+        seen.append((int(fl.lakes), float(fl.parked), float(fl.laid)))
+        return out
+
+    monkeypatch.setattr(orc, "refresh_lakes", checked)
+    for it in range(int(fx["iterations"])):
+        orc.step(st, params, it, n_particles=int(fx["n_particles"]))
+    print("refreshes (lakes taking load, parked, laid):", seen)
+    assert len(seen) >= 3 and any(p > 0.0 for _, p, _ in seen) and any(n > 0 for n, _, _ in seen)
+    for k in ("height", "sediment", "lake_load", "lake_id", "lake_room"):
+        assert np.array_equal(getattr(st, k), fx[k]), k
