@@ -296,7 +296,17 @@ cudaError_t park_wave(const ParkWave &pw, cudaStream_t st)
 // the ordered apply
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int RING = 8;  // entry slots per droplet: entries k .. k+5 are in flight
+// prefetch depth: at entry k the copies of the last LOOKAHEAD entries may still be in flight; the cell data of
+// entry k + CELL_AHEAD and the descriptor of entry k + DESC_AHEAD are issued (the descriptor lands before its
+// cell data is issued, the cell data before its entry and the one before it are applied)
+#ifndef PGE_APPLY_LOOKAHEAD
+#define PGE_APPLY_LOOKAHEAD 1
+#endif
+constexpr int LOOKAHEAD = PGE_APPLY_LOOKAHEAD;
+constexpr int CELL_AHEAD = LOOKAHEAD + 2;
+constexpr int DESC_AHEAD = CELL_AHEAD + LOOKAHEAD + 1;
+constexpr int RING = DESC_AHEAD < 8 ? 8 : (DESC_AHEAD < 16 ? 16 : 32);  // entry slots per droplet (a power of two)
+static_assert(RING > DESC_AHEAD, "the ring holds every entry in flight");
 // two droplets per block: a block's warp slots free up as soon as its two droplets are done, so
 // concurrent passes (other worlds' waves on other streams) pack around the long-lived droplets
 constexpr int APPLY_THREADS = 64;
@@ -516,11 +526,11 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
             continue;
         }
         const long long b0 = q * a.cap;
-        // prologue: descriptors of entries 0..4, then the cell data of entries 0..2
-        for (int j = 0; j < 5 && j < K; j++) stage_desc(a, R[j], b0 + j);
+        // prologue: the descriptors of the first DESC_AHEAD entries, then the cell data of the first CELL_AHEAD
+        for (int j = 0; j < DESC_AHEAD && j < K; j++) stage_desc(a, R[j], b0 + j);
         cp_commit();
         cp_wait<0>();
-        for (int j = 0; j < 3 && j < K; j++) stage_cell<ECAP, LAKE>(a, R[j]);
+        for (int j = 0; j < CELL_AHEAD && j < K; j++) stage_cell<ECAP, LAKE>(a, R[j]);
         cp_commit();
         cp_wait<0>();
         Walk w;
@@ -532,11 +542,11 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
         w.sub_death = w.has_prev = w.have_c = false;
         w.ok = true;
         for (int k = 0; k < K; k++) {
-            // the copies issued two or more entries ago have landed: the descriptor of entry k+3
-            // and the cell data of entries k and k+1
-            cp_wait<1>();
-            if (k + 3 < K) stage_cell<ECAP, LAKE>(a, R[(k + 3) & (RING - 1)]);
-            if (k + 5 < K) stage_desc(a, R[(k + 5) & (RING - 1)], b0 + k + 5);
+            // the copies issued LOOKAHEAD + 1 or more entries ago have landed: the descriptor of entry
+            // k + CELL_AHEAD and the cell data of entries k and k + 1
+            cp_wait<LOOKAHEAD>();
+            if (k + CELL_AHEAD < K) stage_cell<ECAP, LAKE>(a, R[(k + CELL_AHEAD) & (RING - 1)]);
+            if (k + DESC_AHEAD < K) stage_desc(a, R[(k + DESC_AHEAD) & (RING - 1)], b0 + k + DESC_AHEAD);
             cp_commit();
             const Slot &cur = R[k & (RING - 1)];
             const Slot &nx = R[(k + 1) & (RING - 1)];
