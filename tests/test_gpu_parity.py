@@ -120,9 +120,11 @@ def test_map_passes_match_oracle(cuda):
 
 def _mass_balance(stats, m0, m1):
     eroded = stats["eroded"]
-    exported = stats["to_pending"] - stats["released"] + stats["lost_offshore"] + stats["deficit_out"] + stats.get("parked", 0.0)
+    # a deficit left at a list's end is erosion a droplet carried but the terrain could not give: mass the pass
+    # creates (particle.py:964-966, 1043); what the lakes took (erosion.lake_fill) left with the droplets
+    exported = stats["to_pending"] - stats["released"] + stats["lost_offshore"] - stats["deficit_out"] + stats.get("parked", 0.0)
     assert abs(eroded - (stats["deposited"] + exported)) <= 1e-6 * max(eroded, 1e-12), stats
-    assert abs((m1 - m0) + stats["lost_offshore"] + stats["deficit_out"]) <= 1e-6 * max(eroded, 1e-12), (m0, m1, stats)
+    assert abs((m1 - m0) + stats["lost_offshore"] - stats["deficit_out"]) <= 1e-6 * max(eroded, 1e-12), (m0, m1, stats)
 
 
 HYPS_TOL_FIRST = 0.5
