@@ -310,6 +310,11 @@ static_assert(RING > DESC_AHEAD, "the ring holds every entry in flight");
 // two droplets per block: a block's warp slots free up as soon as its two droplets are done, so
 // concurrent passes (other worlds' waves on other streams) pack around the long-lived droplets
 constexpr int APPLY_THREADS = 64;
+// resident blocks asked of the register allocator (0: its own choice, which spills the plain variant at 48
+// registers)
+#ifndef PGE_APPLY_MINB
+#define PGE_APPLY_MINB 0
+#endif
 
 // one entry of a droplet's list as the apply reads it, filled by asynchronous copies
 struct alignas(16) Slot {
@@ -504,7 +509,7 @@ __device__ __forceinline__ void flush_stats(const OrderedArgs &a, const unsigned
 }
 
 template <bool ECAP, bool LAKE>
-__global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const OrderedArgs a)
+__global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_kernel(const OrderedArgs a)
 {
     __shared__ unsigned long long sstat[OS_N];
     extern __shared__ Slot ring[];  // per droplet lane: RING slots
@@ -611,12 +616,32 @@ __global__ void __launch_bounds__(APPLY_THREADS) ordered_apply_kernel(const Orde
 // after the apply: per touched cell, in the serial (droplet, entry) order, the discharge and
 // momentum tracks (particle.py:1013-1018) and the stockpile (:1019-1041); then the cell's net
 // change to the accumulators and its packed samples (:1005-1009); and the wave's eroded and
-// deposited totals (integer fixed point, so their order does not matter)
+// deposited totals (integer fixed point, so their order does not matter).  First every sorted slot
+// gathers what its entry adds into arrays in sorted order (one thread a slot, all loads in flight at
+// once); then one thread a cell sums its run of those arrays in order (contiguous reads).
 // ---------------------------------------------------------------------------
-__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
-                                      unsigned long long invalid)
+__global__ void ordered_gather_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
+                                      unsigned long long invalid, FinishRows g)
 {
-    constexpr int U = 8;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[i];
+        if (key == invalid) continue;
+        const int32_t s = vals[i], q = s / a.cap;
+        const bool active = !a.mask || a.mask[key] == PGE_MASK_ACTIVE;
+        const float v = a.vol[s];
+        const bool track = active && v > 0.0f;
+        g.v[i] = track ? v : 0.0f;
+        g.m0[i] = track ? a.mom[2 * (long long)s] : 0.0f;
+        g.m1[i] = track ? a.mom[2 * (long long)s + 1] : 0.0f;
+        const double amt = a.act[s];
+        g.amt[i] = a.delta[s] < 0.0 ? -amt : amt;  // the sign says erosion (an eroded 0 is -0)
+        g.kp[i] = (a.desc[s].dflags & ENTRY_LAST) && a.dth[q] == (int32_t)key ? a.keep[q] : -1.0;  // keep >= 0
+    }
+}
+
+__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys,
+                                      unsigned long long invalid, FinishRows g)
+{
     __shared__ unsigned long long sfx[2];
     if (threadIdx.x < 2) sfx[threadIdx.x] = 0ull;
     __syncthreads();
@@ -628,54 +653,20 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
         const bool active = !a.mask || a.mask[c] == PGE_MASK_ACTIVE;
         double *accp = a.acc4 + 4 * c;
         double tq = accp[1], ta = accp[2], tb = accp[3], pd = a.pend[c];
-        bool more = true;
-        for (long long j = i; more; j += U) {
-            int32_t sl[U];
-            bool in[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                in[u] = j + u < nslots && keys[j + u] == key;
-                sl[u] = in[u] ? vals[j + u] : 0;
+        for (long long j = i; j < nslots && keys[j] == key; j++) {
+            const float v = g.v[j];
+            if (v > 0.0f) {  // a step of volume > 0 on an active cell (gathered as 0 otherwise)
+                tq += (double)v;
+                ta += (double)g.m0[j];
+                tb += (double)g.m1[j];
             }
-            float v[U], m0[U], m1[U];
-            bool stock[U];
-            double kp[U], amt[U], dl[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                v[u] = 0.0f;
-                m0[u] = m1[u] = 0.0f;
-                stock[u] = false;
-                kp[u] = amt[u] = dl[u] = 0.0;
-                if (in[u]) {
-                    const int32_t s = sl[u], q = s / a.cap;
-                    v[u] = a.vol[s];
-                    amt[u] = a.act[s];
-                    dl[u] = a.delta[s];
-                    if (active && v[u] > 0.0f) {
-                        m0[u] = a.mom[2 * (long long)s];
-                        m1[u] = a.mom[2 * (long long)s + 1];
-                    }
-                    if ((a.desc[s].dflags & ENTRY_LAST) && a.dth[q] == (int32_t)c) {
-                        stock[u] = true;
-                        kp[u] = a.keep[q];
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                if (!in[u]) continue;
-                if (active && v[u] > 0.0f) {
-                    tq += (double)v[u];
-                    ta += (double)m0[u];
-                    tb += (double)m1[u];
-                }
-                if (stock[u]) pd += kp[u];
-                if (dl[u] < 0.0)
-                    eroded += fx_mass(amt[u]);
-                else
-                    deposited += fx_mass(amt[u]);
-            }
-            more = in[U - 1];
+            const double kp = g.kp[j];
+            if (kp >= 0.0) pd += kp;
+            const double x = g.amt[j];
+            if (signbit(x))
+                eroded += fx_mass(-x);
+            else
+                deposited += fx_mass(x);
         }
         accp[1] = tq;
         accp[2] = ta;
@@ -758,7 +749,15 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
         ordered_apply_kernel<false, true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     else
         ordered_apply_kernel<false, false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
-    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
+    // the sort's input keys and the scans' buffers are free again: the gathered rows live there
+    FinishRows g;
+    g.v = reinterpret_cast<float *>(w.runstart);
+    g.m0 = reinterpret_cast<float *>(w.segpos);
+    g.m1 = reinterpret_cast<float *>(w.runscan);
+    g.amt = reinterpret_cast<double *>(w.keys_in);
+    g.kp = w.fin_kp;
+    ordered_gather_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid, g);
+    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.invalid, g);
     return cudaPeekAtLastError();
 }
 
