@@ -54,6 +54,14 @@ inline int grid_for(long long n, int threads = 256)
 }
 
 constexpr long long kSpinLimit = 1LL << 22;  // ~ seconds of polling: far beyond any real hand-off
+// a waiting warp sleeps PGE_POLL_SLEEP_NS after every PGE_POLL_EVERY polls (a power of two)
+#ifndef PGE_POLL_EVERY
+#define PGE_POLL_EVERY 256
+#endif
+#ifndef PGE_POLL_SLEEP_NS
+#define PGE_POLL_SLEEP_NS 32
+#endif
+static_assert((PGE_POLL_EVERY & (PGE_POLL_EVERY - 1)) == 0, "poll interval: a power of two");
 
 // A cell's hand-off word: 16 bytes, two 8-byte halves (acc low 32 bits | count << 32) and (acc high
 // 32 bits | count << 32), where acc is the live net change and count the hand-off counter.  Each
@@ -99,9 +107,9 @@ __device__ __forceinline__ bool acquire(const double2 *hand, long long c, uint32
             acc = hand_acc(w0, w1);
             return true;
         }
-        if ((i & 255) == 255) {
+        if ((i & (PGE_POLL_EVERY - 1)) == PGE_POLL_EVERY - 1) {
             if (*(volatile int *)error) return false;  // another wait gave up: stop waiting
-            __nanosleep(32);
+            __nanosleep(PGE_POLL_SLEEP_NS);
         }
     }
     atomicExch(error, 1);
