@@ -75,6 +75,12 @@ def run_batched(args, rank, world_size, dist, dev):
     from pgerosion import _lib
 
     wave_kw = {} if args.batch_apply == "ordered" else {"apply": _lib.APPLY_WAVE, "wave": max(counts) * 2 if counts else 1}
+    wave = args.batch_apply == "wave"
+    # the wave apply's own-change tables: every world at once holds a share of the GPU's resident ledger threads
+    # (by cost), so that 64 worlds' tables fit; one by one, each world gets all of them (below)
+    quota = batch.thread_quota([w.cost for w in sub]) if wave else [0] * len(sub)
+    for st, q in zip(states, quota):
+        st.max_threads = q
     runner = batch.Runner(states, [w.params for w in sub], costs=[w.cost for w in sub], **wave_kw) if sub else None
     if runner:
         runner.step(1, n_particles=counts)  # warm-up: workspaces, first pass of every world
@@ -84,13 +90,22 @@ def run_batched(args, rank, world_size, dist, dev):
         dist.barrier()
     ev[0].record()
     one, worst = 0, 0.0
+    ms_alone = 0.0
     for i, (st, w) in enumerate(zip(states, sub)):
+        if wave:  # alone, a world's pass takes every resident ledger thread: its full tables, made before timing
+            st.max_threads = 0
+            st.reserve(counts[i] + st.F * st.N * st.N, gm.list_steps_of(w.params.erosion, st.N), 1, wave_tables=True)
+            torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         one += gm.step(st, w.params, st.iteration, n_particles=counts[i], predrawn=pre[(i, st.iteration)], **wave_kw)["droplet_steps"]
         e1.record()
         e1.synchronize()
         worst = max(worst, e0.elapsed_time(e1))
+        ms_alone += e0.elapsed_time(e1)
+        if wave:  # back to the world's share, made again now (outside the timed passes)
+            st.max_threads = quota[i]
+            st.reserve(counts[i] + st.F * st.N * st.N, gm.list_steps_of(w.params.erosion, st.N), 1, wave_tables=True)
     ev[1].record()
     torch.cuda.synchronize()
     if dist:
@@ -102,8 +117,10 @@ def run_batched(args, rank, world_size, dist, dev):
     if runner:
         runner.close()
     together = sum(s["droplet_steps"] for r in res for s in r)
+    # one by one: the sum of the worlds' own passes, each timed on the device (the host's turns between them, and
+    # with the wave apply the workspaces made between them, are not counted)
     (one_all, tog_all), (ms_one, ms_tog, worst) = batch.reduce_totals(
-        dist, [one, together], [ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3]), worst], device=dev)
+        dist, [one, together], [ms_alone, ev[2].elapsed_time(ev[3]), worst], device=dev)
     sizes = sorted(w.N for w in worlds)
     v_one, v_tog = one_all / (ms_one * 1e-3), tog_all / (ms_tog * 1e-3)
     del runner, states

@@ -147,6 +147,9 @@ typedef struct PgeGrid {
                                 0: ordered apply and map passes only */
     int64_t max_droplets;    /* workspace capacity: the most spawns (rain + stockpiles) of one pass */
     int64_t max_wave;        /* workspace capacity: the largest wave of the exact (ordered) apply */
+    int64_t max_threads;     /* the wave apply's resident droplet threads, each with its own-change table
+                                (0: as many as the GPU holds, 1024 a multiprocessor); fewer keep the
+                                tables small for a pass that shares the GPU with other worlds' passes */
 } PgeGrid;
 
 /* the ErosionState arrays (globe/erosion/maps.py:56-115) on the device */

@@ -135,6 +135,7 @@ Layout layout(const PgeGrid &g)
     L.ncell = (long long)g.F * NE * NE;
     L.nmetric = g.metric_shared ? NE * NE : L.ncell;
     L.nslots = droplet_slots();
+    if (g.max_threads > 0 && g.max_threads < L.nslots) L.nslots = g.max_threads < 256 ? 256 : g.max_threads / 256 * 256;
     L.table_cap = ledger_table_cap(g.max_steps);
     L.table_slots = ledger_table_slots(g.max_steps);
     L.max_droplets = g.max_droplets;
@@ -417,7 +418,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
                 a.lanes = (int)(lanes < 1 ? 1 : (lanes > 32 ? 32 : lanes));
                 const int tpb = 32;
                 long long blocks = (nd + a.lanes - 1) / a.lanes;
-                if (blocks * tpb > lay.nslots) blocks = lay.nslots / tpb;
+                if (blocks * tpb > droplet_slots()) blocks = droplet_slots() / tpb;  // no tables: the GPU's resident threads
                 e = p->precision == PGE_PREC_F64 ? launch_droplets_f64(a, (int)blocks, tpb, st)
                                                  : launch_droplets_f32(a, (int)blocks, tpb, st);
                 if (e != cudaSuccess) return cuda_fail(e, "droplet kernel");

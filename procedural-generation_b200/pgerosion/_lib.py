@@ -42,7 +42,7 @@ c_i32, c_i64, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_double, cty
 class PgeGrid(ctypes.Structure):
     _fields_ = [("F", c_i32), ("N", c_i32), ("H", c_i32), ("spherical", c_i32), ("deposit_on_exit", c_i32),
                 ("metric_shared", c_i32), ("max_steps", c_i32), ("wave_tables", c_i32), ("max_droplets", c_i64),
-                ("max_wave", c_i64)]
+                ("max_wave", c_i64), ("max_threads", c_i64)]
 
 
 class PgeState(ctypes.Structure):

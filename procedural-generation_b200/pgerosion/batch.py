@@ -85,6 +85,19 @@ def assign(costs, world_size: int) -> list[list[int]]:
     return [sorted(x) for x in out]
 
 
+#: resident droplet threads of the wave apply's ledger kernel on a B200: one block of 256 a multiprocessor
+LEDGER_THREADS = 148 * 256
+
+
+def thread_quota(costs, total: int = LEDGER_THREADS) -> list[int]:
+    """Each world's share of the wave apply's resident ledger threads, in
+    proportion to its cost, rounded up to whole blocks of 256 (at least
+    one): the per-thread own-change tables of many worlds at once then fit
+    in HBM (``ErosionState.max_threads``)."""
+    tot = float(sum(costs)) or 1.0
+    return [int(min(total, max(256, -(-int(total * float(c) / tot) // 256) * 256))) for c in costs]
+
+
 def my_worlds(costs, rank: int, world_size: int) -> list[int]:
     """The worlds rank ``rank`` erodes."""
     return assign(costs, world_size)[rank]

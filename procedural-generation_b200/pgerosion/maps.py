@@ -82,6 +82,10 @@ class ErosionState:
     max_steps: int = 0
     max_wave: int = 0
     wave_tables: bool = False
+    #: the wave apply's resident droplet threads with own-change tables (0: the GPU's maximum); set lower
+    #: (then call reserve) for a world that shares the GPU with others, to keep its workspace small
+    max_threads: int = 0
+    _ws_threads: int = field(default=-1, repr=False)
     _ws: torch.Tensor = field(default=None, repr=False)
     _halo: tuple = field(default=None, repr=False)
     _erode_cap: torch.Tensor = field(default=None, repr=False)
@@ -194,7 +198,8 @@ class ErosionState:
     def pge_grid(self) -> PgeGrid:
         return PgeGrid(F=self.F, N=self.N, H=self.H, spherical=int(bool(self.spherical)),
                        deposit_on_exit=int(bool(self.deposit_on_exit)), metric_shared=1, max_steps=int(self.max_steps),
-                       wave_tables=int(self.wave_tables), max_droplets=int(self.max_droplets), max_wave=int(self.max_wave))
+                       wave_tables=int(self.wave_tables), max_droplets=int(self.max_droplets), max_wave=int(self.max_wave),
+                       max_threads=int(self.max_threads))
 
     def pge_state(self, parks: bool = False) -> PgeState:
         """The C view of the state; with ``parks`` the lake parks' arrays
@@ -225,8 +230,10 @@ class ErosionState:
         ``max_droplets`` spawns of ``max_steps`` steps and ordered-apply
         waves of up to ``max_wave`` droplets (grows, never shrinks)."""
         if (max_droplets <= self.max_droplets and max_steps <= self.max_steps and max_wave <= self.max_wave
-                and (self.wave_tables or not wave_tables) and self._ws is not None):
+                and (self.wave_tables or not wave_tables) and self._ws is not None and self._ws_threads == self.max_threads):
             return
+        self._ws_threads = int(self.max_threads)
+        self._ws = None  # the old workspace goes before the new one is made
         self.wave_tables = bool(self.wave_tables or wave_tables)
         self.max_droplets = max(int(max_droplets), self.max_droplets)
         self.max_steps = max(int(max_steps), self.max_steps)

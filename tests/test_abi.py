@@ -100,7 +100,9 @@ def test_bank_cut_needs_room_for_two_entries_a_step_without_gpu():
     ws = (raw.ctypes.data + 255) & ~255
     a = np.zeros(64, np.float64)
     ptr = a.ctypes.data
-    st = _lib.PgeState(**{n: ptr for n, _ in _lib.PgeState._fields_ if n not in ("mask", "erodibility", "route", "lake_flag", "roots")})
+    st = _lib.PgeState(**{n: ptr for n, _ in _lib.PgeState._fields_
+                          if n not in ("mask", "erodibility", "route", "lake_flag", "roots", "lake_load", "lake_id", "lake_room",
+                                       "lakes")})
     prm = _lib.PgeParams(max_steps=32, wave=16, precision=_lib.PREC_F64, apply=_lib.APPLY_WAVE, lateral_rate=0.5)
     stats = np.zeros(_lib.STATS_WORDS, np.int64)
     sp = _lib.PgeSpawns(count=0, volume0=1.0)
@@ -111,3 +113,23 @@ def test_bank_cut_needs_room_for_two_entries_a_step_without_gpu():
     rc = L.pge_trace_apply(ctypes.byref(g), ctypes.byref(st), ctypes.byref(sp), ctypes.byref(prm), None, stats.ctypes.data, ws,
                            nbytes, None)
     assert rc == _lib.PGE_E_ARG and "lateral_rate" in _lib.last_error()
+
+
+def test_wave_tables_follow_max_threads_without_gpu():
+    """PgeGrid.max_threads bounds the wave apply's per-thread own-change
+    tables: a grid for 4096 resident droplet threads needs a smaller
+    workspace than one for the whole GPU, and the ordered apply's workspace
+    (no tables) does not depend on it."""
+    L = _lib.load()
+    kw = dict(F=6, N=64, H=2, spherical=1, metric_shared=1, max_steps=128, max_droplets=4096, max_wave=2048)
+    full = int(L.pge_workspace_bytes(ctypes.byref(_lib.PgeGrid(**kw, wave_tables=1))))
+    small = int(L.pge_workspace_bytes(ctypes.byref(_lib.PgeGrid(**kw, wave_tables=1, max_threads=4096))))
+    assert 0 < small < full
+    # 16 bytes a table slot (key and own change) a thread less
+    slots = 16
+    while slots < 2 * (128 + 8 + 2):
+        slots <<= 1
+    assert full - small >= 16 * slots * (148 * 1024 - 4096) - 4096
+    a = int(L.pge_workspace_bytes(ctypes.byref(_lib.PgeGrid(**kw))))
+    b = int(L.pge_workspace_bytes(ctypes.byref(_lib.PgeGrid(**kw, max_threads=4096))))
+    assert a == b

@@ -91,3 +91,13 @@ def test_two_gloo_ranks_share_worlds_and_reduce(tmp_path):
 def test_reduce_totals_single_rank():
     sums, maxes = batch.reduce_totals(None, [1, 2.5], [3.0])
     assert sums == [1.0, 2.5] and maxes == [3.0]
+
+
+def test_thread_quota_shares_the_ledger_threads_by_cost():
+    costs = [w.cost for w in batch.batch_worlds(64, seed=0)]
+    q = batch.thread_quota(costs)
+    assert all(v % 256 == 0 and 256 <= v <= batch.LEDGER_THREADS for v in q)
+    # in proportion to cost, every world at least one block; the total about the GPU's resident threads
+    big, small = max(range(64), key=lambda i: costs[i]), min(range(64), key=lambda i: costs[i])
+    assert q[big] > q[small] == 256
+    assert batch.LEDGER_THREADS <= sum(q) <= batch.LEDGER_THREADS + 64 * 256

@@ -83,3 +83,31 @@ def test_packed_lanes_are_exact(cuda):
     torch.cuda.synchronize()
     for f in FIELDS:
         assert torch.equal(getattr(a, f), getattr(b, f)), f
+
+
+def test_wave_apply_worlds_with_thread_shares_equal_their_single_runs(cuda):
+    """The wave apply's worlds stepped together, each with a share of the
+    ledger threads (``max_threads``: smaller own-change tables, a smaller
+    persistent launch), equal the same worlds stepped alone with every
+    thread: the int64 sums do not depend on which thread took a droplet."""
+    import torch
+
+    from pgerosion import _lib, batch
+    from pgerosion import maps as gm
+
+    ws = _worlds()
+    counts = [min(w.n_particles, 1500) for w in ws]
+    kw = {"apply": _lib.APPLY_WAVE, "wave": 4000}
+    together = batch.build_states(ws)
+    for st, q in zip(together, batch.thread_quota([w.cost for w in ws], total=1024)):
+        st.max_threads = q
+    batch.Runner(together, [w.params for w in ws], **kw).step(2, n_particles=counts)
+    alone = batch.build_states(ws)
+    for i, (st, w) in enumerate(zip(alone, ws)):
+        for it in range(2):
+            gm.step(st, w.params, it, n_particles=counts[i], **kw)
+    torch.cuda.synchronize()
+    assert all(st._ws_threads <= 1024 for st in together)
+    for a, b in zip(together, alone):
+        for f in FIELDS:
+            assert torch.equal(getattr(a, f), getattr(b, f)), f
