@@ -301,13 +301,14 @@ def cpu_baseline(params, P, world, seconds=20.0):
 def launches_per_iteration(nw: int, pending: bool, creep: bool, ordered: bool) -> int:
     """Kernels of this library one plain iteration launches (library kernels
     -- CUB scan / sort / select -- not counted)."""
-    spawn = 3 + (1 if pending else 0)
-    if ordered:   # pack x2, terrain; per wave: trace, keys, flags, ranks, ordered apply, finish; error report, mode, fold+EMA
-        droplets = 3 + 6 * nw + 3
+    # weights, counts, quantised weights, CDF, the total's pairwise sum (plan, leaves, fold), search; the stockpiles
+    spawn = 8 + (1 if pending else 0)
+    if ordered:   # pack x2, terrain; per wave: trace, keys, flags, ranks, ordered apply, gather, finish; error report, mode, fold+EMA
+        droplets = 3 + 7 * nw + 3
     else:         # pack x2; waves and the refreshes between them; mode, fold+EMA
         droplets = 2 + nw + (nw - 1) + 2
     thermal = 4 * (2 if creep else 1)
-    uplift = 3
+    uplift = 4    # the mean's pairwise sum (plan, leaves, fold), the add
     datum = 1 + 8 * 2 + 1
     halo = 4
     return spawn + droplets + thermal + uplift + datum + halo
