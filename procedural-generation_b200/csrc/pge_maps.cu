@@ -35,6 +35,18 @@ inline int grid_for(long long n, int threads = 256)
     long long b = (n + threads - 1) / threads;
     return (int)(b < 1 ? 1 : (b > 1048576 ? 1048576 : b));
 }
+// a grid-stride launch for kernels that end in a few global atomics a block: 8 blocks a multiprocessor
+inline int grid_reduce(long long n, int threads = 256)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+    }
+    const int b = grid_for(n, threads);
+    return b < 8 * sms ? b : 8 * sms;
+}
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -552,12 +564,14 @@ struct Positive {
 // the two halves' sums added.  (numpy's pairwise_sum, the reduction loop of
 // np.add; checked against np.sum on ranges of 1..5000 values of mixed
 // magnitudes.)  The top of the tree is expanded breadth-first into at most
-// PW_MAX_LEVEL_NODES nodes a level; the bottom nodes are summed one per thread
-// and the tree is folded back up in order.
+// PW_MAX_LEVEL_NODES nodes a level (one block, a level at a time); the bottom
+// nodes are summed one per thread and the tree is folded back up in order (one
+// block, a level at a time).
 // ---------------------------------------------------------------------------
 constexpr int PW_LEAF = 128;
-constexpr int PW_MAX_LEVELS = 16;
-constexpr int PW_MAX_LEVEL_NODES = 2048;
+constexpr int PW_MAX_LEVELS = 24;
+constexpr int PW_MAX_LEVEL_NODES = 32768;
+constexpr int PW_THREADS = 1024;
 
 struct PwNode {
     long long lo, n;
@@ -633,18 +647,42 @@ __device__ double pw_sum(const double *a, long long n)
     }
 }
 
-__global__ void pw_plan_kernel(const long long *count, PwNode *nodes, int *level_start)
+// one block of PW_THREADS: a level's nodes split among the threads in order, each thread's children placed
+// after those of the threads before it (a block scan of the counts)
+__global__ void __launch_bounds__(PW_THREADS) pw_plan_kernel(const long long *count, PwNode *nodes, int *level_start)
 {
+    typedef cub::BlockScan<int, PW_THREADS> Scan;
+    typedef cub::BlockReduce<long long, PW_THREADS> Reduce;
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ typename Reduce::TempStorage red_tmp;
+    __shared__ long long s_biggest;
+    __shared__ int s_next;
+    const int t = threadIdx.x;
     const long long M = *count;
-    nodes[0] = PwNode{0, M, -1, 0, 0.0};
+    if (t == 0) {
+        nodes[0] = PwNode{0, M, -1, 0, 0.0};
+        level_start[0] = 0;
+    }
+    __syncthreads();
     int nl = 0, begin = 0, end = 1;
-    level_start[0] = 0;
     while (nl + 1 < PW_MAX_LEVELS) {
-        long long biggest = 0;
-        for (int k = begin; k < end; k++) biggest = nodes[k].n > biggest ? nodes[k].n : biggest;
-        if (biggest <= 8 * PW_LEAF || 2 * (end - begin) > PW_MAX_LEVEL_NODES) break;
-        int next = end;
-        for (int k = begin; k < end; k++) {
+        const int nnodes = end - begin;
+        const int per = (nnodes + PW_THREADS - 1) / PW_THREADS;
+        const int k0 = begin + t * per, k1 = min(k0 + per, end);
+        long long big = 0;
+        int nch = 0;
+        for (int k = k0; k < k1; k++) {
+            big = nodes[k].n > big ? nodes[k].n : big;
+            nch += nodes[k].n > PW_LEAF ? 2 : 1;
+        }
+        const long long b = Reduce(red_tmp).Reduce(big, cub::Max());
+        if (t == 0) s_biggest = b;
+        __syncthreads();
+        if (s_biggest <= 8 * PW_LEAF || 2 * nnodes > PW_MAX_LEVEL_NODES) break;
+        int off, total;
+        Scan(scan_tmp).ExclusiveSum(nch, off, total);
+        int next = end + off;
+        for (int k = k0; k < k1; k++) {
             PwNode &nd = nodes[k];
             nd.child = next;
             if (nd.n > PW_LEAF) {
@@ -657,12 +695,18 @@ __global__ void pw_plan_kernel(const long long *count, PwNode *nodes, int *level
                 nd.nchild = 1;
             }
         }
+        if (t == 0) s_next = end + total;
+        __syncthreads();
         begin = end;
-        end = next;
-        level_start[++nl] = begin;
+        end = s_next;
+        nl++;
+        if (t == 0) level_start[nl] = begin;
+        __syncthreads();
     }
-    level_start[nl + 1] = end;
-    level_start[PW_MAX_LEVELS + 1] = nl;  // the bottom level's index
+    if (t == 0) {
+        level_start[nl + 1] = end;
+        level_start[PW_MAX_LEVELS + 1] = nl;  // the bottom level's index
+    }
 }
 
 __global__ void pw_bottom_kernel(const double *a, PwNode *nodes, const int *level_start)
@@ -673,17 +717,22 @@ __global__ void pw_bottom_kernel(const double *a, PwNode *nodes, const int *leve
         nodes[k].sum = pw_sum(a + nodes[k].lo, nodes[k].n);
 }
 
-// folds the levels back up; out = the sum, or with mean_out the sum / count
-__global__ void pw_fold_kernel(PwNode *nodes, const int *level_start, const long long *count, double *out, int mean_out)
+// folds the levels back up, a level at a time (one block); out = the sum, or with mean_out the sum / count
+__global__ void __launch_bounds__(PW_THREADS) pw_fold_kernel(PwNode *nodes, const int *level_start, const long long *count,
+                                                             double *out, int mean_out)
 {
     const int nl = level_start[PW_MAX_LEVELS + 1];
-    for (int l = nl - 1; l >= 0; l--)
-        for (int k = level_start[l]; k < level_start[l + 1]; k++) {
+    for (int l = nl - 1; l >= 0; l--) {
+        for (int k = level_start[l] + threadIdx.x; k < level_start[l + 1]; k += blockDim.x) {
             PwNode &nd = nodes[k];
             nd.sum = nd.nchild == 2 ? nodes[nd.child].sum + nodes[nd.child + 1].sum : nodes[nd.child].sum;
         }
-    const long long M = *count;
-    *out = mean_out ? (M > 0 ? nodes[0].sum / (double)M : 0.0) : nodes[0].sum;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const long long M = *count;
+        *out = mean_out ? (M > 0 ? nodes[0].sum / (double)M : 0.0) : nodes[0].sum;
+    }
 }
 
 size_t pairwise_scratch_bytes() { return sizeof(PwNode) * (size_t)PW_MAX_LEVELS * PW_MAX_LEVEL_NODES + 256; }
@@ -693,9 +742,9 @@ void pairwise_sum(const double *a, const long long *count, void *scratch, double
 {
     PwNode *nodes = static_cast<PwNode *>(scratch);
     int *level_start = reinterpret_cast<int *>(nodes + (size_t)PW_MAX_LEVELS * PW_MAX_LEVEL_NODES);
-    pw_plan_kernel<<<1, 1, 0, st>>>(count, nodes, level_start);
+    pw_plan_kernel<<<1, PW_THREADS, 0, st>>>(count, nodes, level_start);
     pw_bottom_kernel<<<(PW_MAX_LEVEL_NODES + 127) / 128, 128, 0, st>>>(a, nodes, level_start);
-    pw_fold_kernel<<<1, 1, 0, st>>>(nodes, level_start, count, out, mean);
+    pw_fold_kernel<<<1, PW_THREADS, 0, st>>>(nodes, level_start, count, out, mean);
 }
 
 // ---------------------------------------------------------------------------
@@ -838,7 +887,7 @@ void hold_datum(const PgeGrid &g, PgeState &s, const Layout &lay, void *ws, doub
     SelectState *ss = ws_ptr<SelectState>(ws, lay.partial + 4 * RED_BLOCKS * sizeof(double));
     select_init_kernel<<<1, 256, 0, st>>>(ss, k);
     for (int shift = 56; shift >= 0; shift -= 8) {
-        select_hist_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, ss, shift);
+        select_hist_kernel<<<grid_reduce(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, ss, shift);
         select_pick_kernel<<<1, 256, 0, st>>>(ss, shift);
     }
     datum_shift_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, s.height, s.base, ss, level, plus_one, shift_dev);
@@ -914,10 +963,20 @@ __global__ void spawn_weight_kernel(long long ncell, int NE, int H, int N, const
             emax = e > emax ? e : emax;
         }
     }
-    if (last >= 0) atomicMax(reinterpret_cast<unsigned long long *>(lastc), (unsigned long long)last);
-    if (emax >= 0) {
-        atomicMin(erange, (long long)emin);
-        atomicMax(erange + 1, (long long)emax);
+    // the block's extremes first, then one atomic each a block
+    typedef cub::BlockReduce<long long, 256> BR;
+    typedef cub::BlockReduce<int, 256> BRi;
+    __shared__ typename BR::TempStorage t0;
+    __shared__ typename BRi::TempStorage t1, t2;
+    last = BR(t0).Reduce(last, cub::Max());
+    emin = BRi(t1).Reduce(emin, cub::Min());
+    emax = BRi(t2).Reduce(emax, cub::Max());
+    if (threadIdx.x == 0) {
+        if (last >= 0) atomicMax(reinterpret_cast<unsigned long long *>(lastc), (unsigned long long)last);
+        if (emax >= 0) {
+            atomicMin(erange, (long long)emin);
+            atomicMax(erange + 1, (long long)emax);
+        }
     }
 }
 
@@ -963,8 +1022,10 @@ __global__ void spawn_count_kernel(long long ncell, const double *w, long long *
     long long n = 0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell; c += (long long)gridDim.x * blockDim.x)
         n += w[c] > 0.0;
-    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(0xffffffffu, n, o);
-    if ((threadIdx.x & 31) == 0 && n) atomicAdd(reinterpret_cast<unsigned long long *>(count), (unsigned long long)n);
+    typedef cub::BlockReduce<long long, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    n = BR(tmp).Sum(n);
+    if (threadIdx.x == 0 && n) atomicAdd(reinterpret_cast<unsigned long long *>(count), (unsigned long long)n);
 }
 
 __global__ void spawn_search_kernel(long long ncell, int NE, int H, const double *cdf, const long long *lastc, const double *u,
@@ -1059,9 +1120,9 @@ cudaError_t spawn_rain(const PgeGrid &g, const PgeState &s, const Layout &lay, v
     if ((e = cudaMemsetAsync(erange, 0x7f, sizeof(long long), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(erange + 1, 0, sizeof(long long), st)) != cudaSuccess) return e;
     if (nspawn_dev && (e = cudaMemsetAsync(nspawn_dev, 0, sizeof(long long), st)) != cudaSuccess) return e;
-    spawn_weight_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, s.base, s.mask,
+    spawn_weight_kernel<<<grid_reduce(lay.ncell), 256, 0, st>>>(lay.ncell, NE, g.H, g.N, s.height, s.sediment, s.base, s.mask,
                                                              s.precip, w, lastc, erange);
-    if (nspawn_dev) spawn_count_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, w, nspawn_dev);
+    if (nspawn_dev) spawn_count_kernel<<<grid_reduce(lay.ncell), 256, 0, st>>>(lay.ncell, w, nspawn_dev);
     spawn_quant_kernel<<<grid_for(lay.ncell), 256, 0, st>>>(lay.ncell, w, erange, wq);
     size_t tb = lay.cubtmp_bytes;
     e = cub::DeviceScan::InclusiveSum(ws_ptr<void>(ws, lay.cubtmp), tb, wq, reinterpret_cast<long long *>(cdf), (int)lay.ncell, st);

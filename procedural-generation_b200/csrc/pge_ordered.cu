@@ -160,6 +160,25 @@ __global__ void ordered_keys_kernel(long long nslots, int cap, const int32_t *ce
     }
 }
 
+// the entries of a wave's lists compacted in (droplet, entry) order: entry k of droplet q goes to offsets[q] + k
+__global__ void ordered_compact_keys_kernel(long long nslots, int cap, const int32_t *cell, const int64_t *count,
+                                            const long long *offsets, unsigned long long *keys, int32_t *vals)
+{
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nslots; s += (long long)gridDim.x * blockDim.x) {
+        const long long q = s / cap, k = s - q * cap;
+        if (k < count[q]) {
+            const long long e = offsets[q] + k;
+            keys[e] = (unsigned long long)cell[s];
+            vals[e] = (int32_t)s;
+        }
+    }
+}
+
+__global__ void entry_total_kernel(const int64_t *count, const long long *offsets, long long nw, long long *total)
+{
+    *total = nw > 0 ? offsets[nw - 1] + count[nw - 1] : 0;
+}
+
 // runstart: first slot of a (cell, droplet) run; segpos: position of a cell segment's first slot
 __global__ void ordered_flags_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
                                      unsigned long long invalid, int32_t *runstart, int32_t *segpos)
@@ -220,7 +239,8 @@ struct MaxOp {
 
 size_t ordered_temp_bytes(long long nslots, long long max_wave)
 {
-    size_t a = 0, b = 0, c = 0, d = 0;
+    size_t a = 0, b = 0, c = 0, d = 0, x = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, x, (int64_t *)nullptr, (long long *)nullptr, (int)max_wave);
     cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long *)nullptr, (unsigned long long *)nullptr, (int32_t *)nullptr,
                                     (int32_t *)nullptr, (int)nslots);
     cub::DeviceScan::InclusiveSum(nullptr, b, (int32_t *)nullptr, (int32_t *)nullptr, (int)nslots);
@@ -229,7 +249,8 @@ size_t ordered_temp_bytes(long long nslots, long long max_wave)
                                     (int)(max_wave * LAKE_PARKS));
     size_t m = a > b ? a : b;
     m = m > c ? m : c;
-    return m > d ? m : d;
+    m = m > d ? m : d;
+    return m > x ? m : x;
 }
 
 // ---------------------------------------------------------------------------
@@ -763,11 +784,25 @@ int ordered_blocks_per_sm(int lanes)
 
 cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
 {
-    const long long nslots = w.nw * w.cap;
-    ordered_keys_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.cap, w.a.cell, w.a.count, w.invalid, w.keys_in, w.vals_in);
+    long long nslots = w.nw * w.cap;
     size_t tb = w.temp_bytes;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(w.temp, tb, w.keys_in, w.keys_out, w.vals_in, w.vals_out, (int)nslots, 0,
-                                                    w.end_bit, st);
+    cudaError_t e;
+    if (w.offsets) {
+        // long lists (a lifetime of thousands of steps, most of it unused): only the recorded entries go through
+        // the ranks, in (droplet, entry) order; their count comes back to the host for the library sorts
+        if ((e = cub::DeviceScan::ExclusiveSum(w.temp, tb, w.a.count, w.offsets, (int)w.nw, st)) != cudaSuccess) return e;
+        entry_total_kernel<<<1, 1, 0, st>>>(w.a.count, w.offsets, w.nw, w.offsets + w.nw);
+        long long total = 0;
+        if ((e = cudaMemcpyAsync(&total, w.offsets + w.nw, sizeof(long long), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+        ordered_compact_keys_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.cap, w.a.cell, w.a.count, w.offsets, w.keys_in,
+                                                                      w.vals_in);
+        nslots = total;
+    } else {
+        ordered_keys_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.cap, w.a.cell, w.a.count, w.invalid, w.keys_in, w.vals_in);
+    }
+    tb = w.temp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(w.temp, tb, w.keys_in, w.keys_out, w.vals_in, w.vals_out, (int)nslots, 0, w.end_bit, st);
     if (e != cudaSuccess) return e;
     ordered_flags_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runstart, w.segpos);
     tb = w.temp_bytes;

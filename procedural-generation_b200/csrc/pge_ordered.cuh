@@ -101,7 +101,13 @@ struct OrderedWave {
     size_t temp_bytes;
     long long max_blocks;
     double *fin_kp;  // one double a slot: the gathered stockpile amounts
+    // long lists: the recorded entries compacted before the ranks (nullptr: every slot goes through them);
+    // max_wave + 1 int64: each droplet's first entry, then the wave's total
+    long long *offsets;
 };
+
+// the list length above which a wave's entries are compacted before their ranks (a host read a wave)
+constexpr int COMPACT_CAP = 512;
 
 size_t ordered_temp_bytes(long long nslots, long long max_wave);
 cudaError_t park_wave(const ParkWave &pw, cudaStream_t st);

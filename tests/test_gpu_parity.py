@@ -430,3 +430,20 @@ def test_spawn_feeder_gives_the_reference_draws(cuda):
     finally:
         feeder.close()
 
+
+
+def test_compacted_ranks_equal_the_full_ones(cuda):
+    """A workspace built for long lists (a lifetime of 600 steps: every wave's
+    recorded entries compacted before their ranks, the entry count read back a
+    wave) gives the exact pass of the one that ranks every slot, bit for bit."""
+    c = step_case()
+    outs = []
+    for steps in (600, 0):
+        g = gm.ErosionState.from_world(c["world"])
+        if steps:
+            g.reserve(8192 + g.F * g.N * g.N, steps, 2048)
+        for it in range(3):
+            gm.step(g, c["params"], it, n_particles=4096)
+        outs.append(g.to_numpy())
+    for k in outs[0]:
+        assert outs[0][k].tobytes() == outs[1][k].tobytes(), k
