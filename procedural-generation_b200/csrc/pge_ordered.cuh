@@ -107,7 +107,10 @@ struct OrderedWave {
 };
 
 // the list length above which a wave's entries are compacted before their ranks (a host read a wave)
-constexpr int COMPACT_CAP = 512;
+#ifndef PGE_COMPACT_CAP
+#define PGE_COMPACT_CAP 512
+#endif
+constexpr int COMPACT_CAP = PGE_COMPACT_CAP;
 
 size_t ordered_temp_bytes(long long nslots, long long max_wave);
 cudaError_t park_wave(const ParkWave &pw, cudaStream_t st);
