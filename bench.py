@@ -544,9 +544,12 @@ def run_planet(args, dev):
     build_s = time.time() - t0
     kw = dict(n_particles=P, apply=_lib.APPLY_WAVE, wave=P + P // 8)
     timeline = planet.Timeline(st, every=20)
+    # the rain draws of the next iteration made on the host while the device runs this one (the public API's feeder)
+    feeder = gm.SpawnFeeder(params, P, device=dev)
+    feeder.prefetch((0,))
     total = args.warmup + args.steps if args.planet_iterations <= 0 else args.planet_iterations
     for it in range(args.warmup if args.planet_iterations <= 0 else 0):
-        gm.step(st, params, it, **kw)
+        gm.step(st, params, it, predrawn=feeder.get((it,))[:3], **kw)
         timeline.maybe(it)
     torch.cuda.synchronize()
     first = args.warmup if args.planet_iterations <= 0 else 0
@@ -558,7 +561,7 @@ def run_planet(args, dev):
         ev[0].record()
         for it in range(first, total):
             e = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            s = gm.step(st, params, it, events=e, **kw)
+            s = gm.step(st, params, it, events=e, predrawn=feeder.get((it,))[:3], **kw)
             timeline.maybe(it + 1)
             steps += s["droplet_steps"]
             ta.append(e)
@@ -566,6 +569,7 @@ def run_planet(args, dev):
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
     timeline.wait()
+    feeder.close()
     ms = ev[0].elapsed_time(ev[1])
     n = total - first
     avg = float(np.mean([a.elapsed_time(b) for a, b in ta]))

@@ -425,10 +425,14 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
         log(f"[erosion] resumed from {ck[0].name} (iteration {state.iteration})")
     times, clamped, lost_offshore, datum = [], 0, 0.0, 0.0
     writer = CheckpointWriter(store) if async_checkpoints and ep.checkpoint_every > 0 else None
+    # each iteration's rain draws made on the host one iteration ahead, while the device runs the current one
+    n_particles = max(1, int(round(float(ep.particles_per_cell) * state.n_active_interior())))
+    feeder = gm.SpawnFeeder(params, n_particles, device=state.height.device) if state.iteration < n_iter else None
     while state.iteration < n_iter:
         it = state.iteration
         t0 = time.time()
-        st = gm.step(state, params, it, apply=apply, wave=wave)
+        rng, u, off, _ = feeder.get((it,))
+        st = gm.step(state, params, it, apply=apply, wave=wave, n_particles=n_particles, predrawn=(rng, u, off))
         times.append(time.time() - t0)
         clamped += int(st.get("clamped", 0))
         lost_offshore += float(st.get("lost_offshore", 0.0))
@@ -447,6 +451,8 @@ def run(store, params, log=print, apply: int = _lib.APPLY_ORDERED, wave: int | N
                 log(f"[erosion] checkpoint -> {p.name}")
     if writer is not None:
         writer.close()
+    if feeder is not None:
+        feeder.close()
     # the lakes lay what the last iterations brought them: a run ends between two lake refreshes (run.py:476-483)
     lakes_end = gm.settle_lakes(state, params)
     if lakes_end is not None:
