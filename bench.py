@@ -82,7 +82,7 @@ def run_batched(args, rank, world_size, dist, dev):
     for st, q in zip(states, quota):
         st.max_threads = q
     runner = batch.Runner(states, [w.params for w in sub], costs=[w.cost for w in sub], trace_lanes=args.batch_trace_lanes,
-                          **wave_kw) if sub else None
+                          streams=args.batch_streams or None, **wave_kw) if sub else None
     if runner:
         runner.step(1, n_particles=counts)  # warm-up: workspaces, first pass of every world
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -657,6 +657,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--batch-apply", default="ordered", choices=("ordered", "wave"), help="the batched worlds' apply")
     ap.add_argument("--batch-trace-lanes", type=int, default=32, help="the batched worlds' trace: droplets per warp")
+    ap.add_argument("--batch-streams", type=int, default=0, help="the batched worlds' streams (0: one a world)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the calibration (adjoint) measurement")
     ap.add_argument("--adjoint-reps", type=int, default=2)
     ap.add_argument("--adjoint-only", action="store_true", help="run the calibration (adjoint) measurement alone")
