@@ -304,8 +304,8 @@ def launches_per_iteration(nw: int, pending: bool, creep: bool, ordered: bool) -
     -- CUB scan / sort / select -- not counted)."""
     # weights, counts, quantised weights, CDF, the total's pairwise sum (plan, leaves, fold), search; the stockpiles
     spawn = 8 + (1 if pending else 0)
-    if ordered:   # pack x2, terrain; per wave: trace, keys, flags, ranks, ordered apply, finish; error report, mode, fold+EMA
-        droplets = 3 + 6 * nw + 3
+    if ordered:   # pack x2, terrain; per wave: trace, keys, flags, ranks, ordered apply, gather, finish; error report, mode, fold+EMA
+        droplets = 3 + 7 * nw + 3
     else:         # pack x2; waves and the refreshes between them; mode, fold+EMA
         droplets = 2 + nw + (nw - 1) + 2
     thermal = 4 * (2 if creep else 1)

@@ -195,6 +195,7 @@ Layout layout(const PgeGrid &g)
     L.w_park_n = take(4 * L.max_wave);
     L.w_park_k = take(4 * LAKE_PARKS * L.max_wave);
     L.w_park_rest = take(8 * LAKE_PARKS * L.max_wave);
+    L.w_fin = take(8 * ws);
     L.w_offsets = take(8 * (L.max_wave + 1));
     L.hand = take(16 * L.ncell);
     L.terr = take(16 * L.ncell);
@@ -383,6 +384,7 @@ int run_waves(const PgeGrid *g, PgeState *s, const PgeSpawns *sp, const PgeParam
             ow.segscan = ws_ptr<int32_t>(ws, lay.w_segscan);
             ow.temp = ws_ptr<void>(ws, lay.w_temp);
             ow.temp_bytes = lay.w_temp_bytes;
+            ow.fin_kp = ws_ptr<double>(ws, lay.w_fin);
             ow.offsets = lay.cap >= COMPACT_CAP ? ws_ptr<long long>(ws, lay.w_offsets) : nullptr;
             oa.lanes = p->apply_lanes > 0 ? p->apply_lanes : 1;
             ow.max_blocks = (long long)sm_count() * ordered_blocks_per_sm(oa.lanes);

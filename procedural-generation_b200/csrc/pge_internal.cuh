@@ -66,6 +66,7 @@ struct Layout {
         w_segpos, w_runscan, w_segscan, w_temp, w_temp_bytes, w_dth, w_keep, w_act, hand, terr, error;
     // the lake parks of one wave: per droplet its park count and entry indices, per park the refused rest
     size_t w_park_n, w_park_k, w_park_rest;
+    size_t w_fin;  // the finish's gathered stockpile amounts, one double a slot
     size_t w_offsets;  // long lists: each droplet's first compacted entry, and the wave's total
     int64_t ncell, nmetric, nslots, table_cap, table_slots, max_droplets, max_wave, wave_slots, cap;
 };

@@ -180,10 +180,8 @@ __global__ void entry_total_kernel(const int64_t *count, const long long *offset
 }
 
 // runstart: first slot of a (cell, droplet) run; segpos: position of a cell segment's first slot
-// pairs[i] = (1 at the first slot of a (cell, droplet) run, the position of a cell segment's first slot
-// there); one inclusive scan (sum, max) gives each slot its run count and its segment's start
 __global__ void ordered_flags_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
-                                     unsigned long long invalid, int2 *pairs)
+                                     unsigned long long invalid, int32_t *runstart, int32_t *segpos)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
@@ -197,27 +195,20 @@ __global__ void ordered_flags_kernel(long long nslots, const unsigned long long 
                 sp = newseg ? (int)i : 0;
             }
         }
-        pairs[i] = make_int2(rs, sp);
+        runstart[i] = rs;
+        segpos[i] = sp;
     }
 }
 
-struct RunSegOp {
-    __device__ __forceinline__ int2 operator()(const int2 a, const int2 b) const
-    {
-        return make_int2(a.x + b.x, a.y > b.y ? a.y : b.y);
-    }
-};
-
 __global__ void ordered_rank_kernel(long long nslots, const unsigned long long *keys, const int32_t *vals, int cap,
-                                    unsigned long long invalid, const int2 *scans, const double *delta, const float *vol,
-                                    EntryDesc *desc)
+                                    unsigned long long invalid, const int32_t *runscan, const int32_t *segscan,
+                                    const double *delta, const float *vol, EntryDesc *desc)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
         const unsigned long long k = keys[i];
         if (k == invalid) continue;
         const int32_t s = vals[i];
-        const int2 rs = scans[i];
-        const uint32_t D = (uint32_t)(rs.x - scans[rs.y].x);
+        const uint32_t D = (uint32_t)(runscan[i] - runscan[segscan[i]]);
         bool lst = true;
         if (i + 1 < nslots) lst = keys[i + 1] != k || vals[i + 1] / cap != s / cap;
         const bool fst = i == 0 || keys[i - 1] != k || vals[i - 1] / cap != s / cap;
@@ -250,9 +241,6 @@ size_t ordered_temp_bytes(long long nslots, long long max_wave)
 {
     size_t a = 0, b = 0, c = 0, d = 0, x = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, x, (int64_t *)nullptr, (long long *)nullptr, (int)max_wave);
-    size_t y = 0;
-    cub::DeviceScan::InclusiveScan(nullptr, y, (int2 *)nullptr, (int2 *)nullptr, RunSegOp{}, (int)nslots);
-    x = x > y ? x : y;
     cub::DeviceRadixSort::SortPairs(nullptr, a, (unsigned long long *)nullptr, (unsigned long long *)nullptr, (int32_t *)nullptr,
                                     (int32_t *)nullptr, (int)nslots);
     cub::DeviceScan::InclusiveSum(nullptr, b, (int32_t *)nullptr, (int32_t *)nullptr, (int)nslots);
@@ -661,12 +649,30 @@ __global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_k
 // gathers what its entry adds into arrays in sorted order (one thread a slot, all loads in flight at
 // once); then one thread a cell sums its run of those arrays in order (contiguous reads).
 // ---------------------------------------------------------------------------
+__global__ void ordered_gather_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
+                                      unsigned long long invalid, FinishRows g)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nslots; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[i];
+        if (key == invalid) continue;
+        const int32_t s = vals[i], q = s / a.cap;
+        const bool active = !a.mask || a.mask[key] == PGE_MASK_ACTIVE;
+        const float v = a.vol[s];
+        const bool track = active && v > 0.0f;
+        g.v[i] = track ? v : 0.0f;
+        g.m0[i] = track ? a.mom[2 * (long long)s] : 0.0f;
+        g.m1[i] = track ? a.mom[2 * (long long)s + 1] : 0.0f;
+        const double amt = a.act[s];
+        g.amt[i] = a.delta[s] < 0.0 ? -amt : amt;  // the sign says erosion (an eroded 0 is -0)
+        g.kp[i] = (a.desc[s].dflags & ENTRY_LAST) && a.dth[q] == (int32_t)key ? a.keep[q] : -1.0;  // keep >= 0
+    }
+}
+
 // One warp per 32 consecutive sorted slots; the warp walks every cell run that starts in its slots, 32
-// entries at a time: the lanes load a step's entries at once (each lane one slot's volume, momentum,
-// applied amount and stockpile), then every lane adds them in lane order (the float64 sums in the serial
-// order, the additions shuffled out of the lanes), the integer totals per lane
-__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys, const int32_t *vals,
-                                      unsigned long long invalid)
+// entries at a time: the lanes load a step's rows at once, then every lane adds them in lane order (the
+// float64 sums in the serial order, the additions shuffled out of the lanes), the integer totals per lane
+__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys,
+                                      unsigned long long invalid, FinishRows g)
 {
     __shared__ unsigned long long sfx[2];
     if (threadIdx.x < 2) sfx[threadIdx.x] = 0ull;
@@ -688,26 +694,21 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
             const long long c = (long long)key;
             double *accp = a.acc4 + 4 * c;
             double tq = accp[1], ta = accp[2], tb = accp[3], pd = a.pend[c];
-            const bool active = !a.mask || a.mask[c] == PGE_MASK_ACTIVE;
             for (long long j0 = base + hl;; j0 += 32) {
                 const long long j = j0 + lane;
                 const bool in = j < nslots && keys[j] == key;
                 float v = 0.0f, m0 = 0.0f, m1 = 0.0f;
-                double kp = -1.0;  // the droplet's stockpile where this is its last visit to its stockpile cell
+                double kp = -1.0;
                 if (in) {
-                    const int32_t sl = vals[j], q = sl / a.cap;
-                    const float vs = a.vol[sl];
-                    if (active && vs > 0.0f) {  // a step of volume > 0 on an active cell
-                        v = vs;
-                        m0 = a.mom[2 * (long long)sl];
-                        m1 = a.mom[2 * (long long)sl + 1];
-                    }
-                    if ((a.desc[sl].dflags & ENTRY_LAST) && a.dth[q] == (int32_t)key) kp = a.keep[q];
-                    const double amt = a.act[sl];
-                    if (a.delta[sl] < 0.0)
-                        eroded += fx_mass(amt);
+                    v = g.v[j];
+                    m0 = g.m0[j];
+                    m1 = g.m1[j];
+                    kp = g.kp[j];
+                    const double x = g.amt[j];
+                    if (signbit(x))
+                        eroded += fx_mass(-x);
                     else
-                        deposited += fx_mass(amt);
+                        deposited += fx_mass(x);
                 }
                 // the run covers a prefix of the lanes (keys are sorted)
                 const int n = __popc(__ballot_sync(full, in));
@@ -716,7 +717,7 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
                     const float at = __shfl_sync(full, m0, t);
                     const float bt = __shfl_sync(full, m1, t);
                     const double kt = __shfl_sync(full, kp, t);
-                    if (vt > 0.0f) {  // a step of volume > 0 on an active cell (0 otherwise)
+                    if (vt > 0.0f) {  // a step of volume > 0 on an active cell (gathered as 0 otherwise)
                         tq += (double)vt;
                         ta += (double)at;
                         tb += (double)bt;
@@ -733,7 +734,7 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
                 const unsigned long long *hw = reinterpret_cast<const unsigned long long *>(a.hand + c);
                 const double acc = hand_acc(hw[0], hw[1]);
                 accp[0] = acc;
-                if (active) {
+                if (!a.mask || a.mask[c] == PGE_MASK_ACTIVE) {
                     const float surf = (float)(a.L[c].x + acc);
                     a.A[c].x = surf;
                     const double sd = a.sediment[c] + acc;
@@ -803,14 +804,13 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     tb = w.temp_bytes;
     e = cub::DeviceRadixSort::SortPairs(w.temp, tb, w.keys_in, w.keys_out, w.vals_in, w.vals_out, (int)nslots, 0, w.end_bit, st);
     if (e != cudaSuccess) return e;
-    // the flags in the sort's input keys (free once sorted), their scans in the applied amounts (written by the apply)
-    int2 *pairs = reinterpret_cast<int2 *>(w.keys_in);
-    int2 *scans = reinterpret_cast<int2 *>(w.a.act);
-    ordered_flags_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, pairs);
+    ordered_flags_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runstart, w.segpos);
     tb = w.temp_bytes;
-    if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, pairs, scans, RunSegOp{}, (int)nslots, st)) != cudaSuccess) return e;
-    ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, scans, w.a.delta,
-                                                          w.a.vol, const_cast<EntryDesc *>(w.a.desc));
+    if ((e = cub::DeviceScan::InclusiveSum(w.temp, tb, w.runstart, w.runscan, (int)nslots, st)) != cudaSuccess) return e;
+    tb = w.temp_bytes;
+    if ((e = cub::DeviceScan::InclusiveScan(w.temp, tb, w.segpos, w.segscan, MaxOp{}, (int)nslots, st)) != cudaSuccess) return e;
+    ordered_rank_kernel<<<grid_for(nslots), 256, 0, st>>>(nslots, w.keys_out, w.vals_out, w.cap, w.invalid, w.runscan, w.segscan,
+                                                          w.a.delta, w.a.vol, const_cast<EntryDesc *>(w.a.desc));
     const bool lake = w.a.lakes && w.a.R;
     const long long warps = (w.nw + w.a.lanes - 1) / w.a.lanes;  // a lane per droplet
     long long blocks = (warps * 32 + APPLY_THREADS - 1) / APPLY_THREADS;
@@ -824,7 +824,15 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
         ordered_apply_kernel<false, true><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
     else
         ordered_apply_kernel<false, false><<<(int)blocks, APPLY_THREADS, smem, st>>>(w.a);
-    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid);
+    // the sort's input keys and the scans' buffers are free again: the gathered rows live there
+    FinishRows g;
+    g.v = reinterpret_cast<float *>(w.runstart);
+    g.m0 = reinterpret_cast<float *>(w.segpos);
+    g.m1 = reinterpret_cast<float *>(w.runscan);
+    g.amt = reinterpret_cast<double *>(w.keys_in);
+    g.kp = w.fin_kp;
+    ordered_gather_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid, g);
+    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.invalid, g);
     return cudaPeekAtLastError();
 }
 

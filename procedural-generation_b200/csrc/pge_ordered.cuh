@@ -83,6 +83,13 @@ struct ParkWave {
     size_t temp_bytes;
 };
 
+// what each sorted slot adds to its cell, gathered in sorted order for the finish
+struct FinishRows {
+    float *v, *m0, *m1;  // step volume and momentum (0 unless a step of volume > 0 on an active cell)
+    double *amt;         // the amount applied, negative for an erosion entry
+    double *kp;          // the droplet's stockpile where this is its last visit to its stockpile cell, else -1
+};
+
 struct OrderedWave {
     OrderedArgs a;
     long long nw;
@@ -93,6 +100,7 @@ struct OrderedWave {
     void *temp;
     size_t temp_bytes;
     long long max_blocks;
+    double *fin_kp;  // one double a slot: the gathered stockpile amounts
     // long lists: the recorded entries compacted before the ranks (nullptr: every slot goes through them);
     // max_wave + 1 int64: each droplet's first entry, then the wave's total
     long long *offsets;
