@@ -1126,8 +1126,9 @@ def apply_spawns(state: ErosionState, params, sp_face, sp_x, sp_y, sp_sed, sp_di
     ep = erosion_group(params)
     P = int(len(sp_face))
     max_steps = max_steps_of(ep, state.N)
-    w = default_wave(ep, P) if wave is None else int(wave)
-    state.reserve(P, list_steps_of(ep, state.N), w if apply == _lib.APPLY_ORDERED else 1, wave_tables=apply == _lib.APPLY_WAVE)
+    w = max(1, default_wave(ep, P) if wave is None else int(wave))  # (no spawns: one empty wave)
+    state.reserve(max(P, 1), list_steps_of(ep, state.N), w if apply == _lib.APPLY_ORDERED else 1,
+                  wave_tables=apply == _lib.APPLY_WAVE)
     L = _lib.load()
     dev = state.height.device
     sp = state._spawn
