@@ -552,7 +552,7 @@ def make_params(state: ErosionState, ep, volume0: float, P: int, wave: int, prec
         disc_saturation=float(ep.disc_saturation if disc_sat is None else disc_sat), disc_exponent=float(ep.disc_exponent),
         slope_gain=float(ep.slope_gain), slope_sat=float(ep.slope_saturation), erodibility=float(ep.erodibility),
         cover_depth=cell_units(ep, "cover_depth", u), min_volume=float(ep.min_volume_frac) * float(volume0),
-        max_erode=cell_units(ep, "max_erode", u), conc_scale=float(wave / (volume0 * P)), ocean_rate=float(ep.ocean_deposition_rate),
+        max_erode=cell_units(ep, "max_erode", u), conc_scale=float(wave / (volume0 * P)) if P > 0 and volume0 > 0.0 else 0.0, ocean_rate=float(ep.ocean_deposition_rate),
         fan_room=cell_units(ep, "fan_room", u), dep_floor=cell_units(ep, "dep_floor_m", u), iter_erode=cell_units(ep, "iter_erode", u),
         iter_deposit=float(cell_units(ep, "iter_deposit", u) if iter_deposit is None else iter_deposit),
         fan_slope=float(ep.fan_slope), offshore_writeoff=float(ep.offshore_writeoff), ema=float(ep.ema),
