@@ -140,3 +140,32 @@ def test_active_volcanoes_are_taken_off_and_put_back(cuda, tmp_path):
     np.testing.assert_allclose(ha, hb + cone[:, H:H + N, H:H + N], rtol=0, atol=1e-3)
     for n in ("sediment", "discharge", "momentum"):
         assert out(sa, n).tobytes() == out(sb, n).tobytes(), n
+
+
+def test_lake_parks_are_checkpointed_and_resumed(cuda, tmp_path):
+    """The bake's default lakes (lake_balance with lake_fill: loads parked in
+    the lakes, laid over their floors at each refresh and at the end): the
+    parked loads, the lakes' numbers and rooms are part of the checkpoint
+    (run.py:104-128, 200-224) and a resumed run lands on the continuous run's
+    outputs byte for byte."""
+    import dataclasses
+
+    w = synth.earth_world(seed=11, N=32, H=2, cell_size_m=50.0, land_fraction=0.45)
+    st = stage.LocalStore(tmp_path)
+    for name in ("bedrock", "hardness", "precip", "evap", "uplift"):
+        st.save_field(name, getattr(w, name), w.grid.H)
+    _, p = _world_store(tmp_path / "unused")
+    p = dataclasses.replace(p, erosion=dataclasses.replace(p.erosion, flood_every=2, sea_mask_every=2, lake_balance=True,
+                                                           lake_fill=True, basin_fill_grade=0.1))
+    info = stage.run(st, p, log=lambda m: None)
+    assert info.get("lakes_end") is not None
+    with np.load(st.checkpoint_dir / "erosion_iter0003.npz") as z:
+        assert {"lake_load", "lake_id", "lake_room", "lake_flag"} <= set(z.files)
+        assert (z["lake_id"] >= 0).any() and z["lake_room"].size >= 1
+    out = {n: np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)]) for n in stage.OUTPUTS}
+    for suf in (".npz", ".json"):
+        (st.checkpoint_dir / f"erosion_iter0006{suf}").unlink()
+    stage.run(st, p, log=lambda m: None)
+    for n in stage.OUTPUTS:
+        again = np.stack([np.load(st.coarse / f"{n}.f{k}.npy") for k in range(6)])
+        assert again.tobytes() == out[n].tobytes(), n
