@@ -93,7 +93,7 @@ __device__ __forceinline__ void hand_store(double2 *p, double acc, uint32_t coun
 {
     unsigned long long w0, w1;
     hand_pack(acc, count, w0, w1);
-    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" : : "l"(p), "l"(w0), "l"(w1) : "memory");
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" : : "l"(p), "l"(w0), "l"(w1));
 }
 
 // wait until the D earlier droplets of this wave that visit cell c have handed it on; acc = its net change
@@ -127,15 +127,18 @@ __device__ __forceinline__ double own_value(const double2 *hand, long long c)
 // asynchronous copies into shared memory: the waits count copy groups, so waiting for an old
 // entry's data never waits for the copies issued after it
 __device__ __forceinline__ uint32_t sm_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// (the copies and the commit carry no memory clobber: a ring slot is only read after the group wait that
+// covers its copy, and that wait is the compiler barrier; the compiler may then overlap a copy's issue
+// with the arithmetic around it)
 __device__ __forceinline__ void cp_ca8(void *d, const void *g)
 {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)));
 }
 __device__ __forceinline__ void cp_cg16(void *d, const void *g)
 {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sm_addr(d)), "l"(__cvta_generic_to_global(g)));
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;"); }
 template <int N>
 __device__ __forceinline__ void cp_wait()
 {
@@ -367,6 +370,35 @@ __device__ __forceinline__ void stage_cell(const OrderedArgs &a, Slot &s)
     if (LAKE) cp_ca8(&s.route, a.R + c);
 }
 
+// one entry's slot as registers: read one entry before it is applied, while the entry before it
+// computes, so that the apply's chain from entry to entry holds only its arithmetic
+struct Ent {
+    int32_t c;
+    uint32_t df;
+    double dlt, hs, cap;
+    float base;
+    uint32_t active;
+    unsigned long long h0, h1;
+    float2 route;
+};
+
+template <bool ECAP, bool LAKE>
+__device__ __forceinline__ Ent load_ent(const Slot &s)
+{
+    Ent e;
+    e.c = s.d.cell;
+    e.df = s.d.dflags;
+    e.dlt = s.d.delta;
+    e.hs = s.t.hs;
+    e.base = s.t.base;
+    e.active = s.t.active;
+    e.h0 = s.h0;
+    e.h1 = s.h1;
+    e.cap = ECAP ? s.cap : 0.0;
+    e.route = LAKE ? s.route : make_float2(0.f, 0.f);
+    return e;
+}
+
 // per droplet state carried from entry to entry
 struct Walk {
     double deficit, surplus, prev_live, acc_c;
@@ -575,35 +607,37 @@ __global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_k
         w.w1v = w.w2v = w.w3v = 0.0;
         w.sub_death = w.has_prev = w.have_c = false;
         w.ok = true;
+        Ent cur = load_ent<ECAP, LAKE>(R[0]);
         for (int k = 0; k < K; k++) {
             // the copies issued LOOKAHEAD + 1 or more entries ago have landed: the descriptor of entry
             // k + CELL_AHEAD and the cell data of entries k and k + 1
             cp_wait<LOOKAHEAD>();
+            const bool has_next = k + 1 < K;
+            Ent nx;
+            nx.c = -1;
+            if (has_next) nx = load_ent<ECAP, LAKE>(R[(k + 1) & (RING - 1)]);
             if (k + CELL_AHEAD < K) stage_cell<ECAP, LAKE>(a, R[(k + CELL_AHEAD) & (RING - 1)]);
             if (k + DESC_AHEAD < K) stage_desc(a, R[(k + DESC_AHEAD) & (RING - 1)], b0 + k + DESC_AHEAD);
             cp_commit();
-            const Slot &cur = R[k & (RING - 1)];
-            const Slot &nx = R[(k + 1) & (RING - 1)];
-            const bool has_next = k + 1 < K;
-            const int32_t c = cur.d.cell;
-            const uint32_t df = cur.d.dflags;
-            const double dlt = cur.d.delta;
-            const double hs = cur.t.hs;
-            const double b_c = (double)cur.t.base;
+            const int32_t c = cur.c;
+            const uint32_t df = cur.df;
+            const double dlt = cur.dlt;
+            const double hs = cur.hs;
+            const double b_c = (double)cur.base;
             const bool park = (df & ENTRY_PARK) != 0;  // a lake park changes no terrain (particle.py:912-933)
-            const bool act = cur.t.active != 0 && !park;
+            const bool act = cur.active != 0 && !park;
             if (!w.have_c && !(w.ok = cell_value(a, w, c, df, cur.h0, cur.h1, w.acc_c))) break;
             // an erosion entry (floor) and a final deposit (ceiling) read the next entry's cell live:
             // acquire it now; a step deposit does not, and acquires it only before writing it
             const bool is_step = (df & ENTRY_STEP) != 0;
             const bool reads_next = has_next && !park && (dlt < 0.0 || !is_step);
-            const int32_t ncell = has_next ? nx.d.cell : -1;
+            const int32_t ncell = nx.c;
             double acc_n = 0.0, hs_n = 0.0;
             if (reads_next) {
-                hs_n = nx.t.hs;
+                hs_n = nx.hs;
                 if (ncell == c)
                     acc_n = w.acc_c;
-                else if (!(w.ok = cell_value(a, w, ncell, nx.d.dflags, nx.h0, nx.h1, acc_n)))
+                else if (!(w.ok = cell_value(a, w, ncell, nx.df, nx.h0, nx.h1, acc_n)))
                     break;
             }
             const double acc = w.acc_c;
@@ -629,6 +663,7 @@ __global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_k
                 w.have_c = reads_next;
                 w.acc_c = acc_n;
             }
+            cur = nx;
         }
         cp_wait<0>();
         if (!w.ok) {
