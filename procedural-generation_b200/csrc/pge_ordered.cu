@@ -89,6 +89,12 @@ __device__ __forceinline__ void hand_load(const double2 *p, unsigned long long &
     asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(p) : "memory");
 }
 
+// the same read issued ahead of its use: no compiler barrier, the thread waits only where it uses the word
+__device__ __forceinline__ void hand_load_ahead(const double2 *p, unsigned long long &w0, unsigned long long &w1)
+{
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w0), "=l"(w1) : "l"(p));
+}
+
 __device__ __forceinline__ void hand_store(double2 *p, double acc, uint32_t count)
 {
     unsigned long long w0, w1;
@@ -351,7 +357,7 @@ constexpr int APPLY_THREADS = 64;
 // one entry of a droplet's list as the apply reads it, filled by asynchronous copies
 struct alignas(16) Slot {
     EntryDesc d;                // descriptor
-    unsigned long long h0, h1;  // the cell's hand-off word as prefetched
+    unsigned long long spare[2];  // (the hand-off word is read into registers instead)
     CellTerr t;                 // the cell's read-only terrain
     double cap;                 // the slope erode cap (when on)
     float2 route;               // the cell's packed routing surface and flag (with lakes)
@@ -364,7 +370,6 @@ template <bool ECAP, bool LAKE>
 __device__ __forceinline__ void stage_cell(const OrderedArgs &a, Slot &s)
 {
     const long long c = s.d.cell;
-    cp_cg16(&s.h0, a.hand + c);
     cp_cg16(&s.t, a.terr + c);
     if (ECAP) cp_ca8(&s.cap, a.ecap + c);
     if (LAKE) cp_ca8(&s.route, a.R + c);
@@ -392,8 +397,7 @@ __device__ __forceinline__ Ent load_ent(const Slot &s)
     e.hs = s.t.hs;
     e.base = s.t.base;
     e.active = s.t.active;
-    e.h0 = s.h0;
-    e.h1 = s.h1;
+    e.h0 = e.h1 = 0ull;  // read separately, one entry ahead
     e.cap = ECAP ? s.cap : 0.0;
     e.route = LAKE ? s.route : make_float2(0.f, 0.f);
     return e;
@@ -607,7 +611,12 @@ __global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_k
         w.w1v = w.w2v = w.w3v = 0.0;
         w.sub_death = w.has_prev = w.have_c = false;
         w.ok = true;
+        // the hand-off words are read into registers one entry ahead of the entry that first reads them
+        // (the terrain three ahead, through the ring): a word read later is less often stale
+        unsigned long long p0 = 0ull, p1 = 0ull;
         Ent cur = load_ent<ECAP, LAKE>(R[0]);
+        hand_load_ahead(a.hand + cur.c, cur.h0, cur.h1);
+        if (K > 1) hand_load_ahead(a.hand + R[1].d.cell, p0, p1);
         for (int k = 0; k < K; k++) {
             // the copies issued LOOKAHEAD + 1 or more entries ago have landed: the descriptor of entry
             // k + CELL_AHEAD and the cell data of entries k and k + 1
@@ -615,7 +624,13 @@ __global__ void __launch_bounds__(APPLY_THREADS, PGE_APPLY_MINB) ordered_apply_k
             const bool has_next = k + 1 < K;
             Ent nx;
             nx.c = -1;
-            if (has_next) nx = load_ent<ECAP, LAKE>(R[(k + 1) & (RING - 1)]);
+            if (has_next) {
+                nx = load_ent<ECAP, LAKE>(R[(k + 1) & (RING - 1)]);
+                nx.h0 = p0;
+                nx.h1 = p1;
+            }
+            // entry k + 2's descriptor landed with the group waited for above
+            if (k + 2 < K) hand_load_ahead(a.hand + R[(k + 2) & (RING - 1)].d.cell, p0, p1);
             if (k + CELL_AHEAD < K) stage_cell<ECAP, LAKE>(a, R[(k + CELL_AHEAD) & (RING - 1)]);
             if (k + DESC_AHEAD < K) stage_desc(a, R[(k + DESC_AHEAD) & (RING - 1)], b0 + k + DESC_AHEAD);
             cp_commit();
