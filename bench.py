@@ -10,8 +10,8 @@ that reaches the mass-transfer section).  Data: seeded synthetic world.
 Arms
   default          the CUDA library (libpgerosion.so) through pgerosion.maps
   --impl reference the reference algorithm's CPU restatement (the oracle, a
-                   port of the numba code; the numba code itself cannot run
-                   on the GPU box), timed on all host cores
+                   port of the numba code; numba itself is not installed
+                   where the bench runs), timed on all host cores
 
 Multi-GPU: ``torchrun --nproc-per-node N bench.py --gpus N``: every rank
 erodes its own world (seed = rank), no collective on the data path (weak

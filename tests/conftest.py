@@ -19,6 +19,6 @@ def cuda():
     import torch
 
     # GPU tests fail rather than skip without a device: a skipped parity test
-    # must never read as a pass on the GPU box
+    # must never read as a pass on a machine with a GPU
     assert torch.cuda.is_available(), "this test needs a CUDA device"
     return torch.device("cuda:0")

@@ -32,7 +32,7 @@ def test_stage_run_checkpoints_and_resume(cuda, tmp_path):
     with np.load(st.checkpoint_dir / "erosion_iter0006.npz") as z:
         assert set(z.files) >= {"height", "sediment", "discharge", "momentum", "pending", "lake_load"}
         assert z["height"].dtype == np.float64
-    # drop the last checkpoint: the driver resumes from iteration 3 and lands on the same outputs
+    # drop the last checkpoint: the stage resumes from iteration 3 and lands on the same outputs
     for suf in (".npz", ".json"):
         (st.checkpoint_dir / f"erosion_iter0006{suf}").unlink()
     msgs = []
