@@ -485,10 +485,13 @@ def run_b200(args, rank, world_size, dist):
     per_launch_steps = steps_done / max(args.steps, 1)
     avg_ta = float(np.mean(ta_ms))
     achieved = per_launch_steps * BYTES_PER_STEP / (avg_ta * 1e-3) / 1e9
-    # DRAM bytes per droplet pass: ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches flushed
-    # before each kernel) over one exact pass of the N_c = 256 world measured 31.95 MB per wave;
-    # the per-wave workspace is fixed, so the pass's traffic scales with its waves
-    traffic = TRAFFIC_PER_WAVE * n_waves / max(args.steps, 1) if apply == _lib.APPLY_ORDERED else None
+    # DRAM bytes per droplet pass, from ncu (dram__bytes_read.sum + dram__bytes_write.sum) over the waves of an
+    # exact pass of the N_c = 256 world: with the caches kept from kernel to kernel, as the live pass runs, 40 B
+    # a droplet-step (scaled by the pass's droplet-steps); with ncu's flush before every kernel, 33.7 MB a wave
+    # (the per-wave workspace is fixed, so that one scales with the waves)
+    exact = apply == _lib.APPLY_ORDERED
+    traffic = TRAFFIC_PER_STEP * per_launch_steps if exact else None
+    traffic_cold = TRAFFIC_PER_WAVE_COLD * n_waves / max(args.steps, 1) if exact else None
     out = {
         "metric": "droplet-steps/s", "value": steps_all / (ms_max * 1e-3), "unit": "droplet-steps/s", "n_gpus": world_size,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -502,7 +505,7 @@ def run_b200(args, rank, world_size, dist):
         "e2e": {"value": e2e_all / (e2e_ms_max * 1e-3), "unit": "droplet-steps/s", "h2d_bytes_per_step": h2d // max(args.steps, 1),
                 "d2h_bytes_per_step": d2h // max(args.steps, 1)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_cold": traffic_cold, "peak_kind": peak_kind,
                      "kernel": "droplet pass (pge_trace_apply: trace waves, ordered apply or wave refreshes, pack, fold)",
                      "ms_per_launch": avg_ta, "bytes_per_step": BYTES_PER_STEP},
         "gpu_launches": launches_per_iteration(max(n_waves // max(args.steps, 1), 1), pend_any, params.erosion.creep_rate > 0,
@@ -704,8 +707,10 @@ def main():
 
 #: droplets per wave of the default run (0 = the reference's chunk of 2048)
 DEFAULT_WAVE = 0
-#: DRAM bytes per ordered-apply wave (trace, sort, ranks, apply, finish), from an ncu capture
-TRAFFIC_PER_WAVE = 33.7e6
+#: DRAM bytes of the exact pass (trace, sort, ranks, apply, finish) per droplet-step, caches kept between
+#: kernels, and per wave with the caches flushed before every kernel; both from ncu captures of the N_c = 256 pass
+TRAFFIC_PER_STEP = 40.0
+TRAFFIC_PER_WAVE_COLD = 33.7e6
 
 if __name__ == "__main__":
     main()
