@@ -721,14 +721,20 @@ __global__ void ordered_gather_kernel(const OrderedArgs a, long long nslots, con
 // One warp per 32 consecutive sorted slots; the warp walks every cell run that starts in its slots, 32
 // entries at a time: the lanes load a step's rows at once, then every lane adds them in lane order (the
 // float64 sums in the serial order, the additions shuffled out of the lanes), the integer totals per lane
-__global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys,
+constexpr int FINISH_THREADS = 256, FINISH_WARPS = FINISH_THREADS / 32;
+
+__global__ void __launch_bounds__(FINISH_THREADS) ordered_finish_kernel(const OrderedArgs a, long long nslots, const unsigned long long *keys,
                                       unsigned long long invalid, FinishRows g)
 {
     __shared__ unsigned long long sfx[2];
+    // each warp's window of its run, read in order by every lane (broadcast reads: the loads of later slots
+    // go out ahead of the float64 sums, which keep the serial order)
+    __shared__ float sv[FINISH_WARPS][32], sa[FINISH_WARPS][32], sb[FINISH_WARPS][32];
+    __shared__ double sk[FINISH_WARPS][32];
     if (threadIdx.x < 2) sfx[threadIdx.x] = 0ull;
     __syncthreads();
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     long long eroded = 0, deposited = 0;
@@ -762,11 +768,17 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
                 }
                 // the run covers a prefix of the lanes (keys are sorted)
                 const int n = __popc(__ballot_sync(full, in));
+                sv[wib][lane] = v;
+                sa[wib][lane] = m0;
+                sb[wib][lane] = m1;
+                sk[wib][lane] = kp;
+                __syncwarp();
+#pragma unroll 4
                 for (int t = 0; t < n; t++) {
-                    const float vt = __shfl_sync(full, v, t);
-                    const float at = __shfl_sync(full, m0, t);
-                    const float bt = __shfl_sync(full, m1, t);
-                    const double kt = __shfl_sync(full, kp, t);
+                    const float vt = sv[wib][t];
+                    const float at = sa[wib][t];
+                    const float bt = sb[wib][t];
+                    const double kt = sk[wib][t];
                     if (vt > 0.0f) {  // a step of volume > 0 on an active cell (gathered as 0 otherwise)
                         tq += (double)vt;
                         ta += (double)at;
@@ -774,6 +786,7 @@ __global__ void ordered_finish_kernel(const OrderedArgs a, long long nslots, con
                     }
                     if (kt >= 0.0) pd += kt;
                 }
+                __syncwarp();  // every lane has read the window before the next one is written
                 if (n < 32) break;
             }
             if (lane == 0) {
@@ -882,7 +895,7 @@ cudaError_t ordered_wave(const OrderedWave &w, cudaStream_t st)
     g.amt = reinterpret_cast<double *>(w.keys_in);
     g.kp = w.fin_kp;
     ordered_gather_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.vals_out, w.invalid, g);
-    ordered_finish_kernel<<<grid_for(nslots), 256, 0, st>>>(w.a, nslots, w.keys_out, w.invalid, g);
+    ordered_finish_kernel<<<grid_for(nslots, FINISH_THREADS), FINISH_THREADS, 0, st>>>(w.a, nslots, w.keys_out, w.invalid, g);
     return cudaPeekAtLastError();
 }
 
