@@ -644,7 +644,8 @@ def main():
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="droplet kernel: 2 selects the two-blocks-per-SM variant")
     ap.add_argument("--apply", default="ordered", choices=("ordered", "wave"),
                     help="ordered: the reference's serial apply (default); wave: per-droplet ledgers against wave-start terrain")
-    ap.add_argument("--n", type=int, default=None, help="override N_c (tests)")
+    ap.add_argument("--n", "--nc", dest="n", type=int, default=None,
+                    help="override N_c (tests; under torchrun use --nc, which torchrun's own options do not abbreviate)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-alt", action="store_true", help="skip the secondary wave-apply measurement")
     ap.add_argument("--alt-steps", type=int, default=5)

@@ -26,3 +26,22 @@ def test_reference_arm_prints_one_result_line():
     assert d["config"]["N_c"] == 32 and d["config"]["workload"].startswith("plain erosion iteration, cube-sphere N_c=32")
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "droplet-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_under_torchrun_prints_on_rank_zero_only():
+    """Launched as the multi-GPU runs are (torchrun, two ranks here on the CPU): rank 0 alone runs the
+    reference and prints its line; the other rank exits 0 without work."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="", OMP_NUM_THREADS="1")
+    out = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+                          "--master-addr", "127.0.0.1", "--master-port", str(port), str(ROOT / "bench.py"), "--impl",
+                          "reference", "--gpus", "2", "--nc", "32", "--steps", "1", "--warmup", "3"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    assert json.loads(lines[0])["impl"] == "reference"
